@@ -1,0 +1,358 @@
+#!/usr/bin/env python
+"""Benchmark of the ParaTC per-RK3-substep hot path on B200.
+
+Metric: grid-point RK3 substeps/s = cells x substeps / device time, whole job.
+Workload (default): the closed turbulent channel 128 x 96 x 128 (Re_b = 5600,
+4pi x 2 x 4pi/3, tanh y-grid, RK3, dt = 0.005, constant flow rate, FP64),
+seeded Poiseuille + U(-0.3, 0.3) noise made solenoidal by one projection.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One process per GPU (torchrun for N > 1); every rank advances its own channel
+replica (weak scaling, no data-path collective); the timed region is
+bracketed by a barrier and a device synchronisation and its length is the max
+over ranks.  Between timed steps the L2 is flushed by writing a 256 MB buffer
+(outside the events).  --impl reference times the CPU restatement of the
+reference on all host cores (the reference itself, Fortran + MPI, cannot be
+built on this image).
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "grid-point RK3 substeps/s"
+UNIT = "grid-point substeps/s"
+L2_BYTES = 126 * 1024 * 1024
+
+
+def _args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", default="channel_c1")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    return ap.parse_args()
+
+
+def _case(name):
+    from paratc_b200 import cases
+    if name == "channel_c1":
+        return cases.channel_c1()
+    if name == "turbidity_c5":
+        return cases.turbidity_c5()
+    if name == "lock_exchange_c3":
+        return cases.lock_exchange_c3()
+    raise SystemExit("unknown workload " + name)
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def _traffic_table():
+    """Per-launch DRAM bytes of ncu captures: profiles/ncu_traffic.txt lines
+    '<workload> <kernel class> <bytes per launch>'."""
+    out = {}
+    p = os.path.join(ROOT, "profiles", "ncu_traffic.txt")
+    if os.path.exists(p):
+        for line in open(p):
+            f = line.split()
+            if len(f) == 3 and not line.startswith("#"):
+                out[(f[0], f[1])] = float(f[2])
+    return out
+
+
+def algorithmic_bytes(params):
+    """Compulsory HBM bytes per launch of each kernel class (FP64 words of 8 B,
+    N cells; spectral arrays hold (nx/2+1)*ny*nz complex values)."""
+    N = params.nxc * params.nyc * params.nzc
+    S = 2 * (params.nxc // 2 + 1) * params.nyc * params.nzc  # doubles in the spectral array
+    sc = 1 if params.scalar_on else 0
+    w = 8
+    return {
+        "rhs": (7 + 6 + 4 * sc) * w * N,          # u,v,w,p,H* in; Rhs*,H* out
+        "helmholtz": 9 * w * N,                   # Rhs*, u* in; u* out
+        "helmholtz_scalar": 3 * w * N,
+        "prsrc": 4 * w * N,                       # u,v,w in; src out
+        "fft_x_fwd": w * (N + S),
+        "fft_z_fwd": 2 * w * S,
+        "ysolve": 2 * w * S,
+        "fft_z_bwd": 2 * w * S,
+        "fft_x_bwd": w * (S + N),
+        "project": 9 * w * N,                     # phi,u,v,w,p in; u,v,w,p out
+        "cfl": 3 * w * N,
+        "check": (3 + sc) * w * N,
+    }
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons every 200 ms during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.th = threading.Thread(target=self._read, daemon=True)
+            self.th.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) >= 9:
+                self.rows.append(f)
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[5 + i].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def _dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def cpu_baseline(case, yp, fields, seconds, max_steps=200):
+    """The oracle (CPU restatement of the reference) on all host threads."""
+    from oracle import oracle_lib as ol
+    threads = os.cpu_count() or 1
+    o = ol.Oracle(case.params, yp, threads=threads)
+    o.set_fields(fields["ux"], fields["uy"], fields["uz"], fields["p"], fields["c"])
+    o.project()
+    o.step()  # warm-up
+    n = 0
+    t0 = time.perf_counter()
+    while True:
+        o.step()
+        n += 1
+        el = time.perf_counter() - t0
+        if el >= seconds or n >= max_steps:
+            break
+    o.close()
+    iad = {1: 1, 2: 2, 3: 3}[case.params.ischeme]
+    return {"value": case.n_cells * iad * n / el, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": "%d full RK3 steps of %s on the C oracle (OpenMP, %d threads), %.1f s" % (n, case.name, threads, el)}
+
+
+def run_reference(args):
+    ws, rank, _ = _dist()
+    if rank != 0:
+        return
+    from paratc_b200 import cases
+    from oracle import oracle_lib as ol
+    case = _case(args.workload)
+    m = case.mesh
+    yp = ol.ycoord(m.section_length, m.section_cstret, m.nyc_section, m.stret_type, m.stret_option, case.params.yly)
+    fields = cases.initial_fields(case, yp)
+    threads = os.cpu_count() or 1
+    o = ol.Oracle(case.params, yp, threads=threads)
+    o.set_fields(fields["ux"], fields["uy"], fields["uz"], fields["p"], fields["c"])
+    o.project()
+    for _ in range(args.warmup):
+        o.step()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        o.step()
+    el = time.perf_counter() - t0
+    iad = {1: 1, 2: 2, 3: 3}[case.params.ischeme]
+    val = case.n_cells * iad * args.steps / el
+    line = {"impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": case.name, "grid": [case.params.nxc, case.params.nyc, case.params.nzc],
+                       "scheme": "RK3", "precision": "fp64", "parallelism": "host threads"},
+            "cpu_baseline": {"value": val, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": "%d full RK3 steps of %s on the C oracle (OpenMP, %d threads)" % (args.steps, case.name, threads)},
+            "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args):
+    import torch
+    ws, rank, local = _dist()
+    torch.cuda.set_device(local)
+    dist = None
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    from paratc_b200 import cases
+    from paratc_b200.lib import ChannelSystem, mesh_ycoord
+    case = _case(args.workload)
+    case.seed = case.seed + rank
+    p = case.params
+    yp = mesh_ycoord(case.mesh, p.yly)
+    fields = cases.initial_fields(case, yp)
+    base = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        base = cpu_baseline(case, yp, fields, args.cpu_seconds)
+
+    ctx = ChannelSystem(p, yp, device=local)
+    ctx.set_fields(fields["ux"], fields["uy"], fields["uz"], fields["p"], fields["c"])
+    ctx.project()
+    stream = torch.cuda.ExternalStream(ctx.stream, device=local)
+    flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device=local)
+    iad = {1: 1, 2: 2, 3: 3}[p.ischeme]
+
+    for _ in range(args.warmup):
+        ctx.iterate_async(1)
+    ctx.last_diag()
+    torch.cuda.synchronize()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def timed_pass(profile):
+        if profile:
+            ctx.profile(True)
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+        l0 = ctx.launches
+        for i in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.add_(1.0)
+            ev[i][0].record(stream)
+            ctx.iterate_async(1)
+            ev[i][1].record(stream)
+        d = ctx.last_diag()
+        torch.cuda.synchronize()
+        launches = ctx.launches - l0
+        ms = [a.elapsed_time(b) for a, b in ev]
+        prof = ctx.profile_read() if profile else None
+        if profile:
+            ctx.profile(False)
+        return ms, d, launches, prof
+
+    barrier()
+    sampler = ClockSampler(local)
+    sampler.start()
+    ms, diag, launches, _ = timed_pass(False)
+    clocks = sampler.stop()
+    barrier()
+    total_ms = sum(ms)
+    if dist is not None:
+        t = torch.tensor([total_ms], dtype=torch.float64, device=local)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = ws * p.nxc * p.nyc * p.nzc * iad * args.steps / (total_ms / 1e3)
+
+    # per-kernel timing pass (same workload, events around every launch)
+    _, _, _, prof = timed_pass(True)
+    barrier()
+
+    # end to end through the C ABI with host buffers (pinned)
+    e2e = None
+    if not args.no_e2e:
+        names = ["ux", "uy", "uz", "p", "hx", "hy", "hz"] + (["c", "hc"] if p.scalar_on else [])
+        host = {n: torch.empty(ctx.shape, dtype=torch.float64, pin_memory=True).numpy() for n in names}
+        cur = ctx.get_fields(names)
+        for n in names:
+            host[n][...] = cur[n]
+        nbytes = sum(host[n].nbytes for n in names)
+        t_e2e = 0.0
+        barrier()
+        for i in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.add_(1.0)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            ctx.set_fields(host["ux"], host["uy"], host["uz"], host["p"], host.get("c"), host["hx"], host["hy"],
+                           host["hz"], host.get("hc"))
+            ctx.iterate(1)
+            ctx.get_fields_into(host)
+            t_e2e += time.perf_counter() - t0
+        if dist is not None:
+            t = torch.tensor([t_e2e], dtype=torch.float64, device=local)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            t_e2e = float(t.item())
+        e2e = {"value": ws * p.nxc * p.nyc * p.nzc * iad * args.steps / t_e2e, "unit": UNIT,
+               "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes + 12 * 8,
+               "note": "per step: paratc_set_fields (state from pinned host) + paratc_step + paratc_get_fields (state to host)"}
+
+    # roofline of the dominant kernel
+    peak, peak_kind = _peaks()
+    alg = algorithmic_bytes(p)
+    dom = max(prof.items(), key=lambda kv: kv[1][0])
+    kname, (kms, kn) = dom
+    avg_s = kms / kn / 1e3
+    ach = alg[kname] / avg_s / 1e9
+    traffic = _traffic_table().get((args.workload, kname))
+    share = {k: round(v[0] / sum(x[0] for x in prof.values()), 4) for k, v in sorted(prof.items(), key=lambda kv: -kv[1][0])}
+    roof = {"bound": "hbm", "kernel": kname, "achieved": round(ach, 1), "peak": peak, "unit": "GB/s",
+            "frac": round(ach / peak, 4), "traffic": traffic, "peak_kind": peak_kind,
+            "algorithmic_bytes_per_launch": alg[kname], "avg_launch_us": round(avg_s * 1e6, 2),
+            "kernel_share": share}
+    # whole-substep algorithmic bandwidth (every kernel's compulsory bytes / step time)
+    step_bytes = sum(alg[k] * v[1] for k, v in prof.items() if k in alg) / args.steps
+    roof["step_algorithmic_GBps"] = round(step_bytes / (statistics.mean(ms) / 1e3) / 1e9, 1)
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": case.name, "grid": [p.nxc, p.nyc, p.nzc], "scheme": "RK3",
+                           "precision": "fp64", "parallelism": "replicas x%d" % ws,
+                           "l2": "flushed between timed steps (256 MB write outside the events)",
+                           "divmax_last_step": diag.divmax},
+                "roofline": roof, "cpu_baseline": base, "e2e": e2e, "gpu_launches": launches, "clocks": clocks}
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = _args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

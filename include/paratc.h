@@ -1,0 +1,261 @@
+/*
+ * paratc.h -- C ABI of the B200-native ParaTC per-RK3-substep hot path.
+ *
+ * The hot path of ParaTC (GongZheng-Justin/ParaTC) is the explicit 4th-order
+ * staggered right-hand side (src/m_TScheme.f90), the implicit wall-normal
+ * Helmholtz tridiagonal solves (src/m_TScheme.f90:365-506 with
+ * src/m_Tools.f90:224-251), the FFT-tridiagonal pressure Poisson solve
+ * (src/m_Poisson.f90) and the wall/periodic boundary treatment
+ * (src/m_BC_and_Halo.f90).  In the reference these are Fortran module
+ * procedures called in a fixed order by ChannelIterate
+ * (src/m_ChannelSystem.f90:80-187); here they are one library whose entry
+ * points take plain pointers and sizes and return an int status.
+ *
+ * Conventions
+ *  - Every entry point returns PARATC_OK (0) or a negative PARATC_ERR_* code.
+ *    The reference aborts instead (MainLog%CheckForError(ErrT_Abort, ...),
+ *    src/m_LogInfo.f90; MPI_ABORT in src/m_Decomp2d.f90); a Fortran caller
+ *    maps a non-zero status to ErrT_Abort to keep that behaviour.
+ *  - Host arrays are FP64, Fortran order (x fastest, then y, then z).
+ *    PARATC_LAYOUT_INTERIOR: nxc*nyc*nzc values, indices ic=1..nxc,
+ *    jc=1..nyc, kc=1..nzc (the y1 pencil of one rank, y1start..y1end).
+ *    PARATC_LAYOUT_HALO: (nxc+4)*(nyc+2)*(nzc+4) values with the bounds
+ *    mb1%xmm:xpm = -1:nxc+2, ymm:ypm = 0:nyp, zmm:zpm = -1:nzc+2 that
+ *    myallocate gives the field arrays (src/m_Variables.f90:47-50,
+ *    src/m_Decomp2d.f90:1479-1549).
+ *  - A context is bound to one CUDA device and one stream. Calls on one
+ *    context must not run concurrently; different contexts are independent.
+ *  - The library owns all device memory of a context.
+ */
+#ifndef PARATC_H
+#define PARATC_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------- */
+#define PARATC_OK              0
+#define PARATC_ERR_BAD_ARG    -1  /* invalid size, option or pointer             */
+#define PARATC_ERR_OOM        -2  /* device or host allocation failed            */
+#define PARATC_ERR_CUDA       -3  /* a CUDA runtime call failed                  */
+#define PARATC_ERR_NONFINITE  -4  /* NaN/Inf found in a field                    */
+#define PARATC_ERR_DIV_LIMIT  -5  /* max|div u| > div_limit (ChannelIterate:143) */
+#define PARATC_ERR_VEL_LIMIT  -6  /* min(max|u_i|) > vel_limit (ChannelIterate:145) */
+#define PARATC_ERR_TIMEOUT    -7  /* a bounded device wait gave up               */
+#define PARATC_ERR_IO         -8  /* restart file missing, short or wrong size   */
+#define PARATC_ERR_NO_DEVICE  -9  /* no CUDA device / library built without one  */
+
+/* ---- option values (same numbers as src/m_Parameters.f90) ------------ */
+#define PARATC_FT_CH 1          /* FT_CH: channel, no-slip top and bottom   */
+#define PARATC_FT_HC 2          /* FT_HC: half channel, free-slip top       */
+#define PARATC_AB2   1          /* FI_AB2 */
+#define PARATC_RK2   2          /* FI_RK2 */
+#define PARATC_RK3   3          /* FI_RK3 */
+
+#define PARATC_LAYOUT_INTERIOR 0
+#define PARATC_LAYOUT_HALO     1
+
+/*
+ * Run-time parameters. The values are the ones the module m_Parameters holds
+ * after ReadAndInitParameters (src/m_Parameters.f90:112-188): uCRF is 0 unless
+ * IsUseCRF, uxBcValue already has uCRF subtracted, the scalar vectors are
+ * GravityEffVec = GravityDir*GravityEff and FallingVelVec = GravityDir*FallingVel
+ * (+uCRF in x), SDiffCoe = xnu/SchmidtNumber.  paratc_params_from_namelist()
+ * fills the struct from a ParaTC input file exactly that way.
+ */
+typedef struct paratc_params {
+    int32_t nxc, nyc, nzc;      /* cell counts: nxp-1, nyp-1, nzp-1            */
+    int32_t flow_type;          /* PARATC_FT_CH | PARATC_FT_HC                 */
+    int32_t ischeme;            /* PARATC_AB2 | PARATC_RK2 | PARATC_RK3        */
+    int32_t icfl;               /* 1: dt from CFLc, 2: dt = dtMax              */
+    int32_t is_ux_const;        /* IsUxConst: constant flow-rate forcing       */
+    int32_t scalar_on;          /* built with -DScalarFlow in the reference    */
+    double  xlx, yly, zlz;      /* domain lengths                              */
+    double  xnu;                /* kinematic viscosity                         */
+    double  ubulk;              /* bulk velocity                               */
+    double  ucrf;               /* uCRF (0 when IsUseCRF is false)             */
+    double  dt_max;             /* dtMax                                       */
+    double  cflc;               /* CFLc                                        */
+    double  gravity[3];         /* constant body force                         */
+    double  ux_bc[6], uy_bc[6], uz_bc[6];   /* u?BcValue, index 0..5 = x-,x+,y-,y+,z-,z+ */
+    double  vel_limit, div_limit;
+    /* ScalarFlow options (ignored when scalar_on == 0) */
+    double  sdiff;              /* SDiffCoe                                    */
+    double  gravity_eff_vec[3]; /* GravityEffVec                               */
+    double  falling_vel_vec[3]; /* FallingVelVec                               */
+    int32_t scalar_bc_option[2];/* -1 Dirichlet, -2 Neumann, -3 Robin; y-, y+  */
+    double  scalar_bc_values[4];/* F_b, F_t, S_b, S_t                          */
+    double  scalar_init_value;  /* Scalar_InitValue                            */
+} paratc_params;
+
+/* Per-step diagnostics, the numbers ChannelIterate logs
+ * (src/m_ChannelSystem.f90:172-183). */
+typedef struct paratc_diag {
+    double dt;            /* time step used by this step                       */
+    double cfl;           /* cflmp = uddxmax*dt_prev (ChannelIterate:93-94)    */
+    double sim_time;      /* SimTime after the step                            */
+    double divmax_src;    /* divmax1: max|div u*| seen by the last clcPrSrc    */
+    double divmax;        /* divmax2: CheckDivergence after the step           */
+    double vmax[3];       /* CalcVmax                                          */
+    double pr_grad_aver;  /* PrGradAver (mean pressure gradient of the step)   */
+    double ux_mean;       /* CalcUxAver / ClcMeanValue(1)                      */
+    double sc_mean;       /* ClcMeanValue(2) (0 without scalar)                */
+    double sc2_mean;      /* ClcMeanValue(3) raw mean of c^2 (0 without scalar)*/
+} paratc_diag;
+
+typedef struct paratc_ctx paratc_ctx;
+
+/* ---- set-up ------------------------------------------------------------ */
+
+/* clcYcoord for every section (src/m_MeshAndMetries.f90:143-181,340-408):
+ * fills yp[0..nyp-1] = yp(1..nyp) from the &MeshOptions arrays. */
+int paratc_mesh_ycoord(int nsection, const double* section_length,
+                       const double* section_cstret, const int32_t* nyc_section,
+                       const int32_t* stret_type, const int32_t* stret_option,
+                       double yly, double* yp_out);
+
+/* Reads &BasicParam, &MeshSection, &MeshOptions and (when scalar_on != 0)
+ * &ScalarFlowOptions from a ParaTC input file and applies the derivations
+ * of ReadAndInitParameters (src/m_Parameters.f90:112-188).  yp_out may be
+ * NULL (pass nyp_cap = 0); otherwise it receives yp(1..nyp). */
+int paratc_params_from_namelist(const char* path, int scalar_on,
+                                paratc_params* out, double* yp_out, int nyp_cap);
+
+/* Run control of &BasicParam that main.f90 / ChannelIterate use around the
+ * hot path (src/main.f90:31-33, src/m_ChannelSystem.f90:150-183). */
+typedef struct paratc_run_options {
+    int32_t ifirst, ilast;      /* iteration range                             */
+    int32_t restart_flag;       /* RestartFlag                                 */
+    int32_t backup_freq;        /* BackupFreq                                  */
+    int32_t cmd_lfile_freq;     /* Cmd_LFile_Freq                              */
+    char run_name[64];          /* RunName                                     */
+    char res_dir[256];          /* Res_Dir                                     */
+    char restart_dir[256];      /* RestartDir                                  */
+} paratc_run_options;
+int paratc_run_options_from_namelist(const char* path, paratc_run_options* out);
+
+/* ChannelInitialize minus IO (src/m_ChannelSystem.f90:26-75): metrics
+ * (InitMeshAndMetries), wavenumbers (InitPoissonSolver:36-48), field storage
+ * (AllocateVariables, all zero, scalar = Scalar_InitValue).  yp has nyp
+ * entries yp(1..nyp).  device < 0 means the current device. */
+int paratc_create(const paratc_params* prm, const double* yp, int device,
+                  paratc_ctx** out);
+int paratc_destroy(paratc_ctx* ctx);
+
+/* The CUDA stream of the context (a cudaStream_t), for callers that order
+ * their own work or events against it. */
+void* paratc_stream(paratc_ctx* ctx);
+
+/* ---- state in / out ---------------------------------------------------- */
+
+/* Loads ux, uy, uz, p (c when scalar_on) and the explicit histories
+ * HistX/Y/Z(/C) (NULL = zero), then applies SetBC_and_UpdateHalo,
+ * SetBC_and_UpdateHalo_pr and SetBC_and_UpdateHalo_scalar as
+ * ChannelInitialize does (src/m_ChannelSystem.f90:63-68).  ux is the
+ * velocity in the computing frame (the restart file holds ux+uCRF). */
+int paratc_set_fields(paratc_ctx* ctx, const double* ux, const double* uy,
+                      const double* uz, const double* p, const double* c,
+                      const double* hx, const double* hy, const double* hz,
+                      const double* hc, int layout);
+/* Any output pointer may be NULL. */
+int paratc_get_fields(paratc_ctx* ctx, double* ux, double* uy, double* uz,
+                      double* p, double* c, double* hx, double* hy, double* hz,
+                      double* hc, int layout);
+
+/* Same as the pair above with device pointers (interior layout). */
+int paratc_set_fields_device(paratc_ctx* ctx, const double* ux, const double* uy,
+                             const double* uz, const double* p, const double* c,
+                             const double* hx, const double* hy, const double* hz,
+                             const double* hc);
+int paratc_get_fields_device(paratc_ctx* ctx, double* ux, double* uy, double* uz,
+                             double* p, double* c, double* hx, double* hy,
+                             double* hz, double* hc);
+
+/* SimTime, dt and PrGradAver of the context (m_Parameters globals). */
+int paratc_set_time(paratc_ctx* ctx, double sim_time, double dt);
+int paratc_get_time(paratc_ctx* ctx, double* sim_time, double* dt);
+
+/* ---- the hot path ------------------------------------------------------- */
+
+/* One time step = ChannelIterate without statistics/visu/restart IO
+ * (src/m_ChannelSystem.f90:80-187): CFL -> dt, iadvance substeps,
+ * CheckDivergence / CalcVmax and their limits.  diag may be NULL.
+ * Returns PARATC_ERR_DIV_LIMIT / PARATC_ERR_VEL_LIMIT where the reference
+ * aborts; the fields then hold the state after the step. */
+int paratc_step(paratc_ctx* ctx, paratc_diag* diag);
+
+/* n steps back to back; diag (may be NULL) receives the last step's numbers.
+ * The per-step guard readback is done once at the end. */
+int paratc_steps(paratc_ctx* ctx, int n, paratc_diag* diag);
+
+/* Enqueues n steps on the context's stream and returns without waiting;
+ * the guards are evaluated on the device.  paratc_last_diag() (or any
+ * synchronising call) then reports the diagnostics and the first failing
+ * guard of the steps enqueued since the previous paratc_last_diag. */
+int paratc_steps_async(paratc_ctx* ctx, int n);
+int paratc_last_diag(paratc_ctx* ctx, paratc_diag* diag);
+
+/* One substep ns (1..iadvance) with time step dt: PMcoeUpdate(ns) and the body
+ * of the ns loop (src/m_ChannelSystem.f90:102-140). divmax_src may be NULL. */
+int paratc_substep(paratc_ctx* ctx, int ns, double dt, double* divmax_src);
+
+/* Inspection: the substep above stopped after stage stop_stage (1 clcRhsXYZ
+ * with the flow-rate constraint, 2 the Helmholtz solves clcU1Hat/clcU2Hat/
+ * clcU3Hat/clcScalar, 3 clcPrSrc, 4 clcPPE, 5 complete), so that each
+ * reference routine can be compared on its own. */
+int paratc_substep_stage(paratc_ctx* ctx, int ns, double dt, int stop_stage,
+                         double* divmax_src);
+
+/* Inspection: copies a work array in interior layout to host memory:
+ * 0 RhsX (with the flow-rate term), 1 RhsY, 2 RhsZ, 3 RhsC, 4 prsrc, 5 phi. */
+int paratc_get_work(paratc_ctx* ctx, int which, double* out);
+
+/* clcPPE (src/m_Poisson.f90:352-452, choice 1 on one rank): solves
+ * Lap4(phi) = src with 4th-order modified wavenumbers in x/z, the 2nd-order
+ * Neumann y operator, phi_hat(kx=0,kz=0,jc=1) = 0, scaled by 1/(nxc*nzc).
+ * src and phi are host arrays in interior layout (phi may equal src). */
+int paratc_poisson(paratc_ctx* ctx, const double* src, double* phi);
+/* Same with device pointers (interior layout, nxc*nyc*nzc doubles). */
+int paratc_poisson_device(paratc_ctx* ctx, const double* d_src, double* d_phi);
+
+/* Makes the current velocity field discretely solenoidal with one pressure-free
+ * projection (u -= grad(phi), Lap4(phi) = div u), the same operators as a
+ * substep; used to prepare seeded initial fields. divmax_out may be NULL. */
+int paratc_project(paratc_ctx* ctx, double* divmax_out);
+
+/* Reductions of src/m_Tools.f90 on the current fields. */
+int paratc_diagnostics(paratc_ctx* ctx, paratc_diag* diag);
+
+/* ---- restart files (src/m_IOAndVisu.f90:408-512) ----------------------- */
+/* Raw FP64, headerless, Fortran order: ux+uCRF, uy, uz, p, [c],
+ * [HistX, HistY, HistZ, [HistC]] (histories only when with_hist != 0). */
+int paratc_write_restart(paratc_ctx* ctx, const char* path, int with_hist);
+int paratc_read_restart(paratc_ctx* ctx, const char* path);
+
+/* ---- errors -------------------------------------------------------------- */
+const char* paratc_strerror(int status);
+/* Text of the last failure on this context (empty when none). */
+const char* paratc_last_error(paratc_ctx* ctx);
+
+/* Number of kernel launches issued by this context since creation. */
+int64_t paratc_launch_count(paratc_ctx* ctx);
+
+/* ---- per-kernel timing (CUDA events around every launch, off by default) */
+#define PARATC_PROF_NKERNELS 16
+/* on != 0 starts recording (and clears the totals), 0 stops. */
+int paratc_profile_enable(paratc_ctx* ctx, int on);
+/* Device time (ms, summed) and launch count of kernel class k in
+ * [0, PARATC_PROF_NKERNELS) since the last enable; the pending events are
+ * resolved first (this synchronises the stream). */
+int paratc_profile_get(paratc_ctx* ctx, int k, double* total_ms, int64_t* launches);
+/* Name of kernel class k ("rhs", "helmholtz", "fft_x_fwd", ...). */
+const char* paratc_profile_name(int k);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PARATC_H */

@@ -1,0 +1,715 @@
+// api.cu -- paratc_ctx and the C ABI of include/paratc.h.
+//
+// A context is the B200 counterpart of one ParaTC rank's module state
+// (m_Variables, m_MeshAndMetries, m_Poisson, m_Parameters): all fields live in
+// HBM for the life of the context, one CUDA stream orders every kernel, and a
+// step is enqueued as the fixed kernel sequence of ChannelIterate
+// (src/m_ChannelSystem.f90:80-187) with dt, the RK coefficients and the
+// guards kept on the device, so a step needs no host round trip until its
+// diagnostics are read.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/paratc.h"
+#include "common.cuh"
+#include "host_setup.h"
+#include "kernels.cuh"
+
+using namespace ptc;
+
+// kernel classes of the per-kernel timer
+enum ProfK {
+    PK_COEF = 0, PK_UYYM, PK_RHS, PK_FLOWRATE, PK_HELM, PK_HELM_SC, PK_PRSRC, PK_FFTX_F, PK_FFTZ_F, PK_YSOLVE,
+    PK_FFTZ_B, PK_FFTX_B, PK_PROJECT, PK_CFL, PK_CHECK, PK_BC
+};
+static const char* kProfNames[PARATC_PROF_NKERNELS] = {
+    "coef", "uy_ym", "rhs", "flowrate", "helmholtz", "helmholtz_scalar", "prsrc", "fft_x_fwd", "fft_z_fwd",
+    "ysolve", "fft_z_bwd", "fft_x_bwd", "project", "cfl", "check", "bc"};
+
+struct paratc_ctx {
+    paratc_params prm;
+    int dev = 0;
+    cudaStream_t st = nullptr;
+    int nx = 0, ny = 0, nz = 0, nyp = 0, nyt = 0, M1 = 0;
+    size_t nf = 0, ni = 0, npart = 0;
+    HostMetrics hm;
+    DConst kc;
+    DMetric dm;
+    FftPlan plx, plz;
+    Fields f;
+    std::vector<void*> allocs;
+    double *d_src = nullptr, *d_phi = nullptr, *d_part = nullptr, *d_uy_ym = nullptr, *d_duy_ym = nullptr;
+    double *d_metric = nullptr, *d_scal = nullptr;
+    double2 *d_spec = nullptr, *d_twx = nullptr, *d_postx = nullptr, *d_twz = nullptr;
+    DCoef* d_coef = nullptr;
+    DDiag* d_diag = nullptr;
+    DDiag* d_diag2 = nullptr;
+    DDiag* h_diag = nullptr;   // pinned
+    DCoef* h_coef = nullptr;   // pinned
+    double* h_scal = nullptr;  // pinned
+    std::string err;
+    int64_t launches = 0;
+    // per-kernel timer
+    bool prof_on = false;
+    std::vector<cudaEvent_t> ev;          // pool, pairs (2q, 2q+1)
+    std::vector<int> ev_class;            // class of pending pair q
+    int ev_used = 0;
+    double prof_ms[PARATC_PROF_NKERNELS] = {0};
+    int64_t prof_n[PARATC_PROF_NKERNELS] = {0};
+};
+
+namespace {
+
+void prof_flush(paratc_ctx* ctx);
+
+// brackets one launch with a pair of events when the timer is on
+struct ProfScope {
+    paratc_ctx* ctx;
+    int q = -1;
+    ProfScope(paratc_ctx* c, int cls) : ctx(c) {
+        if (!ctx->prof_on) return;
+        if (ctx->ev_used * 2 + 2 > (int)ctx->ev.size()) prof_flush(ctx);
+        q = ctx->ev_used++;
+        ctx->ev_class[q] = cls;
+        cudaEventRecord(ctx->ev[2 * q], ctx->st);
+    }
+    ~ProfScope() {
+        if (q >= 0) cudaEventRecord(ctx->ev[2 * q + 1], ctx->st);
+    }
+};
+#define PROF(cls) ProfScope prof_scope_##__LINE__(ctx, cls)
+
+void prof_flush(paratc_ctx* ctx) {
+    if (ctx->ev_used == 0) return;
+    cudaStreamSynchronize(ctx->st);
+    for (int q = 0; q < ctx->ev_used; q++) {
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, ctx->ev[2 * q], ctx->ev[2 * q + 1]) == cudaSuccess) {
+            ctx->prof_ms[ctx->ev_class[q]] += ms;
+            ctx->prof_n[ctx->ev_class[q]] += 1;
+        }
+    }
+    ctx->ev_used = 0;
+}
+
+int set_err(paratc_ctx* c, int code, const std::string& msg) {
+    if (c) c->err = msg;
+    return code;
+}
+
+#define CK(call)                                                                                   \
+    do {                                                                                           \
+        cudaError_t e_ = (call);                                                                   \
+        if (e_ != cudaSuccess)                                                                     \
+            return set_err(ctx, PARATC_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+template <class T>
+int dalloc(paratc_ctx* ctx, T** p, size_t n) {
+    void* q = nullptr;
+    cudaError_t e = cudaMalloc(&q, n * sizeof(T) + 256);
+    if (e != cudaSuccess) return set_err(ctx, PARATC_ERR_OOM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    ctx->allocs.push_back(q);
+    cudaMemsetAsync(q, 0, n * sizeof(T) + 256, ctx->st);
+    *p = (T*)q;
+    return PARATC_OK;
+}
+
+int make_plan(int n, FftPlan& pl) {
+    pl.n = n;
+    pl.nr = 0;
+    int m = n;
+    while (m % 4 == 0 && pl.nr < PT_MAX_RADIX_PASSES) { pl.rad[pl.nr++] = 4; m /= 4; }
+    while (m % 2 == 0 && pl.nr < PT_MAX_RADIX_PASSES) { pl.rad[pl.nr++] = 2; m /= 2; }
+    while (m % 3 == 0 && pl.nr < PT_MAX_RADIX_PASSES) { pl.rad[pl.nr++] = 3; m /= 3; }
+    while (m % 5 == 0 && pl.nr < PT_MAX_RADIX_PASSES) { pl.rad[pl.nr++] = 5; m /= 5; }
+    return m == 1 ? PARATC_OK : PARATC_ERR_BAD_ARG;
+}
+
+std::vector<double2> twiddles(int n, int count) {
+    std::vector<double2> w(count);
+    const long double pi = 3.141592653589793238462643383279502884L;
+    for (int k = 0; k < count; k++) {
+        long double a = -2.0L * pi * (long double)k / (long double)n;
+        w[k] = make_double2((double)cosl(a), (double)sinl(a));
+    }
+    return w;
+}
+
+void enqueue_poisson(paratc_ctx* ctx, const double* src, double* out, int padded) {
+    cudaStream_t st = ctx->st;
+    const int nrows = ctx->ny * ctx->nz;
+    { PROF(PK_FFTX_F); launch_fft_x_r2c(st, ctx->nx, nrows, src, ctx->d_spec, ctx->plx, ctx->d_twx, ctx->d_postx); }
+    { PROF(PK_FFTZ_F); launch_fft_z(st, -1, ctx->nx, ctx->ny, ctx->nz, ctx->d_spec, ctx->plz, ctx->d_twz); }
+    { PROF(PK_YSOLVE); launch_ysolve(st, ctx->kc, ctx->dm, ctx->d_spec); }
+    { PROF(PK_FFTZ_B); launch_fft_z(st, +1, ctx->nx, ctx->ny, ctx->nz, ctx->d_spec, ctx->plz, ctx->d_twz); }
+    { PROF(PK_FFTX_B); launch_fft_x_c2r(st, ctx->nx, ctx->ny, nrows, ctx->d_spec, out, ctx->plx, ctx->d_twx, ctx->d_postx,
+                                         ctx->hm.normfft, padded); }
+    ctx->launches += 5;
+}
+
+// body of the ns loop of ChannelIterate (src/m_ChannelSystem.f90:102-140),
+// optionally stopped after stage `stop` (1 rhs, 2 helmholtz, 3 prsrc, 4 ppe)
+void enqueue_substep(paratc_ctx* ctx, int ns, int stop = 5) {
+    cudaStream_t st = ctx->st;
+    const HostMetrics& h = ctx->hm;
+    { PROF(PK_COEF); launch_coef(st, ctx->d_coef, ns, h.gam[ns - 1], h.the[ns - 1], h.alp[ns - 1], ctx->prm.xnu, ctx->prm.sdiff); }
+    { PROF(PK_UYYM); launch_update_uy_ym(st, ctx->nx * ctx->nz, ctx->d_uy_ym, ctx->d_duy_ym); }
+    { PROF(PK_RHS); launch_rhs(st, ctx->kc, ctx->dm, ctx->d_coef, ctx->f, ctx->d_part); }
+    { PROF(PK_FLOWRATE); launch_flowrate(st, ctx->kc, ctx->d_coef, ctx->d_part, (int)cell_grid_blocks(ctx->kc)); }
+    ctx->launches += 4;
+    if (stop == 1) return;
+    if (ctx->prm.scalar_on) { PROF(PK_HELM_SC); launch_helm_scalar(st, ctx->kc, ctx->dm, ctx->d_coef, ctx->f); ctx->launches++; }
+    { PROF(PK_HELM); launch_helm(st, ctx->kc, ctx->dm, ctx->d_coef, ctx->f, ctx->d_duy_ym, ctx->d_uy_ym); }
+    ctx->launches += 1;
+    if (stop == 2) return;
+    { PROF(PK_PRSRC); launch_prsrc(st, ctx->kc, ctx->dm, ctx->d_coef, 0, ctx->f, ctx->d_src, ctx->d_part, &ctx->d_coef->divmax_src); }
+    ctx->launches += 2;
+    if (stop == 3) return;
+    enqueue_poisson(ctx, ctx->d_src, ctx->d_phi, 1);
+    if (stop == 4) return;
+    { PROF(PK_PROJECT); launch_project(st, ctx->kc, ctx->dm, ctx->d_coef, 0, ctx->d_phi, ctx->f, ctx->d_uy_ym); }
+    ctx->launches += 1;
+}
+
+void enqueue_step(paratc_ctx* ctx) {
+    { PROF(PK_CFL); launch_cfl(ctx->st, ctx->kc, ctx->dm, ctx->f, ctx->d_coef, ctx->d_part); }
+    ctx->launches += 2;
+    for (int ns = 1; ns <= ctx->hm.iadvance; ns++) enqueue_substep(ctx, ns);
+    { PROF(PK_CHECK); launch_check(ctx->st, ctx->kc, ctx->dm, ctx->f, ctx->d_coef, ctx->d_diag, ctx->d_part); }
+    ctx->launches += 2;
+}
+
+void diag_out(const DDiag& d, paratc_diag* o) {
+    if (!o) return;
+    o->dt = d.dt; o->cfl = d.cfl; o->sim_time = d.sim_time; o->divmax_src = d.divmax_src; o->divmax = d.divmax;
+    for (int q = 0; q < 3; q++) o->vmax[q] = d.vmax[q];
+    o->pr_grad_aver = d.pr_grad_aver; o->ux_mean = d.ux_mean; o->sc_mean = d.sc_mean; o->sc2_mean = d.sc2_mean;
+}
+
+int sync(paratc_ctx* ctx) {
+    cudaError_t e = cudaStreamSynchronize(ctx->st);
+    if (e != cudaSuccess) return set_err(ctx, PARATC_ERR_CUDA, std::string("kernel execution: ") + cudaGetErrorString(e));
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return set_err(ctx, PARATC_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(e));
+    return PARATC_OK;
+}
+
+// host <-> device copies of one field between a host layout and the padded
+// device layout (rows j = 1..ny of every z slab)
+int copy_field(paratc_ctx* ctx, double* dev, const double* host_src, double* host_dst, int layout, bool dev_is_host_side) {
+    (void)dev_is_host_side;
+    cudaMemcpy3DParms p;
+    std::memset(&p, 0, sizeof(p));
+    const int nx = ctx->nx, ny = ctx->ny, nz = ctx->nz;
+    cudaPitchedPtr dp = make_cudaPitchedPtr(dev, (size_t)nx * sizeof(double), (size_t)nx, (size_t)ctx->nyt);
+    cudaPitchedPtr hp;
+    cudaPos hpos = make_cudaPos(0, 0, 0);
+    if (layout == PARATC_LAYOUT_HALO) {
+        hp = make_cudaPitchedPtr((void*)(host_src ? host_src : host_dst), (size_t)(nx + 4) * sizeof(double), (size_t)(nx + 4),
+                                 (size_t)(ny + 2));
+        hpos = make_cudaPos(2 * sizeof(double), 1, 2);
+    } else {
+        hp = make_cudaPitchedPtr((void*)(host_src ? host_src : host_dst), (size_t)nx * sizeof(double), (size_t)nx, (size_t)ny);
+    }
+    p.extent = make_cudaExtent((size_t)nx * sizeof(double), (size_t)ny, (size_t)nz);
+    if (host_src) {
+        p.srcPtr = hp; p.srcPos = hpos;
+        p.dstPtr = dp; p.dstPos = make_cudaPos(0, 1, 0);
+    } else {
+        p.srcPtr = dp; p.srcPos = make_cudaPos(0, 1, 0);
+        p.dstPtr = hp; p.dstPos = hpos;
+    }
+    p.kind = cudaMemcpyDefault;
+    CK(cudaMemcpy3DAsync(&p, ctx->st));
+    return PARATC_OK;
+}
+
+int load_state_common(paratc_ctx* ctx) {
+    // ChannelInitialize after read_restart (src/m_ChannelSystem.f90:63-68)
+    launch_update_uy_ym(ctx->st, ctx->nx * ctx->nz, ctx->d_uy_ym, ctx->d_duy_ym);
+    DCoef c0;
+    std::memset(&c0, 0, sizeof(c0));
+    c0.dt = ctx->prm.dt_max;
+    c0.sim_time = 0.0;
+    *ctx->h_coef = c0;
+    CK(cudaMemcpyAsync(ctx->d_coef, ctx->h_coef, sizeof(DCoef), cudaMemcpyHostToDevice, ctx->st));
+    launch_bc_all(ctx->st, ctx->kc, ctx->f, ctx->d_uy_ym);
+    ctx->launches += 2;
+    return sync(ctx);
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* paratc_strerror(int status) {
+    switch (status) {
+    case PARATC_OK: return "ok";
+    case PARATC_ERR_BAD_ARG: return "invalid argument";
+    case PARATC_ERR_OOM: return "out of memory";
+    case PARATC_ERR_CUDA: return "CUDA error";
+    case PARATC_ERR_NONFINITE: return "non-finite value in a field";
+    case PARATC_ERR_DIV_LIMIT: return "too big div";
+    case PARATC_ERR_VEL_LIMIT: return "too big velocity";
+    case PARATC_ERR_TIMEOUT: return "device wait timed out";
+    case PARATC_ERR_IO: return "restart/input file error";
+    case PARATC_ERR_NO_DEVICE: return "no CUDA device";
+    default: return "unknown status";
+    }
+}
+
+const char* paratc_last_error(paratc_ctx* ctx) { return ctx ? ctx->err.c_str() : ""; }
+int64_t paratc_launch_count(paratc_ctx* ctx) { return ctx ? ctx->launches : 0; }
+void* paratc_stream(paratc_ctx* ctx) { return ctx ? (void*)ctx->st : nullptr; }
+
+int paratc_profile_enable(paratc_ctx* ctx, int on) {
+    if (!ctx) return PARATC_ERR_BAD_ARG;
+    CK(cudaSetDevice(ctx->dev));
+    if (on) {
+        if (ctx->ev.empty()) {
+            ctx->ev.resize(4096);
+            ctx->ev_class.resize(2048);
+            for (auto& e : ctx->ev) CK(cudaEventCreate(&e));
+        }
+        prof_flush(ctx);
+        for (int k = 0; k < PARATC_PROF_NKERNELS; k++) { ctx->prof_ms[k] = 0.0; ctx->prof_n[k] = 0; }
+        ctx->prof_on = true;
+    } else {
+        prof_flush(ctx);
+        ctx->prof_on = false;
+    }
+    return PARATC_OK;
+}
+
+int paratc_profile_get(paratc_ctx* ctx, int k, double* total_ms, int64_t* launches) {
+    if (!ctx || k < 0 || k >= PARATC_PROF_NKERNELS) return PARATC_ERR_BAD_ARG;
+    prof_flush(ctx);
+    if (total_ms) *total_ms = ctx->prof_ms[k];
+    if (launches) *launches = ctx->prof_n[k];
+    return PARATC_OK;
+}
+
+const char* paratc_profile_name(int k) { return (k >= 0 && k < PARATC_PROF_NKERNELS) ? kProfNames[k] : ""; }
+
+int paratc_destroy(paratc_ctx* ctx) {
+    if (!ctx) return PARATC_OK;
+    if (ctx->st) cudaStreamSynchronize(ctx->st);
+    for (auto& e : ctx->ev) cudaEventDestroy(e);
+    for (void* p : ctx->allocs) cudaFree(p);
+    if (ctx->h_diag) cudaFreeHost(ctx->h_diag);
+    if (ctx->h_coef) cudaFreeHost(ctx->h_coef);
+    if (ctx->h_scal) cudaFreeHost(ctx->h_scal);
+    if (ctx->st) cudaStreamDestroy(ctx->st);
+    delete ctx;
+    return PARATC_OK;
+}
+
+int paratc_create(const paratc_params* prm, const double* yp, int device, paratc_ctx** out) {
+    if (!prm || !yp || !out) return PARATC_ERR_BAD_ARG;
+    *out = nullptr;
+    std::string why;
+    int rc = validate_params(*prm, why);
+    if (rc != PARATC_OK) {
+        std::fprintf(stderr, "paratc_create: %s\n", why.c_str());
+        return rc;
+    }
+    if (!tridiag_supported(prm->nyc)) {
+        std::fprintf(stderr, "paratc_create: nyc=%d outside the supported 3..256\n", prm->nyc);
+        return PARATC_ERR_BAD_ARG;
+    }
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) return PARATC_ERR_NO_DEVICE;
+    paratc_ctx* ctx = new paratc_ctx();
+    ctx->prm = *prm;
+    if (device < 0) cudaGetDevice(&ctx->dev);
+    else ctx->dev = device;
+    if (ctx->dev >= ndev) { delete ctx; return PARATC_ERR_BAD_ARG; }
+    CK(cudaSetDevice(ctx->dev));
+    rc = build_metrics(*prm, yp, ctx->hm);
+    if (rc != PARATC_OK) { delete ctx; return rc; }
+    ctx->nx = prm->nxc; ctx->ny = prm->nyc; ctx->nz = prm->nzc; ctx->nyp = prm->nyc + 1; ctx->nyt = prm->nyc + 2;
+    ctx->M1 = ctx->nx / 2 + 1;
+    ctx->nf = (size_t)ctx->nz * ctx->nyt * ctx->nx;
+    ctx->ni = (size_t)ctx->nz * ctx->ny * ctx->nx;
+    if (make_plan(ctx->nx / 2, ctx->plx) != PARATC_OK || make_plan(ctx->nz, ctx->plz) != PARATC_OK) {
+        std::fprintf(stderr, "paratc_create: nxc/2 and nzc must factor into 2, 3 and 5\n");
+        delete ctx;
+        return PARATC_ERR_BAD_ARG;
+    }
+    if (fft_smem_need(ctx->nx, ctx->nz) > 160 * 1024) {
+        std::fprintf(stderr, "paratc_create: grid too large for the shared-memory FFT\n");
+        delete ctx;
+        return PARATC_ERR_BAD_ARG;
+    }
+    cudaError_t ce = cudaStreamCreateWithFlags(&ctx->st, cudaStreamNonBlocking);
+    if (ce != cudaSuccess) { delete ctx; return PARATC_ERR_CUDA; }
+    static bool inited = false;
+    if (!inited) {
+        fft_init();
+        tridiag_init();
+        inited = true;
+    }
+    const HostMetrics& h = ctx->hm;
+    // ---- constants
+    DConst& kc = ctx->kc;
+    std::memset(&kc, 0, sizeof(kc));
+    kc.nx = ctx->nx; kc.ny = ctx->ny; kc.nz = ctx->nz; kc.nyp = ctx->nyp; kc.nyt = ctx->nyt;
+    kc.flow_type = prm->flow_type; kc.scalar_on = prm->scalar_on; kc.is_ux_const = prm->is_ux_const; kc.icfl = prm->icfl;
+    for (int q = 0; q < 4; q++) { kc.dxC[q] = h.dxC[q]; kc.dzC[q] = h.dzC[q]; kc.IC[q] = h.IC[q]; }
+    for (int q = 0; q < 5; q++) { kc.dxxC[q] = h.dxxC[q]; kc.dzzC[q] = h.dzzC[q]; }
+    kc.rdx = h.rdx; kc.rdz = h.rdz;
+    kc.ucrf = prm->ucrf; kc.xnu = prm->xnu; kc.sdiff = prm->sdiff;
+    for (int q = 0; q < 3; q++) { kc.grav[q] = prm->gravity[q]; kc.gev[q] = prm->gravity_eff_vec[q]; kc.fvv[q] = prm->falling_vel_vec[q]; }
+    kc.uxbc_ym = prm->ux_bc[2]; kc.uxbc_yp = prm->ux_bc[3]; kc.uybc_yp = prm->uy_bc[3];
+    kc.uzbc_ym = prm->uz_bc[2]; kc.uzbc_yp = prm->uz_bc[3];
+    kc.ubulk = prm->ubulk; kc.yly = prm->yly; kc.normfft = h.normfft; kc.dt_max = prm->dt_max; kc.cflc = prm->cflc;
+    kc.sc_r1b = h.sc_r1b; kc.sc_r2b = h.sc_r2b; kc.sc_r1t = h.sc_r1t; kc.sc_r2t = h.sc_r2t;
+    kc.vel_limit = prm->vel_limit; kc.div_limit = prm->div_limit;
+
+    // ---- device memory
+    const size_t nf = ctx->nf;
+    Fields& f = ctx->f;
+    std::memset(&f, 0, sizeof(f));
+    double** fl[] = {&f.ux, &f.uy, &f.uz, &f.pr, &f.hx, &f.hy, &f.hz, &f.rx, &f.ry, &f.rz, &ctx->d_phi};
+    for (double** p : fl)
+        if ((rc = dalloc(ctx, p, nf)) != PARATC_OK) { paratc_destroy(ctx); return rc; }
+    if (prm->scalar_on) {
+        double** fs[] = {&f.sc, &f.hc, &f.rc};
+        for (double** p : fs)
+            if ((rc = dalloc(ctx, p, nf)) != PARATC_OK) { paratc_destroy(ctx); return rc; }
+    }
+    ctx->npart = cell_grid_blocks(kc) * 7 + 64;
+    if ((rc = dalloc(ctx, &ctx->d_src, ctx->ni)) || (rc = dalloc(ctx, &ctx->d_spec, (size_t)ctx->M1 * ctx->ny * ctx->nz)) ||
+        (rc = dalloc(ctx, &ctx->d_part, ctx->npart)) || (rc = dalloc(ctx, &ctx->d_uy_ym, (size_t)ctx->nx * ctx->nz)) ||
+        (rc = dalloc(ctx, &ctx->d_duy_ym, (size_t)ctx->nx * ctx->nz)) || (rc = dalloc(ctx, &ctx->d_coef, 1)) ||
+        (rc = dalloc(ctx, &ctx->d_diag, 1)) || (rc = dalloc(ctx, &ctx->d_diag2, 1)) || (rc = dalloc(ctx, &ctx->d_scal, 16))) {
+        paratc_destroy(ctx);
+        return rc;
+    }
+    // metrics: 25 y-arrays of nyp+1 plus wavenumbers
+    {
+        const size_t ny1 = (size_t)ctx->nyp + 1;
+        std::vector<double> buf;
+        HostMetrics& hm = ctx->hm;
+        std::vector<const std::vector<double>*> ys = {&hm.rdyp, &hm.rdyc, &hm.dyp, &hm.yinterp, &hm.ap2c, &hm.ac2c, &hm.am2c,
+                                                      &hm.ap2p, &hm.ac2p, &hm.am2p, &hm.ap2ph, &hm.ac2ph, &hm.am2ph,
+                                                      &hm.ap2cCN, &hm.ac2cCN, &hm.am2cCN, &hm.ap2cSc, &hm.ac2cSc, &hm.am2cSc,
+                                                      &hm.ap2cScCN, &hm.ac2cScCN, &hm.am2cScCN};
+        for (auto* v : ys) buf.insert(buf.end(), v->begin(), v->end());
+        buf.insert(buf.end(), hm.wnx.begin(), hm.wnx.end());
+        buf.insert(buf.end(), hm.wnz.begin(), hm.wnz.end());
+        if ((rc = dalloc(ctx, &ctx->d_metric, buf.size()))) { paratc_destroy(ctx); return rc; }
+        CK(cudaMemcpyAsync(ctx->d_metric, buf.data(), buf.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->st));
+        const double* b = ctx->d_metric;
+        const double** dst[] = {&ctx->dm.rdyp, &ctx->dm.rdyc, &ctx->dm.dyp, &ctx->dm.yinterp, &ctx->dm.ap2c, &ctx->dm.ac2c,
+                                &ctx->dm.am2c, &ctx->dm.ap2p, &ctx->dm.ac2p, &ctx->dm.am2p, &ctx->dm.ap2ph, &ctx->dm.ac2ph,
+                                &ctx->dm.am2ph, &ctx->dm.ap2cCN, &ctx->dm.ac2cCN, &ctx->dm.am2cCN, &ctx->dm.ap2cSc,
+                                &ctx->dm.ac2cSc, &ctx->dm.am2cSc, &ctx->dm.ap2cScCN, &ctx->dm.ac2cScCN, &ctx->dm.am2cScCN};
+        for (size_t a = 0; a < sizeof(dst) / sizeof(dst[0]); a++) *dst[a] = b + a * ny1;
+        ctx->dm.wnx = b + ys.size() * ny1;
+        ctx->dm.wnz = ctx->dm.wnx + ctx->nx;
+        CK(cudaStreamSynchronize(ctx->st));
+    }
+    // twiddles
+    {
+        std::vector<double2> twx = twiddles(ctx->nx / 2, ctx->nx / 2);
+        std::vector<double2> post = twiddles(ctx->nx, ctx->nx / 2 + 1);
+        std::vector<double2> twz = twiddles(ctx->nz, ctx->nz);
+        if ((rc = dalloc(ctx, &ctx->d_twx, twx.size())) || (rc = dalloc(ctx, &ctx->d_postx, post.size())) ||
+            (rc = dalloc(ctx, &ctx->d_twz, twz.size()))) {
+            paratc_destroy(ctx);
+            return rc;
+        }
+        CK(cudaMemcpy(ctx->d_twx, twx.data(), twx.size() * sizeof(double2), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(ctx->d_postx, post.data(), post.size() * sizeof(double2), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(ctx->d_twz, twz.data(), twz.size() * sizeof(double2), cudaMemcpyHostToDevice));
+    }
+    CK(cudaMallocHost(&ctx->h_diag, sizeof(DDiag)));
+    CK(cudaMallocHost(&ctx->h_coef, sizeof(DCoef)));
+    CK(cudaMallocHost(&ctx->h_scal, 16 * sizeof(double)));
+    // AllocateVariables: scalar = Scalar_InitValue everywhere (src/m_Variables.f90:84)
+    if (prm->scalar_on) {
+        std::vector<double> init(nf, prm->scalar_init_value);
+        CK(cudaMemcpy(f.sc, init.data(), nf * sizeof(double), cudaMemcpyHostToDevice));
+    }
+    rc = load_state_common(ctx);
+    if (rc != PARATC_OK) { paratc_destroy(ctx); return rc; }
+    *out = ctx;
+    return PARATC_OK;
+}
+
+int paratc_set_fields(paratc_ctx* ctx, const double* ux, const double* uy, const double* uz, const double* p,
+                      const double* c, const double* hx, const double* hy, const double* hz, const double* hc, int layout) {
+    if (!ctx || (layout != PARATC_LAYOUT_INTERIOR && layout != PARATC_LAYOUT_HALO)) return PARATC_ERR_BAD_ARG;
+    CK(cudaSetDevice(ctx->dev));
+    struct { double* d; const double* h; bool hist; } tab[] = {
+        {ctx->f.ux, ux, false}, {ctx->f.uy, uy, false}, {ctx->f.uz, uz, false}, {ctx->f.pr, p, false},
+        {ctx->f.sc, c, false}, {ctx->f.hx, hx, true}, {ctx->f.hy, hy, true}, {ctx->f.hz, hz, true}, {ctx->f.hc, hc, true}};
+    for (auto& t : tab) {
+        if (!t.d) continue;
+        if (t.h) {
+            int rc = copy_field(ctx, t.d, t.h, nullptr, layout, false);
+            if (rc) return rc;
+        } else if (t.hist) {
+            CK(cudaMemsetAsync(t.d, 0, ctx->nf * sizeof(double), ctx->st));
+        }
+    }
+    return load_state_common(ctx);
+}
+
+int paratc_get_fields(paratc_ctx* ctx, double* ux, double* uy, double* uz, double* p, double* c, double* hx, double* hy,
+                      double* hz, double* hc, int layout) {
+    if (!ctx || (layout != PARATC_LAYOUT_INTERIOR && layout != PARATC_LAYOUT_HALO)) return PARATC_ERR_BAD_ARG;
+    CK(cudaSetDevice(ctx->dev));
+    struct { double* d; double* h; } tab[] = {{ctx->f.ux, ux}, {ctx->f.uy, uy}, {ctx->f.uz, uz}, {ctx->f.pr, p},
+                                             {ctx->f.sc, c}, {ctx->f.hx, hx}, {ctx->f.hy, hy}, {ctx->f.hz, hz}, {ctx->f.hc, hc}};
+    for (auto& t : tab) {
+        if (!t.d || !t.h) continue;
+        int rc = copy_field(ctx, t.d, nullptr, t.h, layout, false);
+        if (rc) return rc;
+    }
+    return sync(ctx);
+}
+
+int paratc_set_fields_device(paratc_ctx* ctx, const double* ux, const double* uy, const double* uz, const double* p,
+                             const double* c, const double* hx, const double* hy, const double* hz, const double* hc) {
+    return paratc_set_fields(ctx, ux, uy, uz, p, c, hx, hy, hz, hc, PARATC_LAYOUT_INTERIOR);
+}
+
+int paratc_get_fields_device(paratc_ctx* ctx, double* ux, double* uy, double* uz, double* p, double* c, double* hx,
+                             double* hy, double* hz, double* hc) {
+    return paratc_get_fields(ctx, ux, uy, uz, p, c, hx, hy, hz, hc, PARATC_LAYOUT_INTERIOR);
+}
+
+int paratc_set_time(paratc_ctx* ctx, double sim_time, double dt) {
+    if (!ctx) return PARATC_ERR_BAD_ARG;
+    CK(cudaSetDevice(ctx->dev));
+    CK(cudaMemcpyAsync(ctx->h_coef, ctx->d_coef, sizeof(DCoef), cudaMemcpyDeviceToHost, ctx->st));
+    int rc = sync(ctx);
+    if (rc) return rc;
+    ctx->h_coef->sim_time = sim_time;
+    ctx->h_coef->dt = dt;
+    CK(cudaMemcpyAsync(ctx->d_coef, ctx->h_coef, sizeof(DCoef), cudaMemcpyHostToDevice, ctx->st));
+    return sync(ctx);
+}
+
+int paratc_get_time(paratc_ctx* ctx, double* sim_time, double* dt) {
+    if (!ctx) return PARATC_ERR_BAD_ARG;
+    CK(cudaSetDevice(ctx->dev));
+    CK(cudaMemcpyAsync(ctx->h_coef, ctx->d_coef, sizeof(DCoef), cudaMemcpyDeviceToHost, ctx->st));
+    int rc = sync(ctx);
+    if (rc) return rc;
+    if (sim_time) *sim_time = ctx->h_coef->sim_time;
+    if (dt) *dt = ctx->h_coef->dt;
+    return PARATC_OK;
+}
+
+int paratc_steps(paratc_ctx* ctx, int n, paratc_diag* diag) {
+    if (!ctx || n < 1) return PARATC_ERR_BAD_ARG;
+    CK(cudaSetDevice(ctx->dev));
+    CK(cudaMemsetAsync(ctx->d_diag, 0, sizeof(DDiag), ctx->st));
+    for (int s = 0; s < n; s++) enqueue_step(ctx);
+    CK(cudaMemcpyAsync(ctx->h_diag, ctx->d_diag, sizeof(DDiag), cudaMemcpyDeviceToHost, ctx->st));
+    int rc = sync(ctx);
+    if (rc) return rc;
+    diag_out(*ctx->h_diag, diag);
+    if (ctx->h_diag->status != 0) {
+        char b[160];
+        std::snprintf(b, sizeof(b), "%s at step %d of %d (divmax %.6e, vmax %.6e %.6e %.6e)",
+                      paratc_strerror(ctx->h_diag->status), ctx->h_diag->failed_step, n, ctx->h_diag->divmax,
+                      ctx->h_diag->vmax[0], ctx->h_diag->vmax[1], ctx->h_diag->vmax[2]);
+        return set_err(ctx, ctx->h_diag->status, b);
+    }
+    return PARATC_OK;
+}
+
+int paratc_step(paratc_ctx* ctx, paratc_diag* diag) { return paratc_steps(ctx, 1, diag); }
+
+int paratc_steps_async(paratc_ctx* ctx, int n) {
+    if (!ctx || n < 1) return PARATC_ERR_BAD_ARG;
+    CK(cudaSetDevice(ctx->dev));
+    for (int s = 0; s < n; s++) enqueue_step(ctx);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return set_err(ctx, PARATC_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(e));
+    return PARATC_OK;
+}
+
+int paratc_last_diag(paratc_ctx* ctx, paratc_diag* diag) {
+    if (!ctx) return PARATC_ERR_BAD_ARG;
+    CK(cudaSetDevice(ctx->dev));
+    CK(cudaMemcpyAsync(ctx->h_diag, ctx->d_diag, sizeof(DDiag), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaMemsetAsync(ctx->d_diag, 0, sizeof(DDiag), ctx->st));
+    int rc = sync(ctx);
+    if (rc) return rc;
+    diag_out(*ctx->h_diag, diag);
+    if (ctx->h_diag->status != 0) {
+        char b[160];
+        std::snprintf(b, sizeof(b), "%s at step %d (divmax %.6e)", paratc_strerror(ctx->h_diag->status),
+                      ctx->h_diag->failed_step, ctx->h_diag->divmax);
+        return set_err(ctx, ctx->h_diag->status, b);
+    }
+    return PARATC_OK;
+}
+
+int paratc_substep(paratc_ctx* ctx, int ns, double dt, double* divmax_src) {
+    return paratc_substep_stage(ctx, ns, dt, 5, divmax_src);
+}
+
+int paratc_substep_stage(paratc_ctx* ctx, int ns, double dt, int stop_stage, double* divmax_src) {
+    if (!ctx || ns < 1 || ns > ctx->hm.iadvance || stop_stage < 1 || stop_stage > 5) return PARATC_ERR_BAD_ARG;
+    CK(cudaSetDevice(ctx->dev));
+    CK(cudaMemcpyAsync(ctx->h_coef, ctx->d_coef, sizeof(DCoef), cudaMemcpyDeviceToHost, ctx->st));
+    int rc = sync(ctx);
+    if (rc) return rc;
+    ctx->h_coef->dt = dt;
+    CK(cudaMemcpyAsync(ctx->d_coef, ctx->h_coef, sizeof(DCoef), cudaMemcpyHostToDevice, ctx->st));
+    enqueue_substep(ctx, ns, stop_stage);
+    CK(cudaMemcpyAsync(ctx->h_coef, ctx->d_coef, sizeof(DCoef), cudaMemcpyDeviceToHost, ctx->st));
+    rc = sync(ctx);
+    if (rc) return rc;
+    if (divmax_src) *divmax_src = ctx->h_coef->divmax_src;
+    return PARATC_OK;
+}
+
+int paratc_get_work(paratc_ctx* ctx, int which, double* out) {
+    if (!ctx || !out || which < 0 || which > 5) return PARATC_ERR_BAD_ARG;
+    CK(cudaSetDevice(ctx->dev));
+    double* src[] = {ctx->f.rx, ctx->f.ry, ctx->f.rz, ctx->f.rc, ctx->d_src, ctx->d_phi};
+    if (!src[which]) return PARATC_ERR_BAD_ARG;
+    int rc;
+    if (which == 4) {
+        CK(cudaMemcpyAsync(out, ctx->d_src, ctx->ni * sizeof(double), cudaMemcpyDefault, ctx->st));
+        rc = sync(ctx);
+    } else {
+        rc = copy_field(ctx, src[which], nullptr, out, PARATC_LAYOUT_INTERIOR, false);
+        if (rc == PARATC_OK) rc = sync(ctx);
+    }
+    if (rc) return rc;
+    if (which == 0) {
+        CK(cudaMemcpyAsync(ctx->h_coef, ctx->d_coef, sizeof(DCoef), cudaMemcpyDeviceToHost, ctx->st));
+        rc = sync(ctx);
+        if (rc) return rc;
+        const double add = ctx->h_coef->rhsx_add;
+        for (size_t q = 0; q < ctx->ni; q++) out[q] = out[q] + add;
+    }
+    return PARATC_OK;
+}
+
+int paratc_poisson_device(paratc_ctx* ctx, const double* d_src, double* d_phi) {
+    if (!ctx || !d_src || !d_phi) return PARATC_ERR_BAD_ARG;
+    CK(cudaSetDevice(ctx->dev));
+    enqueue_poisson(ctx, d_src, d_phi, 0);
+    return sync(ctx);
+}
+
+int paratc_poisson(paratc_ctx* ctx, const double* src, double* phi) {
+    if (!ctx || !src || !phi) return PARATC_ERR_BAD_ARG;
+    CK(cudaSetDevice(ctx->dev));
+    CK(cudaMemcpyAsync(ctx->d_src, src, ctx->ni * sizeof(double), cudaMemcpyDefault, ctx->st));
+    enqueue_poisson(ctx, ctx->d_src, ctx->d_src, 0);
+    CK(cudaMemcpyAsync(phi, ctx->d_src, ctx->ni * sizeof(double), cudaMemcpyDefault, ctx->st));
+    return sync(ctx);
+}
+
+int paratc_project(paratc_ctx* ctx, double* divmax_out) {
+    if (!ctx) return PARATC_ERR_BAD_ARG;
+    CK(cudaSetDevice(ctx->dev));
+    launch_bc_all(ctx->st, ctx->kc, ctx->f, ctx->d_uy_ym);
+    launch_prsrc(ctx->st, ctx->kc, ctx->dm, ctx->d_coef, 1, ctx->f, ctx->d_src, ctx->d_part, ctx->d_scal);
+    enqueue_poisson(ctx, ctx->d_src, ctx->d_phi, 1);
+    launch_project(ctx->st, ctx->kc, ctx->dm, ctx->d_coef, 1, ctx->d_phi, ctx->f, ctx->d_uy_ym);
+    launch_prsrc(ctx->st, ctx->kc, ctx->dm, ctx->d_coef, 1, ctx->f, nullptr, ctx->d_part, ctx->d_scal + 1);
+    ctx->launches += 6;
+    CK(cudaMemcpyAsync(ctx->h_scal, ctx->d_scal, 2 * sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
+    int rc = sync(ctx);
+    if (rc) return rc;
+    if (divmax_out) *divmax_out = ctx->h_scal[1];
+    return PARATC_OK;
+}
+
+int paratc_diagnostics(paratc_ctx* ctx, paratc_diag* diag) {
+    if (!ctx || !diag) return PARATC_ERR_BAD_ARG;
+    CK(cudaSetDevice(ctx->dev));
+    CK(cudaMemsetAsync(ctx->d_diag2, 0, sizeof(DDiag), ctx->st));
+    launch_check(ctx->st, ctx->kc, ctx->dm, ctx->f, ctx->d_coef, ctx->d_diag2, ctx->d_part);
+    ctx->launches += 2;
+    CK(cudaMemcpyAsync(ctx->h_diag, ctx->d_diag2, sizeof(DDiag), cudaMemcpyDeviceToHost, ctx->st));
+    int rc = sync(ctx);
+    if (rc) return rc;
+    diag_out(*ctx->h_diag, diag);
+    return PARATC_OK;
+}
+
+// restart files: write_restart / read_restart (src/m_IOAndVisu.f90:408-512)
+int paratc_write_restart(paratc_ctx* ctx, const char* path, int with_hist) {
+    if (!ctx || !path) return PARATC_ERR_BAD_ARG;
+    const size_t n = ctx->ni;
+    std::vector<double> buf(n);
+    FILE* fp = std::fopen(path, "wb");
+    if (!fp) return set_err(ctx, PARATC_ERR_IO, std::string("cannot open ") + path);
+    std::vector<double*> order = {ctx->f.ux, ctx->f.uy, ctx->f.uz, ctx->f.pr};
+    if (ctx->prm.scalar_on) order.push_back(ctx->f.sc);
+    if (with_hist) {
+        order.push_back(ctx->f.hx); order.push_back(ctx->f.hy); order.push_back(ctx->f.hz);
+        if (ctx->prm.scalar_on) order.push_back(ctx->f.hc);
+    }
+    for (size_t a = 0; a < order.size(); a++) {
+        int rc = copy_field(ctx, order[a], nullptr, buf.data(), PARATC_LAYOUT_INTERIOR, false);
+        if (rc == PARATC_OK) rc = sync(ctx);
+        if (rc) { std::fclose(fp); return rc; }
+        if (a == 0)
+            for (size_t q = 0; q < n; q++) buf[q] = buf[q] + ctx->prm.ucrf;
+        if (std::fwrite(buf.data(), sizeof(double), n, fp) != n) {
+            std::fclose(fp);
+            return set_err(ctx, PARATC_ERR_IO, "short write");
+        }
+    }
+    std::fclose(fp);
+    return PARATC_OK;
+}
+
+int paratc_read_restart(paratc_ctx* ctx, const char* path) {
+    if (!ctx || !path) return PARATC_ERR_BAD_ARG;
+    FILE* fp = std::fopen(path, "rb");
+    if (!fp) return set_err(ctx, PARATC_ERR_IO, std::string("Cannot open file: ") + path);
+    std::fseek(fp, 0, SEEK_END);
+    const long long bytes = std::ftell(fp);
+    std::fseek(fp, 0, SEEK_SET);
+    const size_t n = ctx->ni;
+    const long long unit = (long long)n * (long long)sizeof(double);
+    const int nb = ctx->prm.scalar_on ? 5 : 4, nh = ctx->prm.scalar_on ? 9 : 7;
+    if (bytes != unit * nb && bytes != unit * nh) {
+        std::fclose(fp);
+        return set_err(ctx, PARATC_ERR_IO, "file byte wrong");
+    }
+    const bool hist = (bytes == unit * nh);
+    std::vector<std::vector<double>> arr(nh, std::vector<double>());
+    const int nread = hist ? nh : nb;
+    for (int a = 0; a < nread; a++) {
+        arr[a].resize(n);
+        if (std::fread(arr[a].data(), sizeof(double), n, fp) != n) {
+            std::fclose(fp);
+            return set_err(ctx, PARATC_ERR_IO, "short read");
+        }
+    }
+    std::fclose(fp);
+    for (size_t q = 0; q < n; q++) arr[0][q] = arr[0][q] - ctx->prm.ucrf;
+    const double* c = ctx->prm.scalar_on ? arr[4].data() : nullptr;
+    const int h0 = nb;
+    const double* hx = hist ? arr[h0].data() : nullptr;
+    const double* hy = hist ? arr[h0 + 1].data() : nullptr;
+    const double* hz = hist ? arr[h0 + 2].data() : nullptr;
+    const double* hc = (hist && ctx->prm.scalar_on) ? arr[h0 + 3].data() : nullptr;
+    int rc = paratc_set_fields(ctx, arr[0].data(), arr[1].data(), arr[2].data(), arr[3].data(), c, hx, hy, hz, hc,
+                               PARATC_LAYOUT_INTERIOR);
+    return rc;
+}
+
+}  // extern "C"

@@ -1,0 +1,85 @@
+// common.cuh -- device-side data structures shared by the kernels of the
+// ParaTC hot path.
+//
+// HBM layout of a 3-D field ("padded layout"): x fastest, then y, then z,
+// index (i, j, k) -> (k*(ny+2) + j)*nx + i with i in [0,nx), j in [0,ny+1],
+// k in [0,nz).  j keeps the Fortran numbering of the reference: j = 0 and
+// j = nyp = ny+1 are the wall ghost rows of mb1 (src/m_Variables.f90:47-50),
+// j = 1..ny the interior.  There are no x/z halo cells: the periodic halos of
+// myupdate_halo (src/m_Decomp2d.f90:1554-1709) become index wrap, which reads
+// the same values because every halo width the reference updates covers what
+// its stencils read.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#define PT_MAX_RADIX_PASSES 24
+
+namespace ptc {
+
+// y-direction metric arrays of m_MeshAndMetries, indexed by the Fortran j
+// (entries 0..nyp); wavenumbers by the 0-based mode number.
+struct DMetric {
+    const double *rdyp, *rdyc, *dyp, *yinterp;
+    const double *ap2c, *ac2c, *am2c;
+    const double *ap2p, *ac2p, *am2p;
+    const double *ap2ph, *ac2ph, *am2ph;
+    const double *ap2cCN, *ac2cCN, *am2cCN;
+    const double *ap2cSc, *ac2cSc, *am2cSc;
+    const double *ap2cScCN, *ac2cScCN, *am2cScCN;
+    const double *wnx, *wnz;
+};
+
+// grid sizes and the scalar constants every stencil needs
+struct DConst {
+    int nx, ny, nz, nyp, nyt;
+    int flow_type, scalar_on, is_ux_const, icfl;
+    double dxC[4], dzC[4], dxxC[5], dzzC[5], IC[4];
+    double rdx, rdz;
+    double ucrf, xnu, grav[3], sdiff, gev[3], fvv[3];
+    double uxbc_ym, uxbc_yp, uybc_yp, uzbc_ym, uzbc_yp;
+    double ubulk, yly, normfft, dt_max, cflc;
+    double sc_r1b, sc_r2b, sc_r1t, sc_r2t;   // scalar ghost: c0 = r1b*c1 + r2b, ...
+    double vel_limit, div_limit;
+};
+
+// per-substep coefficients (PMcoeUpdate, src/m_Parameters.f90:215-230) and
+// the running scalars of a step; lives in device memory so that dt computed
+// on the device (iCFL = 1) needs no host round trip
+struct DCoef {
+    double dt, pmGamma, pmTheta, pmAlpha, pmAlphaC, pmBeta, pmBetaSc;
+    double rhsx_add;        // -dp1ns (no scalar) or +dp1ns (scalar) of the flow-rate constraint
+    double sim_time, pr_grad_aver, cflmp;
+    double divmax_src;
+    int ns, pad;
+};
+
+// diagnostics of one step, copied to pinned host memory at the end
+struct DDiag {
+    double dt, cfl, sim_time, divmax_src, divmax, vmax[3], pr_grad_aver, ux_mean, sc_mean, sc2_mean;
+    int status;             // 0, or the PARATC_ERR_* of the first guard that failed
+    int failed_step;        // 1-based index of that step inside a multi-step call
+    int step_counter;
+    int pad;
+};
+
+struct FftPlan {
+    int n;          // transform length
+    int nr;         // number of radix passes
+    int rad[PT_MAX_RADIX_PASSES];
+};
+
+__device__ __forceinline__ int wrapi(int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); }
+
+__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ double2 cmulc(double2 a, double2 b) {  // a * conj(b)
+    return make_double2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
+}
+__device__ __forceinline__ double2 cconj(double2 a) { return make_double2(a.x, -a.y); }
+__device__ __forceinline__ double2 cscale(double2 a, double s) { return make_double2(a.x * s, a.y * s); }
+
+}  // namespace ptc

@@ -1,0 +1,324 @@
+// k_tridiag.cu -- wall-normal tridiagonal solves on B200.
+//
+// Both the implicit Helmholtz systems (I - beta*Lyy) du = Rhs of clcU1Hat /
+// clcU2Hat / clcU3Hat / clcScalar (src/m_TScheme.f90:365-506) and the
+// spectral Poisson systems (Lyy + lambda_x + lambda_z) phi = f of clcPPE
+// (src/m_Poisson.f90:383-430) are many independent tridiagonal systems along
+// y, one per (x, z) column.  The reference sweeps them with the serial Thomas
+// algorithm InverseTridiagonal (src/m_Tools.f90:224-251), and across ranks
+// with the reduced-system ("PaScaL") Thomas of clcPPE_x1_reduce
+// (src/m_Poisson.f90:457-695).
+//
+// Here one CTA owns 32 adjacent columns (lanes, coalesced in x / kx) and
+// splits y into P partitions, one warp each.  Each thread keeps its partition
+// in registers and eliminates it locally with the modified Thomas sweep of
+// the reduced algorithm, so that every row depends only on the partition's
+// first and last unknowns; the 2P-row reduced system of each column is solved
+// by one thread from shared memory; the back substitution is local again.
+// HBM traffic is one read of the right-hand side (plus the field for the
+// Helmholtz update) and one write per cell.
+#include "common.cuh"
+#include "kernels.cuh"
+
+namespace ptc {
+
+// local elimination of one partition of MR rows (MR >= 3), the modified
+// Thomas sweep of src/m_Poisson.f90:496-537 in registers.  On exit row 0 reads
+// a0*x_prev + x0 + c0*x_last = f0, row r (1..MR-2) a_r*x0 + x_r + c_r*x_last
+// = f_r, row MR-1 a*x0 + x_last + c*x_next = f.  MR is a compile-time
+// constant so that every register array index is static; rows past ny are
+// identity rows (a = c = f = 0, b = 1), decoupled from the system.
+template <int MAXM, int NC, class GetB>
+__device__ __forceinline__ void part_eliminate(double (&a)[MAXM], double (&c)[MAXM], double (&f)[MAXM][NC],
+                                               const GetB& getb) {
+    {
+        const double b0 = getb(0), b1 = getb(1);
+        a[0] = a[0] / b0;
+        c[0] = c[0] / b0;
+        a[1] = a[1] / b1;
+        c[1] = c[1] / b1;
+#pragma unroll
+        for (int q = 0; q < NC; q++) {
+            f[0][q] = f[0][q] / b0;
+            f[1][q] = f[1][q] / b1;
+        }
+    }
+#pragma unroll
+    for (int r = 2; r < MAXM; r++) {
+        const double rr = 1.0 / (getb(r) - a[r] * c[r - 1]);
+#pragma unroll
+        for (int q = 0; q < NC; q++) f[r][q] = rr * (f[r][q] - a[r] * f[r - 1][q]);
+        c[r] = rr * c[r];
+        a[r] = -(rr * a[r] * a[r - 1]);
+    }
+#pragma unroll
+    for (int r = MAXM - 3; r >= 1; r--) {
+#pragma unroll
+        for (int q = 0; q < NC; q++) f[r][q] = f[r][q] - c[r] * f[r + 1][q];
+        a[r] = a[r] - c[r] * a[r + 1];
+        c[r] = -(c[r] * c[r + 1]);
+    }
+    {
+        const double rr = 1.0 / (1.0 - a[1] * c[0]);
+#pragma unroll
+        for (int q = 0; q < NC; q++) f[0][q] = rr * (f[0][q] - c[0] * f[1][q]);
+        a[0] = rr * a[0];
+        c[0] = -(rr * c[0] * c[1]);
+    }
+}
+
+// writes the two reduced rows of this partition, solves the reduced systems
+// (one column per lane of warp 0), returns x_first / x_last of the partition
+template <int MAXM, int NC>
+__device__ __forceinline__ void part_reduced(int P, int w, int lane, const double (&a)[MAXM], const double (&c)[MAXM],
+                                             const double (&f)[MAXM][NC], double* sm, double (&xf)[NC], double (&xl)[NC]) {
+    const int n2 = 2 * P;
+    double* RA = sm;                          // [n2][32]
+    double* RC = RA + n2 * 32;                // [n2][32]
+    double* RW = RC + n2 * 32;                // [n2][32] Thomas factors
+    double* RF = RW + n2 * 32;                // [n2][NC][32]
+    const double al = a[MAXM - 1], cl = c[MAXM - 1];
+    double fl[NC];
+#pragma unroll
+    for (int q = 0; q < NC; q++) fl[q] = f[MAXM - 1][q];
+    const int r0 = 2 * w, r1 = 2 * w + 1;
+    RA[r0 * 32 + lane] = a[0];
+    RC[r0 * 32 + lane] = c[0];
+    RA[r1 * 32 + lane] = al;
+    RC[r1 * 32 + lane] = cl;
+#pragma unroll
+    for (int q = 0; q < NC; q++) {
+        RF[(r0 * NC + q) * 32 + lane] = f[0][q];
+        RF[(r1 * NC + q) * 32 + lane] = fl[q];
+    }
+    __syncthreads();
+    if (w == 0) {
+        // unit-diagonal Thomas (InverseTridiagonal, src/m_Tools.f90:224-251)
+        double vecm = 1.0;
+        double fp[NC];
+#pragma unroll
+        for (int q = 0; q < NC; q++) fp[q] = RF[(0 * NC + q) * 32 + lane];
+        for (int r = 1; r < n2; r++) {
+            const double arr = RC[(r - 1) * 32 + lane] / vecm;
+            const double ar = RA[r * 32 + lane];
+            RW[r * 32 + lane] = arr;
+            vecm = 1.0 - ar * arr;
+#pragma unroll
+            for (int q = 0; q < NC; q++) {
+                const double v = (RF[(r * NC + q) * 32 + lane] - ar * fp[q]) / vecm;
+                RF[(r * NC + q) * 32 + lane] = v;
+                fp[q] = v;
+            }
+        }
+        for (int r = n2 - 2; r >= 0; r--) {
+            const double arr = RW[(r + 1) * 32 + lane];
+#pragma unroll
+            for (int q = 0; q < NC; q++) {
+                const double v = RF[(r * NC + q) * 32 + lane] - arr * fp[q];
+                RF[(r * NC + q) * 32 + lane] = v;
+                fp[q] = v;
+            }
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < NC; q++) {
+        xf[q] = RF[(r0 * NC + q) * 32 + lane];
+        xl[q] = RF[(r1 * NC + q) * 32 + lane];
+    }
+}
+
+// diagonal of row r of a partition starting at Fortran row s
+struct HelmDiag {
+    const double* ac;
+    double beta;
+    int s, ny;
+    bool vrow1;  // clcU2Hat: row 1 is the identity
+    __device__ __forceinline__ double operator()(int r) const {
+        const int jc = s + r;
+        if (jc > ny || (vrow1 && jc == 1)) return 1.0;
+        return -(beta * __ldg(&ac[jc])) + 1.0;
+    }
+};
+struct PoisDiag {
+    const double* ac2ph;
+    double lam;
+    int s, ny;
+    bool dc;  // kx = kz = 0: row 1 is the identity
+    __device__ __forceinline__ double operator()(int r) const {
+        const int jc = s + r;
+        if (jc > ny || (dc && jc == 1)) return 1.0;
+        return __ldg(&ac2ph[jc]) + lam;
+    }
+};
+
+// ---------------------------------------------------------------------------
+// Helmholtz: comp 0 ux (clcU1Hat), 1 uy (clcU2Hat), 2 uz (clcU3Hat),
+// 3 scalar (clcScalar); u(jc) += du(jc); uy and the scalar also get the
+// ghost values that SetBC_and_UpdateHaloForPrSrc / _scalar give them
+// ---------------------------------------------------------------------------
+template <int MR>
+__global__ void __launch_bounds__(512) k_helm(DConst cst, DMetric m, const DCoef* __restrict__ coef, int comp0,
+                                              Fields fl, const double* __restrict__ duy_ym,
+                                              const double* __restrict__ uy_ym) {
+    extern __shared__ double sm[];
+    const int lane = threadIdx.x, w = threadIdx.y, P = blockDim.y;
+    const int nx = cst.nx, ny = cst.ny;
+    const int i = blockIdx.x * 32 + lane;
+    const int k = blockIdx.y;
+    const int comp = comp0 + blockIdx.z;
+    const bool act = i < nx;
+    const int s = w * MR + 1;  // first Fortran row of this partition
+
+    const double *ap, *ac, *am, *rhs;
+    double* u;
+    double beta, add = 0.0;
+    if (comp == 0)      { ap = m.ap2cCN; ac = m.ac2cCN; am = m.am2cCN; u = fl.ux; rhs = fl.rx; beta = coef->pmBeta; add = coef->rhsx_add; }
+    else if (comp == 1) { ap = m.ap2p; ac = m.ac2p; am = m.am2p; u = fl.uy; rhs = fl.ry; beta = coef->pmBeta; }
+    else if (comp == 2) { ap = m.ap2cCN; ac = m.ac2cCN; am = m.am2cCN; u = fl.uz; rhs = fl.rz; beta = coef->pmBeta; }
+    else                { ap = m.ap2cScCN; ac = m.ac2cScCN; am = m.am2cScCN; u = fl.sc; rhs = fl.rc; beta = coef->pmBetaSc; }
+
+    const size_t zc = (size_t)k * cst.nyt * nx;
+    double a[MR], c[MR], f[MR][1];
+#pragma unroll
+    for (int r = 0; r < MR; r++) {
+        a[r] = 0.0; c[r] = 0.0; f[r][0] = 0.0;
+        const int jc = s + r;
+        if (jc <= ny) {
+            if (comp == 1 && jc == 1) {
+                f[r][0] = act ? duy_ym[(size_t)k * nx + i] : 0.0;
+            } else {
+                // aj(1) and cj(nyc) are never read by InverseTridiagonal
+                a[r] = (jc == 1) ? 0.0 : -(beta * __ldg(&am[jc]));
+                c[r] = (jc == ny) ? 0.0 : -(beta * __ldg(&ap[jc]));
+                f[r][0] = act ? rhs[zc + (size_t)jc * nx + i] + add : 0.0;
+            }
+        }
+    }
+    part_eliminate<MR, 1>(a, c, f, HelmDiag{ac, beta, s, ny, comp == 1});
+    double xf[1], xl[1];
+    part_reduced<MR, 1>(P, w, lane, a, c, f, sm, xf, xl);
+    if (!act) return;
+#pragma unroll
+    for (int r = 0; r < MR; r++) {
+        const int jc = s + r;
+        if (jc <= ny) {
+            double x;
+            if (r == 0) x = xf[0];
+            else if (r == MR - 1) x = xl[0];
+            else x = f[r][0] - a[r] * xf[0] - c[r] * xl[0];
+            const size_t q = zc + (size_t)jc * nx + i;
+            double un = u[q] + x;
+            if (comp == 1 && jc == 1) un = uy_ym[(size_t)k * nx + i];
+            u[q] = un;
+            if (comp == 1 && jc == ny) u[q + nx] = (cst.flow_type == 1) ? cst.uybc_yp : 0.0;
+            if (comp == 3 && jc == 1) u[q - nx] = cst.sc_r1b * un + cst.sc_r2b;
+            if (comp == 3 && jc == ny) u[q + nx] = cst.sc_r1t * un + cst.sc_r2t;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// spectral y-solve of clcPPE_x1 (src/m_Poisson.f90:383-430) on the complex
+// coefficients spec[(k*ny + j)*(nx/2+1) + kx].  The real and imaginary parts
+// are two real right-hand sides of the same real matrix, so the array is
+// treated as 2*(nx/2+1) real columns: lane pairs share kx and a warp reads
+// 256 contiguous bytes per row.  The kx = kz = 0 system has its first row
+// replaced by phi = 0 (src/m_Poisson.f90:399-404).
+// ---------------------------------------------------------------------------
+template <int MR>
+__global__ void __launch_bounds__(512) k_ysolve(DConst cst, DMetric m, double* __restrict__ specd) {
+    extern __shared__ double sm[];
+    const int lane = threadIdx.x, w = threadIdx.y, P = blockDim.y;
+    const int ny = cst.ny, ncol = 2 * (cst.nx / 2 + 1);
+    const int cr = blockIdx.x * 32 + lane;
+    const int kx = cr >> 1;
+    const int k = blockIdx.y;
+    const bool act = cr < ncol;
+    const int s = w * MR + 1;
+    const double lam = act ? __ldg(&m.wnx[kx]) + __ldg(&m.wnz[k]) : 0.0;
+    const bool dc = (kx == 0 && k == 0);
+    double* col = specd + (size_t)k * ny * ncol + (act ? cr : 0);
+    double a[MR], c[MR], f[MR][1];
+#pragma unroll
+    for (int r = 0; r < MR; r++) {
+        a[r] = 0.0; c[r] = 0.0; f[r][0] = 0.0;
+        const int jc = s + r;
+        if (jc <= ny && !(dc && jc == 1)) {
+            a[r] = (jc == 1) ? 0.0 : __ldg(&m.am2ph[jc]);
+            c[r] = (jc == ny) ? 0.0 : __ldg(&m.ap2ph[jc]);
+            if (act) f[r][0] = col[(size_t)(jc - 1) * ncol];
+        }
+    }
+    part_eliminate<MR, 1>(a, c, f, PoisDiag{m.ac2ph, lam, s, ny, dc});
+    double xf[1], xl[1];
+    part_reduced<MR, 1>(P, w, lane, a, c, f, sm, xf, xl);
+    if (!act) return;
+#pragma unroll
+    for (int r = 0; r < MR; r++) {
+        const int jc = s + r;
+        if (jc <= ny) {
+            double x;
+            if (r == 0) x = xf[0];
+            else if (r == MR - 1) x = xl[0];
+            else x = f[r][0] - a[r] * xf[0] - c[r] * xl[0];
+            col[(size_t)(jc - 1) * ncol] = x;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// launchers: partition length MR in {8, 12, 16}, P = ceil(ny/MR) <= 16 warps
+// ---------------------------------------------------------------------------
+static int part_len(int ny) { return ny <= 64 ? 8 : (ny <= 192 ? 12 : 16); }
+
+int tridiag_partitions(int ny) {
+    const int mr = part_len(ny);
+    return (ny + mr - 1) / mr;
+}
+
+bool tridiag_supported(int ny) { return ny >= 3 && ny <= 256; }
+
+static size_t red_smem(int P, int nc) { return (size_t)2 * P * 32 * (3 + nc) * sizeof(double); }
+
+void tridiag_init() {
+    cudaFuncSetAttribute(k_helm<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
+    cudaFuncSetAttribute(k_helm<12>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
+    cudaFuncSetAttribute(k_helm<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
+    cudaFuncSetAttribute(k_ysolve<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
+    cudaFuncSetAttribute(k_ysolve<12>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
+    cudaFuncSetAttribute(k_ysolve<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
+}
+
+static void helm_dispatch(cudaStream_t st, const DConst& c, const DMetric& m, const DCoef* coef, int comp0, int ncomp,
+                          const Fields& f, const double* duy_ym, const double* uy_ym) {
+    const int mr = part_len(c.ny), P = tridiag_partitions(c.ny);
+    dim3 blk(32, P);
+    dim3 grd((c.nx + 31) / 32, c.nz, ncomp);
+    const size_t sm = red_smem(P, 1);
+    if (mr == 8) k_helm<8><<<grd, blk, sm, st>>>(c, m, coef, comp0, f, duy_ym, uy_ym);
+    else if (mr == 12) k_helm<12><<<grd, blk, sm, st>>>(c, m, coef, comp0, f, duy_ym, uy_ym);
+    else k_helm<16><<<grd, blk, sm, st>>>(c, m, coef, comp0, f, duy_ym, uy_ym);
+}
+
+void launch_helm(cudaStream_t st, const DConst& c, const DMetric& m, const DCoef* coef, const Fields& f,
+                 const double* duy_ym, const double* uy_ym) {
+    helm_dispatch(st, c, m, coef, 0, 3, f, duy_ym, uy_ym);
+}
+
+void launch_helm_scalar(cudaStream_t st, const DConst& c, const DMetric& m, const DCoef* coef, const Fields& f) {
+    helm_dispatch(st, c, m, coef, 3, 1, f, nullptr, nullptr);
+}
+
+void launch_ysolve(cudaStream_t st, const DConst& c, const DMetric& m, double2* spec) {
+    const int mr = part_len(c.ny), P = tridiag_partitions(c.ny);
+    dim3 blk(32, P);
+    dim3 grd((2 * (c.nx / 2 + 1) + 31) / 32, c.nz);
+    const size_t sm = red_smem(P, 1);
+    double* sd = reinterpret_cast<double*>(spec);
+    if (mr == 8) k_ysolve<8><<<grd, blk, sm, st>>>(c, m, sd);
+    else if (mr == 12) k_ysolve<12><<<grd, blk, sm, st>>>(c, m, sd);
+    else k_ysolve<16><<<grd, blk, sm, st>>>(c, m, sd);
+}
+
+}  // namespace ptc

@@ -1,0 +1,296 @@
+"""ctypes binding of libparatc_gpu.so (include/paratc.h) and a thin host-side
+mirror of ParaTC's channel interface.
+
+ChannelSystem follows m_ChannelSystem (src/m_ChannelSystem.f90): construction
+is ChannelInitialize minus file IO, iterate() is ChannelIterate, and the
+Poisson entry point mirrors the clcPPE procedure pointer
+(src/m_Poisson.f90:16).  Every call goes through the CUDA library; there is no
+CPU fallback -- a missing library or device raises.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+from .abi import (LAYOUT_INTERIOR, PARATC_ERR_DIV_LIMIT, PARATC_ERR_VEL_LIMIT, PARATC_OK, ParatcDiag,
+                  ParatcParams)
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_lib", "libparatc_gpu.so")
+_lib = None
+_dp = ctypes.POINTER(ctypes.c_double)
+_i32p = ctypes.POINTER(ctypes.c_int32)
+
+EXPORTED = [
+    "paratc_mesh_ycoord", "paratc_params_from_namelist", "paratc_run_options_from_namelist", "paratc_create",
+    "paratc_destroy", "paratc_stream", "paratc_set_fields", "paratc_get_fields", "paratc_set_fields_device",
+    "paratc_get_fields_device", "paratc_set_time", "paratc_get_time", "paratc_step", "paratc_steps",
+    "paratc_substep", "paratc_substep_stage", "paratc_get_work", "paratc_poisson", "paratc_poisson_device", "paratc_project", "paratc_diagnostics",
+    "paratc_write_restart", "paratc_read_restart", "paratc_strerror", "paratc_last_error", "paratc_launch_count",
+    "paratc_profile_enable", "paratc_profile_get", "paratc_profile_name", "paratc_steps_async", "paratc_last_diag",
+]
+PROF_NKERNELS = 16
+
+
+class ParatcError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("paratc error %d (%s): %s" % (code, _strerror(code), msg))
+        self.code = code
+
+
+def load(path=None):
+    """Loads the library (building it first if it is missing and nvcc exists)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = path or LIB_PATH
+    if not os.path.exists(path):
+        from . import build as _build
+        _build.build()
+    L = ctypes.CDLL(path)
+    L.paratc_mesh_ycoord.argtypes = [ctypes.c_int, _dp, _dp, _i32p, _i32p, _i32p, ctypes.c_double, _dp]
+    L.paratc_params_from_namelist.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(ParatcParams), _dp,
+                                              ctypes.c_int]
+    L.paratc_create.argtypes = [ctypes.POINTER(ParatcParams), _dp, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]
+    L.paratc_destroy.argtypes = [ctypes.c_void_p]
+    L.paratc_stream.argtypes = [ctypes.c_void_p]
+    L.paratc_stream.restype = ctypes.c_void_p
+    L.paratc_set_fields.argtypes = [ctypes.c_void_p] + [_dp] * 9 + [ctypes.c_int]
+    L.paratc_get_fields.argtypes = [ctypes.c_void_p] + [_dp] * 9 + [ctypes.c_int]
+    L.paratc_set_fields_device.argtypes = [ctypes.c_void_p] + [ctypes.c_void_p] * 9
+    L.paratc_get_fields_device.argtypes = [ctypes.c_void_p] + [ctypes.c_void_p] * 9
+    L.paratc_set_time.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double]
+    L.paratc_get_time.argtypes = [ctypes.c_void_p, _dp, _dp]
+    L.paratc_step.argtypes = [ctypes.c_void_p, ctypes.POINTER(ParatcDiag)]
+    L.paratc_steps.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ParatcDiag)]
+    L.paratc_substep.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, _dp]
+    L.paratc_substep_stage.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_int, _dp]
+    L.paratc_get_work.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp]
+    L.paratc_poisson.argtypes = [ctypes.c_void_p, _dp, _dp]
+    L.paratc_poisson_device.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+    L.paratc_project.argtypes = [ctypes.c_void_p, _dp]
+    L.paratc_diagnostics.argtypes = [ctypes.c_void_p, ctypes.POINTER(ParatcDiag)]
+    L.paratc_write_restart.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int]
+    L.paratc_read_restart.argtypes = [ctypes.c_void_p, ctypes.c_char_p]
+    L.paratc_strerror.argtypes = [ctypes.c_int]
+    L.paratc_strerror.restype = ctypes.c_char_p
+    L.paratc_last_error.argtypes = [ctypes.c_void_p]
+    L.paratc_last_error.restype = ctypes.c_char_p
+    L.paratc_launch_count.argtypes = [ctypes.c_void_p]
+    L.paratc_launch_count.restype = ctypes.c_int64
+    L.paratc_steps_async.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    L.paratc_last_diag.argtypes = [ctypes.c_void_p, ctypes.POINTER(ParatcDiag)]
+    L.paratc_profile_enable.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    L.paratc_profile_get.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, ctypes.POINTER(ctypes.c_int64)]
+    L.paratc_profile_name.argtypes = [ctypes.c_int]
+    L.paratc_profile_name.restype = ctypes.c_char_p
+    _lib = L
+    return L
+
+
+def _strerror(code):
+    try:
+        return load().paratc_strerror(int(code)).decode()
+    except Exception:
+        return "?"
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(_dp)
+
+
+def _f64(a, shape):
+    if a is None:
+        return None
+    return np.ascontiguousarray(a, dtype=np.float64).reshape(shape)
+
+
+def mesh_ycoord(mesh, yly):
+    """yp(1..nyp) for a cases.Mesh (clcYcoord, src/m_MeshAndMetries.f90:340-408)."""
+    L = load()
+    sl = np.ascontiguousarray(mesh.section_length, dtype=np.float64)
+    cs = np.ascontiguousarray(mesh.section_cstret, dtype=np.float64)
+    ny = np.ascontiguousarray(mesh.nyc_section, dtype=np.int32)
+    st = np.ascontiguousarray(mesh.stret_type, dtype=np.int32)
+    so = np.ascontiguousarray(mesh.stret_option, dtype=np.int32)
+    out = np.zeros(int(ny.sum()) + 1)
+    rc = L.paratc_mesh_ycoord(len(sl), _ptr(sl), _ptr(cs), ny.ctypes.data_as(_i32p), st.ctypes.data_as(_i32p),
+                              so.ctypes.data_as(_i32p), float(yly), _ptr(out))
+    if rc != PARATC_OK:
+        raise ParatcError(rc, "paratc_mesh_ycoord")
+    return out
+
+
+def params_from_namelist(path, scalar_on=False, nyp_cap=8192):
+    L = load()
+    p = ParatcParams()
+    yp = np.zeros(nyp_cap)
+    rc = L.paratc_params_from_namelist(path.encode(), int(bool(scalar_on)), ctypes.byref(p), _ptr(yp), nyp_cap)
+    if rc != PARATC_OK:
+        raise ParatcError(rc, "paratc_params_from_namelist(%s)" % path)
+    return p, yp[: p.nyc + 1].copy()
+
+
+class ChannelSystem:
+    """One B200 context: the module state of a ParaTC run on one GPU."""
+
+    FIELDS = ("ux", "uy", "uz", "p", "c", "hx", "hy", "hz", "hc")
+
+    def __init__(self, params, yp, device=-1):
+        L = load()
+        self.params = params.copy()
+        self.shape = (params.nzc, params.nyc, params.nxc)
+        self._yp = np.ascontiguousarray(yp, dtype=np.float64)
+        h = ctypes.c_void_p()
+        rc = L.paratc_create(ctypes.byref(self.params), _ptr(self._yp), int(device), ctypes.byref(h))
+        if rc != PARATC_OK:
+            raise ParatcError(rc, "paratc_create")
+        self._h = h
+        self._L = L
+
+    # -- lifetime
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.paratc_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _check(self, rc, what):
+        if rc != PARATC_OK:
+            raise ParatcError(rc, "%s: %s" % (what, self._L.paratc_last_error(self._h).decode()))
+
+    @property
+    def handle(self):
+        return self._h
+
+    @property
+    def stream(self):
+        return self._L.paratc_stream(self._h)
+
+    @property
+    def launches(self):
+        return int(self._L.paratc_launch_count(self._h))
+
+    # -- state
+    def set_fields(self, ux, uy, uz, p, c=None, hx=None, hy=None, hz=None, hc=None, layout=LAYOUT_INTERIOR):
+        shape = self.shape if layout == LAYOUT_INTERIOR else (self.params.nzc + 4, self.params.nyc + 2, self.params.nxc + 4)
+        arrs = [_f64(a, shape) for a in (ux, uy, uz, p, c, hx, hy, hz, hc)]
+        self._check(self._L.paratc_set_fields(self._h, *[_ptr(a) for a in arrs], int(layout)), "paratc_set_fields")
+
+    def get_fields(self, names=None, layout=LAYOUT_INTERIOR):
+        names = names or self.FIELDS
+        shape = self.shape if layout == LAYOUT_INTERIOR else (self.params.nzc + 4, self.params.nyc + 2, self.params.nxc + 4)
+        out = {}
+        ptrs = []
+        for n in self.FIELDS:
+            if n in names and (n not in ("c", "hc") or self.params.scalar_on):
+                out[n] = np.zeros(shape)
+                ptrs.append(_ptr(out[n]))
+            else:
+                ptrs.append(None)
+        self._check(self._L.paratc_get_fields(self._h, *ptrs, int(layout)), "paratc_get_fields")
+        return out
+
+    def get_fields_into(self, out, layout=LAYOUT_INTERIOR):
+        """Copies the fields named in `out` into its (C-contiguous float64) arrays."""
+        ptrs = [_ptr(out[n]) if n in out and out[n] is not None else None for n in self.FIELDS]
+        self._check(self._L.paratc_get_fields(self._h, *ptrs, int(layout)), "paratc_get_fields")
+
+    def set_time(self, sim_time, dt):
+        self._check(self._L.paratc_set_time(self._h, float(sim_time), float(dt)), "paratc_set_time")
+
+    def get_time(self):
+        a, b = ctypes.c_double(), ctypes.c_double()
+        self._check(self._L.paratc_get_time(self._h, ctypes.byref(a), ctypes.byref(b)), "paratc_get_time")
+        return a.value, b.value
+
+    # -- hot path
+    def iterate(self, nsteps=1, raise_on_guard=True):
+        """ChannelIterate nsteps times; returns the last step's ParatcDiag."""
+        d = ParatcDiag()
+        rc = self._L.paratc_steps(self._h, int(nsteps), ctypes.byref(d))
+        if rc in (PARATC_ERR_DIV_LIMIT, PARATC_ERR_VEL_LIMIT) and not raise_on_guard:
+            return d
+        self._check(rc, "paratc_steps")
+        return d
+
+    def iterate_async(self, nsteps=1):
+        """Enqueues nsteps steps on the context stream without waiting."""
+        self._check(self._L.paratc_steps_async(self._h, int(nsteps)), "paratc_steps_async")
+
+    def last_diag(self, raise_on_guard=True):
+        d = ParatcDiag()
+        rc = self._L.paratc_last_diag(self._h, ctypes.byref(d))
+        if rc in (PARATC_ERR_DIV_LIMIT, PARATC_ERR_VEL_LIMIT) and not raise_on_guard:
+            return d
+        self._check(rc, "paratc_last_diag")
+        return d
+
+    def substep(self, ns, dt):
+        dm = ctypes.c_double()
+        self._check(self._L.paratc_substep(self._h, int(ns), float(dt), ctypes.byref(dm)), "paratc_substep")
+        return dm.value
+
+    WORK = {"rhsx": 0, "rhsy": 1, "rhsz": 2, "rhsc": 3, "prsrc": 4, "phi": 5}
+
+    def substep_stage(self, ns, dt, stop_stage):
+        dm = ctypes.c_double()
+        self._check(self._L.paratc_substep_stage(self._h, int(ns), float(dt), int(stop_stage), ctypes.byref(dm)),
+                    "paratc_substep_stage")
+        return dm.value
+
+    def get_work(self, name):
+        out = np.empty(self.shape)
+        self._check(self._L.paratc_get_work(self._h, self.WORK[name], _ptr(out)), "paratc_get_work")
+        return out
+
+    def poisson(self, src):
+        src = _f64(src, self.shape)
+        phi = np.empty(self.shape)
+        self._check(self._L.paratc_poisson(self._h, _ptr(src), _ptr(phi)), "paratc_poisson")
+        return phi
+
+    def poisson_device(self, d_src_ptr, d_phi_ptr):
+        self._check(self._L.paratc_poisson_device(self._h, ctypes.c_void_p(d_src_ptr), ctypes.c_void_p(d_phi_ptr)),
+                    "paratc_poisson_device")
+
+    def project(self):
+        dm = ctypes.c_double()
+        self._check(self._L.paratc_project(self._h, ctypes.byref(dm)), "paratc_project")
+        return dm.value
+
+    def diagnostics(self):
+        d = ParatcDiag()
+        self._check(self._L.paratc_diagnostics(self._h, ctypes.byref(d)), "paratc_diagnostics")
+        return d
+
+    def profile(self, on):
+        self._check(self._L.paratc_profile_enable(self._h, int(bool(on))), "paratc_profile_enable")
+
+    def profile_read(self):
+        """{kernel class: (total ms, launches)} since profile(True)."""
+        out = {}
+        for k in range(PROF_NKERNELS):
+            ms = ctypes.c_double()
+            n = ctypes.c_int64()
+            self._check(self._L.paratc_profile_get(self._h, k, ctypes.byref(ms), ctypes.byref(n)), "paratc_profile_get")
+            if n.value:
+                out[self._L.paratc_profile_name(k).decode()] = (ms.value, n.value)
+        return out
+
+    def write_restart(self, path, with_hist=False):
+        self._check(self._L.paratc_write_restart(self._h, path.encode(), int(bool(with_hist))), "paratc_write_restart")
+
+    def read_restart(self, path):
+        self._check(self._L.paratc_read_restart(self._h, path.encode()), "paratc_read_restart")

@@ -1,0 +1,125 @@
+"""The C ABI boundary (include/paratc.h) on the CPU: the library loads, exports
+every declared entry point, and its host-side set-up (y-grid, namelist
+reader, argument checks) matches the oracle.  No kernel is launched."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+from oracle import oracle_lib as ol
+from paratc_b200 import abi, cases, lib
+
+from .helpers import rel_err, yp_of
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+GOLD = os.path.join(ROOT, "tests", "golden")
+
+
+def _declared():
+    txt = open(os.path.join(ROOT, "include", "paratc.h")).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"\b(paratc_[a-z_0-9]+)\s*\(", txt)))
+
+
+def test_library_exports_every_declared_symbol():
+    L = lib.load()
+    names = _declared()
+    assert len(names) >= 20
+    for n in names:
+        assert hasattr(L, n), n
+    assert set(lib.EXPORTED) <= set(names)
+
+
+def test_header_structs_match_ctypes():
+    # offsets that a C compiler gives the structs, checked with a tiny probe
+    assert ctypes.sizeof(abi.ParatcParams) % 8 == 0
+    assert abi.ParatcParams.xlx.offset == 32
+    assert ctypes.sizeof(abi.ParatcDiag) == 12 * 8
+
+
+@pytest.mark.parametrize("mesh", [
+    cases.Mesh([1.0, 1.0], [1.5, 1.5], [48, 48], [1, 1], [0, 1]),
+    cases.Mesh([1.0], [0.9], [40], [2], [0]),
+    cases.Mesh([1.0, 3.0], [0.0, 1.05], [10, 30], [0, 3], [0, 1]),
+    cases.Mesh([2.0, 1.0, 1.0], [1.0, 2.0, 0.7], [16, 8, 9], [3, 1, 2], [1, 0, 1]),
+])
+def test_ycoord_library_matches_oracle(mesh):
+    a = lib.mesh_ycoord(mesh, 2.0)
+    b = ol.ycoord(mesh.section_length, mesh.section_cstret, mesh.nyc_section, mesh.stret_type, mesh.stret_option, 2.0)
+    assert np.array_equal(a, b)
+    assert a[0] == 0.0 and a[-1] == 2.0 and np.all(np.diff(a) > 0)
+
+
+def test_namelist_reader():
+    p, yp = lib.params_from_namelist(os.path.join(GOLD, "channel_small.prm"), scalar_on=True)
+    assert (p.nxc, p.nyc, p.nzc) == (32, 24, 16)
+    assert p.flow_type == 1 and p.is_ux_const == 1 and p.ischeme == 3 and p.icfl == 2
+    assert p.ucrf == 0.25 and p.ux_bc[2] == -0.25 and p.ux_bc[3] == -0.25
+    assert p.xnu == 2.381e-4 and p.dt_max == 0.005
+    assert p.sdiff == pytest.approx(2.381e-4 / 2.0, rel=1e-15)
+    assert list(p.gravity_eff_vec) == [0.0, -3.0, 0.0]
+    assert p.falling_vel_vec[0] == 0.25 and p.falling_vel_vec[1] == -0.02
+    assert list(p.scalar_bc_option) == [-3, -2] and p.scalar_bc_values[3] == 0.25
+    ref = cases.tanh_mesh(24, 1.5, True)
+    assert np.array_equal(yp, lib.mesh_ycoord(ref, 2.0))
+    L = lib.load()
+    ro = abi_run_options()
+    assert L.paratc_run_options_from_namelist(os.path.join(GOLD, "channel_small.prm").encode(), ctypes.byref(ro)) == 0
+    assert ro.run_name == b"Small/Chan" and ro.restart_dir == b"./restart/" and ro.ilast == 10
+    assert ro.backup_freq == 5 and ro.cmd_lfile_freq == 2
+
+
+class abi_run_options(ctypes.Structure):
+    _fields_ = [("ifirst", ctypes.c_int32), ("ilast", ctypes.c_int32), ("restart_flag", ctypes.c_int32),
+                ("backup_freq", ctypes.c_int32), ("cmd_lfile_freq", ctypes.c_int32),
+                ("run_name", ctypes.c_char * 64), ("res_dir", ctypes.c_char * 256),
+                ("restart_dir", ctypes.c_char * 256)]
+
+
+def test_namelist_errors(tmp_path):
+    src = open(os.path.join(GOLD, "channel_small.prm")).read()
+    bad = tmp_path / "odd.prm"
+    bad.write_text(src.replace("nxp = 33", "nxp = 32"))
+    with pytest.raises(lib.ParatcError) as e:
+        lib.params_from_namelist(str(bad))
+    assert e.value.code == abi.PARATC_ERR_BAD_ARG
+    with pytest.raises(lib.ParatcError) as e:
+        lib.params_from_namelist(str(tmp_path / "missing.prm"))
+    assert e.value.code == abi.PARATC_ERR_IO
+    bad2 = tmp_path / "ny.prm"
+    bad2.write_text(src.replace("nycSection    =  12    12", "nycSection    =  12    11"))
+    with pytest.raises(lib.ParatcError):
+        lib.params_from_namelist(str(bad2))
+
+
+def test_create_rejects_bad_arguments():
+    L = lib.load()
+    case = cases.small_channel(16, 12, 16)
+    yp = yp_of(case)
+    h = ctypes.c_void_p()
+    for field, val in (("nxc", 15), ("nzc", 2), ("ischeme", 4), ("flow_type", 3), ("icfl", 0), ("nyc", 300)):
+        p = case.params.copy()
+        setattr(p, field, val)
+        ypp = yp if field != "nyc" else np.linspace(0, 2, 301)
+        rc = L.paratc_create(ctypes.byref(p), ypp.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), 0, ctypes.byref(h))
+        assert rc == abi.PARATC_ERR_BAD_ARG, field
+    p = case.params.copy()
+    p.nyc = 13  # channel needs an even nyc
+    rc = L.paratc_create(ctypes.byref(p), np.linspace(0, 2, 14).ctypes.data_as(ctypes.POINTER(ctypes.c_double)), 0,
+                         ctypes.byref(h))
+    assert rc == abi.PARATC_ERR_BAD_ARG
+    assert L.paratc_strerror(abi.PARATC_ERR_DIV_LIMIT) == b"too big div"
+
+
+def test_no_cpu_fallback_without_device():
+    """Without a GPU the library refuses to create a context (it never falls
+    back to a CPU path)."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    case = cases.small_channel(16, 12, 16)
+    with pytest.raises(lib.ParatcError) as e:
+        lib.ChannelSystem(case.params, yp_of(case))
+    assert e.value.code == abi.PARATC_ERR_NO_DEVICE

@@ -1,0 +1,210 @@
+"""Pins of the CPU oracle (no GPU).
+
+The reference ships no tests or golden vectors and cannot run here, so the
+oracle is pinned by: numpy's FFT (FFTW's documented R2HC/HC2R convention),
+scipy's banded solver (the Thomas sweeps), an independent numpy restatement
+of the stencils, and discrete identities of the scheme.
+"""
+import numpy as np
+import pytest
+import scipy.linalg
+
+from oracle import np_restate
+from oracle import oracle_lib as ol
+from paratc_b200 import cases
+
+from .helpers import VARIANTS, discrete_poiseuille, fields_of, rel_err, variant, yp_of
+
+
+@pytest.mark.parametrize("n", [4, 6, 8, 12, 30, 48, 96, 128, 160, 192, 250, 768])
+def test_r2hc_matches_numpy(n):
+    x = np.random.default_rng(n).standard_normal(n)
+    X = np.fft.rfft(x)
+    ref = np.zeros(n)
+    ref[: n // 2 + 1] = X.real
+    for k in range(1, (n + 1) // 2):
+        ref[n - k] = X[k].imag
+    hc = ol.r2hc(x)
+    assert rel_err(hc, ref) < 1e-14
+    assert rel_err(ol.hc2r(hc) / n, x) < 1e-14
+
+
+def _padded(o, name):
+    h = o.get_halo(name)  # (nz+4, ny+2, nx+4)
+    return h[2:-2, :, 2:-2].copy()
+
+
+def _metric(o):
+    names = ["yp", "dyp", "rdyp", "rdyc", "YinterpCoe", "ap2c", "ac2c", "am2c", "ap2p", "ac2p", "am2p", "ap2cSc",
+             "ac2cSc", "am2cSc"]
+    return {n: o.metric(n) for n in names}
+
+
+@pytest.mark.parametrize("name", VARIANTS)
+def test_rhs_matches_numpy_restatement(name):
+    case = variant(name)
+    p = case.params
+    yp = yp_of(case)
+    o = ol.Oracle(p, yp, threads=2)
+    f = fields_of(case, yp)
+    o.set_fields(f["ux"], f["uy"], f["uz"], f["p"], f["c"])
+    dt = p.dt_max
+    o.substep(1, dt)  # histories non-zero
+    st = {n: _padded(o, n) for n in (["ux", "uy", "uz", "p"] + (["c"] if p.scalar_on else []))}
+    fo = o.get_fields()
+    hist = {n: fo[n] for n in ("hx", "hy", "hz", "hc") if fo[n] is not None}
+    ns = 2 if p.ischeme != 1 else 1
+    o.substep(ns, dt, stop_stage=1)
+    sim, dtt, pga = o.get_time()
+    g = [8 / 15, 5 / 12, 3 / 4] if p.ischeme == 3 else ([0.5, 1.0, 0] if p.ischeme == 2 else [1.5, 0, 0])
+    th = [0, -17 / 60, -5 / 12] if p.ischeme == 3 else ([0, -0.5, 0] if p.ischeme == 2 else [-0.5, 0, 0])
+    al = g[ns - 1] + th[ns - 1]
+    coef = dict(pmGamma=g[ns - 1] * dt, pmTheta=th[ns - 1] * dt, pmAlpha=al * dt, pmBeta=0.5 * al * p.xnu * dt,
+                pmBetaSc=0.5 * al * p.sdiff * dt)
+    out, newh, s3 = np_restate.rhs(p, _metric(o), coef, st, hist)
+    # flow-rate constraint (src/m_TScheme.f90:269-300)
+    if p.is_ux_const:
+        if p.scalar_on:
+            dpm = p.ubulk - p.ucrf - s3 / (p.nxc * p.nzc) / p.yly
+            out["rhsx"] = out["rhsx"] + al * dpm
+        else:
+            dpm = p.xnu * s3 / (p.nxc * p.nzc) / p.yly
+            out["rhsx"] = out["rhsx"] - al * dt * dpm
+    for n in out:
+        assert rel_err(o.get_work(n), out[n]) < 1e-12, n
+    fo = o.get_fields()
+    for n in newh:
+        assert rel_err(fo[n], newh[n]) < 1e-12, n
+
+
+@pytest.mark.parametrize("name", ["channel", "halfchannel_scalar", "channel_scalar_crf"])
+def test_helmholtz_matches_banded_solver(name):
+    case = variant(name)
+    p = case.params
+    yp = yp_of(case)
+    o = ol.Oracle(p, yp, threads=2)
+    f = fields_of(case, yp)
+    o.set_fields(f["ux"], f["uy"], f["uz"], f["p"], f["c"])
+    dt = p.dt_max
+    o.substep(1, dt, stop_stage=1)
+    rhs = {n: o.get_work(n) for n in ("rhsx", "rhsy", "rhsz", "rhsc") if n != "rhsc" or p.scalar_on}
+    before = o.get_fields()
+    beta = 0.5 * (8 / 15) * p.xnu * dt
+    o2 = ol.Oracle(p, yp, threads=2)
+    o2.set_fields(f["ux"], f["uy"], f["uz"], f["p"], f["c"])
+    o2.substep(1, dt, stop_stage=2)
+    after = o2.get_fields()
+    ny = p.nyc
+
+    def solve(am, ac, ap, rows):
+        ab = np.zeros((3, ny))
+        ab[0, 1:] = ap[:-1]
+        ab[1, :] = ac
+        ab[2, :-1] = am[1:]
+        return scipy.linalg.solve_banded((1, 1), ab, rows)
+
+    for comp, (u, r) in {"x": ("ux", "rhsx"), "z": ("uz", "rhsz")}.items():
+        am = -beta * o.metric("am2cForCN")
+        ap = -beta * o.metric("ap2cForCN")
+        ac = -beta * o.metric("ac2cForCN") + 1.0
+        rows = rhs[r].transpose(1, 0, 2).reshape(ny, -1)
+        du = solve(am, ac, ap, rows).reshape(ny, p.nzc, p.nxc).transpose(1, 0, 2)
+        assert rel_err(after[u] - before[u], du) < 1e-11, comp
+    am = -beta * o.metric("am2p")
+    ap = -beta * o.metric("ap2p")
+    ac = -beta * o.metric("ac2p") + 1.0
+    am[0], ac[0], ap[0] = 0.0, 1.0, 0.0
+    rows = rhs["rhsy"].transpose(1, 0, 2).reshape(ny, -1).copy()
+    rows[0] = 0.0
+    dv = solve(am, ac, ap, rows).reshape(ny, p.nzc, p.nxc).transpose(1, 0, 2)
+    assert rel_err(after["uy"][:, 1:] - before["uy"][:, 1:], dv[:, 1:]) < 1e-11
+    if p.scalar_on:
+        bs = 0.5 * (8 / 15) * p.sdiff * dt
+        am = -bs * o.metric("am2cScCN")
+        ap = -bs * o.metric("ap2cScCN")
+        ac = -bs * o.metric("ac2cScCN") + 1.0
+        rows = rhs["rhsc"].transpose(1, 0, 2).reshape(ny, -1)
+        dc = solve(am, ac, ap, rows).reshape(ny, p.nzc, p.nxc).transpose(1, 0, 2)
+        assert rel_err(after["c"] - before["c"], dc) < 1e-11
+
+
+def test_poisson_manufactured_oracle():
+    case = cases.small_channel(32, 24, 24)
+    p = case.params
+    yp = yp_of(case)
+    o = ol.Oracle(p, yp, threads=2)
+    nx, nz = p.nxc, p.nzc
+    x = np.arange(nx) * p.xlx / nx
+    z = np.arange(nz) * p.zlz / nz
+    yc = cases.cell_centres_y(yp)
+    gy = np.cos(np.pi * yc / p.yly) + 0.3 * yc
+    phi = np.cos(2 * np.pi * 3 * x / p.xlx)[None, None, :] * np.cos(2 * np.pi * 2 * z / p.zlz)[:, None, None] * gy[None, :, None]
+    wx = o.metric("WaveNumX")[3]
+    wz = o.metric("WaveNumZ")[2]
+    am, ac, ap = o.metric("am2ph"), o.metric("ac2ph"), o.metric("ap2ph")
+    Ly = np.diag(ac) + np.diag(am[1:], -1) + np.diag(ap[:-1], 1)
+    src = np.einsum("ij,kjl->kil", Ly, phi) + (wx + wz) * phi
+    assert rel_err(o.poisson(src), phi) < 1e-12
+
+
+def test_wavenumber_is_symbol_of_d4_squared():
+    """lambda(w) = (1/dx^2)/288 (cos3w - 54cos2w + 783cosw - 730) is the symbol
+    of D4 o D4 with D4 = (1/24, -9/8, 9/8, -1/24)/dx, so the discrete Poisson
+    operator is div o grad and the projected field is divergence free."""
+    case = cases.small_channel(32, 12, 24)
+    p = case.params
+    o = ol.Oracle(p, yp_of(case))
+    dx = p.xlx / p.nxc
+    w = 2 * np.pi * np.arange(p.nxc) / p.nxc
+    d4 = np.array([1 / 24, -9 / 8, 9 / 8, -1 / 24]) / dx
+    # D4 maps cell values to faces: symbol of D4(f)(i+1/2) = sum_m c_m e^{i w (m - 1/2)} with offsets -1,0,1,2
+    offs = np.array([-1, 0, 1, 2]) - 0.5
+    sym = np.array([np.sum(d4 * np.exp(1j * ww * offs)) for ww in w])
+    lam = (sym * np.conj(sym)).real * -1.0
+    assert rel_err(o.metric("WaveNumX"), lam) < 1e-13
+
+
+def test_projection_divergence_oracle():
+    case = cases.small_channel(32, 24, 16)
+    yp = yp_of(case)
+    o = ol.Oracle(case.params, yp, threads=2)
+    f = cases.initial_fields(case, yp)
+    o.set_fields(f["ux"], f["uy"], f["uz"], f["p"])
+    assert o.diagnostics().divmax > 1.0
+    assert o.project() < 1e-12
+    st = {n: _padded(o, n) for n in ("ux", "uy", "uz")}
+    assert np.abs(np_restate.divergence(case.params, _metric(o), st)).max() < 1e-12
+
+
+def test_poiseuille_is_fixed_point_oracle():
+    case = cases.small_channel(16, 24, 16)
+    p = case.params
+    yp = yp_of(case)
+    o = ol.Oracle(p, yp, threads=2)
+    u = discrete_poiseuille(o, p)
+    shape = (p.nzc, p.nyc, p.nxc)
+    ux = np.broadcast_to(u[None, :, None], shape).copy()
+    z = np.zeros(shape)
+    o.set_fields(ux, z, z, z)
+    for _ in range(3):
+        rc, d = o.step()
+        assert rc == 0
+    fo = o.get_fields()
+    assert np.abs(fo["ux"] - ux).max() < 1e-12
+    assert np.abs(fo["uy"]).max() < 1e-14 and np.abs(fo["uz"]).max() < 1e-14
+
+
+def test_oracle_thread_count_invariance():
+    case = variant("halfchannel_scalar")
+    yp = yp_of(case)
+    f = fields_of(case, yp)
+    outs = []
+    for t in (1, 3):
+        ol.set_threads(t)
+        o = ol.Oracle(case.params, yp)
+        o.set_fields(f["ux"], f["uy"], f["uz"], f["p"], f["c"])
+        o.step()
+        outs.append(o.get_fields())
+    ol.set_threads(0)
+    for n in ("ux", "uy", "uz", "p", "c"):
+        assert np.array_equal(outs[0][n], outs[1][n]), n
