@@ -222,6 +222,24 @@ int paratc_poisson(paratc_ctx* ctx, const double* src, double* phi);
 /* Same with device pointers (interior layout, nxc*nyc*nzc doubles). */
 int paratc_poisson_device(paratc_ctx* ctx, const double* d_src, double* d_phi);
 
+/* Poisson solve that allocates no memory.  No counterpart in the reference:
+ * it exists for callers that cannot call cudaMalloc (a loop with a fixed
+ * memory budget, a host code whose allocator owns all device memory, a
+ * caller that cannot keep a context alive between calls).  It solves the same
+ * system as paratc_poisson_device() for the grid of *prm and the y-grid yp
+ * (yp(1..nyp)), d_src -> d_phi (device pointers, interior layout), on
+ * `stream` (a cudaStream_t, NULL = default), and waits for the stream.
+ * Working memory is one fixed device array inside the library of
+ * PARATC_NOALLOC_SCRATCH_DOUBLES doubles (16 MiB, held by every GPU that
+ * loads the library until exit): grids needing more than
+ * 2*(nxc/2+1)*nyc*nzc + O(nxc+nyc+nzc) doubles, or nxc/nzc > 1024, nyc > 256,
+ * are rejected with PARATC_ERR_BAD_ARG.  The first call on a device looks up
+ * the array's device address (make it before any stream capture).  All calls
+ * share the array: calls that overlap on the GPU race. */
+#define PARATC_NOALLOC_SCRATCH_DOUBLES (2 * 1024 * 1024)
+int paratc_poisson_noalloc(const paratc_params* prm, const double* yp,
+                           const double* d_src, double* d_phi, void* stream);
+
 /* Makes the current velocity field discretely solenoidal with one pressure-free
  * projection (u -= grad(phi), Lap4(phi) = div u), the same operators as a
  * substep; used to prepare seeded initial fields. divmax_out may be NULL. */

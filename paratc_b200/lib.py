@@ -28,6 +28,7 @@ EXPORTED = [
     "paratc_substep", "paratc_substep_stage", "paratc_get_work", "paratc_poisson", "paratc_poisson_device", "paratc_project", "paratc_diagnostics",
     "paratc_write_restart", "paratc_read_restart", "paratc_strerror", "paratc_last_error", "paratc_launch_count",
     "paratc_profile_enable", "paratc_profile_get", "paratc_profile_name", "paratc_steps_async", "paratc_last_diag",
+    "paratc_poisson_noalloc",
 ]
 PROF_NKERNELS = 16
 
@@ -78,6 +79,8 @@ def load(path=None):
     L.paratc_last_error.restype = ctypes.c_char_p
     L.paratc_launch_count.argtypes = [ctypes.c_void_p]
     L.paratc_launch_count.restype = ctypes.c_int64
+    L.paratc_poisson_noalloc.argtypes = [ctypes.POINTER(ParatcParams), _dp, ctypes.c_void_p, ctypes.c_void_p,
+                                         ctypes.c_void_p]
     L.paratc_steps_async.argtypes = [ctypes.c_void_p, ctypes.c_int]
     L.paratc_last_diag.argtypes = [ctypes.c_void_p, ctypes.POINTER(ParatcDiag)]
     L.paratc_profile_enable.argtypes = [ctypes.c_void_p, ctypes.c_int]
