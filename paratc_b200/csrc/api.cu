@@ -9,6 +9,7 @@
 // diagnostics are read.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -29,7 +30,7 @@ enum ProfK {
     PK_FFTZ_B, PK_FFTX_B, PK_PROJECT, PK_CFL, PK_CHECK, PK_BC
 };
 static const char* kProfNames[PARATC_PROF_NKERNELS] = {
-    "coef", "uy_ym", "rhs", "flowrate", "helmholtz", "helmholtz_scalar", "prsrc", "fft_x_fwd", "fft_z_fwd",
+    "helm_factors", "uy_ym", "rhs", "flowrate", "helmholtz", "helmholtz_scalar", "prsrc", "fft_x_fwd", "fft_z_fwd",
     "ysolve", "fft_z_bwd", "fft_x_bwd", "project", "cfl", "check", "bc"};
 
 struct paratc_ctx {
@@ -47,9 +48,12 @@ struct paratc_ctx {
     double *d_src = nullptr, *d_phi = nullptr, *d_part = nullptr, *d_uy_ym = nullptr, *d_duy_ym = nullptr;
     double *d_metric = nullptr, *d_scal = nullptr;
     double2 *d_spec = nullptr, *d_twx = nullptr, *d_postx = nullptr, *d_twz = nullptr;
+    bool plane = false;  // whole y-planes fit one CTA: fused 2-D transforms
     DCoef* d_coef = nullptr;
     DDiag* d_diag = nullptr;
     DDiag* d_diag2 = nullptr;
+    unsigned int* d_counter = nullptr;  // grid-completion counters of the last-block reductions
+    double* d_hfac = nullptr;           // Helmholtz factors of the current substep (3 matrix types)
     DDiag* h_diag = nullptr;   // pinned
     DCoef* h_coef = nullptr;   // pinned
     double* h_scal = nullptr;  // pinned
@@ -129,7 +133,9 @@ int make_plan(int n, FftPlan& pl) {
     while (m % 2 == 0 && pl.nr < PT_MAX_RADIX_PASSES) { pl.rad[pl.nr++] = 2; m /= 2; }
     while (m % 3 == 0 && pl.nr < PT_MAX_RADIX_PASSES) { pl.rad[pl.nr++] = 3; m /= 3; }
     while (m % 5 == 0 && pl.nr < PT_MAX_RADIX_PASSES) { pl.rad[pl.nr++] = 5; m /= 5; }
-    return m == 1 ? PARATC_OK : PARATC_ERR_BAD_ARG;
+    pl.code = 0;
+    for (int s = 0; s < pl.nr && s < 16; s++) pl.code |= (unsigned long long)pl.rad[s] << (4 * s);
+    return (m == 1 && pl.nr <= 16) ? PARATC_OK : PARATC_ERR_BAD_ARG;
 }
 
 std::vector<double2> twiddles(int n, int count) {
@@ -142,8 +148,24 @@ std::vector<double2> twiddles(int n, int count) {
     return w;
 }
 
+// the y-solve and the inverse transform, after the forward spectrum is in d_spec
+void enqueue_poisson_tail(paratc_ctx* ctx, double* out, int padded) {
+    cudaStream_t st = ctx->st;
+    { PROF(PK_YSOLVE); launch_ysolve(st, ctx->kc, ctx->dm, ctx->d_spec); }
+    { PROF(PK_FFTX_B); launch_plane_inv(st, ctx->nx, ctx->ny, ctx->nz, ctx->d_spec, out, ctx->plx, ctx->plz, ctx->d_twx,
+                                        ctx->d_postx, ctx->d_twz, ctx->hm.normfft, padded); }
+    ctx->launches += 2;
+}
+
 void enqueue_poisson(paratc_ctx* ctx, const double* src, double* out, int padded) {
     cudaStream_t st = ctx->st;
+    if (ctx->plane) {
+        { PROF(PK_FFTX_F); launch_plane_fwd(st, 2, ctx->kc, ctx->dm, ctx->d_coef, ctx->f, src, ctx->d_spec, ctx->plx, ctx->plz,
+                                            ctx->d_twx, ctx->d_postx, ctx->d_twz, ctx->d_part, ctx->d_counter + 1, ctx->d_scal + 8); }
+        ctx->launches += 1;
+        enqueue_poisson_tail(ctx, out, padded);
+        return;
+    }
     const int nrows = ctx->ny * ctx->nz;
     { PROF(PK_FFTX_F); launch_fft_x_r2c(st, ctx->nx, nrows, src, ctx->d_spec, ctx->plx, ctx->d_twx, ctx->d_postx); }
     { PROF(PK_FFTZ_F); launch_fft_z(st, -1, ctx->nx, ctx->ny, ctx->nz, ctx->d_spec, ctx->plz, ctx->d_twz); }
@@ -159,20 +181,30 @@ void enqueue_poisson(paratc_ctx* ctx, const double* src, double* out, int padded
 void enqueue_substep(paratc_ctx* ctx, int ns, int stop = 5) {
     cudaStream_t st = ctx->st;
     const HostMetrics& h = ctx->hm;
-    { PROF(PK_COEF); launch_coef(st, ctx->d_coef, ns, h.gam[ns - 1], h.the[ns - 1], h.alp[ns - 1], ctx->prm.xnu, ctx->prm.sdiff); }
-    { PROF(PK_UYYM); launch_update_uy_ym(st, ctx->nx * ctx->nz, ctx->d_uy_ym, ctx->d_duy_ym); }
-    { PROF(PK_RHS); launch_rhs(st, ctx->kc, ctx->dm, ctx->d_coef, ctx->f, ctx->d_part); }
-    { PROF(PK_FLOWRATE); launch_flowrate(st, ctx->kc, ctx->d_coef, ctx->d_part, (int)cell_grid_blocks(ctx->kc)); }
-    ctx->launches += 4;
+    {
+        PROF(PK_RHS);
+        launch_rhs_tile(st, ctx->kc, ctx->dm, ctx->d_coef, ctx->f, ctx->d_uy_ym, ctx->d_duy_ym, ns, h.gam[ns - 1],
+                        h.the[ns - 1], h.alp[ns - 1], ctx->d_part, ctx->d_counter);
+    }
+    ctx->launches += 1;
     if (stop == 1) return;
-    if (ctx->prm.scalar_on) { PROF(PK_HELM_SC); launch_helm_scalar(st, ctx->kc, ctx->dm, ctx->d_coef, ctx->f); ctx->launches++; }
-    { PROF(PK_HELM); launch_helm(st, ctx->kc, ctx->dm, ctx->d_coef, ctx->f, ctx->d_duy_ym, ctx->d_uy_ym); }
+    if (ctx->prm.scalar_on) { PROF(PK_HELM_SC); launch_helm_scalar(st, ctx->kc, ctx->d_coef, ctx->f, ctx->d_hfac); ctx->launches++; }
+    { PROF(PK_HELM); launch_helm(st, ctx->kc, ctx->d_coef, ctx->f, ctx->d_duy_ym, ctx->d_uy_ym, ctx->d_hfac); }
     ctx->launches += 1;
     if (stop == 2) return;
-    { PROF(PK_PRSRC); launch_prsrc(st, ctx->kc, ctx->dm, ctx->d_coef, 0, ctx->f, ctx->d_src, ctx->d_part, &ctx->d_coef->divmax_src); }
-    ctx->launches += 2;
-    if (stop == 3) return;
-    enqueue_poisson(ctx, ctx->d_src, ctx->d_phi, 1);
+    if (ctx->plane && stop != 3) {
+        // clcPrSrc fused into the forward plane transform
+        { PROF(PK_FFTX_F); launch_plane_fwd(st, 0, ctx->kc, ctx->dm, ctx->d_coef, ctx->f, nullptr, ctx->d_spec, ctx->plx,
+                                            ctx->plz, ctx->d_twx, ctx->d_postx, ctx->d_twz, ctx->d_part,
+                                            ctx->d_counter + 1, &ctx->d_coef->divmax_src); }
+        ctx->launches += 1;
+        enqueue_poisson_tail(ctx, ctx->d_phi, 1);
+    } else {
+        { PROF(PK_PRSRC); launch_prsrc(st, ctx->kc, ctx->dm, ctx->d_coef, 0, ctx->f, ctx->d_src, ctx->d_part, &ctx->d_coef->divmax_src); }
+        ctx->launches += 2;
+        if (stop == 3) return;
+        enqueue_poisson(ctx, ctx->d_src, ctx->d_phi, 1);
+    }
     if (stop == 4) return;
     { PROF(PK_PROJECT); launch_project(st, ctx->kc, ctx->dm, ctx->d_coef, 0, ctx->d_phi, ctx->f, ctx->d_uy_ym); }
     ctx->launches += 1;
@@ -180,7 +212,8 @@ void enqueue_substep(paratc_ctx* ctx, int ns, int stop = 5) {
 
 void enqueue_step(paratc_ctx* ctx) {
     { PROF(PK_CFL); launch_cfl(ctx->st, ctx->kc, ctx->dm, ctx->f, ctx->d_coef, ctx->d_part); }
-    ctx->launches += 2;
+    { PROF(PK_COEF); launch_helm_factors(ctx->st, ctx->kc, ctx->dm, ctx->d_coef, 1, ctx->hm.iadvance, ctx->hm.alp, ctx->d_hfac); }
+    ctx->launches += 3;
     for (int ns = 1; ns <= ctx->hm.iadvance; ns++) enqueue_substep(ctx, ns);
     { PROF(PK_CHECK); launch_check(ctx->st, ctx->kc, ctx->dm, ctx->f, ctx->d_coef, ctx->d_diag, ctx->d_part); }
     ctx->launches += 2;
@@ -348,12 +381,15 @@ int paratc_create(const paratc_params* prm, const double* yp, int device, paratc
         delete ctx;
         return PARATC_ERR_BAD_ARG;
     }
+    ctx->plane = plane_supported(ctx->nx, ctx->nz, ctx->plx, ctx->plz) && std::getenv("PARATC_NO_PLANE_FFT") == nullptr;
     cudaError_t ce = cudaStreamCreateWithFlags(&ctx->st, cudaStreamNonBlocking);
     if (ce != cudaSuccess) { delete ctx; return PARATC_ERR_CUDA; }
     static bool inited = false;
     if (!inited) {
         fft_init();
         tridiag_init();
+        rhs_init();
+        plane_init();
         inited = true;
     }
     const HostMetrics& h = ctx->hm;
@@ -362,6 +398,7 @@ int paratc_create(const paratc_params* prm, const double* yp, int device, paratc
     std::memset(&kc, 0, sizeof(kc));
     kc.nx = ctx->nx; kc.ny = ctx->ny; kc.nz = ctx->nz; kc.nyp = ctx->nyp; kc.nyt = ctx->nyt;
     kc.flow_type = prm->flow_type; kc.scalar_on = prm->scalar_on; kc.is_ux_const = prm->is_ux_const; kc.icfl = prm->icfl;
+    cudaDeviceGetAttribute(&kc.nsm, cudaDevAttrMultiProcessorCount, ctx->dev);
     for (int q = 0; q < 4; q++) { kc.dxC[q] = h.dxC[q]; kc.dzC[q] = h.dzC[q]; kc.IC[q] = h.IC[q]; }
     for (int q = 0; q < 5; q++) { kc.dxxC[q] = h.dxxC[q]; kc.dzzC[q] = h.dzzC[q]; }
     kc.rdx = h.rdx; kc.rdz = h.rdz;
@@ -385,11 +422,13 @@ int paratc_create(const paratc_params* prm, const double* yp, int device, paratc
         for (double** p : fs)
             if ((rc = dalloc(ctx, p, nf)) != PARATC_OK) { paratc_destroy(ctx); return rc; }
     }
-    ctx->npart = cell_grid_blocks(kc) * 7 + 64;
+    ctx->npart = std::max(cell_grid_blocks(kc) * 7, rhs_grid_blocks(kc)) + 64;
     if ((rc = dalloc(ctx, &ctx->d_src, ctx->ni)) || (rc = dalloc(ctx, &ctx->d_spec, (size_t)ctx->M1 * ctx->ny * ctx->nz)) ||
         (rc = dalloc(ctx, &ctx->d_part, ctx->npart)) || (rc = dalloc(ctx, &ctx->d_uy_ym, (size_t)ctx->nx * ctx->nz)) ||
         (rc = dalloc(ctx, &ctx->d_duy_ym, (size_t)ctx->nx * ctx->nz)) || (rc = dalloc(ctx, &ctx->d_coef, 1)) ||
-        (rc = dalloc(ctx, &ctx->d_diag, 1)) || (rc = dalloc(ctx, &ctx->d_diag2, 1)) || (rc = dalloc(ctx, &ctx->d_scal, 16))) {
+        (rc = dalloc(ctx, &ctx->d_diag, 1)) || (rc = dalloc(ctx, &ctx->d_diag2, 1)) || (rc = dalloc(ctx, &ctx->d_scal, 16)) ||
+        (rc = dalloc(ctx, &ctx->d_counter, 16)) ||
+        (rc = dalloc(ctx, &ctx->d_hfac, helm_fac_doubles(ctx->ny)))) {
         paratc_destroy(ctx);
         return rc;
     }
@@ -570,6 +609,8 @@ int paratc_substep_stage(paratc_ctx* ctx, int ns, double dt, int stop_stage, dou
     if (rc) return rc;
     ctx->h_coef->dt = dt;
     CK(cudaMemcpyAsync(ctx->d_coef, ctx->h_coef, sizeof(DCoef), cudaMemcpyHostToDevice, ctx->st));
+    launch_helm_factors(ctx->st, ctx->kc, ctx->dm, ctx->d_coef, ns, 1, ctx->hm.alp, ctx->d_hfac);
+    ctx->launches += 1;
     enqueue_substep(ctx, ns, stop_stage);
     CK(cudaMemcpyAsync(ctx->h_coef, ctx->d_coef, sizeof(DCoef), cudaMemcpyDeviceToHost, ctx->st));
     rc = sync(ctx);
@@ -622,8 +663,15 @@ int paratc_project(paratc_ctx* ctx, double* divmax_out) {
     if (!ctx) return PARATC_ERR_BAD_ARG;
     CK(cudaSetDevice(ctx->dev));
     launch_bc_all(ctx->st, ctx->kc, ctx->f, ctx->d_uy_ym);
-    launch_prsrc(ctx->st, ctx->kc, ctx->dm, ctx->d_coef, 1, ctx->f, ctx->d_src, ctx->d_part, ctx->d_scal);
-    enqueue_poisson(ctx, ctx->d_src, ctx->d_phi, 1);
+    if (ctx->plane) {
+        launch_plane_fwd(ctx->st, 1, ctx->kc, ctx->dm, ctx->d_coef, ctx->f, nullptr, ctx->d_spec, ctx->plx, ctx->plz,
+                         ctx->d_twx, ctx->d_postx, ctx->d_twz, ctx->d_part, ctx->d_counter + 1, ctx->d_scal);
+        ctx->launches += 1;
+        enqueue_poisson_tail(ctx, ctx->d_phi, 1);
+    } else {
+        launch_prsrc(ctx->st, ctx->kc, ctx->dm, ctx->d_coef, 1, ctx->f, ctx->d_src, ctx->d_part, ctx->d_scal);
+        enqueue_poisson(ctx, ctx->d_src, ctx->d_phi, 1);
+    }
     launch_project(ctx->st, ctx->kc, ctx->dm, ctx->d_coef, 1, ctx->d_phi, ctx->f, ctx->d_uy_ym);
     launch_prsrc(ctx->st, ctx->kc, ctx->dm, ctx->d_coef, 1, ctx->f, nullptr, ctx->d_part, ctx->d_scal + 1);
     ctx->launches += 6;

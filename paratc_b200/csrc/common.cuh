@@ -34,6 +34,7 @@ struct DMetric {
 struct DConst {
     int nx, ny, nz, nyp, nyt;
     int flow_type, scalar_on, is_ux_const, icfl;
+    int nsm;  // streaming multiprocessors of the device
     double dxC[4], dzC[4], dxxC[5], dzzC[5], IC[4];
     double rdx, rdz;
     double ucrf, xnu, grav[3], sdiff, gev[3], fvv[3];
@@ -67,6 +68,7 @@ struct FftPlan {
     int n;          // transform length
     int nr;         // number of radix passes
     int rad[PT_MAX_RADIX_PASSES];
+    unsigned long long code;  // the radices again, 4 bits each (pass s at bits 4s..4s+3)
 };
 
 __device__ __forceinline__ int wrapi(int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); }

@@ -9,323 +9,11 @@
 // bitwise reproducible run to run.
 #include "common.cuh"
 #include "kernels.cuh"
+#include "reduce.cuh"
 
 namespace ptc {
 
-// ---------------------------------------------------------------------------
-// block reductions (deterministic)
-// ---------------------------------------------------------------------------
-template <int NV>
-__device__ __forceinline__ void block_sum_store(double (&v)[NV], double* __restrict__ out_block) {
-    __shared__ double sh[32][NV];
-    const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
-    const int nthr = blockDim.x * blockDim.y * blockDim.z;
-    const int lane = tid & 31, wid = tid >> 5, nw = (nthr + 31) >> 5;
-#pragma unroll
-    for (int q = 0; q < NV; q++)
-        for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_down_sync(0xffffffffu, v[q], o);
-    if (lane == 0)
-#pragma unroll
-        for (int q = 0; q < NV; q++) sh[wid][q] = v[q];
-    __syncthreads();
-    if (wid == 0) {
-#pragma unroll
-        for (int q = 0; q < NV; q++) {
-            double x = lane < nw ? sh[lane][q] : 0.0;
-            for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
-            if (lane == 0) out_block[q] = x;
-        }
-    }
-}
-
-template <int NV>
-__device__ __forceinline__ void block_max_store(double (&v)[NV], double* __restrict__ out_block) {
-    __shared__ double sh[32][NV];
-    const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
-    const int nthr = blockDim.x * blockDim.y * blockDim.z;
-    const int lane = tid & 31, wid = tid >> 5, nw = (nthr + 31) >> 5;
-#pragma unroll
-    for (int q = 0; q < NV; q++)
-        for (int o = 16; o > 0; o >>= 1) v[q] = fmax(v[q], __shfl_down_sync(0xffffffffu, v[q], o));
-    if (lane == 0)
-#pragma unroll
-        for (int q = 0; q < NV; q++) sh[wid][q] = v[q];
-    __syncthreads();
-    if (wid == 0) {
-#pragma unroll
-        for (int q = 0; q < NV; q++) {
-            double x = lane < nw ? sh[lane][q] : 0.0;
-            for (int o = 16; o > 0; o >>= 1) x = fmax(x, __shfl_down_sync(0xffffffffu, x, o));
-            if (lane == 0) out_block[q] = x;
-        }
-    }
-}
-
-// single-block reduction of nparts partial records of NV values, fixed order
-template <int NV, bool MAX>
-__device__ void reduce_parts(const double* __restrict__ parts, int nparts, double (&out)[NV]) {
-    __shared__ double sh[32][NV];
-    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nw = (blockDim.x + 31) >> 5;
-    double v[NV];
-#pragma unroll
-    for (int q = 0; q < NV; q++) v[q] = 0.0;
-    for (int b = tid; b < nparts; b += blockDim.x)
-#pragma unroll
-        for (int q = 0; q < NV; q++) v[q] = MAX ? fmax(v[q], parts[(size_t)b * NV + q]) : v[q] + parts[(size_t)b * NV + q];
-#pragma unroll
-    for (int q = 0; q < NV; q++)
-        for (int o = 16; o > 0; o >>= 1) {
-            double y = __shfl_down_sync(0xffffffffu, v[q], o);
-            v[q] = MAX ? fmax(v[q], y) : v[q] + y;
-        }
-    if (lane == 0)
-#pragma unroll
-        for (int q = 0; q < NV; q++) sh[wid][q] = v[q];
-    __syncthreads();
-#pragma unroll
-    for (int q = 0; q < NV; q++) {
-        double x = 0.0;
-        if (wid == 0) {
-            x = lane < nw ? sh[lane][q] : 0.0;
-            for (int o = 16; o > 0; o >>= 1) {
-                double y = __shfl_down_sync(0xffffffffu, x, o);
-                x = MAX ? fmax(x, y) : x + y;
-            }
-        }
-        out[q] = x;  // valid in thread 0
-    }
-}
-
-// ---------------------------------------------------------------------------
-// PMcoeUpdate (src/m_Parameters.f90:215-230), one thread
-// ---------------------------------------------------------------------------
-__global__ void k_coef(DCoef* coef, int ns, double gam, double the, double alp, double xnu, double sdiff) {
-    if (threadIdx.x != 0) return;
-    DCoef c = *coef;
-    const double dt = c.dt;
-    c.pmGamma = gam * dt;
-    c.pmTheta = the * dt;
-    c.pmAlpha = alp * dt;
-    c.pmBeta = 0.5 * alp * xnu * dt;
-    c.pmBetaSc = 0.5 * alp * sdiff * dt;
-    c.sim_time = c.sim_time + dt * alp;
-    c.pmAlphaC = alp;
-    if (ns == 1) c.pr_grad_aver = 0.0;
-    c.rhsx_add = 0.0;
-    c.ns = ns;
-    *coef = c;
-}
-
-// ---------------------------------------------------------------------------
-// clcRhsXYZ (src/m_TScheme.f90:113-360)
-// ---------------------------------------------------------------------------
 #define LD(A, off) __ldg(&(A)[off])
-
-template <bool SCALAR>
-__global__ void __launch_bounds__(256) k_rhs(DConst c, DMetric m, const DCoef* __restrict__ coef,
-                                             const double* __restrict__ ux, const double* __restrict__ uy,
-                                             const double* __restrict__ uz, const double* __restrict__ pr,
-                                             const double* __restrict__ sc, double* __restrict__ hx,
-                                             double* __restrict__ hy, double* __restrict__ hz,
-                                             double* __restrict__ hc, double* __restrict__ rx,
-                                             double* __restrict__ ry, double* __restrict__ rz,
-                                             double* __restrict__ rc, double* __restrict__ part) {
-    const int nx = c.nx;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int jc = blockIdx.y * blockDim.y + threadIdx.y + 1;
-    const int k = blockIdx.z;
-    double s3[1] = {0.0};
-    if (i < nx && jc <= c.ny) {
-        const double pmGamma = coef->pmGamma, pmTheta = coef->pmTheta, pmAlpha = coef->pmAlpha;
-        const double tb = 2.0 * coef->pmBeta;
-        const size_t pl = (size_t)c.nyt * nx;
-        int xo[7];
-        size_t zo[7];
-#pragma unroll
-        for (int d = 0; d < 7; d++) {
-            xo[d] = wrapi(i + d - 3, nx);
-            zo[d] = (size_t)wrapi(k + d - 3, c.nz) * pl;
-        }
-        const size_t r0 = (size_t)jc * nx, rm = r0 - nx, rp = r0 + nx;
-#define AT(A, dx, row, dz) LD(A, zo[3 + (dz)] + (row) + xo[3 + (dx)])
-        const double I1 = c.IC[0], I2 = c.IC[1], I3 = c.IC[2], I4 = c.IC[3];
-        const double ucrf = c.ucrf, xnu = c.xnu;
-        const bool top = (jc == c.ny);
-        const double IY1 = __ldg(&m.yinterp[jc]), IY2 = 1.0 - IY1;
-        const double IY3 = __ldg(&m.yinterp[jc + 1]), IY4 = 1.0 - IY3;
-        const double rdyp = __ldg(&m.rdyp[jc]), rdyc = __ldg(&m.rdyc[jc]), dyp = __ldg(&m.dyp[jc]);
-        const size_t q0 = zo[3] + r0 + i;
-
-        // ---------------- RhsX (:169-204)
-        double uxx[7], uxz[7];
-#pragma unroll
-        for (int d = 0; d < 7; d++) { uxx[d] = AT(ux, d - 3, r0, 0); uxz[d] = AT(ux, 0, r0, d - 3); }
-        const double uxc = uxx[3], uxjm = AT(ux, 0, rm, 0), uxjp = AT(ux, 0, rp, 0);
-        double conv_x, rhs_x;
-        {
-            const double uxhyc = IY1 * uxjm + IY2 * uxc;
-            const double uxhyp = IY3 * uxc + IY4 * uxjp;
-            double uxhx[4];
-#pragma unroll
-            for (int q = 0; q < 4; q++) uxhx[q] = I1 * uxx[q] + I2 * uxx[q + 1] + I3 * uxx[q + 2] + I4 * uxx[q + 3];
-            const double h11 = c.dxC[0] * uxhx[0] * (uxhx[0] + ucrf) + c.dxC[1] * uxhx[1] * (uxhx[1] + ucrf) +
-                               c.dxC[2] * uxhx[2] * (uxhx[2] + ucrf) + c.dxC[3] * uxhx[3] * (uxhx[3] + ucrf);
-            const double uyhx_j = I1 * AT(uy, -2, r0, 0) + I2 * AT(uy, -1, r0, 0) + I3 * AT(uy, 0, r0, 0) + I4 * AT(uy, 1, r0, 0);
-            const double uyhx_p = top ? 0.0 : I1 * AT(uy, -2, rp, 0) + I2 * AT(uy, -1, rp, 0) + I3 * AT(uy, 0, rp, 0) + I4 * AT(uy, 1, rp, 0);
-            const double h12 = (uyhx_p * uxhyp - uyhx_j * uxhyc) * rdyp;
-            double h13 = 0.0;
-#pragma unroll
-            for (int q = 0; q < 4; q++) {  // z offsets -1..2
-                const double uxhz = I1 * uxz[q] + I2 * uxz[q + 1] + I3 * uxz[q + 2] + I4 * uxz[q + 3];
-                const double uzhx = I1 * AT(uz, -2, r0, q - 1) + I2 * AT(uz, -1, r0, q - 1) + I3 * AT(uz, 0, r0, q - 1) + I4 * AT(uz, 1, r0, q - 1);
-                h13 = (q == 0) ? c.dzC[0] * uxhz * uzhx : h13 + c.dzC[q] * uxhz * uzhx;
-            }
-            const double d11 = c.dxxC[0] * uxx[1] + c.dxxC[1] * uxx[2] + c.dxxC[2] * uxx[3] + c.dxxC[3] * uxx[4] + c.dxxC[4] * uxx[5];
-            const double d22 = __ldg(&m.ap2c[jc]) * uxjp + __ldg(&m.ac2c[jc]) * uxc + __ldg(&m.am2c[jc]) * uxjm;
-            const double d33 = c.dzzC[0] * uxz[1] + c.dzzC[1] * uxz[2] + c.dzzC[2] * uxz[3] + c.dzzC[3] * uxz[4] + c.dzzC[4] * uxz[5];
-            const double dcq13 = d11 + d33;
-            s3[0] = SCALAR ? uxc * dyp : (dcq13 + d22) * dyp;
-            conv_x = -h11 - h12 - h13 + xnu * dcq13 + c.grav[0];
-            const double gradp = c.dxC[0] * AT(pr, -2, r0, 0) + c.dxC[1] * AT(pr, -1, r0, 0) + c.dxC[2] * AT(pr, 0, r0, 0) + c.dxC[3] * AT(pr, 1, r0, 0);
-            rhs_x = pmGamma * conv_x + pmTheta * hx[q0] - pmAlpha * gradp + tb * d22;
-        }
-
-        // ---------------- RhsY (:206-236)
-        double uyx[7], uyz[7];
-#pragma unroll
-        for (int d = 0; d < 7; d++) { uyx[d] = AT(uy, d - 3, r0, 0); uyz[d] = AT(uy, 0, r0, d - 3); }
-        double conv_y, rhs_y;
-        {
-            const double qsucac = 0.25 * rdyc;
-            double uxh[4], uzh[4];
-#pragma unroll
-            for (int q = 0; q < 4; q++) {  // offsets -1..2
-                uxh[q] = IY1 * AT(ux, q - 1, rm, 0) + IY2 * uxx[q + 2] + ucrf;
-                uzh[q] = IY1 * AT(uz, 0, rm, q - 1) + IY2 * AT(uz, 0, r0, q - 1);
-            }
-            double h21 = 0.0, h23 = 0.0;
-#pragma unroll
-            for (int q = 0; q < 4; q++) {
-                const double uyhx = I1 * uyx[q] + I2 * uyx[q + 1] + I3 * uyx[q + 2] + I4 * uyx[q + 3];
-                const double uyhz = I1 * uyz[q] + I2 * uyz[q + 1] + I3 * uyz[q + 2] + I4 * uyz[q + 3];
-                h21 = (q == 0) ? c.dxC[0] * uyhx * uxh[0] : h21 + c.dxC[q] * uyhx * uxh[q];
-                h23 = (q == 0) ? c.dzC[0] * uyhz * uzh[0] : h23 + c.dzC[q] * uyhz * uzh[q];
-            }
-            const double vp = AT(uy, 0, rp, 0), vc = uyx[3], vm = AT(uy, 0, rm, 0);
-            const double h22 = ((vp + vc) * (vp + vc) - (vc + vm) * (vc + vm)) * qsucac;
-            const double d11 = c.dxxC[0] * uyx[1] + c.dxxC[1] * uyx[2] + c.dxxC[2] * uyx[3] + c.dxxC[3] * uyx[4] + c.dxxC[4] * uyx[5];
-            const double d22 = __ldg(&m.ap2p[jc]) * vp + __ldg(&m.ac2p[jc]) * vc + __ldg(&m.am2p[jc]) * vm;
-            const double d33 = c.dzzC[0] * uyz[1] + c.dzzC[1] * uyz[2] + c.dzzC[2] * uyz[3] + c.dzzC[3] * uyz[4] + c.dzzC[4] * uyz[5];
-            conv_y = -h21 - h22 - h23 + xnu * (d11 + d33) + c.grav[1];
-            const double gradp = (AT(pr, 0, r0, 0) - AT(pr, 0, rm, 0)) * rdyc;
-            rhs_y = pmGamma * conv_y + pmTheta * hy[q0] - pmAlpha * gradp + tb * d22;
-        }
-
-        // ---------------- RhsZ (:238-267)
-        double uzx[7], uzz[7];
-#pragma unroll
-        for (int d = 0; d < 7; d++) { uzx[d] = AT(uz, d - 3, r0, 0); uzz[d] = AT(uz, 0, r0, d - 3); }
-        double conv_z, rhs_z;
-        {
-            const double uzc = uzx[3];
-            const double uzhyc = IY1 * AT(uz, 0, rm, 0) + IY2 * uzc;
-            const double uzhyp = IY3 * uzc + IY4 * AT(uz, 0, rp, 0);
-            double h31 = 0.0;
-#pragma unroll
-            for (int q = 0; q < 4; q++) {  // x offsets -1..2
-                const double uzhx = I1 * uzx[q] + I2 * uzx[q + 1] + I3 * uzx[q + 2] + I4 * uzx[q + 3];
-                const double uxhz = I1 * AT(ux, q - 1, r0, -2) + I2 * AT(ux, q - 1, r0, -1) + I3 * AT(ux, q - 1, r0, 0) + I4 * AT(ux, q - 1, r0, 1);
-                h31 = (q == 0) ? c.dxC[0] * uzhx * (uxhz + ucrf) : h31 + c.dxC[q] * uzhx * (uxhz + ucrf);
-            }
-            const double uyhz_j = I1 * uyz[1] + I2 * uyz[2] + I3 * uyz[3] + I4 * uyz[4];
-            const double uyhz_p = top ? 0.0 : I1 * AT(uy, 0, rp, -2) + I2 * AT(uy, 0, rp, -1) + I3 * AT(uy, 0, rp, 0) + I4 * AT(uy, 0, rp, 1);
-            const double h32 = (uyhz_p * uzhyp - uyhz_j * uzhyc) * rdyp;
-            double h33 = 0.0;
-#pragma unroll
-            for (int q = 0; q < 4; q++) {  // z offsets -2..1
-                const double uzhz = I1 * uzz[q] + I2 * uzz[q + 1] + I3 * uzz[q + 2] + I4 * uzz[q + 3];
-                h33 = (q == 0) ? c.dzC[0] * uzhz * uzhz : h33 + c.dzC[q] * uzhz * uzhz;
-            }
-            const double d11 = c.dxxC[0] * uzx[1] + c.dxxC[1] * uzx[2] + c.dxxC[2] * uzx[3] + c.dxxC[3] * uzx[4] + c.dxxC[4] * uzx[5];
-            const double d22 = __ldg(&m.ap2c[jc]) * AT(uz, 0, rp, 0) + __ldg(&m.ac2c[jc]) * uzc + __ldg(&m.am2c[jc]) * AT(uz, 0, rm, 0);
-            const double d33 = c.dzzC[0] * uzz[1] + c.dzzC[1] * uzz[2] + c.dzzC[2] * uzz[3] + c.dzzC[3] * uzz[4] + c.dzzC[4] * uzz[5];
-            conv_z = -h31 - h32 - h33 + xnu * (d11 + d33) + c.grav[2];
-            const double gradp = c.dzC[0] * AT(pr, 0, r0, -2) + c.dzC[1] * AT(pr, 0, r0, -1) + c.dzC[2] * AT(pr, 0, r0, 0) + c.dzC[3] * AT(pr, 0, r0, 1);
-            rhs_z = pmGamma * conv_z + pmTheta * hz[q0] - pmAlpha * gradp + tb * d22;
-        }
-
-        if (SCALAR) {
-            // ---------------- scalar transport (:302-357)
-            double scx[7], scz[7];
-#pragma unroll
-            for (int d = 0; d < 7; d++) { scx[d] = AT(sc, d - 3, r0, 0); scz[d] = AT(sc, 0, r0, d - 3); }
-            const double scc = scx[3];
-            double shx[4], shz[4];  // offsets -1..2
-#pragma unroll
-            for (int q = 0; q < 4; q++) {
-                shx[q] = I1 * scx[q] + I2 * scx[q + 1] + I3 * scx[q + 2] + I4 * scx[q + 3];
-                shz[q] = I1 * scz[q] + I2 * scz[q + 1] + I3 * scz[q + 2] + I4 * scz[q + 3];
-            }
-            const double scjm = AT(sc, 0, rm, 0), scjp = AT(sc, 0, rp, 0);
-            const double shyc = IY1 * scjm + IY2 * scc;
-            const double shyp = IY3 * scc + IY4 * scjp;
-            const double c1 = c.gev[0] * shx[1], c2 = c.gev[1] * shyc, c3 = c.gev[2] * shz[1];
-            rhs_x = rhs_x + pmGamma * c1;
-            rhs_y = rhs_y + pmGamma * c2;
-            rhs_z = rhs_z + pmGamma * c3;
-            conv_x = conv_x + c1;
-            conv_y = conv_y + c2;
-            conv_z = conv_z + c3;
-            double hc1 = 0.0, hc3 = 0.0;
-#pragma unroll
-            for (int q = 0; q < 4; q++) {
-                const double ua = AT(ux, q - 1, r0, 0) + c.fvv[0];
-                const double wa = AT(uz, 0, r0, q - 1) + c.fvv[2];
-                hc1 = (q == 0) ? c.dxC[0] * ua * shx[0] : hc1 + c.dxC[q] * ua * shx[q];
-                hc3 = (q == 0) ? c.dzC[0] * wa * shz[0] : hc3 + c.dzC[q] * wa * shz[q];
-            }
-            const double hc2 = ((AT(uy, 0, rp, 0) + c.fvv[1]) * shyp - (uyx[3] + c.fvv[1]) * shyc) * rdyp;
-            const double d11 = c.dxxC[0] * scx[1] + c.dxxC[1] * scx[2] + c.dxxC[2] * scc + c.dxxC[3] * scx[4] + c.dxxC[4] * scx[5];
-            const double d22 = __ldg(&m.ap2cSc[jc]) * scjp + __ldg(&m.ac2cSc[jc]) * scc + __ldg(&m.am2cSc[jc]) * scjm;
-            const double d33 = c.dzzC[0] * scz[1] + c.dzzC[1] * scz[2] + c.dzzC[2] * scc + c.dzzC[3] * scz[4] + c.dzzC[4] * scz[5];
-            const double convc = -hc1 - hc2 - hc3 + c.sdiff * (d11 + d33);
-            rc[q0] = coef->pmGamma * convc + pmTheta * hc[q0] + 2.0 * coef->pmBetaSc * d22;
-            hc[q0] = convc;
-        }
-#undef AT
-        rx[q0] = rhs_x;
-        ry[q0] = rhs_y;
-        rz[q0] = rhs_z;
-        hx[q0] = conv_x;
-        hy[q0] = conv_y;
-        hz[q0] = conv_z;
-    }
-    const int bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
-    block_sum_store<1>(s3, part + bid);
-}
-
-// flow-rate constraint (src/m_TScheme.f90:269-300): reduce s3tot, set the
-// uniform RhsX correction and accumulate PrGradAver
-__global__ void k_flowrate(DConst c, DCoef* coef, const double* __restrict__ part, int nparts) {
-    double s[1];
-    reduce_parts<1, false>(part, nparts, s);
-    if (threadIdx.x != 0) return;
-    DCoef f = *coef;
-    if (!c.is_ux_const) { f.rhsx_add = 0.0; *coef = f; return; }
-    double s3tot1 = s[0];
-    const double nxz = (double)(c.nx * c.nz);
-    if (c.scalar_on) {
-        s3tot1 = s3tot1 / nxz / c.yly;
-        const double dpmdxns = c.ubulk - c.ucrf - s3tot1;
-        f.rhsx_add = f.pmAlphaC * dpmdxns;
-        f.pr_grad_aver = f.pr_grad_aver + dpmdxns * f.pmAlphaC / f.dt;
-    } else {
-        const double dpmdxns = c.xnu * s3tot1 / nxz / c.yly;
-        f.rhsx_add = -(f.pmAlpha * dpmdxns);
-        f.pr_grad_aver = f.pr_grad_aver + dpmdxns * f.pmAlphaC;
-    }
-    *coef = f;
-}
 
 // ---------------------------------------------------------------------------
 // clcPrSrc (src/m_TScheme.f90:48-77) / CheckDivergence (src/m_Tools.f90:54-81)
@@ -594,23 +282,6 @@ static dim3 cell_grid(const DConst& c) { return dim3((c.nx + 31) / 32, (c.ny + 7
 size_t cell_grid_blocks(const DConst& c) {
     dim3 g = cell_grid(c);
     return (size_t)g.x * g.y * g.z;
-}
-
-void launch_coef(cudaStream_t st, DCoef* coef, int ns, double gam, double the, double alp, double xnu, double sdiff) {
-    k_coef<<<1, 32, 0, st>>>(coef, ns, gam, the, alp, xnu, sdiff);
-}
-
-void launch_rhs(cudaStream_t st, const DConst& c, const DMetric& m, const DCoef* coef, const Fields& f, double* part) {
-    if (c.scalar_on)
-        k_rhs<true><<<cell_grid(c), cell_block(), 0, st>>>(c, m, coef, f.ux, f.uy, f.uz, f.pr, f.sc, f.hx, f.hy, f.hz, f.hc,
-                                                            f.rx, f.ry, f.rz, f.rc, part);
-    else
-        k_rhs<false><<<cell_grid(c), cell_block(), 0, st>>>(c, m, coef, f.ux, f.uy, f.uz, f.pr, f.sc, f.hx, f.hy, f.hz, f.hc,
-                                                             f.rx, f.ry, f.rz, f.rc, part);
-}
-
-void launch_flowrate(cudaStream_t st, const DConst& c, DCoef* coef, const double* part, int nparts) {
-    k_flowrate<<<1, 1024, 0, st>>>(c, coef, part, nparts);
 }
 
 void launch_prsrc(cudaStream_t st, const DConst& c, const DMetric& m, const DCoef* coef, int unit_scale,

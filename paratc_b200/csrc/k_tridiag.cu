@@ -19,6 +19,7 @@
 // Helmholtz update) and one write per cell.
 #include "common.cuh"
 #include "kernels.cuh"
+#include "helm_factor.cuh"
 
 namespace ptc {
 
@@ -154,13 +155,16 @@ struct PoisDiag {
 
 // ---------------------------------------------------------------------------
 // Helmholtz: comp 0 ux (clcU1Hat), 1 uy (clcU2Hat), 2 uz (clcU3Hat),
-// 3 scalar (clcScalar); u(jc) += du(jc); uy and the scalar also get the
-// ghost values that SetBC_and_UpdateHaloForPrSrc / _scalar give them
+// 3 scalar (clcScalar); u(jc) += du(jc).  The factors of the three matrix
+// types come from helm_factor_* (computed once per substep); per column the
+// solve is the same elimination as part_eliminate / part_reduced applied
+// with those multipliers.  uy and the scalar also get the ghost values that
+// SetBC_and_UpdateHaloForPrSrc / _scalar give them.
 // ---------------------------------------------------------------------------
 template <int MR>
-__global__ void __launch_bounds__(512) k_helm(DConst cst, DMetric m, const DCoef* __restrict__ coef, int comp0,
-                                              Fields fl, const double* __restrict__ duy_ym,
-                                              const double* __restrict__ uy_ym) {
+__global__ void __launch_bounds__(512) k_helm(DConst cst, const DCoef* __restrict__ coef, int comp0, Fields fl,
+                                              const double* __restrict__ duy_ym, const double* __restrict__ uy_ym,
+                                              const double* __restrict__ facs) {
     extern __shared__ double sm[];
     const int lane = threadIdx.x, w = threadIdx.y, P = blockDim.y;
     const int nx = cst.nx, ny = cst.ny;
@@ -168,47 +172,69 @@ __global__ void __launch_bounds__(512) k_helm(DConst cst, DMetric m, const DCoef
     const int k = blockIdx.y;
     const int comp = comp0 + blockIdx.z;
     const bool act = i < nx;
-    const int s = w * MR + 1;  // first Fortran row of this partition
-
-    const double *ap, *ac, *am, *rhs;
+    const int s = w * MR + 1;
+    const HelmFacLayout L = helm_fac_layout(MR, P);
+    const int t = comp == 1 ? 1 : (comp == 3 ? 2 : 0);
+    const double* fac = facs + ((size_t)(coef->ns - 1) * 3 + t) * L.stride;
     double* u;
-    double beta, add = 0.0;
-    if (comp == 0)      { ap = m.ap2cCN; ac = m.ac2cCN; am = m.am2cCN; u = fl.ux; rhs = fl.rx; beta = coef->pmBeta; add = coef->rhsx_add; }
-    else if (comp == 1) { ap = m.ap2p; ac = m.ac2p; am = m.am2p; u = fl.uy; rhs = fl.ry; beta = coef->pmBeta; }
-    else if (comp == 2) { ap = m.ap2cCN; ac = m.ac2cCN; am = m.am2cCN; u = fl.uz; rhs = fl.rz; beta = coef->pmBeta; }
-    else                { ap = m.ap2cScCN; ac = m.ac2cScCN; am = m.am2cScCN; u = fl.sc; rhs = fl.rc; beta = coef->pmBetaSc; }
+    const double* rhs;
+    double add = 0.0;
+    if (comp == 0)      { u = fl.ux; rhs = fl.rx; add = coef->rhsx_add; }
+    else if (comp == 1) { u = fl.uy; rhs = fl.ry; }
+    else if (comp == 2) { u = fl.uz; rhs = fl.rz; }
+    else                { u = fl.sc; rhs = fl.rc; }
 
     const size_t zc = (size_t)k * cst.nyt * nx;
-    double a[MR], c[MR], f[MR][1];
+    double f[MR], uo[MR];
 #pragma unroll
     for (int r = 0; r < MR; r++) {
-        a[r] = 0.0; c[r] = 0.0; f[r][0] = 0.0;
         const int jc = s + r;
-        if (jc <= ny) {
-            if (comp == 1 && jc == 1) {
-                f[r][0] = act ? duy_ym[(size_t)k * nx + i] : 0.0;
-            } else {
-                // aj(1) and cj(nyc) are never read by InverseTridiagonal
-                a[r] = (jc == 1) ? 0.0 : -(beta * __ldg(&am[jc]));
-                c[r] = (jc == ny) ? 0.0 : -(beta * __ldg(&ap[jc]));
-                f[r][0] = act ? rhs[zc + (size_t)jc * nx + i] + add : 0.0;
-            }
+        f[r] = 0.0;
+        uo[r] = 0.0;
+        if (act && jc <= ny) {
+            const size_t q = zc + (size_t)jc * nx + i;
+            f[r] = (comp == 1 && jc == 1) ? duy_ym[(size_t)k * nx + i] : rhs[q] + add;
+            uo[r] = u[q];
         }
     }
-    part_eliminate<MR, 1>(a, c, f, HelmDiag{ac, beta, s, ny, comp == 1});
-    double xf[1], xl[1];
-    part_reduced<MR, 1>(P, w, lane, a, c, f, sm, xf, xl);
+    const int g0 = w * MR;
+    f[0] = f[0] * __ldg(&fac[L.F0 + g0]);
+    f[1] = f[1] * __ldg(&fac[L.F0 + g0 + 1]);
+#pragma unroll
+    for (int r = 2; r < MR; r++) f[r] = __ldg(&fac[L.F0 + g0 + r]) * (f[r] - __ldg(&fac[L.A0 + g0 + r]) * f[r - 1]);
+#pragma unroll
+    for (int r = MR - 3; r >= 1; r--) f[r] = f[r] - __ldg(&fac[L.CB + g0 + r]) * f[r + 1];
+    f[0] = __ldg(&fac[L.R0 + w]) * (f[0] - __ldg(&fac[L.C0 + w]) * f[1]);
+
+    // reduced system of the column (unknowns x_first/x_last of every
+    // partition): x = Rinv * F with the precomputed dense inverse, each warp
+    // producing its own two unknowns for the 32 columns
+    double* RF = sm;  // [2P][32]
+    RF[(2 * w) * 32 + lane] = f[0];
+    RF[(2 * w + 1) * 32 + lane] = f[MR - 1];
+    __syncthreads();
+    const int n2 = 2 * P;
+    double xf = 0.0, xl = 0.0;
+    {
+        const double* r0 = fac + L.RI + (size_t)(2 * w) * n2;
+        const double* r1 = r0 + n2;
+        for (int q = 0; q < n2; q++) {
+            const double F = RF[q * 32 + lane];
+            xf += __ldg(&r0[q]) * F;
+            xl += __ldg(&r1[q]) * F;
+        }
+    }
     if (!act) return;
 #pragma unroll
     for (int r = 0; r < MR; r++) {
         const int jc = s + r;
         if (jc <= ny) {
             double x;
-            if (r == 0) x = xf[0];
-            else if (r == MR - 1) x = xl[0];
-            else x = f[r][0] - a[r] * xf[0] - c[r] * xl[0];
+            if (r == 0) x = xf;
+            else if (r == MR - 1) x = xl;
+            else x = f[r] - __ldg(&fac[L.AF + g0 + r]) * xf - __ldg(&fac[L.CF + g0 + r]) * xl;
             const size_t q = zc + (size_t)jc * nx + i;
-            double un = u[q] + x;
+            double un = uo[r] + x;
             if (comp == 1 && jc == 1) un = uy_ym[(size_t)k * nx + i];
             u[q] = un;
             if (comp == 1 && jc == ny) u[q + nx] = (cst.flow_type == 1) ? cst.uybc_yp : 0.0;
@@ -270,12 +296,14 @@ __global__ void __launch_bounds__(512) k_ysolve(DConst cst, DMetric m, double* _
 // ---------------------------------------------------------------------------
 // launchers: partition length MR in {8, 12, 16}, P = ceil(ny/MR) <= 16 warps
 // ---------------------------------------------------------------------------
-static int part_len(int ny) { return ny <= 64 ? 8 : (ny <= 192 ? 12 : 16); }
-
-int tridiag_partitions(int ny) {
-    const int mr = part_len(ny);
+__host__ __device__ inline int part_len_dev(int ny) { return ny <= 64 ? 8 : (ny <= 192 ? 12 : 16); }
+__host__ __device__ inline int tridiag_partitions_dev(int ny) {
+    const int mr = part_len_dev(ny);
     return (ny + mr - 1) / mr;
 }
+static int part_len(int ny) { return part_len_dev(ny); }
+
+int tridiag_partitions(int ny) { return tridiag_partitions_dev(ny); }
 
 bool tridiag_supported(int ny) { return ny >= 3 && ny <= 256; }
 
@@ -290,24 +318,57 @@ void tridiag_init() {
     cudaFuncSetAttribute(k_ysolve<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
 }
 
-static void helm_dispatch(cudaStream_t st, const DConst& c, const DMetric& m, const DCoef* coef, int comp0, int ncomp,
-                          const Fields& f, const double* duy_ym, const double* uy_ym) {
+int tridiag_part_len(int ny) { return part_len(ny); }
+
+size_t helm_fac_doubles(int ny) {
+    const HelmFacLayout L = helm_fac_layout(part_len(ny), tridiag_partitions(ny));
+    return (size_t)9 * L.stride;
+}
+
+// factors of the Helmholtz matrices for substeps ns0..ns0+nsub-1 of the
+// current dt (coef->dt): matrix (ns, t) -> facs + ((ns-1)*3 + t)*stride
+__global__ void k_helm_factors(DConst cst, DMetric m, const DCoef* __restrict__ coef, int ns0, int nsub, double a1,
+                               double a2, double a3, double* __restrict__ facs) {
+    const double dt = coef->dt;
+    const double alps[3] = {a1, a2, a3};
+    double betas[9];
+    int types[9];
+    int nmat = 0;
+    for (int n = ns0; n < ns0 + nsub; n++) {
+        const double alp = alps[n - 1];
+        for (int t = 0; t < 3; t++) {
+            betas[nmat] = (t == 2) ? 0.5 * alp * cst.sdiff * dt : 0.5 * alp * cst.xnu * dt;
+            types[nmat] = t;
+            nmat++;
+        }
+    }
+    const HelmFacLayout L = helm_fac_layout(part_len_dev(cst.ny), tridiag_partitions_dev(cst.ny));
+    helm_factor_block(m, cst.ny, L, nmat, betas, types, facs + (size_t)(ns0 - 1) * 3 * L.stride);
+}
+
+void launch_helm_factors(cudaStream_t st, const DConst& c, const DMetric& m, const DCoef* coef, int ns0, int nsub,
+                         const double* alp, double* fac) {
+    k_helm_factors<<<1, 128, 0, st>>>(c, m, coef, ns0, nsub, alp[0], alp[1], alp[2], fac);
+}
+
+static void helm_dispatch(cudaStream_t st, const DConst& c, const DCoef* coef, int comp0, int ncomp, const Fields& f,
+                          const double* duy_ym, const double* uy_ym, const double* fac) {
     const int mr = part_len(c.ny), P = tridiag_partitions(c.ny);
     dim3 blk(32, P);
     dim3 grd((c.nx + 31) / 32, c.nz, ncomp);
-    const size_t sm = red_smem(P, 1);
-    if (mr == 8) k_helm<8><<<grd, blk, sm, st>>>(c, m, coef, comp0, f, duy_ym, uy_ym);
-    else if (mr == 12) k_helm<12><<<grd, blk, sm, st>>>(c, m, coef, comp0, f, duy_ym, uy_ym);
-    else k_helm<16><<<grd, blk, sm, st>>>(c, m, coef, comp0, f, duy_ym, uy_ym);
+    const size_t sm = (size_t)2 * P * 32 * sizeof(double);
+    if (mr == 8) k_helm<8><<<grd, blk, sm, st>>>(c, coef, comp0, f, duy_ym, uy_ym, fac);
+    else if (mr == 12) k_helm<12><<<grd, blk, sm, st>>>(c, coef, comp0, f, duy_ym, uy_ym, fac);
+    else k_helm<16><<<grd, blk, sm, st>>>(c, coef, comp0, f, duy_ym, uy_ym, fac);
 }
 
-void launch_helm(cudaStream_t st, const DConst& c, const DMetric& m, const DCoef* coef, const Fields& f,
-                 const double* duy_ym, const double* uy_ym) {
-    helm_dispatch(st, c, m, coef, 0, 3, f, duy_ym, uy_ym);
+void launch_helm(cudaStream_t st, const DConst& c, const DCoef* coef, const Fields& f, const double* duy_ym,
+                 const double* uy_ym, const double* fac) {
+    helm_dispatch(st, c, coef, 0, 3, f, duy_ym, uy_ym, fac);
 }
 
-void launch_helm_scalar(cudaStream_t st, const DConst& c, const DMetric& m, const DCoef* coef, const Fields& f) {
-    helm_dispatch(st, c, m, coef, 3, 1, f, nullptr, nullptr);
+void launch_helm_scalar(cudaStream_t st, const DConst& c, const DCoef* coef, const Fields& f, const double* fac) {
+    helm_dispatch(st, c, coef, 3, 1, f, nullptr, nullptr, fac);
 }
 
 void launch_ysolve(cudaStream_t st, const DConst& c, const DMetric& m, double2* spec) {

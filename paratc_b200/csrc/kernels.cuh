@@ -13,9 +13,6 @@ struct Fields {
 
 // k_stencil.cu
 size_t cell_grid_blocks(const DConst& c);
-void launch_coef(cudaStream_t st, DCoef* coef, int ns, double gam, double the, double alp, double xnu, double sdiff);
-void launch_rhs(cudaStream_t st, const DConst& c, const DMetric& m, const DCoef* coef, const Fields& f, double* part);
-void launch_flowrate(cudaStream_t st, const DConst& c, DCoef* coef, const double* part, int nparts);
 void launch_prsrc(cudaStream_t st, const DConst& c, const DMetric& m, const DCoef* coef, int unit_scale,
                   const Fields& f, double* src, double* part, double* out_max);
 void launch_project(cudaStream_t st, const DConst& c, const DMetric& m, const DCoef* coef, int mode, const double* phi,
@@ -26,14 +23,34 @@ void launch_cfl(cudaStream_t st, const DConst& c, const DMetric& m, const Fields
 void launch_check(cudaStream_t st, const DConst& c, const DMetric& m, const Fields& f, const DCoef* coef, DDiag* diag,
                   double* part);
 
+// k_rhs.cu
+size_t rhs_grid_blocks(const DConst& c);
+void rhs_init();
+void launch_rhs_tile(cudaStream_t st, const DConst& c, const DMetric& m, DCoef* coef, const Fields& f, double* uy_ym,
+                     double* duy_ym, int ns, double gam, double the, double alp, double* part, unsigned int* counter);
+
 // k_tridiag.cu
 int tridiag_partitions(int ny);
 bool tridiag_supported(int ny);
 void tridiag_init();
-void launch_helm(cudaStream_t st, const DConst& c, const DMetric& m, const DCoef* coef, const Fields& f,
-                 const double* duy_ym, const double* uy_ym);
-void launch_helm_scalar(cudaStream_t st, const DConst& c, const DMetric& m, const DCoef* coef, const Fields& f);
+int tridiag_part_len(int ny);
+size_t helm_fac_doubles(int ny);
+void launch_helm_factors(cudaStream_t st, const DConst& c, const DMetric& m, const DCoef* coef, int ns0, int nsub,
+                         const double* alp, double* fac);
+void launch_helm(cudaStream_t st, const DConst& c, const DCoef* coef, const Fields& f, const double* duy_ym,
+                 const double* uy_ym, const double* fac);
+void launch_helm_scalar(cudaStream_t st, const DConst& c, const DCoef* coef, const Fields& f, const double* fac);
 void launch_ysolve(cudaStream_t st, const DConst& c, const DMetric& m, double2* spec);
+
+// k_plane.cu
+bool plane_supported(int nx, int nz, const FftPlan& plx, const FftPlan& plz);
+void plane_init();
+void launch_plane_fwd(cudaStream_t st, int mode, const DConst& c, const DMetric& m, DCoef* coef, const Fields& f,
+                      const double* src, double2* spec, const FftPlan& plx, const FftPlan& plz, const double2* twx,
+                      const double2* post, const double2* twz, double* part, unsigned int* counter, double* out_max);
+void launch_plane_inv(cudaStream_t st, int nx, int ny, int nz, const double2* spec, double* phi, const FftPlan& plx,
+                      const FftPlan& plz, const double2* twx, const double2* post, const double2* twz, double scale,
+                      int padded);
 
 // k_fft.cu
 void fft_init();

@@ -71,7 +71,9 @@ bool plan_of(int n, FftPlan& pl) {
     const int rads[4] = {4, 2, 3, 5};
     for (int r : rads)
         while (m % r == 0 && pl.nr < PT_MAX_RADIX_PASSES) { pl.rad[pl.nr++] = r; m /= r; }
-    return m == 1;
+    pl.code = 0;
+    for (int s = 0; s < pl.nr && s < 16; s++) pl.code |= (unsigned long long)pl.rad[s] << (4 * s);
+    return m == 1 && pl.nr <= 16;
 }
 
 void fill_twiddles(double2* w, int n, int count) {
