@@ -91,7 +91,7 @@ def algorithmic_bytes(params):
         "rhs": (7 + 6 + 4 * sc) * w * N,          # u,v,w,p,H* in; Rhs*,H* out
         "helmholtz": 9 * w * N,                   # Rhs*, u* in; u* out
         "helmholtz_scalar": 3 * w * N,
-        "prsrc": 4 * w * N,                       # u,v,w in; src out
+        "prsrc": w * (3 * N + S),                 # u,v,w in; x spectrum out (source fused into the x transform)
         "fft_x_fwd": w * (N + S),
         "fft_z_fwd": 2 * w * S,
         "ysolve": 2 * w * S,

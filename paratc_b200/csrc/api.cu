@@ -48,7 +48,8 @@ struct paratc_ctx {
     double *d_src = nullptr, *d_phi = nullptr, *d_part = nullptr, *d_uy_ym = nullptr, *d_duy_ym = nullptr;
     double *d_metric = nullptr, *d_scal = nullptr;
     double2 *d_spec = nullptr, *d_twx = nullptr, *d_postx = nullptr, *d_twz = nullptr;
-    bool plane = false;  // whole y-planes fit one CTA: fused 2-D transforms
+    bool pfft = false;   // compile-time-length transforms exist for nx/2 and nz
+    double2* d_pfac = nullptr;  // pivots of the spectral y systems, computed once
     DCoef* d_coef = nullptr;
     DDiag* d_diag = nullptr;
     DDiag* d_diag2 = nullptr;
@@ -148,32 +149,50 @@ std::vector<double2> twiddles(int n, int count) {
     return w;
 }
 
-// the y-solve and the inverse transform, after the forward spectrum is in d_spec
+// the z transforms, the y-solve and the x inverse, after the forward x
+// transform has filled d_spec
 void enqueue_poisson_tail(paratc_ctx* ctx, double* out, int padded) {
     cudaStream_t st = ctx->st;
-    { PROF(PK_YSOLVE); launch_ysolve(st, ctx->kc, ctx->dm, ctx->d_spec); }
-    { PROF(PK_FFTX_B); launch_plane_inv(st, ctx->nx, ctx->ny, ctx->nz, ctx->d_spec, out, ctx->plx, ctx->plz, ctx->d_twx,
-                                        ctx->d_postx, ctx->d_twz, ctx->hm.normfft, padded); }
-    ctx->launches += 2;
+    if (ctx->pfft) {
+        { PROF(PK_FFTZ_F); launch_pfft_z(st, -1, ctx->nx, ctx->ny, ctx->nz, ctx->d_spec, ctx->d_twz); }
+        { PROF(PK_YSOLVE); launch_ysolve_fac(st, ctx->kc, ctx->dm, ctx->d_spec, ctx->d_pfac); }
+        { PROF(PK_FFTZ_B); launch_pfft_z(st, +1, ctx->nx, ctx->ny, ctx->nz, ctx->d_spec, ctx->d_twz); }
+        { PROF(PK_FFTX_B); launch_pfft_xb(st, ctx->nx, ctx->ny, ctx->nz, ctx->d_spec, out, ctx->d_twx, ctx->d_postx,
+                                          ctx->hm.normfft, padded); }
+    } else {
+        const int nrows = ctx->ny * ctx->nz;
+        { PROF(PK_FFTZ_F); launch_fft_z(st, -1, ctx->nx, ctx->ny, ctx->nz, ctx->d_spec, ctx->plz, ctx->d_twz); }
+        { PROF(PK_YSOLVE); launch_ysolve_fac(st, ctx->kc, ctx->dm, ctx->d_spec, ctx->d_pfac); }
+        { PROF(PK_FFTZ_B); launch_fft_z(st, +1, ctx->nx, ctx->ny, ctx->nz, ctx->d_spec, ctx->plz, ctx->d_twz); }
+        { PROF(PK_FFTX_B); launch_fft_x_c2r(st, ctx->nx, ctx->ny, nrows, ctx->d_spec, out, ctx->plx, ctx->d_twx,
+                                             ctx->d_postx, ctx->hm.normfft, padded); }
+    }
+    ctx->launches += 4;
+}
+
+// forward x transform of the source; mode 0: divergence of u* / pmAlpha
+// (clcPrSrc, max|div| to out_max), 1: unscaled divergence, 2: array src
+void enqueue_poisson_head(paratc_ctx* ctx, int mode, const double* src, double* out_max) {
+    cudaStream_t st = ctx->st;
+    if (ctx->pfft) {
+        PROF(mode == 2 ? PK_FFTX_F : PK_PRSRC);
+        launch_pfft_xf(st, mode, ctx->kc, ctx->dm, ctx->d_coef, ctx->f, src, ctx->d_spec, ctx->d_twx, ctx->d_postx,
+                       ctx->d_part, ctx->d_counter + 1, out_max);
+        ctx->launches += 1;
+        return;
+    }
+    if (mode != 2) {
+        { PROF(PK_PRSRC); launch_prsrc(st, ctx->kc, ctx->dm, ctx->d_coef, mode, ctx->f, ctx->d_src, ctx->d_part, out_max); }
+        ctx->launches += 2;
+        src = ctx->d_src;
+    }
+    { PROF(PK_FFTX_F); launch_fft_x_r2c(st, ctx->nx, ctx->ny * ctx->nz, src, ctx->d_spec, ctx->plx, ctx->d_twx, ctx->d_postx); }
+    ctx->launches += 1;
 }
 
 void enqueue_poisson(paratc_ctx* ctx, const double* src, double* out, int padded) {
-    cudaStream_t st = ctx->st;
-    if (ctx->plane) {
-        { PROF(PK_FFTX_F); launch_plane_fwd(st, 2, ctx->kc, ctx->dm, ctx->d_coef, ctx->f, src, ctx->d_spec, ctx->plx, ctx->plz,
-                                            ctx->d_twx, ctx->d_postx, ctx->d_twz, ctx->d_part, ctx->d_counter + 1, ctx->d_scal + 8); }
-        ctx->launches += 1;
-        enqueue_poisson_tail(ctx, out, padded);
-        return;
-    }
-    const int nrows = ctx->ny * ctx->nz;
-    { PROF(PK_FFTX_F); launch_fft_x_r2c(st, ctx->nx, nrows, src, ctx->d_spec, ctx->plx, ctx->d_twx, ctx->d_postx); }
-    { PROF(PK_FFTZ_F); launch_fft_z(st, -1, ctx->nx, ctx->ny, ctx->nz, ctx->d_spec, ctx->plz, ctx->d_twz); }
-    { PROF(PK_YSOLVE); launch_ysolve(st, ctx->kc, ctx->dm, ctx->d_spec); }
-    { PROF(PK_FFTZ_B); launch_fft_z(st, +1, ctx->nx, ctx->ny, ctx->nz, ctx->d_spec, ctx->plz, ctx->d_twz); }
-    { PROF(PK_FFTX_B); launch_fft_x_c2r(st, ctx->nx, ctx->ny, nrows, ctx->d_spec, out, ctx->plx, ctx->d_twx, ctx->d_postx,
-                                         ctx->hm.normfft, padded); }
-    ctx->launches += 5;
+    enqueue_poisson_head(ctx, 2, src, nullptr);
+    enqueue_poisson_tail(ctx, out, padded);
 }
 
 // body of the ns loop of ChannelIterate (src/m_ChannelSystem.f90:102-140),
@@ -192,19 +211,15 @@ void enqueue_substep(paratc_ctx* ctx, int ns, int stop = 5) {
     { PROF(PK_HELM); launch_helm(st, ctx->kc, ctx->d_coef, ctx->f, ctx->d_duy_ym, ctx->d_uy_ym, ctx->d_hfac); }
     ctx->launches += 1;
     if (stop == 2) return;
-    if (ctx->plane && stop != 3) {
-        // clcPrSrc fused into the forward plane transform
-        { PROF(PK_FFTX_F); launch_plane_fwd(st, 0, ctx->kc, ctx->dm, ctx->d_coef, ctx->f, nullptr, ctx->d_spec, ctx->plx,
-                                            ctx->plz, ctx->d_twx, ctx->d_postx, ctx->d_twz, ctx->d_part,
-                                            ctx->d_counter + 1, &ctx->d_coef->divmax_src); }
-        ctx->launches += 1;
-        enqueue_poisson_tail(ctx, ctx->d_phi, 1);
-    } else {
+    if (stop == 3) {
+        // the source alone (for a stage-by-stage comparison)
         { PROF(PK_PRSRC); launch_prsrc(st, ctx->kc, ctx->dm, ctx->d_coef, 0, ctx->f, ctx->d_src, ctx->d_part, &ctx->d_coef->divmax_src); }
         ctx->launches += 2;
-        if (stop == 3) return;
-        enqueue_poisson(ctx, ctx->d_src, ctx->d_phi, 1);
+        return;
     }
+    // clcPrSrc fused into the forward x transform
+    enqueue_poisson_head(ctx, 0, nullptr, &ctx->d_coef->divmax_src);
+    enqueue_poisson_tail(ctx, ctx->d_phi, 1);
     if (stop == 4) return;
     { PROF(PK_PROJECT); launch_project(st, ctx->kc, ctx->dm, ctx->d_coef, 0, ctx->d_phi, ctx->f, ctx->d_uy_ym); }
     ctx->launches += 1;
@@ -381,7 +396,7 @@ int paratc_create(const paratc_params* prm, const double* yp, int device, paratc
         delete ctx;
         return PARATC_ERR_BAD_ARG;
     }
-    ctx->plane = plane_supported(ctx->nx, ctx->nz, ctx->plx, ctx->plz) && std::getenv("PARATC_NO_PLANE_FFT") == nullptr;
+    ctx->pfft = pfft_x_supported(ctx->nx / 2) && pfft_z_supported(ctx->nz) && std::getenv("PARATC_GENERIC_FFT") == nullptr;
     cudaError_t ce = cudaStreamCreateWithFlags(&ctx->st, cudaStreamNonBlocking);
     if (ce != cudaSuccess) { delete ctx; return PARATC_ERR_CUDA; }
     static bool inited = false;
@@ -389,7 +404,8 @@ int paratc_create(const paratc_params* prm, const double* yp, int device, paratc
         fft_init();
         tridiag_init();
         rhs_init();
-        plane_init();
+        pfft_x_init();
+        pfft_z_init();
         inited = true;
     }
     const HostMetrics& h = ctx->hm;
@@ -422,13 +438,15 @@ int paratc_create(const paratc_params* prm, const double* yp, int device, paratc
         for (double** p : fs)
             if ((rc = dalloc(ctx, p, nf)) != PARATC_OK) { paratc_destroy(ctx); return rc; }
     }
-    ctx->npart = std::max(cell_grid_blocks(kc) * 7, rhs_grid_blocks(kc)) + 64;
+    ctx->npart = std::max(std::max(cell_grid_blocks(kc) * 7, rhs_grid_blocks(kc)),
+                          (size_t)pfft_x_blocks(ctx->nx, ctx->ny, ctx->nz)) + 64;
     if ((rc = dalloc(ctx, &ctx->d_src, ctx->ni)) || (rc = dalloc(ctx, &ctx->d_spec, (size_t)ctx->M1 * ctx->ny * ctx->nz)) ||
         (rc = dalloc(ctx, &ctx->d_part, ctx->npart)) || (rc = dalloc(ctx, &ctx->d_uy_ym, (size_t)ctx->nx * ctx->nz)) ||
         (rc = dalloc(ctx, &ctx->d_duy_ym, (size_t)ctx->nx * ctx->nz)) || (rc = dalloc(ctx, &ctx->d_coef, 1)) ||
         (rc = dalloc(ctx, &ctx->d_diag, 1)) || (rc = dalloc(ctx, &ctx->d_diag2, 1)) || (rc = dalloc(ctx, &ctx->d_scal, 16)) ||
         (rc = dalloc(ctx, &ctx->d_counter, 16)) ||
-        (rc = dalloc(ctx, &ctx->d_hfac, helm_fac_doubles(ctx->ny)))) {
+        (rc = dalloc(ctx, &ctx->d_hfac, helm_fac_doubles(ctx->ny))) ||
+        (rc = dalloc(ctx, &ctx->d_pfac, (size_t)ctx->M1 * ctx->nz * ctx->ny))) {
         paratc_destroy(ctx);
         return rc;
     }
@@ -454,6 +472,9 @@ int paratc_create(const paratc_params* prm, const double* yp, int device, paratc
         for (size_t a = 0; a < sizeof(dst) / sizeof(dst[0]); a++) *dst[a] = b + a * ny1;
         ctx->dm.wnx = b + ys.size() * ny1;
         ctx->dm.wnz = ctx->dm.wnx + ctx->nx;
+        // pivots of the spectral y systems (constant for the life of the context)
+        launch_pois_factors(ctx->st, kc, ctx->dm, ctx->d_pfac);
+        CK(cudaGetLastError());
         CK(cudaStreamSynchronize(ctx->st));
     }
     // twiddles
@@ -663,18 +684,11 @@ int paratc_project(paratc_ctx* ctx, double* divmax_out) {
     if (!ctx) return PARATC_ERR_BAD_ARG;
     CK(cudaSetDevice(ctx->dev));
     launch_bc_all(ctx->st, ctx->kc, ctx->f, ctx->d_uy_ym);
-    if (ctx->plane) {
-        launch_plane_fwd(ctx->st, 1, ctx->kc, ctx->dm, ctx->d_coef, ctx->f, nullptr, ctx->d_spec, ctx->plx, ctx->plz,
-                         ctx->d_twx, ctx->d_postx, ctx->d_twz, ctx->d_part, ctx->d_counter + 1, ctx->d_scal);
-        ctx->launches += 1;
-        enqueue_poisson_tail(ctx, ctx->d_phi, 1);
-    } else {
-        launch_prsrc(ctx->st, ctx->kc, ctx->dm, ctx->d_coef, 1, ctx->f, ctx->d_src, ctx->d_part, ctx->d_scal);
-        enqueue_poisson(ctx, ctx->d_src, ctx->d_phi, 1);
-    }
+    enqueue_poisson_head(ctx, 1, nullptr, ctx->d_scal);
+    enqueue_poisson_tail(ctx, ctx->d_phi, 1);
     launch_project(ctx->st, ctx->kc, ctx->dm, ctx->d_coef, 1, ctx->d_phi, ctx->f, ctx->d_uy_ym);
     launch_prsrc(ctx->st, ctx->kc, ctx->dm, ctx->d_coef, 1, ctx->f, nullptr, ctx->d_part, ctx->d_scal + 1);
-    ctx->launches += 6;
+    ctx->launches += 4;
     CK(cudaMemcpyAsync(ctx->h_scal, ctx->d_scal, 2 * sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
     int rc = sync(ctx);
     if (rc) return rc;

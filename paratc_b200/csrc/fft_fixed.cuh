@@ -1,0 +1,242 @@
+// fft_fixed.cuh -- batched complex FFTs whose length is a compile-time
+// constant, for the transforms of the pressure Poisson solve.
+//
+// A CTA transforms B sequences of length N held in shared memory as
+// buf[e*PITCH + b] (element e of sequence b; b fastest, so that a warp's 32
+// lanes touch consecutive 16-byte words).  The transform is a sequence of
+// Stockham autosort passes with radices 16, 8, 4, 2, 3 and 5: every index,
+// stride and loop bound is a constant, so a pass is loads, constant-twiddle
+// butterflies and stores, with no integer division at run time.  Pass s of
+// radix R after passes whose radices multiply to NS reads element j + r*N/R
+// (r < R) of butterfly j, multiplies by exp(-+2 pi i (j mod NS) r / (NS R))
+// and writes element (j - j mod NS) R + j mod NS + r NS: the classic Stockham
+// formulation, done in place (all threads load their inputs to registers, the
+// block synchronises, then all store).  Inter-pass twiddles come from a table
+// tw[m] = exp(-2 pi i m / N) that the caller stages in shared memory.
+#pragma once
+#include "common.cuh"
+
+namespace ptc {
+namespace ff {
+
+// radix schedule of N = 2^a 3^b 5^c: the power of two in ceil(a/4) passes of
+// radix <= 16 as even as possible, then radix-3 and radix-5 passes
+struct Sched {
+    int np;
+    int r[12];
+};
+
+__host__ __device__ constexpr Sched make_sched(int n) {
+    Sched s{0, {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0}};
+    int a = 0;
+    while (n % 2 == 0) { n /= 2; a++; }
+    const int p2 = (a + 3) / 4;
+    for (int q = 0; q < p2; q++) s.r[s.np++] = 1 << ((a + q) / p2);
+    while (n % 3 == 0 && s.np < 12) { n /= 3; s.r[s.np++] = 3; }
+    while (n % 5 == 0 && s.np < 12) { n /= 5; s.r[s.np++] = 5; }
+    if (n != 1) s.np = -1;
+    return s;
+}
+
+__host__ __device__ constexpr int sched_rmax(int n) {
+    const Sched s = make_sched(n);
+    int m = 1;
+    for (int q = 0; q < s.np; q++) m = s.r[q] > m ? s.r[q] : m;
+    return m;
+}
+
+// product of the radices of passes 0..S-1
+__host__ __device__ constexpr int sched_ns(int n, int S) {
+    const Sched s = make_sched(n);
+    int p = 1;
+    for (int q = 0; q < S; q++) p *= s.r[q];
+    return p;
+}
+
+// cos and sin of 2 pi k / 16
+__host__ __device__ constexpr double c16(int k) {
+    switch (k & 15) {
+        case 0: return 1.0;
+        case 1: return 0.92387953251128675613;
+        case 2: return 0.70710678118654752440;
+        case 3: return 0.38268343236508977173;
+        case 4: return 0.0;
+        case 5: return -0.38268343236508977173;
+        case 6: return -0.70710678118654752440;
+        case 7: return -0.92387953251128675613;
+        case 8: return -1.0;
+        case 9: return -0.92387953251128675613;
+        case 10: return -0.70710678118654752440;
+        case 11: return -0.38268343236508977173;
+        case 12: return 0.0;
+        case 13: return 0.38268343236508977173;
+        case 14: return 0.70710678118654752440;
+        default: return 0.92387953251128675613;
+    }
+}
+__host__ __device__ constexpr double s16(int k) { return c16(k - 4); }
+
+// v * exp(DIR 2 pi i k / M) for M in {2, 4, 8, 16}, with the trivial angles
+// done exactly
+template <int M, int K, int DIR>
+__device__ __forceinline__ double2 rot(double2 v) {
+    constexpr int k16 = (K * (16 / M)) & 15;
+    if constexpr (k16 == 0) return v;
+    else if constexpr (k16 == 8) return make_double2(-v.x, -v.y);
+    else if constexpr (k16 == 4) return DIR < 0 ? make_double2(v.y, -v.x) : make_double2(-v.y, v.x);
+    else if constexpr (k16 == 12) return DIR < 0 ? make_double2(-v.y, v.x) : make_double2(v.y, -v.x);
+    else {
+        constexpr double c = c16(k16), s = DIR * s16(k16);
+        return make_double2(v.x * c - v.y * s, v.x * s + v.y * c);
+    }
+}
+
+template <int DIR>
+__device__ __forceinline__ void dft2(double2* v) {
+    const double2 t = v[0];
+    v[0] = cadd(t, v[1]);
+    v[1] = csub(t, v[1]);
+}
+
+template <int DIR>
+__device__ __forceinline__ void dft3(double2* v) {
+    const double c = -0.5, s = DIR * 0.86602540378443864676;  // cos, sin of 2 pi / 3
+    const double2 t1 = cadd(v[1], v[2]), t2 = csub(v[1], v[2]);
+    const double2 mm = make_double2(v[0].x + c * t1.x, v[0].y + c * t1.y);
+    const double2 it = make_double2(-s * t2.y, s * t2.x);
+    v[0] = cadd(v[0], t1);
+    v[1] = cadd(mm, it);
+    v[2] = csub(mm, it);
+}
+
+template <int DIR>
+__device__ __forceinline__ void dft5(double2* v) {
+    const double c1 = 0.30901699437494742410, c2 = -0.80901699437494742410;  // cos 2pi/5, cos 4pi/5
+    const double s1 = DIR * 0.95105651629515357212, s2 = DIR * 0.58778525229247312917;
+    const double2 a1 = cadd(v[1], v[4]), b1 = csub(v[1], v[4]);
+    const double2 a2 = cadd(v[2], v[3]), b2 = csub(v[2], v[3]);
+    const double2 m1 = make_double2(v[0].x + c1 * a1.x + c2 * a2.x, v[0].y + c1 * a1.y + c2 * a2.y);
+    const double2 m2 = make_double2(v[0].x + c2 * a1.x + c1 * a2.x, v[0].y + c2 * a1.y + c1 * a2.y);
+    const double2 n1 = make_double2(s1 * b1.x + s2 * b2.x, s1 * b1.y + s2 * b2.y);
+    const double2 n2 = make_double2(s2 * b1.x - s1 * b2.x, s2 * b1.y - s1 * b2.y);
+    const double2 in1 = make_double2(-n1.y, n1.x), in2 = make_double2(-n2.y, n2.x);
+    v[0] = make_double2(v[0].x + a1.x + a2.x, v[0].y + a1.y + a2.y);
+    v[1] = cadd(m1, in1);
+    v[4] = csub(m1, in1);
+    v[2] = cadd(m2, in2);
+    v[3] = csub(m2, in2);
+}
+
+// radix-2 combination of the half-length DFTs of the even (E) and odd (O)
+// samples: X[k] = E[k] + W^k O[k], X[k + H] = E[k] - W^k O[k], W = exp(DIR 2 pi i / 2H)
+template <int H, int DIR, int K = 0>
+__device__ __forceinline__ void combine(const double2* E, const double2* O, double2* X) {
+    if constexpr (K < H) {
+        const double2 t = rot<2 * H, K, DIR>(O[K]);
+        X[K] = cadd(E[K], t);
+        X[K + H] = csub(E[K], t);
+        combine<H, DIR, K + 1>(E, O, X);
+    }
+}
+
+template <int R, int DIR>
+__device__ __forceinline__ void dft(double2* v) {
+    if constexpr (R == 2) dft2<DIR>(v);
+    else if constexpr (R == 3) dft3<DIR>(v);
+    else if constexpr (R == 5) dft5<DIR>(v);
+    else {
+        constexpr int H = R / 2;
+        double2 e[H], o[H];
+#pragma unroll
+        for (int q = 0; q < H; q++) { e[q] = v[2 * q]; o[q] = v[2 * q + 1]; }
+        dft<H, DIR>(e);
+        dft<H, DIR>(o);
+        combine<H, DIR>(e, o, v);
+    }
+}
+
+// One Stockham pass of radix R (passes before it multiply to NS) over B
+// sequences of length N, P threads.  LD(e, b) loads element e of sequence b,
+// ST(e, b, v) stores it; SYNC_MID puts a block barrier between all loads and
+// all stores (an in-place pass on shared memory).  tw: exp(-2 pi i m / N).
+template <int N, int B, int P, int R, int NS, int DIR, bool SYNC_MID, class LD, class ST>
+__device__ __forceinline__ void pass(const LD& ld, const ST& st, const double2* tw, int tid) {
+    constexpr int NB = N / R;
+    constexpr int TOT = B * NB;
+    constexpr int PER = (TOT + P - 1) / P;
+    constexpr int TS = N / (NS * R);
+    double2 v[PER][R];
+    int jb[PER];
+#pragma unroll
+    for (int u = 0; u < PER; u++) {
+        const int t = tid + u * P;
+        jb[u] = -1;
+        if (TOT % P == 0 || t < TOT) {
+            const int b = t % B, j = t / B;
+            const int kk = j % NS;
+#pragma unroll
+            for (int r = 0; r < R; r++) v[u][r] = ld(j + r * NB, b);
+            if constexpr (NS > 1) {
+#pragma unroll
+                for (int r = 1; r < R; r++) {
+                    const double2 w = tw[kk * r * TS];
+                    v[u][r] = (DIR < 0) ? cmul(v[u][r], w) : cmulc(v[u][r], w);
+                }
+            }
+            dft<R, DIR>(v[u]);
+            jb[u] = ((j - kk) * R + kk) * B + b;  // output element * B + b
+        }
+    }
+    if constexpr (SYNC_MID) __syncthreads();
+#pragma unroll
+    for (int u = 0; u < PER; u++) {
+        if (TOT % P == 0 || jb[u] >= 0) {
+            const int b = jb[u] % B, e0 = jb[u] / B;
+#pragma unroll
+            for (int r = 0; r < R; r++) st(e0 + r * NS, b, v[u][r]);
+        }
+    }
+}
+
+// shared-memory accessors of the layout buf[e*PITCH + b]
+template <int PITCH>
+struct SmemLd {
+    const double2* buf;
+    __device__ __forceinline__ double2 operator()(int e, int b) const { return buf[e * PITCH + b]; }
+};
+template <int PITCH>
+struct SmemSt {
+    double2* buf;
+    __device__ __forceinline__ void operator()(int e, int b, double2 v) const { buf[e * PITCH + b] = v; }
+};
+
+// passes S..END-1 in place on shared memory, each followed by a barrier
+template <int N, int B, int PITCH, int P, int DIR, int S, int END>
+__device__ __forceinline__ void smem_passes(double2* buf, const double2* tw, int tid) {
+    constexpr Sched SC = make_sched(N);
+    if constexpr (S < END) {
+        constexpr int R = SC.r[S];
+        constexpr int NS = sched_ns(N, S);
+        pass<N, B, P, R, NS, DIR, true>(SmemLd<PITCH>{buf}, SmemSt<PITCH>{buf}, tw, tid);
+        __syncthreads();
+        smem_passes<N, B, PITCH, P, DIR, S + 1, END>(buf, tw, tid);
+    }
+}
+
+// launch shape of a length-N transform: B sequences per CTA, P threads (one
+// butterfly of the largest radix per thread)
+template <int N>
+struct Shape {
+    static constexpr int RMAX = sched_rmax(N);
+    static constexpr int PMAX = N <= 256 ? 128 : 256;
+    static constexpr int bcalc() {
+        int b = 64;
+        while (b > 1 && b * N / RMAX > PMAX) b /= 2;
+        return b;
+    }
+    static constexpr int B = bcalc();
+    static constexpr int P = B * N / RMAX;
+};
+
+}  // namespace ff
+}  // namespace ptc

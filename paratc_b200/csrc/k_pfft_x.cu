@@ -1,0 +1,256 @@
+// k_pfft_x.cu -- x transforms of the pressure Poisson solve, compile-time
+// lengths.
+//
+// clcPPE (src/m_Poisson.f90:352-452) transforms the source along x with
+// FFTW's R2HC and back with HC2R.  Here the real row of nx values is packed
+// into nx/2 complex values z[m] = x[2m] + i x[2m+1], transformed with an
+// nx/2-point complex FFT (fft_fixed.cuh) and split into the nx/2+1 modes of
+// the real transform (forward), or merged and transformed back (inverse).
+// The modified wavenumber is even in the mode number, so these modes carry
+// the same eigenvalues as the reference's halfcomplex ones.
+//
+// Forward kernel: the source of a row is the divergence of u* computed on
+// the fly (clcPrSrc, src/m_TScheme.f90:48-77: scaled by 1/pmAlpha in mode 0,
+// unscaled in mode 1, with max|div| reduced over the grid by the last CTA)
+// or a given compact source array (mode 2).  Inverse kernel: the merge, the
+// inverse FFT, 1/(nx*nz) and the Neumann ghost rows phi(0) = phi(1),
+// phi(nyp) = phi(nyc) of SetBC_and_UpdateHalo_pr (src/m_BC_and_Halo.f90:
+// 115-120).  A CTA owns B consecutive rows g = k*ny + (jc-1), so its spectral
+// rows spec[g*(nx/2+1) + kx] form one contiguous block.
+#include "common.cuh"
+#include "fft_fixed.cuh"
+#include "kernels.cuh"
+#include "reduce.cuh"
+
+namespace ptc {
+namespace {
+
+__device__ __forceinline__ void cpa16(void* sdst, const void* gsrc) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cpa_wait_all() {
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+}
+
+template <int N>
+struct XK {
+    static constexpr int B = ff::Shape<N>::B;
+    static constexpr int P = ff::Shape<N>::P;
+    static constexpr int PITCH = B + 1;  // odd pitch: row-order accesses hit distinct banks
+    static constexpr size_t smem = ((size_t)(N + 1) * PITCH + N) * sizeof(double2);
+};
+
+template <int N>
+__global__ void __launch_bounds__(XK<N>::P)
+    k_xf(int mode, DConst c, DMetric m, const DCoef* __restrict__ coef, const double* __restrict__ ux,
+         const double* __restrict__ uy, const double* __restrict__ uz, const double* __restrict__ src,
+         double2* __restrict__ spec, const double2* __restrict__ twN, const double2* __restrict__ post,
+         double* __restrict__ part, unsigned int* __restrict__ counter, double* __restrict__ out_max) {
+    constexpr int B = XK<N>::B, P = XK<N>::P, PITCH = XK<N>::PITCH, M1 = N + 1;
+    constexpr ff::Sched SC = ff::make_sched(N);
+    extern __shared__ double2 smx[];
+    double2* buf = smx;
+    double2* tws = smx + (N + 1) * PITCH;
+    const int tid = threadIdx.x;
+    const int nx = 2 * N, ny = c.ny, nz = c.nz, nrows = ny * nz;
+    const int g0 = blockIdx.x * B;
+    for (int t = tid; t < N; t += P) tws[t] = twN[t];
+    double dm = 0.0;
+    if (mode == 2) {
+        for (int f = tid; f < B * N; f += P) {
+            const int b = f / N, e = f - b * N;
+            const int g = g0 + b;
+            if (g < nrows) cpa16(&buf[e * PITCH + b], src + (size_t)g * nx + 2 * e);
+            else buf[e * PITCH + b] = make_double2(0.0, 0.0);
+        }
+        cpa_wait_all();
+    } else {
+        const double sudtal = (mode == 0) ? 1.0 / coef->pmAlpha : 1.0;
+        const size_t pl = (size_t)c.nyt * nx;
+#pragma unroll 2
+        for (int f = tid; f < B * N; f += P) {
+            const int b = f / N, e = f - b * N;
+            const int g = g0 + b;
+            double2 val = make_double2(0.0, 0.0);
+            if (g < nrows) {
+                const int k = g / ny, jc = g - k * ny + 1;
+                const int km = k == 0 ? nz - 1 : k - 1, kp = k == nz - 1 ? 0 : k + 1, ku = kp == nz - 1 ? 0 : kp + 1;
+                const int i0 = 2 * e, im = i0 == 0 ? nx - 1 : i0 - 1, i2 = i0 + 2 == nx ? 0 : i0 + 2;
+                const size_t r0 = (size_t)jc * nx;
+                const double* ur = ux + (size_t)k * pl + r0;
+                const double* vr = uy + (size_t)k * pl + r0;
+                const double2 u01 = __ldg(reinterpret_cast<const double2*>(ur + i0));
+                const double2 u23 = __ldg(reinterpret_cast<const double2*>(ur + i2));
+                const double um = __ldg(ur + im);
+                const double2 v0 = __ldg(reinterpret_cast<const double2*>(vr + i0));
+                const double2 v1 = __ldg(reinterpret_cast<const double2*>(vr + nx + i0));
+                const double2 w0 = __ldg(reinterpret_cast<const double2*>(uz + (size_t)km * pl + r0 + i0));
+                const double2 w1 = __ldg(reinterpret_cast<const double2*>(uz + (size_t)k * pl + r0 + i0));
+                const double2 w2 = __ldg(reinterpret_cast<const double2*>(uz + (size_t)kp * pl + r0 + i0));
+                const double2 w3 = __ldg(reinterpret_cast<const double2*>(uz + (size_t)ku * pl + r0 + i0));
+                const double rdyp = __ldg(&m.rdyp[jc]);
+                const double dudx0 = c.dxC[0] * um + c.dxC[1] * u01.x + c.dxC[2] * u01.y + c.dxC[3] * u23.x;
+                const double dudx1 = c.dxC[0] * u01.x + c.dxC[1] * u01.y + c.dxC[2] * u23.x + c.dxC[3] * u23.y;
+                const double dvdy0 = (v1.x - v0.x) * rdyp, dvdy1 = (v1.y - v0.y) * rdyp;
+                const double dwdz0 = c.dzC[0] * w0.x + c.dzC[1] * w1.x + c.dzC[2] * w2.x + c.dzC[3] * w3.x;
+                const double dwdz1 = c.dzC[0] * w0.y + c.dzC[1] * w1.y + c.dzC[2] * w2.y + c.dzC[3] * w3.y;
+                const double d0 = dudx0 + dvdy0 + dwdz0, d1 = dudx1 + dvdy1 + dwdz1;
+                dm = fmax(dm, fmax(fabs(d0), fabs(d1)));
+                val = make_double2(sudtal * d0, sudtal * d1);
+            }
+            buf[e * PITCH + b] = val;
+        }
+    }
+    __syncthreads();
+    ff::smem_passes<N, B, PITCH, P, -1, 0, SC.np>(buf, tws, tid);
+    // split the packed transform into the nx/2+1 modes of the real row
+    for (int f = tid; f < B * M1; f += P) {
+        const int b = f / M1, a = f - b * M1;
+        if (g0 + b >= nrows) continue;
+        const double2 za = buf[(a == N ? 0 : a) * PITCH + b];
+        const double2 zb = buf[(a == 0 ? 0 : N - a) * PITCH + b];
+        const double2 E = make_double2(0.5 * (za.x + zb.x), 0.5 * (za.y - zb.y));
+        const double2 O = make_double2(0.5 * (za.y + zb.y), -0.5 * (za.x - zb.x));
+        spec[(size_t)g0 * M1 + f] = cadd(E, cmul(__ldg(&post[a]), O));
+    }
+    if (mode == 2) return;
+    double v[1] = {dm};
+    const unsigned int nblocks = gridDim.x;
+    block_max_store<1>(v, part + blockIdx.x);
+    if (!last_block_arrive(counter, nblocks)) return;
+    double tot[1];
+    reduce_records<1, true>(part, (int)nblocks, tot);
+    if (tid == 0) *out_max = tot[0];
+}
+
+template <int N>
+__global__ void __launch_bounds__(XK<N>::P)
+    k_xb(int ny, int nz, const double2* __restrict__ spec, double* __restrict__ phi, const double2* __restrict__ twN,
+         const double2* __restrict__ post, double scale, int padded) {
+    constexpr int B = XK<N>::B, P = XK<N>::P, PITCH = XK<N>::PITCH, M1 = N + 1;
+    constexpr ff::Sched SC = ff::make_sched(N);
+    extern __shared__ double2 smx[];
+    double2* buf = smx;
+    double2* tws = smx + (N + 1) * PITCH;
+    const int tid = threadIdx.x;
+    const int nx = 2 * N, nrows = ny * nz;
+    const int g0 = blockIdx.x * B;
+    for (int t = tid; t < N; t += P) tws[t] = twN[t];
+    for (int f = tid; f < B * M1; f += P) {
+        const int b = f / M1, a = f - b * M1;
+        if (g0 + b < nrows) cpa16(&buf[a * PITCH + b], spec + (size_t)g0 * M1 + f);
+        else buf[a * PITCH + b] = make_double2(0.0, 0.0);
+    }
+    cpa_wait_all();
+    __syncthreads();
+    // merge modes a and N-a of every row into z[a], z[N-a] (the DC and
+    // Nyquist coefficients are real)
+    for (int f = tid; f < B * (N / 2 + 1); f += P) {
+        const int a = f / B, b = f - a * B;
+        const int bn = N - a;
+        double2 xa = buf[a * PITCH + b], xb = buf[bn * PITCH + b];
+        if (a == 0) { xa.y = 0.0; xb.y = 0.0; }
+        const double2 e2a = make_double2(xa.x + xb.x, xa.y - xb.y);
+        const double2 da = make_double2(xa.x - xb.x, xa.y + xb.y);
+        const double2 o2a = cmulc(da, __ldg(&post[a]));
+        const double2 za = make_double2(e2a.x - o2a.y, e2a.y + o2a.x);
+        if (a == 0) {
+            buf[b] = za;
+        } else {
+            const double2 e2b = make_double2(xb.x + xa.x, xb.y - xa.y);
+            const double2 db = make_double2(xb.x - xa.x, xb.y + xa.y);
+            const double2 o2b = cmulc(db, __ldg(&post[bn]));
+            const double2 zb = make_double2(e2b.x - o2b.y, e2b.y + o2b.x);
+            buf[a * PITCH + b] = za;
+            if (bn != a) buf[bn * PITCH + b] = zb;
+        }
+    }
+    __syncthreads();
+    ff::smem_passes<N, B, PITCH, P, 1, 0, SC.np>(buf, tws, tid);
+    const int nyt = ny + 2;
+    for (int f = tid; f < B * N; f += P) {
+        const int b = f / N, e = f - b * N;
+        const int g = g0 + b;
+        if (g >= nrows) continue;
+        const double2 z = buf[e * PITCH + b];
+        const double2 v = make_double2(z.x * scale, z.y * scale);
+        if (!padded) {
+            reinterpret_cast<double2*>(phi + (size_t)g * nx)[e] = v;
+            continue;
+        }
+        const int k = g / ny, jc = g - k * ny + 1;
+        double* rowp = phi + ((size_t)k * nyt + jc) * nx;
+        reinterpret_cast<double2*>(rowp)[e] = v;
+        if (jc == 1) reinterpret_cast<double2*>(rowp - nx)[e] = v;
+        if (jc == ny) reinterpret_cast<double2*>(rowp + nx)[e] = v;
+    }
+}
+
+#define PFFT_X_SIZES(X) X(8) X(12) X(16) X(24) X(32) X(40) X(48) X(64) X(96) X(128) X(192) X(256) X(384) X(512) \
+    X(768) X(1024) X(1152) X(1536)
+
+}  // namespace
+
+bool pfft_x_supported(int n) {
+    switch (n) {
+#define X_CASE(n) case n:
+        PFFT_X_SIZES(X_CASE)
+#undef X_CASE
+        return true;
+        default: return false;
+    }
+}
+
+int pfft_x_blocks(int nx, int ny, int nz) {
+    int b = 1;
+    switch (nx / 2) {
+#define X_CASE(n) case n: b = XK<n>::B; break;
+        PFFT_X_SIZES(X_CASE)
+#undef X_CASE
+        default: break;
+    }
+    return (ny * nz + b - 1) / b;
+}
+
+void pfft_x_init() {
+#define X_CASE(n)                                                                                              \
+    cudaFuncSetAttribute(k_xf<n>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)XK<n>::smem);              \
+    cudaFuncSetAttribute(k_xb<n>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)XK<n>::smem);
+    PFFT_X_SIZES(X_CASE)
+#undef X_CASE
+}
+
+void launch_pfft_xf(cudaStream_t st, int mode, const DConst& c, const DMetric& m, const DCoef* coef, const Fields& f,
+                    const double* src, double2* spec, const double2* twx, const double2* post, double* part,
+                    unsigned int* counter, double* out_max) {
+    const int nrows = c.ny * c.nz;
+    switch (c.nx / 2) {
+#define X_CASE(n)                                                                                              \
+    case n:                                                                                                    \
+        k_xf<n><<<(nrows + XK<n>::B - 1) / XK<n>::B, XK<n>::P, XK<n>::smem, st>>>(                             \
+            mode, c, m, coef, f.ux, f.uy, f.uz, src, spec, twx, post, part, counter, out_max);                 \
+        break;
+        PFFT_X_SIZES(X_CASE)
+#undef X_CASE
+        default: break;
+    }
+}
+
+void launch_pfft_xb(cudaStream_t st, int nx, int ny, int nz, const double2* spec, double* phi, const double2* twx,
+                    const double2* post, double scale, int padded) {
+    const int nrows = ny * nz;
+    switch (nx / 2) {
+#define X_CASE(n)                                                                                              \
+    case n:                                                                                                    \
+        k_xb<n><<<(nrows + XK<n>::B - 1) / XK<n>::B, XK<n>::P, XK<n>::smem, st>>>(ny, nz, spec, phi, twx,      \
+                                                                                  post, scale, padded);        \
+        break;
+        PFFT_X_SIZES(X_CASE)
+#undef X_CASE
+        default: break;
+    }
+}
+
+}  // namespace ptc

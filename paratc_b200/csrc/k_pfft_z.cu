@@ -1,0 +1,106 @@
+// k_pfft_z.cu -- z transforms of the pressure Poisson solve, compile-time
+// lengths.
+//
+// After the x transform the spectrum is spec[(kz*ny + j)*(nx/2+1) + kx]; for
+// a fixed kz the (j, kx) pairs form one contiguous run of ncol = ny*(nx/2+1)
+// complex values, so the z transform works on "columns" q = j*(nx/2+1) + kx
+// whose element kz sits at spec[kz*ncol + q].  A CTA owns B consecutive
+// columns: every load and store of a pass moves B contiguous 16-byte values.
+// The first pass reads its inputs straight from global memory and the last
+// pass writes its outputs straight back, so a two-pass length (64, 128, 256)
+// touches shared memory once.  Unnormalised, as FFTW's R2HC / HC2R along z in
+// clcPPE (src/m_Poisson.f90:352-452); the 1/(nx*nz) is applied after the x
+// inverse.
+#include "common.cuh"
+#include "fft_fixed.cuh"
+#include "kernels.cuh"
+
+namespace ptc {
+namespace {
+
+template <int N>
+struct ZK {
+    static constexpr int B = ff::Shape<N>::B < 4 ? 4 : ff::Shape<N>::B;
+    static constexpr int P = B * N / ff::Shape<N>::RMAX;
+    static constexpr size_t smem = ((size_t)N * B + N) * sizeof(double2);
+};
+
+struct GLd {
+    const double2* base;
+    int ncol, nvalid;
+    __device__ __forceinline__ double2 operator()(int e, int b) const {
+        return b < nvalid ? base[(size_t)e * ncol + b] : make_double2(0.0, 0.0);
+    }
+};
+struct GSt {
+    double2* base;
+    int ncol, nvalid;
+    __device__ __forceinline__ void operator()(int e, int b, double2 v) const {
+        if (b < nvalid) base[(size_t)e * ncol + b] = v;
+    }
+};
+
+template <int N, int DIR>
+__global__ void __launch_bounds__(ZK<N>::P) k_zt(int ncol, double2* __restrict__ spec, const double2* __restrict__ twN) {
+    constexpr int B = ZK<N>::B, P = ZK<N>::P;
+    constexpr ff::Sched SC = ff::make_sched(N);
+    extern __shared__ double2 smz[];
+    double2* buf = smz;
+    double2* tws = smz + N * B;
+    const int tid = threadIdx.x;
+    const int q0 = blockIdx.x * B;
+    const int nvalid = min(B, ncol - q0);
+    const GLd gl{spec + q0, ncol, nvalid};
+    const GSt gs{spec + q0, ncol, nvalid};
+    if constexpr (SC.np == 1) {
+        ff::pass<N, B, P, SC.r[0], 1, DIR, false>(gl, gs, tws, tid);
+    } else {
+        for (int t = tid; t < N; t += P) tws[t] = twN[t];
+        ff::pass<N, B, P, SC.r[0], 1, DIR, false>(gl, ff::SmemSt<B>{buf}, tws, tid);
+        __syncthreads();
+        ff::smem_passes<N, B, B, P, DIR, 1, SC.np - 1>(buf, tws, tid);
+        constexpr int L = SC.np - 1;
+        ff::pass<N, B, P, SC.r[L], ff::sched_ns(N, L), DIR, false>(ff::SmemLd<B>{buf}, gs, tws, tid);
+    }
+}
+
+#define PFFT_Z_SIZES(X) X(8) X(12) X(16) X(24) X(30) X(32) X(40) X(48) X(64) X(96) X(128) X(192) X(256) X(384) \
+    X(512) X(768) X(1024) X(1152) X(1536)
+
+}  // namespace
+
+bool pfft_z_supported(int n) {
+    switch (n) {
+#define Z_CASE(n) case n:
+        PFFT_Z_SIZES(Z_CASE)
+#undef Z_CASE
+        return true;
+        default: return false;
+    }
+}
+
+void pfft_z_init() {
+#define Z_CASE(n)                                                                                              \
+    cudaFuncSetAttribute(k_zt<n, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ZK<n>::smem);         \
+    cudaFuncSetAttribute(k_zt<n, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ZK<n>::smem);
+    PFFT_Z_SIZES(Z_CASE)
+#undef Z_CASE
+}
+
+void launch_pfft_z(cudaStream_t st, int dir, int nx, int ny, int nz, double2* spec, const double2* twz) {
+    const int ncol = ny * (nx / 2 + 1);
+    switch (nz) {
+#define Z_CASE(n)                                                                                              \
+    case n: {                                                                                                  \
+        const int grid = (ncol + ZK<n>::B - 1) / ZK<n>::B;                                                     \
+        if (dir < 0) k_zt<n, -1><<<grid, ZK<n>::P, ZK<n>::smem, st>>>(ncol, spec, twz);                        \
+        else k_zt<n, 1><<<grid, ZK<n>::P, ZK<n>::smem, st>>>(ncol, spec, twz);                                 \
+        break;                                                                                                 \
+    }
+        PFFT_Z_SIZES(Z_CASE)
+#undef Z_CASE
+        default: break;
+    }
+}
+
+}  // namespace ptc

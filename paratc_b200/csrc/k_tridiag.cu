@@ -294,6 +294,206 @@ __global__ void __launch_bounds__(512) k_ysolve(DConst cst, DMetric m, double* _
 }
 
 // ---------------------------------------------------------------------------
+// Spectral y-solve with the factors computed once.  The Poisson matrices
+// (am2ph, ac2ph + lambda_x(kx) + lambda_z(kz), ap2ph) depend on the mesh and
+// the wavenumbers only, so the pivots of InverseTridiagonal
+// (src/m_Tools.f90:224-251) are computed once per context: for complex
+// column q = kz*(nx/2+1) + kx and Fortran row jc, fac[(jc-1)*NQ + q] =
+// {1/vecm(jc), arr(jc)} with vecm(1) = b(1), arr(jc) = c(jc-1)/vecm(jc-1),
+// vecm(jc) = b(jc) - a(jc)*arr(jc), evaluated in the reference's order
+// without contraction.  A solve is then the two sweeps
+//   f(1) = f(1)/vecm(1),  f(jc) = (f(jc) - a(jc) f(jc-1)) / vecm(jc),
+//   f(jc) = f(jc) - arr(jc+1) f(jc+1),
+// with no division left on the dependent chain (1/vecm is a multiply).
+// The kx = kz = 0 system has row 1 replaced by phi = 0 (b = 1, c = 0,
+// f = 0; src/m_Poisson.f90:399-404).
+// ---------------------------------------------------------------------------
+__global__ void k_pois_factors(int ny, int M1, int nz, DMetric m, double2* __restrict__ fac) {
+    const int NQ = M1 * nz;
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= NQ) return;
+    const int kz = q / M1, kx = q - kz * M1;
+    const double wx = m.wnx[kx], wz = m.wnz[kz];
+    const bool dc = (q == 0);
+    double vecm = dc ? 1.0 : __dadd_rn(__dadd_rn(m.ac2ph[1], wx), wz);
+    fac[q] = make_double2(1.0 / vecm, 0.0);
+    for (int jc = 2; jc <= ny; jc++) {
+        const double cp = (dc && jc == 2) ? 0.0 : m.ap2ph[jc - 1];
+        const double arr = cp / vecm;
+        const double b = __dadd_rn(__dadd_rn(m.ac2ph[jc], wx), wz);
+        vecm = __dsub_rn(b, __dmul_rn(m.am2ph[jc], arr));
+        fac[(size_t)(jc - 1) * NQ + q] = make_double2(1.0 / vecm, arr);
+    }
+}
+
+namespace {
+__device__ __forceinline__ void cpa16t(void* sdst, const void* gsrc) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gsrc) : "memory");
+}
+constexpr int YS_U = 8;  // rows loaded ahead of the dependent chain
+}  // namespace
+
+// Small grids (one wave): a one-warp CTA stages 16 complex columns of the
+// spectrum and their factors in shared memory with cp.async, then lane l
+// sweeps the real (l even) or imaginary (l odd) part of column l/2.
+__global__ void __launch_bounds__(32) k_ys_staged(int ny, int M1, int nz, const double* __restrict__ am2ph,
+                                                  double2* __restrict__ spec, const double2* __restrict__ fac) {
+    extern __shared__ double2 sy[];
+    const int lane = threadIdx.x;
+    const int NQ = M1 * nz;
+    const int q0 = blockIdx.x * 16;
+    const int nv = min(16, NQ - q0);
+    double2* sd = sy;                   // [ny][16] spectrum
+    double2* sf = sy + ny * 16;         // [ny][16] factors
+    double* sa = reinterpret_cast<double*>(sf + ny * 16);  // am2ph[0..ny]
+    for (int idx = lane; idx < ny * 16; idx += 32) {
+        const int j = idx >> 4, cq = idx & 15;
+        if (cq < nv) {
+            const int q = q0 + cq;
+            const int kz = q / M1, kx = q - kz * M1;
+            cpa16t(&sd[idx], spec + ((size_t)kz * ny + j) * M1 + kx);
+            cpa16t(&sf[idx], fac + (size_t)j * NQ + q);
+        }
+    }
+    for (int j = lane; j <= ny; j += 32) sa[j] = __ldg(&am2ph[j]);
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    __syncthreads();
+    double* sdd = reinterpret_cast<double*>(sd);
+    const int cq = lane >> 1;
+    const bool dc = (q0 + cq) == 0;
+    double fp = 0.0;
+    for (int j0 = 0; j0 < ny; j0 += YS_U) {
+        double d[YS_U], rv[YS_U], a[YS_U];
+#pragma unroll
+        for (int u = 0; u < YS_U; u++) {
+            const int j = j0 + u;
+            if (j < ny) {
+                d[u] = sdd[j * 32 + lane];
+                rv[u] = sf[j * 16 + cq].x;
+                a[u] = sa[j + 1];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < YS_U; u++) {
+            const int j = j0 + u;
+            if (j < ny) {
+                const double f = (j == 0) ? (dc ? 0.0 : d[u]) * rv[u] : (d[u] - a[u] * fp) * rv[u];
+                sdd[j * 32 + lane] = f;
+                fp = f;
+            }
+        }
+    }
+    double xn = fp;
+    for (int j0 = ny - 2; j0 >= 0; j0 -= YS_U) {
+        double d[YS_U], ar[YS_U];
+#pragma unroll
+        for (int u = 0; u < YS_U; u++) {
+            const int j = j0 - u;
+            if (j >= 0) {
+                d[u] = sdd[j * 32 + lane];
+                ar[u] = sf[(j + 1) * 16 + cq].y;
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < YS_U; u++) {
+            const int j = j0 - u;
+            if (j >= 0) {
+                const double x = d[u] - ar[u] * xn;
+                sdd[j * 32 + lane] = x;
+                xn = x;
+            }
+        }
+    }
+    __syncthreads();
+    for (int idx = lane; idx < ny * 16; idx += 32) {
+        const int j = idx >> 4, c2 = idx & 15;
+        if (c2 < nv) {
+            const int q = q0 + c2;
+            const int kz = q / M1, kx = q - kz * M1;
+            spec[((size_t)kz * ny + j) * M1 + kx] = sd[idx];
+        }
+    }
+}
+
+// Large grids: one thread per real column straight from global memory, the
+// rows of a chunk loaded ahead of its chain, latency hidden by occupancy.
+__global__ void __launch_bounds__(128) k_ys_global(int ny, int M1, int nz, const double* __restrict__ am2ph,
+                                                   double* __restrict__ specd, const double2* __restrict__ fac) {
+    const int W = 2 * M1, NQ = M1 * nz;
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= W * nz) return;
+    const int kz = g / W, cr = g - kz * W, q = g >> 1;
+    double* col = specd + (size_t)kz * ny * W + cr;
+    const double2* fc = fac + q;
+    const bool dc = (q == 0);
+    double fp = 0.0;
+    for (int j0 = 0; j0 < ny; j0 += YS_U) {
+        double d[YS_U], rv[YS_U], a[YS_U];
+#pragma unroll
+        for (int u = 0; u < YS_U; u++) {
+            const int j = j0 + u;
+            if (j < ny) {
+                d[u] = col[(size_t)j * W];
+                rv[u] = __ldg(&fc[(size_t)j * NQ]).x;
+                a[u] = __ldg(&am2ph[j + 1]);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < YS_U; u++) {
+            const int j = j0 + u;
+            if (j < ny) {
+                const double f = (j == 0) ? (dc ? 0.0 : d[u]) * rv[u] : (d[u] - a[u] * fp) * rv[u];
+                col[(size_t)j * W] = f;
+                fp = f;
+            }
+        }
+    }
+    double xn = fp;
+    for (int j0 = ny - 2; j0 >= 0; j0 -= YS_U) {
+        double d[YS_U], ar[YS_U];
+#pragma unroll
+        for (int u = 0; u < YS_U; u++) {
+            const int j = j0 - u;
+            if (j >= 0) {
+                d[u] = col[(size_t)j * W];
+                ar[u] = __ldg(&fc[(size_t)(j + 1) * NQ]).y;
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < YS_U; u++) {
+            const int j = j0 - u;
+            if (j >= 0) {
+                const double x = d[u] - ar[u] * xn;
+                col[(size_t)j * W] = x;
+                xn = x;
+            }
+        }
+    }
+}
+
+void launch_pois_factors(cudaStream_t st, const DConst& c, const DMetric& m, double2* fac) {
+    const int M1 = c.nx / 2 + 1, NQ = M1 * c.nz;
+    k_pois_factors<<<(NQ + 127) / 128, 128, 0, st>>>(c.ny, M1, c.nz, m, fac);
+}
+
+static size_t ys_staged_smem(int ny) { return (size_t)ny * 16 * 2 * sizeof(double2) + (size_t)(ny + 1) * sizeof(double); }
+
+void launch_ysolve_fac(cudaStream_t st, const DConst& c, const DMetric& m, double2* spec, const double2* fac) {
+    const int M1 = c.nx / 2 + 1, NQ = M1 * c.nz;
+    const size_t sm = ys_staged_smem(c.ny);
+    const int per_sm = sm > 0 ? (int)((220 * 1024) / sm) : 0;
+    const int ctas = (NQ + 15) / 16;
+    if (per_sm >= 1 && ctas <= per_sm * c.nsm) {
+        k_ys_staged<<<ctas, 32, sm, st>>>(c.ny, M1, c.nz, m.am2ph, spec, fac);
+    } else {
+        const int n = 2 * M1 * c.nz;
+        k_ys_global<<<(n + 127) / 128, 128, 0, st>>>(c.ny, M1, c.nz, m.am2ph, reinterpret_cast<double*>(spec), fac);
+    }
+}
+
+// ---------------------------------------------------------------------------
 // launchers: partition length MR in {8, 12, 16}, P = ceil(ny/MR) <= 16 warps
 // ---------------------------------------------------------------------------
 __host__ __device__ inline int part_len_dev(int ny) { return ny <= 64 ? 8 : (ny <= 192 ? 12 : 16); }
@@ -316,6 +516,7 @@ void tridiag_init() {
     cudaFuncSetAttribute(k_ysolve<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
     cudaFuncSetAttribute(k_ysolve<12>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
     cudaFuncSetAttribute(k_ysolve<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
+    cudaFuncSetAttribute(k_ys_staged, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
 }
 
 int tridiag_part_len(int ny) { return part_len(ny); }

@@ -42,15 +42,22 @@ void launch_helm(cudaStream_t st, const DConst& c, const DCoef* coef, const Fiel
 void launch_helm_scalar(cudaStream_t st, const DConst& c, const DCoef* coef, const Fields& f, const double* fac);
 void launch_ysolve(cudaStream_t st, const DConst& c, const DMetric& m, double2* spec);
 
-// k_plane.cu
-bool plane_supported(int nx, int nz, const FftPlan& plx, const FftPlan& plz);
-void plane_init();
-void launch_plane_fwd(cudaStream_t st, int mode, const DConst& c, const DMetric& m, DCoef* coef, const Fields& f,
-                      const double* src, double2* spec, const FftPlan& plx, const FftPlan& plz, const double2* twx,
-                      const double2* post, const double2* twz, double* part, unsigned int* counter, double* out_max);
-void launch_plane_inv(cudaStream_t st, int nx, int ny, int nz, const double2* spec, double* phi, const FftPlan& plx,
-                      const FftPlan& plz, const double2* twx, const double2* post, const double2* twz, double scale,
-                      int padded);
+// k_tridiag.cu: spectral y-solve with the pivots computed once per context
+void launch_pois_factors(cudaStream_t st, const DConst& c, const DMetric& m, double2* fac);
+void launch_ysolve_fac(cudaStream_t st, const DConst& c, const DMetric& m, double2* spec, const double2* fac);
+
+// k_pfft_x.cu / k_pfft_z.cu: compile-time-length transforms of the Poisson solve
+bool pfft_x_supported(int n);
+bool pfft_z_supported(int n);
+int pfft_x_blocks(int nx, int ny, int nz);
+void pfft_x_init();
+void pfft_z_init();
+void launch_pfft_xf(cudaStream_t st, int mode, const DConst& c, const DMetric& m, const DCoef* coef, const Fields& f,
+                    const double* src, double2* spec, const double2* twx, const double2* post, double* part,
+                    unsigned int* counter, double* out_max);
+void launch_pfft_xb(cudaStream_t st, int nx, int ny, int nz, const double2* spec, double* phi, const double2* twx,
+                    const double2* post, double scale, int padded);
+void launch_pfft_z(cudaStream_t st, int dir, int nx, int ny, int nz, double2* spec, const double2* twz);
 
 // k_fft.cu
 void fft_init();
