@@ -54,7 +54,8 @@ struct paratc_ctx {
     DDiag* d_diag = nullptr;
     DDiag* d_diag2 = nullptr;
     unsigned int* d_counter = nullptr;  // grid-completion counters of the last-block reductions
-    double* d_hfac = nullptr;           // Helmholtz factors of the current substep (3 matrix types)
+    double* d_hfac = nullptr;           // Helmholtz pivots of the substeps of a step (3 matrix types each)
+    double hfac_dt = -1.0;              // the fixed dt d_hfac holds pivots for (iCFL != 1), else < 0
     DDiag* h_diag = nullptr;   // pinned
     DCoef* h_coef = nullptr;   // pinned
     double* h_scal = nullptr;  // pinned
@@ -227,8 +228,14 @@ void enqueue_substep(paratc_ctx* ctx, int ns, int stop = 5) {
 
 void enqueue_step(paratc_ctx* ctx) {
     { PROF(PK_CFL); launch_cfl(ctx->st, ctx->kc, ctx->dm, ctx->f, ctx->d_coef, ctx->d_part); }
-    { PROF(PK_COEF); launch_helm_factors(ctx->st, ctx->kc, ctx->dm, ctx->d_coef, 1, ctx->hm.iadvance, ctx->hm.alp, ctx->d_hfac); }
-    ctx->launches += 3;
+    // with a fixed time step (iCFL != 1) the Helmholtz matrices never change:
+    // their pivots are computed once and kept
+    if (ctx->prm.icfl == 1 || ctx->hfac_dt != ctx->prm.dt_max) {
+        { PROF(PK_COEF); launch_helm_factors(ctx->st, ctx->kc, ctx->dm, ctx->d_coef, 1, ctx->hm.iadvance, ctx->hm.alp, ctx->d_hfac); }
+        ctx->launches += 1;
+        ctx->hfac_dt = (ctx->prm.icfl == 1) ? -1.0 : ctx->prm.dt_max;
+    }
+    ctx->launches += 2;
     for (int ns = 1; ns <= ctx->hm.iadvance; ns++) enqueue_substep(ctx, ns);
     { PROF(PK_CHECK); launch_check(ctx->st, ctx->kc, ctx->dm, ctx->f, ctx->d_coef, ctx->d_diag, ctx->d_part); }
     ctx->launches += 2;
@@ -631,6 +638,7 @@ int paratc_substep_stage(paratc_ctx* ctx, int ns, double dt, int stop_stage, dou
     ctx->h_coef->dt = dt;
     CK(cudaMemcpyAsync(ctx->d_coef, ctx->h_coef, sizeof(DCoef), cudaMemcpyHostToDevice, ctx->st));
     launch_helm_factors(ctx->st, ctx->kc, ctx->dm, ctx->d_coef, ns, 1, ctx->hm.alp, ctx->d_hfac);
+    ctx->hfac_dt = -1.0;  // pivots of substep ns now hold this call's dt
     ctx->launches += 1;
     enqueue_substep(ctx, ns, stop_stage);
     CK(cudaMemcpyAsync(ctx->h_coef, ctx->d_coef, sizeof(DCoef), cudaMemcpyDeviceToHost, ctx->st));

@@ -9,17 +9,17 @@
 // with the reduced-system ("PaScaL") Thomas of clcPPE_x1_reduce
 // (src/m_Poisson.f90:457-695).
 //
-// Here one CTA owns 32 adjacent columns (lanes, coalesced in x / kx) and
-// splits y into P partitions, one warp each.  Each thread keeps its partition
-// in registers and eliminates it locally with the modified Thomas sweep of
-// the reduced algorithm, so that every row depends only on the partition's
-// first and last unknowns; the 2P-row reduced system of each column is solved
-// by one thread from shared memory; the back substitution is local again.
-// HBM traffic is one read of the right-hand side (plus the field for the
-// Helmholtz update) and one write per cell.
+// The matrices never depend on the column's data, only on the row (the
+// Helmholtz systems, per step) or on the row and the wavenumber pair (the
+// Poisson systems, per context).  So the Thomas pivots are computed apart
+// from the solves, and a solve is a chain of multiply-adds per column with
+// its loads issued ahead: k_helm (pivots per step, k_helm_factors) and
+// k_ys_staged / k_ys_global (pivots per context, k_pois_factors).  The
+// partitioned reduced-system solver (part_eliminate / part_reduced /
+// k_ysolve) computes its pivots in place; the allocation-free Poisson entry
+// point uses it because it has no room to keep pivots between calls.
 #include "common.cuh"
 #include "kernels.cuh"
-#include "helm_factor.cuh"
 
 namespace ptc {
 
@@ -130,17 +130,6 @@ __device__ __forceinline__ void part_reduced(int P, int w, int lane, const doubl
 }
 
 // diagonal of row r of a partition starting at Fortran row s
-struct HelmDiag {
-    const double* ac;
-    double beta;
-    int s, ny;
-    bool vrow1;  // clcU2Hat: row 1 is the identity
-    __device__ __forceinline__ double operator()(int r) const {
-        const int jc = s + r;
-        if (jc > ny || (vrow1 && jc == 1)) return 1.0;
-        return -(beta * __ldg(&ac[jc])) + 1.0;
-    }
-};
 struct PoisDiag {
     const double* ac2ph;
     double lam;
@@ -155,92 +144,126 @@ struct PoisDiag {
 
 // ---------------------------------------------------------------------------
 // Helmholtz: comp 0 ux (clcU1Hat), 1 uy (clcU2Hat), 2 uz (clcU3Hat),
-// 3 scalar (clcScalar); u(jc) += du(jc).  The factors of the three matrix
-// types come from helm_factor_* (computed once per substep); per column the
-// solve is the same elimination as part_eliminate / part_reduced applied
-// with those multipliers.  uy and the scalar also get the ghost values that
+// 3 scalar (clcScalar); u(jc) += du(jc) with (I - beta*Lyy) du = Rhs
+// (src/m_TScheme.f90:365-506).  The matrices depend on the row only, so
+// their Thomas pivots (InverseTridiagonal, src/m_Tools.f90:224-251) are
+// computed once per step by k_helm_factors: for matrix (ns, type) and row jc,
+// A = a(jc), RV = 1/vecm(jc), AR = arr(jc), evaluated in the reference's
+// order without contraction.  A warp then sweeps 32 adjacent columns (i)
+// straight from memory: rows come in chunks of HY_U held in a three-chunk
+// register ring, so two chunks are in flight while one is on the dependent
+// chain.  The forward sweep writes f(jc) back over Rhs (it stays in L2 for
+// the backward sweep), the backward sweep adds the solution to u.
+// uy and the scalar also get the ghost values that
 // SetBC_and_UpdateHaloForPrSrc / _scalar give them.
 // ---------------------------------------------------------------------------
-template <int MR>
-__global__ void __launch_bounds__(512) k_helm(DConst cst, const DCoef* __restrict__ coef, int comp0, Fields fl,
+namespace {
+constexpr int HY_U = 8;  // rows per chunk; three chunks in registers, two in flight
+__host__ __device__ inline int helm_stride(int ny) { return 3 * (ny + 2); }
+}  // namespace
+
+// lane = column i of the strip [32*blockIdx.x, +32) at z index
+// blockIdx.y*4 + threadIdx.y, component comp0 + blockIdx.z
+__global__ void __launch_bounds__(128) k_helm(DConst cst, const DCoef* __restrict__ coef, int comp0, Fields fl,
                                               const double* __restrict__ duy_ym, const double* __restrict__ uy_ym,
                                               const double* __restrict__ facs) {
-    extern __shared__ double sm[];
-    const int lane = threadIdx.x, w = threadIdx.y, P = blockDim.y;
     const int nx = cst.nx, ny = cst.ny;
-    const int i = blockIdx.x * 32 + lane;
-    const int k = blockIdx.y;
+    const int i = blockIdx.x * 32 + threadIdx.x;
+    const int k = blockIdx.y * blockDim.y + threadIdx.y;
     const int comp = comp0 + blockIdx.z;
-    const bool act = i < nx;
-    const int s = w * MR + 1;
-    const HelmFacLayout L = helm_fac_layout(MR, P);
+    if (i >= nx || k >= cst.nz) return;
     const int t = comp == 1 ? 1 : (comp == 3 ? 2 : 0);
-    const double* fac = facs + ((size_t)(coef->ns - 1) * 3 + t) * L.stride;
+    const double* __restrict__ F = facs + (size_t)((coef->ns - 1) * 3 + t) * helm_stride(ny);
+    const double* __restrict__ FA = F;
+    const double* __restrict__ FR = F + (ny + 2);
+    const double* __restrict__ FW = F + 2 * (ny + 2);
     double* u;
-    const double* rhs;
+    double* rhs;
     double add = 0.0;
     if (comp == 0)      { u = fl.ux; rhs = fl.rx; add = coef->rhsx_add; }
     else if (comp == 1) { u = fl.uy; rhs = fl.ry; }
     else if (comp == 2) { u = fl.uz; rhs = fl.rz; }
     else                { u = fl.sc; rhs = fl.rc; }
+    const size_t col = (size_t)k * cst.nyt * nx + i;
+    double* rc = rhs + col;
+    double* uc = u + col;
+    const int nch = (ny + HY_U - 1) / HY_U;
+    const double r1 = (comp == 1) ? duy_ym[(size_t)k * nx + i] : 0.0;
 
-    const size_t zc = (size_t)k * cst.nyt * nx;
-    double f[MR], uo[MR];
+    // forward sweep, rows 1..ny; f(jc) is written back over Rhs
+    double fp = 0.0;
+    double A[HY_U], B[HY_U], C[HY_U];
+    auto ldr = [&](double (&X)[HY_U], int cc) {
 #pragma unroll
-    for (int r = 0; r < MR; r++) {
-        const int jc = s + r;
-        f[r] = 0.0;
-        uo[r] = 0.0;
-        if (act && jc <= ny) {
-            const size_t q = zc + (size_t)jc * nx + i;
-            f[r] = (comp == 1 && jc == 1) ? duy_ym[(size_t)k * nx + i] : rhs[q] + add;
-            uo[r] = u[q];
+        for (int q = 0; q < HY_U; q++) {
+            const int j = 1 + cc * HY_U + q;
+            if (cc < nch && j <= ny) X[q] = rc[(size_t)j * nx];
         }
+    };
+    auto fwd = [&](const double (&X)[HY_U], int cc) {
+        if (cc >= nch) return;
+#pragma unroll
+        for (int q = 0; q < HY_U; q++) {
+            const int j = 1 + cc * HY_U + q;
+            if (j <= ny) {
+                const double f = (j == 1) ? ((comp == 1) ? r1 : X[q] + add) * FR[1]
+                                          : ((X[q] + add) - FA[j] * fp) * FR[j];
+                rc[(size_t)j * nx] = f;
+                fp = f;
+            }
+        }
+    };
+    ldr(A, 0);
+    ldr(B, 1);
+    ldr(C, 2);
+    for (int c = 0; c < nch; c += 3) {
+        fwd(A, c);
+        ldr(A, c + 3);
+        fwd(B, c + 1);
+        ldr(B, c + 4);
+        fwd(C, c + 2);
+        ldr(C, c + 5);
     }
-    const int g0 = w * MR;
-    f[0] = f[0] * __ldg(&fac[L.F0 + g0]);
-    f[1] = f[1] * __ldg(&fac[L.F0 + g0 + 1]);
+    // backward sweep, rows ny..1; u(jc) += x(jc)
+    double xn = 0.0;
+    double DA[HY_U], DB[HY_U], DC[HY_U], UA[HY_U], UB[HY_U], UC[HY_U];
+    auto ldb = [&](double (&D)[HY_U], double (&U)[HY_U], int cc) {
 #pragma unroll
-    for (int r = 2; r < MR; r++) f[r] = __ldg(&fac[L.F0 + g0 + r]) * (f[r] - __ldg(&fac[L.A0 + g0 + r]) * f[r - 1]);
-#pragma unroll
-    for (int r = MR - 3; r >= 1; r--) f[r] = f[r] - __ldg(&fac[L.CB + g0 + r]) * f[r + 1];
-    f[0] = __ldg(&fac[L.R0 + w]) * (f[0] - __ldg(&fac[L.C0 + w]) * f[1]);
-
-    // reduced system of the column (unknowns x_first/x_last of every
-    // partition): x = Rinv * F with the precomputed dense inverse, each warp
-    // producing its own two unknowns for the 32 columns
-    double* RF = sm;  // [2P][32]
-    RF[(2 * w) * 32 + lane] = f[0];
-    RF[(2 * w + 1) * 32 + lane] = f[MR - 1];
-    __syncthreads();
-    const int n2 = 2 * P;
-    double xf = 0.0, xl = 0.0;
-    {
-        const double* r0 = fac + L.RI + (size_t)(2 * w) * n2;
-        const double* r1 = r0 + n2;
-        for (int q = 0; q < n2; q++) {
-            const double F = RF[q * 32 + lane];
-            xf += __ldg(&r0[q]) * F;
-            xl += __ldg(&r1[q]) * F;
+        for (int q = 0; q < HY_U; q++) {
+            const int j = ny - cc * HY_U - q;
+            if (cc < nch && j >= 1) {
+                D[q] = rc[(size_t)j * nx];
+                U[q] = uc[(size_t)j * nx];
+            }
         }
-    }
-    if (!act) return;
+    };
+    auto bwd = [&](const double (&D)[HY_U], const double (&U)[HY_U], int cc) {
+        if (cc >= nch) return;
 #pragma unroll
-    for (int r = 0; r < MR; r++) {
-        const int jc = s + r;
-        if (jc <= ny) {
-            double x;
-            if (r == 0) x = xf;
-            else if (r == MR - 1) x = xl;
-            else x = f[r] - __ldg(&fac[L.AF + g0 + r]) * xf - __ldg(&fac[L.CF + g0 + r]) * xl;
-            const size_t q = zc + (size_t)jc * nx + i;
-            double un = uo[r] + x;
-            if (comp == 1 && jc == 1) un = uy_ym[(size_t)k * nx + i];
-            u[q] = un;
-            if (comp == 1 && jc == ny) u[q + nx] = (cst.flow_type == 1) ? cst.uybc_yp : 0.0;
-            if (comp == 3 && jc == 1) u[q - nx] = cst.sc_r1b * un + cst.sc_r2b;
-            if (comp == 3 && jc == ny) u[q + nx] = cst.sc_r1t * un + cst.sc_r2t;
+        for (int q = 0; q < HY_U; q++) {
+            const int j = ny - cc * HY_U - q;
+            if (j >= 1) {
+                const double x = (j == ny) ? D[q] : D[q] - FW[j + 1] * xn;
+                xn = x;
+                double unew = U[q] + x;
+                if (comp == 1 && j == 1) unew = uy_ym[(size_t)k * nx + i];
+                uc[(size_t)j * nx] = unew;
+                if (comp == 1 && j == ny) uc[(size_t)(ny + 1) * nx] = (cst.flow_type == 1) ? cst.uybc_yp : 0.0;
+                if (comp == 3 && j == 1) uc[0] = cst.sc_r1b * unew + cst.sc_r2b;
+                if (comp == 3 && j == ny) uc[(size_t)(ny + 1) * nx] = cst.sc_r1t * unew + cst.sc_r2t;
+            }
         }
+    };
+    ldb(DA, UA, 0);
+    ldb(DB, UB, 1);
+    ldb(DC, UC, 2);
+    for (int c = 0; c < nch; c += 3) {
+        bwd(DA, UA, c);
+        ldb(DA, UA, c + 3);
+        bwd(DB, UB, c + 1);
+        ldb(DB, UB, c + 4);
+        bwd(DC, UC, c + 2);
+        ldb(DC, UC, c + 5);
     }
 }
 
@@ -347,22 +370,25 @@ __global__ void __launch_bounds__(32) k_ys_staged(int ny, int M1, int nz, const 
     double2* sd = sy;                   // [ny][16] spectrum
     double2* sf = sy + ny * 16;         // [ny][16] factors
     double* sa = reinterpret_cast<double*>(sf + ny * 16);  // am2ph[0..ny]
-    for (int idx = lane; idx < ny * 16; idx += 32) {
-        const int j = idx >> 4, cq = idx & 15;
-        if (cq < nv) {
-            const int q = q0 + cq;
-            const int kz = q / M1, kx = q - kz * M1;
-            cpa16t(&sd[idx], spec + ((size_t)kz * ny + j) * M1 + kx);
-            cpa16t(&sf[idx], fac + (size_t)j * NQ + q);
+    // lane (cq, half) copies rows half, half+2, ... of complex column q0+cq
+    const int cq = lane & 15, half = lane >> 4;
+    const bool cval = cq < nv;
+    const int qq = q0 + (cval ? cq : 0);
+    const int kz = qq / M1, kx = qq - kz * M1;
+    double2* scol = spec + (size_t)kz * ny * M1 + kx;
+    const double2* fcol = fac + qq;
+    if (cval)
+        for (int j = half; j < ny; j += 2) {
+            cpa16t(&sd[j * 16 + cq], scol + (size_t)j * M1);
+            cpa16t(&sf[j * 16 + cq], fcol + (size_t)j * NQ);
         }
-    }
     for (int j = lane; j <= ny; j += 32) sa[j] = __ldg(&am2ph[j]);
     asm volatile("cp.async.commit_group;\n" ::: "memory");
     asm volatile("cp.async.wait_group 0;\n" ::: "memory");
     __syncthreads();
     double* sdd = reinterpret_cast<double*>(sd);
-    const int cq = lane >> 1;
-    const bool dc = (q0 + cq) == 0;
+    const int cp = lane >> 1;  // complex column of this lane's real or imaginary part
+    const bool dc = (q0 + cp) == 0;
     double fp = 0.0;
     for (int j0 = 0; j0 < ny; j0 += YS_U) {
         double d[YS_U], rv[YS_U], a[YS_U];
@@ -371,7 +397,7 @@ __global__ void __launch_bounds__(32) k_ys_staged(int ny, int M1, int nz, const 
             const int j = j0 + u;
             if (j < ny) {
                 d[u] = sdd[j * 32 + lane];
-                rv[u] = sf[j * 16 + cq].x;
+                rv[u] = sf[j * 16 + cp].x;
                 a[u] = sa[j + 1];
             }
         }
@@ -393,7 +419,7 @@ __global__ void __launch_bounds__(32) k_ys_staged(int ny, int M1, int nz, const 
             const int j = j0 - u;
             if (j >= 0) {
                 d[u] = sdd[j * 32 + lane];
-                ar[u] = sf[(j + 1) * 16 + cq].y;
+                ar[u] = sf[(j + 1) * 16 + cp].y;
             }
         }
 #pragma unroll
@@ -407,14 +433,8 @@ __global__ void __launch_bounds__(32) k_ys_staged(int ny, int M1, int nz, const 
         }
     }
     __syncthreads();
-    for (int idx = lane; idx < ny * 16; idx += 32) {
-        const int j = idx >> 4, c2 = idx & 15;
-        if (c2 < nv) {
-            const int q = q0 + c2;
-            const int kz = q / M1, kx = q - kz * M1;
-            spec[((size_t)kz * ny + j) * M1 + kx] = sd[idx];
-        }
-    }
+    if (cval)
+        for (int j = half; j < ny; j += 2) scol[(size_t)j * M1] = sd[j * 16 + cq];
 }
 
 // Large grids: one thread per real column straight from global memory, the
@@ -509,58 +529,78 @@ bool tridiag_supported(int ny) { return ny >= 3 && ny <= 256; }
 
 static size_t red_smem(int P, int nc) { return (size_t)2 * P * 32 * (3 + nc) * sizeof(double); }
 
+__global__ void k_helm_factors(DConst cst, DMetric m, const DCoef* __restrict__ coef, int ns0, int nsub, double a1,
+                               double a2, double a3, double* __restrict__ facs);
+
 void tridiag_init() {
-    cudaFuncSetAttribute(k_helm<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
-    cudaFuncSetAttribute(k_helm<12>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
-    cudaFuncSetAttribute(k_helm<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
     cudaFuncSetAttribute(k_ysolve<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
     cudaFuncSetAttribute(k_ysolve<12>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
     cudaFuncSetAttribute(k_ysolve<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
     cudaFuncSetAttribute(k_ys_staged, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
+    cudaFuncSetAttribute(k_helm_factors, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
 }
 
 int tridiag_part_len(int ny) { return part_len(ny); }
 
-size_t helm_fac_doubles(int ny) {
-    const HelmFacLayout L = helm_fac_layout(part_len(ny), tridiag_partitions(ny));
-    return (size_t)9 * L.stride;
-}
+size_t helm_fac_doubles(int ny) { return (size_t)9 * helm_stride(ny); }
 
-// factors of the Helmholtz matrices for substeps ns0..ns0+nsub-1 of the
-// current dt (coef->dt): matrix (ns, t) -> facs + ((ns-1)*3 + t)*stride
-__global__ void k_helm_factors(DConst cst, DMetric m, const DCoef* __restrict__ coef, int ns0, int nsub, double a1,
-                               double a2, double a3, double* __restrict__ facs) {
+// pivots of the Helmholtz matrices of substeps ns0..ns0+nsub-1 for the
+// current dt (coef->dt): one thread per (substep, type) runs the forward
+// elimination of InverseTridiagonal on the coefficients of clcU1Hat /
+// clcU2Hat / clcScalar (src/m_TScheme.f90:374-380,409-420,486-492)
+__global__ void __launch_bounds__(32) k_helm_factors(DConst cst, DMetric m, const DCoef* __restrict__ coef, int ns0,
+                                                     int nsub, double a1, double a2, double a3,
+                                                     double* __restrict__ facs) {
+    extern __shared__ double shm[];  // ap, ac, am of the three types, rows 0..ny+1
+    const int ny = cst.ny, L = ny + 2;
+    const double* srcs[9] = {m.ap2cCN, m.ac2cCN, m.am2cCN, m.ap2p, m.ac2p, m.am2p, m.ap2cScCN, m.ac2cScCN, m.am2cScCN};
+    for (int a = 0; a < 9; a++)
+        for (int j = threadIdx.x; j < L; j += blockDim.x) shm[a * L + j] = srcs[a][j];
+    __syncthreads();
+    const int q = threadIdx.x;
+    if (q >= 3 * nsub) return;
+    const int ns = ns0 + q / 3, t = q % 3;
+    const double alp = ns == 1 ? a1 : (ns == 2 ? a2 : a3);
     const double dt = coef->dt;
-    const double alps[3] = {a1, a2, a3};
-    double betas[9];
-    int types[9];
-    int nmat = 0;
-    for (int n = ns0; n < ns0 + nsub; n++) {
-        const double alp = alps[n - 1];
-        for (int t = 0; t < 3; t++) {
-            betas[nmat] = (t == 2) ? 0.5 * alp * cst.sdiff * dt : 0.5 * alp * cst.xnu * dt;
-            types[nmat] = t;
-            nmat++;
-        }
+    const double beta = (t == 2) ? 0.5 * alp * cst.sdiff * dt : 0.5 * alp * cst.xnu * dt;
+    const double* ap = shm + (3 * t) * L;
+    const double* ac = ap + L;
+    const double* am = ac + L;
+    double* F = facs + (size_t)((ns - 1) * 3 + t) * helm_stride(ny);
+    double* FA = F;
+    double* FR = F + (ny + 2);
+    double* FW = F + 2 * (ny + 2);
+    const bool vrow1 = (t == 1);  // clcU2Hat: row 1 is the identity
+    double vecm = vrow1 ? 1.0 : __dadd_rn(-__dmul_rn(beta, ac[1]), 1.0);
+    double cprev = vrow1 ? 0.0 : -__dmul_rn(beta, ap[1]);
+    FA[0] = FR[0] = FW[0] = 0.0;
+    FA[1] = 0.0;
+    FR[1] = 1.0 / vecm;
+    FW[1] = 0.0;
+    for (int jc = 2; jc <= ny; jc++) {
+        const double arr = cprev / vecm;
+        const double a = -__dmul_rn(beta, am[jc]);
+        const double b = __dadd_rn(-__dmul_rn(beta, ac[jc]), 1.0);
+        vecm = __dsub_rn(b, __dmul_rn(a, arr));
+        FA[jc] = a;
+        FR[jc] = 1.0 / vecm;
+        FW[jc] = arr;
+        cprev = -__dmul_rn(beta, ap[jc]);
     }
-    const HelmFacLayout L = helm_fac_layout(part_len_dev(cst.ny), tridiag_partitions_dev(cst.ny));
-    helm_factor_block(m, cst.ny, L, nmat, betas, types, facs + (size_t)(ns0 - 1) * 3 * L.stride);
+    FA[ny + 1] = FR[ny + 1] = FW[ny + 1] = 0.0;
 }
 
 void launch_helm_factors(cudaStream_t st, const DConst& c, const DMetric& m, const DCoef* coef, int ns0, int nsub,
                          const double* alp, double* fac) {
-    k_helm_factors<<<1, 128, 0, st>>>(c, m, coef, ns0, nsub, alp[0], alp[1], alp[2], fac);
+    k_helm_factors<<<1, 32, (size_t)9 * (c.ny + 2) * sizeof(double), st>>>(c, m, coef, ns0, nsub, alp[0], alp[1],
+                                                                           alp[2], fac);
 }
 
 static void helm_dispatch(cudaStream_t st, const DConst& c, const DCoef* coef, int comp0, int ncomp, const Fields& f,
                           const double* duy_ym, const double* uy_ym, const double* fac) {
-    const int mr = part_len(c.ny), P = tridiag_partitions(c.ny);
-    dim3 blk(32, P);
-    dim3 grd((c.nx + 31) / 32, c.nz, ncomp);
-    const size_t sm = (size_t)2 * P * 32 * sizeof(double);
-    if (mr == 8) k_helm<8><<<grd, blk, sm, st>>>(c, coef, comp0, f, duy_ym, uy_ym, fac);
-    else if (mr == 12) k_helm<12><<<grd, blk, sm, st>>>(c, coef, comp0, f, duy_ym, uy_ym, fac);
-    else k_helm<16><<<grd, blk, sm, st>>>(c, coef, comp0, f, duy_ym, uy_ym, fac);
+    dim3 blk(32, 4);
+    dim3 grd((c.nx + 31) / 32, (c.nz + 3) / 4, ncomp);
+    k_helm<<<grd, blk, 0, st>>>(c, coef, comp0, f, duy_ym, uy_ym, fac);
 }
 
 void launch_helm(cudaStream_t st, const DConst& c, const DCoef* coef, const Fields& f, const double* duy_ym,
