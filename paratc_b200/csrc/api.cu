@@ -422,6 +422,12 @@ int paratc_create(const paratc_params* prm, const double* yp, int device, paratc
     kc.nx = ctx->nx; kc.ny = ctx->ny; kc.nz = ctx->nz; kc.nyp = ctx->nyp; kc.nyt = ctx->nyt;
     kc.flow_type = prm->flow_type; kc.scalar_on = prm->scalar_on; kc.is_ux_const = prm->is_ux_const; kc.icfl = prm->icfl;
     cudaDeviceGetAttribute(&kc.nsm, cudaDevAttrMultiProcessorCount, ctx->dev);
+    {
+        // PARATC_YSOLVER=staged|streaming pins the variant of the y-solve
+        // kernels (both are exact; the choice is normally made by size)
+        const char* e = std::getenv("PARATC_YSOLVER");
+        kc.solver_sel = !e ? 0 : (std::strcmp(e, "staged") == 0 ? 1 : (std::strcmp(e, "streaming") == 0 ? 2 : 0));
+    }
     for (int q = 0; q < 4; q++) { kc.dxC[q] = h.dxC[q]; kc.dzC[q] = h.dzC[q]; kc.IC[q] = h.IC[q]; }
     for (int q = 0; q < 5; q++) { kc.dxxC[q] = h.dxxC[q]; kc.dzzC[q] = h.dzzC[q]; }
     kc.rdx = h.rdx; kc.rdz = h.rdz;

@@ -35,6 +35,7 @@ struct DConst {
     int nx, ny, nz, nyp, nyt;
     int flow_type, scalar_on, is_ux_const, icfl;
     int nsm;  // streaming multiprocessors of the device
+    int solver_sel;  // 0 automatic; 1 forces the staged, 2 the streaming y-solve kernels (tests)
     double dxC[4], dzC[4], dxxC[5], dzzC[5], IC[4];
     double rdx, rdz;
     double ucrf, xnu, grav[3], sdiff, gev[3], fvv[3];

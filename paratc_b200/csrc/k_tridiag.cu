@@ -162,21 +162,31 @@ constexpr int HY_U = 8;  // rows per chunk; three chunks in registers, two in fl
 __host__ __device__ inline int helm_stride(int ny) { return 3 * (ny + 2); }
 }  // namespace
 
-// lane = column i of the strip [32*blockIdx.x, +32) at z index
-// blockIdx.y*4 + threadIdx.y, component comp0 + blockIdx.z
+// thread = column i = 128*blockIdx.x + 32*threadIdx.y + lane at z index
+// blockIdx.y, component comp0 + blockIdx.z: the four warps of a CTA read
+// one contiguous 1 KB stretch of a row together.  The pivots sit in shared
+// memory; rows are addressed by pointer steps; the wall rows need no case of
+// their own in the sweeps (a(1) = 0, arr(ny+1) = 0, and clcU2Hat's row-1
+// value is substituted before the sweep and its result after it).
 __global__ void __launch_bounds__(128) k_helm(DConst cst, const DCoef* __restrict__ coef, int comp0, Fields fl,
                                               const double* __restrict__ duy_ym, const double* __restrict__ uy_ym,
                                               const double* __restrict__ facs) {
+    extern __shared__ double shf[];
     const int nx = cst.nx, ny = cst.ny;
-    const int i = blockIdx.x * 32 + threadIdx.x;
-    const int k = blockIdx.y * blockDim.y + threadIdx.y;
     const int comp = comp0 + blockIdx.z;
-    if (i >= nx || k >= cst.nz) return;
     const int t = comp == 1 ? 1 : (comp == 3 ? 2 : 0);
-    const double* __restrict__ F = facs + (size_t)((coef->ns - 1) * 3 + t) * helm_stride(ny);
-    const double* __restrict__ FA = F;
-    const double* __restrict__ FR = F + (ny + 2);
-    const double* __restrict__ FW = F + 2 * (ny + 2);
+    {
+        const double* F = facs + (size_t)((coef->ns - 1) * 3 + t) * helm_stride(ny);
+        const int tid = threadIdx.y * 32 + threadIdx.x;
+        for (int q = tid; q < helm_stride(ny); q += 128) shf[q] = F[q];
+    }
+    __syncthreads();
+    const double* SA = shf;
+    const double* SR = shf + (ny + 2);
+    const double* SW = shf + 2 * (ny + 2);
+    const int i = (blockIdx.x * 4 + threadIdx.y) * 32 + threadIdx.x;
+    const int k = blockIdx.y;
+    if (i >= nx) return;
     double* u;
     double* rhs;
     double add = 0.0;
@@ -188,32 +198,39 @@ __global__ void __launch_bounds__(128) k_helm(DConst cst, const DCoef* __restric
     double* rc = rhs + col;
     double* uc = u + col;
     const int nch = (ny + HY_U - 1) / HY_U;
-    const double r1 = (comp == 1) ? duy_ym[(size_t)k * nx + i] : 0.0;
+    const size_t step = (size_t)HY_U * nx;
 
-    // forward sweep, rows 1..ny; f(jc) is written back over Rhs
-    double fp = 0.0;
+    // forward sweep, rows 1..ny: f = ((r + add) - a f_prev) / vecm, written over Rhs
     double A[HY_U], B[HY_U], C[HY_U];
     auto ldr = [&](double (&X)[HY_U], int cc) {
+        if (cc >= nch) return;
+        const double* b = rc + (size_t)(cc * HY_U + 1) * nx;
+        const int nr = ny - cc * HY_U;
 #pragma unroll
         for (int q = 0; q < HY_U; q++) {
-            const int j = 1 + cc * HY_U + q;
-            if (cc < nch && j <= ny) X[q] = rc[(size_t)j * nx];
+            if (q < nr) X[q] = *b;
+            b += nx;
         }
     };
+    double fp = 0.0;
+    double* wp = rc + nx;
     auto fwd = [&](const double (&X)[HY_U], int cc) {
         if (cc >= nch) return;
+        const int nr = ny - cc * HY_U;
+        const double* sa = SA + cc * HY_U + 1;
+        const double* sr = SR + cc * HY_U + 1;
 #pragma unroll
         for (int q = 0; q < HY_U; q++) {
-            const int j = 1 + cc * HY_U + q;
-            if (j <= ny) {
-                const double f = (j == 1) ? ((comp == 1) ? r1 : X[q] + add) * FR[1]
-                                          : ((X[q] + add) - FA[j] * fp) * FR[j];
-                rc[(size_t)j * nx] = f;
+            if (q < nr) {
+                const double f = ((X[q] + add) - sa[q] * fp) * sr[q];
+                *wp = f;
                 fp = f;
             }
+            wp += nx;
         }
     };
     ldr(A, 0);
+    if (comp == 1) A[0] = duy_ym[(size_t)k * nx + i];  // clcU2Hat: the row-1 value is the wall increment
     ldr(B, 1);
     ldr(C, 2);
     for (int c = 0; c < nch; c += 3) {
@@ -224,34 +241,36 @@ __global__ void __launch_bounds__(128) k_helm(DConst cst, const DCoef* __restric
         fwd(C, c + 2);
         ldr(C, c + 5);
     }
-    // backward sweep, rows ny..1; u(jc) += x(jc)
-    double xn = 0.0;
+    // backward sweep, rows ny..1: x = f - arr(j+1) x(j+1), u += x
     double DA[HY_U], DB[HY_U], DC[HY_U], UA[HY_U], UB[HY_U], UC[HY_U];
     auto ldb = [&](double (&D)[HY_U], double (&U)[HY_U], int cc) {
+        if (cc >= nch) return;
+        const size_t off = (size_t)(ny - cc * HY_U) * nx;
+        const double* bd = rc + off;
+        const double* bu = uc + off;
+        const int nr = ny - cc * HY_U;
 #pragma unroll
         for (int q = 0; q < HY_U; q++) {
-            const int j = ny - cc * HY_U - q;
-            if (cc < nch && j >= 1) {
-                D[q] = rc[(size_t)j * nx];
-                U[q] = uc[(size_t)j * nx];
-            }
+            if (q < nr) { D[q] = *bd; U[q] = *bu; }
+            bd -= nx;
+            bu -= nx;
         }
     };
+    double xn = 0.0, unew = 0.0, utop = 0.0;
+    double* up = uc + (size_t)ny * nx;
     auto bwd = [&](const double (&D)[HY_U], const double (&U)[HY_U], int cc) {
         if (cc >= nch) return;
+        const int nr = ny - cc * HY_U;
+        const double* sw = SW + ny + 1 - cc * HY_U;
 #pragma unroll
         for (int q = 0; q < HY_U; q++) {
-            const int j = ny - cc * HY_U - q;
-            if (j >= 1) {
-                const double x = (j == ny) ? D[q] : D[q] - FW[j + 1] * xn;
+            if (q < nr) {
+                const double x = D[q] - sw[-q] * xn;
                 xn = x;
-                double unew = U[q] + x;
-                if (comp == 1 && j == 1) unew = uy_ym[(size_t)k * nx + i];
-                uc[(size_t)j * nx] = unew;
-                if (comp == 1 && j == ny) uc[(size_t)(ny + 1) * nx] = (cst.flow_type == 1) ? cst.uybc_yp : 0.0;
-                if (comp == 3 && j == 1) uc[0] = cst.sc_r1b * unew + cst.sc_r2b;
-                if (comp == 3 && j == ny) uc[(size_t)(ny + 1) * nx] = cst.sc_r1t * unew + cst.sc_r2t;
+                unew = U[q] + x;
+                *up = unew;
             }
+            up -= nx;
         }
     };
     ldb(DA, UA, 0);
@@ -259,11 +278,20 @@ __global__ void __launch_bounds__(128) k_helm(DConst cst, const DCoef* __restric
     ldb(DC, UC, 2);
     for (int c = 0; c < nch; c += 3) {
         bwd(DA, UA, c);
+        if (c == 0) utop = DA[0] + UA[0];  // u(ny): x(ny) = f(ny)
         ldb(DA, UA, c + 3);
         bwd(DB, UB, c + 1);
         ldb(DB, UB, c + 4);
         bwd(DC, UC, c + 2);
         ldb(DC, UC, c + 5);
+    }
+    // wall rows: unew now holds u(1)
+    if (comp == 1) {
+        uc[nx] = uy_ym[(size_t)k * nx + i];
+        uc[(size_t)(ny + 1) * nx] = (cst.flow_type == 1) ? cst.uybc_yp : 0.0;
+    } else if (comp == 3) {
+        uc[0] = cst.sc_r1b * unew + cst.sc_r2b;
+        uc[(size_t)(ny + 1) * nx] = cst.sc_r1t * utop + cst.sc_r2t;
     }
 }
 
@@ -505,7 +533,7 @@ void launch_ysolve_fac(cudaStream_t st, const DConst& c, const DMetric& m, doubl
     const size_t sm = ys_staged_smem(c.ny);
     const int per_sm = sm > 0 ? (int)((220 * 1024) / sm) : 0;
     const int ctas = (NQ + 15) / 16;
-    if (per_sm >= 1 && ctas <= per_sm * c.nsm) {
+    if (per_sm >= 1 && (c.solver_sel == 1 || (c.solver_sel == 0 && ctas <= per_sm * c.nsm))) {
         k_ys_staged<<<ctas, 32, sm, st>>>(c.ny, M1, c.nz, m.am2ph, spec, fac);
     } else {
         const int n = 2 * M1 * c.nz;
@@ -599,8 +627,8 @@ void launch_helm_factors(cudaStream_t st, const DConst& c, const DMetric& m, con
 static void helm_dispatch(cudaStream_t st, const DConst& c, const DCoef* coef, int comp0, int ncomp, const Fields& f,
                           const double* duy_ym, const double* uy_ym, const double* fac) {
     dim3 blk(32, 4);
-    dim3 grd((c.nx + 31) / 32, (c.nz + 3) / 4, ncomp);
-    k_helm<<<grd, blk, 0, st>>>(c, coef, comp0, f, duy_ym, uy_ym, fac);
+    dim3 grd((c.nx + 127) / 128, c.nz, ncomp);
+    k_helm<<<grd, blk, helm_stride(c.ny) * sizeof(double), st>>>(c, coef, comp0, f, duy_ym, uy_ym, fac);
 }
 
 void launch_helm(cudaStream_t st, const DConst& c, const DCoef* coef, const Fields& f, const double* duy_ym,

@@ -1,8 +1,9 @@
 """Parity of the CUDA hot path (through the C ABI) with the CPU oracle.
 
-Tolerances (FP64 on both sides; the kernels contract multiply-adds into FMA
-and solve the tridiagonal systems by partitions, so results agree to
-rounding, not bit for bit):
+Tolerances (FP64 on both sides; the kernels contract multiply-adds into FMA,
+multiply by precomputed pivot reciprocals where the reference divides, and
+sum the FFTs in another order, so results agree to rounding, not bit for
+bit):
   - each routine of one substep (clcRhsXYZ, the Helmholtz solves, clcPrSrc,
     clcPPE, the projection): relative max error <= 1e-11
   - Poisson solve: <= 1e-12 (relative to max|phi|)

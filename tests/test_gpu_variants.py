@@ -1,0 +1,81 @@
+"""Parity of the alternative kernel variants that size selects automatically.
+
+The spectral y-solve has a staged variant (whole column strips copied to
+shared memory first) and a streaming variant (rows streamed from HBM), chosen
+by grid size; the Poisson transforms have compile-time-length kernels and a
+generic Stockham path for lengths outside their list.  The small grids of
+the other tests reach only one variant of each, so here every variant is
+forced through the environment (read when a context is created) and
+compared with the oracle.  Tolerances as in test_gpu_parity.
+"""
+import pytest
+
+from oracle import oracle_lib as ol
+from paratc_b200 import cases
+from paratc_b200.lib import ChannelSystem
+
+from .helpers import fields_of, rel_err, variant, yp_of
+
+pytestmark = pytest.mark.gpu
+
+TOL_STEP1 = 1e-10
+TOL_STEPS = 1e-8
+TOL_POISSON = 1e-12
+
+
+def _steps_vs_oracle(case, nsteps):
+    yp = yp_of(case)
+    f = fields_of(case, yp)
+    o = ol.Oracle(case.params, yp)
+    g = ChannelSystem(case.params, yp)
+    o.set_fields(f["ux"], f["uy"], f["uz"], f["p"], f["c"])
+    g.set_fields(f["ux"], f["uy"], f["uz"], f["p"], f["c"])
+    for s in range(nsteps):
+        rc, _ = o.step()
+        assert rc == 0
+        g.iterate(1, raise_on_guard=False)
+        fo, fg = o.get_fields(), g.get_fields()
+        tol = TOL_STEP1 if s == 0 else TOL_STEPS
+        for n in ("ux", "uy", "uz", "p", "c"):
+            if fo.get(n) is None:
+                continue
+            e = rel_err(fg[n], fo[n])
+            assert e <= tol, "%s step %d: %s rel err %.3e" % (case.name, s + 1, n, e)
+
+
+@pytest.mark.parametrize("solver", ["staged", "streaming"])
+@pytest.mark.parametrize("name", ["channel", "halfchannel_scalar"])
+def test_solver_variants_steps(monkeypatch, solver, name):
+    monkeypatch.setenv("PARATC_YSOLVER", solver)
+    _steps_vs_oracle(variant(name), 3)
+
+
+@pytest.mark.parametrize("solver", [None, "staged", "streaming"])
+def test_tall_columns(monkeypatch, solver):
+    """A tall grid (ny = 120): long dependent chains in every y-solve."""
+    if solver:
+        monkeypatch.setenv("PARATC_YSOLVER", solver)
+    _steps_vs_oracle(cases.small_channel(16, 120, 8), 2)
+
+
+@pytest.mark.parametrize("dims", [(24, 20, 30), (32, 24, 16)])
+def test_generic_fft_path(monkeypatch, dims):
+    monkeypatch.setenv("PARATC_GENERIC_FFT", "1")
+    _steps_vs_oracle(cases.small_channel(*dims), 2)
+    case = cases.small_channel(*dims)
+    yp = yp_of(case)
+    src = cases.gaussian_source(cases.Case("src", case.params, case.mesh, "gauss_src", 42, 1.0))
+    phi_o = ol.Oracle(case.params, yp).poisson(src)
+    phi_g = ChannelSystem(case.params, yp).poisson(src)
+    assert rel_err(phi_g, phi_o) <= TOL_POISSON
+
+
+@pytest.mark.parametrize("dims", [(48, 16, 24), (96, 12, 40), (80, 10, 64)])
+def test_fixed_length_sizes(dims):
+    """Other compile-time lengths (nx/2 = 24, 48, 40; nz = 24, 40, 64)."""
+    case = cases.small_channel(*dims)
+    yp = yp_of(case)
+    src = cases.gaussian_source(cases.Case("src", case.params, case.mesh, "gauss_src", 7, 1.0))
+    phi_o = ol.Oracle(case.params, yp).poisson(src)
+    phi_g = ChannelSystem(case.params, yp).poisson(src)
+    assert rel_err(phi_g, phi_o) <= TOL_POISSON
