@@ -56,6 +56,7 @@ struct paratc_ctx {
     unsigned int* d_counter = nullptr;  // grid-completion counters of the last-block reductions
     double* d_hfac = nullptr;           // Helmholtz pivots of the substeps of a step (3 matrix types each)
     double hfac_dt = -1.0;              // the fixed dt d_hfac holds pivots for (iCFL != 1), else < 0
+    bool next_ready = false;            // the last step's end kernel already computed this step's dt
     DDiag* h_diag = nullptr;   // pinned
     DCoef* h_coef = nullptr;   // pinned
     double* h_scal = nullptr;  // pinned
@@ -227,7 +228,11 @@ void enqueue_substep(paratc_ctx* ctx, int ns, int stop = 5) {
 }
 
 void enqueue_step(paratc_ctx* ctx) {
-    { PROF(PK_CFL); launch_cfl(ctx->st, ctx->kc, ctx->dm, ctx->f, ctx->d_coef, ctx->d_part); }
+    // clcCFL: done by the previous step's end kernel unless the state changed since
+    if (!ctx->next_ready) {
+        { PROF(PK_CFL); launch_cfl(ctx->st, ctx->kc, ctx->dm, ctx->f, ctx->d_coef, ctx->d_part); }
+        ctx->launches += 2;
+    }
     // with a fixed time step (iCFL != 1) the Helmholtz matrices never change:
     // their pivots are computed once and kept
     if (ctx->prm.icfl == 1 || ctx->hfac_dt != ctx->prm.dt_max) {
@@ -235,10 +240,10 @@ void enqueue_step(paratc_ctx* ctx) {
         ctx->launches += 1;
         ctx->hfac_dt = (ctx->prm.icfl == 1) ? -1.0 : ctx->prm.dt_max;
     }
-    ctx->launches += 2;
     for (int ns = 1; ns <= ctx->hm.iadvance; ns++) enqueue_substep(ctx, ns);
-    { PROF(PK_CHECK); launch_check(ctx->st, ctx->kc, ctx->dm, ctx->f, ctx->d_coef, ctx->d_diag, ctx->d_part); }
-    ctx->launches += 2;
+    { PROF(PK_CHECK); launch_endstep(ctx->st, ctx->kc, ctx->dm, ctx->f, ctx->d_coef, ctx->d_diag, ctx->d_part, ctx->d_counter + 3, 1); }
+    ctx->next_ready = true;
+    ctx->launches += 1;
 }
 
 void diag_out(const DDiag& d, paratc_diag* o) {
@@ -451,8 +456,11 @@ int paratc_create(const paratc_params* prm, const double* yp, int device, paratc
         for (double** p : fs)
             if ((rc = dalloc(ctx, p, nf)) != PARATC_OK) { paratc_destroy(ctx); return rc; }
     }
-    ctx->npart = std::max(std::max(cell_grid_blocks(kc) * 7, rhs_grid_blocks(kc)),
-                          (size_t)pfft_x_blocks(ctx->nx, ctx->ny, ctx->nz)) + 64;
+    // partial-result records of the grid reductions: one per block of k_prsrc /
+    // k_cfl, one per block of the RHS and forward-x kernels, 8 per block of the
+    // end-of-step kernel
+    ctx->npart = std::max(std::max(cell_grid_blocks(kc), rhs_grid_blocks(kc)),
+                          std::max((size_t)pfft_x_blocks(ctx->nx, ctx->ny, ctx->nz), endstep_blocks(kc) * 8)) + 64;
     if ((rc = dalloc(ctx, &ctx->d_src, ctx->ni)) || (rc = dalloc(ctx, &ctx->d_spec, (size_t)ctx->M1 * ctx->ny * ctx->nz)) ||
         (rc = dalloc(ctx, &ctx->d_part, ctx->npart)) || (rc = dalloc(ctx, &ctx->d_uy_ym, (size_t)ctx->nx * ctx->nz)) ||
         (rc = dalloc(ctx, &ctx->d_duy_ym, (size_t)ctx->nx * ctx->nz)) || (rc = dalloc(ctx, &ctx->d_coef, 1)) ||
@@ -522,6 +530,7 @@ int paratc_set_fields(paratc_ctx* ctx, const double* ux, const double* uy, const
                       const double* c, const double* hx, const double* hy, const double* hz, const double* hc, int layout) {
     if (!ctx || (layout != PARATC_LAYOUT_INTERIOR && layout != PARATC_LAYOUT_HALO)) return PARATC_ERR_BAD_ARG;
     CK(cudaSetDevice(ctx->dev));
+    ctx->next_ready = false;
     struct { double* d; const double* h; bool hist; } tab[] = {
         {ctx->f.ux, ux, false}, {ctx->f.uy, uy, false}, {ctx->f.uz, uz, false}, {ctx->f.pr, p, false},
         {ctx->f.sc, c, false}, {ctx->f.hx, hx, true}, {ctx->f.hy, hy, true}, {ctx->f.hz, hz, true}, {ctx->f.hc, hc, true}};
@@ -569,6 +578,7 @@ int paratc_set_time(paratc_ctx* ctx, double sim_time, double dt) {
     if (rc) return rc;
     ctx->h_coef->sim_time = sim_time;
     ctx->h_coef->dt = dt;
+    ctx->next_ready = false;
     CK(cudaMemcpyAsync(ctx->d_coef, ctx->h_coef, sizeof(DCoef), cudaMemcpyHostToDevice, ctx->st));
     return sync(ctx);
 }
@@ -580,7 +590,8 @@ int paratc_get_time(paratc_ctx* ctx, double* sim_time, double* dt) {
     int rc = sync(ctx);
     if (rc) return rc;
     if (sim_time) *sim_time = ctx->h_coef->sim_time;
-    if (dt) *dt = ctx->h_coef->dt;
+    // after a step the device already holds the next step's dt; report the last one
+    if (dt) *dt = ctx->next_ready ? ctx->h_coef->dt_last : ctx->h_coef->dt;
     return PARATC_OK;
 }
 
@@ -638,6 +649,7 @@ int paratc_substep(paratc_ctx* ctx, int ns, double dt, double* divmax_src) {
 int paratc_substep_stage(paratc_ctx* ctx, int ns, double dt, int stop_stage, double* divmax_src) {
     if (!ctx || ns < 1 || ns > ctx->hm.iadvance || stop_stage < 1 || stop_stage > 5) return PARATC_ERR_BAD_ARG;
     CK(cudaSetDevice(ctx->dev));
+    ctx->next_ready = false;
     CK(cudaMemcpyAsync(ctx->h_coef, ctx->d_coef, sizeof(DCoef), cudaMemcpyDeviceToHost, ctx->st));
     int rc = sync(ctx);
     if (rc) return rc;
@@ -697,6 +709,7 @@ int paratc_poisson(paratc_ctx* ctx, const double* src, double* phi) {
 int paratc_project(paratc_ctx* ctx, double* divmax_out) {
     if (!ctx) return PARATC_ERR_BAD_ARG;
     CK(cudaSetDevice(ctx->dev));
+    ctx->next_ready = false;
     launch_bc_all(ctx->st, ctx->kc, ctx->f, ctx->d_uy_ym);
     enqueue_poisson_head(ctx, 1, nullptr, ctx->d_scal);
     enqueue_poisson_tail(ctx, ctx->d_phi, 1);
@@ -714,8 +727,8 @@ int paratc_diagnostics(paratc_ctx* ctx, paratc_diag* diag) {
     if (!ctx || !diag) return PARATC_ERR_BAD_ARG;
     CK(cudaSetDevice(ctx->dev));
     CK(cudaMemsetAsync(ctx->d_diag2, 0, sizeof(DDiag), ctx->st));
-    launch_check(ctx->st, ctx->kc, ctx->dm, ctx->f, ctx->d_coef, ctx->d_diag2, ctx->d_part);
-    ctx->launches += 2;
+    launch_endstep(ctx->st, ctx->kc, ctx->dm, ctx->f, ctx->d_coef, ctx->d_diag2, ctx->d_part, ctx->d_counter + 3, 0);
+    ctx->launches += 1;
     CK(cudaMemcpyAsync(ctx->h_diag, ctx->d_diag2, sizeof(DDiag), cudaMemcpyDeviceToHost, ctx->st));
     int rc = sync(ctx);
     if (rc) return rc;

@@ -53,6 +53,7 @@ struct DCoef {
     double rhsx_add;        // -dp1ns (no scalar) or +dp1ns (scalar) of the flow-rate constraint
     double sim_time, pr_grad_aver, cflmp;
     double divmax_src;
+    double dt_last;         // dt of the last completed step, once dt holds the next step's
     int ns, pad;
 };
 

@@ -184,70 +184,92 @@ __global__ void k_cfl_final(DConst c, DCoef* coef, const double* __restrict__ pa
 }
 
 // ---------------------------------------------------------------------------
-// end-of-step checks: CheckDivergence, CalcVmax, CalcUxAver / ClcMeanValue
-// (src/m_Tools.f90:54-110,256-301); per block: 4 maxima + 3 sums
+// End of a step, one pass over the velocity: CheckDivergence, CalcVmax,
+// CalcUxAver / ClcMeanValue (src/m_Tools.f90:54-110,256-301) for the step's
+// diagnostics and guards, and (next != 0) clcCFL (src/m_TScheme.f90:20-46)
+// of the step that follows, which reads the same velocity.  A warp takes whole
+// x rows (grid-stride over the (k, jc) rows, one wave of CTAs); every CTA
+// stores one record of 5 maxima and 3 sums and the last CTA to finish reduces
+// the records in index order.  It first fills the diagnostics from this
+// step's dt and CFL number, then writes the next step's: cflmp = uddxmax*dt
+// with the dt just used, dt = min(cflc/uddxmax, dt_max) for iCFL = 1 (or
+// dt_max), exactly as clcCFL would at the start of the next step.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_check(DConst c, DMetric m, const double* __restrict__ ux,
-                                               const double* __restrict__ uy, const double* __restrict__ uz,
-                                               const double* __restrict__ sc, double* __restrict__ part) {
-    const int nx = c.nx;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int jc = blockIdx.y * blockDim.y + threadIdx.y + 1;
-    const int k = blockIdx.z;
-    double mx[4] = {0.0, 0.0, 0.0, 0.0};
+constexpr int ENDSTEP_THREADS = 256;
+
+__global__ void __launch_bounds__(ENDSTEP_THREADS)
+    k_endstep(DConst c, DMetric m, const double* __restrict__ ux, const double* __restrict__ uy,
+              const double* __restrict__ uz, const double* __restrict__ sc, DCoef* __restrict__ coef,
+              DDiag* __restrict__ diag, double* __restrict__ part, unsigned int* __restrict__ counter, int next) {
+    const int nx = c.nx, ny = c.ny, nz = c.nz;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int nwarps = gridDim.x * (ENDSTEP_THREADS / 32);
+    const size_t pl = (size_t)c.nyt * nx;
+    double mx[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
     double sm[3] = {0.0, 0.0, 0.0};
-    if (i < nx && jc <= c.ny) {
-        const size_t pl = (size_t)c.nyt * nx, zc = (size_t)k * pl, r0 = (size_t)jc * nx;
-        const size_t q = zc + r0 + i;
-        const int im = wrapi(i - 1, nx), ip = wrapi(i + 1, nx), iu = wrapi(i + 2, nx);
-        const size_t zm = (size_t)wrapi(k - 1, c.nz) * pl, zp = (size_t)wrapi(k + 1, c.nz) * pl, zu = (size_t)wrapi(k + 2, c.nz) * pl;
-        const double dudx = c.dxC[0] * LD(ux, zc + r0 + im) + c.dxC[1] * LD(ux, q) + c.dxC[2] * LD(ux, zc + r0 + ip) + c.dxC[3] * LD(ux, zc + r0 + iu);
-        const double dvdy = (LD(uy, q + nx) - LD(uy, q)) * __ldg(&m.rdyp[jc]);
-        const double dwdz = c.dzC[0] * LD(uz, zm + r0 + i) + c.dzC[1] * LD(uz, q) + c.dzC[2] * LD(uz, zp + r0 + i) + c.dzC[3] * LD(uz, zu + r0 + i);
-        mx[0] = fabs(dudx + dvdy + dwdz);
-        const double u = LD(ux, q);
-        mx[1] = fabs(u);
-        mx[2] = fabs(LD(uy, q));
-        mx[3] = fabs(LD(uz, q));
-        const double dy = __ldg(&m.dyp[jc]);
-        sm[0] = u * dy;
-        if (c.scalar_on) {
-            const double s = LD(sc, q);
-            sm[1] = dy * s;
-            sm[2] = dy * s * s;
+    for (int r = blockIdx.x * (ENDSTEP_THREADS / 32) + warp; r < ny * nz; r += nwarps) {
+        const int k = r / ny, jc = r - k * ny + 1;
+        const int km = k == 0 ? nz - 1 : k - 1, kp = k == nz - 1 ? 0 : k + 1, ku = kp == nz - 1 ? 0 : kp + 1;
+        const size_t r0 = (size_t)jc * nx;
+        const double* ur = ux + (size_t)k * pl + r0;
+        const double* vr = uy + (size_t)k * pl + r0;
+        const double* w1 = uz + (size_t)k * pl + r0;
+        const double* w0 = uz + (size_t)km * pl + r0;
+        const double* w2 = uz + (size_t)kp * pl + r0;
+        const double* w3 = uz + (size_t)ku * pl + r0;
+        const double rdyp = __ldg(&m.rdyp[jc]), dy = __ldg(&m.dyp[jc]);
+        for (int i = lane; i < nx; i += 32) {
+            const int im = i == 0 ? nx - 1 : i - 1, ip = i == nx - 1 ? 0 : i + 1, iu = ip == nx - 1 ? 0 : ip + 1;
+            const double u0 = __ldg(&ur[i]), up = __ldg(&ur[ip]);
+            const double v0 = __ldg(&vr[i]), vp = __ldg(&vr[nx + i]);
+            const double z1 = __ldg(&w1[i]), z2 = __ldg(&w2[i]);
+            const double dudx = c.dxC[0] * __ldg(&ur[im]) + c.dxC[1] * u0 + c.dxC[2] * up + c.dxC[3] * __ldg(&ur[iu]);
+            const double dvdy = (vp - v0) * rdyp;
+            const double dwdz = c.dzC[0] * __ldg(&w0[i]) + c.dzC[1] * z1 + c.dzC[2] * z2 + c.dzC[3] * __ldg(&w3[i]);
+            mx[0] = fmax(mx[0], fabs(dudx + dvdy + dwdz));
+            mx[1] = fmax(mx[1], fabs(u0));
+            mx[2] = fmax(mx[2], fabs(v0));
+            mx[3] = fmax(mx[3], fabs(z1));
+            if (next)
+                mx[4] = fmax(mx[4], fabs(u0 + up) * c.rdx + fabs(v0 + vp) * rdyp + fabs(z1 + z2) * c.rdz);
+            sm[0] += u0 * dy;
+            if (c.scalar_on) {
+                const double s = __ldg(&sc[(size_t)k * pl + r0 + i]);
+                sm[1] += dy * s;
+                sm[2] += dy * s * s;
+            }
         }
     }
-    const int bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
-    block_max_store<4>(mx, part + (size_t)bid * 7);
+    block_max_store<5>(mx, part + (size_t)blockIdx.x * 8);
     __syncthreads();
-    block_sum_store<3>(sm, part + (size_t)bid * 7 + 4);
-}
-
-__global__ void k_check_final(DConst c, const DCoef* __restrict__ coef, DDiag* __restrict__ diag,
-                              const double* __restrict__ part, int nparts) {
-    // maxima and sums are interleaved per block: reduce in two passes
-    __shared__ double sh[32][7];
-    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nw = (blockDim.x + 31) >> 5;
-    double v[7] = {0, 0, 0, 0, 0, 0, 0};
-    for (int b = tid; b < nparts; b += blockDim.x) {
-        const double* p = part + (size_t)b * 7;
-        for (int q = 0; q < 4; q++) v[q] = fmax(v[q], p[q]);
-        for (int q = 4; q < 7; q++) v[q] += p[q];
+    block_sum_store<3>(sm, part + (size_t)blockIdx.x * 8 + 5);
+    if (!last_block_arrive(counter, gridDim.x)) return;
+    // the last CTA: records in index order, thread t takes records t, t+256, ...
+    __shared__ double sh[ENDSTEP_THREADS / 32][8];
+    double v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (int b = threadIdx.x; b < (int)gridDim.x; b += ENDSTEP_THREADS) {
+        const double* p = part + (size_t)b * 8;
+#pragma unroll
+        for (int q = 0; q < 5; q++) v[q] = fmax(v[q], __ldcg(&p[q]));
+#pragma unroll
+        for (int q = 5; q < 8; q++) v[q] += __ldcg(&p[q]);
     }
-    for (int q = 0; q < 7; q++)
+#pragma unroll
+    for (int q = 0; q < 8; q++)
         for (int o = 16; o > 0; o >>= 1) {
-            double y = __shfl_down_sync(0xffffffffu, v[q], o);
-            v[q] = q < 4 ? fmax(v[q], y) : v[q] + y;
+            const double y = __shfl_down_sync(0xffffffffu, v[q], o);
+            v[q] = q < 5 ? fmax(v[q], y) : v[q] + y;
         }
     if (lane == 0)
-        for (int q = 0; q < 7; q++) sh[wid][q] = v[q];
+#pragma unroll
+        for (int q = 0; q < 8; q++) sh[warp][q] = v[q];
     __syncthreads();
-    if (tid != 0) return;
-    double r[7] = {0, 0, 0, 0, 0, 0, 0};
-    for (int w = 0; w < nw; w++)
-        for (int q = 0; q < 7; q++) r[q] = q < 4 ? fmax(r[q], sh[w][q]) : r[q] + sh[w][q];
+    if (threadIdx.x != 0) return;
+    double r[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (int w = 0; w < ENDSTEP_THREADS / 32; w++)
+        for (int q = 0; q < 8; q++) r[q] = q < 5 ? fmax(r[q], sh[w][q]) : r[q] + sh[w][q];
     DDiag d = *diag;
-    const DCoef f = *coef;
+    DCoef f = *coef;
     d.step_counter += 1;
     d.dt = f.dt;
     d.cfl = f.cflmp;
@@ -257,9 +279,9 @@ __global__ void k_check_final(DConst c, const DCoef* __restrict__ coef, DDiag* _
     d.vmax[0] = r[1]; d.vmax[1] = r[2]; d.vmax[2] = r[3];
     d.pr_grad_aver = f.pr_grad_aver;
     const double nxz = (double)(c.nx * c.nz);
-    d.ux_mean = r[4] / nxz / c.yly;
-    d.sc_mean = r[5] / nxz / c.yly;
-    d.sc2_mean = r[6] / nxz / c.yly;
+    d.ux_mean = r[5] / nxz / c.yly;
+    d.sc_mean = r[6] / nxz / c.yly;
+    d.sc2_mean = r[7] / nxz / c.yly;
     if (d.status == 0) {
         double vmin = fmin(fmin(r[1], r[2]), r[3]);
         if (!(r[0] == r[0]) || !(vmin == vmin)) { d.status = -4; d.failed_step = d.step_counter; }
@@ -267,6 +289,13 @@ __global__ void k_check_final(DConst c, const DCoef* __restrict__ coef, DDiag* _
         else if (vmin > c.vel_limit) { d.status = -6; d.failed_step = d.step_counter; }
     }
     *diag = d;
+    if (next) {
+        const double uddxmax = r[4] * 0.5;
+        f.dt_last = f.dt;
+        f.cflmp = uddxmax * f.dt;
+        f.dt = (c.icfl == 1) ? fmin(c.cflc / uddxmax, c.dt_max) : c.dt_max;
+        *coef = f;
+    }
 }
 
 __global__ void k_store_divsrc(DCoef* coef, const double* __restrict__ v) {
@@ -310,10 +339,12 @@ void launch_cfl(cudaStream_t st, const DConst& c, const DMetric& m, const Fields
     k_cfl_final<<<1, 1024, 0, st>>>(c, coef, part, (int)cell_grid_blocks(c));
 }
 
-void launch_check(cudaStream_t st, const DConst& c, const DMetric& m, const Fields& f, const DCoef* coef, DDiag* diag,
-                  double* part) {
-    k_check<<<cell_grid(c), cell_block(), 0, st>>>(c, m, f.ux, f.uy, f.uz, f.sc, part);
-    k_check_final<<<1, 1024, 0, st>>>(c, coef, diag, part, (int)cell_grid_blocks(c));
+size_t endstep_blocks(const DConst& c) { return (size_t)2 * (c.nsm > 0 ? c.nsm : 148); }
+
+void launch_endstep(cudaStream_t st, const DConst& c, const DMetric& m, const Fields& f, DCoef* coef, DDiag* diag,
+                    double* part, unsigned int* counter, int next) {
+    k_endstep<<<(unsigned)endstep_blocks(c), ENDSTEP_THREADS, 0, st>>>(c, m, f.ux, f.uy, f.uz, f.sc, coef, diag, part,
+                                                                       counter, next);
 }
 
 }  // namespace ptc

@@ -20,8 +20,9 @@ void launch_project(cudaStream_t st, const DConst& c, const DMetric& m, const DC
 void launch_bc_all(cudaStream_t st, const DConst& c, const Fields& f, const double* uy_ym);
 void launch_update_uy_ym(cudaStream_t st, int n, double* uy_ym, double* duy_ym);
 void launch_cfl(cudaStream_t st, const DConst& c, const DMetric& m, const Fields& f, DCoef* coef, double* part);
-void launch_check(cudaStream_t st, const DConst& c, const DMetric& m, const Fields& f, const DCoef* coef, DDiag* diag,
-                  double* part);
+size_t endstep_blocks(const DConst& c);
+void launch_endstep(cudaStream_t st, const DConst& c, const DMetric& m, const Fields& f, DCoef* coef, DDiag* diag,
+                    double* part, unsigned int* counter, int next);
 
 // k_rhs.cu
 size_t rhs_grid_blocks(const DConst& c);
