@@ -196,8 +196,9 @@ __global__ void k_cfl_final(DConst c, DCoef* coef, const double* __restrict__ pa
 // dt_max), exactly as clcCFL would at the start of the next step.
 // ---------------------------------------------------------------------------
 constexpr int ENDSTEP_THREADS = 256;
+constexpr int ENDSTEP_U = 4;
 
-__global__ void __launch_bounds__(ENDSTEP_THREADS)
+__global__ void __launch_bounds__(ENDSTEP_THREADS, 2)
     k_endstep(DConst c, DMetric m, const double* __restrict__ ux, const double* __restrict__ uy,
               const double* __restrict__ uz, const double* __restrict__ sc, DCoef* __restrict__ coef,
               DDiag* __restrict__ diag, double* __restrict__ part, unsigned int* __restrict__ counter, int next) {
@@ -218,25 +219,37 @@ __global__ void __launch_bounds__(ENDSTEP_THREADS)
         const double* w2 = uz + (size_t)kp * pl + r0;
         const double* w3 = uz + (size_t)ku * pl + r0;
         const double rdyp = __ldg(&m.rdyp[jc]), dy = __ldg(&m.dyp[jc]);
-        for (int i = lane; i < nx; i += 32) {
-            const int im = i == 0 ? nx - 1 : i - 1, ip = i == nx - 1 ? 0 : i + 1, iu = ip == nx - 1 ? 0 : ip + 1;
-            const double u0 = __ldg(&ur[i]), up = __ldg(&ur[ip]);
-            const double v0 = __ldg(&vr[i]), vp = __ldg(&vr[nx + i]);
-            const double z1 = __ldg(&w1[i]), z2 = __ldg(&w2[i]);
-            const double dudx = c.dxC[0] * __ldg(&ur[im]) + c.dxC[1] * u0 + c.dxC[2] * up + c.dxC[3] * __ldg(&ur[iu]);
-            const double dvdy = (vp - v0) * rdyp;
-            const double dwdz = c.dzC[0] * __ldg(&w0[i]) + c.dzC[1] * z1 + c.dzC[2] * z2 + c.dzC[3] * __ldg(&w3[i]);
-            mx[0] = fmax(mx[0], fabs(dudx + dvdy + dwdz));
-            mx[1] = fmax(mx[1], fabs(u0));
-            mx[2] = fmax(mx[2], fabs(v0));
-            mx[3] = fmax(mx[3], fabs(z1));
-            if (next)
-                mx[4] = fmax(mx[4], fabs(u0 + up) * c.rdx + fabs(v0 + vp) * rdyp + fabs(z1 + z2) * c.rdz);
-            sm[0] += u0 * dy;
-            if (c.scalar_on) {
-                const double s = __ldg(&sc[(size_t)k * pl + r0 + i]);
-                sm[1] += dy * s;
-                sm[2] += dy * s * s;
+        // ENDSTEP_U cells per lane with every load issued before the arithmetic
+        for (int i0 = 0; i0 < nx; i0 += 32 * ENDSTEP_U) {
+            double a[ENDSTEP_U][11];
+#pragma unroll
+            for (int u = 0; u < ENDSTEP_U; u++) {
+                const int i = min(i0 + lane + 32 * u, nx - 1);
+                const int im = i == 0 ? nx - 1 : i - 1, ip = i == nx - 1 ? 0 : i + 1, iu = ip == nx - 1 ? 0 : ip + 1;
+                a[u][0] = __ldg(&ur[im]); a[u][1] = __ldg(&ur[i]); a[u][2] = __ldg(&ur[ip]); a[u][3] = __ldg(&ur[iu]);
+                a[u][4] = __ldg(&vr[i]); a[u][5] = __ldg(&vr[nx + i]);
+                a[u][6] = __ldg(&w0[i]); a[u][7] = __ldg(&w1[i]); a[u][8] = __ldg(&w2[i]); a[u][9] = __ldg(&w3[i]);
+                a[u][10] = c.scalar_on ? __ldg(&sc[(size_t)k * pl + r0 + i]) : 0.0;
+            }
+#pragma unroll
+            for (int u = 0; u < ENDSTEP_U; u++) {
+                if (i0 + lane + 32 * u >= nx) continue;
+                const double u0 = a[u][1], up = a[u][2], v0 = a[u][4], vp = a[u][5], z1 = a[u][7], z2 = a[u][8];
+                const double dudx = c.dxC[0] * a[u][0] + c.dxC[1] * u0 + c.dxC[2] * up + c.dxC[3] * a[u][3];
+                const double dvdy = (vp - v0) * rdyp;
+                const double dwdz = c.dzC[0] * a[u][6] + c.dzC[1] * z1 + c.dzC[2] * z2 + c.dzC[3] * a[u][9];
+                mx[0] = fmax(mx[0], fabs(dudx + dvdy + dwdz));
+                mx[1] = fmax(mx[1], fabs(u0));
+                mx[2] = fmax(mx[2], fabs(v0));
+                mx[3] = fmax(mx[3], fabs(z1));
+                if (next)
+                    mx[4] = fmax(mx[4], fabs(u0 + up) * c.rdx + fabs(v0 + vp) * rdyp + fabs(z1 + z2) * c.rdz);
+                sm[0] += u0 * dy;
+                if (c.scalar_on) {
+                    const double s = a[u][10];
+                    sm[1] += dy * s;
+                    sm[2] += dy * s * s;
+                }
             }
         }
     }
