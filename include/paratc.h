@@ -175,7 +175,10 @@ int paratc_get_fields_device(paratc_ctx* ctx, double* ux, double* uy, double* uz
                              double* p, double* c, double* hx, double* hy,
                              double* hz, double* hc);
 
-/* SimTime, dt and PrGradAver of the context (m_Parameters globals). */
+/* SimTime and dt of the context (m_Parameters globals).  After a step,
+ * paratc_get_time reports the dt that step used (the device already holds
+ * the next step's dt, computed from the same velocity by the step's end
+ * kernel).  paratc_set_time makes the next step recompute its CFL. */
 int paratc_set_time(paratc_ctx* ctx, double sim_time, double dt);
 int paratc_get_time(paratc_ctx* ctx, double* sim_time, double* dt);
 
@@ -211,7 +214,11 @@ int paratc_substep_stage(paratc_ctx* ctx, int ns, double dt, int stop_stage,
                          double* divmax_src);
 
 /* Inspection: copies a work array in interior layout to host memory:
- * 0 RhsX (with the flow-rate term), 1 RhsY, 2 RhsZ, 3 RhsC, 4 prsrc, 5 phi. */
+ * 0 RhsX (with the flow-rate term), 1 RhsY, 2 RhsZ, 3 RhsC, 4 prsrc, 5 phi.
+ * The Rhs arrays hold the right-hand sides after a substep stopped at stage 1
+ * (the Helmholtz forward sweep overwrites them, as InverseTridiagonal
+ * overwrites its right-hand side in the reference); prsrc is filled by a
+ * substep stopped at stage 3. */
 int paratc_get_work(paratc_ctx* ctx, int which, double* out);
 
 /* clcPPE (src/m_Poisson.f90:352-452, choice 1 on one rank): solves
