@@ -24,6 +24,11 @@
 
 using namespace ptc;
 
+bool ptc::pdl_enabled() {
+    static const bool on = std::getenv("PARATC_NO_PDL") == nullptr;
+    return on;
+}
+
 // kernel classes of the per-kernel timer
 enum ProfK {
     PK_COEF = 0, PK_UYYM, PK_RHS, PK_FLOWRATE, PK_HELM, PK_HELM_SC, PK_PRSRC, PK_FFTX_F, PK_FFTZ_F, PK_YSOLVE,

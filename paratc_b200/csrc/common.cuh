@@ -73,6 +73,15 @@ struct FftPlan {
     unsigned long long code;  // the radices again, 4 bits each (pass s at bits 4s..4s+3)
 };
 
+// Programmatic dependent launch: a kernel launched with launch_pdl may start
+// while its predecessor in the stream drains; pdl_wait() blocks until the
+// predecessor grid has completed and its memory is visible, so every read of
+// data an earlier kernel produced, and every global write, comes after it.
+// pdl_trigger() lets the successor launch now.  Both are no-ops when the
+// launch carried no programmatic attribute.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 __device__ __forceinline__ int wrapi(int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); }
 
 __device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }

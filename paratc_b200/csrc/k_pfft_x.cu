@@ -57,6 +57,8 @@ __global__ void __launch_bounds__(XK<N>::P)
     const int nx = 2 * N, ny = c.ny, nz = c.nz, nrows = ny * nz;
     const int g0 = blockIdx.x * B;
     for (int t = tid; t < N; t += P) tws[t] = twN[t];
+    pdl_wait();
+    pdl_trigger();
     double dm = 0.0;
     if (mode == 2) {
         for (int f = tid; f < B * N; f += P) {
@@ -138,6 +140,8 @@ __global__ void __launch_bounds__(XK<N>::P)
     const int nx = 2 * N, nrows = ny * nz;
     const int g0 = blockIdx.x * B;
     for (int t = tid; t < N; t += P) tws[t] = twN[t];
+    pdl_wait();
+    pdl_trigger();
     for (int f = tid; f < B * M1; f += P) {
         const int b = f / M1, a = f - b * M1;
         if (g0 + b < nrows) cpa16(&buf[a * PITCH + b], spec + (size_t)g0 * M1 + f);
@@ -229,8 +233,8 @@ void launch_pfft_xf(cudaStream_t st, int mode, const DConst& c, const DMetric& m
     switch (c.nx / 2) {
 #define X_CASE(n)                                                                                              \
     case n:                                                                                                    \
-        k_xf<n><<<(nrows + XK<n>::B - 1) / XK<n>::B, XK<n>::P, XK<n>::smem, st>>>(                             \
-            mode, c, m, coef, f.ux, f.uy, f.uz, src, spec, twx, post, part, counter, out_max);                 \
+        launch_pdl(k_xf<n>, dim3((nrows + XK<n>::B - 1) / XK<n>::B), dim3(XK<n>::P), XK<n>::smem, st, mode, c, m, \
+                   coef, f.ux, f.uy, f.uz, src, spec, twx, post, part, counter, out_max);                      \
         break;
         PFFT_X_SIZES(X_CASE)
 #undef X_CASE
@@ -244,8 +248,8 @@ void launch_pfft_xb(cudaStream_t st, int nx, int ny, int nz, const double2* spec
     switch (nx / 2) {
 #define X_CASE(n)                                                                                              \
     case n:                                                                                                    \
-        k_xb<n><<<(nrows + XK<n>::B - 1) / XK<n>::B, XK<n>::P, XK<n>::smem, st>>>(ny, nz, spec, phi, twx,      \
-                                                                                  post, scale, padded);        \
+        launch_pdl(k_xb<n>, dim3((nrows + XK<n>::B - 1) / XK<n>::B), dim3(XK<n>::P), XK<n>::smem, st, ny, nz,    \
+                   spec, phi, twx, post, scale, padded);                                                       \
         break;
         PFFT_X_SIZES(X_CASE)
 #undef X_CASE

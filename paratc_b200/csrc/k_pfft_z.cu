@@ -53,9 +53,13 @@ __global__ void __launch_bounds__(ZK<N>::P) k_zt(int ncol, double2* __restrict__
     const GLd gl{spec + q0, ncol, nvalid};
     const GSt gs{spec + q0, ncol, nvalid};
     if constexpr (SC.np == 1) {
+        pdl_wait();
+        pdl_trigger();
         ff::pass<N, B, P, SC.r[0], 1, DIR, false>(gl, gs, tws, tid);
     } else {
         for (int t = tid; t < N; t += P) tws[t] = twN[t];
+        pdl_wait();
+        pdl_trigger();
         ff::pass<N, B, P, SC.r[0], 1, DIR, false>(gl, ff::SmemSt<B>{buf}, tws, tid);
         __syncthreads();
         ff::smem_passes<N, B, B, P, DIR, 1, SC.np - 1>(buf, tws, tid);
@@ -93,8 +97,8 @@ void launch_pfft_z(cudaStream_t st, int dir, int nx, int ny, int nz, double2* sp
 #define Z_CASE(n)                                                                                              \
     case n: {                                                                                                  \
         const int grid = (ncol + ZK<n>::B - 1) / ZK<n>::B;                                                     \
-        if (dir < 0) k_zt<n, -1><<<grid, ZK<n>::P, ZK<n>::smem, st>>>(ncol, spec, twz);                        \
-        else k_zt<n, 1><<<grid, ZK<n>::P, ZK<n>::smem, st>>>(ncol, spec, twz);                                 \
+        if (dir < 0) launch_pdl(k_zt<n, -1>, dim3(grid), dim3(ZK<n>::P), ZK<n>::smem, st, ncol, spec, twz);     \
+        else launch_pdl(k_zt<n, 1>, dim3(grid), dim3(ZK<n>::P), ZK<n>::smem, st, ncol, spec, twz);              \
         break;                                                                                                 \
     }
         PFFT_Z_SIZES(Z_CASE)

@@ -64,6 +64,8 @@ __global__ void __launch_bounds__(NTHR, 2)
     const long long W = (long long)ntx * ntz * ny;
     const long long gbeg = W * blockIdx.x / gridDim.x, gend = W * (blockIdx.x + 1) / gridDim.x;
     (void)ychunk;
+    pdl_wait();
+    pdl_trigger();
 
     // PMcoeUpdate from the device dt
     const double dt = coef->dt;
@@ -337,11 +339,11 @@ void launch_rhs_tile(cudaStream_t st, const DConst& c, const DMetric& m, DCoef* 
     dim3 grd((unsigned)rhs_grid_blocks(c));
     dim3 blk(32, TZ);
     if (c.scalar_on)
-        k_rhs_tile<true><<<grd, blk, NB * 5 * SLAB * 8, st>>>(c, m, coef, f, uy_ym, duy_ym, ns, gam, the, alp, yc, part,
-                                                               counter);
+        launch_pdl(k_rhs_tile<true>, grd, blk, NB * 5 * SLAB * 8, st, c, m, coef, f, uy_ym, duy_ym, ns, gam, the, alp,
+                   yc, part, counter);
     else
-        k_rhs_tile<false><<<grd, blk, NB * 4 * SLAB * 8, st>>>(c, m, coef, f, uy_ym, duy_ym, ns, gam, the, alp, yc, part,
-                                                                counter);
+        launch_pdl(k_rhs_tile<false>, grd, blk, NB * 4 * SLAB * 8, st, c, m, coef, f, uy_ym, duy_ym, ns, gam, the, alp,
+                   yc, part, counter);
 }
 
 }  // namespace ptc

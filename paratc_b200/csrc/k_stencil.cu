@@ -67,6 +67,7 @@ __global__ void __launch_bounds__(256) k_project(DConst c, DMetric m, const DCoe
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int jc = blockIdx.y * blockDim.y + threadIdx.y + 1;
     const int k = blockIdx.z;
+    pdl_wait();
     if (i >= nx || jc > c.ny) return;
     const double alpha = mode == 0 ? coef->pmAlpha : 1.0;
     const size_t pl = (size_t)c.nyt * nx;
@@ -208,6 +209,8 @@ __global__ void __launch_bounds__(ENDSTEP_THREADS, 2)
     const size_t pl = (size_t)c.nyt * nx;
     double mx[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
     double sm[3] = {0.0, 0.0, 0.0};
+    pdl_wait();
+    pdl_trigger();
     for (int r = blockIdx.x * (ENDSTEP_THREADS / 32) + warp; r < ny * nz; r += nwarps) {
         const int k = r / ny, jc = r - k * ny + 1;
         const int km = k == 0 ? nz - 1 : k - 1, kp = k == nz - 1 ? 0 : k + 1, ku = kp == nz - 1 ? 0 : kp + 1;
@@ -336,7 +339,7 @@ void launch_store_divsrc(cudaStream_t st, DCoef* coef, const double* v) { k_stor
 
 void launch_project(cudaStream_t st, const DConst& c, const DMetric& m, const DCoef* coef, int mode, const double* phi,
                     const Fields& f, const double* uy_ym) {
-    k_project<<<cell_grid(c), cell_block(), 0, st>>>(c, m, coef, mode, phi, f.ux, f.uy, f.uz, f.pr, uy_ym);
+    launch_pdl(k_project, cell_grid(c), cell_block(), 0, st, c, m, coef, mode, phi, f.ux, f.uy, f.uz, f.pr, uy_ym);
 }
 
 void launch_bc_all(cudaStream_t st, const DConst& c, const Fields& f, const double* uy_ym) {
@@ -356,8 +359,8 @@ size_t endstep_blocks(const DConst& c) { return (size_t)2 * (c.nsm > 0 ? c.nsm :
 
 void launch_endstep(cudaStream_t st, const DConst& c, const DMetric& m, const Fields& f, DCoef* coef, DDiag* diag,
                     double* part, unsigned int* counter, int next) {
-    k_endstep<<<(unsigned)endstep_blocks(c), ENDSTEP_THREADS, 0, st>>>(c, m, f.ux, f.uy, f.uz, f.sc, coef, diag, part,
-                                                                       counter, next);
+    launch_pdl(k_endstep, dim3((unsigned)endstep_blocks(c)), dim3(ENDSTEP_THREADS), 0, st, c, m, f.ux, f.uy, f.uz,
+               f.sc, coef, diag, part, counter, next);
 }
 
 }  // namespace ptc

@@ -175,6 +175,8 @@ __global__ void __launch_bounds__(128) k_helm(DConst cst, const DCoef* __restric
     const int nx = cst.nx, ny = cst.ny;
     const int comp = comp0 + blockIdx.z;
     const int t = comp == 1 ? 1 : (comp == 3 ? 2 : 0);
+    pdl_wait();
+    pdl_trigger();
     {
         const double* F = facs + (size_t)((coef->ns - 1) * 3 + t) * helm_stride(ny);
         const int tid = threadIdx.y * 32 + threadIdx.x;
@@ -398,6 +400,8 @@ __global__ void __launch_bounds__(32) k_ys_staged(int ny, int M1, int nz, const 
     double2* sd = sy;                   // [ny][16] spectrum
     double2* sf = sy + ny * 16;         // [ny][16] factors
     double* sa = reinterpret_cast<double*>(sf + ny * 16);  // am2ph[0..ny]
+    pdl_wait();
+    pdl_trigger();
     // lane (cq, half) copies rows half, half+2, ... of complex column q0+cq
     const int cq = lane & 15, half = lane >> 4;
     const bool cval = cq < nv;
@@ -471,6 +475,8 @@ __global__ void __launch_bounds__(128) k_ys_global(int ny, int M1, int nz, const
                                                    double* __restrict__ specd, const double2* __restrict__ fac) {
     const int W = 2 * M1, NQ = M1 * nz;
     const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    pdl_wait();
+    pdl_trigger();
     if (g >= W * nz) return;
     const int kz = g / W, cr = g - kz * W, q = g >> 1;
     double* col = specd + (size_t)kz * ny * W + cr;
@@ -534,10 +540,11 @@ void launch_ysolve_fac(cudaStream_t st, const DConst& c, const DMetric& m, doubl
     const int per_sm = sm > 0 ? (int)((220 * 1024) / sm) : 0;
     const int ctas = (NQ + 15) / 16;
     if (per_sm >= 1 && (c.solver_sel == 1 || (c.solver_sel == 0 && ctas <= per_sm * c.nsm))) {
-        k_ys_staged<<<ctas, 32, sm, st>>>(c.ny, M1, c.nz, m.am2ph, spec, fac);
+        launch_pdl(k_ys_staged, dim3(ctas), dim3(32), sm, st, c.ny, M1, c.nz, m.am2ph, spec, fac);
     } else {
         const int n = 2 * M1 * c.nz;
-        k_ys_global<<<(n + 127) / 128, 128, 0, st>>>(c.ny, M1, c.nz, m.am2ph, reinterpret_cast<double*>(spec), fac);
+        launch_pdl(k_ys_global, dim3((n + 127) / 128), dim3(128), 0, st, c.ny, M1, c.nz, m.am2ph,
+                   reinterpret_cast<double*>(spec), (const double2*)fac);
     }
 }
 
@@ -585,6 +592,8 @@ __global__ void __launch_bounds__(32) k_helm_factors(DConst cst, DMetric m, cons
     for (int a = 0; a < 9; a++)
         for (int j = threadIdx.x; j < L; j += blockDim.x) shm[a * L + j] = srcs[a][j];
     __syncthreads();
+    pdl_wait();
+    pdl_trigger();
     const int q = threadIdx.x;
     if (q >= 3 * nsub) return;
     const int ns = ns0 + q / 3, t = q % 3;
@@ -620,15 +629,15 @@ __global__ void __launch_bounds__(32) k_helm_factors(DConst cst, DMetric m, cons
 
 void launch_helm_factors(cudaStream_t st, const DConst& c, const DMetric& m, const DCoef* coef, int ns0, int nsub,
                          const double* alp, double* fac) {
-    k_helm_factors<<<1, 32, (size_t)9 * (c.ny + 2) * sizeof(double), st>>>(c, m, coef, ns0, nsub, alp[0], alp[1],
-                                                                           alp[2], fac);
+    launch_pdl(k_helm_factors, dim3(1), dim3(32), (size_t)9 * (c.ny + 2) * sizeof(double), st, c, m, coef, ns0, nsub,
+               alp[0], alp[1], alp[2], fac);
 }
 
 static void helm_dispatch(cudaStream_t st, const DConst& c, const DCoef* coef, int comp0, int ncomp, const Fields& f,
                           const double* duy_ym, const double* uy_ym, const double* fac) {
     dim3 blk(32, 4);
     dim3 grd((c.nx + 127) / 128, c.nz, ncomp);
-    k_helm<<<grd, blk, helm_stride(c.ny) * sizeof(double), st>>>(c, coef, comp0, f, duy_ym, uy_ym, fac);
+    launch_pdl(k_helm, grd, blk, helm_stride(c.ny) * sizeof(double), st, c, coef, comp0, f, duy_ym, uy_ym, fac);
 }
 
 void launch_helm(cudaStream_t st, const DConst& c, const DCoef* coef, const Fields& f, const double* duy_ym,

@@ -1,8 +1,32 @@
 // kernels.cuh -- host-side launchers of the hot-path kernels.
 #pragma once
+#include <utility>
+
 #include "common.cuh"
 
 namespace ptc {
+
+// true unless the environment sets PARATC_NO_PDL (read once)
+bool pdl_enabled();
+
+// launch with programmatic stream serialization, so that the kernel's CTAs
+// can be scheduled while the previous kernel in the stream drains; the
+// kernel itself calls pdl_wait() before touching data of earlier kernels
+template <typename... KArgs, typename... Args>
+inline void launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+                       Args&&... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = pdl_enabled() ? 1 : 0;
+    cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
 
 // device pointers of the fields of one context (padded layout, see common.cuh)
 struct Fields {
