@@ -55,7 +55,7 @@ def _case(name):
         return cases.turbidity_c5()
     if name == "lock_exchange_c3":
         return cases.lock_exchange_c3()
-    raise SystemExit("unknown workload " + name)
+    raise SystemExit("unknown workload " + name + " (ensemble_c4 has its own driver)")
 
 
 def _peaks():
@@ -287,7 +287,13 @@ def run_ours(args):
     # end to end through the C ABI with host buffers (pinned)
     e2e = None
     if not args.no_e2e:
-        names = ["ux", "uy", "uz", "p", "hx", "hy", "hz"] + (["c", "hc"] if p.scalar_on else [])
+        # the state a step consumes and produces: u, v, w, p (and the scalar);
+        # the explicit histories only for AB2, whose first substep reads the
+        # previous step's (RK2/RK3 start with zeta_1 = 0, and the reference
+        # restarts them without history, src/m_IOAndVisu.f90:485)
+        names = ["ux", "uy", "uz", "p"] + (["c"] if p.scalar_on else [])
+        if p.ischeme == 1:
+            names += ["hx", "hy", "hz"] + (["hc"] if p.scalar_on else [])
         host = {n: torch.empty(ctx.shape, dtype=torch.float64, pin_memory=True).numpy() for n in names}
         cur = ctx.get_fields(names)
         for n in names:
@@ -300,8 +306,8 @@ def run_ours(args):
                 flush.add_(1.0)
             torch.cuda.synchronize()
             t0 = time.perf_counter()
-            ctx.set_fields(host["ux"], host["uy"], host["uz"], host["p"], host.get("c"), host["hx"], host["hy"],
-                           host["hz"], host.get("hc"))
+            ctx.set_fields(host["ux"], host["uy"], host["uz"], host["p"], host.get("c"), host.get("hx"), host.get("hy"),
+                           host.get("hz"), host.get("hc"))
             ctx.iterate(1)
             ctx.get_fields_into(host)
             t_e2e += time.perf_counter() - t0
@@ -311,7 +317,8 @@ def run_ours(args):
             t_e2e = float(t.item())
         e2e = {"value": ws * p.nxc * p.nyc * p.nzc * iad * args.steps / t_e2e, "unit": UNIT,
                "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes + 12 * 8,
-               "note": "per step: paratc_set_fields (state from pinned host) + paratc_step + paratc_get_fields (state to host)"}
+               "note": "per step: paratc_set_fields (%s from pinned host) + paratc_step + paratc_get_fields (same to host)"
+                       % ",".join(names)}
 
     # roofline of the dominant kernel
     peak, peak_kind = _peaks()
@@ -346,10 +353,120 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def run_ensemble(args):
+    """The C4 ensemble: 32 channel instances of uneven grids and Re_tau
+    advanced together by the batch API, every step-round one CUDA graph
+    launch; reported against the same instances stepped one after another
+    (each alone on the GPU).  The ensemble's working set (several GB) exceeds
+    the L2, so no flush is needed between timed steps."""
+    import torch
+    ws, rank, local = _dist()
+    torch.cuda.set_device(local)
+    dist = None
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    from paratc_b200 import cases
+    from paratc_b200.lib import BatchSystem, mesh_ycoord
+    cs = cases.ensemble_c4(seed=2024 + rank)
+    yps = [mesh_ycoord(c.mesh, c.params.yly) for c in cs]
+    b = BatchSystem([c.params for c in cs], yps, device=local)
+    cells = 0
+    for c, y, m in zip(cs, yps, b.members):
+        f = cases.initial_fields(c, y)
+        m.set_fields(f["ux"], f["uy"], f["uz"], f["p"], f["c"])
+        m.project()
+        cells += c.params.nxc * c.params.nyc * c.params.nzc
+    stream = torch.cuda.ExternalStream(b.stream, device=local)
+    b.iterate(args.warmup)
+    torch.cuda.synchronize()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    barrier()
+    sampler = ClockSampler(local)
+    sampler.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    diags = b.iterate(args.steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    ms = e0.elapsed_time(e1)
+    if dist is not None:
+        t = torch.tensor([ms], dtype=torch.float64, device=local)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = ws * cells * 3 * args.steps / (ms / 1e3)
+    # the same members one at a time, each alone on the GPU
+    seq_ms = 0.0
+    for m in b.members:
+        st = torch.cuda.ExternalStream(m.stream, device=local)
+        a, z = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(st)
+        m.iterate_async(args.steps)
+        z.record(st)
+        m.last_diag()
+        torch.cuda.synchronize()
+        seq_ms += a.elapsed_time(z)
+    seq_value = cells * 3 * args.steps / (seq_ms / 1e3)
+    # end to end: every member's state in from pinned host memory, one batch
+    # step, every member's state back
+    names = ["ux", "uy", "uz", "p"]
+    host = []
+    nbytes = 0
+    for c, m in zip(cs, b.members):
+        h = {n: torch.empty(m.shape, dtype=torch.float64, pin_memory=True).numpy() for n in names}
+        cur = m.get_fields(names)
+        for n in names:
+            h[n][...] = cur[n]
+            nbytes += h[n].nbytes
+        host.append(h)
+    barrier()
+    t_e2e = 0.0
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        for m, h in zip(b.members, host):
+            m.set_fields(h["ux"], h["uy"], h["uz"], h["p"])
+        b.iterate(1)
+        for m, h in zip(b.members, host):
+            m.get_fields_into(h)
+        t_e2e += time.perf_counter() - t0
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": "ensemble_c4: 32 channels, (nx,nz) in {64,96,128,192}, ny in {48,64,96,128}, "
+                                       "Re_tau U[120,395], seed 2024",
+                           "cells": cells, "precision": "fp64", "parallelism": "ensemble in one CUDA graph x%d" % ws,
+                           "l2": "working set %.1f GB > L2, no flush" % (cells * 17 * 8 / 1e9),
+                           "graph_kernels_per_step": b.graph_kernels,
+                           "divmax_last_step_max": max(d.divmax for d in diags)},
+                "sequential": {"value": seq_value, "unit": UNIT, "ms_per_step": seq_ms / args.steps,
+                               "note": "the same 32 instances stepped one after another, each alone on the GPU"},
+                "speedup_vs_sequential": value / seq_value,
+                "roofline": None, "cpu_baseline": None,
+                "e2e": {"value": ws * cells * 3 * args.steps / t_e2e, "unit": UNIT, "h2d_bytes_per_step": nbytes,
+                        "d2h_bytes_per_step": nbytes,
+                        "note": "per step: every member's u,v,w,p from pinned host + one batch step + back"},
+                "gpu_launches": b.graph_kernels * args.steps, "clocks": clocks}
+        print(json.dumps(line), flush=True)
+    b.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def main():
     args = _args()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "ensemble_c4":
+        run_ensemble(args)
     else:
         run_ours(args)
 

@@ -280,6 +280,38 @@ int paratc_profile_get(paratc_ctx* ctx, int k, double* total_ms, int64_t* launch
 /* Name of kernel class k ("rhs", "helmholtz", "fft_x_fwd", ...). */
 const char* paratc_profile_name(int k);
 
+/* ---- Ensembles.  No counterpart in the reference, which advances one case
+ * per MPI job; this is the batched form of ChannelIterate
+ * (src/m_ChannelSystem.f90:119-226) for many independent channel instances of
+ * uneven grid sizes and parameters on one device.  Every member is an ordinary
+ * context (create / set / get through paratc_batch_member) with its own
+ * stream; a step of the batch advances every member by one ChannelIterate,
+ * the members' kernels running concurrently.  With use_graph != 0 the
+ * members' steps are captured once into one CUDA graph (fork/join over the
+ * member streams) and every further step of the batch is one graph launch;
+ * a member whose state was changed since (set_fields, project, substep, a dt
+ * change) first takes one ordinary step, so the graph never replays a step
+ * whose clcCFL or Helmholtz pivots are stale.  Calls on one batch must not be
+ * concurrent; members must not be stepped on their own while a batch call
+ * runs. */
+typedef struct paratc_batch paratc_batch;
+
+/* n members; prm[i] and yp[i] (nyc+1 y-faces) as for paratc_create. */
+int paratc_batch_create(int n, const paratc_params* prm, const double* const* yp, int device,
+                        paratc_batch** out);
+int paratc_batch_destroy(paratc_batch* b);
+/* The context of member i (owned by the batch: do not paratc_destroy it). */
+int paratc_batch_member(paratc_batch* b, int i, paratc_ctx** ctx);
+/* nsteps steps of every member; diag (n entries, may be NULL) receives each
+ * member's last step.  Returns the first failing member's status. */
+int paratc_batch_steps(paratc_batch* b, int nsteps, int use_graph, paratc_diag* diag);
+/* Kernels one graph launch of the batch runs (0 before the first capture). */
+int64_t paratc_batch_graph_kernels(paratc_batch* b);
+/* The stream the batch's graph is launched on (cudaStream_t); work queued on
+ * it before paratc_batch_steps precedes the steps, work queued after them
+ * follows them. */
+void* paratc_batch_stream(paratc_batch* b);
+
 #ifdef __cplusplus
 }
 #endif

@@ -807,3 +807,204 @@ int paratc_read_restart(paratc_ctx* ctx, const char* path) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// ensembles
+// ---------------------------------------------------------------------------
+struct paratc_batch {
+    int n = 0, dev = 0;
+    std::vector<paratc_ctx*> m;
+    cudaStream_t st = nullptr;          // stream the graph is captured on and launched from
+    cudaEvent_t fork = nullptr, done = nullptr;
+    std::vector<cudaEvent_t> join;      // one per member
+    cudaGraphExec_t exec = nullptr;
+    bool graph_failed = false;
+    int64_t graph_kernels = 0;
+    std::string err;
+};
+
+namespace {
+
+// a member whose next step is the steady step the graph holds: clcCFL done by
+// its last end-of-step kernel, Helmholtz pivots current (or recomputed every
+// step, iCFL = 1)
+bool member_steady(const paratc_ctx* c) {
+    return c->next_ready && (c->prm.icfl == 1 || c->hfac_dt == c->prm.dt_max);
+}
+
+void batch_free_graph(paratc_batch* b) {
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    b->exec = nullptr;
+}
+
+// b->st waits for everything already queued on the member streams
+cudaError_t batch_join_members(paratc_batch* b) {
+    for (int i = 0; i < b->n; i++) {
+        cudaError_t e = cudaEventRecord(b->join[i], b->m[i]->st);
+        if (e != cudaSuccess) return e;
+        if ((e = cudaStreamWaitEvent(b->st, b->join[i], 0)) != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+// the member streams wait for everything queued on b->st
+cudaError_t batch_fork_members(paratc_batch* b) {
+    cudaError_t e = cudaEventRecord(b->done, b->st);
+    if (e != cudaSuccess) return e;
+    for (int i = 0; i < b->n; i++)
+        if ((e = cudaStreamWaitEvent(b->m[i]->st, b->done, 0)) != cudaSuccess) return e;
+    return cudaSuccess;
+}
+
+int batch_capture(paratc_batch* b) {
+    cudaGraph_t g = nullptr;
+    int64_t l0 = 0;
+    for (auto* c : b->m) l0 += c->launches;
+    cudaError_t e = cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return (int)e;
+    bool ok = cudaEventRecord(b->fork, b->st) == cudaSuccess;
+    for (int i = 0; ok && i < b->n; i++) {
+        paratc_ctx* c = b->m[i];
+        ok = cudaStreamWaitEvent(c->st, b->fork, 0) == cudaSuccess;
+        if (ok) enqueue_step(c);
+        ok = ok && cudaEventRecord(b->join[i], c->st) == cudaSuccess;
+        ok = ok && cudaStreamWaitEvent(b->st, b->join[i], 0) == cudaSuccess;
+    }
+    e = cudaStreamEndCapture(b->st, &g);
+    if (!ok || e != cudaSuccess || !g) {
+        if (g) cudaGraphDestroy(g);
+        cudaGetLastError();
+        return ok ? (int)e : -1;
+    }
+    e = cudaGraphInstantiate(&b->exec, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+        b->exec = nullptr;
+        cudaGetLastError();
+        return (int)e;
+    }
+    int64_t l1 = 0;
+    for (auto* c : b->m) l1 += c->launches;
+    b->graph_kernels = l1 - l0;
+    return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int paratc_batch_create(int n, const paratc_params* prm, const double* const* yp, int device, paratc_batch** out) {
+    if (n < 1 || !prm || !yp || !out) return PARATC_ERR_BAD_ARG;
+    *out = nullptr;
+    paratc_batch* b = new paratc_batch();
+    b->n = n;
+    b->dev = device;
+    for (int i = 0; i < n; i++) {
+        paratc_ctx* c = nullptr;
+        int rc = paratc_create(&prm[i], yp[i], device, &c);
+        if (rc != PARATC_OK) {
+            paratc_batch_destroy(b);
+            return rc;
+        }
+        b->m.push_back(c);
+    }
+    b->dev = b->m[0]->dev;  // the device paratc_create resolved (device < 0: the current one)
+    b->join.assign(n, nullptr);
+    bool ok = cudaSetDevice(b->dev) == cudaSuccess &&
+              cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) == cudaSuccess &&
+              cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming) == cudaSuccess;
+    for (int i = 0; ok && i < n; i++) ok = cudaEventCreateWithFlags(&b->join[i], cudaEventDisableTiming) == cudaSuccess;
+    if (!ok) {
+        paratc_batch_destroy(b);
+        return PARATC_ERR_CUDA;
+    }
+    *out = b;
+    return PARATC_OK;
+}
+
+int paratc_batch_destroy(paratc_batch* b) {
+    if (!b) return PARATC_OK;
+    if (b->st) cudaStreamSynchronize(b->st);
+    batch_free_graph(b);
+    for (cudaEvent_t e : b->join)
+        if (e) cudaEventDestroy(e);
+    if (b->fork) cudaEventDestroy(b->fork);
+    if (b->done) cudaEventDestroy(b->done);
+    if (b->st) cudaStreamDestroy(b->st);
+    for (auto* c : b->m) paratc_destroy(c);
+    delete b;
+    return PARATC_OK;
+}
+
+int paratc_batch_member(paratc_batch* b, int i, paratc_ctx** ctx) {
+    if (!b || !ctx || i < 0 || i >= b->n) return PARATC_ERR_BAD_ARG;
+    *ctx = b->m[i];
+    return PARATC_OK;
+}
+
+int64_t paratc_batch_graph_kernels(paratc_batch* b) { return b ? b->graph_kernels : 0; }
+
+void* paratc_batch_stream(paratc_batch* b) { return b ? (void*)b->st : nullptr; }
+
+int paratc_batch_steps(paratc_batch* b, int nsteps, int use_graph, paratc_diag* diag) {
+    if (!b || nsteps < 1) return PARATC_ERR_BAD_ARG;
+    if (cudaSetDevice(b->dev) != cudaSuccess) return PARATC_ERR_CUDA;
+    if (batch_fork_members(b) != cudaSuccess) return PARATC_ERR_CUDA;  // after what the caller queued on b->st
+    for (auto* c : b->m) {
+        c->prof_on = false;  // the event timer cannot live inside a graph
+        if (cudaMemsetAsync(c->d_diag, 0, sizeof(DDiag), c->st) != cudaSuccess) return PARATC_ERR_CUDA;
+    }
+    int s = 0;
+    const bool graph = use_graph && !b->graph_failed;
+    if (graph) {
+        bool steady = true;
+        for (auto* c : b->m) steady = steady && member_steady(c);
+        if (!steady) {
+            for (auto* c : b->m) enqueue_step(c);
+            s++;
+        }
+        if (s < nsteps && !b->exec) {
+            // the capture needs every member in the steady state first
+            bool st2 = true;
+            for (auto* c : b->m) st2 = st2 && member_steady(c);
+            if (!st2 || batch_capture(b) != 0) {
+                b->graph_failed = true;
+                batch_free_graph(b);
+            }
+        }
+        if (b->exec && s < nsteps) {
+            if (batch_join_members(b) != cudaSuccess) return PARATC_ERR_CUDA;
+            for (; s < nsteps; s++)
+                if (cudaGraphLaunch(b->exec, b->st) != cudaSuccess) return PARATC_ERR_CUDA;
+            for (auto* c : b->m) c->launches += b->graph_kernels / b->n;
+            if (batch_fork_members(b) != cudaSuccess) return PARATC_ERR_CUDA;
+        }
+    }
+    for (; s < nsteps; s++)
+        for (auto* c : b->m) enqueue_step(c);
+    if (batch_join_members(b) != cudaSuccess) return PARATC_ERR_CUDA;  // b->st follows every member
+    int first = PARATC_OK;
+    for (int i = 0; i < b->n; i++) {
+        paratc_ctx* c = b->m[i];
+        if (cudaMemcpyAsync(c->h_diag, c->d_diag, sizeof(DDiag), cudaMemcpyDeviceToHost, c->st) != cudaSuccess)
+            return PARATC_ERR_CUDA;
+    }
+    for (int i = 0; i < b->n; i++) {
+        paratc_ctx* c = b->m[i];
+        int rc = sync(c);
+        if (rc) return rc;
+        if (diag) diag_out(*c->h_diag, &diag[i]);
+        if (c->h_diag->status != 0 && first == PARATC_OK) {
+            first = c->h_diag->status;
+            char msg[160];
+            std::snprintf(msg, sizeof(msg), "member %d: %s at step %d (divmax %.6e)", i,
+                          paratc_strerror(c->h_diag->status), c->h_diag->failed_step, c->h_diag->divmax);
+            b->err = msg;
+            set_err(c, first, msg);
+        }
+    }
+    return first;
+}
+
+}  // extern "C"

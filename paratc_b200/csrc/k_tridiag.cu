@@ -200,7 +200,6 @@ __global__ void __launch_bounds__(128) k_helm(DConst cst, const DCoef* __restric
     double* rc = rhs + col;
     double* uc = u + col;
     const int nch = (ny + HY_U - 1) / HY_U;
-    const size_t step = (size_t)HY_U * nx;
 
     // forward sweep, rows 1..ny: f = ((r + add) - a f_prev) / vecm, written over Rhs
     double A[HY_U], B[HY_U], C[HY_U];

@@ -28,7 +28,8 @@ EXPORTED = [
     "paratc_substep", "paratc_substep_stage", "paratc_get_work", "paratc_poisson", "paratc_poisson_device", "paratc_project", "paratc_diagnostics",
     "paratc_write_restart", "paratc_read_restart", "paratc_strerror", "paratc_last_error", "paratc_launch_count",
     "paratc_profile_enable", "paratc_profile_get", "paratc_profile_name", "paratc_steps_async", "paratc_last_diag",
-    "paratc_poisson_noalloc",
+    "paratc_poisson_noalloc", "paratc_batch_create", "paratc_batch_destroy", "paratc_batch_member",
+    "paratc_batch_steps", "paratc_batch_graph_kernels", "paratc_batch_stream",
 ]
 PROF_NKERNELS = 16
 
@@ -87,6 +88,15 @@ def load(path=None):
     L.paratc_profile_get.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, ctypes.POINTER(ctypes.c_int64)]
     L.paratc_profile_name.argtypes = [ctypes.c_int]
     L.paratc_profile_name.restype = ctypes.c_char_p
+    L.paratc_batch_create.argtypes = [ctypes.c_int, ctypes.POINTER(ParatcParams), ctypes.POINTER(_dp), ctypes.c_int,
+                                      ctypes.POINTER(ctypes.c_void_p)]
+    L.paratc_batch_destroy.argtypes = [ctypes.c_void_p]
+    L.paratc_batch_member.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]
+    L.paratc_batch_steps.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ParatcDiag)]
+    L.paratc_batch_graph_kernels.argtypes = [ctypes.c_void_p]
+    L.paratc_batch_graph_kernels.restype = ctypes.c_int64
+    L.paratc_batch_stream.argtypes = [ctypes.c_void_p]
+    L.paratc_batch_stream.restype = ctypes.c_void_p
     _lib = L
     return L
 
@@ -139,22 +149,27 @@ class ChannelSystem:
 
     FIELDS = ("ux", "uy", "uz", "p", "c", "hx", "hy", "hz", "hc")
 
-    def __init__(self, params, yp, device=-1):
+    def __init__(self, params, yp, device=-1, _borrowed=None):
         L = load()
         self.params = params.copy()
         self.shape = (params.nzc, params.nyc, params.nxc)
         self._yp = np.ascontiguousarray(yp, dtype=np.float64)
+        self._L = L
+        self._owner = _borrowed is None
+        if _borrowed is not None:  # a member of a BatchSystem, destroyed with it
+            self._h = _borrowed
+            return
         h = ctypes.c_void_p()
         rc = L.paratc_create(ctypes.byref(self.params), _ptr(self._yp), int(device), ctypes.byref(h))
         if rc != PARATC_OK:
             raise ParatcError(rc, "paratc_create")
         self._h = h
-        self._L = L
 
     # -- lifetime
     def close(self):
         if getattr(self, "_h", None):
-            self._L.paratc_destroy(self._h)
+            if self._owner:
+                self._L.paratc_destroy(self._h)
             self._h = None
 
     def __del__(self):
@@ -297,3 +312,63 @@ class ChannelSystem:
 
     def read_restart(self, path):
         self._check(self._L.paratc_read_restart(self._h, path.encode()), "paratc_read_restart")
+
+
+class BatchSystem:
+    """An ensemble of independent contexts that advance together
+    (paratc_batch_*): members[i] is a ChannelSystem view of member i."""
+
+    def __init__(self, params_list, yp_list, device=-1):
+        L = load()
+        n = len(params_list)
+        self._L = L
+        self._params = (ParatcParams * n)(*[p.copy() for p in params_list])
+        self._yps = [np.ascontiguousarray(y, dtype=np.float64) for y in yp_list]
+        ptrs = (_dp * n)(*[_ptr(y) for y in self._yps])
+        h = ctypes.c_void_p()
+        rc = L.paratc_batch_create(n, self._params, ptrs, int(device), ctypes.byref(h))
+        if rc != PARATC_OK:
+            raise ParatcError(rc, "paratc_batch_create")
+        self._h = h
+        self.members = []
+        for i in range(n):
+            m = ctypes.c_void_p()
+            rc = L.paratc_batch_member(h, i, ctypes.byref(m))
+            if rc != PARATC_OK:
+                raise ParatcError(rc, "paratc_batch_member")
+            self.members.append(ChannelSystem(params_list[i], yp_list[i], _borrowed=m))
+
+    def __len__(self):
+        return len(self.members)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            for m in self.members:
+                m.close()
+            self._L.paratc_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def iterate(self, nsteps=1, use_graph=True, raise_on_guard=True):
+        """nsteps ChannelIterate steps of every member; returns the members'
+        last-step diagnostics."""
+        n = len(self.members)
+        d = (ParatcDiag * n)()
+        rc = self._L.paratc_batch_steps(self._h, int(nsteps), int(bool(use_graph)), d)
+        if rc != PARATC_OK and (raise_on_guard or rc not in (PARATC_ERR_DIV_LIMIT, PARATC_ERR_VEL_LIMIT)):
+            raise ParatcError(rc, "paratc_batch_steps")
+        return list(d)
+
+    @property
+    def graph_kernels(self):
+        return int(self._L.paratc_batch_graph_kernels(self._h))
+
+    @property
+    def stream(self):
+        return self._L.paratc_batch_stream(self._h)
+
