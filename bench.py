@@ -26,6 +26,8 @@ import sys
 import threading
 import time
 
+import numpy as np
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
@@ -461,12 +463,89 @@ def run_ensemble(args):
         dist.destroy_process_group()
 
 
+def run_poisson(args):
+    """C2: the standalone pressure Poisson solve, 512 x 256 x 512, seeded
+    Gaussian right-hand side with its mean removed.  `value` in grid points
+    solved per second; the roofline counts 6 words per cell (forward 2-D FFT,
+    y-Thomas, inverse 2-D FFT, each a read and a write).  src and phi (537 MB
+    each) exceed the L2, so no flush is needed between solves."""
+    import torch
+    ws, rank, local = _dist()
+    torch.cuda.set_device(local)
+    from paratc_b200 import cases
+    from paratc_b200.lib import ChannelSystem, mesh_ycoord
+    case = cases.poisson_c2()
+    p = case.params
+    yp = mesh_ycoord(case.mesh, p.yly)
+    src = cases.gaussian_source(cases.Case("src", p, case.mesh, "gauss_src", 42 + rank, 1.0))
+    cells = p.nxc * p.nyc * p.nzc
+    ctx = ChannelSystem(p, yp, device=local)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=local)
+    d_src = torch.from_numpy(src).to("cuda:%d" % local)
+    d_phi = torch.empty_like(d_src)
+    torch.cuda.synchronize()
+    for _ in range(args.warmup):
+        ctx.poisson_device(d_src.data_ptr(), d_phi.data_ptr())
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    sampler = ClockSampler(local)
+    sampler.start()
+    for a, b in evs:
+        a.record(stream)
+        ctx.poisson_device_async(d_src.data_ptr(), d_phi.data_ptr())
+        b.record(stream)
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    ms = sum(a.elapsed_time(b) for a, b in evs)
+    phi_g = d_phi.cpu().numpy()
+    # end to end: host source in, host potential out (paratc_poisson)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        phi_h = ctx.poisson(src)
+    t_e2e = time.perf_counter() - t0
+    base = None
+    err = None
+    if rank == 0 and not args.no_cpu_baseline:
+        from oracle import oracle_lib as ol
+        threads = os.cpu_count() or 1
+        o = ol.Oracle(p, yp, threads=threads)
+        t0 = time.perf_counter()
+        phi_o = o.poisson(src)
+        t_o = time.perf_counter() - t0
+        o.close()
+        err = float(np.abs(phi_g - phi_o).max() / np.abs(phi_o).max())
+        base = {"value": cells / t_o, "unit": "grid-point Poisson solves/s", "cores": threads, "kind": "port",
+                "sample": "one 512x256x512 solve on the C oracle (OpenMP, %d threads), %.1f s" % (threads, t_o)}
+    peak, peak_kind = _peaks()
+    alg = 6 * 8 * cells
+    ach = alg / (ms / args.steps / 1e3) / 1e9
+    if rank == 0:
+        line = {"metric": "grid-point Poisson solves/s", "value": ws * cells * args.steps / (ms / 1e3),
+                "unit": "grid-point Poisson solves/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f64", "data": "synthetic",
+                "config": {"workload": case.name, "grid": [p.nxc, p.nyc, p.nzc], "precision": "fp64",
+                           "l2": "src and phi 537 MB each > L2, no flush",
+                           "max_rel_err_vs_oracle": err, "mean_phi_e2e_equal": bool(np.array_equal(phi_h, phi_g))},
+                "roofline": {"bound": "hbm", "kernel": "poisson solve (5 kernels)", "achieved": round(ach, 1),
+                             "peak": peak, "unit": "GB/s", "frac": round(ach / peak, 4), "traffic": None,
+                             "peak_kind": peak_kind, "algorithmic_bytes_per_launch": alg},
+                "cpu_baseline": base,
+                "e2e": {"value": cells * args.steps / t_e2e, "unit": "grid-point Poisson solves/s",
+                        "h2d_bytes_per_step": src.nbytes, "d2h_bytes_per_step": src.nbytes,
+                        "note": "paratc_poisson with host arrays: source in, potential out"},
+                "gpu_launches": None, "clocks": clocks}
+        print(json.dumps(line), flush=True)
+    ctx.close()
+
+
 def main():
     args = _args()
     if args.impl == "reference":
         run_reference(args)
     elif args.workload == "ensemble_c4":
         run_ensemble(args)
+    elif args.workload == "poisson_c2":
+        run_poisson(args)
     else:
         run_ours(args)
 

@@ -228,6 +228,9 @@ int paratc_get_work(paratc_ctx* ctx, int which, double* out);
 int paratc_poisson(paratc_ctx* ctx, const double* src, double* phi);
 /* Same with device pointers (interior layout, nxc*nyc*nzc doubles). */
 int paratc_poisson_device(paratc_ctx* ctx, const double* d_src, double* d_phi);
+/* As paratc_poisson_device, but returns once the solve is queued on the
+ * context's stream (paratc_stream), without waiting for it. */
+int paratc_poisson_device_async(paratc_ctx* ctx, const double* d_src, double* d_phi);
 
 /* Poisson solve that allocates no memory.  No counterpart in the reference:
  * it exists for callers that cannot call cudaMalloc (a loop with a fixed

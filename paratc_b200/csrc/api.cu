@@ -702,6 +702,14 @@ int paratc_poisson_device(paratc_ctx* ctx, const double* d_src, double* d_phi) {
     return sync(ctx);
 }
 
+int paratc_poisson_device_async(paratc_ctx* ctx, const double* d_src, double* d_phi) {
+    if (!ctx || !d_src || !d_phi) return PARATC_ERR_BAD_ARG;
+    CK(cudaSetDevice(ctx->dev));
+    enqueue_poisson(ctx, d_src, d_phi, 0);
+    CK(cudaGetLastError());
+    return PARATC_OK;
+}
+
 int paratc_poisson(paratc_ctx* ctx, const double* src, double* phi) {
     if (!ctx || !src || !phi) return PARATC_ERR_BAD_ARG;
     CK(cudaSetDevice(ctx->dev));

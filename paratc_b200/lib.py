@@ -25,7 +25,7 @@ EXPORTED = [
     "paratc_mesh_ycoord", "paratc_params_from_namelist", "paratc_run_options_from_namelist", "paratc_create",
     "paratc_destroy", "paratc_stream", "paratc_set_fields", "paratc_get_fields", "paratc_set_fields_device",
     "paratc_get_fields_device", "paratc_set_time", "paratc_get_time", "paratc_step", "paratc_steps",
-    "paratc_substep", "paratc_substep_stage", "paratc_get_work", "paratc_poisson", "paratc_poisson_device", "paratc_project", "paratc_diagnostics",
+    "paratc_substep", "paratc_substep_stage", "paratc_get_work", "paratc_poisson", "paratc_poisson_device", "paratc_poisson_device_async", "paratc_project", "paratc_diagnostics",
     "paratc_write_restart", "paratc_read_restart", "paratc_strerror", "paratc_last_error", "paratc_launch_count",
     "paratc_profile_enable", "paratc_profile_get", "paratc_profile_name", "paratc_steps_async", "paratc_last_diag",
     "paratc_poisson_noalloc", "paratc_batch_create", "paratc_batch_destroy", "paratc_batch_member",
@@ -70,6 +70,7 @@ def load(path=None):
     L.paratc_get_work.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp]
     L.paratc_poisson.argtypes = [ctypes.c_void_p, _dp, _dp]
     L.paratc_poisson_device.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+    L.paratc_poisson_device_async.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
     L.paratc_project.argtypes = [ctypes.c_void_p, _dp]
     L.paratc_diagnostics.argtypes = [ctypes.c_void_p, ctypes.POINTER(ParatcDiag)]
     L.paratc_write_restart.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int]
@@ -282,6 +283,10 @@ class ChannelSystem:
     def poisson_device(self, d_src_ptr, d_phi_ptr):
         self._check(self._L.paratc_poisson_device(self._h, ctypes.c_void_p(d_src_ptr), ctypes.c_void_p(d_phi_ptr)),
                     "paratc_poisson_device")
+
+    def poisson_device_async(self, d_src_ptr, d_phi_ptr):
+        self._check(self._L.paratc_poisson_device_async(self._h, ctypes.c_void_p(d_src_ptr), ctypes.c_void_p(d_phi_ptr)),
+                    "paratc_poisson_device_async")
 
     def project(self):
         dm = ctypes.c_double()
