@@ -54,7 +54,7 @@ struct paratc_ctx {
     double *d_metric = nullptr, *d_scal = nullptr;
     double2 *d_spec = nullptr, *d_twx = nullptr, *d_postx = nullptr, *d_twz = nullptr;
     bool pfft = false;   // compile-time-length transforms exist for nx/2 and nz
-    double2* d_pfac = nullptr;  // pivots of the spectral y systems, computed once
+    double* d_pfac = nullptr;   // pivots of the spectral y systems (1/vecm, then arr), computed once
     DCoef* d_coef = nullptr;
     DDiag* d_diag = nullptr;
     DDiag* d_diag2 = nullptr;
@@ -472,7 +472,7 @@ int paratc_create(const paratc_params* prm, const double* yp, int device, paratc
         (rc = dalloc(ctx, &ctx->d_diag, 1)) || (rc = dalloc(ctx, &ctx->d_diag2, 1)) || (rc = dalloc(ctx, &ctx->d_scal, 16)) ||
         (rc = dalloc(ctx, &ctx->d_counter, 16)) ||
         (rc = dalloc(ctx, &ctx->d_hfac, helm_fac_doubles(ctx->ny))) ||
-        (rc = dalloc(ctx, &ctx->d_pfac, (size_t)ctx->M1 * ctx->nz * ctx->ny))) {
+        (rc = dalloc(ctx, &ctx->d_pfac, (size_t)2 * ctx->M1 * ctx->nz * ctx->ny))) {
         paratc_destroy(ctx);
         return rc;
     }

@@ -350,8 +350,9 @@ __global__ void __launch_bounds__(512) k_ysolve(DConst cst, DMetric m, double* _
 // (am2ph, ac2ph + lambda_x(kx) + lambda_z(kz), ap2ph) depend on the mesh and
 // the wavenumbers only, so the pivots of InverseTridiagonal
 // (src/m_Tools.f90:224-251) are computed once per context: for complex
-// column q = kz*(nx/2+1) + kx and Fortran row jc, fac[(jc-1)*NQ + q] =
-// {1/vecm(jc), arr(jc)} with vecm(1) = b(1), arr(jc) = c(jc-1)/vecm(jc-1),
+// column q = kz*(nx/2+1) + kx and Fortran row jc, rv[(jc-1)*NQ + q] =
+// 1/vecm(jc) and ar[(jc-1)*NQ + q] = arr(jc) (two arrays, so that each sweep
+// reads only the one it needs) with vecm(1) = b(1), arr(jc) = c(jc-1)/vecm(jc-1),
 // vecm(jc) = b(jc) - a(jc)*arr(jc), evaluated in the reference's order
 // without contraction.  A solve is then the two sweeps
 //   f(1) = f(1)/vecm(1),  f(jc) = (f(jc) - a(jc) f(jc-1)) / vecm(jc),
@@ -360,7 +361,7 @@ __global__ void __launch_bounds__(512) k_ysolve(DConst cst, DMetric m, double* _
 // The kx = kz = 0 system has row 1 replaced by phi = 0 (b = 1, c = 0,
 // f = 0; src/m_Poisson.f90:399-404).
 // ---------------------------------------------------------------------------
-__global__ void k_pois_factors(int ny, int M1, int nz, DMetric m, double2* __restrict__ fac) {
+__global__ void k_pois_factors(int ny, int M1, int nz, DMetric m, double* __restrict__ rv, double* __restrict__ ar) {
     const int NQ = M1 * nz;
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= NQ) return;
@@ -368,13 +369,15 @@ __global__ void k_pois_factors(int ny, int M1, int nz, DMetric m, double2* __res
     const double wx = m.wnx[kx], wz = m.wnz[kz];
     const bool dc = (q == 0);
     double vecm = dc ? 1.0 : __dadd_rn(__dadd_rn(m.ac2ph[1], wx), wz);
-    fac[q] = make_double2(1.0 / vecm, 0.0);
+    rv[q] = 1.0 / vecm;
+    ar[q] = 0.0;
     for (int jc = 2; jc <= ny; jc++) {
         const double cp = (dc && jc == 2) ? 0.0 : m.ap2ph[jc - 1];
         const double arr = cp / vecm;
         const double b = __dadd_rn(__dadd_rn(m.ac2ph[jc], wx), wz);
         vecm = __dsub_rn(b, __dmul_rn(m.am2ph[jc], arr));
-        fac[(size_t)(jc - 1) * NQ + q] = make_double2(1.0 / vecm, arr);
+        rv[(size_t)(jc - 1) * NQ + q] = 1.0 / vecm;
+        ar[(size_t)(jc - 1) * NQ + q] = arr;
     }
 }
 
@@ -390,29 +393,48 @@ constexpr int YS_U = 8;  // rows loaded ahead of the dependent chain
 // spectrum and their factors in shared memory with cp.async, then lane l
 // sweeps the real (l even) or imaginary (l odd) part of column l/2.
 __global__ void __launch_bounds__(32) k_ys_staged(int ny, int M1, int nz, const double* __restrict__ am2ph,
-                                                  double2* __restrict__ spec, const double2* __restrict__ fac) {
+                                                  double2* __restrict__ spec, const double* __restrict__ fac) {
     extern __shared__ double2 sy[];
     const int lane = threadIdx.x;
     const int NQ = M1 * nz;
     const int q0 = blockIdx.x * 16;
     const int nv = min(16, NQ - q0);
-    double2* sd = sy;                   // [ny][16] spectrum
-    double2* sf = sy + ny * 16;         // [ny][16] factors
-    double* sa = reinterpret_cast<double*>(sf + ny * 16);  // am2ph[0..ny]
+    double2* sd = sy;                                          // [ny][16] spectrum
+    double* srv = reinterpret_cast<double*>(sy + ny * 16);     // [ny][16] 1/vecm
+    double* sar = srv + ny * 16;                               // [ny][16] arr
+    double* sa = sar + ny * 16;                                // am2ph[0..ny]
     pdl_wait();
     pdl_trigger();
-    // lane (cq, half) copies rows half, half+2, ... of complex column q0+cq
+    // one 16-byte copy per lane and row: lanes 0-15 the spectrum of column
+    // q0+lane, lanes 16-23 two 1/vecm of columns q0+2(lane-16)+{0,1}, lanes
+    // 24-31 two arr (NQ is even, so the pairs are aligned and never split)
     const int cq = lane & 15, half = lane >> 4;
     const bool cval = cq < nv;
     const int qq = q0 + (cval ? cq : 0);
     const int kz = qq / M1, kx = qq - kz * M1;
     double2* scol = spec + (size_t)kz * ny * M1 + kx;
-    const double2* fcol = fac + qq;
-    if (cval)
-        for (int j = half; j < ny; j += 2) {
-            cpa16t(&sd[j * 16 + cq], scol + (size_t)j * M1);
-            cpa16t(&sf[j * 16 + cq], fcol + (size_t)j * NQ);
-        }
+    const char* gsrc;
+    char* sdst;
+    size_t gstride;
+    int sstride;
+    bool cvalid;
+    if (lane < 16) {
+        gsrc = reinterpret_cast<const char*>(scol);
+        gstride = (size_t)M1 * sizeof(double2);
+        sdst = reinterpret_cast<char*>(sd + lane);
+        sstride = 16 * sizeof(double2);
+        cvalid = cval;
+    } else {
+        const int pr = (lane & 7) * 2;
+        const double* base = fac + (lane < 24 ? (size_t)0 : (size_t)NQ * ny) + q0 + pr;
+        gsrc = reinterpret_cast<const char*>(base);
+        gstride = (size_t)NQ * sizeof(double);
+        sdst = reinterpret_cast<char*>((lane < 24 ? srv : sar) + pr);
+        sstride = 16 * sizeof(double);
+        cvalid = pr < nv;
+    }
+    if (cvalid)
+        for (int j = 0; j < ny; j++) cpa16t(sdst + (size_t)j * sstride, gsrc + (size_t)j * gstride);
     for (int j = lane; j <= ny; j += 32) sa[j] = __ldg(&am2ph[j]);
     asm volatile("cp.async.commit_group;\n" ::: "memory");
     asm volatile("cp.async.wait_group 0;\n" ::: "memory");
@@ -428,7 +450,7 @@ __global__ void __launch_bounds__(32) k_ys_staged(int ny, int M1, int nz, const 
             const int j = j0 + u;
             if (j < ny) {
                 d[u] = sdd[j * 32 + lane];
-                rv[u] = sf[j * 16 + cp].x;
+                rv[u] = srv[j * 16 + cp];
                 a[u] = sa[j + 1];
             }
         }
@@ -450,7 +472,7 @@ __global__ void __launch_bounds__(32) k_ys_staged(int ny, int M1, int nz, const 
             const int j = j0 - u;
             if (j >= 0) {
                 d[u] = sdd[j * 32 + lane];
-                ar[u] = sf[(j + 1) * 16 + cp].y;
+                ar[u] = sar[(j + 1) * 16 + cp];
             }
         }
 #pragma unroll
@@ -471,7 +493,7 @@ __global__ void __launch_bounds__(32) k_ys_staged(int ny, int M1, int nz, const 
 // Large grids: one thread per real column straight from global memory, the
 // rows of a chunk loaded ahead of its chain, latency hidden by occupancy.
 __global__ void __launch_bounds__(128) k_ys_global(int ny, int M1, int nz, const double* __restrict__ am2ph,
-                                                   double* __restrict__ specd, const double2* __restrict__ fac) {
+                                                   double* __restrict__ specd, const double* __restrict__ fac) {
     const int W = 2 * M1, NQ = M1 * nz;
     const int g = blockIdx.x * blockDim.x + threadIdx.x;
     pdl_wait();
@@ -479,7 +501,8 @@ __global__ void __launch_bounds__(128) k_ys_global(int ny, int M1, int nz, const
     if (g >= W * nz) return;
     const int kz = g / W, cr = g - kz * W, q = g >> 1;
     double* col = specd + (size_t)kz * ny * W + cr;
-    const double2* fc = fac + q;
+    const double* frv = fac + q;
+    const double* far = fac + (size_t)NQ * ny + q;
     const bool dc = (q == 0);
     double fp = 0.0;
     for (int j0 = 0; j0 < ny; j0 += YS_U) {
@@ -489,7 +512,7 @@ __global__ void __launch_bounds__(128) k_ys_global(int ny, int M1, int nz, const
             const int j = j0 + u;
             if (j < ny) {
                 d[u] = col[(size_t)j * W];
-                rv[u] = __ldg(&fc[(size_t)j * NQ]).x;
+                rv[u] = __ldg(&frv[(size_t)j * NQ]);
                 a[u] = __ldg(&am2ph[j + 1]);
             }
         }
@@ -511,7 +534,7 @@ __global__ void __launch_bounds__(128) k_ys_global(int ny, int M1, int nz, const
             const int j = j0 - u;
             if (j >= 0) {
                 d[u] = col[(size_t)j * W];
-                ar[u] = __ldg(&fc[(size_t)(j + 1) * NQ]).y;
+                ar[u] = __ldg(&far[(size_t)(j + 1) * NQ]);
             }
         }
 #pragma unroll
@@ -526,14 +549,14 @@ __global__ void __launch_bounds__(128) k_ys_global(int ny, int M1, int nz, const
     }
 }
 
-void launch_pois_factors(cudaStream_t st, const DConst& c, const DMetric& m, double2* fac) {
+void launch_pois_factors(cudaStream_t st, const DConst& c, const DMetric& m, double* fac) {
     const int M1 = c.nx / 2 + 1, NQ = M1 * c.nz;
-    k_pois_factors<<<(NQ + 127) / 128, 128, 0, st>>>(c.ny, M1, c.nz, m, fac);
+    k_pois_factors<<<(NQ + 127) / 128, 128, 0, st>>>(c.ny, M1, c.nz, m, fac, fac + (size_t)NQ * c.ny);
 }
 
 static size_t ys_staged_smem(int ny) { return (size_t)ny * 16 * 2 * sizeof(double2) + (size_t)(ny + 1) * sizeof(double); }
 
-void launch_ysolve_fac(cudaStream_t st, const DConst& c, const DMetric& m, double2* spec, const double2* fac) {
+void launch_ysolve_fac(cudaStream_t st, const DConst& c, const DMetric& m, double2* spec, const double* fac) {
     const int M1 = c.nx / 2 + 1, NQ = M1 * c.nz;
     const size_t sm = ys_staged_smem(c.ny);
     const int per_sm = sm > 0 ? (int)((220 * 1024) / sm) : 0;
@@ -543,7 +566,7 @@ void launch_ysolve_fac(cudaStream_t st, const DConst& c, const DMetric& m, doubl
     } else {
         const int n = 2 * M1 * c.nz;
         launch_pdl(k_ys_global, dim3((n + 127) / 128), dim3(128), 0, st, c.ny, M1, c.nz, m.am2ph,
-                   reinterpret_cast<double*>(spec), (const double2*)fac);
+                   reinterpret_cast<double*>(spec), fac);
     }
 }
 

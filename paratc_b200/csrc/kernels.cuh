@@ -68,8 +68,8 @@ void launch_helm_scalar(cudaStream_t st, const DConst& c, const DCoef* coef, con
 void launch_ysolve(cudaStream_t st, const DConst& c, const DMetric& m, double2* spec);
 
 // k_tridiag.cu: spectral y-solve with the pivots computed once per context
-void launch_pois_factors(cudaStream_t st, const DConst& c, const DMetric& m, double2* fac);
-void launch_ysolve_fac(cudaStream_t st, const DConst& c, const DMetric& m, double2* spec, const double2* fac);
+void launch_pois_factors(cudaStream_t st, const DConst& c, const DMetric& m, double* fac);
+void launch_ysolve_fac(cudaStream_t st, const DConst& c, const DMetric& m, double2* spec, const double* fac);
 
 // k_pfft_x.cu / k_pfft_z.cu: compile-time-length transforms of the Poisson solve
 bool pfft_x_supported(int n);
