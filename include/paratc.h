@@ -283,6 +283,19 @@ int paratc_profile_get(paratc_ctx* ctx, int k, double* total_ms, int64_t* launch
 /* Name of kernel class k ("rhs", "helmholtz", "fft_x_fwd", ...). */
 const char* paratc_profile_name(int k);
 
+/* ---- Statistics (clcStat, src/m_FlowCase.f90:257-428).  FP64 accumulators
+ * on the device: SumStat(k, jc) += <q_k>_xz for the 35 moments of clcStat (40
+ * with the scalar) at rows jc = 1..nyc and the three top-wall moments at
+ * jc = nyp, PrGradsum += PrGradAver, nfstime += 1.  The caller decides the
+ * cadence (every ivstats steps in the reference, :191).  The accumulators start
+ * at zero when the context is created. */
+int paratc_stats_reset(paratc_ctx* ctx);
+int paratc_stats_accumulate(paratc_ctx* ctx);
+/* SumStat in the reference's memory order (k fastest: sumstat[(jc-1)*nstat +
+ * k-1], nyp*nstat doubles; may be NULL), the moment count, nfstime and
+ * PrGradsum. */
+int paratc_stats_get(paratc_ctx* ctx, double* sumstat, int* nstat, int* nfstime, double* prgradsum);
+
 /* ---- Ensembles.  No counterpart in the reference, which advances one case
  * per MPI job; this is the batched form of ChannelIterate
  * (src/m_ChannelSystem.f90:119-226) for many independent channel instances of

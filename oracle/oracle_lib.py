@@ -48,6 +48,7 @@ def lib():
         L.orc_project.argtypes = [ctypes.c_void_p, _dp]
         L.orc_diagnostics.argtypes = [ctypes.c_void_p, ctypes.POINTER(ParatcDiag)]
         L.orc_metric.argtypes = [ctypes.c_void_p, ctypes.c_char_p, _dp, ctypes.c_int]
+        L.orc_stats.argtypes = [ctypes.c_void_p, _dp]
         L.orc_r2hc.argtypes = [ctypes.c_int, _dp, _dp]
         L.orc_hc2r.argtypes = [ctypes.c_int, _dp, _dp]
         L.orc_ycoord.argtypes = [ctypes.c_int, _dp, _dp, ctypes.POINTER(ctypes.c_int32),
@@ -204,6 +205,16 @@ class Oracle:
         d = ParatcDiag()
         lib().orc_diagnostics(self._h, ctypes.byref(d))
         return d
+
+    def stats(self):
+        """clcStat's contribution of the current fields: array [nyp, nstat]
+        (SumVec/(nx nz) per row jc = 1..nyp)."""
+        nst = 40 if self.params.scalar_on else 35
+        out = np.zeros((self.params.nyc + 1, nst))
+        rc = lib().orc_stats(self._h, _ptr(out))
+        if rc != 0:
+            raise RuntimeError("orc_stats rc=%d" % rc)
+        return out
 
     def metric(self, name):
         buf = np.empty(max(self.params.nxc, self.params.nyc, self.params.nzc) + 8)

@@ -1143,6 +1143,148 @@ int orc_diagnostics(orc_t* o, paratc_diag* d) {
 }
 
 /* ------------------------------------------------------------------------
+ * clcStat (src/m_FlowCase.f90:257-428): one call's contribution
+ * SumVec(k)*inxz to SumStat(k, jc), jc = 1..nyp, k fastest in out[]; nst = 35
+ * (40 with the scalar).  Loop order and expressions as the reference.
+ * ---------------------------------------------------------------------- */
+int orc_stats(orc_t* o, double* out) {
+    if (!o || !out) return PARATC_ERR_BAD_ARG;
+    const int nxc = o->nxc, nyc = o->nyc, nzc = o->nzc, nyp = o->nyp;
+    const int nst = o->p.scalar_on ? 40 : 35;
+    const double *ux = o->ux, *uy = o->uy, *uz = o->uz, *pr = o->pr, *sc = o->sc;
+    const double *dxC = o->dxC, *dzC = o->dzC, *dxxC = o->dxxC, *dzzC = o->dzzC, *IC = o->IC;
+    const double uCRF = o->p.ucrf;
+    upd_halo(o, o->ux, 2, 2, 2, 2);
+    upd_halo(o, o->uy, 2, 2, 2, 2);
+    upd_halo(o, o->uz, 2, 2, 2, 2);
+    upd_halo(o, o->pr, 2, 1, 2, 1);
+    if (o->p.scalar_on) upd_halo(o, o->sc, 2, 2, 2, 2);
+    const double rdxt = o->rdx / 12.0, rdzt = o->rdz / 12.0;
+    const double inxz = one / ((double)nxc * (double)nzc);
+#pragma omp parallel for schedule(static)
+    for (int jc = 1; jc <= nyc; jc++) {
+        const int jp = jc + 1, jm = jc - 1;
+        const double InterpY1 = o->yinterp[jc], InterpY2 = one - InterpY1;
+        const double cac = o->rdyc[jc], cacU = o->rdyc[jp], caj = o->rdyp[jc];
+        double SumVec[40];
+        for (int q = 0; q < 40; q++) SumVec[q] = zero;
+        for (int kc = 1; kc <= nzc; kc++) {
+            const int ks = kc - 2, km = kc - 1, kp = kc + 1, ku = kc + 2;
+            for (int ic = 1; ic <= nxc; ic++) {
+                const int is = ic - 2, im = ic - 1, ip = ic + 1, iu = ic + 2;
+#define A(a, i, j, k) (a)[HX(o, i, j, k)]
+                double uxloc = A(ux, ic, jc, kc) + uCRF;
+                double uyloc = A(uy, ic, jc, kc);
+                double uzloc = A(uz, ic, jc, kc);
+                double prloc = A(pr, ic, jc, kc);
+                double uxCell = IC[0] * A(ux, im, jc, kc) + IC[1] * A(ux, ic, jc, kc) + IC[2] * A(ux, ip, jc, kc) + IC[3] * A(ux, iu, jc, kc) + uCRF;
+                double uyCell = (uyloc + A(uy, ic, jp, kc)) * half;
+                double uy_xc = IC[0] * A(uy, is, jc, kc) + IC[1] * A(uy, im, jc, kc) + IC[2] * A(uy, ic, jc, kc) + IC[3] * A(uy, ip, jc, kc);
+                double uy_xp = IC[0] * A(uy, is, jp, kc) + IC[1] * A(uy, im, jp, kc) + IC[2] * A(uy, ic, jp, kc) + IC[3] * A(uy, ip, jp, kc);
+                double uzCell = IC[0] * A(uz, ic, jc, km) + IC[1] * A(uz, ic, jc, kc) + IC[2] * A(uz, ic, jc, kp) + IC[3] * A(uz, ic, jc, ku);
+                double prloc2 = InterpY1 * (IC[0] * A(pr, is, jm, kc) + IC[1] * A(pr, im, jm, kc) + IC[2] * A(pr, ic, jm, kc) + IC[3] * A(pr, ip, jm, kc)) +
+                                InterpY2 * (IC[0] * A(pr, is, jc, kc) + IC[1] * A(pr, im, jc, kc) + IC[2] * A(pr, ic, jc, kc) + IC[3] * A(pr, ip, jc, kc));
+                double dudx = dxC[0] * A(ux, im, jc, kc) + dxC[1] * A(ux, ic, jc, kc) + dxC[2] * A(ux, ip, jc, kc) + dxC[3] * A(ux, iu, jc, kc);
+                double dudy = (A(ux, ic, jc, kc) - A(ux, ic, jm, kc)) * cac;
+                double dudz = dzC[0] * A(ux, ic, jc, ks) + dzC[1] * A(ux, ic, jc, km) + dzC[2] * A(ux, ic, jc, kc) + dzC[3] * A(ux, ic, jc, kp);
+                double dvdx = dxC[0] * A(uy, is, jc, kc) + dxC[1] * A(uy, im, jc, kc) + dxC[2] * A(uy, ic, jc, kc) + dxC[3] * A(uy, ip, jc, kc);
+                double dvdy = (A(uy, ic, jp, kc) - uyloc) * caj;
+                double dvdz = dzC[0] * A(uy, ic, jc, ks) + dzC[1] * A(uy, ic, jc, km) + dzC[2] * A(uy, ic, jc, kc) + dzC[3] * A(uy, ic, jc, kp);
+                double dwdx = dxC[0] * A(uz, is, jc, kc) + dxC[1] * A(uz, im, jc, kc) + dxC[2] * A(uz, ic, jc, kc) + dxC[3] * A(uz, ip, jc, kc);
+                double dwdy = (uzloc - A(uz, ic, jm, kc)) * cac;
+                double dwdz = dzC[0] * A(uz, ic, jc, km) + dzC[1] * A(uz, ic, jc, kc) + dzC[2] * A(uz, ic, jc, kp) + dzC[3] * A(uz, ic, jc, ku);
+                double dudxx = dxxC[0] * A(ux, is, jc, kc) + dxxC[1] * A(ux, im, jc, kc) + dxxC[2] * A(ux, ic, jc, kc) + dxxC[3] * A(ux, ip, jc, kc) + dxxC[4] * A(ux, iu, jc, kc);
+                double dudyy = o->ap2c[jc] * A(ux, ic, jp, kc) + o->ac2c[jc] * A(ux, ic, jc, kc) + o->am2c[jc] * A(ux, ic, jm, kc);
+                double dudzz = dzzC[0] * A(ux, ic, jc, ks) + dzzC[1] * A(ux, ic, jc, km) + dzzC[2] * A(ux, ic, jc, kc) + dzzC[3] * A(ux, ic, jc, kp) + dzzC[4] * A(ux, ic, jc, ku);
+                double dvdxx = dxxC[0] * A(uy, is, jc, kc) + dxxC[1] * A(uy, im, jc, kc) + dxxC[2] * A(uy, ic, jc, kc) + dxxC[3] * A(uy, ip, jc, kc) + dxxC[4] * A(uy, iu, jc, kc);
+                double dvdyy = o->ap2p[jc] * A(uy, ic, jp, kc) + o->ac2p[jc] * A(uy, ic, jc, kc) + o->am2p[jc] * A(uy, ic, jm, kc);
+                double dvdzz = dzzC[0] * A(uy, ic, jc, ks) + dzzC[1] * A(uy, ic, jc, km) + dzzC[2] * A(uy, ic, jc, kc) + dzzC[3] * A(uy, ic, jc, kp) + dzzC[4] * A(uy, ic, jc, ku);
+                double dwdxx = dxxC[0] * A(uz, is, jc, kc) + dxxC[1] * A(uz, im, jc, kc) + dxxC[2] * A(uz, ic, jc, kc) + dxxC[3] * A(uz, ip, jc, kc) + dxxC[4] * A(uz, iu, jc, kc);
+                double dwdyy = o->ap2c[jc] * A(uz, ic, jp, kc) + o->ac2c[jc] * A(uz, ic, jc, kc) + o->am2c[jc] * A(uz, ic, jm, kc);
+                double dwdzz = dzzC[0] * A(uz, ic, jc, ks) + dzzC[1] * A(uz, ic, jc, km) + dzzC[2] * A(uz, ic, jc, kc) + dzzC[3] * A(uz, ic, jc, kp) + dzzC[4] * A(uz, ic, jc, ku);
+                double vor_x = dwdy - dvdz, vor_y = dudz - dwdx, vor_z = dvdx - dudy;
+                double dudxC = (-A(ux, iu, jc, kc) + eight * A(ux, ip, jc, kc) - eight * A(ux, im, jc, kc) + A(ux, is, jc, kc)) * rdxt;
+                double dvdxU = dxC[0] * A(uy, is, jp, kc) + dxC[1] * A(uy, im, jp, kc) + dxC[2] * A(uy, ic, jp, kc) + dxC[3] * A(uy, ip, jp, kc);
+                double dudyU = (A(ux, ic, jp, kc) - A(ux, ic, jc, kc)) * cacU;
+                double dudzC = (InterpY1 * (-A(ux, ic, jm, ku) + eight * A(ux, ic, jm, kp) - eight * A(ux, ic, jm, km) + A(ux, ic, jm, ks)) +
+                                InterpY2 * (-A(ux, ic, jc, ku) + eight * A(ux, ic, jc, kp) - eight * A(ux, ic, jc, km) + A(ux, ic, jc, ks))) * rdzt;
+                double dvdzC = ((-A(uy, is, jc, ku) + eight * A(uy, is, jc, kp) - eight * A(uy, is, jc, km) + A(uy, is, jc, ks)) * IC[0] +
+                                (-A(uy, im, jc, ku) + eight * A(uy, im, jc, kp) - eight * A(uy, im, jc, km) + A(uy, im, jc, ks)) * IC[1] +
+                                (-A(uy, ic, jc, ku) + eight * A(uy, ic, jc, kp) - eight * A(uy, ic, jc, km) + A(uy, ic, jc, ks)) * IC[2] +
+                                (-A(uy, ip, jc, ku) + eight * A(uy, ip, jc, kp) - eight * A(uy, ip, jc, km) + A(uy, ip, jc, ks)) * IC[3]) * rdzt;
+                SumVec[0] += uxloc;
+                SumVec[1] += uyloc;
+                SumVec[2] += uzloc;
+                SumVec[3] += prloc;
+                SumVec[4] += uxloc * uxloc;
+                SumVec[5] += uyloc * uyloc;
+                SumVec[6] += uzloc * uzloc;
+                SumVec[7] += prloc * prloc;
+                SumVec[8] += uxCell * uyCell;
+                SumVec[9] += uyCell * uzCell;
+                SumVec[10] += uxCell * uzCell;
+                SumVec[11] += uxCell * prloc;
+                SumVec[12] += uyCell * prloc;
+                SumVec[13] += uzCell * prloc;
+                SumVec[14] += uxCell * uxCell * uyCell;
+                SumVec[15] += uyloc * uyloc * uyloc;
+                SumVec[16] += uzCell * uzCell * uyCell;
+                SumVec[17] += uxCell * uyCell * uyCell;
+                SumVec[18] += uxloc * uxloc * uxloc;
+                SumVec[19] += uzloc * uzloc * uzloc;
+                SumVec[20] += uxloc * uxloc * uxloc * uxloc;
+                SumVec[21] += uyloc * uyloc * uyloc * uyloc;
+                SumVec[22] += uzloc * uzloc * uzloc * uzloc;
+                SumVec[23] += prloc * dudx;
+                SumVec[24] += prloc * dvdy;
+                SumVec[25] += prloc * dwdz;
+                SumVec[26] += prloc2 * (dudy + dvdx);
+                SumVec[27] += uxloc * (dudxx + dudyy + dudzz);
+                SumVec[28] += uyloc * (dvdxx + dvdyy + dvdzz);
+                SumVec[29] += uzloc * (dwdxx + dwdyy + dwdzz);
+                SumVec[30] += (dudxC * (dvdxU + dvdx) + (dudyU + dudy) * (uy_xp - uy_xc) * caj) * half;
+                SumVec[31] += dudzC * dvdzC;
+                SumVec[32] += vor_x * vor_x;
+                SumVec[33] += vor_y * vor_y;
+                SumVec[34] += vor_z * vor_z;
+                if (nst > 35) {
+                    double scloc = A(sc, ic, jc, kc);
+                    SumVec[35] += scloc;
+                    SumVec[36] += scloc * scloc;
+                    SumVec[37] += scloc * uxCell;
+                    SumVec[38] += scloc * uyCell;
+                    SumVec[39] += scloc * uzCell;
+                }
+            }
+        }
+        for (int q = 0; q < nst; q++) out[(size_t)(jc - 1) * nst + q] = SumVec[q] * inxz;
+    }
+    /* nyp only */
+    {
+        const int jc = nyp, jm = jc - 1;
+        const double cac = o->rdyc[jc];
+        const double InterpY1 = o->yinterp[jc], InterpY2 = one - InterpY1;
+        double SumVec[40];
+        for (int q = 0; q < 40; q++) SumVec[q] = zero;
+        for (int kc = 1; kc <= nzc; kc++)
+            for (int ic = 1; ic <= nxc; ic++) {
+                const int is = ic - 2, im = ic - 1, ip = ic + 1;
+                double prloc2 = InterpY1 * (IC[0] * A(pr, is, jm, kc) + IC[1] * A(pr, im, jm, kc) + IC[2] * A(pr, ic, jm, kc) + IC[3] * A(pr, ip, jm, kc)) +
+                                InterpY2 * (IC[0] * A(pr, is, jc, kc) + IC[1] * A(pr, im, jc, kc) + IC[2] * A(pr, ic, jc, kc) + IC[3] * A(pr, ip, jc, kc));
+                double dudy = (A(ux, ic, jc, kc) - A(ux, ic, jm, kc)) * cac;
+                double dwdy = (A(uz, ic, jc, kc) - A(uz, ic, jm, kc)) * cac;
+                double vor_x = dwdy, vor_z = -dudy;
+                SumVec[26] += prloc2 * (dudy + zero);
+                SumVec[32] += vor_x * vor_x;
+                SumVec[34] += vor_z * vor_z;
+            }
+#undef A
+        for (int q = 0; q < nst; q++) out[(size_t)(jc - 1) * nst + q] = SumVec[q] * inxz;
+    }
+    return 0;
+}
+
+/* ------------------------------------------------------------------------
  * one substep: body of the ns loop of ChannelIterate
  * (src/m_ChannelSystem.f90:102-140)
  * ---------------------------------------------------------------------- */

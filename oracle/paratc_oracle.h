@@ -49,6 +49,8 @@ int  orc_diagnostics(orc_t* o, paratc_diag* diag);
 /* 1D metric arrays by name (e.g. "yp", "ac2ph", "am2cForCN"); returns the
  * number of values written (Fortran index from the array's lower bound). */
 int  orc_metric(orc_t* o, const char* name, double* out, int cap);
+/* clcStat: one call's SumVec*inxz per row jc = 1..nyp (k fastest; 35 or 40) */
+int  orc_stats(orc_t* o, double* out);
 
 /* real DFT helpers in FFTW's halfcomplex convention (for pinning) */
 int  orc_r2hc(int n, const double* in, double* out);

@@ -62,6 +62,9 @@ struct paratc_ctx {
     double* d_hfac = nullptr;           // Helmholtz pivots of the substeps of a step (3 matrix types each)
     double hfac_dt = -1.0;              // the fixed dt d_hfac holds pivots for (iCFL != 1), else < 0
     bool next_ready = false;            // the last step's end kernel already computed this step's dt
+    double* d_stats = nullptr;          // SumStat [nyp][nstat] then PrGradsum (FP64 accumulators)
+    double* d_stats_part = nullptr;     // per-slice partial sums of clcStat
+    int nfstime = 0;                    // statistics steps accumulated
     DDiag* h_diag = nullptr;   // pinned
     DCoef* h_coef = nullptr;   // pinned
     double* h_scal = nullptr;  // pinned
@@ -472,7 +475,9 @@ int paratc_create(const paratc_params* prm, const double* yp, int device, paratc
         (rc = dalloc(ctx, &ctx->d_diag, 1)) || (rc = dalloc(ctx, &ctx->d_diag2, 1)) || (rc = dalloc(ctx, &ctx->d_scal, 16)) ||
         (rc = dalloc(ctx, &ctx->d_counter, 16)) ||
         (rc = dalloc(ctx, &ctx->d_hfac, helm_fac_doubles(ctx->ny))) ||
-        (rc = dalloc(ctx, &ctx->d_pfac, (size_t)2 * ctx->M1 * ctx->nz * ctx->ny))) {
+        (rc = dalloc(ctx, &ctx->d_pfac, (size_t)2 * ctx->M1 * ctx->nz * ctx->ny)) ||
+        (rc = dalloc(ctx, &ctx->d_stats, (size_t)ctx->nyp * 40 + 1)) ||
+        (rc = dalloc(ctx, &ctx->d_stats_part, stats_part_doubles(kc)))) {
         paratc_destroy(ctx);
         return rc;
     }
@@ -812,6 +817,37 @@ int paratc_read_restart(paratc_ctx* ctx, const char* path) {
     int rc = paratc_set_fields(ctx, arr[0].data(), arr[1].data(), arr[2].data(), arr[3].data(), c, hx, hy, hz, hc,
                                PARATC_LAYOUT_INTERIOR);
     return rc;
+}
+
+int paratc_stats_reset(paratc_ctx* ctx) {
+    if (!ctx) return PARATC_ERR_BAD_ARG;
+    CK(cudaSetDevice(ctx->dev));
+    CK(cudaMemsetAsync(ctx->d_stats, 0, ((size_t)ctx->nyp * 40 + 1) * sizeof(double), ctx->st));
+    ctx->nfstime = 0;
+    return sync(ctx);
+}
+
+int paratc_stats_accumulate(paratc_ctx* ctx) {
+    if (!ctx) return PARATC_ERR_BAD_ARG;
+    CK(cudaSetDevice(ctx->dev));
+    const int ns = stats_count(ctx->kc);
+    launch_stats(ctx->st, ctx->kc, ctx->dm, ctx->f, ctx->d_coef, ctx->d_stats_part, ctx->d_stats,
+                 ctx->d_stats + (size_t)ctx->nyp * ns);
+    ctx->launches += 2;
+    ctx->nfstime += 1;
+    CK(cudaGetLastError());
+    return PARATC_OK;
+}
+
+int paratc_stats_get(paratc_ctx* ctx, double* sumstat, int* nstat, int* nfstime, double* prgradsum) {
+    if (!ctx) return PARATC_ERR_BAD_ARG;
+    CK(cudaSetDevice(ctx->dev));
+    const int ns = stats_count(ctx->kc);
+    if (nstat) *nstat = ns;
+    if (nfstime) *nfstime = ctx->nfstime;
+    if (sumstat) CK(cudaMemcpyAsync(sumstat, ctx->d_stats, (size_t)ctx->nyp * ns * sizeof(double), cudaMemcpyDefault, ctx->st));
+    if (prgradsum) CK(cudaMemcpyAsync(prgradsum, ctx->d_stats + (size_t)ctx->nyp * ns, sizeof(double), cudaMemcpyDefault, ctx->st));
+    return sync(ctx);
 }
 
 }  // extern "C"

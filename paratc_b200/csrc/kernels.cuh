@@ -71,6 +71,13 @@ void launch_ysolve(cudaStream_t st, const DConst& c, const DMetric& m, double2* 
 void launch_pois_factors(cudaStream_t st, const DConst& c, const DMetric& m, double* fac);
 void launch_ysolve_fac(cudaStream_t st, const DConst& c, const DMetric& m, double2* spec, const double* fac);
 
+// k_stats.cu: clcStat accumulation
+int stats_count(const DConst& c);
+int stats_splits(const DConst& c);
+size_t stats_part_doubles(const DConst& c);
+void launch_stats(cudaStream_t st, const DConst& c, const DMetric& m, const Fields& f, const DCoef* coef,
+                  double* part, double* sumstat, double* prgradsum);
+
 // k_pfft_x.cu / k_pfft_z.cu: compile-time-length transforms of the Poisson solve
 bool pfft_x_supported(int n);
 bool pfft_z_supported(int n);

@@ -29,7 +29,8 @@ EXPORTED = [
     "paratc_write_restart", "paratc_read_restart", "paratc_strerror", "paratc_last_error", "paratc_launch_count",
     "paratc_profile_enable", "paratc_profile_get", "paratc_profile_name", "paratc_steps_async", "paratc_last_diag",
     "paratc_poisson_noalloc", "paratc_batch_create", "paratc_batch_destroy", "paratc_batch_member",
-    "paratc_batch_steps", "paratc_batch_graph_kernels", "paratc_batch_stream",
+    "paratc_batch_steps", "paratc_batch_graph_kernels", "paratc_batch_stream", "paratc_stats_reset",
+    "paratc_stats_accumulate", "paratc_stats_get",
 ]
 PROF_NKERNELS = 16
 
@@ -96,6 +97,10 @@ def load(path=None):
     L.paratc_batch_steps.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ParatcDiag)]
     L.paratc_batch_graph_kernels.argtypes = [ctypes.c_void_p]
     L.paratc_batch_graph_kernels.restype = ctypes.c_int64
+    L.paratc_stats_reset.argtypes = [ctypes.c_void_p]
+    L.paratc_stats_accumulate.argtypes = [ctypes.c_void_p]
+    L.paratc_stats_get.argtypes = [ctypes.c_void_p, _dp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                                   _dp]
     L.paratc_batch_stream.argtypes = [ctypes.c_void_p]
     L.paratc_batch_stream.restype = ctypes.c_void_p
     _lib = L
@@ -287,6 +292,22 @@ class ChannelSystem:
     def poisson_device_async(self, d_src_ptr, d_phi_ptr):
         self._check(self._L.paratc_poisson_device_async(self._h, ctypes.c_void_p(d_src_ptr), ctypes.c_void_p(d_phi_ptr)),
                     "paratc_poisson_device_async")
+
+    # -- statistics (clcStat)
+    def stats_reset(self):
+        self._check(self._L.paratc_stats_reset(self._h), "paratc_stats_reset")
+
+    def stats_accumulate(self):
+        self._check(self._L.paratc_stats_accumulate(self._h), "paratc_stats_accumulate")
+
+    def stats_get(self):
+        """(SumStat [nyp, nstat], nfstime, PrGradsum)."""
+        nst = 40 if self.params.scalar_on else 35
+        out = np.zeros((self.params.nyc + 1, nst))
+        n, nf, pg = ctypes.c_int(), ctypes.c_int(), ctypes.c_double()
+        self._check(self._L.paratc_stats_get(self._h, _ptr(out), ctypes.byref(n), ctypes.byref(nf), ctypes.byref(pg)),
+                    "paratc_stats_get")
+        return out, nf.value, pg.value
 
     def project(self):
         dm = ctypes.c_double()

@@ -211,3 +211,28 @@ def test_halo_layout_roundtrip():
     ho = o.get_halo("ux")
     inner = (slice(2, -2), slice(1, -1), slice(2, -2))
     assert rel_err(fh["ux"][inner], ho[inner]) < 1e-9
+
+
+@pytest.mark.parametrize("name", ["channel", "channel_odd", "halfchannel_scalar", "channel_scalar_crf"])
+def test_stats_accumulate(name):
+    """clcStat accumulated over two steps on both sides: every moment of every
+    row within 1e-12 of the moment's largest magnitude over the rows."""
+    case = variant(name)
+    o, g, _ = _pair(case)
+    acc = None
+    for _ in range(2):
+        o.step()
+        g.iterate(1, raise_on_guard=False)
+        so = o.stats()
+        acc = so if acc is None else acc + so
+        g.stats_accumulate()
+    sg, nf, pg = g.stats_get()
+    assert nf == 2
+    assert sg.shape == acc.shape
+    for q in range(acc.shape[1]):
+        scale = max(np.abs(acc[:, q]).max(), 1e-300)
+        e = np.abs(sg[:, q] - acc[:, q]).max() / scale
+        assert e <= 1e-12 or scale < 1e-14, "%s moment %d rel err %.3e" % (name, q + 1, e)
+    g.stats_reset()
+    sg, nf, pg = g.stats_get()
+    assert nf == 0 and not sg.any() and pg == 0.0

@@ -208,3 +208,29 @@ def test_oracle_thread_count_invariance():
     ol.set_threads(0)
     for n in ("ux", "uy", "uz", "p", "c"):
         assert np.array_equal(outs[0][n], outs[1][n]), n
+
+
+def test_stats_moments_pinned_by_numpy():
+    """clcStat (src/m_FlowCase.f90:298-384) restated in the oracle: the point
+    moments 1-8, 16, 19-23 are plain x-z means of the staggered values and are
+    recomputed here from the fields; the rest follow the same expressions."""
+    case = variant("channel")
+    yp = yp_of(case)
+    o = ol.Oracle(case.params, yp)
+    f = fields_of(case, yp)
+    o.set_fields(f["ux"], f["uy"], f["uz"], f["p"], f["c"])
+    o.step()
+    s = o.stats()
+    g = o.get_fields()
+    ux = g["ux"] + case.params.ucrf
+    uy, uz, p = g["uy"], g["uz"], g["p"]
+    checks = {0: ux, 1: uy, 2: uz, 3: p, 4: ux * ux, 5: uy * uy, 6: uz * uz, 7: p * p, 15: uy ** 3,
+              18: ux ** 3, 19: uz ** 3, 20: ux ** 4, 21: uy ** 4, 22: uz ** 4}
+    ny = case.params.nyc
+    for q, a in checks.items():
+        ref = a.mean(axis=(0, 2))  # fields are [z, y, x]
+        scale = np.abs(a).mean(axis=(0, 2)).max()  # the v mean is zero up to rounding
+        err = np.abs(s[:ny, q] - ref).max() / scale
+        assert err < 1e-13, (q, err)
+    # the top wall row carries only moments 27, 33 and 35
+    assert np.count_nonzero(s[ny][[q for q in range(35) if q not in (26, 32, 34)]]) == 0
