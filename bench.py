@@ -497,6 +497,14 @@ def run_poisson(args):
     clocks = sampler.stop()
     ms = sum(a.elapsed_time(b) for a, b in evs)
     phi_g = d_phi.cpu().numpy()
+    # per-kernel event times of the same solves
+    ctx.profile(True)
+    for _ in range(args.steps):
+        ctx.poisson_device_async(d_src.data_ptr(), d_phi.data_ptr())
+    torch.cuda.synchronize()
+    prof = ctx.profile_read()
+    ctx.profile(False)
+    kern = {k: round(v[0] / max(v[1], 1) * 1e3, 1) for k, v in prof.items() if v[1] > 0}
     # end to end: host source in, host potential out (paratc_poisson)
     t0 = time.perf_counter()
     for _ in range(args.steps):
@@ -528,7 +536,8 @@ def run_poisson(args):
                            "max_rel_err_vs_oracle": err, "mean_phi_e2e_equal": bool(np.array_equal(phi_h, phi_g))},
                 "roofline": {"bound": "hbm", "kernel": "poisson solve (5 kernels)", "achieved": round(ach, 1),
                              "peak": peak, "unit": "GB/s", "frac": round(ach / peak, 4), "traffic": None,
-                             "peak_kind": peak_kind, "algorithmic_bytes_per_launch": alg},
+                             "peak_kind": peak_kind, "algorithmic_bytes_per_launch": alg,
+                             "kernel_us": kern},
                 "cpu_baseline": base,
                 "e2e": {"value": cells * args.steps / t_e2e, "unit": "grid-point Poisson solves/s",
                         "h2d_bytes_per_step": src.nbytes, "d2h_bytes_per_step": src.nbytes,
