@@ -54,6 +54,7 @@ struct paratc_ctx {
     double *d_metric = nullptr, *d_scal = nullptr;
     double2 *d_spec = nullptr, *d_twx = nullptr, *d_postx = nullptr, *d_twz = nullptr;
     bool pfft = false;   // compile-time-length transforms exist for nx/2 and nz
+    bool plane = false;  // a whole y-plane of the spectrum fits one CTA: fused 2-D transforms
     double* d_pfac = nullptr;   // pivots of the spectral y systems (1/vecm, then arr), computed once
     DCoef* d_coef = nullptr;
     DDiag* d_diag = nullptr;
@@ -163,6 +164,13 @@ std::vector<double2> twiddles(int n, int count) {
 // transform has filled d_spec
 void enqueue_poisson_tail(paratc_ctx* ctx, double* out, int padded) {
     cudaStream_t st = ctx->st;
+    if (ctx->plane) {
+        { PROF(PK_YSOLVE); launch_ysolve_fac(st, ctx->kc, ctx->dm, ctx->d_spec, ctx->d_pfac); }
+        { PROF(PK_FFTX_B); launch_plane_b(st, ctx->nx, ctx->ny, ctx->nz, ctx->d_spec, out, ctx->d_twx, ctx->d_postx,
+                                          ctx->d_twz, ctx->hm.normfft, padded); }
+        ctx->launches += 2;
+        return;
+    }
     if (ctx->pfft) {
         { PROF(PK_FFTZ_F); launch_pfft_z(st, -1, ctx->nx, ctx->ny, ctx->nz, ctx->d_spec, ctx->d_twz); }
         { PROF(PK_YSOLVE); launch_ysolve_fac(st, ctx->kc, ctx->dm, ctx->d_spec, ctx->d_pfac); }
@@ -184,6 +192,13 @@ void enqueue_poisson_tail(paratc_ctx* ctx, double* out, int padded) {
 // (clcPrSrc, max|div| to out_max), 1: unscaled divergence, 2: array src
 void enqueue_poisson_head(paratc_ctx* ctx, int mode, const double* src, double* out_max) {
     cudaStream_t st = ctx->st;
+    if (ctx->plane) {
+        PROF(mode == 2 ? PK_FFTX_F : PK_PRSRC);
+        launch_plane_f(st, mode, ctx->kc, ctx->dm, ctx->d_coef, ctx->f, src, ctx->d_spec, ctx->d_twx, ctx->d_postx,
+                       ctx->d_twz, ctx->d_part, ctx->d_counter + 1, out_max);
+        ctx->launches += 1;
+        return;
+    }
     if (ctx->pfft) {
         PROF(mode == 2 ? PK_FFTX_F : PK_PRSRC);
         launch_pfft_xf(st, mode, ctx->kc, ctx->dm, ctx->d_coef, ctx->f, src, ctx->d_spec, ctx->d_twx, ctx->d_postx,
@@ -417,6 +432,8 @@ int paratc_create(const paratc_params* prm, const double* yp, int device, paratc
         return PARATC_ERR_BAD_ARG;
     }
     ctx->pfft = pfft_x_supported(ctx->nx / 2) && pfft_z_supported(ctx->nz) && std::getenv("PARATC_GENERIC_FFT") == nullptr;
+    // PARATC_NO_PLANE keeps the separate x and z transform kernels (both exact)
+    ctx->plane = ctx->pfft && plane_supported(ctx->nx, ctx->nz) && std::getenv("PARATC_NO_PLANE") == nullptr;
     cudaError_t ce = cudaStreamCreateWithFlags(&ctx->st, cudaStreamNonBlocking);
     if (ce != cudaSuccess) { delete ctx; return PARATC_ERR_CUDA; }
     static bool inited = false;
@@ -426,6 +443,7 @@ int paratc_create(const paratc_params* prm, const double* yp, int device, paratc
         rhs_init();
         pfft_x_init();
         pfft_z_init();
+        plane_init();
         inited = true;
     }
     const HostMetrics& h = ctx->hm;

@@ -19,18 +19,19 @@
 namespace ptc {
 namespace ff {
 
-// radix schedule of N = 2^a 3^b 5^c: the power of two in ceil(a/4) passes of
-// radix <= 16 as even as possible, then radix-3 and radix-5 passes
+// radix schedule of N = 2^a 3^b 5^c: the power of two in ceil(a/maxbits)
+// passes of radix <= 2^maxbits as even as possible, then radix-3 and radix-5
+// passes
 struct Sched {
     int np;
     int r[12];
 };
 
-__host__ __device__ constexpr Sched make_sched(int n) {
+__host__ __device__ constexpr Sched make_sched(int n, int maxbits = 4) {
     Sched s{0, {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0}};
     int a = 0;
     while (n % 2 == 0) { n /= 2; a++; }
-    const int p2 = (a + 3) / 4;
+    const int p2 = (a + maxbits - 1) / maxbits;
     for (int q = 0; q < p2; q++) s.r[s.np++] = 1 << ((a + q) / p2);
     while (n % 3 == 0 && s.np < 12) { n /= 3; s.r[s.np++] = 3; }
     while (n % 5 == 0 && s.np < 12) { n /= 5; s.r[s.np++] = 5; }
@@ -46,8 +47,8 @@ __host__ __device__ constexpr int sched_rmax(int n) {
 }
 
 // product of the radices of passes 0..S-1
-__host__ __device__ constexpr int sched_ns(int n, int S) {
-    const Sched s = make_sched(n);
+__host__ __device__ constexpr int sched_ns(int n, int S, int maxbits = 4) {
+    const Sched s = make_sched(n, maxbits);
     int p = 1;
     for (int q = 0; q < S; q++) p *= s.r[q];
     return p;
@@ -210,16 +211,33 @@ struct SmemSt {
     __device__ __forceinline__ void operator()(int e, int b, double2 v) const { buf[e * PITCH + b] = v; }
 };
 
-// passes S..END-1 in place on shared memory, each followed by a barrier
-template <int N, int B, int PITCH, int P, int DIR, int S, int END>
+// shared-memory accessors with the sequence index major: element e of
+// sequence b at buf[b*PITCH + e]
+template <int PITCH>
+struct SmemLdT {
+    const double2* buf;
+    __device__ __forceinline__ double2 operator()(int e, int b) const { return buf[b * PITCH + e]; }
+};
+template <int PITCH>
+struct SmemStT {
+    double2* buf;
+    __device__ __forceinline__ void operator()(int e, int b, double2 v) const { buf[b * PITCH + e] = v; }
+};
+
+// passes S..END-1 in place on shared memory, each followed by a barrier;
+// TRANSPOSED selects the layout buf[b*PITCH + e] instead of buf[e*PITCH + b]
+template <int N, int B, int PITCH, int P, int DIR, int S, int END, int MAXBITS = 4, bool TRANSPOSED = false>
 __device__ __forceinline__ void smem_passes(double2* buf, const double2* tw, int tid) {
-    constexpr Sched SC = make_sched(N);
+    constexpr Sched SC = make_sched(N, MAXBITS);
     if constexpr (S < END) {
         constexpr int R = SC.r[S];
-        constexpr int NS = sched_ns(N, S);
-        pass<N, B, P, R, NS, DIR, true>(SmemLd<PITCH>{buf}, SmemSt<PITCH>{buf}, tw, tid);
+        constexpr int NS = sched_ns(N, S, MAXBITS);
+        if constexpr (TRANSPOSED)
+            pass<N, B, P, R, NS, DIR, true>(SmemLdT<PITCH>{buf}, SmemStT<PITCH>{buf}, tw, tid);
+        else
+            pass<N, B, P, R, NS, DIR, true>(SmemLd<PITCH>{buf}, SmemSt<PITCH>{buf}, tw, tid);
         __syncthreads();
-        smem_passes<N, B, PITCH, P, DIR, S + 1, END>(buf, tw, tid);
+        smem_passes<N, B, PITCH, P, DIR, S + 1, END, MAXBITS, TRANSPOSED>(buf, tw, tid);
     }
 }
 

@@ -78,6 +78,15 @@ size_t stats_part_doubles(const DConst& c);
 void launch_stats(cudaStream_t st, const DConst& c, const DMetric& m, const Fields& f, const DCoef* coef,
                   double* part, double* sumstat, double* prgradsum);
 
+// k_plane.cu: both transforms of a y-plane in one CTA (planes that fit shared memory)
+bool plane_supported(int nx, int nz);
+void plane_init();
+void launch_plane_f(cudaStream_t st, int mode, const DConst& c, const DMetric& m, const DCoef* coef, const Fields& f,
+                    const double* src, double2* spec, const double2* twx, const double2* post, const double2* twz,
+                    double* part, unsigned int* counter, double* out_max);
+void launch_plane_b(cudaStream_t st, int nx, int ny, int nz, const double2* spec, double* phi, const double2* twx,
+                    const double2* post, const double2* twz, double scale, int padded);
+
 // k_pfft_x.cu / k_pfft_z.cu: compile-time-length transforms of the Poisson solve
 bool pfft_x_supported(int n);
 bool pfft_z_supported(int n);

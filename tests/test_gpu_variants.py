@@ -79,3 +79,20 @@ def test_fixed_length_sizes(dims):
     phi_o = ol.Oracle(case.params, yp).poisson(src)
     phi_g = ChannelSystem(case.params, yp).poisson(src)
     assert rel_err(phi_g, phi_o) <= TOL_POISSON
+
+
+@pytest.mark.parametrize("plane", [True, False])
+@pytest.mark.parametrize("dims", [(64, 24, 64), (96, 20, 96), (128, 96, 128)])
+def test_plane_and_split_transforms(monkeypatch, plane, dims):
+    """The one-CTA-per-plane transforms (k_plane.cu) and the separate x / z
+    kernels on the same grids (plane pairs (32,64), (48,96), (64,128))."""
+    if not plane:
+        monkeypatch.setenv("PARATC_NO_PLANE", "1")
+    case = cases.small_channel(*dims)
+    yp = yp_of(case)
+    src = cases.gaussian_source(cases.Case("src", case.params, case.mesh, "gauss_src", 11, 1.0))
+    phi_o = ol.Oracle(case.params, yp).poisson(src)
+    phi_g = ChannelSystem(case.params, yp).poisson(src)
+    assert rel_err(phi_g, phi_o) <= TOL_POISSON
+    if dims[1] <= 24:
+        _steps_vs_oracle(case, 2)
