@@ -29,7 +29,8 @@ constexpr int SX = TX + 2 * HX;  // 38
 constexpr int SZ = TZ + 2 * HZ;  // 14
 constexpr int SLAB = SX * SZ;    // 532 doubles per field and row
 constexpr int NB = 4;            // ring slots
-constexpr int NTHR = TX * TZ;    // 256
+constexpr int ZC = 2;            // z-adjacent cells per thread: their shared stencil taps are loaded once
+constexpr int NTHR = TX * TZ / ZC;  // 128
 constexpr int NSLOT = (SLAB + NTHR - 1) / NTHR;
 
 __device__ __forceinline__ void cp_async8(double* sdst, const double* gsrc) {
@@ -54,7 +55,7 @@ __global__ void __launch_bounds__(NTHR, 2)
                double* __restrict__ part, unsigned int* __restrict__ counter) {
     constexpr int NF = SCALAR ? 5 : 4;
     extern __shared__ double sm[];  // [NB][NF][SLAB]
-    const int lane = threadIdx.x, w = threadIdx.y, tid = w * 32 + lane;
+    const int lane = threadIdx.x, wq = threadIdx.y, tid = wq * 32 + lane;
     const int nx = c.nx, nz = c.nz, ny = c.ny;
     const size_t pl = (size_t)c.nyt * nx;
     // work = the (tile, row) pairs in tile-major order; block b takes the
@@ -108,34 +109,49 @@ __global__ void __launch_bounds__(NTHR, 2)
         LOAD_ROW(j0 + 1);
         cp_async_commit();
 
-        const int i = i0 + lane, k = k0 + w;
-        const bool act = (i < nx) && (k < nz);
-        if (act && j0 == 1) {
-            const size_t t = (size_t)k * nx + i;
-            const double d = uy_ym[t];
-            uy_ym[t] = 0.0;
-            duy_ym[t] = uy_ym[t] - d;
-        }
+        const int i = i0 + lane;
+        int kk[ZC];
+        bool act[ZC];
         // explicit histories of the next row are loaded one row ahead
-        double hxn = 0.0, hyn = 0.0, hzn = 0.0, hcn = 0.0;
-        if (act) {
-            const size_t q = (size_t)k * pl + (size_t)j0 * nx + i;
-            hxn = fl.hx[q]; hyn = fl.hy[q]; hzn = fl.hz[q];
-            if (SCALAR) hcn = fl.hc[q];
+        double hxn[ZC], hyn[ZC], hzn[ZC], hcn[ZC];
+#pragma unroll
+        for (int cz = 0; cz < ZC; cz++) {
+            kk[cz] = k0 + wq * ZC + cz;
+            act[cz] = (i < nx) && (kk[cz] < nz);
+            if (act[cz] && j0 == 1) {
+                const size_t t = (size_t)kk[cz] * nx + i;
+                const double d = uy_ym[t];
+                uy_ym[t] = 0.0;
+                duy_ym[t] = uy_ym[t] - d;
+            }
+            hxn[cz] = hyn[cz] = hzn[cz] = hcn[cz] = 0.0;
+            if (act[cz]) {
+                const size_t q = (size_t)kk[cz] * pl + (size_t)j0 * nx + i;
+                hxn[cz] = fl.hx[q]; hyn[cz] = fl.hy[q]; hzn[cz] = fl.hz[q];
+                if (SCALAR) hcn[cz] = fl.hc[q];
+            }
         }
 
         for (int j = j0; j <= j1; j++) {
             if (j + 2 <= j1 + 1) LOAD_ROW(j + 2);
             cp_async_commit();
-            const double hx0 = hxn, hy0 = hyn, hz0 = hzn, hc0 = hcn;
-            const size_t q0 = (size_t)k * pl + (size_t)j * nx + i;
-            if (act && j + 1 <= j1) {
-                hxn = fl.hx[q0 + nx]; hyn = fl.hy[q0 + nx]; hzn = fl.hz[q0 + nx];
-                if (SCALAR) hcn = fl.hc[q0 + nx];
+            double hx0a[ZC], hy0a[ZC], hz0a[ZC], hc0a[ZC];
+            size_t q0a[ZC];
+#pragma unroll
+            for (int cz = 0; cz < ZC; cz++) {
+                hx0a[cz] = hxn[cz]; hy0a[cz] = hyn[cz]; hz0a[cz] = hzn[cz]; hc0a[cz] = hcn[cz];
+                q0a[cz] = (size_t)kk[cz] * pl + (size_t)j * nx + i;
+                if (act[cz] && j + 1 <= j1) {
+                    hxn[cz] = fl.hx[q0a[cz] + nx]; hyn[cz] = fl.hy[q0a[cz] + nx]; hzn[cz] = fl.hz[q0a[cz] + nx];
+                    if (SCALAR) hcn[cz] = fl.hc[q0a[cz] + nx];
+                }
             }
             cp_async_wait<1>();
             __syncthreads();
-            if (act) {
+            // both cells are computed before any global store, so that the
+            // compiler may load a tap the two cells share once
+            double o_rx[ZC], o_ry[ZC], o_rz[ZC], o_hx[ZC], o_hy[ZC], o_hz[ZC], o_rc[ZC], o_hc[ZC];
+            {
                 const double* Sm = sm + (size_t)((j - 1) % NB) * NF * SLAB;
                 const double* Sc = sm + (size_t)(j % NB) * NF * SLAB;
                 const double* Sp = sm + (size_t)((j + 1) % NB) * NF * SLAB;
@@ -144,6 +160,11 @@ __global__ void __launch_bounds__(NTHR, 2)
             const double IY1 = __ldg(&m.yinterp[j]), IY2 = 1.0 - IY1;
             const double IY3 = __ldg(&m.yinterp[j + 1]), IY4 = 1.0 - IY3;
             const double rdyp = __ldg(&m.rdyp[j]), rdyc = __ldg(&m.rdyc[j]), dyp = __ldg(&m.dyp[j]);
+#pragma unroll
+            for (int cz = 0; cz < ZC; cz++) {
+            const int w = wq * ZC + cz;
+            const double hx0 = hx0a[cz], hy0 = hy0a[cz], hz0 = hz0a[cz], hc0 = hc0a[cz];
+            (void)hc0;
 
             // ---------------- RhsX (:169-204)
             double conv_x, rhs_x;
@@ -173,7 +194,7 @@ __global__ void __launch_bounds__(NTHR, 2)
                 const double d22 = __ldg(&m.ap2c[j]) * uxjp + __ldg(&m.ac2c[j]) * uxc + __ldg(&m.am2c[j]) * uxjm;
                 const double d33 = c.dzzC[0] * V(Sc, 0, 0, -2) + c.dzzC[1] * V(Sc, 0, 0, -1) + c.dzzC[2] * uxc + c.dzzC[3] * V(Sc, 0, 0, 1) + c.dzzC[4] * V(Sc, 0, 0, 2);
                 const double dcq13 = d11 + d33;
-                s3 += SCALAR ? uxc * dyp : (dcq13 + d22) * dyp;
+                if (act[cz]) s3 += SCALAR ? uxc * dyp : (dcq13 + d22) * dyp;
                 conv_x = -h11 - h12 - h13 + xnu * dcq13 + c.grav[0];
                 const double gradp = c.dxC[0] * V(Sc, 3, -2, 0) + c.dxC[1] * V(Sc, 3, -1, 0) + c.dxC[2] * V(Sc, 3, 0, 0) + c.dxC[3] * V(Sc, 3, 1, 0);
                 rhs_x = pmGamma * conv_x + pmTheta * hx0 - pmAlpha * gradp + tb * d22;
@@ -258,17 +279,29 @@ __global__ void __launch_bounds__(NTHR, 2)
                 const double d22 = __ldg(&m.ap2cSc[j]) * scjp + __ldg(&m.ac2cSc[j]) * scc + __ldg(&m.am2cSc[j]) * scjm;
                 const double d33 = c.dzzC[0] * V(Sc, 4, 0, -2) + c.dzzC[1] * V(Sc, 4, 0, -1) + c.dzzC[2] * scc + c.dzzC[3] * V(Sc, 4, 0, 1) + c.dzzC[4] * V(Sc, 4, 0, 2);
                 const double convc = -hc1 - hc2 - hc3 + c.sdiff * (d11 + d33);
-                fl.rc[q0] = pmGamma * convc + pmTheta * hc0 + tbs * d22;
-                fl.hc[q0] = convc;
+                o_rc[cz] = pmGamma * convc + pmTheta * hc0 + tbs * d22;
+                o_hc[cz] = convc;
             }
 #undef V
-            fl.rx[q0] = rhs_x;
-            fl.ry[q0] = rhs_y;
-            fl.rz[q0] = rhs_z;
-            fl.hx[q0] = conv_x;
-            fl.hy[q0] = conv_y;
-            fl.hz[q0] = conv_z;
-        }
+            o_rx[cz] = rhs_x; o_ry[cz] = rhs_y; o_rz[cz] = rhs_z;
+            o_hx[cz] = conv_x; o_hy[cz] = conv_y; o_hz[cz] = conv_z;
+            }
+            }
+#pragma unroll
+            for (int cz = 0; cz < ZC; cz++) {
+                if (!act[cz]) continue;
+                const size_t q0 = q0a[cz];
+                fl.rx[q0] = o_rx[cz];
+                fl.ry[q0] = o_ry[cz];
+                fl.rz[q0] = o_rz[cz];
+                fl.hx[q0] = o_hx[cz];
+                fl.hy[q0] = o_hy[cz];
+                fl.hz[q0] = o_hz[cz];
+                if (SCALAR) {
+                    fl.rc[q0] = o_rc[cz];
+                    fl.hc[q0] = o_hc[cz];
+                }
+            }
         __syncthreads();
         }
 #undef LOAD_ROW
@@ -337,7 +370,7 @@ void launch_rhs_tile(cudaStream_t st, const DConst& c, const DMetric& m, DCoef* 
                      double* duy_ym, int ns, double gam, double the, double alp, double* part, unsigned int* counter) {
     const int yc = rhs_ychunk(c);
     dim3 grd((unsigned)rhs_grid_blocks(c));
-    dim3 blk(32, TZ);
+    dim3 blk(32, TZ / ZC);
     if (c.scalar_on)
         launch_pdl(k_rhs_tile<true>, grd, blk, NB * 5 * SLAB * 8, st, c, m, coef, f, uy_ym, duy_ym, ns, gam, the, alp,
                    yc, part, counter);

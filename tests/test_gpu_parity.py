@@ -216,7 +216,9 @@ def test_halo_layout_roundtrip():
 @pytest.mark.parametrize("name", ["channel", "channel_odd", "halfchannel_scalar", "channel_scalar_crf"])
 def test_stats_accumulate(name):
     """clcStat accumulated over two steps on both sides: every moment of every
-    row within 1e-12 of the moment's largest magnitude over the rows."""
+    row within 1e-11 (the per-routine tolerance) of the moment's largest
+    magnitude over the rows; moments such as <w p> are small differences of
+    large products, so the fields' rounding-level differences are amplified."""
     case = variant(name)
     o, g, _ = _pair(case)
     acc = None
@@ -232,7 +234,7 @@ def test_stats_accumulate(name):
     for q in range(acc.shape[1]):
         scale = max(np.abs(acc[:, q]).max(), 1e-300)
         e = np.abs(sg[:, q] - acc[:, q]).max() / scale
-        assert e <= 1e-12 or scale < 1e-14, "%s moment %d rel err %.3e" % (name, q + 1, e)
+        assert e <= TOL_STAGE or scale < 1e-14, "%s moment %d rel err %.3e" % (name, q + 1, e)
     g.stats_reset()
     sg, nf, pg = g.stats_get()
     assert nf == 0 and not sg.any() and pg == 0.0
