@@ -175,6 +175,19 @@ int paratc_get_fields_device(paratc_ctx* ctx, double* ux, double* uy, double* uz
                              double* p, double* c, double* hx, double* hy,
                              double* hz, double* hc);
 
+/* Asynchronous forms: the copies (and the boundary / ghost refresh of
+ * set_fields) are queued on the context's stream and the call returns at
+ * once; the host arrays must stay valid, and should be page-locked, until
+ * paratc_sync (or a synchronous call) returns.  Independent contexts used this
+ * way overlap one context's transfers with another's steps. */
+int paratc_set_fields_async(paratc_ctx* ctx, const double* ux, const double* uy, const double* uz,
+                            const double* p, const double* c, const double* hx, const double* hy,
+                            const double* hz, const double* hc, int layout);
+int paratc_get_fields_async(paratc_ctx* ctx, double* ux, double* uy, double* uz, double* p, double* c,
+                            double* hx, double* hy, double* hz, double* hc, int layout);
+/* Waits for everything queued on the context's stream. */
+int paratc_sync(paratc_ctx* ctx);
+
 /* SimTime and dt of the context (m_Parameters globals).  After a step,
  * paratc_get_time reports the dt that step used (the device already holds
  * the next step's dt, computed from the same velocity by the step's end

@@ -68,6 +68,7 @@ struct paratc_ctx {
     int nfstime = 0;                    // statistics steps accumulated
     DDiag* h_diag = nullptr;   // pinned
     DCoef* h_coef = nullptr;   // pinned
+    DCoef* h_coef0 = nullptr;  // pinned, the coefficient block of a freshly loaded state (never rewritten)
     double* h_scal = nullptr;  // pinned
     std::string err;
     int64_t launches = 0;
@@ -314,18 +315,13 @@ int copy_field(paratc_ctx* ctx, double* dev, const double* host_src, double* hos
     return PARATC_OK;
 }
 
-int load_state_common(paratc_ctx* ctx) {
+int load_state_common(paratc_ctx* ctx, bool wait) {
     // ChannelInitialize after read_restart (src/m_ChannelSystem.f90:63-68)
     launch_update_uy_ym(ctx->st, ctx->nx * ctx->nz, ctx->d_uy_ym, ctx->d_duy_ym);
-    DCoef c0;
-    std::memset(&c0, 0, sizeof(c0));
-    c0.dt = ctx->prm.dt_max;
-    c0.sim_time = 0.0;
-    *ctx->h_coef = c0;
-    CK(cudaMemcpyAsync(ctx->d_coef, ctx->h_coef, sizeof(DCoef), cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaMemcpyAsync(ctx->d_coef, ctx->h_coef0, sizeof(DCoef), cudaMemcpyHostToDevice, ctx->st));
     launch_bc_all(ctx->st, ctx->kc, ctx->f, ctx->d_uy_ym);
     ctx->launches += 2;
-    return sync(ctx);
+    return wait ? sync(ctx) : PARATC_OK;
 }
 
 }  // namespace
@@ -388,6 +384,7 @@ int paratc_destroy(paratc_ctx* ctx) {
     for (void* p : ctx->allocs) cudaFree(p);
     if (ctx->h_diag) cudaFreeHost(ctx->h_diag);
     if (ctx->h_coef) cudaFreeHost(ctx->h_coef);
+    if (ctx->h_coef0) cudaFreeHost(ctx->h_coef0);
     if (ctx->h_scal) cudaFreeHost(ctx->h_scal);
     if (ctx->st) cudaStreamDestroy(ctx->st);
     delete ctx;
@@ -542,20 +539,24 @@ int paratc_create(const paratc_params* prm, const double* yp, int device, paratc
     }
     CK(cudaMallocHost(&ctx->h_diag, sizeof(DDiag)));
     CK(cudaMallocHost(&ctx->h_coef, sizeof(DCoef)));
+    CK(cudaMallocHost(&ctx->h_coef0, sizeof(DCoef)));
+    std::memset(ctx->h_coef0, 0, sizeof(DCoef));
+    ctx->h_coef0->dt = ctx->prm.dt_max;
     CK(cudaMallocHost(&ctx->h_scal, 16 * sizeof(double)));
     // AllocateVariables: scalar = Scalar_InitValue everywhere (src/m_Variables.f90:84)
     if (prm->scalar_on) {
         std::vector<double> init(nf, prm->scalar_init_value);
         CK(cudaMemcpy(f.sc, init.data(), nf * sizeof(double), cudaMemcpyHostToDevice));
     }
-    rc = load_state_common(ctx);
+    rc = load_state_common(ctx, true);
     if (rc != PARATC_OK) { paratc_destroy(ctx); return rc; }
     *out = ctx;
     return PARATC_OK;
 }
 
-int paratc_set_fields(paratc_ctx* ctx, const double* ux, const double* uy, const double* uz, const double* p,
-                      const double* c, const double* hx, const double* hy, const double* hz, const double* hc, int layout) {
+static int set_fields_impl(paratc_ctx* ctx, const double* ux, const double* uy, const double* uz, const double* p,
+                           const double* c, const double* hx, const double* hy, const double* hz, const double* hc,
+                           int layout, bool wait) {
     if (!ctx || (layout != PARATC_LAYOUT_INTERIOR && layout != PARATC_LAYOUT_HALO)) return PARATC_ERR_BAD_ARG;
     CK(cudaSetDevice(ctx->dev));
     ctx->next_ready = false;
@@ -571,11 +572,22 @@ int paratc_set_fields(paratc_ctx* ctx, const double* ux, const double* uy, const
             CK(cudaMemsetAsync(t.d, 0, ctx->nf * sizeof(double), ctx->st));
         }
     }
-    return load_state_common(ctx);
+    return load_state_common(ctx, wait);
 }
 
-int paratc_get_fields(paratc_ctx* ctx, double* ux, double* uy, double* uz, double* p, double* c, double* hx, double* hy,
-                      double* hz, double* hc, int layout) {
+int paratc_set_fields(paratc_ctx* ctx, const double* ux, const double* uy, const double* uz, const double* p,
+                      const double* c, const double* hx, const double* hy, const double* hz, const double* hc, int layout) {
+    return set_fields_impl(ctx, ux, uy, uz, p, c, hx, hy, hz, hc, layout, true);
+}
+
+int paratc_set_fields_async(paratc_ctx* ctx, const double* ux, const double* uy, const double* uz, const double* p,
+                            const double* c, const double* hx, const double* hy, const double* hz, const double* hc,
+                            int layout) {
+    return set_fields_impl(ctx, ux, uy, uz, p, c, hx, hy, hz, hc, layout, false);
+}
+
+static int get_fields_impl(paratc_ctx* ctx, double* ux, double* uy, double* uz, double* p, double* c, double* hx,
+                           double* hy, double* hz, double* hc, int layout, bool wait) {
     if (!ctx || (layout != PARATC_LAYOUT_INTERIOR && layout != PARATC_LAYOUT_HALO)) return PARATC_ERR_BAD_ARG;
     CK(cudaSetDevice(ctx->dev));
     struct { double* d; double* h; } tab[] = {{ctx->f.ux, ux}, {ctx->f.uy, uy}, {ctx->f.uz, uz}, {ctx->f.pr, p},
@@ -585,6 +597,22 @@ int paratc_get_fields(paratc_ctx* ctx, double* ux, double* uy, double* uz, doubl
         int rc = copy_field(ctx, t.d, nullptr, t.h, layout, false);
         if (rc) return rc;
     }
+    return wait ? sync(ctx) : PARATC_OK;
+}
+
+int paratc_get_fields(paratc_ctx* ctx, double* ux, double* uy, double* uz, double* p, double* c, double* hx, double* hy,
+                      double* hz, double* hc, int layout) {
+    return get_fields_impl(ctx, ux, uy, uz, p, c, hx, hy, hz, hc, layout, true);
+}
+
+int paratc_get_fields_async(paratc_ctx* ctx, double* ux, double* uy, double* uz, double* p, double* c, double* hx,
+                            double* hy, double* hz, double* hc, int layout) {
+    return get_fields_impl(ctx, ux, uy, uz, p, c, hx, hy, hz, hc, layout, false);
+}
+
+int paratc_sync(paratc_ctx* ctx) {
+    if (!ctx) return PARATC_ERR_BAD_ARG;
+    CK(cudaSetDevice(ctx->dev));
     return sync(ctx);
 }
 

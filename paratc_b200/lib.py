@@ -30,7 +30,8 @@ EXPORTED = [
     "paratc_profile_enable", "paratc_profile_get", "paratc_profile_name", "paratc_steps_async", "paratc_last_diag",
     "paratc_poisson_noalloc", "paratc_batch_create", "paratc_batch_destroy", "paratc_batch_member",
     "paratc_batch_steps", "paratc_batch_graph_kernels", "paratc_batch_stream", "paratc_stats_reset",
-    "paratc_stats_accumulate", "paratc_stats_get",
+    "paratc_stats_accumulate", "paratc_stats_get", "paratc_set_fields_async", "paratc_get_fields_async",
+    "paratc_sync",
 ]
 PROF_NKERNELS = 16
 
@@ -60,6 +61,9 @@ def load(path=None):
     L.paratc_stream.restype = ctypes.c_void_p
     L.paratc_set_fields.argtypes = [ctypes.c_void_p] + [_dp] * 9 + [ctypes.c_int]
     L.paratc_get_fields.argtypes = [ctypes.c_void_p] + [_dp] * 9 + [ctypes.c_int]
+    L.paratc_set_fields_async.argtypes = [ctypes.c_void_p] + [_dp] * 9 + [ctypes.c_int]
+    L.paratc_get_fields_async.argtypes = [ctypes.c_void_p] + [_dp] * 9 + [ctypes.c_int]
+    L.paratc_sync.argtypes = [ctypes.c_void_p]
     L.paratc_set_fields_device.argtypes = [ctypes.c_void_p] + [ctypes.c_void_p] * 9
     L.paratc_get_fields_device.argtypes = [ctypes.c_void_p] + [ctypes.c_void_p] * 9
     L.paratc_set_time.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double]
@@ -230,6 +234,23 @@ class ChannelSystem:
         """Copies the fields named in `out` into its (C-contiguous float64) arrays."""
         ptrs = [_ptr(out[n]) if n in out and out[n] is not None else None for n in self.FIELDS]
         self._check(self._L.paratc_get_fields(self._h, *ptrs, int(layout)), "paratc_get_fields")
+
+    def set_fields_async(self, ux, uy, uz, p, c=None, hx=None, hy=None, hz=None, hc=None):
+        """Queues the copies; the (C-contiguous float64, ideally pinned) arrays
+        must stay alive until sync()."""
+        arrs = [None if a is None else a for a in (ux, uy, uz, p, c, hx, hy, hz, hc)]
+        for a in arrs:
+            if a is not None and not (a.flags.c_contiguous and a.dtype == np.float64 and a.shape == self.shape):
+                raise ValueError("set_fields_async needs C-contiguous float64 arrays of shape %s" % (self.shape,))
+        self._check(self._L.paratc_set_fields_async(self._h, *[_ptr(a) for a in arrs], LAYOUT_INTERIOR),
+                    "paratc_set_fields_async")
+
+    def get_fields_into_async(self, out):
+        ptrs = [_ptr(out[n]) if n in out and out[n] is not None else None for n in self.FIELDS]
+        self._check(self._L.paratc_get_fields_async(self._h, *ptrs, LAYOUT_INTERIOR), "paratc_get_fields_async")
+
+    def sync(self):
+        self._check(self._L.paratc_sync(self._h), "paratc_sync")
 
     def set_time(self, sim_time, dt):
         self._check(self._L.paratc_set_time(self._h, float(sim_time), float(dt)), "paratc_set_time")

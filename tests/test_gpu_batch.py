@@ -77,3 +77,29 @@ def test_batch_members_are_contexts():
         s.iterate(2)
     _same(b, singles)
     b.close()
+
+
+def test_async_transfers_equal_sync():
+    """paratc_set_fields_async / steps_async / get_fields_async on pinned
+    buffers give the fields of the synchronous calls."""
+    import torch
+
+    case = cases.small_channel(32, 24, 16)
+    yp = yp_of(case)
+    f = fields_of(case, yp)
+    a = ChannelSystem(case.params, yp)
+    s = ChannelSystem(case.params, yp)
+    pin = {n: torch.empty(a.shape, dtype=torch.float64, pin_memory=True).numpy() for n in ("ux", "uy", "uz", "p")}
+    for n in pin:
+        pin[n][...] = f[n]
+    for _ in range(3):
+        a.set_fields_async(pin["ux"], pin["uy"], pin["uz"], pin["p"])
+        a.iterate_async(1)
+        a.get_fields_into_async(pin)
+        a.sync()
+        s.set_fields(f["ux"], f["uy"], f["uz"], f["p"])
+        s.iterate(1)
+        f = s.get_fields()
+        for n in pin:
+            assert np.array_equal(pin[n], f[n]), n
+    a.last_diag()
