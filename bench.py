@@ -151,10 +151,8 @@ class ClockSampler:
 
 
 def _dist():
-    ws = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return ws, rank, local
+    from paratc_b200.replicas import dist_env
+    return dist_env()
 
 
 def cpu_baseline(case, yp, fields, seconds, max_steps=200):
@@ -216,15 +214,12 @@ def run_ours(args):
     import torch
     ws, rank, local = _dist()
     torch.cuda.set_device(local)
-    dist = None
-    if ws > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    from paratc_b200 import replicas
+    dist = replicas.init("nccl")
     from paratc_b200 import cases
     from paratc_b200.lib import ChannelSystem, mesh_ycoord
     case = _case(args.workload)
-    case.seed = case.seed + rank
+    case.seed = replicas.replica_seed(case.seed, rank)
     p = case.params
     yp = mesh_ycoord(case.mesh, p.yly)
     fields = cases.initial_fields(case, yp)
@@ -275,11 +270,7 @@ def run_ours(args):
     ms, diag, launches, _ = timed_pass(False)
     clocks = sampler.stop()
     barrier()
-    total_ms = sum(ms)
-    if dist is not None:
-        t = torch.tensor([total_ms], dtype=torch.float64, device=local)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = replicas.max_over_ranks(sum(ms), dist, device=local)
     value = ws * p.nxc * p.nyc * p.nzc * iad * args.steps / (total_ms / 1e3)
 
     # per-kernel timing pass (same workload, events around every launch)
@@ -313,10 +304,7 @@ def run_ours(args):
             ctx.iterate(1)
             ctx.get_fields_into(host)
             t_e2e += time.perf_counter() - t0
-        if dist is not None:
-            t = torch.tensor([t_e2e], dtype=torch.float64, device=local)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            t_e2e = float(t.item())
+        t_e2e = replicas.max_over_ranks(t_e2e, dist, device=local)
         e2e = {"value": ws * p.nxc * p.nyc * p.nzc * iad * args.steps / t_e2e, "unit": UNIT,
                "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes + 12 * 8,
                "note": "per step: paratc_set_fields (%s from pinned host) + paratc_step + paratc_get_fields (same to host)"
@@ -364,14 +352,11 @@ def run_ensemble(args):
     import torch
     ws, rank, local = _dist()
     torch.cuda.set_device(local)
-    dist = None
-    if ws > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    from paratc_b200 import replicas
+    dist = replicas.init("nccl")
     from paratc_b200 import cases
     from paratc_b200.lib import BatchSystem, mesh_ycoord
-    cs = cases.ensemble_c4(seed=2024 + rank)
+    cs = cases.ensemble_c4(seed=replicas.replica_seed(2024, rank))
     yps = [mesh_ycoord(c.mesh, c.params.yly) for c in cs]
     b = BatchSystem([c.params for c in cs], yps, device=local)
     cells = 0
@@ -398,11 +383,7 @@ def run_ensemble(args):
     e1.record(stream)
     torch.cuda.synchronize()
     clocks = sampler.stop()
-    ms = e0.elapsed_time(e1)
-    if dist is not None:
-        t = torch.tensor([ms], dtype=torch.float64, device=local)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = replicas.max_over_ranks(e0.elapsed_time(e1), dist, device=local)
     value = ws * cells * 3 * args.steps / (ms / 1e3)
     # the same members one at a time, each alone on the GPU
     seq_ms = 0.0
