@@ -309,6 +309,28 @@ int paratc_stats_accumulate(paratc_ctx* ctx);
  * PrGradsum. */
 int paratc_stats_get(paratc_ctx* ctx, double* sumstat, int* nstat, int* nfstime, double* prgradsum);
 
+/* ---- 1-D spectra (clcStat's spectra section, src/m_FlowCase.f90:430-806,
+ * with clcEnergySpectraX/Z, clcLTS_x/z_real/imag and clcCospectraX/Z at
+ * :954-1180).  FP64 accumulators on the device, EnergySpecX(kx, jc, m) and
+ * EnergySpecZ(kz, jc, m), m = 1..8 (9 with the scalar) in the reference's
+ * order: ux+uCRF, uy, uz, p, the cospectra <ux uy_c> and <ux_c uy_c> (uy and
+ * ux interpolated to the cell centre), the real and imaginary linear
+ * coherence spectrum of ux against the row jForLCS (mirrored to
+ * nyc+1-jForLCS in the upper half of a channel) [, scalar].  One accumulate
+ * call is one spectra step of the reference (every ivSpec steps, :431) and
+ * adds EgyX*normEgy and EgyZ*normEgy; nSpectime counts the calls.  nx and nz
+ * must be lengths the transform kernels are built for (2^a 3^b 5^c, listed
+ * in k_spectra.cu), else PARATC_ERR_BAD_ARG.  The accumulators are created
+ * and zeroed on first use. */
+int paratc_spectra_reset(paratc_ctx* ctx);
+/* jlcs: jForLCS of &SpectraOptions, 1..nyc. */
+int paratc_spectra_accumulate(paratc_ctx* ctx, int jlcs);
+/* spec_x[(m-1)*nyc*(nxc/2+1) + (jc-1)*(nxc/2+1) + kx] (the reference's
+ * Fortran order of EnergySpecX(nxhp, nyc, m)), spec_z likewise with nzc/2+1
+ * modes; either may be NULL.  nspec: 8 or 9; nspectime: samples summed (the
+ * reference divides by it when it writes SpecX/SpecZ, :841-884). */
+int paratc_spectra_get(paratc_ctx* ctx, double* spec_x, double* spec_z, int* nspec, int* nspectime);
+
 /* ---- Ensembles.  No counterpart in the reference, which advances one case
  * per MPI job; this is the batched form of ChannelIterate
  * (src/m_ChannelSystem.f90:119-226) for many independent channel instances of

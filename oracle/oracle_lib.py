@@ -49,6 +49,7 @@ def lib():
         L.orc_diagnostics.argtypes = [ctypes.c_void_p, ctypes.POINTER(ParatcDiag)]
         L.orc_metric.argtypes = [ctypes.c_void_p, ctypes.c_char_p, _dp, ctypes.c_int]
         L.orc_stats.argtypes = [ctypes.c_void_p, _dp]
+        L.orc_spectra.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, _dp]
         L.orc_r2hc.argtypes = [ctypes.c_int, _dp, _dp]
         L.orc_hc2r.argtypes = [ctypes.c_int, _dp, _dp]
         L.orc_ycoord.argtypes = [ctypes.c_int, _dp, _dp, ctypes.POINTER(ctypes.c_int32),
@@ -215,6 +216,19 @@ class Oracle:
         if rc != 0:
             raise RuntimeError("orc_stats rc=%d" % rc)
         return out
+
+    def spectra(self, jlcs):
+        """clcStat's 1-D spectra of the current fields (one sample, already
+        times normEgy): (x spectra [nsp, nyc, nxc/2+1], z spectra [nsp, nyc,
+        nzc/2+1]), nsp = 8, or 9 with the scalar."""
+        p = self.params
+        nsp = 9 if p.scalar_on else 8
+        ex = np.zeros((nsp, p.nyc, p.nxc // 2 + 1))
+        ez = np.zeros((nsp, p.nyc, p.nzc // 2 + 1))
+        rc = lib().orc_spectra(self._h, int(jlcs), _ptr(ex), _ptr(ez))
+        if rc != 0:
+            raise RuntimeError("orc_spectra rc=%d" % rc)
+        return ex, ez
 
     def metric(self, name):
         buf = np.empty(max(self.params.nxc, self.params.nyc, self.params.nzc) + 8)

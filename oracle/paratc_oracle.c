@@ -1285,6 +1285,129 @@ int orc_stats(orc_t* o, double* out) {
 }
 
 /* ------------------------------------------------------------------------
+ * 1-D spectra of clcStat (src/m_FlowCase.f90:430-806) with the helpers
+ * clcEnergySpectraX/Z, clcLTS_x/z_real, clcLTS_x/z_imag and clcCospectraX/Z
+ * (:954-1180), on halfcomplex rows h[0..n-1].  Index a = ic-1 of the
+ * Fortran arrays; the mirror icCnter = n+2-ic is c = n-a.
+ * ---------------------------------------------------------------------- */
+static void spec_energy(int n, const double* h, double* E) {        /* :954-977 */
+    const int nh = n / 2;
+    E[0] = E[0] + h[0] * h[0];
+    E[nh] = E[nh] + h[nh] * h[nh];
+    for (int a = 1; a < nh; a++) {
+        const int c = n - a;
+        E[a] = E[a] + (h[a] * h[a] + h[c] * h[c]) * two;
+    }
+}
+static void spec_cos(int n, const double* h, const double* g, double* E) {   /* :1032-1055 */
+    const int nh = n / 2;
+    E[0] = E[0] + h[0] * g[0];
+    E[nh] = E[nh] + h[nh] * g[nh];
+    for (int a = 1; a < nh; a++) {
+        const int c = n - a;
+        E[a] = E[a] + (h[a] * g[a] + h[c] * g[c]) * two;
+    }
+}
+/* clcLTS_real on the product array P[a] = h[a]*r[a] (:471-510, :982-1003) */
+static void spec_lcs_real(int n, const double* h, const double* r, double* E) {
+    const int nh = n / 2;
+    E[0] = E[0] + h[0] * r[0];
+    E[nh] = E[nh] + h[nh] * r[nh];
+    for (int a = 1; a < nh; a++) {
+        const int c = n - a;
+        E[a] = E[a] + (h[a] * r[a] + h[c] * r[c]);
+    }
+}
+/* clcLTS_imag on Q[a] = h[n-a]*r[a] (the swapped row of :513-520 times the
+ * reference plane, :521-545, :1008-1027); the two end modes stay zero */
+static void spec_lcs_imag(int n, const double* h, const double* r, double* E) {
+    const int nh = n / 2;
+    E[0] = zero;
+    E[nh] = zero;
+    for (int a = 1; a < nh; a++) {
+        const int c = n - a;
+        E[a] = E[a] + (h[c] * r[a] - h[a] * r[c]);
+    }
+}
+
+/* one row of every field along the transform direction: r[0] ux+uCRF, r[1]
+ * ux+uCRF on the LCS reference row, r[2] uy, r[3] uz, r[4] p, r[5] uy at the
+ * cell centre, r[6] ux at the cell centre (+uCRF), r[7] the scalar (or 0);
+ * E[m][a] gets spectrum m+1 of the reference's numbering */
+static void spec_rows(const fftplan* pl, int n, double* const* r, double* const* h, cplx* z, int nsp, int nhp,
+                      double* E) {
+    r2hc_pair(pl, r[0], r[1], h[0], h[1], z, z + n);
+    r2hc_pair(pl, r[2], r[3], h[2], h[3], z, z + n);
+    r2hc_pair(pl, r[4], r[5], h[4], h[5], z, z + n);
+    r2hc_pair(pl, r[6], r[7], h[6], h[7], z, z + n);
+    spec_energy(n, h[0], E + 0 * nhp);
+    spec_lcs_real(n, h[0], h[1], E + 6 * nhp);
+    spec_lcs_imag(n, h[0], h[1], E + 7 * nhp);
+    spec_energy(n, h[2], E + 1 * nhp);
+    spec_energy(n, h[3], E + 2 * nhp);
+    spec_energy(n, h[4], E + 3 * nhp);
+    spec_cos(n, h[0], h[5], E + 4 * nhp);
+    spec_cos(n, h[6], h[5], E + 5 * nhp);
+    if (nsp > 8) spec_energy(n, h[7], E + 8 * nhp);
+}
+
+int orc_spectra(orc_t* o, int jlcs, double* egx, double* egz) {
+    if (!o || !egx || !egz || jlcs < 1 || jlcs > o->nyc) return PARATC_ERR_BAD_ARG;
+    const int nxc = o->nxc, nyc = o->nyc, nzc = o->nzc;
+    const int nsp = o->p.scalar_on ? 9 : 8;
+    const int nxhp = nxc / 2 + 1, nzhp = nzc / 2 + 1;
+    const double *ux = o->ux, *uy = o->uy, *uz = o->uz, *pr = o->pr, *sc = o->sc, *IC = o->IC;
+    const double uCRF = o->p.ucrf;
+    const int is_hc = (o->p.flow_type == PARATC_FT_HC);
+    upd_halo(o, o->ux, 2, 2, 2, 2);
+    const double normx = one / ((double)nxc * (double)nxc * (double)nzc);
+    const double normz = one / ((double)nxc * (double)nzc * (double)nzc);
+    for (int dir = 0; dir < 2; dir++) {
+        const int n = dir == 0 ? nxc : nzc, nhp = dir == 0 ? nxhp : nzhp, nl = dir == 0 ? nzc : nxc;
+        const fftplan* pl = dir == 0 ? &o->px : &o->pz;
+        double* out = dir == 0 ? egx : egz;
+        const double norm = dir == 0 ? normx : normz;
+#pragma omp parallel
+        {
+            double* wk = (double*)malloc(sizeof(double) * (16 * (size_t)n + 9 * (size_t)nhp));
+            cplx* z = (cplx*)malloc(sizeof(cplx) * 2 * (size_t)n);
+            double *r[8], *h[8];
+            for (int q = 0; q < 8; q++) { r[q] = wk + (size_t)q * n; h[q] = wk + (size_t)(8 + q) * n; }
+            double* E = wk + 16 * (size_t)n;
+#pragma omp for schedule(static)
+            for (int jc = 1; jc <= nyc; jc++) {
+                const int jr = (is_hc || jc <= nyc / 2) ? jlcs : nyc + 1 - jlcs;
+                for (int q = 0; q < 9 * nhp; q++) E[q] = zero;
+                for (int l = 1; l <= nl; l++) {
+                    for (int e = 1; e <= n; e++) {
+                        const int ic = dir == 0 ? e : l, kc = dir == 0 ? l : e;
+                        const int im = ic - 1, ip = ic + 1, iu = ic + 2;
+#define A(a, i, j, k) (a)[HX(o, i, j, k)]
+                        r[0][e - 1] = A(ux, ic, jc, kc) + uCRF;
+                        r[1][e - 1] = A(ux, ic, jr, kc) + uCRF;
+                        r[2][e - 1] = A(uy, ic, jc, kc);
+                        r[3][e - 1] = A(uz, ic, jc, kc);
+                        r[4][e - 1] = A(pr, ic, jc, kc);
+                        r[5][e - 1] = half * (A(uy, ic, jc, kc) + A(uy, ic, jc + 1, kc));
+                        r[6][e - 1] = IC[0] * A(ux, im, jc, kc) + IC[1] * A(ux, ic, jc, kc) + IC[2] * A(ux, ip, jc, kc) +
+                                      IC[3] * A(ux, iu, jc, kc) + uCRF;
+                        r[7][e - 1] = nsp > 8 ? A(sc, ic, jc, kc) : zero;
+#undef A
+                    }
+                    spec_rows(pl, n, r, h, z, nsp, nhp, E);
+                }
+                for (int m = 0; m < nsp; m++)
+                    for (int a = 0; a < nhp; a++)
+                        out[((size_t)m * nyc + (jc - 1)) * nhp + a] = E[(size_t)m * nhp + a] * norm;
+            }
+            free(wk);
+            free(z);
+        }
+    }
+    return 0;
+}
+
+/* ------------------------------------------------------------------------
  * one substep: body of the ns loop of ChannelIterate
  * (src/m_ChannelSystem.f90:102-140)
  * ---------------------------------------------------------------------- */

@@ -51,6 +51,12 @@ int  orc_diagnostics(orc_t* o, paratc_diag* diag);
 int  orc_metric(orc_t* o, const char* name, double* out, int cap);
 /* clcStat: one call's SumVec*inxz per row jc = 1..nyp (k fastest; 35 or 40) */
 int  orc_stats(orc_t* o, double* out);
+/* clcStat's 1-D spectra: one call's EgyX*normEgy / EgyZ*normEgy,
+ * egx[(m*nyc + jc-1)*(nxc/2+1) + kx], egz likewise with nzc/2+1 modes, for
+ * the reference's spectra m = 1..8 (9 with the scalar) in its order: ux, uy,
+ * uz, p, the cospectra <ux uy_c> and <ux_c uy_c>, LCS real, LCS imaginary
+ * [, scalar]; jlcs is jForLCS (1..nyc). */
+int  orc_spectra(orc_t* o, int jlcs, double* egx, double* egz);
 
 /* real DFT helpers in FFTW's halfcomplex convention (for pinning) */
 int  orc_r2hc(int n, const double* in, double* out);

@@ -66,6 +66,11 @@ struct paratc_ctx {
     double* d_stats = nullptr;          // SumStat [nyp][nstat] then PrGradsum (FP64 accumulators)
     double* d_stats_part = nullptr;     // per-slice partial sums of clcStat
     int nfstime = 0;                    // statistics steps accumulated
+    double* d_specx = nullptr;          // 1-D spectra accumulators [nsp][ny][nx/2+1], [nsp][ny][nz/2+1]
+    double* d_specz = nullptr;          //   (created on first use)
+    double* d_spec_part = nullptr;      // per-slice partial records of the spectra kernels
+    double2* d_twxf = nullptr;          // exp(-2 pi i m / nx), m < nx (full-length x transforms)
+    int nspectime = 0;                  // spectra samples accumulated
     DDiag* h_diag = nullptr;   // pinned
     DCoef* h_coef = nullptr;   // pinned
     DCoef* h_coef0 = nullptr;  // pinned, the coefficient block of a freshly loaded state (never rewritten)
@@ -441,6 +446,7 @@ int paratc_create(const paratc_params* prm, const double* yp, int device, paratc
         pfft_x_init();
         pfft_z_init();
         plane_init();
+        spectra_init();
         inited = true;
     }
     const HostMetrics& h = ctx->hm;
@@ -533,9 +539,11 @@ int paratc_create(const paratc_params* prm, const double* yp, int device, paratc
             paratc_destroy(ctx);
             return rc;
         }
-        CK(cudaMemcpy(ctx->d_twx, twx.data(), twx.size() * sizeof(double2), cudaMemcpyHostToDevice));
-        CK(cudaMemcpy(ctx->d_postx, post.data(), post.size() * sizeof(double2), cudaMemcpyHostToDevice));
-        CK(cudaMemcpy(ctx->d_twz, twz.data(), twz.size() * sizeof(double2), cudaMemcpyHostToDevice));
+        // on the context's stream, after dalloc's zero fill; the host vectors live until the sync
+        CK(cudaMemcpyAsync(ctx->d_twx, twx.data(), twx.size() * sizeof(double2), cudaMemcpyHostToDevice, ctx->st));
+        CK(cudaMemcpyAsync(ctx->d_postx, post.data(), post.size() * sizeof(double2), cudaMemcpyHostToDevice, ctx->st));
+        CK(cudaMemcpyAsync(ctx->d_twz, twz.data(), twz.size() * sizeof(double2), cudaMemcpyHostToDevice, ctx->st));
+        CK(cudaStreamSynchronize(ctx->st));
     }
     CK(cudaMallocHost(&ctx->h_diag, sizeof(DDiag)));
     CK(cudaMallocHost(&ctx->h_coef, sizeof(DCoef)));
@@ -893,6 +901,66 @@ int paratc_stats_get(paratc_ctx* ctx, double* sumstat, int* nstat, int* nfstime,
     if (nfstime) *nfstime = ctx->nfstime;
     if (sumstat) CK(cudaMemcpyAsync(sumstat, ctx->d_stats, (size_t)ctx->nyp * ns * sizeof(double), cudaMemcpyDefault, ctx->st));
     if (prgradsum) CK(cudaMemcpyAsync(prgradsum, ctx->d_stats + (size_t)ctx->nyp * ns, sizeof(double), cudaMemcpyDefault, ctx->st));
+    return sync(ctx);
+}
+
+
+// the spectra accumulators, partial records and full-length x twiddles, on first use
+static int spectra_alloc(paratc_ctx* ctx) {
+    if (ctx->d_specx) return PARATC_OK;
+    if (!spectra_supported(ctx->nx) || !spectra_supported(ctx->nz))
+        return set_err(ctx, PARATC_ERR_BAD_ARG, "spectra: no transform kernel for nx or nz");
+    int rc;
+    const std::vector<double2> tw = twiddles(ctx->nx, ctx->nx);
+    if ((rc = dalloc(ctx, &ctx->d_specx, (size_t)9 * ctx->ny * (ctx->nx / 2 + 1))) ||
+        (rc = dalloc(ctx, &ctx->d_specz, (size_t)9 * ctx->ny * (ctx->nz / 2 + 1))) ||
+        (rc = dalloc(ctx, &ctx->d_spec_part, spectra_part_doubles(ctx->kc))) ||
+        (rc = dalloc(ctx, &ctx->d_twxf, tw.size())))
+        return rc;
+    CK(cudaMemcpyAsync(ctx->d_twxf, tw.data(), tw.size() * sizeof(double2), cudaMemcpyHostToDevice, ctx->st));
+    ctx->nspectime = 0;
+    return sync(ctx);
+}
+
+int paratc_spectra_reset(paratc_ctx* ctx) {
+    if (!ctx) return PARATC_ERR_BAD_ARG;
+    CK(cudaSetDevice(ctx->dev));
+    int rc = spectra_alloc(ctx);
+    if (rc != PARATC_OK) return rc;
+    CK(cudaMemsetAsync(ctx->d_specx, 0, (size_t)9 * ctx->ny * (ctx->nx / 2 + 1) * sizeof(double), ctx->st));
+    CK(cudaMemsetAsync(ctx->d_specz, 0, (size_t)9 * ctx->ny * (ctx->nz / 2 + 1) * sizeof(double), ctx->st));
+    ctx->nspectime = 0;
+    return sync(ctx);
+}
+
+int paratc_spectra_accumulate(paratc_ctx* ctx, int jlcs) {
+    if (!ctx || jlcs < 1 || jlcs > ctx->ny) return PARATC_ERR_BAD_ARG;
+    CK(cudaSetDevice(ctx->dev));
+    int rc = spectra_alloc(ctx);
+    if (rc != PARATC_OK) return rc;
+    launch_spectra(ctx->st, 0, ctx->kc, ctx->f, jlcs, ctx->d_twxf, ctx->d_spec_part, ctx->d_specx);
+    launch_spectra(ctx->st, 1, ctx->kc, ctx->f, jlcs, ctx->d_twz, ctx->d_spec_part, ctx->d_specz);
+    ctx->launches += 4;
+    ctx->nspectime += 1;
+    CK(cudaGetLastError());
+    return PARATC_OK;
+}
+
+int paratc_spectra_get(paratc_ctx* ctx, double* spec_x, double* spec_z, int* nspec, int* nspectime) {
+    if (!ctx) return PARATC_ERR_BAD_ARG;
+    CK(cudaSetDevice(ctx->dev));
+    const int nsp = spectra_count(ctx->kc);
+    if (nspec) *nspec = nsp;
+    if (nspectime) *nspectime = ctx->nspectime;
+    if (!spec_x && !spec_z) return PARATC_OK;
+    int rc = spectra_alloc(ctx);
+    if (rc != PARATC_OK) return rc;
+    if (spec_x)
+        CK(cudaMemcpyAsync(spec_x, ctx->d_specx, (size_t)nsp * ctx->ny * (ctx->nx / 2 + 1) * sizeof(double),
+                           cudaMemcpyDefault, ctx->st));
+    if (spec_z)
+        CK(cudaMemcpyAsync(spec_z, ctx->d_specz, (size_t)nsp * ctx->ny * (ctx->nz / 2 + 1) * sizeof(double),
+                           cudaMemcpyDefault, ctx->st));
     return sync(ctx);
 }
 

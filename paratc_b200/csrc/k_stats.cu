@@ -19,7 +19,6 @@
 namespace ptc {
 namespace {
 
-constexpr int NST_MAX = 40;
 constexpr int STAT_THREADS = 256;
 
 template <int NS>
@@ -27,7 +26,7 @@ __global__ void __launch_bounds__(STAT_THREADS)
     k_stats(DConst c, DMetric m, const double* __restrict__ ux, const double* __restrict__ uy,
             const double* __restrict__ uz, const double* __restrict__ pr, const double* __restrict__ sc, int splits,
             double* __restrict__ part) {
-    const int nx = c.nx, ny = c.ny, nz = c.nz, nyp = c.nyp;
+    const int nx = c.nx, ny = c.ny, nz = c.nz;
     const int jc = blockIdx.x + 1;  // 1..nyp
     const int s = blockIdx.y;
     const int k0 = (int)((long long)nz * s / splits), k1 = (int)((long long)nz * (s + 1) / splits);

@@ -78,6 +78,15 @@ size_t stats_part_doubles(const DConst& c);
 void launch_stats(cudaStream_t st, const DConst& c, const DMetric& m, const Fields& f, const DCoef* coef,
                   double* part, double* sumstat, double* prgradsum);
 
+// k_spectra.cu: clcStat's 1-D spectra (energy, cospectra, linear coherence)
+bool spectra_supported(int n);
+int spectra_count(const DConst& c);
+int spectra_splits(const DConst& c, int axis);
+size_t spectra_part_doubles(const DConst& c);
+void spectra_init();
+void launch_spectra(cudaStream_t st, int axis, const DConst& c, const Fields& f, int jlcs, const double2* tw,
+                    double* part, double* out);
+
 // k_plane.cu: both transforms of a y-plane in one CTA (planes that fit shared memory)
 bool plane_supported(int nx, int nz);
 void plane_init();

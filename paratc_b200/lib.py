@@ -31,7 +31,7 @@ EXPORTED = [
     "paratc_poisson_noalloc", "paratc_batch_create", "paratc_batch_destroy", "paratc_batch_member",
     "paratc_batch_steps", "paratc_batch_graph_kernels", "paratc_batch_stream", "paratc_stats_reset",
     "paratc_stats_accumulate", "paratc_stats_get", "paratc_set_fields_async", "paratc_get_fields_async",
-    "paratc_sync",
+    "paratc_sync", "paratc_spectra_reset", "paratc_spectra_accumulate", "paratc_spectra_get",
 ]
 PROF_NKERNELS = 16
 
@@ -107,6 +107,10 @@ def load(path=None):
                                    _dp]
     L.paratc_batch_stream.argtypes = [ctypes.c_void_p]
     L.paratc_batch_stream.restype = ctypes.c_void_p
+    L.paratc_spectra_reset.argtypes = [ctypes.c_void_p]
+    L.paratc_spectra_accumulate.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    L.paratc_spectra_get.argtypes = [ctypes.c_void_p, _dp, _dp, ctypes.POINTER(ctypes.c_int),
+                                     ctypes.POINTER(ctypes.c_int)]
     _lib = L
     return L
 
@@ -329,6 +333,25 @@ class ChannelSystem:
         self._check(self._L.paratc_stats_get(self._h, _ptr(out), ctypes.byref(n), ctypes.byref(nf), ctypes.byref(pg)),
                     "paratc_stats_get")
         return out, nf.value, pg.value
+
+    # -- 1-D spectra (clcStat's spectra section)
+    def spectra_reset(self):
+        self._check(self._L.paratc_spectra_reset(self._h), "paratc_spectra_reset")
+
+    def spectra_accumulate(self, jlcs):
+        self._check(self._L.paratc_spectra_accumulate(self._h, int(jlcs)), "paratc_spectra_accumulate")
+
+    def spectra_get(self):
+        """(x spectra [nsp, nyc, nxc/2+1], z spectra [nsp, nyc, nzc/2+1],
+        nSpectime): the sums of EgyX*normEgy and EgyZ*normEgy over the samples."""
+        p = self.params
+        nsp = 9 if p.scalar_on else 8
+        ex = np.zeros((nsp, p.nyc, p.nxc // 2 + 1))
+        ez = np.zeros((nsp, p.nyc, p.nzc // 2 + 1))
+        n, ns = ctypes.c_int(), ctypes.c_int()
+        self._check(self._L.paratc_spectra_get(self._h, _ptr(ex), _ptr(ez), ctypes.byref(n), ctypes.byref(ns)),
+                    "paratc_spectra_get")
+        return ex, ez, ns.value
 
     def project(self):
         dm = ctypes.c_double()

@@ -3,7 +3,8 @@
 C2 (512 x 256 x 512) reaches the kernels only large grids use (the streaming
 y-solve, 512-point z transforms, 256-point x transforms); the oracle solves
 it in a few seconds on the host.  C1 (128 x 96 x 128) is the bench workload:
-two full RK3 steps against the oracle, and the solenoidality of the result.
+two full RK3 steps against the oracle, the solenoidality of the result, and
+the 1-D spectra of the stepped fields.
 Tolerances as in test_gpu_parity (Poisson 1e-12 relative to max|phi|; fields
 after one step 1e-10, after two 1e-8).
 """
@@ -54,4 +55,17 @@ def test_channel_c1_two_steps():
             assert e <= tol, "C1 step %d %s rel err %.3e" % (s, n, e)
         assert dg.divmax <= 1e-10
         assert abs(dg.dt - do.dt) <= 1e-12 * do.dt
+    # 1-D spectra at the bench size (128-point x and z transforms, 96 rows),
+    # on the oracle's fields loaded into the context: transform rounding only
+    fo = o.get_fields()
+    g.set_fields(fo["ux"], fo["uy"], fo["uz"], fo["p"])
+    jl = 24
+    ref = o.spectra(jl)
+    g.spectra_accumulate(jl)
+    ex, ez, ns = g.spectra_get()
+    assert ns == 1
+    for got, r in zip((ex, ez), ref):
+        for m in range(r.shape[0]):
+            e = np.abs(got[m] - r[m]).max() / np.abs(r[m]).max()
+            assert e <= 1e-12, "C1 spectrum %d rel err %.3e" % (m + 1, e)
     g.close()

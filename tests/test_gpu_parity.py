@@ -238,3 +238,57 @@ def test_stats_accumulate(name):
     g.stats_reset()
     sg, nf, pg = g.stats_get()
     assert nf == 0 and not sg.any() and pg == 0.0
+
+
+@pytest.mark.parametrize("name", ["channel", "channel_odd", "halfchannel_scalar", "channel_scalar_crf"])
+def test_spectra_accumulate(name):
+    """clcStat's 1-D spectra (energy, cospectra, linear coherence) summed over
+    two samples on both sides: every spectrum within 1e-11 of its largest
+    magnitude (the fields already differ at rounding level after a step)."""
+    case = variant(name)
+    o, g, _ = _pair(case)
+    ny = case.params.nyc
+    acc = None
+    for s, jl in enumerate((max(1, ny // 5), 1)):
+        o.step()
+        g.iterate(1, raise_on_guard=False)
+        so = o.spectra(jl)
+        acc = so if acc is None else (acc[0] + so[0], acc[1] + so[1])
+        g.spectra_accumulate(jl)
+    ex, ez, ns = g.spectra_get()
+    assert ns == 2
+    for got, ref in zip((ex, ez), acc):
+        assert got.shape == ref.shape
+        for m in range(ref.shape[0]):
+            scale = max(np.abs(ref[m]).max(), 1e-300)
+            e = np.abs(got[m] - ref[m]).max() / scale
+            assert e <= TOL_STAGE, "%s spectrum %d rel err %.3e" % (name, m + 1, e)
+    with pytest.raises(Exception):
+        g.spectra_accumulate(0)
+    with pytest.raises(Exception):
+        g.spectra_accumulate(ny + 1)
+    g.spectra_reset()
+    ex, ez, ns = g.spectra_get()
+    assert ns == 0 and not ex.any() and not ez.any()
+
+
+@pytest.mark.parametrize("name", ["channel", "halfchannel_scalar"])
+def test_spectra_same_fields(name):
+    """On identical fields (the oracle's, after a step, loaded into the
+    context) the spectra differ only by the transforms' rounding: 1e-12 of
+    each spectrum's largest magnitude."""
+    case = variant(name)
+    o, g, _ = _pair(case)
+    o.step()
+    fo = o.get_fields()
+    g.set_fields(fo["ux"], fo["uy"], fo["uz"], fo["p"], fo["c"])
+    jl = max(1, case.params.nyc // 3)
+    ref = o.spectra(jl)
+    g.spectra_reset()
+    g.spectra_accumulate(jl)
+    ex, ez, ns = g.spectra_get()
+    assert ns == 1
+    for got, r in zip((ex, ez), ref):
+        for m in range(r.shape[0]):
+            e = np.abs(got[m] - r[m]).max() / max(np.abs(r[m]).max(), 1e-300)
+            assert e <= 1e-12, "%s spectrum %d rel err %.3e" % (name, m + 1, e)

@@ -234,3 +234,75 @@ def test_stats_moments_pinned_by_numpy():
         assert err < 1e-13, (q, err)
     # the top wall row carries only moments 27, 33 and 35
     assert np.count_nonzero(s[ny][[q for q in range(35) if q not in (26, 32, 34)]]) == 0
+
+
+def numpy_spectra(params, g, jlcs):
+    """clcStat's 1-D spectra (src/m_FlowCase.f90:430-806, :954-1180) in
+    complex form with numpy's real FFT: E = w |X|^2 and the cospectra
+    w Re(X conj Y) with w = 2 except at the mean and last mode, LCS =
+    X conj(X_ref) (imaginary part zero at the end modes), all summed over the
+    other homogeneous direction and times 1/(n_dir^2 n_other).  g: interior
+    fields [z, y, x]."""
+    p = params
+    nx, ny, nz = p.nxc, p.nyc, p.nzc
+    ux = g["ux"] + p.ucrf
+    uy = g["uy"]
+    top = p.uy_bc[3] if p.flow_type == cases.FT_CH else 0.0
+    uyn = np.concatenate([uy, np.full((nz, 1, nx), top)], axis=1)
+    uyc = 0.5 * (uyn[:, :-1] + uyn[:, 1:])
+    ic = (-1 / 16, 9 / 16, 9 / 16, -1 / 16)
+    u0 = g["ux"]
+    uxc = ic[0] * np.roll(u0, 1, 2) + ic[1] * u0 + ic[2] * np.roll(u0, -1, 2) + ic[3] * np.roll(u0, -2, 2) + p.ucrf
+    jr = np.array([jlcs if (p.flow_type == cases.FT_HC or jc <= ny // 2) else ny + 1 - jlcs
+                   for jc in range(1, ny + 1)]) - 1
+    fields = [ux, uy, g["uz"], g["p"]] + ([g["c"]] if p.scalar_on else [])
+    out = []
+    for axis, n, other in ((2, nx, nz), (0, nz, nx)):
+        nh = n // 2
+        w = np.full(nh + 1, 2.0)
+        w[0] = w[nh] = 1.0
+        norm = 1.0 / (n * n * other)
+        sum_ax = 0 if axis == 2 else 1  # the other homogeneous direction
+
+        def hat(a):
+            # x: [z, y, kx]; z: [y, x, kz]
+            return np.moveaxis(np.fft.rfft(a, axis=axis), axis, 2)
+
+        def rsum(a):
+            return a.sum(axis=sum_ax) * norm  # [y, k]
+
+        X = hat(ux)
+        Y = hat(uyc)
+        spec = [rsum(w * np.abs(hat(f)) ** 2) for f in fields[:4]]
+        spec.append(rsum(w * (X * np.conj(Y)).real))
+        spec.append(rsum(w * (hat(uxc) * np.conj(Y)).real))
+        lcs = X * np.conj(X[:, jr] if axis == 2 else X[jr])
+        li = lcs.imag.copy()
+        li[..., 0] = 0.0
+        li[..., nh] = 0.0
+        spec.append(rsum(lcs.real))
+        spec.append(rsum(li))
+        if p.scalar_on:
+            spec.append(rsum(w * np.abs(hat(fields[4])) ** 2))
+        out.append(np.stack(spec))
+    return out
+
+
+@pytest.mark.parametrize("name", ["channel", "halfchannel_scalar", "channel_scalar_crf", "channel_odd"])
+def test_spectra_pinned_by_numpy(name):
+    """The oracle's halfcomplex restatement of the 1-D energy spectra,
+    cospectra and linear coherence spectra against numpy's complex FFT."""
+    case = variant(name)
+    yp = yp_of(case)
+    o = ol.Oracle(case.params, yp)
+    f = fields_of(case, yp)
+    o.set_fields(f["ux"], f["uy"], f["uz"], f["p"], f["c"])
+    o.step()
+    jlcs = max(1, case.params.nyc // 5)
+    ex, ez = o.spectra(jlcs)
+    rx, rz = numpy_spectra(case.params, o.get_fields(), jlcs)
+    for got, ref in ((ex, rx), (ez, rz)):
+        assert got.shape == ref.shape
+        for m in range(got.shape[0]):
+            err = np.abs(got[m] - ref[m]).max() / max(np.abs(ref[m]).max(), 1e-300)
+            assert err < 1e-12, (name, m, err)
