@@ -331,6 +331,26 @@ int paratc_spectra_accumulate(paratc_ctx* ctx, int jlcs);
  * reference divides by it when it writes SpecX/SpecZ, :841-884). */
 int paratc_spectra_get(paratc_ctx* ctx, double* spec_x, double* spec_z, int* nspec, int* nspectime);
 
+/* ---- 2-D spectra (clcStat's 2-D section, src/m_FlowCase.f90:780-803, with
+ * clcEnergySpectra2D and clcCosSpectra2D at :1186-1375).  Each field is
+ * transformed R2HC along x and then R2HC along z (a halfcomplex-of-
+ * halfcomplex array, as the reference does, not a complex 2-D transform);
+ * at the rows iySpec2D the squares are added with normEgy = (1/(nxc nzc))^2,
+ * halved in a channel, where the mirrored row is added too (nyp+1-jct for
+ * the uy faces, nyc+1-jct otherwise).  Spectra m = 1..5 (6 with the scalar):
+ * ux (without uCRF), uy, uz, p, the cospectrum of ux at the cell centre
+ * (+uCRF) with uy at the cell centre (minus the mirrored product), scalar.
+ * setup takes &Spectra2DOpt's iySpec2D (nsel = nySpec2D rows; 2..nyc/2 in a
+ * channel, 2..nyc otherwise, as InitStatVar checks, :220-232, else
+ * PARATC_ERR_BAD_ARG) and zeroes the accumulators; accumulate is one spectra
+ * step. */
+int paratc_spectra2d_setup(paratc_ctx* ctx, int nsel, const int* iy);
+int paratc_spectra2d_reset(paratc_ctx* ctx);
+int paratc_spectra2d_accumulate(paratc_ctx* ctx);
+/* out[((m-1)*nzc + kc)*nsel*nxc + (q-1)*nxc + ic] (EnergySpec2D(nxc, nySpec2D,
+ * nzc, m) in Fortran order; may be NULL), nspec: 5 or 6, nsel, nspectime. */
+int paratc_spectra2d_get(paratc_ctx* ctx, double* out, int* nspec, int* nsel, int* nspectime);
+
 /* ---- Ensembles.  No counterpart in the reference, which advances one case
  * per MPI job; this is the batched form of ChannelIterate
  * (src/m_ChannelSystem.f90:119-226) for many independent channel instances of

@@ -50,6 +50,7 @@ def lib():
         L.orc_metric.argtypes = [ctypes.c_void_p, ctypes.c_char_p, _dp, ctypes.c_int]
         L.orc_stats.argtypes = [ctypes.c_void_p, _dp]
         L.orc_spectra.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, _dp]
+        L.orc_spectra2d.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int32), _dp]
         L.orc_r2hc.argtypes = [ctypes.c_int, _dp, _dp]
         L.orc_hc2r.argtypes = [ctypes.c_int, _dp, _dp]
         L.orc_ycoord.argtypes = [ctypes.c_int, _dp, _dp, ctypes.POINTER(ctypes.c_int32),
@@ -229,6 +230,19 @@ class Oracle:
         if rc != 0:
             raise RuntimeError("orc_spectra rc=%d" % rc)
         return ex, ez
+
+    def spectra2d(self, iy):
+        """clcStat's 2-D spectra of the current fields at the rows iy
+        (iySpec2D, 1-based): one sample, [nsp2, nzc, nsel, nxc] (EnergySpec2D's
+        Fortran order reversed), nsp2 = 5, or 6 with the scalar."""
+        p = self.params
+        iy = np.ascontiguousarray(iy, dtype=np.int32)
+        nsp = 6 if p.scalar_on else 5
+        out = np.zeros((nsp, p.nzc, len(iy), p.nxc))
+        rc = lib().orc_spectra2d(self._h, len(iy), iy.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), _ptr(out))
+        if rc != 0:
+            raise RuntimeError("orc_spectra2d rc=%d" % rc)
+        return out
 
     def metric(self, name):
         buf = np.empty(max(self.params.nxc, self.params.nyc, self.params.nzc) + 8)

@@ -1408,6 +1408,113 @@ int orc_spectra(orc_t* o, int jlcs, double* egx, double* egz) {
 }
 
 /* ------------------------------------------------------------------------
+ * 2-D spectra of clcStat (src/m_FlowCase.f90:780-803) with
+ * clcEnergySpectra2D and clcCosSpectra2D (:1186-1375): the field is
+ * transformed R2HC along x, then R2HC along z (a halfcomplex-of-halfcomplex
+ * array, not a complex 2-D transform), and at the rows iySpec2D the squares
+ * (products for the cospectrum) are added with normEgy = (1/(nxc nzc))^2,
+ * halved in a channel, where the mirrored row is added too (nyp+1-jct for the
+ * uy faces, nyc+1-jct otherwise; the cospectrum subtracts it, IsSymmetry =
+ * .false.).  Fields: 1 ux (no uCRF), 2 uy, 3 uz, 4 p, 5 <ux_c uy_c> with ux_c
+ * the cell-centre interpolation + uCRF (:434-444) and uy_c = (uy_j +
+ * uy_j+1)/2 (:784-793) [, 6 scalar].  out[((m*nzc + kc)*nsel + q)*nxc + ic]
+ * gets one call's contribution (EnergySpec2D's Fortran order).
+ * ---------------------------------------------------------------------- */
+/* hc-hc transform of one y row of field f: H[kc*nxc + ic] */
+static void hc2d_row(orc_t* o, int f, int j, double* H, double* row, double* hrow, cplx* z) {
+    const int nxc = o->nxc, nzc = o->nzc;
+    const double *ux = o->ux, *uy = o->uy, *uz = o->uz, *pr = o->pr, *sc = o->sc, *IC = o->IC;
+    const double uCRF = o->p.ucrf;
+    double* zero_row = row + (nxc > nzc ? nxc : nzc);
+    for (int q = 0; q < (nxc > nzc ? nxc : nzc); q++) zero_row[q] = zero;
+    for (int kc = 1; kc <= nzc; kc++) {
+        for (int ic = 1; ic <= nxc; ic++) {
+#define A(a, i, jj, k) (a)[HX(o, i, jj, k)]
+            double v;
+            switch (f) {
+                case 0: v = A(ux, ic, j, kc); break;
+                case 1: v = A(uy, ic, j, kc); break;
+                case 2: v = A(uz, ic, j, kc); break;
+                case 3: v = A(pr, ic, j, kc); break;
+                case 4: v = IC[0] * A(ux, ic - 1, j, kc) + IC[1] * A(ux, ic, j, kc) + IC[2] * A(ux, ic + 1, j, kc) +
+                            IC[3] * A(ux, ic + 2, j, kc) + uCRF; break;
+                case 5: v = half * (A(uy, ic, j, kc) + A(uy, ic, j + 1, kc)); break;
+                default: v = A(sc, ic, j, kc); break;
+            }
+#undef A
+            row[ic - 1] = v;
+        }
+        r2hc_pair(&o->px, row, zero_row, H + (size_t)(kc - 1) * nxc, hrow, z, z + nxc);
+    }
+    for (int ic = 0; ic < nxc; ic++) {
+        for (int kc = 0; kc < nzc; kc++) row[kc] = H[(size_t)kc * nxc + ic];
+        r2hc_pair(&o->pz, row, zero_row, hrow, hrow + nzc, z, z + nzc);
+        for (int kc = 0; kc < nzc; kc++) H[(size_t)kc * nxc + ic] = hrow[kc];
+    }
+}
+
+int orc_spectra2d(orc_t* o, int nsel, const int* iy, double* out) {
+    if (!o || !out || !iy || nsel < 1) return PARATC_ERR_BAD_ARG;
+    const int nxc = o->nxc, nyc = o->nyc, nzc = o->nzc, nyp = o->nyp;
+    const int is_hc = (o->p.flow_type == PARATC_FT_HC);
+    for (int q = 0; q < nsel; q++)
+        if (iy[q] < 2 || iy[q] > (o->p.flow_type == PARATC_FT_CH ? nyc / 2 : nyc)) return PARATC_ERR_BAD_ARG;
+    const int nsp = o->p.scalar_on ? 6 : 5;
+    upd_halo(o, o->ux, 2, 2, 2, 2);
+    double normEgy = one / ((double)nxc * (double)nzc);
+    normEgy = normEgy * normEgy;
+    if (o->p.flow_type == PARATC_FT_CH) normEgy = normEgy * half;
+    const size_t pl = (size_t)nxc * nzc;
+    const int nmax = nxc > nzc ? nxc : nzc;
+#pragma omp parallel
+    {
+        double* H = (double*)malloc(sizeof(double) * 4 * pl);
+        double* row = (double*)malloc(sizeof(double) * 4 * (size_t)nmax);
+        cplx* z = (cplx*)malloc(sizeof(cplx) * 2 * (size_t)nmax);
+#pragma omp for schedule(static) collapse(2)
+        for (int q = 0; q < nsel; q++) {
+            for (int m = 0; m < nsp; m++) {
+                const int jct = iy[q];
+                double *H1 = H, *H2 = H + pl, *H3 = H + 2 * pl, *H4 = H + 3 * pl;
+                if (m == 4) {                                   /* clcCosSpectra2D(ArrTemp1, ArrTemp2, 5, .false.) */
+                    hc2d_row(o, 4, jct, H1, row, row + 2 * nmax, z);
+                    hc2d_row(o, 5, jct, H2, row, row + 2 * nmax, z);
+                    if (!is_hc) {
+                        const int jcs = nyc + 1 - jct;
+                        hc2d_row(o, 4, jcs, H3, row, row + 2 * nmax, z);
+                        hc2d_row(o, 5, jcs, H4, row, row + 2 * nmax, z);
+                    }
+                    for (size_t e = 0; e < pl; e++) {
+                        const double rt1 = H1[e] * H2[e];
+                        double v;
+                        if (is_hc) v = normEgy * rt1;
+                        else { const double rt2 = H3[e] * H4[e]; v = normEgy * (rt1 + (-one) * rt2); }
+                        const size_t kc = e / nxc, ic = e % nxc;
+                        out[(((size_t)m * nzc + kc) * nsel + q) * nxc + ic] = v;
+                    }
+                } else {                                         /* clcEnergySpectra2D */
+                    const int f = m < 4 ? m : 6;
+                    hc2d_row(o, f, jct, H1, row, row + 2 * nmax, z);
+                    if (!is_hc) hc2d_row(o, f, (f == 1 ? nyp : nyc) + 1 - jct, H2, row, row + 2 * nmax, z);
+                    for (size_t e = 0; e < pl; e++) {
+                        const double rt1 = H1[e];
+                        double v;
+                        if (is_hc) v = normEgy * rt1 * rt1;
+                        else { const double rt2 = H2[e]; v = normEgy * (rt1 * rt1 + rt2 * rt2); }
+                        const size_t kc = e / nxc, ic = e % nxc;
+                        out[(((size_t)m * nzc + kc) * nsel + q) * nxc + ic] = v;
+                    }
+                }
+            }
+        }
+        free(H);
+        free(row);
+        free(z);
+    }
+    return 0;
+}
+
+/* ------------------------------------------------------------------------
  * one substep: body of the ns loop of ChannelIterate
  * (src/m_ChannelSystem.f90:102-140)
  * ---------------------------------------------------------------------- */

@@ -57,6 +57,11 @@ int  orc_stats(orc_t* o, double* out);
  * uz, p, the cospectra <ux uy_c> and <ux_c uy_c>, LCS real, LCS imaginary
  * [, scalar]; jlcs is jForLCS (1..nyc). */
 int  orc_spectra(orc_t* o, int jlcs, double* egx, double* egz);
+/* clcStat's 2-D spectra at the rows iy[0..nsel-1] (iySpec2D): one call's
+ * contribution, out[((m*nzc + kc)*nsel + q)*nxc + ic] for m = 1..5 (6 with
+ * the scalar): ux, uy, uz, p, <ux_c uy_c> [, scalar] of the halfcomplex-of-
+ * halfcomplex x-z transform. */
+int  orc_spectra2d(orc_t* o, int nsel, const int* iy, double* out);
 
 /* real DFT helpers in FFTW's halfcomplex convention (for pinning) */
 int  orc_r2hc(int n, const double* in, double* out);

@@ -71,6 +71,12 @@ struct paratc_ctx {
     double* d_spec_part = nullptr;      // per-slice partial records of the spectra kernels
     double2* d_twxf = nullptr;          // exp(-2 pi i m / nx), m < nx (full-length x transforms)
     int nspectime = 0;                  // spectra samples accumulated
+    double* d_spec2d = nullptr;         // 2-D spectra accumulators [nsp2][nz][nsel][nx]
+    double* d_s2 = nullptr;             // hc-hc transforms of the listed (field, row) pairs
+    int2* d_fj = nullptr;               // the (field, row) pairs
+    int nsel2 = 0, nfj2 = 0, nmir2 = 0, nfld2 = 0;
+    size_t spec2d_cap = 0, s2_cap = 0, fj_cap = 0;  // capacities of the three buffers (elements)
+    int nspectime2 = 0;                 // 2-D spectra samples accumulated
     DDiag* h_diag = nullptr;   // pinned
     DCoef* h_coef = nullptr;   // pinned
     DCoef* h_coef0 = nullptr;  // pinned, the coefficient block of a freshly loaded state (never rewritten)
@@ -961,6 +967,85 @@ int paratc_spectra_get(paratc_ctx* ctx, double* spec_x, double* spec_z, int* nsp
     if (spec_z)
         CK(cudaMemcpyAsync(spec_z, ctx->d_specz, (size_t)nsp * ctx->ny * (ctx->nz / 2 + 1) * sizeof(double),
                            cudaMemcpyDefault, ctx->st));
+    return sync(ctx);
+}
+
+int paratc_spectra2d_setup(paratc_ctx* ctx, int nsel, const int* iy) {
+    if (!ctx || nsel < 1 || !iy) return PARATC_ERR_BAD_ARG;
+    CK(cudaSetDevice(ctx->dev));
+    const int ny = ctx->ny, nyp = ctx->nyp;
+    const int jmax = ctx->prm.flow_type == PARATC_FT_CH ? ny / 2 : ny;
+    for (int q = 0; q < nsel; q++)
+        if (iy[q] < 2 || iy[q] > jmax) return set_err(ctx, PARATC_ERR_BAD_ARG, "spectra2d: iySpec2D out of range");
+    int rc = spectra_alloc(ctx);  // the full-length x twiddles
+    if (rc != PARATC_OK) return rc;
+    const int nmir = ctx->prm.flow_type == PARATC_FT_HC ? 1 : 2;
+    const int nfld = ctx->prm.scalar_on ? 7 : 6;
+    std::vector<int2> fj;
+    for (int q = 0; q < nsel; q++)
+        for (int f = 0; f < nfld; f++)
+            for (int h = 0; h < nmir; h++) {
+                const int jct = iy[q];
+                const int row = h == 0 ? jct : (f == 1 ? nyp + 1 - jct : ny + 1 - jct);
+                fj.push_back(make_int2(f, row));
+            }
+    const int nsp = ctx->prm.scalar_on ? 6 : 5;
+    const size_t pl = (size_t)ctx->nx * ctx->nz;
+    const size_t need_out = (size_t)nsp * nsel * pl, need_s = fj.size() * pl;
+    if (need_out > ctx->spec2d_cap) {
+        if ((rc = dalloc(ctx, &ctx->d_spec2d, need_out))) return rc;
+        ctx->spec2d_cap = need_out;
+    }
+    if (need_s > ctx->s2_cap) {
+        if ((rc = dalloc(ctx, &ctx->d_s2, need_s))) return rc;
+        ctx->s2_cap = need_s;
+    }
+    if (fj.size() > ctx->fj_cap) {
+        if ((rc = dalloc(ctx, &ctx->d_fj, fj.size()))) return rc;
+        ctx->fj_cap = fj.size();
+    }
+    CK(cudaMemcpyAsync(ctx->d_fj, fj.data(), fj.size() * sizeof(int2), cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaMemsetAsync(ctx->d_spec2d, 0, need_out * sizeof(double), ctx->st));
+    ctx->nsel2 = nsel;
+    ctx->nfj2 = (int)fj.size();
+    ctx->nmir2 = nmir;
+    ctx->nfld2 = nfld;
+    ctx->nspectime2 = 0;
+    return sync(ctx);
+}
+
+int paratc_spectra2d_reset(paratc_ctx* ctx) {
+    if (!ctx) return PARATC_ERR_BAD_ARG;
+    if (ctx->nsel2 == 0) return set_err(ctx, PARATC_ERR_BAD_ARG, "spectra2d: not set up");
+    CK(cudaSetDevice(ctx->dev));
+    const size_t n = (size_t)(ctx->prm.scalar_on ? 6 : 5) * ctx->nsel2 * ctx->nx * ctx->nz;
+    CK(cudaMemsetAsync(ctx->d_spec2d, 0, n * sizeof(double), ctx->st));
+    ctx->nspectime2 = 0;
+    return sync(ctx);
+}
+
+int paratc_spectra2d_accumulate(paratc_ctx* ctx) {
+    if (!ctx) return PARATC_ERR_BAD_ARG;
+    if (ctx->nsel2 == 0) return set_err(ctx, PARATC_ERR_BAD_ARG, "spectra2d: not set up");
+    CK(cudaSetDevice(ctx->dev));
+    launch_spectra2d(ctx->st, ctx->kc, ctx->f, ctx->d_fj, ctx->nfj2, ctx->nsel2, ctx->nmir2, ctx->nfld2, ctx->d_twxf,
+                     ctx->d_twz, ctx->d_s2, ctx->d_spec2d);
+    ctx->launches += 3;
+    ctx->nspectime2 += 1;
+    CK(cudaGetLastError());
+    return PARATC_OK;
+}
+
+int paratc_spectra2d_get(paratc_ctx* ctx, double* out, int* nspec, int* nsel, int* nspectime) {
+    if (!ctx) return PARATC_ERR_BAD_ARG;
+    CK(cudaSetDevice(ctx->dev));
+    const int nsp = ctx->prm.scalar_on ? 6 : 5;
+    if (nspec) *nspec = nsp;
+    if (nsel) *nsel = ctx->nsel2;
+    if (nspectime) *nspectime = ctx->nspectime2;
+    if (!out || ctx->nsel2 == 0) return PARATC_OK;
+    CK(cudaMemcpyAsync(out, ctx->d_spec2d, (size_t)nsp * ctx->nsel2 * ctx->nx * ctx->nz * sizeof(double),
+                       cudaMemcpyDefault, ctx->st));
     return sync(ctx);
 }
 

@@ -27,6 +27,8 @@
 // partial record in a fixed order, and a second kernel adds the slices of a
 // row in index order, times the norm, to the accumulators.  Results are
 // independent of scheduling.
+#include <algorithm>
+
 #include "common.cuh"
 #include "fft_fixed.cuh"
 #include "kernels.cuh"
@@ -188,6 +190,128 @@ __global__ void k_spec_final(int ny, int nh, int nsp, int splits, double norm, c
     }
 }
 
+// ---------------------------------------------------------------------------
+// 2-D spectra (clcEnergySpectra2D / clcCosSpectra2D, src/m_FlowCase.f90:
+// 1186-1375): R2HC along x, then R2HC along z, of whole x-z rows of the
+// fields, in FFTW's halfcomplex order (r_0..r_{n/2}, then i_k at n-k), two
+// real sequences packed per complex FFT.  Mode 0 transforms the x rows of
+// the listed (field, row) pairs fj[q] into S[(q*nz + k)*nx + a]; mode 1
+// transforms the columns of S along z in place (a CTA reads all its columns
+// before it writes them).  Fields: 0 ux, 1 uy, 2 uz, 3 p, 4 ux at the cell
+// centre + uCRF, 5 uy at the cell centre, 6 the scalar.
+template <int N>
+__global__ void __launch_bounds__(SpK<N>::P)
+    k_hc(int mode, DConst c, const double* __restrict__ ux, const double* __restrict__ uy,
+         const double* __restrict__ uz, const double* __restrict__ pr, const double* __restrict__ sc,
+         const int2* __restrict__ fj, int nseq, const double2* __restrict__ twN, double* S) {
+    constexpr int B = SpK<N>::B, P = SpK<N>::P, PITCH = SpK<N>::PITCH;
+    constexpr ff::Sched SC = ff::make_sched(N);
+    extern __shared__ double2 sms[];
+    double2* buf = sms;
+    double* bufd = reinterpret_cast<double*>(sms);
+    double2* tws = sms + (size_t)N * PITCH;
+    const int tid = threadIdx.x;
+    const int nx = c.nx, nz = c.nz;
+    const size_t pl = (size_t)c.nyt * nx;
+    const double I1 = c.IC[0], I2 = c.IC[1], I3 = c.IC[2], I4 = c.IC[3], ucrf = c.ucrf;
+    const int s0 = blockIdx.x * 2 * B;
+    for (int t = tid; t < N; t += P) tws[t] = twN[t];
+    // real sequence r of the CTA (0..2B-1) is the real (r even) or imaginary
+    // part of complex sequence r/2; mode 0 reads along rows, mode 1 across
+    // columns (consecutive threads, consecutive sequences)
+    for (int f = tid; f < 2 * B * N; f += P) {
+        int r, e;
+        if (mode == 0) { r = f / N; e = f - r * N; }
+        else { e = f / (2 * B); r = f - e * 2 * B; }
+        const int s = s0 + r;
+        double v = 0.0;
+        if (s < nseq) {
+            if (mode == 0) {
+                const int q = s / nz, k = s - q * nz;
+                const int2 d = fj[q];
+                const int i = e;
+                const size_t rw = (size_t)k * pl + (size_t)d.y * nx, o = rw + i;
+                switch (d.x) {
+                    case 0: v = __ldg(&ux[o]); break;
+                    case 1: v = __ldg(&uy[o]); break;
+                    case 2: v = __ldg(&uz[o]); break;
+                    case 3: v = __ldg(&pr[o]); break;
+                    case 4: {
+                        const int im = i >= 1 ? i - 1 : nx - 1, ip = i + 1 < nx ? i + 1 : i + 1 - nx;
+                        const int iu = i + 2 < nx ? i + 2 : i + 2 - nx;
+                        v = I1 * __ldg(&ux[rw + im]) + I2 * __ldg(&ux[o]) + I3 * __ldg(&ux[rw + ip]) + I4 * __ldg(&ux[rw + iu]) + ucrf;
+                        break;
+                    }
+                    case 5: v = 0.5 * (__ldg(&uy[o]) + __ldg(&uy[o + nx])); break;
+                    default: v = __ldg(&sc[o]); break;
+                }
+            } else {
+                const int q = s / nx, a = s - q * nx;
+                v = S[((size_t)q * nz + e) * nx + a];
+            }
+        }
+        bufd[2 * (e * PITCH + (r >> 1)) + (r & 1)] = v;
+    }
+    __syncthreads();
+    ff::smem_passes<N, B, PITCH, P, -1, 0, SC.np>(buf, tws, tid);
+    for (int f = tid; f < 2 * B * N; f += P) {
+        int r, a;
+        if (mode == 0) { r = f / N; a = f - r * N; }
+        else { a = f / (2 * B); r = f - a * 2 * B; }
+        const int s = s0 + r;
+        if (s >= nseq) continue;
+        const int b = r >> 1;
+        double v;
+        if (a <= N / 2) {  // Re of mode a
+            const double2 za = buf[a * PITCH + b], zn = buf[(a == 0 ? 0 : N - a) * PITCH + b];
+            v = (r & 1) == 0 ? 0.5 * (za.x + zn.x) : 0.5 * (za.y + zn.y);
+        } else {  // Im of mode N - a
+            const double2 zk = buf[(N - a) * PITCH + b], za = buf[a * PITCH + b];
+            v = (r & 1) == 0 ? 0.5 * (zk.y - za.y) : 0.5 * (za.x - zk.x);
+        }
+        if (mode == 0) {
+            const int q = s / nz, k = s - q * nz;
+            S[((size_t)q * nz + k) * nx + a] = v;
+        } else {
+            const int q = s / nx, col = s - q * nx;
+            S[((size_t)q * nz + a) * nx + col] = v;
+        }
+    }
+}
+
+// EnergySpec2D(ic, q, kc, m) += normEgy * (H^2 [+ H_mirror^2]) for m = ux, uy,
+// uz, p [, scalar]; the cospectrum m = 5 takes H_uxc H_uyc [- the mirrored
+// product].  fj of (row q, field f, mirror h) = (q*nfld + f)*nmir + h.
+__global__ void k_spec2d_acc(int nx, int nz, int nsel, int nsp, int nmir, int nfld, double norm,
+                             const double* __restrict__ S, double* __restrict__ out) {
+    const size_t tot = (size_t)nsp * nz * nsel * nx;
+    for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < tot; t += (size_t)gridDim.x * blockDim.x) {
+        const int ic = (int)(t % nx);
+        size_t r = t / nx;
+        const int q = (int)(r % nsel);
+        r /= nsel;
+        const int kc = (int)(r % nz);
+        const int m = (int)(r / nz);
+        const size_t e = (size_t)kc * nx + ic, pl = (size_t)nx * nz;
+        const double* Sq = S + (size_t)q * nfld * nmir * pl;
+        double v;
+        if (m == 4) {
+            const double rt1 = Sq[(4 * nmir) * pl + e] * Sq[(5 * nmir) * pl + e];
+            if (nmir == 1) v = norm * rt1;
+            else v = norm * (rt1 + (-1.0) * (Sq[(4 * nmir + 1) * pl + e] * Sq[(5 * nmir + 1) * pl + e]));
+        } else {
+            const int f = m < 4 ? m : 6;
+            const double rt1 = Sq[(f * nmir) * pl + e];
+            if (nmir == 1) v = norm * rt1 * rt1;
+            else {
+                const double rt2 = Sq[(f * nmir + 1) * pl + e];
+                v = norm * (rt1 * rt1 + rt2 * rt2);
+            }
+        }
+        out[t] += v;
+    }
+}
+
 #define SPEC_SIZES(X) X(8) X(12) X(16) X(24) X(30) X(32) X(40) X(48) X(64) X(80) X(96) X(128) X(192) X(256) \
     X(384) X(512) X(768) X(1024) X(1152) X(1536) X(2048) X(2304) X(3072)
 
@@ -223,7 +347,9 @@ size_t spectra_part_doubles(const DConst& c) {
 }
 
 void spectra_init() {
-#define X_CASE(n) cudaFuncSetAttribute(k_spec<n>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SpK<n>::smem);
+#define X_CASE(n)                                                                                              \
+    cudaFuncSetAttribute(k_spec<n>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SpK<n>::smem);           \
+    cudaFuncSetAttribute(k_hc<n>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SpK<n>::smem);
     SPEC_SIZES(X_CASE)
 #undef X_CASE
 }
@@ -249,6 +375,35 @@ void launch_spectra(cudaStream_t st, int axis, const DConst& c, const Fields& f,
                                   : 1.0 / ((double)c.nx * (double)c.nz * (double)c.nz);
     const int nsp = spectra_count(c);
     k_spec_final<<<dim3(c.ny, nsp), 128, 0, st>>>(c.ny, n / 2 + 1, nsp, splits, norm, part, out);
+}
+
+// 2-D spectra of the nfj (field, row) pairs fj: hc-hc transforms into S
+// (nfj*nx*nz doubles), then the accumulation into out
+// [nsp][nz][nsel][nx]; twx / twz: exp(-2 pi i m / n) for n = nx, nz
+void launch_spectra2d(cudaStream_t st, const DConst& c, const Fields& f, const int2* fj, int nfj, int nsel, int nmir,
+                      int nfld, const double2* twx, const double2* twz, double* S, double* out) {
+    for (int mode = 0; mode < 2; mode++) {
+        const int n = mode == 0 ? c.nx : c.nz;
+        const int nseq = nfj * (mode == 0 ? c.nz : c.nx);
+        const double2* tw = mode == 0 ? twx : twz;
+        switch (n) {
+#define X_CASE(n)                                                                                              \
+    case n:                                                                                                    \
+        k_hc<n><<<(nseq + 2 * SpK<n>::B - 1) / (2 * SpK<n>::B), SpK<n>::P, SpK<n>::smem, st>>>(                \
+            mode, c, f.ux, f.uy, f.uz, f.pr, f.sc, fj, nseq, tw, S);                                          \
+        break;
+            SPEC_SIZES(X_CASE)
+#undef X_CASE
+            default: return;
+        }
+    }
+    double norm = 1.0 / ((double)c.nx * (double)c.nz);
+    norm = norm * norm;
+    if (c.flow_type == 1) norm = norm * 0.5;
+    const int nsp = c.scalar_on ? 6 : 5;
+    const size_t tot = (size_t)nsp * c.nz * nsel * c.nx;
+    const int blocks = (int)std::min<size_t>((tot + 255) / 256, (size_t)8 * (c.nsm > 0 ? c.nsm : 148));
+    k_spec2d_acc<<<blocks, 256, 0, st>>>(c.nx, c.nz, nsel, nsp, nmir, nfld, norm, S, out);
 }
 
 }  // namespace ptc

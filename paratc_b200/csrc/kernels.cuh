@@ -86,6 +86,8 @@ size_t spectra_part_doubles(const DConst& c);
 void spectra_init();
 void launch_spectra(cudaStream_t st, int axis, const DConst& c, const Fields& f, int jlcs, const double2* tw,
                     double* part, double* out);
+void launch_spectra2d(cudaStream_t st, const DConst& c, const Fields& f, const int2* fj, int nfj, int nsel, int nmir,
+                      int nfld, const double2* twx, const double2* twz, double* S, double* out);
 
 // k_plane.cu: both transforms of a y-plane in one CTA (planes that fit shared memory)
 bool plane_supported(int nx, int nz);

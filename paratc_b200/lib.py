@@ -32,6 +32,7 @@ EXPORTED = [
     "paratc_batch_steps", "paratc_batch_graph_kernels", "paratc_batch_stream", "paratc_stats_reset",
     "paratc_stats_accumulate", "paratc_stats_get", "paratc_set_fields_async", "paratc_get_fields_async",
     "paratc_sync", "paratc_spectra_reset", "paratc_spectra_accumulate", "paratc_spectra_get",
+    "paratc_spectra2d_setup", "paratc_spectra2d_reset", "paratc_spectra2d_accumulate", "paratc_spectra2d_get",
 ]
 PROF_NKERNELS = 16
 
@@ -111,6 +112,11 @@ def load(path=None):
     L.paratc_spectra_accumulate.argtypes = [ctypes.c_void_p, ctypes.c_int]
     L.paratc_spectra_get.argtypes = [ctypes.c_void_p, _dp, _dp, ctypes.POINTER(ctypes.c_int),
                                      ctypes.POINTER(ctypes.c_int)]
+    L.paratc_spectra2d_setup.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
+    L.paratc_spectra2d_reset.argtypes = [ctypes.c_void_p]
+    L.paratc_spectra2d_accumulate.argtypes = [ctypes.c_void_p]
+    L.paratc_spectra2d_get.argtypes = [ctypes.c_void_p, _dp, ctypes.POINTER(ctypes.c_int),
+                                       ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
     _lib = L
     return L
 
@@ -352,6 +358,28 @@ class ChannelSystem:
         self._check(self._L.paratc_spectra_get(self._h, _ptr(ex), _ptr(ez), ctypes.byref(n), ctypes.byref(ns)),
                     "paratc_spectra_get")
         return ex, ez, ns.value
+
+    # -- 2-D spectra at the rows iySpec2D
+    def spectra2d_setup(self, iy):
+        iy = np.ascontiguousarray(iy, dtype=np.int32)
+        self._check(self._L.paratc_spectra2d_setup(self._h, len(iy), iy.ctypes.data_as(ctypes.POINTER(ctypes.c_int))),
+                    "paratc_spectra2d_setup")
+
+    def spectra2d_reset(self):
+        self._check(self._L.paratc_spectra2d_reset(self._h), "paratc_spectra2d_reset")
+
+    def spectra2d_accumulate(self):
+        self._check(self._L.paratc_spectra2d_accumulate(self._h), "paratc_spectra2d_accumulate")
+
+    def spectra2d_get(self):
+        """(EnergySpec2D sums [nsp2, nzc, nsel, nxc], nSpectime)."""
+        p = self.params
+        nsp, nsel, ns = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        self._check(self._L.paratc_spectra2d_get(self._h, None, ctypes.byref(nsp), ctypes.byref(nsel),
+                                                 ctypes.byref(ns)), "paratc_spectra2d_get")
+        out = np.zeros((nsp.value, p.nzc, nsel.value, p.nxc))
+        self._check(self._L.paratc_spectra2d_get(self._h, _ptr(out), None, None, None), "paratc_spectra2d_get")
+        return out, ns.value
 
     def project(self):
         dm = ctypes.c_double()

@@ -292,3 +292,34 @@ def test_spectra_same_fields(name):
         for m in range(r.shape[0]):
             e = np.abs(got[m] - r[m]).max() / max(np.abs(r[m]).max(), 1e-300)
             assert e <= 1e-12, "%s spectrum %d rel err %.3e" % (name, m + 1, e)
+
+
+@pytest.mark.parametrize("name", ["channel", "halfchannel_scalar", "channel_odd"])
+def test_spectra2d_accumulate(name):
+    """clcStat's 2-D spectra (halfcomplex-of-halfcomplex x-z transforms at
+    the rows iySpec2D) on identical fields, two samples: 1e-12 of each
+    spectrum's largest magnitude; out-of-range rows are rejected."""
+    case = variant(name)
+    o, g, _ = _pair(case)
+    ny = case.params.nyc
+    iy = [2, ny // 2 - 1, ny // 2] if case.params.flow_type == cases.FT_CH else [2, ny // 2, ny]
+    g.spectra2d_setup(iy)
+    acc = None
+    for _ in range(2):
+        o.step()
+        fo = o.get_fields()
+        g.set_fields(fo["ux"], fo["uy"], fo["uz"], fo["p"], fo["c"])
+        r = o.spectra2d(iy)
+        acc = r if acc is None else acc + r
+        g.spectra2d_accumulate()
+    got, ns = g.spectra2d_get()
+    assert ns == 2 and got.shape == acc.shape
+    for m in range(acc.shape[0]):
+        e = np.abs(got[m] - acc[m]).max() / max(np.abs(acc[m]).max(), 1e-300)
+        assert e <= 1e-12, "%s 2-D spectrum %d rel err %.3e" % (name, m + 1, e)
+    bad = [1] if case.params.flow_type == cases.FT_HC else [ny // 2 + 1]
+    with pytest.raises(Exception):
+        g.spectra2d_setup(bad)
+    g.spectra2d_reset()
+    got, ns = g.spectra2d_get()
+    assert ns == 0 and not got.any()

@@ -306,3 +306,70 @@ def test_spectra_pinned_by_numpy(name):
         for m in range(got.shape[0]):
             err = np.abs(got[m] - ref[m]).max() / max(np.abs(ref[m]).max(), 1e-300)
             assert err < 1e-12, (name, m, err)
+
+
+def _hc(a, axis):
+    """FFTW's R2HC along an axis with numpy: r_0..r_{n/2}, then i_k at n-k."""
+    n = a.shape[axis]
+    X = np.moveaxis(np.fft.rfft(a, axis=axis), axis, -1)
+    out = np.zeros(X.shape[:-1] + (n,))
+    out[..., : n // 2 + 1] = X.real
+    for k in range(1, (n + 1) // 2):
+        out[..., n - k] = X[..., k].imag
+    return np.moveaxis(out, -1, axis)
+
+
+def numpy_spectra2d(params, g, iy):
+    """clcEnergySpectra2D / clcCosSpectra2D (src/m_FlowCase.f90:1186-1375)
+    with numpy: R2HC along x then along z, squares at the rows iy (plus the
+    mirrored row in a channel, the cospectrum subtracting it)."""
+    p = params
+    nx, ny, nz = p.nxc, p.nyc, p.nzc
+    top = p.uy_bc[3] if p.flow_type == cases.FT_CH else 0.0
+    uyn = np.concatenate([g["uy"], np.full((nz, 1, nx), top)], axis=1)
+    uyc = 0.5 * (uyn[:, :-1] + uyn[:, 1:])
+    ic = (-1 / 16, 9 / 16, 9 / 16, -1 / 16)
+    u0 = g["ux"]
+    uxc = ic[0] * np.roll(u0, 1, 2) + ic[1] * u0 + ic[2] * np.roll(u0, -1, 2) + ic[3] * np.roll(u0, -2, 2) + p.ucrf
+    norm = (1.0 / (nx * nz)) ** 2 * (0.5 if p.flow_type == cases.FT_CH else 1.0)
+    hc = p.flow_type == cases.FT_HC
+
+    def H(a, j):  # j: 1-based row; a [z, y, x] (uy may carry the wall row)
+        return _hc(_hc(a[:, j - 1, :], 1), 0)  # [z-hc, x-hc]
+
+    out = []
+    fields = [g["ux"], uyn, g["uz"], g["p"]] + ([g["c"]] if p.scalar_on else [])
+    for m in range(6 if p.scalar_on else 5):
+        planes = []
+        for j in iy:
+            if m == 4:
+                v = H(uxc, j) * H(uyc, j)
+                if not hc:
+                    v = v - H(uxc, ny + 1 - j) * H(uyc, ny + 1 - j)
+            else:
+                a = fields[m if m < 4 else 4]
+                js = (ny + 2 - j) if m == 1 else (ny + 1 - j)
+                v = H(a, j) ** 2 + (0 if hc else H(a, js) ** 2)
+            planes.append(norm * v)
+        out.append(np.stack(planes, axis=1))  # [z, q, x]
+    return np.stack(out)
+
+
+@pytest.mark.parametrize("name", ["channel", "halfchannel_scalar", "channel_odd"])
+def test_spectra2d_pinned_by_numpy(name):
+    case = variant(name)
+    yp = yp_of(case)
+    o = ol.Oracle(case.params, yp)
+    f = fields_of(case, yp)
+    o.set_fields(f["ux"], f["uy"], f["uz"], f["p"], f["c"])
+    o.step()
+    ny = case.params.nyc
+    iy = [2, ny // 2 - 1, ny // 2] if case.params.flow_type == cases.FT_CH else [2, ny // 2, ny]
+    got = o.spectra2d(iy)
+    ref = numpy_spectra2d(case.params, o.get_fields(), iy)
+    assert got.shape == ref.shape
+    for m in range(ref.shape[0]):
+        err = np.abs(got[m] - ref[m]).max() / np.abs(ref[m]).max()
+        assert err < 1e-12, (name, m, err)
+    with pytest.raises(RuntimeError):
+        o.spectra2d([1])
