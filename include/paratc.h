@@ -48,6 +48,7 @@ extern "C" {
 #define PARATC_ERR_TIMEOUT    -7  /* a bounded device wait gave up               */
 #define PARATC_ERR_IO         -8  /* restart file missing, short or wrong size   */
 #define PARATC_ERR_NO_DEVICE  -9  /* no CUDA device / library built without one  */
+#define PARATC_ERR_NUMERIC   -10  /* lambda2 met complex roots (Clc_lamda2 stops) */
 
 /* ---- option values (same numbers as src/m_Parameters.f90) ------------ */
 #define PARATC_FT_CH 1          /* FT_CH: channel, no-slip top and bottom   */
@@ -350,6 +351,63 @@ int paratc_spectra2d_accumulate(paratc_ctx* ctx);
 /* out[((m-1)*nzc + kc)*nsel*nxc + (q-1)*nxc + ic] (EnergySpec2D(nxc, nySpec2D,
  * nzc, m) in Fortran order; may be NULL), nspec: 5 or 6, nsel, nspectime. */
 int paratc_spectra2d_get(paratc_ctx* ctx, double* out, int* nspec, int* nsel, int* nspectime);
+
+/* ---- visualisation dumps (dump_visu, src/m_IOAndVisu.f90:182-385, and the
+ * XDMF index of InitVisu, :29-175) ---------------------------------------- */
+#define PARATC_VISU_UX      0   /* (ux_i + ux_i+1)/2 + uCRF; node: ux + uCRF   */
+#define PARATC_VISU_UY      1   /* (uy_j + uy_j+1)/2;        node: uy          */
+#define PARATC_VISU_UZ      2   /* (uz_k + uz_k+1)/2;        node: uz          */
+#define PARATC_VISU_PR      3   /* pressure                                    */
+#define PARATC_VISU_WX      4   /* vorticity components (2nd-order, :264-330)  */
+#define PARATC_VISU_WY      5
+#define PARATC_VISU_WZ      6
+#define PARATC_VISU_WMAG    7   /* |vorticity|                                 */
+#define PARATC_VISU_Q       8   /* Q criterion (Clc_Q_vor)                     */
+#define PARATC_VISU_LAMDA2  9   /* lambda2 (Clc_lamda2)                        */
+#define PARATC_VISU_SCALAR 10   /* scalar (scalar_on only)                     */
+#define PARATC_VISU_NQ     11
+
+/* One quantity at the points decomp_2d_write_every keeps with from1 = .true.
+ * (src/m_Decomp2d.f90:1232-1389): global indices 1, 1+skip, ... in each
+ * direction, nxo = ceil(nxc/iskip) (likewise y, z) values in Fortran order
+ * (x fastest), FP64.  node != 0 selects the SaveNode build (staggered
+ * velocities instead of cell-centre averages).  count (may be NULL) gets
+ * nxo*nyo*nzo; out may be NULL to query it.  Returns PARATC_ERR_NUMERIC
+ * (after filling out) when lambda2 met a point whose cubic has complex
+ * roots, where the reference stops. */
+int paratc_visu_quantity(paratc_ctx* ctx, int q, int iskip, int jskip, int kskip, int node, double* out,
+                         int64_t* count);
+/* Name of quantity q as it appears in the file names ("ux", ..., "wMag",
+ * "Q", "lamda2", "scalar"). */
+const char* paratc_visu_name(int q);
+/* dump_visu: for every q with bit q of save_mask set, writes
+ * res_dir + "VisuFor" + run_name + "_" + name + "_" + ntime (10 digits,
+ * zero padded): the kept points in Fortran order as REAL(8), or REAL(4)
+ * when single != 0 (the SAVE_SINGLE build). */
+int paratc_dump_visu(paratc_ctx* ctx, const char* res_dir, const char* run_name, int ntime, int save_mask, int iskip,
+                     int jskip, int kskip, int node, int single);
+/* InitVisu's XDMF index res_dir + "VisuFor" + run_name + ".xmf": the
+ * rectilinear grid (XDMF_SET_TYPE 0: cell corners x = (i-1) dx, yp, z; 1:
+ * cell centres) and one temporal entry per ifld = ifirst-1, ifirst-1 +
+ * save_visu, ..., ilast with a binary attribute per quantity in save_mask.
+ * yp: yp(1..nyp). */
+int paratc_write_xdmf(const paratc_params* prm, const double* yp, const char* res_dir, const char* run_name,
+                      int ifirst, int ilast, int save_visu, int save_mask, int xdmf_set_type, int single);
+
+/* &IO_Options (+ &SaveScalarOption), &SpectraOptions + &Spectra2DOpt and the
+ * output cadences of &BasicParam (src/m_IOAndVisu.f90:37-41,
+ * src/m_FlowCase.f90:140-151,209-214, src/m_Parameters.f90:118-121). */
+#define PARATC_MAX_SPEC2D 64
+typedef struct paratc_io_options {
+    int32_t ivstats, save_stat, save_visu;           /* &BasicParam            */
+    int32_t iskip, jskip, kskip, xdmf_set_type;      /* &IO_Options            */
+    int32_t save_mask;                               /* bit PARATC_VISU_* set when save_<name> = T */
+    int32_t write_hist_old, read_hist_old;
+    int32_t clc_spectra1d, iv_spec, j_for_lcs;       /* &SpectraOptions        */
+    int32_t clc_spectra2d, ny_spec2d;
+    int32_t iy_spec2d[PARATC_MAX_SPEC2D];            /* &Spectra2DOpt          */
+} paratc_io_options;
+int paratc_io_options_from_namelist(const char* path, int scalar_on, paratc_io_options* out);
 
 /* ---- Ensembles.  No counterpart in the reference, which advances one case
  * per MPI job; this is the batched form of ChannelIterate

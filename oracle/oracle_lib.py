@@ -51,6 +51,7 @@ def lib():
         L.orc_stats.argtypes = [ctypes.c_void_p, _dp]
         L.orc_spectra.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, _dp]
         L.orc_spectra2d.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int32), _dp]
+        L.orc_visu.argtypes = [ctypes.c_void_p] + [ctypes.c_int] * 5 + [_dp]
         L.orc_r2hc.argtypes = [ctypes.c_int, _dp, _dp]
         L.orc_hc2r.argtypes = [ctypes.c_int, _dp, _dp]
         L.orc_ycoord.argtypes = [ctypes.c_int, _dp, _dp, ctypes.POINTER(ctypes.c_int32),
@@ -242,6 +243,17 @@ class Oracle:
         rc = lib().orc_spectra2d(self._h, len(iy), iy.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), _ptr(out))
         if rc != 0:
             raise RuntimeError("orc_spectra2d rc=%d" % rc)
+        return out
+
+    def visu(self, q, skip=(1, 1, 1), node=False):
+        """dump_visu's quantity q (PARATC_VISU_* number) at the kept points
+        1, 1+skip, ...: [nzo, nyo, nxo]; raises on complex lambda2 roots."""
+        p = self.params
+        shape = tuple(-(-a // s) for a, s in zip((p.nzc, p.nyc, p.nxc), (skip[2], skip[1], skip[0])))
+        out = np.zeros(shape)
+        rc = lib().orc_visu(self._h, int(q), int(skip[0]), int(skip[1]), int(skip[2]), int(bool(node)), _ptr(out))
+        if rc != 0:
+            raise RuntimeError("orc_visu rc=%d" % rc)
         return out
 
     def metric(self, name):

@@ -1708,3 +1708,119 @@ int orc_metric(orc_t* o, const char* name, double* out, int cap) {
     }
     return PARATC_ERR_BAD_ARG;
 }
+
+
+/* ------------------------------------------------------------------------
+ * dump_visu (src/m_IOAndVisu.f90:182-385) with Clc_Q_vor, Clc_lamda2 and
+ * CubicRoot (src/m_Tools.f90:305-440, 494-570), at the points
+ * decomp_2d_write_every keeps with from1 = .true. (src/m_Decomp2d.f90:
+ * 1232-1389): ic = 1, 1+iskip, ... (likewise j, k), Fortran order.
+ * Quantity numbers as PARATC_VISU_*.  Returns PARATC_ERR_NUMERIC after
+ * filling out when lambda2 met complex roots (the reference stops there).
+ * ---------------------------------------------------------------------- */
+static double cubic_root2(double b, double c, double d, int* allreal) {
+    const double SMALL = 1.0E-12, OneThird = 0.3333333333333333333333;
+    const double Pi = 3.141592653589793238462643383279502884;
+    double p = c - OneThird * b * b;
+    double q = (2.0 * b * b * b - 9.0 * b * c + 27.0 * d) / 27.0;
+    double t = q * q / 4.0 + p * p * p / 27.0;
+    if (t < 0.0) {
+        *allreal = 1;
+        t = -OneThird * b;
+        double rho = pow(-p, 1.5) / sqrt(27.0);
+        double eta = acos(0.5 * q / rho);
+        rho = -2.0 * pow(rho, OneThird);
+        double root1 = cos(OneThird * eta) * rho + t;
+        double root2 = cos(OneThird * (2.0 * Pi + eta)) * rho + t;
+        double root3 = cos(OneThird * (4.0 * Pi + eta)) * rho + t;
+        if (root1 < root2 && root1 < root3) return root2 < root3 ? root2 : root3;
+        else if (root1 > root2 && root1 > root3) return root2 < root3 ? root3 : root2;
+        else return root1;
+    } else if (t < SMALL) {
+        *allreal = 1;
+        double rho = 0.5 * q;
+        if (rho < 0.0) rho = pow(-rho, OneThird);
+        else rho = -pow(rho, OneThird);
+        return -rho - OneThird * b;
+    }
+    *allreal = 0;
+    t = sqrt(t);
+    double rho = 0.5 * q + t, eta = 0.5 * q - t;
+    if (rho < 0.0) rho = pow(-rho, OneThird); else rho = -pow(rho, OneThird);
+    if (eta < 0.0) eta = pow(-eta, OneThird); else eta = -pow(eta, OneThird);
+    return -0.5 * (rho + eta) - OneThird * b;
+}
+
+int orc_visu(orc_t* o, int qn, int iskip, int jskip, int kskip, int node, double* out) {
+    if (!o || !out || qn < 0 || qn > 10 || iskip < 1 || jskip < 1 || kskip < 1) return PARATC_ERR_BAD_ARG;
+    if (qn == 10 && !o->p.scalar_on) return PARATC_ERR_BAD_ARG;
+    const int nxc = o->nxc, nyc = o->nyc, nzc = o->nzc;
+    const int nxo = (nxc + iskip - 1) / iskip, nyo = (nyc + jskip - 1) / jskip, nzo = (nzc + kskip - 1) / kskip;
+    const double *ux = o->ux, *uy = o->uy, *uz = o->uz, *pr = o->pr, *sc = o->sc;
+    const double rdx = o->rdx, rdz = o->rdz, uCRF = o->p.ucrf;
+    upd_halo(o, o->ux, 2, 2, 2, 2);
+    upd_halo(o, o->uy, 2, 2, 2, 2);
+    upd_halo(o, o->uz, 2, 2, 2, 2);
+    int nbad = 0;
+#pragma omp parallel for schedule(static) reduction(+ : nbad)
+    for (int ko = 0; ko < nzo; ko++) {
+        const int kc = 1 + ko * kskip, kp = kc + 1, km = kc - 1;
+        for (int jo = 0; jo < nyo; jo++) {
+            const int jc = 1 + jo * jskip, jp = jc + 1, jm = jc - 1;
+            const double caj = o->rdyp[jc], cac1 = o->rdyc[jc], cac2 = o->rdyc[jp], cac12 = cac1 - cac2;
+            for (int io = 0; io < nxo; io++) {
+                const int ic = 1 + io * iskip, ip = ic + 1, im = ic - 1;
+#define A(a, i, j, k) (a)[HX(o, i, j, k)]
+                double v;
+                if (qn == 0) v = node ? A(ux, ic, jc, kc) + uCRF : half * (A(ux, ic + 1, jc, kc) + A(ux, ic, jc, kc)) + uCRF;
+                else if (qn == 1) v = node ? A(uy, ic, jc, kc) : half * (A(uy, ic, jc + 1, kc) + A(uy, ic, jc, kc));
+                else if (qn == 2) v = node ? A(uz, ic, jc, kc) : half * (A(uz, ic, jc, kc + 1) + A(uz, ic, jc, kc));
+                else if (qn == 3) v = A(pr, ic, jc, kc);
+                else if (qn == 10) v = A(sc, ic, jc, kc);
+                else {
+                    double dudx = (A(ux, ip, jc, kc) - A(ux, ic, jc, kc)) * rdx;
+                    double dudy = ((A(ux, ip, jp, kc) + A(ux, ic, jp, kc)) * cac2 + (A(ux, ip, jc, kc) + A(ux, ic, jc, kc)) * cac12 -
+                                   (A(ux, ip, jm, kc) + A(ux, ic, jm, kc)) * cac1) * quarter;
+                    double dudz = (A(ux, ip, jc, kp) + A(ux, ic, jc, kp) - A(ux, ip, jc, km) - A(ux, ic, jc, km)) * rdz * quarter;
+                    double dvdx = (A(uy, ip, jp, kc) - A(uy, im, jp, kc) + A(uy, ip, jc, kc) - A(uy, im, jc, kc)) * rdx * quarter;
+                    double dvdy = (A(uy, ic, jp, kc) - A(uy, ic, jc, kc)) * caj;
+                    double dvdz = (A(uy, ic, jp, kp) + A(uy, ic, jc, kp) - A(uy, ic, jp, km) - A(uy, ic, jc, km)) * rdz * quarter;
+                    double dwdx = (A(uz, ip, jc, kp) - A(uz, im, jc, kp) + A(uz, ip, jc, kc) - A(uz, im, jc, kc)) * rdx * quarter;
+                    double dwdy = ((A(uz, ic, jp, kp) + A(uz, ic, jp, kc)) * cac2 + (A(uz, ic, jc, kp) + A(uz, ic, jc, kc)) * cac12 -
+                                   (A(uz, ic, jm, kp) + A(uz, ic, jm, kc)) * cac1) * quarter;
+                    double dwdz = (A(uz, ic, jc, kp) - A(uz, ic, jc, kc)) * rdz;
+#undef A
+                    if (qn == 4) v = dwdy - dvdz;
+                    else if (qn == 5) v = dudz - dwdx;
+                    else if (qn == 6) v = dvdx - dudy;
+                    else if (qn == 7) {
+                        double vor_x = dwdy - dvdz, vor_y = dudz - dwdx, vor_z = dvdx - dudy;
+                        v = sqrt(vor_x * vor_x + vor_y * vor_y + vor_z * vor_z);
+                    } else if (qn == 8) {
+                        double udiv = dudx + dvdy + dwdz;
+                        v = half * (udiv * udiv - dudx * dudx - dvdy * dvdy - dwdz * dwdz) - dudy * dvdx - dudz * dwdx - dvdz * dwdy;
+                    } else {
+                        double Ome12 = dvdx - dudy, Ome23 = dwdy - dvdz, Ome31 = dudz - dwdx;
+                        double Eps11 = dudx + dudx, Eps12 = dudy + dvdx, Eps13 = dudz + dwdx;
+                        double Eps22 = dvdy + dvdy, Eps23 = dvdz + dwdy, Eps33 = dwdz + dwdz;
+                        double Lam12 = Eps11 * Eps12 + Eps12 * Eps22 + Eps13 * Eps23 + Ome31 * Ome23;
+                        double Lam13 = Eps11 * Eps13 + Eps12 * Eps23 + Eps13 * Eps33 + Ome12 * Ome23;
+                        double Lam23 = Eps12 * Eps13 + Eps22 * Eps23 + Eps23 * Eps33 + Ome12 * Ome31;
+                        double Lam11 = Eps11 * Eps11 + Eps12 * Eps12 + Eps13 * Eps13 - Ome12 * Ome12 - Ome31 * Ome31;
+                        double Lam22 = Eps12 * Eps12 + Eps22 * Eps22 + Eps23 * Eps23 - Ome12 * Ome12 - Ome23 * Ome23;
+                        double Lam33 = Eps13 * Eps13 + Eps23 * Eps23 + Eps33 * Eps33 - Ome31 * Ome31 - Ome23 * Ome23;
+                        double rb = -(Lam11 + Lam22 + Lam33);
+                        double rc = Lam11 * Lam22 + Lam22 * Lam33 + Lam33 * Lam11 - Lam12 * Lam12 - Lam13 * Lam13 - Lam23 * Lam23;
+                        double rd = Lam12 * Lam12 * Lam33 + Lam13 * Lam13 * Lam22 + Lam23 * Lam23 * Lam11 - Lam11 * Lam22 * Lam33 -
+                                    2.0 * Lam12 * Lam23 * Lam13;
+                        int allreal;
+                        v = quarter * cubic_root2(rb, rc, rd, &allreal);
+                        if (!allreal) nbad++;
+                    }
+                }
+                out[((size_t)ko * nyo + jo) * nxo + io] = v;
+            }
+        }
+    }
+    return nbad ? PARATC_ERR_NUMERIC : 0;
+}

@@ -62,6 +62,10 @@ int  orc_spectra(orc_t* o, int jlcs, double* egx, double* egz);
  * the scalar): ux, uy, uz, p, <ux_c uy_c> [, scalar] of the halfcomplex-of-
  * halfcomplex x-z transform. */
 int  orc_spectra2d(orc_t* o, int nsel, const int* iy, double* out);
+/* dump_visu's quantity q (PARATC_VISU_* numbering) at the points
+ * decomp_2d_write_every keeps (1, 1+skip, ...), Fortran order; node != 0 is
+ * the SaveNode build.  PARATC_ERR_NUMERIC when lambda2 met complex roots. */
+int  orc_visu(orc_t* o, int q, int iskip, int jskip, int kskip, int node, double* out);
 
 /* real DFT helpers in FFTW's halfcomplex convention (for pinning) */
 int  orc_r2hc(int n, const double* in, double* out);

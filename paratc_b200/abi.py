@@ -14,12 +14,18 @@ PARATC_ERR_VEL_LIMIT = -6
 PARATC_ERR_TIMEOUT = -7
 PARATC_ERR_IO = -8
 PARATC_ERR_NO_DEVICE = -9
+PARATC_ERR_NUMERIC = -10
 
 FT_CH = 1
 FT_HC = 2
 AB2, RK2, RK3 = 1, 2, 3
 LAYOUT_INTERIOR = 0
 LAYOUT_HALO = 1
+
+# dump_visu quantities (PARATC_VISU_*)
+VISU_NAMES = ("ux", "uy", "uz", "pr", "wx", "wy", "wz", "wMag", "Q", "lamda2", "scalar")
+VISU = {n: q for q, n in enumerate(VISU_NAMES)}
+MAX_SPEC2D = 64
 
 _d3 = ctypes.c_double * 3
 _d6 = ctypes.c_double * 6
@@ -72,3 +78,17 @@ class ParatcDiag(ctypes.Structure):
             "pr_grad_aver": self.pr_grad_aver, "ux_mean": self.ux_mean,
             "sc_mean": self.sc_mean, "sc2_mean": self.sc2_mean,
         }
+
+
+class ParatcIoOptions(ctypes.Structure):
+    """struct paratc_io_options (include/paratc.h)."""
+
+    _fields_ = [
+        ("ivstats", ctypes.c_int32), ("save_stat", ctypes.c_int32), ("save_visu", ctypes.c_int32),
+        ("iskip", ctypes.c_int32), ("jskip", ctypes.c_int32), ("kskip", ctypes.c_int32),
+        ("xdmf_set_type", ctypes.c_int32), ("save_mask", ctypes.c_int32),
+        ("write_hist_old", ctypes.c_int32), ("read_hist_old", ctypes.c_int32),
+        ("clc_spectra1d", ctypes.c_int32), ("iv_spec", ctypes.c_int32), ("j_for_lcs", ctypes.c_int32),
+        ("clc_spectra2d", ctypes.c_int32), ("ny_spec2d", ctypes.c_int32),
+        ("iy_spec2d", ctypes.c_int32 * MAX_SPEC2D),
+    ]

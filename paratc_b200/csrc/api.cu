@@ -77,6 +77,8 @@ struct paratc_ctx {
     int nsel2 = 0, nfj2 = 0, nmir2 = 0, nfld2 = 0;
     size_t spec2d_cap = 0, s2_cap = 0, fj_cap = 0;  // capacities of the three buffers (elements)
     int nspectime2 = 0;                 // 2-D spectra samples accumulated
+    double* d_visu = nullptr;           // one visu quantity at the kept points (nx*ny*nz doubles, first use)
+    unsigned int* d_visu_bad = nullptr; // lambda2 points with complex roots
     DDiag* h_diag = nullptr;   // pinned
     DCoef* h_coef = nullptr;   // pinned
     DCoef* h_coef0 = nullptr;  // pinned, the coefficient block of a freshly loaded state (never rewritten)
@@ -351,6 +353,7 @@ const char* paratc_strerror(int status) {
     case PARATC_ERR_TIMEOUT: return "device wait timed out";
     case PARATC_ERR_IO: return "restart/input file error";
     case PARATC_ERR_NO_DEVICE: return "no CUDA device";
+    case PARATC_ERR_NUMERIC: return "lamda2 wrong";
     default: return "unknown status";
     }
 }
@@ -1047,6 +1050,74 @@ int paratc_spectra2d_get(paratc_ctx* ctx, double* out, int* nspec, int* nsel, in
     CK(cudaMemcpyAsync(out, ctx->d_spec2d, (size_t)nsp * ctx->nsel2 * ctx->nx * ctx->nz * sizeof(double),
                        cudaMemcpyDefault, ctx->st));
     return sync(ctx);
+}
+
+const char* paratc_visu_name(int q) {
+    static const char* names[PARATC_VISU_NQ] = {"ux", "uy", "uz", "pr", "wx", "wy", "wz", "wMag", "Q", "lamda2", "scalar"};
+    return (q >= 0 && q < PARATC_VISU_NQ) ? names[q] : "";
+}
+
+int paratc_visu_quantity(paratc_ctx* ctx, int q, int iskip, int jskip, int kskip, int node, double* out,
+                         int64_t* count) {
+    if (!ctx || q < 0 || q >= PARATC_VISU_NQ || iskip < 1 || jskip < 1 || kskip < 1) return PARATC_ERR_BAD_ARG;
+    if (q == PARATC_VISU_SCALAR && !ctx->prm.scalar_on) return PARATC_ERR_BAD_ARG;
+    const int64_t n = (int64_t)visu_count(ctx->nx, iskip) * visu_count(ctx->ny, jskip) * visu_count(ctx->nz, kskip);
+    if (count) *count = n;
+    if (!out) return PARATC_OK;
+    CK(cudaSetDevice(ctx->dev));
+    int rc;
+    if (!ctx->d_visu) {
+        if ((rc = dalloc(ctx, &ctx->d_visu, ctx->ni)) || (rc = dalloc(ctx, &ctx->d_visu_bad, 1))) return rc;
+    }
+    CK(cudaMemsetAsync(ctx->d_visu_bad, 0, sizeof(unsigned int), ctx->st));
+    launch_visu(ctx->st, q, iskip, jskip, kskip, node, ctx->kc, ctx->dm, ctx->f, ctx->d_visu, ctx->d_visu_bad);
+    ctx->launches += 1;
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(out, ctx->d_visu, (size_t)n * sizeof(double), cudaMemcpyDefault, ctx->st));
+    unsigned int* hb = reinterpret_cast<unsigned int*>(ctx->h_scal);
+    CK(cudaMemcpyAsync(hb, ctx->d_visu_bad, sizeof(unsigned int), cudaMemcpyDeviceToHost, ctx->st));
+    if ((rc = sync(ctx))) return rc;
+    if (*hb) {
+        char b[128];
+        std::snprintf(b, sizeof(b), "lamda2 wrong: %u points with complex roots", *hb);
+        return set_err(ctx, PARATC_ERR_NUMERIC, b);
+    }
+    return PARATC_OK;
+}
+
+int paratc_dump_visu(paratc_ctx* ctx, const char* res_dir, const char* run_name, int ntime, int save_mask, int iskip,
+                     int jskip, int kskip, int node, int single) {
+    if (!ctx || !res_dir || !run_name || ntime < 0) return PARATC_ERR_BAD_ARG;
+    // the order dump_visu writes them in
+    const int order[PARATC_VISU_NQ] = {PARATC_VISU_UX, PARATC_VISU_UY, PARATC_VISU_UZ, PARATC_VISU_PR,
+                                       PARATC_VISU_SCALAR, PARATC_VISU_WX, PARATC_VISU_WY, PARATC_VISU_WZ,
+                                       PARATC_VISU_WMAG, PARATC_VISU_Q, PARATC_VISU_LAMDA2};
+    int64_t n = 0;
+    int rc = paratc_visu_quantity(ctx, PARATC_VISU_UX, iskip, jskip, kskip, node, nullptr, &n);
+    if (rc) return rc;
+    std::vector<double> buf((size_t)n);
+    std::vector<float> fbuf(single ? (size_t)n : 0);
+    for (int a = 0; a < PARATC_VISU_NQ; a++) {
+        const int q = order[a];
+        if (!(save_mask & (1 << q))) continue;
+        if (q == PARATC_VISU_SCALAR && !ctx->prm.scalar_on) continue;
+        if ((rc = paratc_visu_quantity(ctx, q, iskip, jskip, kskip, node, buf.data(), nullptr))) return rc;
+        char tail[32];
+        std::snprintf(tail, sizeof(tail), "_%010d", ntime);
+        const std::string path = std::string(res_dir) + "VisuFor" + run_name + "_" + paratc_visu_name(q) + tail;
+        FILE* fp = std::fopen(path.c_str(), "wb");
+        if (!fp) return set_err(ctx, PARATC_ERR_IO, "Cannot open file: " + path);
+        size_t w;
+        if (single) {
+            for (size_t e = 0; e < buf.size(); e++) fbuf[e] = (float)buf[e];
+            w = std::fwrite(fbuf.data(), sizeof(float), fbuf.size(), fp);
+        } else {
+            w = std::fwrite(buf.data(), sizeof(double), buf.size(), fp);
+        }
+        std::fclose(fp);
+        if (w != buf.size()) return set_err(ctx, PARATC_ERR_IO, "short write: " + path);
+    }
+    return PARATC_OK;
 }
 
 }  // extern "C"

@@ -514,3 +514,157 @@ extern "C" int paratc_run_options_from_namelist(const char* path, paratc_run_opt
     std::snprintf(out->restart_dir, sizeof(out->restart_dir), "%s", ro.restart_dir);
     return PARATC_OK;
 }
+
+// ---------------------------------------------------------------------------
+// output options: &IO_Options and &SaveScalarOption (InitVisu,
+// src/m_IOAndVisu.f90:29-53), &SpectraOptions and &Spectra2DOpt
+// (InitStatVar, src/m_FlowCase.f90:127-235) and the output cadences of
+// &BasicParam, with the checks those routines make
+// ---------------------------------------------------------------------------
+extern "C" int paratc_io_options_from_namelist(const char* path, int scalar_on, paratc_io_options* out) {
+    if (!path || !out) return PARATC_ERR_BAD_ARG;
+    std::memset(out, 0, sizeof(*out));
+    std::ifstream in(path);
+    if (!in) { std::fprintf(stderr, "paratc_io_options_from_namelist: Cannot open file: %s\n", path); return PARATC_ERR_IO; }
+    std::stringstream ss;
+    ss << in.rdbuf();
+    const std::string text = ss.str();
+    using Group = std::map<std::string, std::vector<std::string>>;
+    Group bp, io, sso, sp, s2;
+    auto fail = [&](const char* why) {
+        std::fprintf(stderr, "paratc_io_options_from_namelist: %s\n", why);
+        return PARATC_ERR_BAD_ARG;
+    };
+    if (ptc::read_group(text, "BasicParam", bp) != PARATC_OK) return fail("&BasicParam missing or malformed");
+    if (ptc::read_group(text, "IO_Options", io) != PARATC_OK) return fail("&IO_Options missing or malformed");
+    if (ptc::read_group(text, "SpectraOptions", sp) != PARATC_OK) return fail("&SpectraOptions missing or malformed");
+    if (scalar_on && ptc::read_group(text, "SaveScalarOption", sso) != PARATC_OK)
+        return fail("&SaveScalarOption missing or malformed");
+    auto geti = [&](Group& g, const char* n, int idx, int dflt) {
+        auto it = g.find(ptc::lower(n));
+        if (it == g.end() || (int)it->second.size() <= idx) return dflt;
+        return (int)std::lround(ptc::to_d(it->second[idx]));
+    };
+    auto getb = [&](Group& g, const char* n, bool dflt) {
+        auto it = g.find(ptc::lower(n));
+        if (it == g.end() || it->second.empty()) return dflt;
+        return ptc::to_b(it->second[0]);
+    };
+    out->ivstats = geti(bp, "ivstats", 0, 1);
+    out->save_stat = geti(bp, "SaveStat", 0, 1);
+    out->save_visu = geti(bp, "SaveVisu", 0, 1);
+    out->iskip = geti(io, "iskip", 0, 1);
+    out->jskip = geti(io, "jskip", 0, 1);
+    out->kskip = geti(io, "kskip", 0, 1);
+    out->xdmf_set_type = geti(io, "XDMF_SET_TYPE", 0, 0);
+    const char* flags[PARATC_VISU_NQ] = {"save_ux", "save_uy", "save_uz", "save_pr", "save_wx", "save_wy",
+                                         "save_wz", "save_wMag", "save_Q_vor", "save_lamda2", nullptr};
+    for (int q = 0; q < PARATC_VISU_NQ; q++) {
+        const bool on = (q == PARATC_VISU_SCALAR) ? (scalar_on && getb(sso, "save_scalar", false)) : getb(io, flags[q], false);
+        if (on) out->save_mask |= 1 << q;
+    }
+    out->write_hist_old = getb(io, "WriteHistOld", false) ? 1 : 0;
+    out->read_hist_old = getb(io, "ReadHistOld", false) ? 1 : 0;
+    out->clc_spectra1d = getb(sp, "clcSpectra1D", false) ? 1 : 0;
+    out->iv_spec = geti(sp, "ivSpec", 0, 1);
+    out->j_for_lcs = geti(sp, "jForLCS", 0, 1);
+    out->clc_spectra2d = getb(sp, "clcSpectra2D", false) ? 1 : 0;
+    out->ny_spec2d = geti(sp, "nySpec2D", 0, 0);
+    if (out->ivstats < 1 || out->save_stat < 1 || out->save_visu < 1 || out->iskip < 1 || out->jskip < 1 || out->kskip < 1)
+        return fail("ivstats, SaveStat, SaveVisu and the skips must be >= 1");
+    if (out->save_stat % out->ivstats != 0) return fail("ivstats wrong !!!");
+    if (out->clc_spectra1d && (out->iv_spec < 1 || out->save_stat % out->iv_spec != 0 || out->iv_spec % out->ivstats != 0))
+        return fail("ivSpec wrong !!!");
+    if (out->ny_spec2d < 1) out->clc_spectra2d = 0;
+    if (out->clc_spectra2d) {
+        if (out->ny_spec2d > PARATC_MAX_SPEC2D) return fail("nySpec2D above PARATC_MAX_SPEC2D");
+        if (ptc::read_group(text, "Spectra2DOpt", s2) != PARATC_OK) return fail("&Spectra2DOpt missing or malformed");
+        for (int q = 0; q < out->ny_spec2d; q++) out->iy_spec2d[q] = geti(s2, "iySpec2D", q, 0);
+    }
+    return PARATC_OK;
+}
+
+// Fortran's Ew.d edit descriptor for w = d + 7 (the coordinates of the XDMF
+// index are written with E14.7): right-justified [-]0.ddddddd E+ee
+static std::string fortran_e(double v, int w, int d) {
+    char m[64];
+    std::snprintf(m, sizeof(m), "%.*e", d - 1, v);  // d significant digits: x.xxxxxxe+yy
+    std::string s(m);
+    const bool neg = s[0] == '-';
+    if (neg) s = s.substr(1);
+    const size_t epos = s.find('e');
+    std::string digits = s.substr(0, 1) + s.substr(2, epos - 2);
+    int ex = std::atoi(s.c_str() + epos + 1) + 1;
+    if (v == 0.0) ex = 0;
+    char e[16];
+    std::snprintf(e, sizeof(e), "E%c%02d", ex < 0 ? '-' : '+', ex < 0 ? -ex : ex);
+    std::string r = std::string(neg ? "-" : "") + "0." + digits + e;
+    if ((int)r.size() < w) r = std::string(w - r.size(), ' ') + r;
+    return r;
+}
+
+extern "C" int paratc_write_xdmf(const paratc_params* prm, const double* yp, const char* res_dir, const char* run_name,
+                                 int ifirst, int ilast, int save_visu, int save_mask, int xdmf_set_type, int single) {
+    if (!prm || !yp || !res_dir || !run_name || save_visu < 1) return PARATC_ERR_BAD_ARG;
+    const int nxc = prm->nxc, nyc = prm->nyc, nzc = prm->nzc;
+    const int iprec = single ? 4 : 8;
+    const double dx = prm->xlx / (double)nxc, dz = prm->zlz / (double)nzc, half = 0.5;
+    const std::string path = std::string(res_dir) + "VisuFor" + run_name + ".xmf";
+    FILE* fp = std::fopen(path.c_str(), "w");
+    if (!fp) { std::fprintf(stderr, "paratc_write_xdmf: Cannot open file: %s\n", path.c_str()); return PARATC_ERR_IO; }
+    const char* set_str = xdmf_set_type == 0 ? "\" Center=\"Cell\">" : "\" Center=\"Node\">";
+    const int nxo = xdmf_set_type == 0 ? nxc + 1 : nxc, nyo = xdmf_set_type == 0 ? nyc + 1 : nyc;
+    const int nzo = xdmf_set_type == 0 ? nzc + 1 : nzc;
+    std::fprintf(fp, "<?xml version=\"1.0\" ?>\n");
+    std::fprintf(fp, "<!DOCTYPE Xdmf SYSTEM \"Xdmf.dtd\" []>\n");
+    std::fprintf(fp, "<Xdmf xmlns:xi=\"http://www.w3.org/2001/XInclude\" Version=\"2.0\">\n");
+    std::fprintf(fp, "<Domain>\n");
+    std::fprintf(fp, "    <Topology name=\"TOPO\" TopologyType=\"3DRectMesh\" Dimensions=\"%5d%5d%5d\"/>\n", nzo, nyo, nxo);
+    std::fprintf(fp, "    <Geometry name=\"GEO\" GeometryType=\"VXVYVZ\">\n");
+    auto axis = [&](int n, auto coord) {
+        std::fprintf(fp, "        <DataItem Format=\"XML\" DataType=\"Float\" Precision=\"%1d\" Endian=\"Native\" Dimensions=\"%5d\">\n",
+                     iprec, n);
+        std::fprintf(fp, "        ");
+        for (int i = 1; i <= n; i++) std::fprintf(fp, "%s", fortran_e(coord(i), 14, 7).c_str());
+        std::fprintf(fp, " \n");
+        std::fprintf(fp, "        </DataItem>\n");
+    };
+    axis(nxo, [&](int i) { return xdmf_set_type == 0 ? (double)(i - 1) * dx : (double)(i - 1) * dx + dx * half; });
+    axis(nyo, [&](int j) { return xdmf_set_type == 0 ? yp[j - 1] : half * (yp[j - 1] + yp[j]); });
+    axis(nzo, [&](int k) { return xdmf_set_type == 0 ? (double)(k - 1) * dz : (double)(k - 1) * dz + dz * half; });
+    std::fprintf(fp, "    </Geometry>\n");
+    const int nflds = (ilast - ifirst + 1) / save_visu + 1;
+    std::fprintf(fp, "    <Grid Name=\"TimeSeries\" GridType=\"Collection\" CollectionType=\"Temporal\">\n");
+    std::fprintf(fp, "        <Time TimeType=\"List\">\n");
+    std::fprintf(fp, "        <DataItem Format=\"XML\" NumberType=\"Int\" Dimensions=\"%6d\">\n", nflds);
+    std::fprintf(fp, "        ");
+    for (int f = ifirst - 1; f <= ilast; f += save_visu) std::fprintf(fp, "%10d", f);
+    std::fprintf(fp, "        </DataItem>\n");
+    std::fprintf(fp, " \n");
+    std::fprintf(fp, "       </Time>\n");
+    // the order of InitVisu's Write_XDMF_One calls
+    const int order[PARATC_VISU_NQ] = {PARATC_VISU_UX, PARATC_VISU_UY, PARATC_VISU_UZ, PARATC_VISU_PR,
+                                       PARATC_VISU_WX, PARATC_VISU_WY, PARATC_VISU_WZ, PARATC_VISU_WMAG,
+                                       PARATC_VISU_Q, PARATC_VISU_LAMDA2, PARATC_VISU_SCALAR};
+    for (int f = ifirst - 1; f <= ilast; f += save_visu) {
+        std::fprintf(fp, "        <Grid Name=\"T%010d\" GridType=\"Uniform\">\n", f);
+        std::fprintf(fp, "            <Topology Reference=\"/Xdmf/Domain/Topology[1]\"/>\n");
+        std::fprintf(fp, "            <Geometry Reference=\"/Xdmf/Domain/Geometry[1]\"/>\n");
+        for (int a = 0; a < PARATC_VISU_NQ; a++) {
+            const int q = order[a];
+            if (!(save_mask & (1 << q)) || (q == PARATC_VISU_SCALAR && !prm->scalar_on)) continue;
+            const char* name = paratc_visu_name(q);
+            std::fprintf(fp, "            <Attribute Name=\"%s%s\n", name, set_str);
+            std::fprintf(fp, "                <DataItem Format=\"Binary\" DataType=\"Float\" Precision=\"%1d\" Endian=\"Native\" Dimensions=\"%5d%5d%5d\">\n",
+                         iprec, nzc, nyc, nxc);
+            std::fprintf(fp, "                    VisuFor%s_%s_%010d\n", run_name, name, f);
+            std::fprintf(fp, "                </DataItem>\n");
+            std::fprintf(fp, "            </Attribute>\n");
+        }
+        std::fprintf(fp, "        </Grid>\n");
+    }
+    std::fprintf(fp, "    </Grid>\n");
+    std::fprintf(fp, "</Domain>\n");
+    std::fprintf(fp, "</Xdmf>\n");
+    return std::fclose(fp) == 0 ? PARATC_OK : PARATC_ERR_IO;
+}

@@ -89,6 +89,11 @@ void launch_spectra(cudaStream_t st, int axis, const DConst& c, const Fields& f,
 void launch_spectra2d(cudaStream_t st, const DConst& c, const Fields& f, const int2* fj, int nfj, int nsel, int nmir,
                       int nfld, const double2* twx, const double2* twz, double* S, double* out);
 
+// k_visu.cu: the quantities of dump_visu at the kept points
+int visu_count(int n, int skip);
+void launch_visu(cudaStream_t st, int q, int iskip, int jskip, int kskip, int node, const DConst& c, const DMetric& m,
+                 const Fields& f, double* out, unsigned int* nbad);
+
 // k_plane.cu: both transforms of a y-plane in one CTA (planes that fit shared memory)
 bool plane_supported(int nx, int nz);
 void plane_init();

@@ -12,7 +12,7 @@ import os
 
 import numpy as np
 
-from .abi import (LAYOUT_INTERIOR, PARATC_ERR_DIV_LIMIT, PARATC_ERR_VEL_LIMIT, PARATC_OK, ParatcDiag,
+from .abi import (LAYOUT_INTERIOR, VISU, VISU_NAMES, ParatcIoOptions, PARATC_ERR_DIV_LIMIT, PARATC_ERR_VEL_LIMIT, PARATC_OK, ParatcDiag,
                   ParatcParams)
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
@@ -33,6 +33,8 @@ EXPORTED = [
     "paratc_stats_accumulate", "paratc_stats_get", "paratc_set_fields_async", "paratc_get_fields_async",
     "paratc_sync", "paratc_spectra_reset", "paratc_spectra_accumulate", "paratc_spectra_get",
     "paratc_spectra2d_setup", "paratc_spectra2d_reset", "paratc_spectra2d_accumulate", "paratc_spectra2d_get",
+    "paratc_visu_name", "paratc_visu_quantity", "paratc_dump_visu", "paratc_write_xdmf",
+    "paratc_io_options_from_namelist",
 ]
 PROF_NKERNELS = 16
 
@@ -68,6 +70,13 @@ def load(path=None):
     L.paratc_set_fields_device.argtypes = [ctypes.c_void_p] + [ctypes.c_void_p] * 9
     L.paratc_get_fields_device.argtypes = [ctypes.c_void_p] + [ctypes.c_void_p] * 9
     L.paratc_set_time.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double]
+    L.paratc_visu_name.argtypes = [ctypes.c_int]
+    L.paratc_visu_name.restype = ctypes.c_char_p
+    L.paratc_visu_quantity.argtypes = [ctypes.c_void_p] + [ctypes.c_int] * 5 + [_dp, ctypes.POINTER(ctypes.c_int64)]
+    L.paratc_dump_visu.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_char_p] + [ctypes.c_int] * 7
+    L.paratc_write_xdmf.argtypes = [ctypes.POINTER(ParatcParams), _dp, ctypes.c_char_p, ctypes.c_char_p] + \
+        [ctypes.c_int] * 6
+    L.paratc_io_options_from_namelist.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(ParatcIoOptions)]
     L.paratc_get_time.argtypes = [ctypes.c_void_p, _dp, _dp]
     L.paratc_step.argtypes = [ctypes.c_void_p, ctypes.POINTER(ParatcDiag)]
     L.paratc_steps.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ParatcDiag)]
@@ -162,6 +171,33 @@ def params_from_namelist(path, scalar_on=False, nyp_cap=8192):
     if rc != PARATC_OK:
         raise ParatcError(rc, "paratc_params_from_namelist(%s)" % path)
     return p, yp[: p.nyc + 1].copy()
+
+
+def io_options_from_namelist(path, scalar_on=False):
+    """&IO_Options, &SpectraOptions (+ &Spectra2DOpt, &SaveScalarOption) and
+    the output cadences of &BasicParam."""
+    o = ParatcIoOptions()
+    rc = load().paratc_io_options_from_namelist(path.encode(), int(bool(scalar_on)), ctypes.byref(o))
+    if rc != PARATC_OK:
+        raise ParatcError(rc, "paratc_io_options_from_namelist(%s)" % path)
+    return o
+
+
+def write_xdmf(params, yp, res_dir, run_name, ifirst, ilast, save_visu, save_mask, xdmf_set_type=0, single=False):
+    """InitVisu's XDMF index res_dir + "VisuFor" + run_name + ".xmf"."""
+    yp = np.ascontiguousarray(yp, dtype=np.float64)
+    p = params.copy()
+    rc = load().paratc_write_xdmf(ctypes.byref(p), _ptr(yp), res_dir.encode(), run_name.encode(), int(ifirst),
+                                  int(ilast), int(save_visu), int(save_mask), int(xdmf_set_type), int(bool(single)))
+    if rc != PARATC_OK:
+        raise ParatcError(rc, "paratc_write_xdmf")
+
+
+def visu_mask(*names):
+    m = 0
+    for n in names:
+        m |= 1 << VISU[n]
+    return m
 
 
 class ChannelSystem:
@@ -380,6 +416,26 @@ class ChannelSystem:
         out = np.zeros((nsp.value, p.nzc, nsel.value, p.nxc))
         self._check(self._L.paratc_spectra2d_get(self._h, _ptr(out), None, None, None), "paratc_spectra2d_get")
         return out, ns.value
+
+    # -- visualisation dumps (dump_visu)
+    def visu_quantity(self, name, skip=(1, 1, 1), node=False):
+        """dump_visu's quantity `name` at the kept points, [nzo, nyo, nxo]."""
+        q = VISU[name] if isinstance(name, str) else int(name)
+        n = ctypes.c_int64()
+        self._check(self._L.paratc_visu_quantity(self._h, q, skip[0], skip[1], skip[2], int(bool(node)), None,
+                                                 ctypes.byref(n)), "paratc_visu_quantity")
+        p = self.params
+        shape = tuple(-(-a // s) for a, s in zip((p.nzc, p.nyc, p.nxc), (skip[2], skip[1], skip[0])))
+        out = np.zeros(shape)
+        assert out.size == n.value
+        self._check(self._L.paratc_visu_quantity(self._h, q, skip[0], skip[1], skip[2], int(bool(node)), _ptr(out),
+                                                 None), "paratc_visu_quantity")
+        return out
+
+    def dump_visu(self, res_dir, run_name, ntime, save_mask, skip=(1, 1, 1), node=False, single=False):
+        self._check(self._L.paratc_dump_visu(self._h, res_dir.encode(), run_name.encode(), int(ntime), int(save_mask),
+                                             skip[0], skip[1], skip[2], int(bool(node)), int(bool(single))),
+                    "paratc_dump_visu")
 
     def project(self):
         dm = ctypes.c_double()

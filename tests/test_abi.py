@@ -123,3 +123,69 @@ def test_no_cpu_fallback_without_device():
     with pytest.raises(lib.ParatcError) as e:
         lib.ChannelSystem(case.params, yp_of(case))
     assert e.value.code == abi.PARATC_ERR_NO_DEVICE
+
+
+def test_io_options_reader():
+    o = lib.io_options_from_namelist(os.path.join(GOLD, "channel_small.prm"), scalar_on=True)
+    assert (o.ivstats, o.save_stat, o.save_visu) == (20, 200, 5)
+    assert (o.iskip, o.jskip, o.kskip, o.xdmf_set_type) == (2, 1, 3, 1)
+    assert o.save_mask == lib.visu_mask("ux", "uz", "wz", "pr", "Q", "scalar")
+    assert (o.write_hist_old, o.read_hist_old) == (1, 0)
+    assert (o.clc_spectra1d, o.iv_spec, o.j_for_lcs, o.clc_spectra2d, o.ny_spec2d) == (1, 40, 5, 1, 3)
+    assert list(o.iy_spec2d[:3]) == [2, 6, 12]
+    o2 = lib.io_options_from_namelist(os.path.join(GOLD, "channel_small.prm"), scalar_on=False)
+    assert not o2.save_mask & lib.visu_mask("scalar")
+
+
+@pytest.mark.parametrize("edit", [("ivSpec   = 40", "ivSpec   = 30"),     # mod(SaveStat, ivSpec) /= 0
+                                  ("SaveStat = 200", "SaveStat = 210"),    # mod(SaveStat, ivstats) /= 0
+                                  ("&IO_Options", "&IO_Optionz")])         # InitVisu reads it unconditionally
+def test_io_options_errors(tmp_path, edit):
+    txt = open(os.path.join(GOLD, "channel_small.prm")).read().replace(*edit)
+    bad = tmp_path / "bad.prm"
+    bad.write_text(txt)
+    with pytest.raises(lib.ParatcError):
+        lib.io_options_from_namelist(str(bad), scalar_on=True)
+
+
+@pytest.mark.parametrize("set_type,single", [(0, False), (1, True)])
+def test_xdmf_index(tmp_path, set_type, single):
+    """InitVisu's XDMF index (src/m_IOAndVisu.f90:56-175): a well-formed
+    XDMF file with the rectilinear grid written in Fortran's E14.7, the time
+    list and one binary attribute per saved quantity and output step."""
+    import xml.etree.ElementTree as ET
+
+    p, yp = lib.params_from_namelist(os.path.join(GOLD, "channel_small.prm"), scalar_on=True)
+    mask = lib.visu_mask("ux", "Q", "scalar")
+    lib.write_xdmf(p, yp, str(tmp_path) + "/", "Run", 1, 10, 5, mask, set_type, single)
+    path = tmp_path / "VisuForRun.xmf"
+    txt = path.read_text()
+    root = ET.fromstring(txt.split("\n", 2)[2])  # past the xml and DOCTYPE lines
+    dom = root.find("Domain")
+    nxo, nyo, nzo = (33, 25, 17) if set_type == 0 else (32, 24, 16)
+    assert dom.find("Topology").get("Dimensions") == "%5d%5d%5d" % (nzo, nyo, nxo)
+    axes = dom.find("Geometry").findall("DataItem")
+    vals = [np.array([float(v) for v in re.findall(r"-?\d\.\d{7}E[+-]\d\d", a.text)]) for a in axes]
+    assert [len(v) for v in vals] == [nxo, nyo, nzo]
+    assert all(a.get("Precision") == ("4" if single else "8") for a in axes)
+    dx = p.xlx / p.nxc
+    xs = np.arange(nxo) * dx + (0 if set_type == 0 else dx / 2)
+    ys = yp if set_type == 0 else 0.5 * (yp[:-1] + yp[1:])
+    assert np.allclose(vals[0], xs, rtol=6e-7, atol=1e-7) and np.allclose(vals[1], ys, rtol=6e-7, atol=1e-7)
+    # E14.7: 14 characters, 0.ddddddd mantissa
+    if set_type == 0:
+        assert "         0.0000000E+00 0.3926991E+00" in txt and " 0.2000000E+01 \n" in txt
+    else:
+        assert "         0.1963495E+00 0.5890486E+00" in txt
+    coll = dom.find("Grid")
+    times = coll.find("Time").find("DataItem")
+    assert times.get("Dimensions") == "%6d" % 3 and times.text.split() == ["0", "5", "10"]
+    steps = coll.findall("Grid")
+    assert [g.get("Name") for g in steps] == ["T0000000000", "T0000000005", "T0000000010"]
+    for g, t in zip(steps, (0, 5, 10)):
+        at = g.findall("Attribute")
+        assert [a.get("Name") for a in at] == ["ux", "Q", "scalar"]
+        assert all(a.get("Center") == ("Cell" if set_type == 0 else "Node") for a in at)
+        di = at[1].find("DataItem")
+        assert di.get("Dimensions") == "%5d%5d%5d" % (16, 24, 32) and di.get("Format") == "Binary"
+        assert di.text.strip() == "VisuForRun_Q_%010d" % t

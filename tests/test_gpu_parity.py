@@ -323,3 +323,52 @@ def test_spectra2d_accumulate(name):
     g.spectra2d_reset()
     got, ns = g.spectra2d_get()
     assert ns == 0 and not got.any()
+
+
+def _visu_names(p):
+    return ["ux", "uy", "uz", "pr", "wx", "wy", "wz", "wMag", "Q", "lamda2"] + (["scalar"] if p.scalar_on else [])
+
+
+@pytest.mark.parametrize("name", ["channel", "halfchannel_scalar", "channel_odd"])
+def test_visu_quantities(name):
+    """dump_visu's quantities on identical fields: the finite-difference ones
+    within 1e-13 of their largest magnitude, lambda2 (closed-form cubic with
+    CUDA's pow/acos/cos against the host's) within 1e-10; every skip pattern
+    keeps the points 1, 1+skip, ..."""
+    from paratc_b200.abi import VISU
+    case = variant(name)
+    o, g, _ = _pair(case)
+    o.step()
+    fo = o.get_fields()
+    g.set_fields(fo["ux"], fo["uy"], fo["uz"], fo["p"], fo["c"])
+    for n in _visu_names(case.params):
+        for node in ((False, True) if n in ("ux", "uy", "uz") else (False,)):
+            for skip in ((1, 1, 1), (2, 3, 2)):
+                ref = o.visu(VISU[n], skip=skip, node=node)
+                got = g.visu_quantity(n, skip=skip, node=node)
+                assert got.shape == ref.shape
+                tol = 1e-10 if n == "lamda2" else 1e-13
+                e = np.abs(got - ref).max() / max(np.abs(ref).max(), 1e-300)
+                assert e <= tol, "%s %s node=%s skip=%s rel err %.3e" % (name, n, node, skip, e)
+
+
+def test_dump_visu_files():
+    """paratc_dump_visu writes VisuFor<RunName>_<name>_<ntime> as raw
+    Fortran-order REAL(8) (or REAL(4)) arrays of the kept points."""
+    from paratc_b200.lib import visu_mask
+    case = variant("halfchannel_scalar")
+    o, g, _ = _pair(case)
+    g.iterate(1)
+    mask = visu_mask("ux", "uy", "pr", "wMag", "Q", "lamda2", "scalar")
+    with tempfile.TemporaryDirectory() as d:
+        for single in (False, True):
+            g.dump_visu(d + "/", "Case", 7, mask, skip=(2, 1, 3), single=single)
+            for n in ("ux", "uy", "pr", "wMag", "Q", "lamda2", "scalar"):
+                ref = g.visu_quantity(n, skip=(2, 1, 3))
+                path = os.path.join(d, "VisuForCase_%s_%010d" % (n, 7))
+                got = np.fromfile(path, dtype=np.float32 if single else np.float64).reshape(ref.shape)
+                if single:
+                    assert np.array_equal(got, ref.astype(np.float32)), n
+                else:
+                    assert np.array_equal(got, ref), n
+            assert not os.path.exists(os.path.join(d, "VisuForCase_wx_%010d" % 7))

@@ -373,3 +373,85 @@ def test_spectra2d_pinned_by_numpy(name):
         assert err < 1e-12, (name, m, err)
     with pytest.raises(RuntimeError):
         o.spectra2d([1])
+
+
+def numpy_visu(params, o, g, name, node=False):
+    """dump_visu's quantities (src/m_IOAndVisu.f90:182-385, Clc_Q_vor and
+    Clc_lamda2 of src/m_Tools.f90) with numpy on the halo'd fields; lambda2
+    as the middle eigenvalue of the symmetric tensor by numpy's eigvalsh
+    instead of the reference's closed-form cubic."""
+    p = params
+    H = {n: o.get_halo(n) for n in ("ux", "uy", "uz")}  # [z+4, y+2, x+4], interior at [2:-2, 1:-1, 2:-2]
+    nz, ny, nx = p.nzc, p.nyc, p.nxc
+
+    def sh(a, di=0, dj=0, dk=0):
+        return a[2 + dk:2 + dk + nz, 1 + dj:1 + dj + ny, 2 + di:2 + di + nx]
+
+    ux, uy, uz = H["ux"], H["uy"], H["uz"]
+    if name == "ux":
+        return sh(ux) + p.ucrf if node else 0.5 * (sh(ux, 1) + sh(ux)) + p.ucrf
+    if name == "uy":
+        return sh(uy) if node else 0.5 * (sh(uy, 0, 1) + sh(uy))
+    if name == "uz":
+        return sh(uz) if node else 0.5 * (sh(uz, 0, 0, 1) + sh(uz))
+    if name == "pr":
+        return g["p"]
+    if name == "scalar":
+        return g["c"]
+    rdx, rdz = p.nxc / p.xlx, p.nzc / p.zlz
+    rdyc = o.metric("rdyc")  # rdyc(1..nyp)
+    rdyp = o.metric("rdyp")  # rdyp(0..nyp)
+    c1 = rdyc[0:ny][None, :, None]
+    c2 = rdyc[1:ny + 1][None, :, None]
+    c12 = c1 - c2
+    q4 = 0.25
+    dudx = (sh(ux, 1) - sh(ux)) * rdx
+    dudy = ((sh(ux, 1, 1) + sh(ux, 0, 1)) * c2 + (sh(ux, 1) + sh(ux)) * c12 - (sh(ux, 1, -1) + sh(ux, 0, -1)) * c1) * q4
+    dudz = (sh(ux, 1, 0, 1) + sh(ux, 0, 0, 1) - sh(ux, 1, 0, -1) - sh(ux, 0, 0, -1)) * rdz * q4
+    dvdx = (sh(uy, 1, 1) - sh(uy, -1, 1) + sh(uy, 1) - sh(uy, -1)) * rdx * q4
+    dvdy = (sh(uy, 0, 1) - sh(uy)) * rdyp[1:ny + 1][None, :, None]
+    dvdz = (sh(uy, 0, 1, 1) + sh(uy, 0, 0, 1) - sh(uy, 0, 1, -1) - sh(uy, 0, 0, -1)) * rdz * q4
+    dwdx = (sh(uz, 1, 0, 1) - sh(uz, -1, 0, 1) + sh(uz, 1) - sh(uz, -1)) * rdx * q4
+    dwdy = ((sh(uz, 0, 1, 1) + sh(uz, 0, 1)) * c2 + (sh(uz, 0, 0, 1) + sh(uz)) * c12 - (sh(uz, 0, -1, 1) + sh(uz, 0, -1)) * c1) * q4
+    dwdz = (sh(uz, 0, 0, 1) - sh(uz)) * rdz
+    wx, wy, wz = dwdy - dvdz, dudz - dwdx, dvdx - dudy
+    if name == "wx":
+        return wx
+    if name == "wy":
+        return wy
+    if name == "wz":
+        return wz
+    if name == "wMag":
+        return np.sqrt(wx * wx + wy * wy + wz * wz)
+    G = np.stack([np.stack([dudx, dudy, dudz], -1), np.stack([dvdx, dvdy, dvdz], -1),
+                  np.stack([dwdx, dwdy, dwdz], -1)], -2)  # G[..., i, j] = du_i/dx_j
+    if name == "Q":
+        return 0.5 * (np.trace(G, axis1=-2, axis2=-1) ** 2 - np.einsum("...ij,...ji->...", G, G))
+    S = 0.5 * (G + np.swapaxes(G, -1, -2))
+    W = 0.5 * (G - np.swapaxes(G, -1, -2))
+    return np.linalg.eigvalsh(S @ S + W @ W)[..., 1]
+
+
+@pytest.mark.parametrize("name", ["channel", "halfchannel_scalar"])
+def test_visu_pinned_by_numpy(name):
+    """The oracle's dump_visu quantities against numpy (Q as the invariant
+    (tr(G)^2 - tr(G G))/2, lambda2 by eigvalsh), all points and a skipped
+    sampling."""
+    case = variant(name)
+    yp = yp_of(case)
+    o = ol.Oracle(case.params, yp)
+    f = fields_of(case, yp)
+    o.set_fields(f["ux"], f["uy"], f["uz"], f["p"], f["c"])
+    o.step()
+    g = o.get_fields()
+    names = ["ux", "uy", "uz", "pr", "wx", "wy", "wz", "wMag", "Q", "lamda2"] + (["scalar"] if case.params.scalar_on else [])
+    from paratc_b200.abi import VISU
+    for n in names:
+        for node in ((False, True) if n in ("ux", "uy", "uz") else (False,)):
+            ref = numpy_visu(case.params, o, g, n, node)
+            got = o.visu(VISU[n], node=node)
+            tol = 1e-10 if n == "lamda2" else 1e-13
+            err = np.abs(got - ref).max() / np.abs(ref).max()
+            assert err < tol, (name, n, node, err)
+            sk = o.visu(VISU[n], skip=(3, 2, 5), node=node)
+            assert np.array_equal(sk, got[::5, ::2, ::3]), (n, "skip")
