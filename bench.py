@@ -534,6 +534,66 @@ def run_poisson(args):
     ctx.close()
 
 
+def run_diagnostics(args):
+    """The output-side kernels on C1 (128 x 96 x 128, fields after 20 steps):
+    one clcStat accumulation, one 1-D spectra sample (x and z), one 2-D
+    spectra sample at 9 rows (+ mirrored rows), and every dump_visu quantity
+    at all points, each timed with CUDA events on the context's stream over
+    `steps` calls after `warmup` calls.  Reports microseconds per call and the
+    HBM rate of the algorithmic bytes (each field read once, the output
+    written once)."""
+    import torch
+    ws, rank, local = _dist()
+    torch.cuda.set_device(local)
+    from paratc_b200 import cases
+    from paratc_b200.abi import VISU_NAMES
+    from paratc_b200.lib import ChannelSystem, mesh_ycoord
+    case = cases.channel_c1()
+    p = case.params
+    yp = mesh_ycoord(case.mesh, p.yly)
+    f = cases.initial_fields(case, yp)
+    ctx = ChannelSystem(p, yp, device=local)
+    ctx.set_fields(f["ux"], f["uy"], f["uz"], f["p"])
+    ctx.project()
+    ctx.iterate(20)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=local)
+    cells = p.nxc * p.nyc * p.nzc
+    out = torch.empty(cells, dtype=torch.float64, device="cuda:%d" % local)
+    iy = [5, 10, 15, 20, 25, 30, 35, 40, 45]
+    ctx.spectra2d_setup(iy)
+    calls = {
+        "stats": (lambda: ctx.stats_accumulate(), 4 * 8 * cells),
+        "spectra_1d": (lambda: ctx.spectra_accumulate(20), 2 * 6 * 8 * cells),
+        "spectra_2d_9rows": (lambda: ctx.spectra2d_accumulate(), 6 * 2 * len(iy) * 8 * p.nxc * p.nzc * 3),
+    }
+    for n in VISU_NAMES:
+        if n == "scalar":
+            continue
+        nread = 1 if n in ("ux", "uy", "uz", "pr") else 3
+        calls["visu_" + n] = ((lambda n=n: ctx.visu_quantity_device_async(n, out.data_ptr())), (nread + 1) * 8 * cells)
+    res = {}
+    for name, (fn, alg) in calls.items():
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(args.steps):
+            fn()
+        b.record(stream)
+        torch.cuda.synchronize()
+        us = a.elapsed_time(b) / args.steps * 1e3
+        res[name] = {"us_per_call": round(us, 1), "alg_GBs": round(alg / (us * 1e-6) / 1e9, 1)}
+    ctx.spectra_reset()
+    ctx.stats_reset()
+    if rank == 0:
+        peak, peak_kind = _peaks()
+        print(json.dumps({"metric": "diagnostic call time", "workload": case.name, "unit": "us per call",
+                          "grid": [p.nxc, p.nyc, p.nzc], "steps": args.steps, "warmup": args.warmup,
+                          "peak_GBs": peak, "peak_kind": peak_kind, "calls": res}), flush=True)
+    ctx.close()
+
+
 def main():
     args = _args()
     if args.impl == "reference":
@@ -542,6 +602,8 @@ def main():
         run_ensemble(args)
     elif args.workload == "poisson_c2":
         run_poisson(args)
+    elif args.workload == "diagnostics_c1":
+        run_diagnostics(args)
     else:
         run_ours(args)
 

@@ -377,6 +377,11 @@ int paratc_spectra2d_get(paratc_ctx* ctx, double* out, int* nspec, int* nsel, in
  * roots, where the reference stops. */
 int paratc_visu_quantity(paratc_ctx* ctx, int q, int iskip, int jskip, int kskip, int node, double* out,
                          int64_t* count);
+/* The same into device memory d_out (nxo*nyo*nzo doubles), asynchronous on
+ * the context's stream; the count of lambda2 points with complex roots is
+ * added to the device counter *d_nbad (NULL: an internal counter). */
+int paratc_visu_quantity_device(paratc_ctx* ctx, int q, int iskip, int jskip, int kskip, int node, double* d_out,
+                                unsigned int* d_nbad);
 /* Name of quantity q as it appears in the file names ("ux", ..., "wMag",
  * "Q", "lamda2", "scalar"). */
 const char* paratc_visu_name(int q);

@@ -1085,6 +1085,24 @@ int paratc_visu_quantity(paratc_ctx* ctx, int q, int iskip, int jskip, int kskip
     return PARATC_OK;
 }
 
+int paratc_visu_quantity_device(paratc_ctx* ctx, int q, int iskip, int jskip, int kskip, int node, double* d_out,
+                                unsigned int* d_nbad) {
+    if (!ctx || !d_out || q < 0 || q >= PARATC_VISU_NQ || iskip < 1 || jskip < 1 || kskip < 1) return PARATC_ERR_BAD_ARG;
+    if (q == PARATC_VISU_SCALAR && !ctx->prm.scalar_on) return PARATC_ERR_BAD_ARG;
+    CK(cudaSetDevice(ctx->dev));
+    if (!d_nbad) {
+        if (!ctx->d_visu_bad) {
+            int rc = dalloc(ctx, &ctx->d_visu_bad, 1);
+            if (rc) return rc;
+        }
+        d_nbad = ctx->d_visu_bad;
+    }
+    launch_visu(ctx->st, q, iskip, jskip, kskip, node, ctx->kc, ctx->dm, ctx->f, d_out, d_nbad);
+    ctx->launches += 1;
+    CK(cudaGetLastError());
+    return PARATC_OK;
+}
+
 int paratc_dump_visu(paratc_ctx* ctx, const char* res_dir, const char* run_name, int ntime, int save_mask, int iskip,
                      int jskip, int kskip, int node, int single) {
     if (!ctx || !res_dir || !run_name || ntime < 0) return PARATC_ERR_BAD_ARG;

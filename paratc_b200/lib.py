@@ -34,7 +34,7 @@ EXPORTED = [
     "paratc_sync", "paratc_spectra_reset", "paratc_spectra_accumulate", "paratc_spectra_get",
     "paratc_spectra2d_setup", "paratc_spectra2d_reset", "paratc_spectra2d_accumulate", "paratc_spectra2d_get",
     "paratc_visu_name", "paratc_visu_quantity", "paratc_dump_visu", "paratc_write_xdmf",
-    "paratc_io_options_from_namelist",
+    "paratc_io_options_from_namelist", "paratc_visu_quantity_device",
 ]
 PROF_NKERNELS = 16
 
@@ -73,6 +73,7 @@ def load(path=None):
     L.paratc_visu_name.argtypes = [ctypes.c_int]
     L.paratc_visu_name.restype = ctypes.c_char_p
     L.paratc_visu_quantity.argtypes = [ctypes.c_void_p] + [ctypes.c_int] * 5 + [_dp, ctypes.POINTER(ctypes.c_int64)]
+    L.paratc_visu_quantity_device.argtypes = [ctypes.c_void_p] + [ctypes.c_int] * 5 + [ctypes.c_void_p] * 2
     L.paratc_dump_visu.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_char_p] + [ctypes.c_int] * 7
     L.paratc_write_xdmf.argtypes = [ctypes.POINTER(ParatcParams), _dp, ctypes.c_char_p, ctypes.c_char_p] + \
         [ctypes.c_int] * 6
@@ -431,6 +432,14 @@ class ChannelSystem:
         self._check(self._L.paratc_visu_quantity(self._h, q, skip[0], skip[1], skip[2], int(bool(node)), _ptr(out),
                                                  None), "paratc_visu_quantity")
         return out
+
+    def visu_quantity_device_async(self, name, d_out, skip=(1, 1, 1), node=False, d_nbad=None):
+        """Into a device pointer (int), asynchronous on the context's stream."""
+        q = VISU[name] if isinstance(name, str) else int(name)
+        self._check(self._L.paratc_visu_quantity_device(self._h, q, skip[0], skip[1], skip[2], int(bool(node)),
+                                                        ctypes.c_void_p(d_out),
+                                                        None if d_nbad is None else ctypes.c_void_p(d_nbad)),
+                    "paratc_visu_quantity_device")
 
     def dump_visu(self, res_dir, run_name, ntime, save_mask, skip=(1, 1, 1), node=False, single=False):
         self._check(self._L.paratc_dump_visu(self._h, res_dir.encode(), run_name.encode(), int(ntime), int(save_mask),
