@@ -297,6 +297,25 @@ int paratc_profile_get(paratc_ctx* ctx, int k, double* total_ms, int64_t* launch
 /* Name of kernel class k ("rhs", "helmholtz", "fft_x_fwd", ...). */
 const char* paratc_profile_name(int k);
 
+/* ---- Poisson schedule auto-tuning (the four-choice search of
+ * InitPoissonSolver, src/m_Poisson.f90:50-175, which times 15 solves of each
+ * transpose/solver variant and keeps the fastest).  The schedules here:
+ * choice = 2*s + y, s = 0 fused y-plane transforms (grids whose plane fits
+ * one CTA), 1 separate compile-time-length x and z transforms, 2 generic
+ * mixed-radix transforms (any 2^a 3^b 5^c size); y = 0 staged (one-warp CTAs,
+ * cp.async row staging), 1 streaming (a thread per column) spectral y-solve.
+ * paratc_create picks a schedule by rule; paratc_autotune times nrep solves
+ * in the step's form (divergence source, transforms, y-solve, inverse with
+ * the Neumann ghosts; the state is not touched) for every supported choice,
+ * writes the times (ms for nrep solves, -1 where unsupported) to
+ * times_ms[PARATC_SCHED_NCHOICES] (may be NULL) and keeps the fastest.  All
+ * choices solve the same system; results differ by rounding only. */
+#define PARATC_SCHED_NCHOICES 6
+int paratc_autotune(paratc_ctx* ctx, int nrep, int* choice, double* times_ms);
+int paratc_get_schedule(paratc_ctx* ctx, int* choice);
+/* pin a choice (PARATC_ERR_BAD_ARG when this grid has no such kernels) */
+int paratc_set_schedule(paratc_ctx* ctx, int choice);
+
 /* ---- Statistics (clcStat, src/m_FlowCase.f90:257-428).  FP64 accumulators
  * on the device: SumStat(k, jc) += <q_k>_xz for the 35 moments of clcStat (40
  * with the scalar) at rows jc = 1..nyc and the three top-wall moments at

@@ -55,6 +55,7 @@ struct paratc_ctx {
     double2 *d_spec = nullptr, *d_twx = nullptr, *d_postx = nullptr, *d_twz = nullptr;
     bool pfft = false;   // compile-time-length transforms exist for nx/2 and nz
     bool plane = false;  // a whole y-plane of the spectrum fits one CTA: fused 2-D transforms
+    int sched_gen = 0;   // bumped whenever the Poisson schedule changes (captured graphs hold the old one)
     double* d_pfac = nullptr;   // pivots of the spectral y systems (1/vecm, then arr), computed once
     DCoef* d_coef = nullptr;
     DDiag* d_diag = nullptr;
@@ -787,6 +788,74 @@ int paratc_poisson(paratc_ctx* ctx, const double* src, double* phi) {
     return sync(ctx);
 }
 
+// Poisson schedules: 2*s + (y-1), s 0 fused y-plane transforms, 1 separate
+// compile-time-length x / z transforms, 2 generic mixed-radix transforms; y 1
+// staged, 2 streaming spectral y-solve
+static bool sched_supported(const paratc_ctx* ctx, int choice) {
+    if (choice < 0 || choice >= PARATC_SCHED_NCHOICES) return false;
+    const int sc = choice / 2;
+    const bool pfft_ok = pfft_x_supported(ctx->nx / 2) && pfft_z_supported(ctx->nz);
+    if (sc == 0) return pfft_ok && plane_supported(ctx->nx, ctx->nz);
+    if (sc == 1) return pfft_ok;
+    return true;
+}
+
+static void sched_apply(paratc_ctx* ctx, int choice) {
+    ctx->plane = choice / 2 == 0;
+    ctx->pfft = choice / 2 <= 1;
+    ctx->kc.solver_sel = choice % 2 + 1;
+    ctx->sched_gen++;
+}
+
+int paratc_get_schedule(paratc_ctx* ctx, int* choice) {
+    if (!ctx || !choice) return PARATC_ERR_BAD_ARG;
+    const int sc = ctx->plane ? 0 : (ctx->pfft ? 1 : 2);
+    *choice = 2 * sc + (ctx->kc.solver_sel == 2 ? 1 : 0);
+    return PARATC_OK;
+}
+
+int paratc_set_schedule(paratc_ctx* ctx, int choice) {
+    if (!ctx || !sched_supported(ctx, choice)) return PARATC_ERR_BAD_ARG;
+    sched_apply(ctx, choice);
+    return PARATC_OK;
+}
+
+int paratc_autotune(paratc_ctx* ctx, int nrep, int* choice, double* times_ms) {
+    if (!ctx || nrep < 1) return PARATC_ERR_BAD_ARG;
+    CK(cudaSetDevice(ctx->dev));
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    int best = -1;
+    float best_ms = 0.f;
+    int rc = PARATC_OK;
+    for (int c = 0; c < PARATC_SCHED_NCHOICES && rc == PARATC_OK; c++) {
+        if (times_ms) times_ms[c] = -1.0;
+        if (!sched_supported(ctx, c)) continue;
+        sched_apply(ctx, c);
+        // the step's form of the solve: divergence source, transforms, y-solve,
+        // inverse into phi with its Neumann ghosts (state untouched)
+        for (int r = 0; r < nrep + 2; r++) {
+            if (r == 2) cudaEventRecord(e0, ctx->st);
+            enqueue_poisson_head(ctx, 1, nullptr, ctx->d_scal);
+            enqueue_poisson_tail(ctx, ctx->d_phi, 1);
+        }
+        cudaEventRecord(e1, ctx->st);
+        rc = sync(ctx);
+        float ms = 0.f;
+        if (rc == PARATC_OK && cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) rc = PARATC_ERR_CUDA;
+        if (rc != PARATC_OK) break;
+        if (times_ms) times_ms[c] = ms;
+        if (best < 0 || ms < best_ms) { best = c; best_ms = ms; }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc != PARATC_OK) return rc;
+    sched_apply(ctx, best);
+    if (choice) *choice = best;
+    return PARATC_OK;
+}
+
 int paratc_project(paratc_ctx* ctx, double* divmax_out) {
     if (!ctx) return PARATC_ERR_BAD_ARG;
     CK(cudaSetDevice(ctx->dev));
@@ -1150,6 +1219,7 @@ struct paratc_batch {
     cudaEvent_t fork = nullptr, done = nullptr;
     std::vector<cudaEvent_t> join;      // one per member
     cudaGraphExec_t exec = nullptr;
+    std::vector<int> gens;              // the members' sched_gen when the graph was captured
     bool graph_failed = false;
     int64_t graph_kernels = 0;
     std::string err;
@@ -1218,6 +1288,8 @@ int batch_capture(paratc_batch* b) {
     int64_t l1 = 0;
     for (auto* c : b->m) l1 += c->launches;
     b->graph_kernels = l1 - l0;
+    b->gens.clear();
+    for (auto* c : b->m) b->gens.push_back(c->sched_gen);
     return 0;
 }
 
@@ -1289,6 +1361,11 @@ int paratc_batch_steps(paratc_batch* b, int nsteps, int use_graph, paratc_diag* 
     }
     int s = 0;
     const bool graph = use_graph && !b->graph_failed;
+    if (graph && b->exec) {
+        // a member re-tuned since the capture: the graph holds its old kernels
+        for (int i = 0; i < b->n; i++)
+            if (b->m[i]->sched_gen != b->gens[i]) { batch_free_graph(b); break; }
+    }
     if (graph) {
         bool steady = true;
         for (auto* c : b->m) steady = steady && member_steady(c);

@@ -34,7 +34,8 @@ EXPORTED = [
     "paratc_sync", "paratc_spectra_reset", "paratc_spectra_accumulate", "paratc_spectra_get",
     "paratc_spectra2d_setup", "paratc_spectra2d_reset", "paratc_spectra2d_accumulate", "paratc_spectra2d_get",
     "paratc_visu_name", "paratc_visu_quantity", "paratc_dump_visu", "paratc_write_xdmf",
-    "paratc_io_options_from_namelist", "paratc_visu_quantity_device",
+    "paratc_io_options_from_namelist", "paratc_visu_quantity_device", "paratc_autotune", "paratc_get_schedule",
+    "paratc_set_schedule",
 ]
 PROF_NKERNELS = 16
 
@@ -74,6 +75,9 @@ def load(path=None):
     L.paratc_visu_name.restype = ctypes.c_char_p
     L.paratc_visu_quantity.argtypes = [ctypes.c_void_p] + [ctypes.c_int] * 5 + [_dp, ctypes.POINTER(ctypes.c_int64)]
     L.paratc_visu_quantity_device.argtypes = [ctypes.c_void_p] + [ctypes.c_int] * 5 + [ctypes.c_void_p] * 2
+    L.paratc_autotune.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int), _dp]
+    L.paratc_get_schedule.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]
+    L.paratc_set_schedule.argtypes = [ctypes.c_void_p, ctypes.c_int]
     L.paratc_dump_visu.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_char_p] + [ctypes.c_int] * 7
     L.paratc_write_xdmf.argtypes = [ctypes.POINTER(ParatcParams), _dp, ctypes.c_char_p, ctypes.c_char_p] + \
         [ctypes.c_int] * 6
@@ -432,6 +436,25 @@ class ChannelSystem:
         self._check(self._L.paratc_visu_quantity(self._h, q, skip[0], skip[1], skip[2], int(bool(node)), _ptr(out),
                                                  None), "paratc_visu_quantity")
         return out
+
+    # -- Poisson schedule (InitPoissonSolver's auto-tuning)
+    def autotune(self, nrep=15):
+        """Times every supported schedule and keeps the fastest: (choice, ms
+        for nrep solves per choice, -1 where unsupported)."""
+        ch = ctypes.c_int()
+        t = np.zeros(6)
+        self._check(self._L.paratc_autotune(self._h, int(nrep), ctypes.byref(ch), _ptr(t)), "paratc_autotune")
+        return ch.value, t
+
+    @property
+    def schedule(self):
+        ch = ctypes.c_int()
+        self._check(self._L.paratc_get_schedule(self._h, ctypes.byref(ch)), "paratc_get_schedule")
+        return ch.value
+
+    @schedule.setter
+    def schedule(self, choice):
+        self._check(self._L.paratc_set_schedule(self._h, int(choice)), "paratc_set_schedule")
 
     def visu_quantity_device_async(self, name, d_out, skip=(1, 1, 1), node=False, d_nbad=None):
         """Into a device pointer (int), asynchronous on the context's stream."""

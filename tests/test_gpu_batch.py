@@ -103,3 +103,22 @@ def test_async_transfers_equal_sync():
         for n in pin:
             assert np.array_equal(pin[n], f[n]), n
     a.last_diag()
+
+
+def test_batch_recaptures_after_schedule_change():
+    """A member whose Poisson schedule changes after the graph was captured
+    (auto-tuning, or a pinned choice) is stepped with the new kernels: the
+    graph is captured again."""
+    cs = [cases.small_channel(16, 12, 16), cases.small_channel(32, 24, 16)]
+    b, singles, _ = _setup(cs)
+    b.iterate(3, use_graph=True)
+    for s in singles:
+        s.iterate(3)
+    _same(b, singles)
+    for g in (b.members[1], singles[1]):
+        g.schedule = 5  # generic transforms, streaming y-solve
+    b.iterate(3, use_graph=True)
+    for s in singles:
+        s.iterate(3)
+    _same(b, singles)
+    b.close()

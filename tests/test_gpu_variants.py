@@ -96,3 +96,38 @@ def test_plane_and_split_transforms(monkeypatch, plane, dims):
     assert rel_err(phi_g, phi_o) <= TOL_POISSON
     if dims[1] <= 24:
         _steps_vs_oracle(case, 2)
+
+
+@pytest.mark.parametrize("dims", [(64, 48, 64), (24, 20, 30), (128, 96, 128)])
+def test_schedules_and_autotune(dims):
+    """Every Poisson schedule this grid supports (fused plane transforms,
+    separate fixed-length transforms, generic transforms; staged or
+    streaming y-solve) gives the oracle's fields after two steps; the
+    auto-tuner times all of them and keeps the fastest."""
+    case = cases.small_channel(*dims)
+    yp = yp_of(case)
+    f = fields_of(case, yp)
+    o = ol.Oracle(case.params, yp)
+    o.set_fields(f["ux"], f["uy"], f["uz"], f["p"])
+    for _ in range(2):
+        o.step()
+    fo = o.get_fields()
+    g = ChannelSystem(case.params, yp)
+    choice, times = g.autotune(nrep=3)
+    assert times[choice] > 0 and times[choice] == min(t for t in times if t > 0)
+    assert g.schedule == choice
+    supported = [c for c in range(6) if times[c] > 0]
+    assert 4 in supported and 5 in supported  # the generic transforms take any 2^a 3^b 5^c size
+    for c in range(6):
+        if c not in supported:
+            with pytest.raises(Exception):
+                g.schedule = c
+            continue
+        g.schedule = c
+        g.set_fields(f["ux"], f["uy"], f["uz"], f["p"])
+        g.iterate(2)
+        fg = g.get_fields()
+        for n in ("ux", "uy", "uz", "p"):
+            e = rel_err(fg[n], fo[n])
+            assert e <= 1e-8, "schedule %d %s rel err %.3e" % (c, n, e)
+    g.close()
