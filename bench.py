@@ -46,6 +46,8 @@ def _args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64",
+                    help="mixed: the explicit right-hand side in FP32 arithmetic, all else FP64")
     return ap.parse_args()
 
 
@@ -228,6 +230,7 @@ def run_ours(args):
         base = cpu_baseline(case, yp, fields, args.cpu_seconds)
 
     ctx = ChannelSystem(p, yp, device=local)
+    ctx.precision = args.precision
     ctx.set_fields(fields["ux"], fields["uy"], fields["uz"], fields["p"], fields["c"])
     ctx.project()
     stream = torch.cuda.ExternalStream(ctx.stream, device=local)
@@ -310,6 +313,22 @@ def run_ours(args):
                "note": "per step: paratc_set_fields (%s from pinned host) + paratc_step + paratc_get_fields (same to host)"
                        % ",".join(names)}
 
+    # the mixed form against the FP64 path: the same initial fields advanced by
+    # the same number of steps (warm-up, timed, profiled, end to end)
+    mixed_err = None
+    if args.precision == "mixed":
+        nsteps = args.warmup + 2 * args.steps + (0 if args.no_e2e else args.steps)
+        ref = ChannelSystem(p, yp, device=local)
+        ref.set_fields(fields["ux"], fields["uy"], fields["uz"], fields["p"], fields["c"])
+        ref.project()
+        ref.iterate(nsteps)
+        fr, fm = ref.get_fields(), ctx.get_fields()
+        mixed_err = {"steps": nsteps}
+        for n in ("ux", "uy", "uz", "p", "c"):
+            if fr.get(n) is not None:
+                mixed_err[n] = float(np.abs(fm[n] - fr[n]).max() / np.abs(fr[n]).max())
+        ref.close()
+
     # roofline of the dominant kernel
     peak, peak_kind = _peaks()
     alg = algorithmic_bytes(p)
@@ -330,11 +349,13 @@ def run_ours(args):
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "scaling": "weak", "vs_baseline": None,
+                "dtype": "f64" if args.precision == "fp64" else "f32 rhs + f64", "data": "synthetic",
                 "config": {"workload": case.name, "grid": [p.nxc, p.nyc, p.nzc], "scheme": "RK3",
-                           "precision": "fp64", "parallelism": "replicas x%d" % ws,
+                           "precision": args.precision, "parallelism": "replicas x%d" % ws,
                            "l2": "flushed between timed steps (256 MB write outside the events)",
-                           "divmax_last_step": diag.divmax},
+                           "divmax_last_step": diag.divmax,
+                           "field_rel_err_vs_fp64_path": mixed_err},
                 "roofline": roof, "cpu_baseline": base, "e2e": e2e, "gpu_launches": launches, "clocks": clocks}
         print(json.dumps(line), flush=True)
     ctx.close()

@@ -297,6 +297,22 @@ int paratc_profile_get(paratc_ctx* ctx, int k, double* total_ms, int64_t* launch
 /* Name of kernel class k ("rhs", "helmholtz", "fft_x_fwd", ...). */
 const char* paratc_profile_name(int k);
 
+/* ---- precision of the step.  PARATC_PREC_FP64 (the default) is the
+ * reference's arithmetic.  PARATC_PREC_MIXED computes the explicit
+ * right-hand side (clcRhsXYZ's stencils, interpolations and products) in
+ * FP32 arithmetic from the FP64 state and writes it in FP64; the state, the
+ * explicit histories, the Helmholtz and Poisson solves, the projection, the
+ * flow-rate constraint sum (s3tot) and every reduction stay FP64, so the
+ * divergence after a step is at the FP64 level while the fields differ from
+ * the FP64 path by the FP32 rounding of one explicit term per substep.  (An
+ * FP32 solve with FP64 iterative refinement is not offered: on this direct
+ * FFT-Thomas solver each refinement sweep moves more bytes than the single
+ * FP64 solve it replaces.) */
+#define PARATC_PREC_FP64  0
+#define PARATC_PREC_MIXED 1
+int paratc_set_precision(paratc_ctx* ctx, int prec);
+int paratc_get_precision(paratc_ctx* ctx, int* prec);
+
 /* ---- Poisson schedule auto-tuning (the four-choice search of
  * InitPoissonSolver, src/m_Poisson.f90:50-175, which times 15 solves of each
  * transpose/solver variant and keeps the fastest).  The schedules here:

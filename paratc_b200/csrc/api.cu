@@ -482,6 +482,10 @@ int paratc_create(const paratc_params* prm, const double* yp, int device, paratc
     kc.ubulk = prm->ubulk; kc.yly = prm->yly; kc.normfft = h.normfft; kc.dt_max = prm->dt_max; kc.cflc = prm->cflc;
     kc.sc_r1b = h.sc_r1b; kc.sc_r2b = h.sc_r2b; kc.sc_r1t = h.sc_r1t; kc.sc_r2t = h.sc_r2t;
     kc.vel_limit = prm->vel_limit; kc.div_limit = prm->div_limit;
+    for (int q = 0; q < 4; q++) { kc.fdxC[q] = (float)kc.dxC[q]; kc.fdzC[q] = (float)kc.dzC[q]; kc.fIC[q] = (float)kc.IC[q]; }
+    for (int q = 0; q < 5; q++) { kc.fdxxC[q] = (float)kc.dxxC[q]; kc.fdzzC[q] = (float)kc.dzzC[q]; }
+    for (int q = 0; q < 3; q++) { kc.fgrav[q] = (float)kc.grav[q]; kc.fgev[q] = (float)kc.gev[q]; kc.ffvv[q] = (float)kc.fvv[q]; }
+    kc.fucrf = (float)kc.ucrf; kc.fxnu = (float)kc.xnu; kc.fsdiff = (float)kc.sdiff;
 
     // ---- device memory
     const size_t nf = ctx->nf;
@@ -817,6 +821,19 @@ int paratc_get_schedule(paratc_ctx* ctx, int* choice) {
 int paratc_set_schedule(paratc_ctx* ctx, int choice) {
     if (!ctx || !sched_supported(ctx, choice)) return PARATC_ERR_BAD_ARG;
     sched_apply(ctx, choice);
+    return PARATC_OK;
+}
+
+int paratc_set_precision(paratc_ctx* ctx, int prec) {
+    if (!ctx || (prec != PARATC_PREC_FP64 && prec != PARATC_PREC_MIXED)) return PARATC_ERR_BAD_ARG;
+    ctx->kc.fp32_rhs = prec == PARATC_PREC_MIXED ? 1 : 0;
+    ctx->sched_gen++;  // captured graphs hold the other kernels
+    return PARATC_OK;
+}
+
+int paratc_get_precision(paratc_ctx* ctx, int* prec) {
+    if (!ctx || !prec) return PARATC_ERR_BAD_ARG;
+    *prec = ctx->kc.fp32_rhs ? PARATC_PREC_MIXED : PARATC_PREC_FP64;
     return PARATC_OK;
 }
 

@@ -36,6 +36,7 @@ struct DConst {
     int flow_type, scalar_on, is_ux_const, icfl;
     int nsm;  // streaming multiprocessors of the device
     int solver_sel;  // 0 automatic; 1 forces the staged, 2 the streaming y-solve kernels (tests)
+    int fp32_rhs;    // 1: the explicit right-hand side computed in FP32 arithmetic (FP64 state)
     double dxC[4], dzC[4], dxxC[5], dzzC[5], IC[4];
     double rdx, rdz;
     double ucrf, xnu, grav[3], sdiff, gev[3], fvv[3];
@@ -43,6 +44,9 @@ struct DConst {
     double ubulk, yly, normfft, dt_max, cflc;
     double sc_r1b, sc_r2b, sc_r1t, sc_r2t;   // scalar ghost: c0 = r1b*c1 + r2b, ...
     double vel_limit, div_limit;
+    // FP32 copies of the stencil constants for the FP32 right-hand side
+    float fdxC[4], fdzC[4], fdxxC[5], fdzzC[5], fIC[4], fgrav[3], fgev[3], ffvv[3];
+    float fucrf, fxnu, fsdiff;
 };
 
 // per-substep coefficients (PMcoeUpdate, src/m_Parameters.f90:215-230) and

@@ -12,6 +12,16 @@
 // explicit histories, reading every neighbour from shared memory; the six
 // interpolated fields of the reference and their halo updates never exist.
 //
+// Two precisions of the same kernel: FP64 (the reference's arithmetic) and a
+// mixed form whose stencil arithmetic and row slabs are FP32 while the state,
+// the outputs and the flow-rate sum stay FP64.  In the FP32 form the slabs
+// take half the shared memory and the registers, so a CTA runs 256 threads
+// with one cell each; its row slabs are loaded into registers one row ahead
+// and converted when stored, and s3tot sums the wall-normal viscous term
+// d22 from FP64 loads of the thread's own column (the x and z second
+// differences sum to zero over a periodic line, so they carry nothing into
+// s3tot but rounding).
+//
 // The same kernel performs PMcoeUpdate (src/m_Parameters.f90:215-230),
 // Update_uy_ym (src/m_FlowCase.f90:112-122) and the flow-rate constraint
 // (src/m_TScheme.f90:269-300): every CTA writes its partial of s3tot and the
@@ -28,10 +38,20 @@ constexpr int TX = 32, TZ = 8, HX = 3, HZ = 3;
 constexpr int SX = TX + 2 * HX;  // 38
 constexpr int SZ = TZ + 2 * HZ;  // 14
 constexpr int SLAB = SX * SZ;    // 532 doubles per field and row
-constexpr int NB = 4;            // ring slots
-constexpr int ZC = 2;            // z-adjacent cells per thread: their shared stencil taps are loaded once
-constexpr int NTHR = TX * TZ / ZC;  // 128
-constexpr int NSLOT = (SLAB + NTHR - 1) / NTHR;
+constexpr int PF = 2;            // FP64: rows loaded ahead beyond row j+1 (cp.async groups in flight)
+// per precision: z-adjacent cells per thread (FP64: 2, whose shared stencil
+// taps then load once; FP32: 1) and threads per CTA
+template <class T>
+struct RhsCfg {
+    static constexpr int NB = sizeof(T) == 8 ? 3 + PF : 4;  // ring slots: rows j-1..j+1 and the rows in flight
+    static constexpr int ZC = sizeof(T) == 8 ? 2 : 1;
+    static constexpr int NTHR = TX * TZ / ZC;  // 128 or 256
+    static constexpr int NSLOT = (SLAB + NTHR - 1) / NTHR;
+};
+template <bool SCALAR, class T>
+constexpr size_t rhs_smem_bytes() {
+    return (size_t)RhsCfg<T>::NB * (SCALAR ? 5 : 4) * SLAB * sizeof(T);
+}
 
 __device__ __forceinline__ void cp_async8(double* sdst, const double* gsrc) {
     const unsigned s = (unsigned)__cvta_generic_to_shared(sdst);
@@ -48,13 +68,16 @@ __device__ __forceinline__ int modp(int i, int n) {
 
 }  // namespace
 
-template <bool SCALAR>
-__global__ void __launch_bounds__(NTHR, 2)
+template <bool SCALAR, class T>
+__global__ void __launch_bounds__(RhsCfg<T>::NTHR, 2)
     k_rhs_tile(DConst c, DMetric m, DCoef* __restrict__ coef, Fields fl, double* __restrict__ uy_ym,
                double* __restrict__ duy_ym, int ns, double gam, double the, double alp, int ychunk,
                double* __restrict__ part, unsigned int* __restrict__ counter) {
     constexpr int NF = SCALAR ? 5 : 4;
-    extern __shared__ double sm[];  // [NB][NF][SLAB]
+    constexpr bool F64 = sizeof(T) == 8;
+    constexpr int ZC = RhsCfg<T>::ZC, NTHR = RhsCfg<T>::NTHR, NSLOT = RhsCfg<T>::NSLOT, NB = RhsCfg<T>::NB;
+    extern __shared__ __align__(16) unsigned char sm_raw[];
+    T* sm = reinterpret_cast<T*>(sm_raw);  // [NB][NF][SLAB]
     const int lane = threadIdx.x, wq = threadIdx.y, tid = wq * 32 + lane;
     const int nx = c.nx, nz = c.nz, ny = c.ny;
     const size_t pl = (size_t)c.nyt * nx;
@@ -73,8 +96,21 @@ __global__ void __launch_bounds__(NTHR, 2)
     const double pmGamma = gam * dt, pmTheta = the * dt, pmAlpha = alp * dt;
     const double pmBeta = 0.5 * alp * c.xnu * dt, pmBetaSc = 0.5 * alp * c.sdiff * dt;
     const double tb = 2.0 * pmBeta, tbs = 2.0 * pmBetaSc;
-    const double I1 = c.IC[0], I2 = c.IC[1], I3 = c.IC[2], I4 = c.IC[3];
-    const double ucrf = c.ucrf, xnu = c.xnu;
+    // stencil constants straight from the parameter bank, in the kernel's precision
+    const double* const dc64[8] = {c.dxC, c.dzC, c.dxxC, c.dzzC, c.IC, c.grav, c.gev, c.fvv};
+    const float* const dc32[8] = {c.fdxC, c.fdzC, c.fdxxC, c.fdzzC, c.fIC, c.fgrav, c.fgev, c.ffvv};
+#define KC(a, q) (F64 ? (T)dc64[a][q] : (T)dc32[a][q])
+#define dxC(q) KC(0, q)
+#define dzC(q) KC(1, q)
+#define dxxC(q) KC(2, q)
+#define dzzC(q) KC(3, q)
+#define grav(q) KC(5, q)
+#define gev(q) KC(6, q)
+#define fvv(q) KC(7, q)
+    const T I1 = KC(4, 0), I2 = KC(4, 1), I3 = KC(4, 2), I4 = KC(4, 3);
+    const T ucrf = F64 ? (T)c.ucrf : (T)c.fucrf, xnu = F64 ? (T)c.xnu : (T)c.fxnu;
+    const T tpG = (T)pmGamma, tpT = (T)pmTheta, tpA = (T)pmAlpha, ttb = (T)tb, ttbs = (T)tbs;
+    const T tsdiff = F64 ? (T)c.sdiff : (T)c.fsdiff;
     const double* fsrc[5] = {fl.ux, fl.uy, fl.uz, fl.pr, fl.sc};
     double s3 = 0.0;
 
@@ -95,25 +131,42 @@ __global__ void __launch_bounds__(NTHR, 2)
             goff[s] = (size_t)modp(k0 - HZ + zz, nz) * pl + (size_t)modp(i0 - HX + xx, nx);
             soff[s] = e;
         }
+        // FP64: cp.async straight into the ring; FP32: load, convert, store
 #define LOAD_ROW(jrow)                                                                   \
     do {                                                                                 \
-        double* dst_ = sm + (size_t)((jrow) % NB) * NF * SLAB;                           \
+        T* dst_ = sm + (size_t)((jrow) % NB) * NF * SLAB;                                \
         const size_t ro_ = (size_t)(jrow) * nx;                                          \
         _Pragma("unroll") for (int f_ = 0; f_ < NF; f_++)                                \
-            _Pragma("unroll") for (int s_ = 0; s_ < NSLOT; s_++) if (sval[s_])           \
-                cp_async8(dst_ + f_ * SLAB + soff[s_], fsrc[f_] + goff[s_] + ro_);       \
+            _Pragma("unroll") for (int s_ = 0; s_ < NSLOT; s_++) if (sval[s_]) {         \
+                if constexpr (F64)                                                       \
+                    cp_async8(reinterpret_cast<double*>(dst_) + f_ * SLAB + soff[s_],    \
+                              fsrc[f_] + goff[s_] + ro_);                                \
+                else                                                                     \
+                    dst_[f_ * SLAB + soff[s_]] = (T)__ldg(fsrc[f_] + goff[s_] + ro_);    \
+            }                                                                            \
     } while (0)
 
         LOAD_ROW(j0 - 1);
         LOAD_ROW(j0);
         LOAD_ROW(j0 + 1);
-        cp_async_commit();
+        if constexpr (F64) {
+            cp_async_commit();
+            // rows j0+2 .. j0+PF, one commit group each
+#pragma unroll
+            for (int d = 2; d <= PF; d++) {
+                if (j0 + d <= j1 + 1) LOAD_ROW(j0 + d);
+                cp_async_commit();
+            }
+        } else {
+            __syncthreads();
+        }
 
         const int i = i0 + lane;
         int kk[ZC];
         bool act[ZC];
         // explicit histories of the next row are loaded one row ahead
         double hxn[ZC], hyn[ZC], hzn[ZC], hcn[ZC];
+        double u64m[ZC], u64c[ZC], u64p[ZC];  // FP32 form: FP64 ux of the own column, rows j-1, j, j+1
 #pragma unroll
         for (int cz = 0; cz < ZC; cz++) {
             kk[cz] = k0 + wq * ZC + cz;
@@ -125,16 +178,34 @@ __global__ void __launch_bounds__(NTHR, 2)
                 duy_ym[t] = uy_ym[t] - d;
             }
             hxn[cz] = hyn[cz] = hzn[cz] = hcn[cz] = 0.0;
+            u64m[cz] = u64c[cz] = u64p[cz] = 0.0;
             if (act[cz]) {
                 const size_t q = (size_t)kk[cz] * pl + (size_t)j0 * nx + i;
                 hxn[cz] = fl.hx[q]; hyn[cz] = fl.hy[q]; hzn[cz] = fl.hz[q];
                 if (SCALAR) hcn[cz] = fl.hc[q];
+                if constexpr (!F64) {
+                    u64m[cz] = __ldg(&fl.ux[q - nx]);
+                    u64c[cz] = __ldg(&fl.ux[q]);
+                    u64p[cz] = __ldg(&fl.ux[q + nx]);
+                }
             }
         }
 
         for (int j = j0; j <= j1; j++) {
-            if (j + 2 <= j1 + 1) LOAD_ROW(j + 2);
-            cp_async_commit();
+            // FP32 form: row j+2 in registers now, converted and stored after
+            // the arithmetic of row j
+            double pre[NF][NSLOT];
+            const bool more = j + 2 <= j1 + 1;
+            if constexpr (F64) {
+                if (j + 1 + PF <= j1 + 1) LOAD_ROW(j + 1 + PF);
+                cp_async_commit();
+            } else if (more) {
+                const size_t ro = (size_t)(j + 2) * nx;
+#pragma unroll
+                for (int f = 0; f < NF; f++)
+#pragma unroll
+                    for (int sl = 0; sl < NSLOT; sl++) pre[f][sl] = sval[sl] ? __ldg(fsrc[f] + goff[sl] + ro) : 0.0;
+            }
             double hx0a[ZC], hy0a[ZC], hz0a[ZC], hc0a[ZC];
             size_t q0a[ZC];
 #pragma unroll
@@ -146,140 +217,154 @@ __global__ void __launch_bounds__(NTHR, 2)
                     if (SCALAR) hcn[cz] = fl.hc[q0a[cz] + nx];
                 }
             }
-            cp_async_wait<1>();
-            __syncthreads();
+            // FP32 form: ux of row j+2 for the next row's s3tot term, one row ahead
+            double u64n[ZC];
+#pragma unroll
+            for (int cz = 0; cz < ZC; cz++)
+                u64n[cz] = (!F64 && act[cz] && j + 2 <= ny + 1) ? __ldg(&fl.ux[q0a[cz] + 2 * nx]) : 0.0;
+            if constexpr (F64) {
+                cp_async_wait<PF>();  // the group holding row j+1 is complete
+                __syncthreads();
+            }
             // both cells are computed before any global store, so that the
             // compiler may load a tap the two cells share once
-            double o_rx[ZC], o_ry[ZC], o_rz[ZC], o_hx[ZC], o_hy[ZC], o_hz[ZC], o_rc[ZC], o_hc[ZC];
+            T o_rx[ZC], o_ry[ZC], o_rz[ZC], o_hx[ZC], o_hy[ZC], o_hz[ZC], o_rc[ZC], o_hc[ZC];
             {
-                const double* Sm = sm + (size_t)((j - 1) % NB) * NF * SLAB;
-                const double* Sc = sm + (size_t)(j % NB) * NF * SLAB;
-                const double* Sp = sm + (size_t)((j + 1) % NB) * NF * SLAB;
+                const T* Sm = sm + (size_t)((j - 1) % NB) * NF * SLAB;
+                const T* Sc = sm + (size_t)(j % NB) * NF * SLAB;
+                const T* Sp = sm + (size_t)((j + 1) % NB) * NF * SLAB;
 #define V(S, f, dx, dz) (S)[(f) * SLAB + (w + HZ + (dz)) * SX + (lane + HX + (dx))]
             const bool top = (j == ny);
-            const double IY1 = __ldg(&m.yinterp[j]), IY2 = 1.0 - IY1;
-            const double IY3 = __ldg(&m.yinterp[j + 1]), IY4 = 1.0 - IY3;
-            const double rdyp = __ldg(&m.rdyp[j]), rdyc = __ldg(&m.rdyc[j]), dyp = __ldg(&m.dyp[j]);
+            const double IY1d = __ldg(&m.yinterp[j]), IY3d = __ldg(&m.yinterp[j + 1]);
+            const T IY1 = (T)IY1d, IY2 = (T)(1.0 - IY1d), IY3 = (T)IY3d, IY4 = (T)(1.0 - IY3d);
+            const T rdyp = (T)__ldg(&m.rdyp[j]), rdyc = (T)__ldg(&m.rdyc[j]);
+            const double dyp = __ldg(&m.dyp[j]);
+            const T ap2c = (T)__ldg(&m.ap2c[j]), ac2c = (T)__ldg(&m.ac2c[j]), am2c = (T)__ldg(&m.am2c[j]);
 #pragma unroll
             for (int cz = 0; cz < ZC; cz++) {
             const int w = wq * ZC + cz;
-            const double hx0 = hx0a[cz], hy0 = hy0a[cz], hz0 = hz0a[cz], hc0 = hc0a[cz];
+            const T hx0 = (T)hx0a[cz], hy0 = (T)hy0a[cz], hz0 = (T)hz0a[cz], hc0 = (T)hc0a[cz];
             (void)hc0;
 
             // ---------------- RhsX (:169-204)
-            double conv_x, rhs_x;
+            T conv_x, rhs_x;
             {
-                const double uxc = V(Sc, 0, 0, 0), uxjm = V(Sm, 0, 0, 0), uxjp = V(Sp, 0, 0, 0);
-                const double uxhyc = IY1 * uxjm + IY2 * uxc;
-                const double uxhyp = IY3 * uxc + IY4 * uxjp;
-                double h11 = 0.0;
+                const T uxc = V(Sc, 0, 0, 0), uxjm = V(Sm, 0, 0, 0), uxjp = V(Sp, 0, 0, 0);
+                const T uxhyc = IY1 * uxjm + IY2 * uxc;
+                const T uxhyp = IY3 * uxc + IY4 * uxjp;
+                T h11 = 0;
 #pragma unroll
                 for (int q = 0; q < 4; q++) {  // uxhx at x offsets -2..1
                     const int d = q - 2;
-                    const double uh = I1 * V(Sc, 0, d - 1, 0) + I2 * V(Sc, 0, d, 0) + I3 * V(Sc, 0, d + 1, 0) + I4 * V(Sc, 0, d + 2, 0);
-                    h11 = (q == 0) ? c.dxC[0] * uh * (uh + ucrf) : h11 + c.dxC[q] * uh * (uh + ucrf);
+                    const T uh = I1 * V(Sc, 0, d - 1, 0) + I2 * V(Sc, 0, d, 0) + I3 * V(Sc, 0, d + 1, 0) + I4 * V(Sc, 0, d + 2, 0);
+                    h11 = (q == 0) ? dxC(0) * uh * (uh + ucrf) : h11 + dxC(q) * uh * (uh + ucrf);
                 }
-                const double uyhx_j = I1 * V(Sc, 1, -2, 0) + I2 * V(Sc, 1, -1, 0) + I3 * V(Sc, 1, 0, 0) + I4 * V(Sc, 1, 1, 0);
-                const double uyhx_p = top ? 0.0 : I1 * V(Sp, 1, -2, 0) + I2 * V(Sp, 1, -1, 0) + I3 * V(Sp, 1, 0, 0) + I4 * V(Sp, 1, 1, 0);
-                const double h12 = (uyhx_p * uxhyp - uyhx_j * uxhyc) * rdyp;
-                double h13 = 0.0;
+                const T uyhx_j = I1 * V(Sc, 1, -2, 0) + I2 * V(Sc, 1, -1, 0) + I3 * V(Sc, 1, 0, 0) + I4 * V(Sc, 1, 1, 0);
+                const T uyhx_p = top ? T(0) : I1 * V(Sp, 1, -2, 0) + I2 * V(Sp, 1, -1, 0) + I3 * V(Sp, 1, 0, 0) + I4 * V(Sp, 1, 1, 0);
+                const T h12 = (uyhx_p * uxhyp - uyhx_j * uxhyc) * rdyp;
+                T h13 = 0;
 #pragma unroll
                 for (int q = 0; q < 4; q++) {  // z offsets -1..2
                     const int d = q - 1;
-                    const double uxhz = I1 * V(Sc, 0, 0, d - 2) + I2 * V(Sc, 0, 0, d - 1) + I3 * V(Sc, 0, 0, d) + I4 * V(Sc, 0, 0, d + 1);
-                    const double uzhx = I1 * V(Sc, 2, -2, d) + I2 * V(Sc, 2, -1, d) + I3 * V(Sc, 2, 0, d) + I4 * V(Sc, 2, 1, d);
-                    h13 = (q == 0) ? c.dzC[0] * uxhz * uzhx : h13 + c.dzC[q] * uxhz * uzhx;
+                    const T uxhz = I1 * V(Sc, 0, 0, d - 2) + I2 * V(Sc, 0, 0, d - 1) + I3 * V(Sc, 0, 0, d) + I4 * V(Sc, 0, 0, d + 1);
+                    const T uzhx = I1 * V(Sc, 2, -2, d) + I2 * V(Sc, 2, -1, d) + I3 * V(Sc, 2, 0, d) + I4 * V(Sc, 2, 1, d);
+                    h13 = (q == 0) ? dzC(0) * uxhz * uzhx : h13 + dzC(q) * uxhz * uzhx;
                 }
-                const double d11 = c.dxxC[0] * V(Sc, 0, -2, 0) + c.dxxC[1] * V(Sc, 0, -1, 0) + c.dxxC[2] * uxc + c.dxxC[3] * V(Sc, 0, 1, 0) + c.dxxC[4] * V(Sc, 0, 2, 0);
-                const double d22 = __ldg(&m.ap2c[j]) * uxjp + __ldg(&m.ac2c[j]) * uxc + __ldg(&m.am2c[j]) * uxjm;
-                const double d33 = c.dzzC[0] * V(Sc, 0, 0, -2) + c.dzzC[1] * V(Sc, 0, 0, -1) + c.dzzC[2] * uxc + c.dzzC[3] * V(Sc, 0, 0, 1) + c.dzzC[4] * V(Sc, 0, 0, 2);
-                const double dcq13 = d11 + d33;
-                if (act[cz]) s3 += SCALAR ? uxc * dyp : (dcq13 + d22) * dyp;
-                conv_x = -h11 - h12 - h13 + xnu * dcq13 + c.grav[0];
-                const double gradp = c.dxC[0] * V(Sc, 3, -2, 0) + c.dxC[1] * V(Sc, 3, -1, 0) + c.dxC[2] * V(Sc, 3, 0, 0) + c.dxC[3] * V(Sc, 3, 1, 0);
-                rhs_x = pmGamma * conv_x + pmTheta * hx0 - pmAlpha * gradp + tb * d22;
+                const T d11 = dxxC(0) * V(Sc, 0, -2, 0) + dxxC(1) * V(Sc, 0, -1, 0) + dxxC(2) * uxc + dxxC(3) * V(Sc, 0, 1, 0) + dxxC(4) * V(Sc, 0, 2, 0);
+                const T d22 = ap2c * uxjp + ac2c * uxc + am2c * uxjm;
+                const T d33 = dzzC(0) * V(Sc, 0, 0, -2) + dzzC(1) * V(Sc, 0, 0, -1) + dzzC(2) * uxc + dzzC(3) * V(Sc, 0, 0, 1) + dzzC(4) * V(Sc, 0, 0, 2);
+                const T dcq13 = d11 + d33;
+                if constexpr (F64) {
+                    if (act[cz]) s3 += SCALAR ? uxc * dyp : (dcq13 + d22) * dyp;
+                } else if (act[cz]) {
+                    s3 += SCALAR ? u64c[cz] * dyp
+                                 : (__ldg(&m.ap2c[j]) * u64p[cz] + __ldg(&m.ac2c[j]) * u64c[cz] + __ldg(&m.am2c[j]) * u64m[cz]) * dyp;
+                }
+                conv_x = -h11 - h12 - h13 + xnu * dcq13 + grav(0);
+                const T gradp = dxC(0) * V(Sc, 3, -2, 0) + dxC(1) * V(Sc, 3, -1, 0) + dxC(2) * V(Sc, 3, 0, 0) + dxC(3) * V(Sc, 3, 1, 0);
+                rhs_x = tpG * conv_x + tpT * hx0 - tpA * gradp + ttb * d22;
             }
             // ---------------- RhsY (:206-236)
-            double conv_y, rhs_y;
+            T conv_y, rhs_y;
             {
-                const double qsucac = 0.25 * rdyc;
-                double h21 = 0.0, h23 = 0.0;
+                const T qsucac = T(0.25) * rdyc;
+                T h21 = 0.0, h23 = 0.0;
 #pragma unroll
                 for (int q = 0; q < 4; q++) {  // offsets -1..2
                     const int d = q - 1;
-                    const double uxh = IY1 * V(Sm, 0, d, 0) + IY2 * V(Sc, 0, d, 0) + ucrf;
-                    const double uzh = IY1 * V(Sm, 2, 0, d) + IY2 * V(Sc, 2, 0, d);
-                    const double uyhx = I1 * V(Sc, 1, d - 2, 0) + I2 * V(Sc, 1, d - 1, 0) + I3 * V(Sc, 1, d, 0) + I4 * V(Sc, 1, d + 1, 0);
-                    const double uyhz = I1 * V(Sc, 1, 0, d - 2) + I2 * V(Sc, 1, 0, d - 1) + I3 * V(Sc, 1, 0, d) + I4 * V(Sc, 1, 0, d + 1);
-                    h21 = (q == 0) ? c.dxC[0] * uyhx * uxh : h21 + c.dxC[q] * uyhx * uxh;
-                    h23 = (q == 0) ? c.dzC[0] * uyhz * uzh : h23 + c.dzC[q] * uyhz * uzh;
+                    const T uxh = IY1 * V(Sm, 0, d, 0) + IY2 * V(Sc, 0, d, 0) + ucrf;
+                    const T uzh = IY1 * V(Sm, 2, 0, d) + IY2 * V(Sc, 2, 0, d);
+                    const T uyhx = I1 * V(Sc, 1, d - 2, 0) + I2 * V(Sc, 1, d - 1, 0) + I3 * V(Sc, 1, d, 0) + I4 * V(Sc, 1, d + 1, 0);
+                    const T uyhz = I1 * V(Sc, 1, 0, d - 2) + I2 * V(Sc, 1, 0, d - 1) + I3 * V(Sc, 1, 0, d) + I4 * V(Sc, 1, 0, d + 1);
+                    h21 = (q == 0) ? dxC(0) * uyhx * uxh : h21 + dxC(q) * uyhx * uxh;
+                    h23 = (q == 0) ? dzC(0) * uyhz * uzh : h23 + dzC(q) * uyhz * uzh;
                 }
-                const double vp = V(Sp, 1, 0, 0), vc = V(Sc, 1, 0, 0), vm = V(Sm, 1, 0, 0);
-                const double h22 = ((vp + vc) * (vp + vc) - (vc + vm) * (vc + vm)) * qsucac;
-                const double d11 = c.dxxC[0] * V(Sc, 1, -2, 0) + c.dxxC[1] * V(Sc, 1, -1, 0) + c.dxxC[2] * vc + c.dxxC[3] * V(Sc, 1, 1, 0) + c.dxxC[4] * V(Sc, 1, 2, 0);
-                const double d22 = __ldg(&m.ap2p[j]) * vp + __ldg(&m.ac2p[j]) * vc + __ldg(&m.am2p[j]) * vm;
-                const double d33 = c.dzzC[0] * V(Sc, 1, 0, -2) + c.dzzC[1] * V(Sc, 1, 0, -1) + c.dzzC[2] * vc + c.dzzC[3] * V(Sc, 1, 0, 1) + c.dzzC[4] * V(Sc, 1, 0, 2);
-                conv_y = -h21 - h22 - h23 + xnu * (d11 + d33) + c.grav[1];
-                const double gradp = (V(Sc, 3, 0, 0) - V(Sm, 3, 0, 0)) * rdyc;
-                rhs_y = pmGamma * conv_y + pmTheta * hy0 - pmAlpha * gradp + tb * d22;
+                const T vp = V(Sp, 1, 0, 0), vc = V(Sc, 1, 0, 0), vm = V(Sm, 1, 0, 0);
+                const T h22 = ((vp + vc) * (vp + vc) - (vc + vm) * (vc + vm)) * qsucac;
+                const T d11 = dxxC(0) * V(Sc, 1, -2, 0) + dxxC(1) * V(Sc, 1, -1, 0) + dxxC(2) * vc + dxxC(3) * V(Sc, 1, 1, 0) + dxxC(4) * V(Sc, 1, 2, 0);
+                const T d22 = (T)__ldg(&m.ap2p[j]) * vp + (T)__ldg(&m.ac2p[j]) * vc + (T)__ldg(&m.am2p[j]) * vm;
+                const T d33 = dzzC(0) * V(Sc, 1, 0, -2) + dzzC(1) * V(Sc, 1, 0, -1) + dzzC(2) * vc + dzzC(3) * V(Sc, 1, 0, 1) + dzzC(4) * V(Sc, 1, 0, 2);
+                conv_y = -h21 - h22 - h23 + xnu * (d11 + d33) + grav(1);
+                const T gradp = (V(Sc, 3, 0, 0) - V(Sm, 3, 0, 0)) * rdyc;
+                rhs_y = tpG * conv_y + tpT * hy0 - tpA * gradp + ttb * d22;
             }
             // ---------------- RhsZ (:238-267)
-            double conv_z, rhs_z;
+            T conv_z, rhs_z;
             {
-                const double uzc = V(Sc, 2, 0, 0);
-                const double uzhyc = IY1 * V(Sm, 2, 0, 0) + IY2 * uzc;
-                const double uzhyp = IY3 * uzc + IY4 * V(Sp, 2, 0, 0);
-                double h31 = 0.0, h33 = 0.0;
+                const T uzc = V(Sc, 2, 0, 0);
+                const T uzhyc = IY1 * V(Sm, 2, 0, 0) + IY2 * uzc;
+                const T uzhyp = IY3 * uzc + IY4 * V(Sp, 2, 0, 0);
+                T h31 = 0.0, h33 = 0.0;
 #pragma unroll
                 for (int q = 0; q < 4; q++) {
                     const int d = q - 1;  // x offsets -1..2 for h31
-                    const double uzhx = I1 * V(Sc, 2, d - 2, 0) + I2 * V(Sc, 2, d - 1, 0) + I3 * V(Sc, 2, d, 0) + I4 * V(Sc, 2, d + 1, 0);
-                    const double uxhz = I1 * V(Sc, 0, d, -2) + I2 * V(Sc, 0, d, -1) + I3 * V(Sc, 0, d, 0) + I4 * V(Sc, 0, d, 1);
-                    h31 = (q == 0) ? c.dxC[0] * uzhx * (uxhz + ucrf) : h31 + c.dxC[q] * uzhx * (uxhz + ucrf);
+                    const T uzhx = I1 * V(Sc, 2, d - 2, 0) + I2 * V(Sc, 2, d - 1, 0) + I3 * V(Sc, 2, d, 0) + I4 * V(Sc, 2, d + 1, 0);
+                    const T uxhz = I1 * V(Sc, 0, d, -2) + I2 * V(Sc, 0, d, -1) + I3 * V(Sc, 0, d, 0) + I4 * V(Sc, 0, d, 1);
+                    h31 = (q == 0) ? dxC(0) * uzhx * (uxhz + ucrf) : h31 + dxC(q) * uzhx * (uxhz + ucrf);
                     const int e = q - 2;  // z offsets -2..1 for h33
-                    const double uzhz = I1 * V(Sc, 2, 0, e - 1) + I2 * V(Sc, 2, 0, e) + I3 * V(Sc, 2, 0, e + 1) + I4 * V(Sc, 2, 0, e + 2);
-                    h33 = (q == 0) ? c.dzC[0] * uzhz * uzhz : h33 + c.dzC[q] * uzhz * uzhz;
+                    const T uzhz = I1 * V(Sc, 2, 0, e - 1) + I2 * V(Sc, 2, 0, e) + I3 * V(Sc, 2, 0, e + 1) + I4 * V(Sc, 2, 0, e + 2);
+                    h33 = (q == 0) ? dzC(0) * uzhz * uzhz : h33 + dzC(q) * uzhz * uzhz;
                 }
-                const double uyhz_j = I1 * V(Sc, 1, 0, -2) + I2 * V(Sc, 1, 0, -1) + I3 * V(Sc, 1, 0, 0) + I4 * V(Sc, 1, 0, 1);
-                const double uyhz_p = top ? 0.0 : I1 * V(Sp, 1, 0, -2) + I2 * V(Sp, 1, 0, -1) + I3 * V(Sp, 1, 0, 0) + I4 * V(Sp, 1, 0, 1);
-                const double h32 = (uyhz_p * uzhyp - uyhz_j * uzhyc) * rdyp;
-                const double d11 = c.dxxC[0] * V(Sc, 2, -2, 0) + c.dxxC[1] * V(Sc, 2, -1, 0) + c.dxxC[2] * uzc + c.dxxC[3] * V(Sc, 2, 1, 0) + c.dxxC[4] * V(Sc, 2, 2, 0);
-                const double d22 = __ldg(&m.ap2c[j]) * V(Sp, 2, 0, 0) + __ldg(&m.ac2c[j]) * uzc + __ldg(&m.am2c[j]) * V(Sm, 2, 0, 0);
-                const double d33 = c.dzzC[0] * V(Sc, 2, 0, -2) + c.dzzC[1] * V(Sc, 2, 0, -1) + c.dzzC[2] * uzc + c.dzzC[3] * V(Sc, 2, 0, 1) + c.dzzC[4] * V(Sc, 2, 0, 2);
-                conv_z = -h31 - h32 - h33 + xnu * (d11 + d33) + c.grav[2];
-                const double gradp = c.dzC[0] * V(Sc, 3, 0, -2) + c.dzC[1] * V(Sc, 3, 0, -1) + c.dzC[2] * V(Sc, 3, 0, 0) + c.dzC[3] * V(Sc, 3, 0, 1);
-                rhs_z = pmGamma * conv_z + pmTheta * hz0 - pmAlpha * gradp + tb * d22;
+                const T uyhz_j = I1 * V(Sc, 1, 0, -2) + I2 * V(Sc, 1, 0, -1) + I3 * V(Sc, 1, 0, 0) + I4 * V(Sc, 1, 0, 1);
+                const T uyhz_p = top ? T(0) : I1 * V(Sp, 1, 0, -2) + I2 * V(Sp, 1, 0, -1) + I3 * V(Sp, 1, 0, 0) + I4 * V(Sp, 1, 0, 1);
+                const T h32 = (uyhz_p * uzhyp - uyhz_j * uzhyc) * rdyp;
+                const T d11 = dxxC(0) * V(Sc, 2, -2, 0) + dxxC(1) * V(Sc, 2, -1, 0) + dxxC(2) * uzc + dxxC(3) * V(Sc, 2, 1, 0) + dxxC(4) * V(Sc, 2, 2, 0);
+                const T d22 = ap2c * V(Sp, 2, 0, 0) + ac2c * uzc + am2c * V(Sm, 2, 0, 0);
+                const T d33 = dzzC(0) * V(Sc, 2, 0, -2) + dzzC(1) * V(Sc, 2, 0, -1) + dzzC(2) * uzc + dzzC(3) * V(Sc, 2, 0, 1) + dzzC(4) * V(Sc, 2, 0, 2);
+                conv_z = -h31 - h32 - h33 + xnu * (d11 + d33) + grav(2);
+                const T gradp = dzC(0) * V(Sc, 3, 0, -2) + dzC(1) * V(Sc, 3, 0, -1) + dzC(2) * V(Sc, 3, 0, 0) + dzC(3) * V(Sc, 3, 0, 1);
+                rhs_z = tpG * conv_z + tpT * hz0 - tpA * gradp + ttb * d22;
             }
             if (SCALAR) {
                 // ---------------- scalar transport (:302-357)
-                const double scc = V(Sc, 4, 0, 0), scjm = V(Sm, 4, 0, 0), scjp = V(Sp, 4, 0, 0);
-                const double shyc = IY1 * scjm + IY2 * scc;
-                const double shyp = IY3 * scc + IY4 * scjp;
-                double hc1 = 0.0, hc3 = 0.0, shx0 = 0.0, shz0 = 0.0;
+                const T scc = V(Sc, 4, 0, 0), scjm = V(Sm, 4, 0, 0), scjp = V(Sp, 4, 0, 0);
+                const T shyc = IY1 * scjm + IY2 * scc;
+                const T shyp = IY3 * scc + IY4 * scjp;
+                T hc1 = 0, hc3 = 0, shx0 = 0, shz0 = 0;
 #pragma unroll
                 for (int q = 0; q < 4; q++) {
                     const int d = q - 1;
-                    const double shx = I1 * V(Sc, 4, d - 2, 0) + I2 * V(Sc, 4, d - 1, 0) + I3 * V(Sc, 4, d, 0) + I4 * V(Sc, 4, d + 1, 0);
-                    const double shz = I1 * V(Sc, 4, 0, d - 2) + I2 * V(Sc, 4, 0, d - 1) + I3 * V(Sc, 4, 0, d) + I4 * V(Sc, 4, 0, d + 1);
+                    const T shx = I1 * V(Sc, 4, d - 2, 0) + I2 * V(Sc, 4, d - 1, 0) + I3 * V(Sc, 4, d, 0) + I4 * V(Sc, 4, d + 1, 0);
+                    const T shz = I1 * V(Sc, 4, 0, d - 2) + I2 * V(Sc, 4, 0, d - 1) + I3 * V(Sc, 4, 0, d) + I4 * V(Sc, 4, 0, d + 1);
                     if (q == 1) { shx0 = shx; shz0 = shz; }
-                    const double ua = V(Sc, 0, d, 0) + c.fvv[0];
-                    const double wa = V(Sc, 2, 0, d) + c.fvv[2];
-                    hc1 = (q == 0) ? c.dxC[0] * ua * shx : hc1 + c.dxC[q] * ua * shx;
-                    hc3 = (q == 0) ? c.dzC[0] * wa * shz : hc3 + c.dzC[q] * wa * shz;
+                    const T ua = V(Sc, 0, d, 0) + fvv(0);
+                    const T wa = V(Sc, 2, 0, d) + fvv(2);
+                    hc1 = (q == 0) ? dxC(0) * ua * shx : hc1 + dxC(q) * ua * shx;
+                    hc3 = (q == 0) ? dzC(0) * wa * shz : hc3 + dzC(q) * wa * shz;
                 }
-                const double c1 = c.gev[0] * shx0, c2 = c.gev[1] * shyc, c3 = c.gev[2] * shz0;
-                rhs_x = rhs_x + pmGamma * c1;
-                rhs_y = rhs_y + pmGamma * c2;
-                rhs_z = rhs_z + pmGamma * c3;
+                const T c1 = gev(0) * shx0, c2 = gev(1) * shyc, c3 = gev(2) * shz0;
+                rhs_x = rhs_x + tpG * c1;
+                rhs_y = rhs_y + tpG * c2;
+                rhs_z = rhs_z + tpG * c3;
                 conv_x = conv_x + c1;
                 conv_y = conv_y + c2;
                 conv_z = conv_z + c3;
-                const double hc2 = ((V(Sp, 1, 0, 0) + c.fvv[1]) * shyp - (V(Sc, 1, 0, 0) + c.fvv[1]) * shyc) * rdyp;
-                const double d11 = c.dxxC[0] * V(Sc, 4, -2, 0) + c.dxxC[1] * V(Sc, 4, -1, 0) + c.dxxC[2] * scc + c.dxxC[3] * V(Sc, 4, 1, 0) + c.dxxC[4] * V(Sc, 4, 2, 0);
-                const double d22 = __ldg(&m.ap2cSc[j]) * scjp + __ldg(&m.ac2cSc[j]) * scc + __ldg(&m.am2cSc[j]) * scjm;
-                const double d33 = c.dzzC[0] * V(Sc, 4, 0, -2) + c.dzzC[1] * V(Sc, 4, 0, -1) + c.dzzC[2] * scc + c.dzzC[3] * V(Sc, 4, 0, 1) + c.dzzC[4] * V(Sc, 4, 0, 2);
-                const double convc = -hc1 - hc2 - hc3 + c.sdiff * (d11 + d33);
-                o_rc[cz] = pmGamma * convc + pmTheta * hc0 + tbs * d22;
+                const T hc2 = ((V(Sp, 1, 0, 0) + fvv(1)) * shyp - (V(Sc, 1, 0, 0) + fvv(1)) * shyc) * rdyp;
+                const T d11 = dxxC(0) * V(Sc, 4, -2, 0) + dxxC(1) * V(Sc, 4, -1, 0) + dxxC(2) * scc + dxxC(3) * V(Sc, 4, 1, 0) + dxxC(4) * V(Sc, 4, 2, 0);
+                const T d22 = (T)__ldg(&m.ap2cSc[j]) * scjp + (T)__ldg(&m.ac2cSc[j]) * scc + (T)__ldg(&m.am2cSc[j]) * scjm;
+                const T d33 = dzzC(0) * V(Sc, 4, 0, -2) + dzzC(1) * V(Sc, 4, 0, -1) + dzzC(2) * scc + dzzC(3) * V(Sc, 4, 0, 1) + dzzC(4) * V(Sc, 4, 0, 2);
+                const T convc = -hc1 - hc2 - hc3 + tsdiff * (d11 + d33);
+                o_rc[cz] = tpG * convc + tpT * hc0 + ttbs * d22;
                 o_hc[cz] = convc;
             }
 #undef V
@@ -291,22 +376,42 @@ __global__ void __launch_bounds__(NTHR, 2)
             for (int cz = 0; cz < ZC; cz++) {
                 if (!act[cz]) continue;
                 const size_t q0 = q0a[cz];
-                fl.rx[q0] = o_rx[cz];
-                fl.ry[q0] = o_ry[cz];
-                fl.rz[q0] = o_rz[cz];
-                fl.hx[q0] = o_hx[cz];
-                fl.hy[q0] = o_hy[cz];
-                fl.hz[q0] = o_hz[cz];
+                fl.rx[q0] = (double)o_rx[cz];
+                fl.ry[q0] = (double)o_ry[cz];
+                fl.rz[q0] = (double)o_rz[cz];
+                fl.hx[q0] = (double)o_hx[cz];
+                fl.hy[q0] = (double)o_hy[cz];
+                fl.hz[q0] = (double)o_hz[cz];
                 if (SCALAR) {
-                    fl.rc[q0] = o_rc[cz];
-                    fl.hc[q0] = o_hc[cz];
+                    fl.rc[q0] = (double)o_rc[cz];
+                    fl.hc[q0] = (double)o_hc[cz];
                 }
+            }
+            if constexpr (!F64) {
+                if (more) {
+                    T* dst = sm + (size_t)((j + 2) % NB) * NF * SLAB;
+#pragma unroll
+                    for (int f = 0; f < NF; f++)
+#pragma unroll
+                        for (int sl = 0; sl < NSLOT; sl++)
+                            if (sval[sl]) dst[f * SLAB + soff[sl]] = (T)pre[f][sl];
+                }
+#pragma unroll
+                for (int cz = 0; cz < ZC; cz++) { u64m[cz] = u64c[cz]; u64c[cz] = u64p[cz]; u64p[cz] = u64n[cz]; }
             }
         __syncthreads();
         }
 #undef LOAD_ROW
     }
-    cp_async_wait<0>();
+    if constexpr (F64) cp_async_wait<0>();
+#undef KC
+#undef dxC
+#undef dzC
+#undef dxxC
+#undef dzzC
+#undef grav
+#undef gev
+#undef fvv
 
     // flow-rate constraint and the substep coefficients (last CTA)
     double s3v[1] = {s3};
@@ -362,21 +467,30 @@ size_t rhs_grid_blocks(const DConst& c) {
 }
 
 void rhs_init() {
-    cudaFuncSetAttribute(k_rhs_tile<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, NB * 4 * SLAB * 8);
-    cudaFuncSetAttribute(k_rhs_tile<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, NB * 5 * SLAB * 8);
+    cudaFuncSetAttribute(k_rhs_tile<false, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rhs_smem_bytes<false, double>());
+    cudaFuncSetAttribute(k_rhs_tile<true, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rhs_smem_bytes<true, double>());
+    cudaFuncSetAttribute(k_rhs_tile<false, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rhs_smem_bytes<false, float>());
+    cudaFuncSetAttribute(k_rhs_tile<true, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rhs_smem_bytes<true, float>());
+}
+
+template <bool SCALAR, class T>
+static void launch_rhs_t(cudaStream_t st, const DConst& c, const DMetric& m, DCoef* coef, const Fields& f, double* uy_ym,
+                         double* duy_ym, int ns, double gam, double the, double alp, double* part, unsigned int* counter) {
+    const dim3 grd((unsigned)rhs_grid_blocks(c));
+    const dim3 blk(32, TZ / RhsCfg<T>::ZC);
+    launch_pdl(k_rhs_tile<SCALAR, T>, grd, blk, rhs_smem_bytes<SCALAR, T>(), st, c, m, coef, f, uy_ym, duy_ym, ns, gam,
+               the, alp, rhs_ychunk(c), part, counter);
 }
 
 void launch_rhs_tile(cudaStream_t st, const DConst& c, const DMetric& m, DCoef* coef, const Fields& f, double* uy_ym,
                      double* duy_ym, int ns, double gam, double the, double alp, double* part, unsigned int* counter) {
-    const int yc = rhs_ychunk(c);
-    dim3 grd((unsigned)rhs_grid_blocks(c));
-    dim3 blk(32, TZ / ZC);
-    if (c.scalar_on)
-        launch_pdl(k_rhs_tile<true>, grd, blk, NB * 5 * SLAB * 8, st, c, m, coef, f, uy_ym, duy_ym, ns, gam, the, alp,
-                   yc, part, counter);
-    else
-        launch_pdl(k_rhs_tile<false>, grd, blk, NB * 4 * SLAB * 8, st, c, m, coef, f, uy_ym, duy_ym, ns, gam, the, alp,
-                   yc, part, counter);
+    if (c.fp32_rhs) {
+        if (c.scalar_on) launch_rhs_t<true, float>(st, c, m, coef, f, uy_ym, duy_ym, ns, gam, the, alp, part, counter);
+        else launch_rhs_t<false, float>(st, c, m, coef, f, uy_ym, duy_ym, ns, gam, the, alp, part, counter);
+    } else {
+        if (c.scalar_on) launch_rhs_t<true, double>(st, c, m, coef, f, uy_ym, duy_ym, ns, gam, the, alp, part, counter);
+        else launch_rhs_t<false, double>(st, c, m, coef, f, uy_ym, duy_ym, ns, gam, the, alp, part, counter);
+    }
 }
 
 }  // namespace ptc

@@ -35,7 +35,7 @@ EXPORTED = [
     "paratc_spectra2d_setup", "paratc_spectra2d_reset", "paratc_spectra2d_accumulate", "paratc_spectra2d_get",
     "paratc_visu_name", "paratc_visu_quantity", "paratc_dump_visu", "paratc_write_xdmf",
     "paratc_io_options_from_namelist", "paratc_visu_quantity_device", "paratc_autotune", "paratc_get_schedule",
-    "paratc_set_schedule",
+    "paratc_set_schedule", "paratc_set_precision", "paratc_get_precision",
 ]
 PROF_NKERNELS = 16
 
@@ -78,6 +78,8 @@ def load(path=None):
     L.paratc_autotune.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int), _dp]
     L.paratc_get_schedule.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]
     L.paratc_set_schedule.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    L.paratc_set_precision.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    L.paratc_get_precision.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]
     L.paratc_dump_visu.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_char_p] + [ctypes.c_int] * 7
     L.paratc_write_xdmf.argtypes = [ctypes.POINTER(ParatcParams), _dp, ctypes.c_char_p, ctypes.c_char_p] + \
         [ctypes.c_int] * 6
@@ -436,6 +438,17 @@ class ChannelSystem:
         self._check(self._L.paratc_visu_quantity(self._h, q, skip[0], skip[1], skip[2], int(bool(node)), _ptr(out),
                                                  None), "paratc_visu_quantity")
         return out
+
+    # -- precision: "fp64" (default) or "mixed" (FP32 right-hand side)
+    @property
+    def precision(self):
+        v = ctypes.c_int()
+        self._check(self._L.paratc_get_precision(self._h, ctypes.byref(v)), "paratc_get_precision")
+        return ("fp64", "mixed")[v.value]
+
+    @precision.setter
+    def precision(self, name):
+        self._check(self._L.paratc_set_precision(self._h, {"fp64": 0, "mixed": 1}[name]), "paratc_set_precision")
 
     # -- Poisson schedule (InitPoissonSolver's auto-tuning)
     def autotune(self, nrep=15):
