@@ -38,12 +38,13 @@ constexpr int TX = 32, TZ = 8, HX = 3, HZ = 3;
 constexpr int SX = TX + 2 * HX;  // 38
 constexpr int SZ = TZ + 2 * HZ;  // 14
 constexpr int SLAB = SX * SZ;    // 532 doubles per field and row
-constexpr int PF = 2;            // FP64: rows loaded ahead beyond row j+1 (cp.async groups in flight)
+constexpr int PF = 1;            // FP64: rows loaded ahead beyond row j+1 (cp.async groups in flight)
 // per precision: z-adjacent cells per thread (FP64: 2, whose shared stencil
 // taps then load once; FP32: 1) and threads per CTA
 template <class T>
 struct RhsCfg {
     static constexpr int NB = sizeof(T) == 8 ? 3 + PF : 4;  // ring slots: rows j-1..j+1 and the rows in flight
+    static constexpr int MINB = 2;                            // resident CTAs per SM (FP64: 3 spills and is slower)
     static constexpr int ZC = sizeof(T) == 8 ? 2 : 1;
     static constexpr int NTHR = TX * TZ / ZC;  // 128 or 256
     static constexpr int NSLOT = (SLAB + NTHR - 1) / NTHR;
@@ -69,7 +70,7 @@ __device__ __forceinline__ int modp(int i, int n) {
 }  // namespace
 
 template <bool SCALAR, class T>
-__global__ void __launch_bounds__(RhsCfg<T>::NTHR, 2)
+__global__ void __launch_bounds__(RhsCfg<T>::NTHR, RhsCfg<T>::MINB)
     k_rhs_tile(DConst c, DMetric m, DCoef* __restrict__ coef, Fields fl, double* __restrict__ uy_ym,
                double* __restrict__ duy_ym, int ns, double gam, double the, double alp, int ychunk,
                double* __restrict__ part, unsigned int* __restrict__ counter) {
@@ -459,11 +460,16 @@ static int rhs_ychunk(const DConst& c) {
     return (c.ny + nch - 1) / nch;
 }
 
-// one wave: two resident CTAs per SM (shared memory and registers allow 2)
-size_t rhs_grid_blocks(const DConst& c) {
+// one wave of resident CTAs (MINB per SM for the precision; the record
+// count is sized for the larger)
+static size_t rhs_blocks(const DConst& c, int minb) {
     const long long rows = (long long)((c.nx + TX - 1) / TX) * ((c.nz + TZ - 1) / TZ) * c.ny;
-    const long long b = 2LL * (c.nsm > 0 ? c.nsm : 148);
+    const long long b = (long long)minb * (c.nsm > 0 ? c.nsm : 148);
     return (size_t)(rows < b ? rows : b);
+}
+
+size_t rhs_grid_blocks(const DConst& c) {
+    return rhs_blocks(c, RhsCfg<double>::MINB > RhsCfg<float>::MINB ? RhsCfg<double>::MINB : RhsCfg<float>::MINB);
 }
 
 void rhs_init() {
@@ -476,7 +482,7 @@ void rhs_init() {
 template <bool SCALAR, class T>
 static void launch_rhs_t(cudaStream_t st, const DConst& c, const DMetric& m, DCoef* coef, const Fields& f, double* uy_ym,
                          double* duy_ym, int ns, double gam, double the, double alp, double* part, unsigned int* counter) {
-    const dim3 grd((unsigned)rhs_grid_blocks(c));
+    const dim3 grd((unsigned)rhs_blocks(c, RhsCfg<T>::MINB));
     const dim3 blk(32, TZ / RhsCfg<T>::ZC);
     launch_pdl(k_rhs_tile<SCALAR, T>, grd, blk, rhs_smem_bytes<SCALAR, T>(), st, c, m, coef, f, uy_ym, duy_ym, ns, gam,
                the, alp, rhs_ychunk(c), part, counter);
