@@ -383,6 +383,7 @@ def run_ensemble(args):
     cells = 0
     for c, y, m in zip(cs, yps, b.members):
         f = cases.initial_fields(c, y)
+        m.precision = args.precision
         m.set_fields(f["ux"], f["uy"], f["uz"], f["p"], f["c"])
         m.project()
         cells += c.params.nxc * c.params.nyc * c.params.nzc
@@ -448,10 +449,11 @@ def run_ensemble(args):
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "scaling": "weak", "vs_baseline": None,
+                "dtype": "f64" if args.precision == "fp64" else "f32 rhs + f64", "data": "synthetic",
                 "config": {"workload": "ensemble_c4: 32 channels, (nx,nz) in {64,96,128,192}, ny in {48,64,96,128}, "
                                        "Re_tau U[120,395], seed 2024",
-                           "cells": cells, "precision": "fp64", "parallelism": "ensemble in one CUDA graph x%d" % ws,
+                           "cells": cells, "precision": args.precision, "parallelism": "ensemble in one CUDA graph x%d" % ws,
                            "l2": "working set %.1f GB > L2, no flush" % (cells * 17 * 8 / 1e9),
                            "graph_kernels_per_step": b.graph_kernels,
                            "divmax_last_step_max": max(d.divmax for d in diags)},
