@@ -146,16 +146,19 @@ class Oracle:
         if rc != 0:
             raise ValueError("orc_set_fields failed: %d" % rc)
 
-    def get_fields(self):
-        names = ["ux", "uy", "uz", "p", "c", "hx", "hy", "hz", "hc"]
+    def get_fields(self, names=None):
+        """The interior fields; `names` selects some of them (the others are
+        not copied)."""
+        allnames = ["ux", "uy", "uz", "p", "c", "hx", "hy", "hz", "hc"]
+        want = set(allnames if names is None else names)
         out = {}
-        for n in names:
-            if n in ("c", "hc") and not self.params.scalar_on:
+        for n in allnames:
+            if n not in want or (n in ("c", "hc") and not self.params.scalar_on):
                 out[n] = None
             else:
                 out[n] = np.empty(self.shape)
-        lib().orc_get_fields(self._h, *[_ptr(out[n]) for n in names])
-        return out
+        lib().orc_get_fields(self._h, *[_ptr(out[n]) for n in allnames])
+        return {n: v for n, v in out.items() if names is None or n in want}
 
     def get_halo(self, name):
         out = np.empty(self.hshape)

@@ -69,3 +69,84 @@ def test_channel_c1_two_steps():
             e = np.abs(got[m] - r[m]).max() / np.abs(r[m]).max()
             assert e <= 1e-12, "C1 spectrum %d rel err %.3e" % (m + 1, e)
     g.close()
+
+
+def test_lock_exchange_c3_two_steps():
+    """C3 (1536 x 160 x 256, half channel, settling scalar with a Robin
+    bottom, CFL-controlled dt) at full size: two steps from the lock
+    initial state against the oracle (fields relative to their largest
+    magnitude: 1e-10 after one step, 1e-8 after two)."""
+    case = cases.lock_exchange_c3()
+    yp = yp_of(case)
+    f = cases.initial_fields(case, yp)
+    o = ol.Oracle(case.params, yp)
+    g = ChannelSystem(case.params, yp)
+    o.set_fields(f["ux"], f["uy"], f["uz"], f["p"], f["c"])
+    g.set_fields(f["ux"], f["uy"], f["uz"], f["p"], f["c"])
+    for s, tol in ((1, 1e-10), (2, 1e-8)):
+        rc, do = o.step()
+        assert rc == 0
+        dg = g.iterate(1)
+        fo, fg = o.get_fields(), g.get_fields()
+        for n in ("ux", "uy", "uz", "p", "c"):
+            e = rel_err(fg[n], fo[n])
+            assert e <= tol, "C3 step %d %s rel err %.3e" % (s, n, e)
+        assert abs(dg.dt - do.dt) <= 1e-12 * do.dt
+        assert dg.divmax <= 1e-10
+    g.close()
+    o.close()
+
+
+def test_turbidity_c5_full_size():
+    """C5 (2304 x 192 x 768, 340 M cells): a manufactured single-mode Poisson
+    solution recovered to 1e-12 through the 1152-point x and 768-point z
+    transforms; then one step of the turbidity case against the oracle
+    (about 60 GB of host memory; fields within 1e-10 of their largest
+    magnitude) and a second one staying solenoidal and finite."""
+    case = cases.turbidity_c5()
+    p = case.params
+    yp = yp_of(case)
+    g = ChannelSystem(p, yp)
+    nx, ny, nz = p.nxc, p.nyc, p.nzc
+    # manufactured solution: phi = cos(2 pi 5 x/Lx) cos(2 pi 3 z/Lz) g(y);
+    # src = (lambda_x + lambda_z) phi + Lyy phi with the solver's own operator
+    o = ol.Oracle(cases.make_params(nx, ny, 8, flow_type=p.flow_type, xlx=p.xlx, yly=p.yly, zlz=p.zlz), yp)
+    wx = o.metric("WaveNumX")[5]
+    am, ac, ap = o.metric("am2ph"), o.metric("ac2ph"), o.metric("ap2ph")
+    o.close()
+    lz = (p.nzc / p.zlz) ** 2 / 288.0
+    w3 = 2 * np.pi * 3 / nz
+    wz = lz * (np.cos(3 * w3) - 54 * np.cos(2 * w3) + 783 * np.cos(w3) - 730)
+    yc = cases.cell_centres_y(yp)
+    gy = np.cos(np.pi * yc / p.yly) + 0.3 * yc
+    lyg = ac * gy
+    lyg[1:] += am[1:] * gy[:-1]
+    lyg[:-1] += ap[:-1] * gy[1:]
+    cx = np.cos(2 * np.pi * 5 * np.arange(nx) / nx)
+    cz = np.cos(2 * np.pi * 3 * np.arange(nz) / nz)
+    src = cz[:, None, None] * ((wx + wz) * gy + lyg)[None, :, None] * cx[None, None, :]
+    phi = g.poisson(src)
+    del src
+    ref = cz[:, None, None] * gy[None, :, None] * cx[None, None, :]
+    assert rel_err(phi, ref) <= 1e-12
+    del phi, ref
+    f = cases.initial_fields(case, yp)
+    o = ol.Oracle(p, yp)
+    for side in (o, g):
+        side.set_fields(f["ux"], f["uy"], f["uz"], f["p"], f["c"])
+    del f
+    o.project()
+    assert g.project() <= 1e-10
+    rc, do = o.step()
+    assert rc == 0
+    dg = g.iterate(1)
+    assert abs(dg.dt - do.dt) <= 1e-12 * do.dt and dg.divmax <= 1e-10
+    for n in ("ux", "uy", "uz", "p", "c"):
+        e = rel_err(g.get_fields([n])[n], o.get_fields([n])[n])
+        assert e <= 1e-10, "C5 step 1 %s rel err %.3e" % (n, e)
+    o.close()
+    d = g.iterate(1)
+    assert d.divmax <= 1e-10 and np.isfinite(d.dt) and d.dt > 0
+    fg = g.get_fields(["ux", "c"])
+    assert np.isfinite(fg["ux"]).all() and np.isfinite(fg["c"]).all()
+    g.close()
