@@ -141,6 +141,19 @@ int set_err(paratc_ctx* c, int code, const std::string& msg) {
             return set_err(ctx, PARATC_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
     } while (0)
 
+// releases a buffer from dalloc before its context ends (a buffer that grows)
+template <class T>
+void dfree(paratc_ctx* ctx, T** p) {
+    if (!*p) return;
+    for (size_t a = 0; a < ctx->allocs.size(); a++)
+        if (ctx->allocs[a] == (void*)*p) {
+            cudaFree(ctx->allocs[a]);
+            ctx->allocs.erase(ctx->allocs.begin() + (long)a);
+            break;
+        }
+    *p = nullptr;
+}
+
 template <class T>
 int dalloc(paratc_ctx* ctx, T** p, size_t n) {
     void* q = nullptr;
@@ -1081,15 +1094,26 @@ int paratc_spectra2d_setup(paratc_ctx* ctx, int nsel, const int* iy) {
     const int nsp = ctx->prm.scalar_on ? 6 : 5;
     const size_t pl = (size_t)ctx->nx * ctx->nz;
     const size_t need_out = (size_t)nsp * nsel * pl, need_s = fj.size() * pl;
+    // grow the buffers (the old ones are released; nothing is in flight on
+    // them once the stream is idle)
+    if (need_out > ctx->spec2d_cap || need_s > ctx->s2_cap || fj.size() > ctx->fj_cap) {
+        if ((rc = sync(ctx))) return rc;
+    }
     if (need_out > ctx->spec2d_cap) {
+        dfree(ctx, &ctx->d_spec2d);
+        ctx->spec2d_cap = 0;
         if ((rc = dalloc(ctx, &ctx->d_spec2d, need_out))) return rc;
         ctx->spec2d_cap = need_out;
     }
     if (need_s > ctx->s2_cap) {
+        dfree(ctx, &ctx->d_s2);
+        ctx->s2_cap = 0;
         if ((rc = dalloc(ctx, &ctx->d_s2, need_s))) return rc;
         ctx->s2_cap = need_s;
     }
     if (fj.size() > ctx->fj_cap) {
+        dfree(ctx, &ctx->d_fj);
+        ctx->fj_cap = 0;
         if ((rc = dalloc(ctx, &ctx->d_fj, fj.size()))) return rc;
         ctx->fj_cap = fj.size();
     }
