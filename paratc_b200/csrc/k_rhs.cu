@@ -5,12 +5,13 @@
 // For every row j it needs rows j-1, j, j+1 of ux, uy, uz, p (and the
 // scalar) over the tile plus the x/z halo of 3 cells that the interpolated
 // face velocities and the 4th-order stencils read (38 x 14 values per field
-// and row).  Those row-slabs sit in a ring of 4 slots in shared memory; the
-// slab of row j+2 is copied in with cp.async while row j is computed, so the
-// HBM loads of one row overlap the arithmetic of the previous one.  Each
-// thread computes one cell per row: RhsX/RhsY/RhsZ (and RhsC) and the new
-// explicit histories, reading every neighbour from shared memory; the six
-// interpolated fields of the reference and their halo updates never exist.
+// and row).  Those row-slabs sit in a ring of 3 + PF slots in shared memory;
+// the slabs of rows j+2 .. j+1+PF are copied in with cp.async while row j is
+// computed, so the HBM loads overlap the arithmetic.  Each thread computes
+// two z-adjacent cells per row (FP64; one in the FP32 form): RhsX/RhsY/RhsZ
+// (and RhsC) and the new explicit histories, reading every neighbour from
+// shared memory; the six interpolated fields of the reference and their halo
+// updates never exist.
 //
 // Two precisions of the same kernel: FP64 (the reference's arithmetic) and a
 // mixed form whose stencil arithmetic and row slabs are FP32 while the state,
@@ -98,17 +99,15 @@ __global__ void __launch_bounds__(RhsCfg<T>::NTHR, RhsCfg<T>::MINB)
     const double pmBeta = 0.5 * alp * c.xnu * dt, pmBetaSc = 0.5 * alp * c.sdiff * dt;
     const double tb = 2.0 * pmBeta, tbs = 2.0 * pmBetaSc;
     // stencil constants straight from the parameter bank, in the kernel's precision
-    const double* const dc64[8] = {c.dxC, c.dzC, c.dxxC, c.dzzC, c.IC, c.grav, c.gev, c.fvv};
-    const float* const dc32[8] = {c.fdxC, c.fdzC, c.fdxxC, c.fdzzC, c.fIC, c.fgrav, c.fgev, c.ffvv};
-#define KC(a, q) (F64 ? (T)dc64[a][q] : (T)dc32[a][q])
-#define dxC(q) KC(0, q)
-#define dzC(q) KC(1, q)
-#define dxxC(q) KC(2, q)
-#define dzzC(q) KC(3, q)
-#define grav(q) KC(5, q)
-#define gev(q) KC(6, q)
-#define fvv(q) KC(7, q)
-    const T I1 = KC(4, 0), I2 = KC(4, 1), I3 = KC(4, 2), I4 = KC(4, 3);
+#define KC(a64, a32, q) (F64 ? (T)c.a64[q] : (T)c.a32[q])
+#define dxC(q) KC(dxC, fdxC, q)
+#define dzC(q) KC(dzC, fdzC, q)
+#define dxxC(q) KC(dxxC, fdxxC, q)
+#define dzzC(q) KC(dzzC, fdzzC, q)
+#define grav(q) KC(grav, fgrav, q)
+#define gev(q) KC(gev, fgev, q)
+#define fvv(q) KC(fvv, ffvv, q)
+    const T I1 = KC(IC, fIC, 0), I2 = KC(IC, fIC, 1), I3 = KC(IC, fIC, 2), I4 = KC(IC, fIC, 3);
     const T ucrf = F64 ? (T)c.ucrf : (T)c.fucrf, xnu = F64 ? (T)c.xnu : (T)c.fxnu;
     const T tpG = (T)pmGamma, tpT = (T)pmTheta, tpA = (T)pmAlpha, ttb = (T)tb, ttbs = (T)tbs;
     const T tsdiff = F64 ? (T)c.sdiff : (T)c.fsdiff;
