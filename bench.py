@@ -46,6 +46,8 @@ def _args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--schedule", type=int, default=-1,
+                    help="pin a Poisson schedule (0-5, paratc_set_schedule) instead of auto-tuning it")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64",
                     help="mixed: the explicit right-hand side in FP32 arithmetic, all else FP64")
     return ap.parse_args()
@@ -152,6 +154,15 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.rows)}
 
 
+def _set_schedule(ctx, args):
+    """The Poisson schedule: auto-tuned (5 solves per choice) unless pinned."""
+    if args.schedule >= 0:
+        ctx.schedule = args.schedule
+        return args.schedule
+    choice, _ = ctx.autotune(nrep=5)
+    return choice
+
+
 def _dist():
     from paratc_b200.replicas import dist_env
     return dist_env()
@@ -234,7 +245,7 @@ def run_ours(args):
     ctx.set_fields(fields["ux"], fields["uy"], fields["uz"], fields["p"], fields["c"])
     ctx.project()
     # InitPoissonSolver's auto-tuning (src/m_Poisson.f90:50-175), before timing
-    schedule, _ = ctx.autotune(nrep=5)
+    schedule = _set_schedule(ctx, args)
     stream = torch.cuda.ExternalStream(ctx.stream, device=local)
     flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device=local)
     iad = {1: 1, 2: 2, 3: 3}[p.ischeme]
@@ -492,7 +503,7 @@ def run_poisson(args):
     src = cases.gaussian_source(cases.Case("src", p, case.mesh, "gauss_src", 42 + rank, 1.0))
     cells = p.nxc * p.nyc * p.nzc
     ctx = ChannelSystem(p, yp, device=local)
-    schedule, _ = ctx.autotune(nrep=5)  # InitPoissonSolver's auto-tuning, before timing
+    schedule = _set_schedule(ctx, args)  # InitPoissonSolver's auto-tuning, before timing
     stream = torch.cuda.ExternalStream(ctx.stream, device=local)
     d_src = torch.from_numpy(src).to("cuda:%d" % local)
     d_phi = torch.empty_like(d_src)
