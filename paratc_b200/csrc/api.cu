@@ -55,6 +55,10 @@ struct paratc_ctx {
     double2 *d_spec = nullptr, *d_twx = nullptr, *d_postx = nullptr, *d_twz = nullptr;
     bool pfft = false;   // compile-time-length transforms exist for nx/2 and nz
     bool plane = false;  // a whole y-plane of the spectrum fits one CTA: fused 2-D transforms
+    bool ztma = false;   // z transforms through the TMA-fed persistent kernel (split path)
+    bool ztma_ok = false;  // its tensor map is encoded (nz supported, driver entry point found)
+    alignas(64) unsigned char zt_tmap[128];  // its tensor map (a CUtensorMap)
+    unsigned int* d_zt_err = nullptr;        // set by a TMA-fed kernel whose bounded wait ran out
     int sched_gen = 0;   // bumped whenever the Poisson schedule changes (captured graphs hold the old one)
     double* d_pfac = nullptr;   // pivots of the spectral y systems (1/vecm, then arr), computed once
     DCoef* d_coef = nullptr;
@@ -200,9 +204,12 @@ void enqueue_poisson_tail(paratc_ctx* ctx, double* out, int padded) {
         return;
     }
     if (ctx->pfft) {
-        { PROF(PK_FFTZ_F); launch_pfft_z(st, -1, ctx->nx, ctx->ny, ctx->nz, ctx->d_spec, ctx->d_twz); }
+        const int ncol = ctx->ny * (ctx->nx / 2 + 1);
+        if (ctx->ztma) { PROF(PK_FFTZ_F); launch_zt_tma(st, -1, ncol, ctx->nz, ctx->zt_tmap, ctx->d_twz, ctx->kc.nsm, ctx->d_zt_err); }
+        else { PROF(PK_FFTZ_F); launch_pfft_z(st, -1, ctx->nx, ctx->ny, ctx->nz, ctx->d_spec, ctx->d_twz); }
         { PROF(PK_YSOLVE); launch_ysolve_fac(st, ctx->kc, ctx->dm, ctx->d_spec, ctx->d_pfac); }
-        { PROF(PK_FFTZ_B); launch_pfft_z(st, +1, ctx->nx, ctx->ny, ctx->nz, ctx->d_spec, ctx->d_twz); }
+        if (ctx->ztma) { PROF(PK_FFTZ_B); launch_zt_tma(st, +1, ncol, ctx->nz, ctx->zt_tmap, ctx->d_twz, ctx->kc.nsm, ctx->d_zt_err); }
+        else { PROF(PK_FFTZ_B); launch_pfft_z(st, +1, ctx->nx, ctx->ny, ctx->nz, ctx->d_spec, ctx->d_twz); }
         { PROF(PK_FFTX_B); launch_pfft_xb(st, ctx->nx, ctx->ny, ctx->nz, ctx->d_spec, out, ctx->d_twx, ctx->d_postx,
                                           ctx->hm.normfft, padded); }
     } else {
@@ -309,6 +316,14 @@ int sync(paratc_ctx* ctx) {
     if (e != cudaSuccess) return set_err(ctx, PARATC_ERR_CUDA, std::string("kernel execution: ") + cudaGetErrorString(e));
     e = cudaGetLastError();
     if (e != cudaSuccess) return set_err(ctx, PARATC_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(e));
+    if (ctx->ztma) {
+        // a TMA-fed transform whose bounded wait ran out left its flag
+        unsigned int* hb = reinterpret_cast<unsigned int*>(ctx->h_scal);
+        e = cudaMemcpyAsync(hb, ctx->d_zt_err, sizeof(unsigned int), cudaMemcpyDeviceToHost, ctx->st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->st);
+        if (e != cudaSuccess) return set_err(ctx, PARATC_ERR_CUDA, std::string("error flag: ") + cudaGetErrorString(e));
+        if (*hb) return set_err(ctx, PARATC_ERR_TIMEOUT, "z transform: a TMA wait gave up");
+    }
     return PARATC_OK;
 }
 
@@ -469,6 +484,7 @@ int paratc_create(const paratc_params* prm, const double* yp, int device, paratc
         pfft_x_init();
         pfft_z_init();
         plane_init();
+        zt_tma_init();
         spectra_init();
         inited = true;
     }
@@ -525,7 +541,8 @@ int paratc_create(const paratc_params* prm, const double* yp, int device, paratc
         (rc = dalloc(ctx, &ctx->d_hfac, helm_fac_doubles(ctx->ny))) ||
         (rc = dalloc(ctx, &ctx->d_pfac, (size_t)2 * ctx->M1 * ctx->nz * ctx->ny)) ||
         (rc = dalloc(ctx, &ctx->d_stats, (size_t)ctx->nyp * 40 + 1)) ||
-        (rc = dalloc(ctx, &ctx->d_stats_part, stats_part_doubles(kc)))) {
+        (rc = dalloc(ctx, &ctx->d_stats_part, stats_part_doubles(kc))) ||
+        (rc = dalloc(ctx, &ctx->d_zt_err, 1))) {
         paratc_destroy(ctx);
         return rc;
     }
@@ -555,6 +572,14 @@ int paratc_create(const paratc_params* prm, const double* yp, int device, paratc
         launch_pois_factors(ctx->st, kc, ctx->dm, ctx->d_pfac);
         CK(cudaGetLastError());
         CK(cudaStreamSynchronize(ctx->st));
+    }
+    // z transforms fed by TMA: the default of the separate-transform path
+    // where nz has a kernel; PARATC_ZT_TMA=0 keeps the register-fed k_zt
+    if (ctx->pfft && zt_tma_supported(ctx->nz))
+        ctx->ztma_ok = zt_tma_prepare(ctx->d_spec, ctx->ny * (ctx->nx / 2 + 1), ctx->nz, ctx->zt_tmap);
+    {
+        const char* e = std::getenv("PARATC_ZT_TMA");
+        ctx->ztma = ctx->ztma_ok && !ctx->plane && !(e && std::atoi(e) == 0);
     }
     // twiddles
     {
@@ -806,27 +831,30 @@ int paratc_poisson(paratc_ctx* ctx, const double* src, double* phi) {
 }
 
 // Poisson schedules: 2*s + (y-1), s 0 fused y-plane transforms, 1 separate
-// compile-time-length x / z transforms, 2 generic mixed-radix transforms; y 1
-// staged, 2 streaming spectral y-solve
+// compile-time-length x / z transforms, 2 generic mixed-radix transforms, 3
+// as 1 with TMA-fed z transforms; y 1 staged, 2 streaming spectral y-solve
 static bool sched_supported(const paratc_ctx* ctx, int choice) {
     if (choice < 0 || choice >= PARATC_SCHED_NCHOICES) return false;
     const int sc = choice / 2;
     const bool pfft_ok = pfft_x_supported(ctx->nx / 2) && pfft_z_supported(ctx->nz);
     if (sc == 0) return pfft_ok && plane_supported(ctx->nx, ctx->nz);
     if (sc == 1) return pfft_ok;
+    if (sc == 3) return pfft_ok && ctx->ztma_ok;
     return true;
 }
 
 static void sched_apply(paratc_ctx* ctx, int choice) {
-    ctx->plane = choice / 2 == 0;
-    ctx->pfft = choice / 2 <= 1;
+    const int sc = choice / 2;
+    ctx->plane = sc == 0;
+    ctx->pfft = sc == 0 || sc == 1 || sc == 3;
+    ctx->ztma = sc == 3;
     ctx->kc.solver_sel = choice % 2 + 1;
     ctx->sched_gen++;
 }
 
 int paratc_get_schedule(paratc_ctx* ctx, int* choice) {
     if (!ctx || !choice) return PARATC_ERR_BAD_ARG;
-    const int sc = ctx->plane ? 0 : (ctx->pfft ? 1 : 2);
+    const int sc = ctx->plane ? 0 : (ctx->ztma ? 3 : (ctx->pfft ? 1 : 2));
     *choice = 2 * sc + (ctx->kc.solver_sel == 2 ? 1 : 0);
     return PARATC_OK;
 }

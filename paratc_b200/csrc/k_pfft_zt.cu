@@ -1,0 +1,229 @@
+// k_pfft_zt.cu -- the z transforms of the Poisson solve fed by TMA.
+//
+// Same transform as k_zt (k_pfft_z.cu): the spectrum for a fixed kz is one
+// contiguous run of ncol = ny*(nx/2+1) complex values, and a batch is B
+// consecutive columns, i.e. a (2B doubles) x (nz rows) box of the 2-D tensor
+// [nz][2*ncol] -- a plain tiled TMA box.  A persistent CTA walks its batches
+// with two shared-memory stages: while it transforms batch n in place, the
+// tensor-memory accelerator loads batch n+1 into the other stage
+// (cp.async.bulk.tensor, completion on an mbarrier) and the store of batch n
+// (cp.async.bulk.tensor from shared memory) overlaps the next batch's
+// passes.  Every wait on an mbarrier or a bulk group is bounded: after
+// kSpinLimit polls the CTA records an error (*err |= 1) and stops.  No
+// multicast; only this GPU's memory.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <cstdio>
+
+#include "common.cuh"
+#include "fft_fixed.cuh"
+#include "kernels.cuh"
+
+namespace ptc {
+namespace {
+
+template <int N>
+struct ZT {
+    static constexpr int B = ff::Shape<N>::B < 4 ? 4 : ff::Shape<N>::B;
+    static constexpr int P = B * N / ff::Shape<N>::RMAX;
+    static constexpr int ROWS = N < 256 ? N : 256;  // TMA box rows (at most 256)
+    static constexpr int NBOX = N / ROWS;
+    static constexpr unsigned STAGE_BYTES = (unsigned)N * B * 16u;
+    static constexpr size_t smem = 1024 + 2 * (size_t)STAGE_BYTES + (size_t)N * 16;
+};
+
+constexpr long long kSpinLimit = 1LL << 22;
+
+__device__ __forceinline__ unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(unsigned long long* m, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_addr(m)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* m, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_addr(m)), "r"(bytes) : "memory");
+}
+// true once phase `parity` of the barrier has completed; false after the spin limit
+__device__ __forceinline__ bool mbar_wait(unsigned long long* m, unsigned parity) {
+    const unsigned a = smem_addr(m);
+    for (long long it = 0; it < kSpinLimit; it++) {
+        unsigned done;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(done)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* tm, int x, int y, unsigned long long* m) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];\n" ::"r"(
+            smem_addr(dst)),
+        "l"(reinterpret_cast<unsigned long long>(tm)), "r"(x), "r"(y), "r"(smem_addr(m))
+        : "memory");
+}
+__device__ __forceinline__ void tma_store_2d(const CUtensorMap* tm, int x, int y, const void* src) {
+    asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.tile.bulk_group [%0, {%1, %2}], [%3];\n" ::"l"(
+                     reinterpret_cast<unsigned long long>(tm)),
+                 "r"(x), "r"(y), "r"(smem_addr(src))
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_read0() { asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait0() { asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory"); }
+
+// whether the CTA's iteration i has a batch (and so a load was issued for it)
+__device__ __forceinline__ bool b_first_unused(int i, int nb) {
+    return (long long)blockIdx.x + (long long)i * gridDim.x < nb;
+}
+
+template <int N, int DIR>
+__global__ void __launch_bounds__(ZT<N>::P) k_zt_tma(const __grid_constant__ CUtensorMap tm, int nb,
+                                                       const double2* __restrict__ twN, unsigned int* __restrict__ err) {
+    constexpr int B = ZT<N>::B, P = ZT<N>::P, ROWS = ZT<N>::ROWS, NBOX = ZT<N>::NBOX;
+    constexpr unsigned SB = ZT<N>::STAGE_BYTES;
+    constexpr ff::Sched SC = ff::make_sched(N);
+    extern __shared__ unsigned char smraw[];
+    // 1 KB-aligned stages (TMA destinations), then the twiddles, then the barriers
+    unsigned char* base = smraw + ((1024 - (smem_addr(smraw) & 1023)) & 1023);
+    double2* stage[2] = {reinterpret_cast<double2*>(base), reinterpret_cast<double2*>(base + SB)};
+    double2* tws = reinterpret_cast<double2*>(base + 2 * SB);
+    __shared__ unsigned long long mbar[2];
+    __shared__ int s_bad;
+    const int tid = threadIdx.x;
+    for (int t = tid; t < N; t += P) tws[t] = twN[t];
+    if (tid == 0) {
+        mbar_init(&mbar[0], 1);
+        mbar_init(&mbar[1], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+        s_bad = 0;
+    }
+    __syncthreads();
+    pdl_wait();  // the spectrum is written by the kernel before this one
+    pdl_trigger();
+    auto issue = [&](int s, int b) {
+        mbar_expect_tx(&mbar[s], SB);
+#pragma unroll
+        for (int r = 0; r < NBOX; r++)
+            tma_load_2d(stage[s] + (size_t)r * ROWS * B, &tm, 2 * B * b, r * ROWS, &mbar[s]);
+    };
+    if (tid == 0) {
+        if ((int)blockIdx.x < nb) issue(0, blockIdx.x);
+        if ((int)(blockIdx.x + gridDim.x) < nb) issue(1, blockIdx.x + gridDim.x);
+    }
+    int it = 0;
+    for (int b = blockIdx.x; b < nb; b += gridDim.x, it++) {
+        const int s = it & 1;
+        double2* buf = stage[s];
+        if (!mbar_wait(&mbar[s], (unsigned)((it >> 1) & 1))) s_bad = 1;
+        __syncthreads();
+        if (s_bad) break;
+        ff::smem_passes<N, B, B, P, DIR, 0, SC.np>(buf, tws, tid);
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        __syncthreads();
+        if (tid == 0) {
+#pragma unroll
+            for (int r = 0; r < NBOX; r++) tma_store_2d(&tm, 2 * B * b, r * ROWS, buf + (size_t)r * ROWS * B);
+            bulk_commit();
+            const int bn = b + 2 * gridDim.x;
+            if (bn < nb) {
+                bulk_wait_read0();  // the store has read this stage
+                issue(s, bn);
+            }
+        }
+    }
+    if (tid == 0) {
+        bulk_wait0();
+        if (s_bad) {
+            atomicOr(err, 1u);
+            // loads still in flight land in this CTA's stages: wait for them (bounded)
+            for (int t = 0; t < 2; t++) {
+                const int i = ((it & 1) == t) ? it : it + 1;  // the stage's oldest unconsumed use
+                if (b_first_unused(i, nb)) mbar_wait(&mbar[t], (unsigned)((i >> 1) & 1));
+            }
+        }
+    }
+}
+
+#define ZT_SIZES(X) X(128) X(256) X(512) X(768) X(1024)
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        cudaDriverEntryPointQueryResult q;
+        void* p = nullptr;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }
+    return fn;
+}
+
+template <int N>
+int zt_batch() { return ZT<N>::B; }
+
+}  // namespace
+
+bool zt_tma_supported(int nz) {
+    switch (nz) {
+#define X_CASE(n) case n:
+        ZT_SIZES(X_CASE)
+#undef X_CASE
+        return true;
+        default: return false;
+    }
+}
+
+void zt_tma_init() {
+#define X_CASE(n)                                                                                              \
+    cudaFuncSetAttribute(k_zt_tma<n, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ZT<n>::smem);     \
+    cudaFuncSetAttribute(k_zt_tma<n, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ZT<n>::smem);
+    ZT_SIZES(X_CASE)
+#undef X_CASE
+}
+
+// the tensor map of the spectrum viewed as [nz][2*ncol] doubles with the
+// batch box (2B x min(nz, 256)); false when the driver cannot encode it
+bool zt_tma_prepare(double2* spec, int ncol, int nz, void* tmap_out) {
+    PFN_cuTensorMapEncodeTiled_v12000 enc = encode_fn();
+    if (!enc || !zt_tma_supported(nz)) return false;
+    int B = 0;
+    switch (nz) {
+#define X_CASE(n) case n: B = zt_batch<n>(); break;
+        ZT_SIZES(X_CASE)
+#undef X_CASE
+        default: return false;
+    }
+    const cuuint64_t dims[2] = {(cuuint64_t)2 * ncol, (cuuint64_t)nz};
+    const cuuint64_t strides[1] = {(cuuint64_t)ncol * 16};
+    const cuuint32_t box[2] = {(cuuint32_t)(2 * B), (cuuint32_t)(nz < 256 ? nz : 256)};
+    const cuuint32_t estr[2] = {1, 1};
+    const CUresult r = enc(reinterpret_cast<CUtensorMap*>(tmap_out), CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, spec, dims,
+                           strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                           CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
+
+void launch_zt_tma(cudaStream_t st, int dir, int ncol, int nz, const void* tmap, const double2* twz, int nsm,
+                   unsigned int* err) {
+    const CUtensorMap& tm = *reinterpret_cast<const CUtensorMap*>(tmap);
+    switch (nz) {
+#define X_CASE(n)                                                                                              \
+    case n: {                                                                                                  \
+        const int nb = (ncol + ZT<n>::B - 1) / ZT<n>::B;                                                       \
+        const int per_sm = (int)((220 * 1024) / ZT<n>::smem);                                                  \
+        int grid = (per_sm > 0 ? per_sm : 1) * nsm;                                                            \
+        if (grid > nb) grid = nb;                                                                              \
+        if (dir < 0) launch_pdl(k_zt_tma<n, -1>, dim3(grid), dim3(ZT<n>::P), ZT<n>::smem, st, tm, nb, twz, err); \
+        else launch_pdl(k_zt_tma<n, 1>, dim3(grid), dim3(ZT<n>::P), ZT<n>::smem, st, tm, nb, twz, err);         \
+        break;                                                                                                 \
+    }
+        ZT_SIZES(X_CASE)
+#undef X_CASE
+        default: break;
+    }
+}
+
+}  // namespace ptc

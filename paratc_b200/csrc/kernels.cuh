@@ -94,6 +94,13 @@ int visu_count(int n, int skip);
 void launch_visu(cudaStream_t st, int q, int iskip, int jskip, int kskip, int node, const DConst& c, const DMetric& m,
                  const Fields& f, double* out, unsigned int* nbad);
 
+// k_pfft_zt.cu: z transforms fed by TMA (persistent CTAs, two stages)
+bool zt_tma_supported(int nz);
+void zt_tma_init();
+bool zt_tma_prepare(double2* spec, int ncol, int nz, void* tmap_out);
+void launch_zt_tma(cudaStream_t st, int dir, int ncol, int nz, const void* tmap, const double2* twz, int nsm,
+                   unsigned int* err);
+
 // k_plane.cu: both transforms of a y-plane in one CTA (planes that fit shared memory)
 bool plane_supported(int nx, int nz);
 void plane_init();

@@ -455,7 +455,7 @@ class ChannelSystem:
         """Times every supported schedule and keeps the fastest: (choice, ms
         for nrep solves per choice, -1 where unsupported)."""
         ch = ctypes.c_int()
-        t = np.zeros(6)
+        t = np.zeros(8)
         self._check(self._L.paratc_autotune(self._h, int(nrep), ctypes.byref(ch), _ptr(t)), "paratc_autotune")
         return ch.value, t
 

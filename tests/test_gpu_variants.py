@@ -98,12 +98,13 @@ def test_plane_and_split_transforms(monkeypatch, plane, dims):
         _steps_vs_oracle(case, 2)
 
 
-@pytest.mark.parametrize("dims", [(64, 48, 64), (24, 20, 30), (128, 96, 128)])
+@pytest.mark.parametrize("dims", [(64, 48, 64), (24, 20, 30), (128, 96, 128), (32, 24, 256)])
 def test_schedules_and_autotune(dims):
     """Every Poisson schedule this grid supports (fused plane transforms,
-    separate fixed-length transforms, generic transforms; staged or
-    streaming y-solve) gives the oracle's fields after two steps; the
-    auto-tuner times all of them and keeps the fastest."""
+    separate fixed-length transforms, generic transforms, separate transforms
+    with TMA-fed z passes; staged or streaming y-solve) gives the oracle's
+    fields after two steps; the auto-tuner times all of them and keeps the
+    fastest."""
     case = cases.small_channel(*dims)
     yp = yp_of(case)
     f = fields_of(case, yp)
@@ -116,9 +117,10 @@ def test_schedules_and_autotune(dims):
     choice, times = g.autotune(nrep=3)
     assert times[choice] > 0 and times[choice] == min(t for t in times if t > 0)
     assert g.schedule == choice
-    supported = [c for c in range(6) if times[c] > 0]
+    supported = [c for c in range(8) if times[c] > 0]
     assert 4 in supported and 5 in supported  # the generic transforms take any 2^a 3^b 5^c size
-    for c in range(6):
+    assert (6 in supported) == (dims[2] in (128, 256, 512, 768, 1024))
+    for c in range(8):
         if c not in supported:
             with pytest.raises(Exception):
                 g.schedule = c
