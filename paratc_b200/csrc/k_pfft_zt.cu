@@ -11,14 +11,12 @@
 // passes.  Every wait on an mbarrier or a bulk group is bounded: after
 // kSpinLimit polls the CTA records an error (*err |= 1) and stops.  No
 // multicast; only this GPU's memory.
-#include <cuda.h>
-#include <cudaTypedefs.h>
-
 #include <cstdio>
 
 #include "common.cuh"
 #include "fft_fixed.cuh"
 #include "kernels.cuh"
+#include "tma.cuh"
 
 namespace ptc {
 namespace {
@@ -33,47 +31,6 @@ struct ZT {
     static constexpr size_t smem = 1024 + 2 * (size_t)STAGE_BYTES + (size_t)N * 16;
 };
 
-constexpr long long kSpinLimit = 1LL << 22;
-
-__device__ __forceinline__ unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ void mbar_init(unsigned long long* m, unsigned count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_addr(m)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(unsigned long long* m, unsigned bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_addr(m)), "r"(bytes) : "memory");
-}
-// true once phase `parity` of the barrier has completed; false after the spin limit
-__device__ __forceinline__ bool mbar_wait(unsigned long long* m, unsigned parity) {
-    const unsigned a = smem_addr(m);
-    for (long long it = 0; it < kSpinLimit; it++) {
-        unsigned done;
-        asm volatile(
-            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-            : "=r"(done)
-            : "r"(a), "r"(parity)
-            : "memory");
-        if (done) return true;
-    }
-    return false;
-}
-__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* tm, int x, int y, unsigned long long* m) {
-    asm volatile(
-        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];\n" ::"r"(
-            smem_addr(dst)),
-        "l"(reinterpret_cast<unsigned long long>(tm)), "r"(x), "r"(y), "r"(smem_addr(m))
-        : "memory");
-}
-__device__ __forceinline__ void tma_store_2d(const CUtensorMap* tm, int x, int y, const void* src) {
-    asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.tile.bulk_group [%0, {%1, %2}], [%3];\n" ::"l"(
-                     reinterpret_cast<unsigned long long>(tm)),
-                 "r"(x), "r"(y), "r"(smem_addr(src))
-                 : "memory");
-}
-__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void bulk_wait_read0() { asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory"); }
-__device__ __forceinline__ void bulk_wait0() { asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory"); }
-
 // whether the CTA's iteration i has a batch (and so a load was issued for it)
 __device__ __forceinline__ bool b_first_unused(int i, int nb) {
     return (long long)blockIdx.x + (long long)i * gridDim.x < nb;
@@ -87,7 +44,7 @@ __global__ void __launch_bounds__(ZT<N>::P) k_zt_tma(const __grid_constant__ CUt
     constexpr ff::Sched SC = ff::make_sched(N);
     extern __shared__ unsigned char smraw[];
     // 1 KB-aligned stages (TMA destinations), then the twiddles, then the barriers
-    unsigned char* base = smraw + ((1024 - (smem_addr(smraw) & 1023)) & 1023);
+    unsigned char* base = smraw + ((1024 - (tma::smem_addr(smraw) & 1023)) & 1023);
     double2* stage[2] = {reinterpret_cast<double2*>(base), reinterpret_cast<double2*>(base + SB)};
     double2* tws = reinterpret_cast<double2*>(base + 2 * SB);
     __shared__ unsigned long long mbar[2];
@@ -95,19 +52,19 @@ __global__ void __launch_bounds__(ZT<N>::P) k_zt_tma(const __grid_constant__ CUt
     const int tid = threadIdx.x;
     for (int t = tid; t < N; t += P) tws[t] = twN[t];
     if (tid == 0) {
-        mbar_init(&mbar[0], 1);
-        mbar_init(&mbar[1], 1);
-        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+        tma::mbar_init(&mbar[0], 1);
+        tma::mbar_init(&mbar[1], 1);
+        tma::fence_mbar_init();
         s_bad = 0;
     }
     __syncthreads();
     pdl_wait();  // the spectrum is written by the kernel before this one
     pdl_trigger();
     auto issue = [&](int s, int b) {
-        mbar_expect_tx(&mbar[s], SB);
+        tma::mbar_expect_tx(&mbar[s], SB);
 #pragma unroll
         for (int r = 0; r < NBOX; r++)
-            tma_load_2d(stage[s] + (size_t)r * ROWS * B, &tm, 2 * B * b, r * ROWS, &mbar[s]);
+            tma::load_2d(stage[s] + (size_t)r * ROWS * B, &tm, 2 * B * b, r * ROWS, &mbar[s]);
     };
     if (tid == 0) {
         if ((int)blockIdx.x < nb) issue(0, blockIdx.x);
@@ -117,31 +74,31 @@ __global__ void __launch_bounds__(ZT<N>::P) k_zt_tma(const __grid_constant__ CUt
     for (int b = blockIdx.x; b < nb; b += gridDim.x, it++) {
         const int s = it & 1;
         double2* buf = stage[s];
-        if (!mbar_wait(&mbar[s], (unsigned)((it >> 1) & 1))) s_bad = 1;
+        if (!tma::mbar_wait(&mbar[s], (unsigned)((it >> 1) & 1))) s_bad = 1;
         __syncthreads();
         if (s_bad) break;
         ff::smem_passes<N, B, B, P, DIR, 0, SC.np>(buf, tws, tid);
-        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        tma::fence_async_smem();
         __syncthreads();
         if (tid == 0) {
 #pragma unroll
-            for (int r = 0; r < NBOX; r++) tma_store_2d(&tm, 2 * B * b, r * ROWS, buf + (size_t)r * ROWS * B);
-            bulk_commit();
+            for (int r = 0; r < NBOX; r++) tma::store_2d(&tm, 2 * B * b, r * ROWS, buf + (size_t)r * ROWS * B);
+            tma::bulk_commit();
             const int bn = b + 2 * gridDim.x;
             if (bn < nb) {
-                bulk_wait_read0();  // the store has read this stage
+                tma::bulk_wait_read0();  // the store has read this stage
                 issue(s, bn);
             }
         }
     }
     if (tid == 0) {
-        bulk_wait0();
+        tma::bulk_wait0();
         if (s_bad) {
             atomicOr(err, 1u);
             // loads still in flight land in this CTA's stages: wait for them (bounded)
             for (int t = 0; t < 2; t++) {
                 const int i = ((it & 1) == t) ? it : it + 1;  // the stage's oldest unconsumed use
-                if (b_first_unused(i, nb)) mbar_wait(&mbar[t], (unsigned)((i >> 1) & 1));
+                if (b_first_unused(i, nb)) tma::mbar_wait(&mbar[t], (unsigned)((i >> 1) & 1));
             }
         }
     }
@@ -149,7 +106,12 @@ __global__ void __launch_bounds__(ZT<N>::P) k_zt_tma(const __grid_constant__ CUt
 
 #define ZT_SIZES(X) X(128) X(256) X(512) X(768) X(1024)
 
-PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+template <int N>
+int zt_batch() { return ZT<N>::B; }
+
+}  // namespace
+
+PFN_cuTensorMapEncodeTiled_v12000 tma_encode_fn() {
     static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
     if (!fn) {
         cudaDriverEntryPointQueryResult q;
@@ -160,11 +122,6 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
     }
     return fn;
 }
-
-template <int N>
-int zt_batch() { return ZT<N>::B; }
-
-}  // namespace
 
 bool zt_tma_supported(int nz) {
     switch (nz) {
@@ -187,7 +144,7 @@ void zt_tma_init() {
 // the tensor map of the spectrum viewed as [nz][2*ncol] doubles with the
 // batch box (2B x min(nz, 256)); false when the driver cannot encode it
 bool zt_tma_prepare(double2* spec, int ncol, int nz, void* tmap_out) {
-    PFN_cuTensorMapEncodeTiled_v12000 enc = encode_fn();
+    PFN_cuTensorMapEncodeTiled_v12000 enc = tma_encode_fn();
     if (!enc || !zt_tma_supported(nz)) return false;
     int B = 0;
     switch (nz) {

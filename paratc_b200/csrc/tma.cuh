@@ -1,0 +1,75 @@
+// tma.cuh -- the tensor-memory-accelerator (TMA) and mbarrier operations the
+// TMA-fed kernels use, as inline PTX: tiled 2-D / 3-D loads into shared
+// memory completing on an mbarrier, tiled stores from shared memory in bulk
+// groups, and bounded waits.  Only this GPU's memory; no cluster multicast.
+#pragma once
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+namespace ptc {
+namespace tma {
+
+// polls of a bounded wait before it gives up
+constexpr long long kSpinLimit = 1LL << 22;
+
+__device__ __forceinline__ unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(unsigned long long* m, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_addr(m)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* m, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_addr(m)), "r"(bytes) : "memory");
+}
+// true once phase `parity` of the barrier has completed; false after the spin limit
+__device__ __forceinline__ bool mbar_wait(unsigned long long* m, unsigned parity) {
+    const unsigned a = smem_addr(m);
+    for (long long it = 0; it < kSpinLimit; it++) {
+        unsigned done;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(done)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+__device__ __forceinline__ void load_2d(void* dst, const CUtensorMap* tm, int x, int y, unsigned long long* m) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];\n" ::"r"(
+            smem_addr(dst)),
+        "l"(reinterpret_cast<unsigned long long>(tm)), "r"(x), "r"(y), "r"(smem_addr(m))
+        : "memory");
+}
+__device__ __forceinline__ void load_3d(void* dst, const CUtensorMap* tm, int x, int y, int z, unsigned long long* m) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];\n" ::"r"(
+            smem_addr(dst)),
+        "l"(reinterpret_cast<unsigned long long>(tm)), "r"(x), "r"(y), "r"(z), "r"(smem_addr(m))
+        : "memory");
+}
+__device__ __forceinline__ void store_2d(const CUtensorMap* tm, int x, int y, const void* src) {
+    asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.tile.bulk_group [%0, {%1, %2}], [%3];\n" ::"l"(
+                     reinterpret_cast<unsigned long long>(tm)),
+                 "r"(x), "r"(y), "r"(smem_addr(src))
+                 : "memory");
+}
+__device__ __forceinline__ void store_3d(const CUtensorMap* tm, int x, int y, int z, const void* src) {
+    asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.tile.bulk_group [%0, {%1, %2, %3}], [%4];\n" ::"l"(
+                     reinterpret_cast<unsigned long long>(tm)),
+                 "r"(x), "r"(y), "r"(z), "r"(smem_addr(src))
+                 : "memory");
+}
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_read0() { asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait0() { asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory"); }
+
+}  // namespace tma
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (null if
+// the driver has none)
+PFN_cuTensorMapEncodeTiled_v12000 tma_encode_fn();
+
+}  // namespace ptc
