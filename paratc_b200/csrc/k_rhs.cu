@@ -7,7 +7,9 @@
 // face velocities and the 4th-order stencils read (38 x 14 values per field
 // and row).  Those row-slabs sit in a ring of 3 + PF slots in shared memory;
 // the slabs of rows j+2 .. j+1+PF are copied in with cp.async while row j is
-// computed, so the HBM loads overlap the arithmetic.  Each thread computes
+// computed, so the HBM loads overlap the arithmetic.  The row's metric
+// coefficients (interpolation weights, 1/dy, the d2/dy2 stencils) travel in
+// the same ring, so no global load sits on a row's dependent path.  Each thread computes
 // two z-adjacent cells per row (FP64; one in the FP32 form): RhsX/RhsY/RhsZ
 // (and RhsC) and the new explicit histories, reading every neighbour from
 // shared memory; the six interpolated fields of the reference and their halo
@@ -63,6 +65,30 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
+// the per-row metric coefficients a row of the RHS reads, staged in shared
+// memory with the row slabs so that no global load sits on a row's path:
+// 0 yinterp(j), 1 yinterp(j+1), 2 rdyp, 3 rdyc, 4 dyp, 5-7 ap2c/ac2c/am2c,
+// 8-10 ap2p/ac2p/am2p, 11-13 ap2cSc/ac2cSc/am2cSc (row j)
+constexpr int MSTRIDE = 16;
+__device__ __forceinline__ const double* met_base(const DMetric& m, int q) {
+    switch (q) {
+        case 0: return m.yinterp;
+        case 1: return m.yinterp + 1;
+        case 2: return m.rdyp;
+        case 3: return m.rdyc;
+        case 4: return m.dyp;
+        case 5: return m.ap2c;
+        case 6: return m.ac2c;
+        case 7: return m.am2c;
+        case 8: return m.ap2p;
+        case 9: return m.ac2p;
+        case 10: return m.am2p;
+        case 11: return m.ap2cSc;
+        case 12: return m.ac2cSc;
+        default: return m.am2cSc;
+    }
+}
+
 __device__ __forceinline__ int modp(int i, int n) {
     int r = i % n;
     return r < 0 ? r + n : r;
@@ -78,9 +104,15 @@ __global__ void __launch_bounds__(RhsCfg<T>::NTHR, RhsCfg<T>::MINB)
     constexpr int NF = SCALAR ? 5 : 4;
     constexpr bool F64 = sizeof(T) == 8;
     constexpr int ZC = RhsCfg<T>::ZC, NTHR = RhsCfg<T>::NTHR, NSLOT = RhsCfg<T>::NSLOT, NB = RhsCfg<T>::NB;
+    // FP64 with the scalar runs at the register limit already; there the
+    // coefficients stay plain loads (staging them spills)
+    constexpr bool MSTAGE = !(SCALAR && F64);
+    constexpr int NMET = MSTAGE ? 11 : 0;
     extern __shared__ __align__(16) unsigned char sm_raw[];
     T* sm = reinterpret_cast<T*>(sm_raw);  // [NB][NF][SLAB]
+    __shared__ __align__(16) double smet[NB][MSTRIDE];
     const int lane = threadIdx.x, wq = threadIdx.y, tid = wq * 32 + lane;
+    const double* mbase = tid < NMET ? met_base(m, tid) : nullptr;
     const int nx = c.nx, nz = c.nz, ny = c.ny;
     const size_t pl = (size_t)c.nyt * nx;
     // work = the (tile, row) pairs in tile-major order; block b takes the
@@ -144,6 +176,10 @@ __global__ void __launch_bounds__(RhsCfg<T>::NTHR, RhsCfg<T>::MINB)
                 else                                                                     \
                     dst_[f_ * SLAB + soff[s_]] = (T)__ldg(fsrc[f_] + goff[s_] + ro_);    \
             }                                                                            \
+        if (tid < NMET && (jrow) >= 1 && (jrow) <= ny) {                                 \
+            if constexpr (F64) cp_async8(&smet[(jrow) % NB][tid], mbase + (jrow));       \
+            else smet[(jrow) % NB][tid] = __ldg(mbase + (jrow));                         \
+        }                                                                                \
     } while (0)
 
         LOAD_ROW(j0 - 1);
@@ -195,6 +231,7 @@ __global__ void __launch_bounds__(RhsCfg<T>::NTHR, RhsCfg<T>::MINB)
             // FP32 form: row j+2 in registers now, converted and stored after
             // the arithmetic of row j
             double pre[NF][NSLOT];
+            double mpre = 0.0;
             const bool more = j + 2 <= j1 + 1;
             if constexpr (F64) {
                 if (j + 1 + PF <= j1 + 1) LOAD_ROW(j + 1 + PF);
@@ -205,6 +242,7 @@ __global__ void __launch_bounds__(RhsCfg<T>::NTHR, RhsCfg<T>::MINB)
                 for (int f = 0; f < NF; f++)
 #pragma unroll
                     for (int sl = 0; sl < NSLOT; sl++) pre[f][sl] = sval[sl] ? __ldg(fsrc[f] + goff[sl] + ro) : 0.0;
+                if (tid < NMET && j + 2 <= ny) mpre = __ldg(mbase + j + 2);
             }
             double hx0a[ZC], hy0a[ZC], hz0a[ZC], hc0a[ZC];
             size_t q0a[ZC];
@@ -235,11 +273,13 @@ __global__ void __launch_bounds__(RhsCfg<T>::NTHR, RhsCfg<T>::MINB)
                 const T* Sp = sm + (size_t)((j + 1) % NB) * NF * SLAB;
 #define V(S, f, dx, dz) (S)[(f) * SLAB + (w + HZ + (dz)) * SX + (lane + HX + (dx))]
             const bool top = (j == ny);
-            const double IY1d = __ldg(&m.yinterp[j]), IY3d = __ldg(&m.yinterp[j + 1]);
+            const double* M = smet[j % NB];
+#define MET(q, arr) (MSTAGE ? M[q] : __ldg(&m.arr[j]))
+            const double IY1d = MET(0, yinterp), IY3d = MSTAGE ? M[1] : __ldg(&m.yinterp[j + 1]);
             const T IY1 = (T)IY1d, IY2 = (T)(1.0 - IY1d), IY3 = (T)IY3d, IY4 = (T)(1.0 - IY3d);
-            const T rdyp = (T)__ldg(&m.rdyp[j]), rdyc = (T)__ldg(&m.rdyc[j]);
-            const double dyp = __ldg(&m.dyp[j]);
-            const T ap2c = (T)__ldg(&m.ap2c[j]), ac2c = (T)__ldg(&m.ac2c[j]), am2c = (T)__ldg(&m.am2c[j]);
+            const T rdyp = (T)MET(2, rdyp), rdyc = (T)MET(3, rdyc);
+            const double dyp = MET(4, dyp);
+            const T ap2c = (T)MET(5, ap2c), ac2c = (T)MET(6, ac2c), am2c = (T)MET(7, am2c);
 #pragma unroll
             for (int cz = 0; cz < ZC; cz++) {
             const int w = wq * ZC + cz;
@@ -278,7 +318,7 @@ __global__ void __launch_bounds__(RhsCfg<T>::NTHR, RhsCfg<T>::MINB)
                     if (act[cz]) s3 += SCALAR ? uxc * dyp : (dcq13 + d22) * dyp;
                 } else if (act[cz]) {
                     s3 += SCALAR ? u64c[cz] * dyp
-                                 : (__ldg(&m.ap2c[j]) * u64p[cz] + __ldg(&m.ac2c[j]) * u64c[cz] + __ldg(&m.am2c[j]) * u64m[cz]) * dyp;
+                                 : (MET(5, ap2c) * u64p[cz] + MET(6, ac2c) * u64c[cz] + MET(7, am2c) * u64m[cz]) * dyp;
                 }
                 conv_x = -h11 - h12 - h13 + xnu * dcq13 + grav(0);
                 const T gradp = dxC(0) * V(Sc, 3, -2, 0) + dxC(1) * V(Sc, 3, -1, 0) + dxC(2) * V(Sc, 3, 0, 0) + dxC(3) * V(Sc, 3, 1, 0);
@@ -302,7 +342,7 @@ __global__ void __launch_bounds__(RhsCfg<T>::NTHR, RhsCfg<T>::MINB)
                 const T vp = V(Sp, 1, 0, 0), vc = V(Sc, 1, 0, 0), vm = V(Sm, 1, 0, 0);
                 const T h22 = ((vp + vc) * (vp + vc) - (vc + vm) * (vc + vm)) * qsucac;
                 const T d11 = dxxC(0) * V(Sc, 1, -2, 0) + dxxC(1) * V(Sc, 1, -1, 0) + dxxC(2) * vc + dxxC(3) * V(Sc, 1, 1, 0) + dxxC(4) * V(Sc, 1, 2, 0);
-                const T d22 = (T)__ldg(&m.ap2p[j]) * vp + (T)__ldg(&m.ac2p[j]) * vc + (T)__ldg(&m.am2p[j]) * vm;
+                const T d22 = (T)MET(8, ap2p) * vp + (T)MET(9, ac2p) * vc + (T)MET(10, am2p) * vm;
                 const T d33 = dzzC(0) * V(Sc, 1, 0, -2) + dzzC(1) * V(Sc, 1, 0, -1) + dzzC(2) * vc + dzzC(3) * V(Sc, 1, 0, 1) + dzzC(4) * V(Sc, 1, 0, 2);
                 conv_y = -h21 - h22 - h23 + xnu * (d11 + d33) + grav(1);
                 const T gradp = (V(Sc, 3, 0, 0) - V(Sm, 3, 0, 0)) * rdyc;
@@ -368,6 +408,7 @@ __global__ void __launch_bounds__(RhsCfg<T>::NTHR, RhsCfg<T>::MINB)
                 o_hc[cz] = convc;
             }
 #undef V
+#undef MET
             o_rx[cz] = rhs_x; o_ry[cz] = rhs_y; o_rz[cz] = rhs_z;
             o_hx[cz] = conv_x; o_hy[cz] = conv_y; o_hz[cz] = conv_z;
             }
@@ -395,6 +436,7 @@ __global__ void __launch_bounds__(RhsCfg<T>::NTHR, RhsCfg<T>::MINB)
 #pragma unroll
                         for (int sl = 0; sl < NSLOT; sl++)
                             if (sval[sl]) dst[f * SLAB + soff[sl]] = (T)pre[f][sl];
+                    if (tid < NMET && j + 2 <= ny) smet[(j + 2) % NB][tid] = mpre;
                 }
 #pragma unroll
                 for (int cz = 0; cz < ZC; cz++) { u64m[cz] = u64c[cz]; u64c[cz] = u64p[cz]; u64p[cz] = u64n[cz]; }
