@@ -57,6 +57,7 @@ struct paratc_ctx {
     bool plane = false;  // a whole y-plane of the spectrum fits one CTA: fused 2-D transforms
     bool ztma = false;   // z transforms through the TMA-fed persistent kernel (split path)
     bool ztma_ok = false;  // its tensor map is encoded (nz supported, driver entry point found)
+    bool xtma = false;     // x transforms through the bulk-copy-fed persistent kernels (split path)
     alignas(64) unsigned char zt_tmap[128];  // its tensor map (a CUtensorMap)
     unsigned int* d_zt_err = nullptr;        // set by a TMA-fed kernel whose bounded wait ran out
     int sched_gen = 0;   // bumped whenever the Poisson schedule changes (captured graphs hold the old one)
@@ -192,6 +193,8 @@ std::vector<double2> twiddles(int n, int count) {
     return w;
 }
 
+static bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
 // the z transforms, the y-solve and the x inverse, after the forward x
 // transform has filled d_spec
 void enqueue_poisson_tail(paratc_ctx* ctx, double* out, int padded) {
@@ -210,8 +213,15 @@ void enqueue_poisson_tail(paratc_ctx* ctx, double* out, int padded) {
         { PROF(PK_YSOLVE); launch_ysolve_fac(st, ctx->kc, ctx->dm, ctx->d_spec, ctx->d_pfac); }
         if (ctx->ztma) { PROF(PK_FFTZ_B); launch_zt_tma(st, +1, ncol, ctx->nz, ctx->zt_tmap, ctx->d_twz, ctx->kc.nsm, ctx->d_zt_err); }
         else { PROF(PK_FFTZ_B); launch_pfft_z(st, +1, ctx->nx, ctx->ny, ctx->nz, ctx->d_spec, ctx->d_twz); }
-        { PROF(PK_FFTX_B); launch_pfft_xb(st, ctx->nx, ctx->ny, ctx->nz, ctx->d_spec, out, ctx->d_twx, ctx->d_postx,
-                                          ctx->hm.normfft, padded); }
+        if (ctx->xtma && aligned16(out)) {
+            PROF(PK_FFTX_B);
+            launch_xb_tma(st, ctx->nx, ctx->ny, ctx->nz, ctx->d_spec, out, ctx->d_twx, ctx->d_postx, ctx->hm.normfft,
+                          padded, ctx->kc.nsm, ctx->d_zt_err);
+        } else {
+            PROF(PK_FFTX_B);
+            launch_pfft_xb(st, ctx->nx, ctx->ny, ctx->nz, ctx->d_spec, out, ctx->d_twx, ctx->d_postx, ctx->hm.normfft,
+                           padded);
+        }
     } else {
         const int nrows = ctx->ny * ctx->nz;
         { PROF(PK_FFTZ_F); launch_fft_z(st, -1, ctx->nx, ctx->ny, ctx->nz, ctx->d_spec, ctx->plz, ctx->d_twz); }
@@ -231,6 +241,13 @@ void enqueue_poisson_head(paratc_ctx* ctx, int mode, const double* src, double* 
         PROF(mode == 2 ? PK_FFTX_F : PK_PRSRC);
         launch_plane_f(st, mode, ctx->kc, ctx->dm, ctx->d_coef, ctx->f, src, ctx->d_spec, ctx->d_twx, ctx->d_postx,
                        ctx->d_twz, ctx->d_part, ctx->d_counter + 1, out_max);
+        ctx->launches += 1;
+        return;
+    }
+    if (ctx->pfft && mode == 2 && ctx->xtma && aligned16(src)) {
+        PROF(PK_FFTX_F);
+        launch_xf_tma(st, ctx->nx, ctx->ny, ctx->nz, src, ctx->d_spec, ctx->d_twx, ctx->d_postx, ctx->kc.nsm,
+                      ctx->d_zt_err);
         ctx->launches += 1;
         return;
     }
@@ -316,13 +333,14 @@ int sync(paratc_ctx* ctx) {
     if (e != cudaSuccess) return set_err(ctx, PARATC_ERR_CUDA, std::string("kernel execution: ") + cudaGetErrorString(e));
     e = cudaGetLastError();
     if (e != cudaSuccess) return set_err(ctx, PARATC_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(e));
-    if (ctx->ztma) {
+    if (ctx->ztma || ctx->xtma) {
         // a TMA-fed transform whose bounded wait ran out left its flag
         unsigned int* hb = reinterpret_cast<unsigned int*>(ctx->h_scal);
         e = cudaMemcpyAsync(hb, ctx->d_zt_err, sizeof(unsigned int), cudaMemcpyDeviceToHost, ctx->st);
         if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->st);
         if (e != cudaSuccess) return set_err(ctx, PARATC_ERR_CUDA, std::string("error flag: ") + cudaGetErrorString(e));
-        if (*hb) return set_err(ctx, PARATC_ERR_TIMEOUT, "z transform: a TMA wait gave up");
+        if (*hb) return set_err(ctx, PARATC_ERR_TIMEOUT, (*hb & 1u) ? "z transform: a TMA wait gave up"
+                                                                      : "x transform: a TMA wait gave up");
     }
     return PARATC_OK;
 }
@@ -485,6 +503,7 @@ int paratc_create(const paratc_params* prm, const double* yp, int device, paratc
         pfft_z_init();
         plane_init();
         zt_tma_init();
+        xt_tma_init();
         spectra_init();
         inited = true;
     }
@@ -580,6 +599,8 @@ int paratc_create(const paratc_params* prm, const double* yp, int device, paratc
     {
         const char* e = std::getenv("PARATC_ZT_TMA");
         ctx->ztma = ctx->ztma_ok && !ctx->plane && !(e && std::atoi(e) == 0);
+        const char* ex = std::getenv("PARATC_XT_TMA");
+        ctx->xtma = ctx->pfft && xt_tma_supported(ctx->nx / 2) && !(ex && std::atoi(ex) == 0);
     }
     // twiddles
     {

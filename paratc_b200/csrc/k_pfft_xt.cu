@@ -1,0 +1,304 @@
+// k_pfft_xt.cu -- the x transforms of the Poisson solve fed by bulk copies.
+//
+// The same packed real transforms as k_xf (given source) and k_xb
+// (k_pfft_x.cu), with the rows moved by the tensor-memory accelerator
+// instead of by threads.  A persistent CTA keeps two shared-memory stages of
+// B rows, each row contiguous (row b at b*PITCH complex values, which is the
+// layout the bulk copies need), and walks its batches: while it transforms
+// one stage, cp.async.bulk loads (completion on an mbarrier) fill the other,
+// and the previous results leave through bulk stores from shared memory.
+//
+// Inverse (k_xb_tma): spectrum rows of nx/2+1 complex values in, merge of
+// modes a and N-a with 1/(nx*nz) folded in, inverse FFT, phi rows out, with
+// the Neumann ghost copies phi(0) = phi(1), phi(nyp) = phi(nyc) of the
+// padded layout (SetBC_and_UpdateHalo_pr, src/m_BC_and_Halo.f90:115-120).
+// Forward (k_xf_tma): rows of a given source in, FFT, split in place into
+// the nx/2+1 modes of the real transform, spectrum rows out.
+//
+// Every wait is bounded: after kSpinLimit polls the CTA records an error
+// (*err |= 2), waits (bounded) for its own copies in flight and stops.  No
+// multicast; only this GPU's memory.
+#include "common.cuh"
+#include "fft_fixed.cuh"
+#include "kernels.cuh"
+#include "tma.cuh"
+
+namespace ptc {
+namespace {
+
+template <int N>
+struct XT {
+    static constexpr int B = ff::Shape<N>::B;
+    static constexpr int P = ff::Shape<N>::P;
+    static constexpr int M1 = N + 1;
+    // row pitch in complex values: at least N+1, with B*PITCH residues that
+    // spread a quarter warp's (row, element) pairs over the eight 16-byte
+    // bank groups (b fastest across lanes, then consecutive elements)
+    static constexpr int pitch() {
+        const int want = B >= 8 ? 1 : 8 / B;
+        int p = M1;
+        while (B > 1 && p % 8 != want % 8) p++;
+        return p;
+    }
+    static constexpr int PITCH = pitch();
+    static constexpr unsigned STAGE = (unsigned)B * PITCH;  // complex values per stage
+    static constexpr size_t smem = 2 * (size_t)STAGE * sizeof(double2);
+};
+
+// whether the CTA's iteration i has a batch (and so a load was issued for it)
+__device__ __forceinline__ bool xt_has(int i, int nb) {
+    return (long long)blockIdx.x + (long long)i * gridDim.x < nb;
+}
+
+// the error path: record, then wait (bounded) for the loads still in flight
+// into this CTA's stages; it runs in thread 0 after its stores drained
+__device__ __forceinline__ void xt_fail(unsigned long long* mbar, int it, int nb, unsigned int* err) {
+    atomicOr(err, 2u);
+    for (int t = 0; t < 2; t++) {
+        const int i = ((it & 1) == t) ? it : it + 1;  // the stage's oldest unconsumed use
+        if (xt_has(i, nb)) tma::mbar_wait(&mbar[t], (unsigned)((i >> 1) & 1));
+    }
+}
+
+template <int N>
+__global__ void __launch_bounds__(XT<N>::P)
+    k_xb_tma(int nrows, int ny, const double2* __restrict__ spec, double* __restrict__ phi,
+             const double2* __restrict__ twN, const double2* __restrict__ post, double scale, int padded,
+             unsigned int* __restrict__ err) {
+    constexpr int B = XT<N>::B, P = XT<N>::P, PITCH = XT<N>::PITCH, M1 = N + 1;
+    constexpr unsigned SB = XT<N>::STAGE;
+    constexpr ff::Sched SC = ff::make_sched(N);
+    extern __shared__ __align__(128) unsigned char smraw[];
+    double2* stage[2] = {reinterpret_cast<double2*>(smraw), reinterpret_cast<double2*>(smraw) + SB};
+    __shared__ unsigned long long mbar[2];
+    __shared__ int s_bad;
+    const int tid = threadIdx.x;
+    const int nb = (nrows + B - 1) / B;
+    const int nx = 2 * N, nyt = ny + 2;
+    if (tid == 0) {
+        tma::mbar_init(&mbar[0], 1);
+        tma::mbar_init(&mbar[1], 1);
+        tma::fence_mbar_init();
+        s_bad = 0;
+    }
+    __syncthreads();
+    pdl_wait();  // the spectrum is written by the kernel before this one
+    pdl_trigger();
+    auto issue = [&](int s, int bt) {
+        const int g0 = bt * B, nv = min(B, nrows - g0);
+        tma::mbar_expect_tx(&mbar[s], (unsigned)nv * M1 * (unsigned)sizeof(double2));
+        for (int b = 0; b < nv; b++)
+            tma::bulk_load(stage[s] + b * PITCH, spec + (size_t)(g0 + b) * M1, M1 * (unsigned)sizeof(double2), &mbar[s]);
+    };
+    if (tid == 0) {
+        if ((int)blockIdx.x < nb) issue(0, blockIdx.x);
+        if ((int)(blockIdx.x + gridDim.x) < nb) issue(1, blockIdx.x + gridDim.x);
+    }
+    int it = 0;
+    for (int bt = blockIdx.x; bt < nb; bt += gridDim.x, it++) {
+        const int s = it & 1;
+        double2* buf = stage[s];
+        if (!tma::mbar_wait(&mbar[s], (unsigned)((it >> 1) & 1))) s_bad = 1;
+        __syncthreads();
+        if (s_bad) break;
+        // merge modes a and N-a of every row into z[a], z[N-a] (the DC and
+        // Nyquist coefficients are real), scaled by 1/(nx*nz)
+        for (int f = tid; f < B * (N / 2 + 1); f += P) {
+            const int a = f / B, b = f - a * B;
+            const int bn = N - a;
+            double2* rb = buf + b * PITCH;
+            double2 xa = rb[a], xb = rb[bn];
+            if (a == 0) { xa.y = 0.0; xb.y = 0.0; }
+            const double2 e2a = make_double2(xa.x + xb.x, xa.y - xb.y);
+            const double2 da = make_double2(xa.x - xb.x, xa.y + xb.y);
+            const double2 o2a = cmulc(da, __ldg(&post[a]));
+            const double2 za = make_double2(scale * (e2a.x - o2a.y), scale * (e2a.y + o2a.x));
+            if (a == 0) {
+                rb[0] = za;
+            } else {
+                const double2 e2b = make_double2(xb.x + xa.x, xb.y - xa.y);
+                const double2 db = make_double2(xb.x - xa.x, xb.y + xa.y);
+                const double2 o2b = cmulc(db, __ldg(&post[bn]));
+                rb[a] = za;
+                if (bn != a) rb[bn] = make_double2(scale * (e2b.x - o2b.y), scale * (e2b.y + o2b.x));
+            }
+        }
+        __syncthreads();
+        ff::smem_passes<N, B, PITCH, P, 1, 0, SC.np, 4, true>(buf, twN, tid);
+        tma::fence_async_smem();
+        __syncthreads();
+        if (tid == 0) {
+            const int g0 = bt * B, nv = min(B, nrows - g0);
+            constexpr unsigned RB = N * (unsigned)sizeof(double2);
+            for (int b = 0; b < nv; b++) {
+                const int g = g0 + b;
+                const double2* row = buf + b * PITCH;
+                if (!padded) {
+                    tma::bulk_store(phi + (size_t)g * nx, row, RB);
+                    continue;
+                }
+                const int k = g / ny, jc = g - k * ny + 1;
+                double* rowp = phi + ((size_t)k * nyt + jc) * nx;
+                tma::bulk_store(rowp, row, RB);
+                if (jc == 1) tma::bulk_store(rowp - nx, row, RB);
+                if (jc == ny) tma::bulk_store(rowp + nx, row, RB);
+            }
+            tma::bulk_commit();
+            const int bn = bt + 2 * gridDim.x;
+            if (bn < nb) {
+                tma::bulk_wait_read0();  // the stores have read this stage
+                issue(s, bn);
+            }
+        }
+    }
+    if (tid == 0) {
+        tma::bulk_wait0();
+        if (s_bad) xt_fail(mbar, it, nb, err);
+    }
+}
+
+template <int N>
+__global__ void __launch_bounds__(XT<N>::P)
+    k_xf_tma(int nrows, const double* __restrict__ src, double2* __restrict__ spec, const double2* __restrict__ twN,
+             const double2* __restrict__ post, unsigned int* __restrict__ err) {
+    constexpr int B = XT<N>::B, P = XT<N>::P, PITCH = XT<N>::PITCH, M1 = N + 1;
+    constexpr unsigned SB = XT<N>::STAGE;
+    constexpr ff::Sched SC = ff::make_sched(N);
+    extern __shared__ __align__(128) unsigned char smraw[];
+    double2* stage[2] = {reinterpret_cast<double2*>(smraw), reinterpret_cast<double2*>(smraw) + SB};
+    __shared__ unsigned long long mbar[2];
+    __shared__ int s_bad;
+    const int tid = threadIdx.x;
+    const int nb = (nrows + B - 1) / B;
+    const int nx = 2 * N;
+    if (tid == 0) {
+        tma::mbar_init(&mbar[0], 1);
+        tma::mbar_init(&mbar[1], 1);
+        tma::fence_mbar_init();
+        s_bad = 0;
+    }
+    __syncthreads();
+    pdl_wait();
+    pdl_trigger();
+    auto issue = [&](int s, int bt) {
+        const int g0 = bt * B, nv = min(B, nrows - g0);
+        tma::mbar_expect_tx(&mbar[s], (unsigned)nv * N * (unsigned)sizeof(double2));
+        for (int b = 0; b < nv; b++)
+            tma::bulk_load(stage[s] + b * PITCH, src + (size_t)(g0 + b) * nx, N * (unsigned)sizeof(double2), &mbar[s]);
+    };
+    if (tid == 0) {
+        if ((int)blockIdx.x < nb) issue(0, blockIdx.x);
+        if ((int)(blockIdx.x + gridDim.x) < nb) issue(1, blockIdx.x + gridDim.x);
+    }
+    int it = 0;
+    for (int bt = blockIdx.x; bt < nb; bt += gridDim.x, it++) {
+        const int s = it & 1;
+        double2* buf = stage[s];
+        if (!tma::mbar_wait(&mbar[s], (unsigned)((it >> 1) & 1))) s_bad = 1;
+        __syncthreads();
+        if (s_bad) break;
+        ff::smem_passes<N, B, PITCH, P, -1, 0, SC.np, 4, true>(buf, twN, tid);
+        // split the packed transform into the nx/2+1 modes, in place: one
+        // thread takes the pair (a, N-a) (and a = 0 also writes mode N)
+        for (int f = tid; f < B * (N / 2 + 1); f += P) {
+            const int a = f / B, b = f - a * B;
+            const int bn = N - a;
+            double2* rb = buf + b * PITCH;
+            const double2 za = rb[a], zb = rb[a == 0 ? 0 : bn];
+            const double2 E = make_double2(0.5 * (za.x + zb.x), 0.5 * (za.y - zb.y));
+            const double2 O = make_double2(0.5 * (za.y + zb.y), -0.5 * (za.x - zb.x));
+            const double2 xa = cadd(E, cmul(__ldg(&post[a]), O));
+            if (a == 0) {
+                rb[0] = xa;
+                rb[N] = cadd(E, cmul(__ldg(&post[N]), O));
+            } else if (bn != a) {
+                const double2 E2 = make_double2(0.5 * (zb.x + za.x), 0.5 * (zb.y - za.y));
+                const double2 O2 = make_double2(0.5 * (zb.y + za.y), -0.5 * (zb.x - za.x));
+                rb[a] = xa;
+                rb[bn] = cadd(E2, cmul(__ldg(&post[bn]), O2));
+            } else {
+                rb[a] = xa;
+            }
+        }
+        tma::fence_async_smem();
+        __syncthreads();
+        if (tid == 0) {
+            const int g0 = bt * B, nv = min(B, nrows - g0);
+            for (int b = 0; b < nv; b++)
+                tma::bulk_store(spec + (size_t)(g0 + b) * M1, buf + b * PITCH, M1 * (unsigned)sizeof(double2));
+            tma::bulk_commit();
+            const int bn = bt + 2 * gridDim.x;
+            if (bn < nb) {
+                tma::bulk_wait_read0();
+                issue(s, bn);
+            }
+        }
+    }
+    if (tid == 0) {
+        tma::bulk_wait0();
+        if (s_bad) xt_fail(mbar, it, nb, err);
+    }
+}
+
+#define XT_SIZES(X) X(8) X(12) X(16) X(24) X(32) X(40) X(48) X(64) X(96) X(128) X(192) X(256) X(384) X(512) \
+    X(768) X(1024) X(1152) X(1536)
+
+template <int N>
+int xt_grid(int nrows, int nsm) {
+    const int nb = (nrows + XT<N>::B - 1) / XT<N>::B;
+    const int per_sm = (int)((220 * 1024) / (XT<N>::smem + 1024));
+    int grid = (per_sm > 0 ? per_sm : 1) * nsm;
+    return grid < nb ? grid : nb;
+}
+
+}  // namespace
+
+bool xt_tma_supported(int n) {
+    switch (n) {
+#define X_CASE(n) case n:
+        XT_SIZES(X_CASE)
+#undef X_CASE
+        return true;
+        default: return false;
+    }
+}
+
+void xt_tma_init() {
+#define X_CASE(n)                                                                                              \
+    cudaFuncSetAttribute(k_xb_tma<n>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)XT<n>::smem);          \
+    cudaFuncSetAttribute(k_xf_tma<n>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)XT<n>::smem);
+    XT_SIZES(X_CASE)
+#undef X_CASE
+}
+
+void launch_xb_tma(cudaStream_t st, int nx, int ny, int nz, const double2* spec, double* phi, const double2* twx,
+                   const double2* post, double scale, int padded, int nsm, unsigned int* err) {
+    const int nrows = ny * nz;
+    switch (nx / 2) {
+#define X_CASE(n)                                                                                              \
+    case n:                                                                                                    \
+        launch_pdl(k_xb_tma<n>, dim3(xt_grid<n>(nrows, nsm)), dim3(XT<n>::P), XT<n>::smem, st, nrows, ny, spec, \
+                   phi, twx, post, scale, padded, err);                                                        \
+        break;
+        XT_SIZES(X_CASE)
+#undef X_CASE
+        default: break;
+    }
+}
+
+void launch_xf_tma(cudaStream_t st, int nx, int ny, int nz, const double* src, double2* spec, const double2* twx,
+                   const double2* post, int nsm, unsigned int* err) {
+    const int nrows = ny * nz;
+    switch (nx / 2) {
+#define X_CASE(n)                                                                                              \
+    case n:                                                                                                    \
+        launch_pdl(k_xf_tma<n>, dim3(xt_grid<n>(nrows, nsm)), dim3(XT<n>::P), XT<n>::smem, st, nrows, src, spec, \
+                   twx, post, err);                                                                            \
+        break;
+        XT_SIZES(X_CASE)
+#undef X_CASE
+        default: break;
+    }
+}
+
+}  // namespace ptc

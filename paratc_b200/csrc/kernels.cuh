@@ -101,6 +101,15 @@ bool zt_tma_prepare(double2* spec, int ncol, int nz, void* tmap_out);
 void launch_zt_tma(cudaStream_t st, int dir, int ncol, int nz, const void* tmap, const double2* twz, int nsm,
                    unsigned int* err);
 
+// k_pfft_xt.cu: x transforms fed by bulk copies (persistent CTAs, two stages);
+// row pointers must be 16-byte aligned
+bool xt_tma_supported(int n);
+void xt_tma_init();
+void launch_xb_tma(cudaStream_t st, int nx, int ny, int nz, const double2* spec, double* phi, const double2* twx,
+                   const double2* post, double scale, int padded, int nsm, unsigned int* err);
+void launch_xf_tma(cudaStream_t st, int nx, int ny, int nz, const double* src, double2* spec, const double2* twx,
+                   const double2* post, int nsm, unsigned int* err);
+
 // k_plane.cu: both transforms of a y-plane in one CTA (planes that fit shared memory)
 bool plane_supported(int nx, int nz);
 void plane_init();

@@ -1,7 +1,7 @@
 // tma.cuh -- the tensor-memory-accelerator (TMA) and mbarrier operations the
 // TMA-fed kernels use, as inline PTX: tiled 2-D / 3-D loads into shared
 // memory completing on an mbarrier, tiled stores from shared memory in bulk
-// groups, and bounded waits.  Only this GPU's memory; no cluster multicast.
+// groups, untiled bulk copies of contiguous runs, and bounded waits.  Only this GPU's memory; no cluster multicast.
 #pragma once
 #include <cuda.h>
 #include <cudaTypedefs.h>
@@ -59,6 +59,19 @@ __device__ __forceinline__ void store_3d(const CUtensorMap* tm, int x, int y, in
     asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.tile.bulk_group [%0, {%1, %2, %3}], [%4];\n" ::"l"(
                      reinterpret_cast<unsigned long long>(tm)),
                  "r"(x), "r"(y), "r"(z), "r"(smem_addr(src))
+                 : "memory");
+}
+// untiled bulk copies: both addresses 16-byte aligned, bytes a multiple of 16
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned bytes, unsigned long long* m) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                     smem_addr(dst)),
+                 "l"(reinterpret_cast<unsigned long long>(src)), "r"(bytes), "r"(smem_addr(m))
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_store(void* dst, const void* src, unsigned bytes) {
+    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;\n" ::"l"(
+                     reinterpret_cast<unsigned long long>(dst)),
+                 "r"(smem_addr(src)), "r"(bytes)
                  : "memory");
 }
 __device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
