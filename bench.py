@@ -47,7 +47,7 @@ def _args():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--schedule", type=int, default=-1,
-                    help="pin a Poisson schedule (0-5, paratc_set_schedule) instead of auto-tuning it")
+                    help="pin a Poisson schedule (0-9, paratc_set_schedule) instead of auto-tuning it")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64",
                     help="mixed: the explicit right-hand side in FP32 arithmetic, all else FP64")
     return ap.parse_args()
@@ -155,12 +155,13 @@ class ClockSampler:
 
 
 def _set_schedule(ctx, args):
-    """The Poisson schedule: auto-tuned (5 solves per choice) unless pinned."""
+    """The Poisson schedule: auto-tuned (5 solves per choice) unless pinned;
+    returns the choice and the tuner's ms per 5 solves (-1: unsupported)."""
     if args.schedule >= 0:
         ctx.schedule = args.schedule
-        return args.schedule
-    choice, _ = ctx.autotune(nrep=5)
-    return choice
+        return args.schedule, None
+    choice, times = ctx.autotune(nrep=5)
+    return choice, [round(float(t), 4) for t in times]
 
 
 def _dist():
@@ -245,7 +246,7 @@ def run_ours(args):
     ctx.set_fields(fields["ux"], fields["uy"], fields["uz"], fields["p"], fields["c"])
     ctx.project()
     # InitPoissonSolver's auto-tuning (src/m_Poisson.f90:50-175), before timing
-    schedule = _set_schedule(ctx, args)
+    schedule, tune_ms = _set_schedule(ctx, args)
     stream = torch.cuda.ExternalStream(ctx.stream, device=local)
     flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device=local)
     iad = {1: 1, 2: 2, 3: 3}[p.ischeme]
@@ -367,7 +368,7 @@ def run_ours(args):
                 "config": {"workload": case.name, "grid": [p.nxc, p.nyc, p.nzc], "scheme": "RK3",
                            "precision": args.precision, "parallelism": "replicas x%d" % ws,
                            "l2": "flushed between timed steps (256 MB write outside the events)",
-                           "divmax_last_step": diag.divmax, "poisson_schedule": schedule,
+                           "divmax_last_step": diag.divmax, "poisson_schedule": schedule, "autotune_ms": tune_ms,
                            "field_rel_err_vs_fp64_path": mixed_err},
                 "roofline": roof, "cpu_baseline": base, "e2e": e2e, "gpu_launches": launches, "clocks": clocks}
         print(json.dumps(line), flush=True)
@@ -503,7 +504,7 @@ def run_poisson(args):
     src = cases.gaussian_source(cases.Case("src", p, case.mesh, "gauss_src", 42 + rank, 1.0))
     cells = p.nxc * p.nyc * p.nzc
     ctx = ChannelSystem(p, yp, device=local)
-    schedule = _set_schedule(ctx, args)  # InitPoissonSolver's auto-tuning, before timing
+    schedule, tune_ms = _set_schedule(ctx, args)  # InitPoissonSolver's auto-tuning, before timing
     stream = torch.cuda.ExternalStream(ctx.stream, device=local)
     d_src = torch.from_numpy(src).to("cuda:%d" % local)
     d_phi = torch.empty_like(d_src)
@@ -557,7 +558,7 @@ def run_poisson(args):
                 "dtype": "f64", "data": "synthetic",
                 "config": {"workload": case.name, "grid": [p.nxc, p.nyc, p.nzc], "precision": "fp64",
                            "l2": "src and phi 537 MB each > L2, no flush",
-                           "max_rel_err_vs_oracle": err, "poisson_schedule": schedule, "mean_phi_e2e_equal": bool(np.array_equal(phi_h, phi_g))},
+                           "max_rel_err_vs_oracle": err, "poisson_schedule": schedule, "autotune_ms": tune_ms, "mean_phi_e2e_equal": bool(np.array_equal(phi_h, phi_g))},
                 "roofline": {"bound": "hbm", "kernel": "poisson solve (5 kernels)", "achieved": round(ach, 1),
                              "peak": peak, "unit": "GB/s", "frac": round(ach / peak, 4), "traffic": None,
                              "peak_kind": peak_kind, "algorithmic_bytes_per_launch": alg,

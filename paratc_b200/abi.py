@@ -22,6 +22,9 @@ AB2, RK2, RK3 = 1, 2, 3
 LAYOUT_INTERIOR = 0
 LAYOUT_HALO = 1
 
+# Poisson schedule choices (PARATC_SCHED_NCHOICES of include/paratc.h)
+SCHED_NCHOICES = 10
+
 # dump_visu quantities (PARATC_VISU_*)
 VISU_NAMES = ("ux", "uy", "uz", "pr", "wx", "wy", "wz", "wMag", "Q", "lamda2", "scalar")
 VISU = {n: q for q, n in enumerate(VISU_NAMES)}

@@ -156,11 +156,36 @@ __device__ __forceinline__ void dft(double2* v) {
     }
 }
 
+// barrier of the P threads that run the transform: the whole CTA (BAR = 0)
+// or named barrier BAR over the first P threads (warp-specialised kernels)
+template <int BAR, int P>
+__device__ __forceinline__ void group_sync() {
+    if constexpr (BAR == 0) __syncthreads();
+    else asm volatile("bar.sync %0, %1;\n" ::"n"(BAR), "n"(P) : "memory");
+}
+
+// barrier of the same group that also returns, to every thread, whether any
+// thread of the group passed a true predicate (a uniform decision)
+template <int BAR, int P>
+__device__ __forceinline__ bool group_any(bool pred) {
+    if constexpr (BAR == 0) {
+        return __syncthreads_or(pred ? 1 : 0) != 0;
+    } else {
+        unsigned r;
+        asm volatile(
+            "{\n .reg .pred p, q;\n setp.ne.u32 p, %1, 0;\n bar.red.or.pred q, %2, %3, p;\n selp.u32 %0, 1, 0, q;\n}\n"
+            : "=r"(r)
+            : "r"(pred ? 1u : 0u), "n"(BAR), "n"(P)
+            : "memory");
+        return r != 0;
+    }
+}
+
 // One Stockham pass of radix R (passes before it multiply to NS) over B
 // sequences of length N, P threads.  LD(e, b) loads element e of sequence b,
 // ST(e, b, v) stores it; SYNC_MID puts a block barrier between all loads and
 // all stores (an in-place pass on shared memory).  tw: exp(-2 pi i m / N).
-template <int N, int B, int P, int R, int NS, int DIR, bool SYNC_MID, class LD, class ST>
+template <int N, int B, int P, int R, int NS, int DIR, bool SYNC_MID, class LD, class ST, int BAR = 0>
 __device__ __forceinline__ void pass(const LD& ld, const ST& st, const double2* tw, int tid) {
     constexpr int NB = N / R;
     constexpr int TOT = B * NB;
@@ -188,7 +213,7 @@ __device__ __forceinline__ void pass(const LD& ld, const ST& st, const double2* 
             jb[u] = ((j - kk) * R + kk) * B + b;  // output element * B + b
         }
     }
-    if constexpr (SYNC_MID) __syncthreads();
+    if constexpr (SYNC_MID) group_sync<BAR, P>();
 #pragma unroll
     for (int u = 0; u < PER; u++) {
         if (TOT % P == 0 || jb[u] >= 0) {
@@ -225,19 +250,23 @@ struct SmemStT {
 };
 
 // passes S..END-1 in place on shared memory, each followed by a barrier;
-// TRANSPOSED selects the layout buf[b*PITCH + e] instead of buf[e*PITCH + b]
-template <int N, int B, int PITCH, int P, int DIR, int S, int END, int MAXBITS = 4, bool TRANSPOSED = false>
+// TRANSPOSED selects the layout buf[b*PITCH + e] instead of buf[e*PITCH + b];
+// BAR != 0 synchronises only the P transforming threads (named barrier BAR)
+template <int N, int B, int PITCH, int P, int DIR, int S, int END, int MAXBITS = 4, bool TRANSPOSED = false,
+          int BAR = 0>
 __device__ __forceinline__ void smem_passes(double2* buf, const double2* tw, int tid) {
     constexpr Sched SC = make_sched(N, MAXBITS);
     if constexpr (S < END) {
         constexpr int R = SC.r[S];
         constexpr int NS = sched_ns(N, S, MAXBITS);
         if constexpr (TRANSPOSED)
-            pass<N, B, P, R, NS, DIR, true>(SmemLdT<PITCH>{buf}, SmemStT<PITCH>{buf}, tw, tid);
+            pass<N, B, P, R, NS, DIR, true, SmemLdT<PITCH>, SmemStT<PITCH>, BAR>(SmemLdT<PITCH>{buf},
+                                                                               SmemStT<PITCH>{buf}, tw, tid);
         else
-            pass<N, B, P, R, NS, DIR, true>(SmemLd<PITCH>{buf}, SmemSt<PITCH>{buf}, tw, tid);
-        __syncthreads();
-        smem_passes<N, B, PITCH, P, DIR, S + 1, END, MAXBITS, TRANSPOSED>(buf, tw, tid);
+            pass<N, B, P, R, NS, DIR, true, SmemLd<PITCH>, SmemSt<PITCH>, BAR>(SmemLd<PITCH>{buf},
+                                                                             SmemSt<PITCH>{buf}, tw, tid);
+        group_sync<BAR, P>();
+        smem_passes<N, B, PITCH, P, DIR, S + 1, END, MAXBITS, TRANSPOSED, BAR>(buf, tw, tid);
     }
 }
 

@@ -20,10 +20,13 @@
 #include "common.cuh"
 #include "fft_fixed.cuh"
 #include "kernels.cuh"
+#include "div_src.cuh"
 #include "reduce.cuh"
 
 namespace ptc {
 namespace {
+
+constexpr int XF_DIV_U = 2;  // divergence point pairs in flight per thread
 
 __device__ __forceinline__ void cpa16(void* sdst, const void* gsrc) {
     const unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
@@ -54,7 +57,7 @@ __global__ void __launch_bounds__(XK<N>::P)
     double2* buf = smx;
     double2* tws = smx + (N + 1) * PITCH;
     const int tid = threadIdx.x;
-    const int nx = 2 * N, ny = c.ny, nz = c.nz, nrows = ny * nz;
+    const int nx = 2 * N, nrows = c.ny * c.nz;
     const int g0 = blockIdx.x * B;
     for (int t = tid; t < N; t += P) tws[t] = twN[t];
     pdl_wait();
@@ -70,40 +73,8 @@ __global__ void __launch_bounds__(XK<N>::P)
         cpa_wait_all();
     } else {
         const double sudtal = (mode == 0) ? 1.0 / coef->pmAlpha : 1.0;
-        const size_t pl = (size_t)c.nyt * nx;
-#pragma unroll 2
-        for (int f = tid; f < B * N; f += P) {
-            const int b = f / N, e = f - b * N;
-            const int g = g0 + b;
-            double2 val = make_double2(0.0, 0.0);
-            if (g < nrows) {
-                const int k = g / ny, jc = g - k * ny + 1;
-                const int km = k == 0 ? nz - 1 : k - 1, kp = k == nz - 1 ? 0 : k + 1, ku = kp == nz - 1 ? 0 : kp + 1;
-                const int i0 = 2 * e, im = i0 == 0 ? nx - 1 : i0 - 1, i2 = i0 + 2 == nx ? 0 : i0 + 2;
-                const size_t r0 = (size_t)jc * nx;
-                const double* ur = ux + (size_t)k * pl + r0;
-                const double* vr = uy + (size_t)k * pl + r0;
-                const double2 u01 = __ldg(reinterpret_cast<const double2*>(ur + i0));
-                const double2 u23 = __ldg(reinterpret_cast<const double2*>(ur + i2));
-                const double um = __ldg(ur + im);
-                const double2 v0 = __ldg(reinterpret_cast<const double2*>(vr + i0));
-                const double2 v1 = __ldg(reinterpret_cast<const double2*>(vr + nx + i0));
-                const double2 w0 = __ldg(reinterpret_cast<const double2*>(uz + (size_t)km * pl + r0 + i0));
-                const double2 w1 = __ldg(reinterpret_cast<const double2*>(uz + (size_t)k * pl + r0 + i0));
-                const double2 w2 = __ldg(reinterpret_cast<const double2*>(uz + (size_t)kp * pl + r0 + i0));
-                const double2 w3 = __ldg(reinterpret_cast<const double2*>(uz + (size_t)ku * pl + r0 + i0));
-                const double rdyp = __ldg(&m.rdyp[jc]);
-                const double dudx0 = c.dxC[0] * um + c.dxC[1] * u01.x + c.dxC[2] * u01.y + c.dxC[3] * u23.x;
-                const double dudx1 = c.dxC[0] * u01.x + c.dxC[1] * u01.y + c.dxC[2] * u23.x + c.dxC[3] * u23.y;
-                const double dvdy0 = (v1.x - v0.x) * rdyp, dvdy1 = (v1.y - v0.y) * rdyp;
-                const double dwdz0 = c.dzC[0] * w0.x + c.dzC[1] * w1.x + c.dzC[2] * w2.x + c.dzC[3] * w3.x;
-                const double dwdz1 = c.dzC[0] * w0.y + c.dzC[1] * w1.y + c.dzC[2] * w2.y + c.dzC[3] * w3.y;
-                const double d0 = dudx0 + dvdy0 + dwdz0, d1 = dudx1 + dvdy1 + dwdz1;
-                dm = fmax(dm, fmax(fabs(d0), fabs(d1)));
-                val = make_double2(sudtal * d0, sudtal * d1);
-            }
-            buf[e * PITCH + b] = val;
-        }
+        div_batch<N, B, P, XF_DIV_U>(c, m, ux, uy, uz, g0, nrows, sudtal, tid, dm,
+                                     [&](int b, int e, double2 v) { buf[e * PITCH + b] = v; });
     }
     __syncthreads();
     ff::smem_passes<N, B, PITCH, P, -1, 0, SC.np>(buf, tws, tid);

@@ -21,6 +21,8 @@
 #include "common.cuh"
 #include "fft_fixed.cuh"
 #include "kernels.cuh"
+#include "div_src.cuh"
+#include "reduce.cuh"
 #include "tma.cuh"
 
 namespace ptc {
@@ -98,9 +100,13 @@ __global__ void __launch_bounds__(XT<N>::P)
     for (int bt = blockIdx.x; bt < nb; bt += gridDim.x, it++) {
         const int s = it & 1;
         double2* buf = stage[s];
-        if (!tma::mbar_wait(&mbar[s], (unsigned)((it >> 1) & 1))) s_bad = 1;
-        __syncthreads();
-        if (s_bad) break;
+        // one decision for the whole CTA: a flag read after a plain barrier
+        // could be set by a faster thread's next wait before a slower one
+        // reads it, and the two would then part at the next barrier
+        if (__syncthreads_or(tma::mbar_wait(&mbar[s], (unsigned)((it >> 1) & 1)) ? 0 : 1)) {
+            s_bad = 1;
+            break;
+        }
         // merge modes a and N-a of every row into z[a], z[N-a] (the DC and
         // Nyquist coefficients are real), scaled by 1/(nx*nz)
         for (int f = tid; f < B * (N / 2 + 1); f += P) {
@@ -194,9 +200,13 @@ __global__ void __launch_bounds__(XT<N>::P)
     for (int bt = blockIdx.x; bt < nb; bt += gridDim.x, it++) {
         const int s = it & 1;
         double2* buf = stage[s];
-        if (!tma::mbar_wait(&mbar[s], (unsigned)((it >> 1) & 1))) s_bad = 1;
-        __syncthreads();
-        if (s_bad) break;
+        // one decision for the whole CTA: a flag read after a plain barrier
+        // could be set by a faster thread's next wait before a slower one
+        // reads it, and the two would then part at the next barrier
+        if (__syncthreads_or(tma::mbar_wait(&mbar[s], (unsigned)((it >> 1) & 1)) ? 0 : 1)) {
+            s_bad = 1;
+            break;
+        }
         ff::smem_passes<N, B, PITCH, P, -1, 0, SC.np, 4, true>(buf, twN, tid);
         // split the packed transform into the nx/2+1 modes, in place: one
         // thread takes the pair (a, N-a) (and a = 0 also writes mode N)
@@ -240,6 +250,148 @@ __global__ void __launch_bounds__(XT<N>::P)
     }
 }
 
+// ---------------------------------------------------------------------------
+// Forward transform of the divergence source (clcPrSrc, src/m_TScheme.f90:
+// 48-77: scaled by 1/pmAlpha in mode 0, unscaled in mode 1, max|div| reduced
+// over the grid by the last CTA), warp-specialised: XD_Q producer threads
+// compute the divergence of the next batch's rows from u, v, w into one
+// stage while the P consumer threads transform the other stage, split it
+// into the nx/2+1 modes and send the spectrum rows out by bulk stores.
+// Stages change hands through mbarriers: full[s] (the producers' arrivals,
+// release) and empty[s] (consumer thread 0, once the stores have read the
+// stage).  The consumers synchronise among themselves on named barrier 1,
+// the producers on named barrier 2; a group decides to stop on a barrier
+// that reduces the predicate, so all its threads decide alike.  Every wait is
+// bounded; a group that gives up leaves its loop, the other group's waits
+// then run out too, and the CTA records *err |= 4.
+// ---------------------------------------------------------------------------
+constexpr int XD_Q = 256;      // producer threads
+constexpr int XD_DIV_U = 2;    // divergence point pairs in flight per producer thread
+
+template <int N>
+struct XD {
+    static constexpr int RMAX = ff::Shape<N>::RMAX;
+    // rows per batch: the transform's batch, doubled until its thread count
+    // is whole warps (named barriers count warps)
+    static constexpr int bcalc() {
+        int b = ff::Shape<N>::B;
+        while ((b * N / RMAX) % 32 != 0 && b < 64) b *= 2;
+        return b;
+    }
+    static constexpr int B = bcalc();
+    static constexpr int P = B * N / RMAX;
+    static constexpr int pitch() {
+        const int want = B >= 8 ? 1 : 8 / B;
+        int p = N + 1;
+        while (B > 1 && p % 8 != want % 8) p++;
+        return p;
+    }
+    static constexpr int PITCH = pitch();
+    static constexpr unsigned STAGE = (unsigned)B * PITCH;
+    static constexpr int NT = P + XD_Q;
+    static constexpr size_t smem = 2 * (size_t)STAGE * sizeof(double2);
+};
+
+template <int N>
+__global__ void __launch_bounds__(XD<N>::NT, 1)
+    k_xf_div(int mode, DConst c, DMetric m, const DCoef* __restrict__ coef, const double* __restrict__ ux,
+             const double* __restrict__ uy, const double* __restrict__ uz, double2* __restrict__ spec,
+             const double2* __restrict__ twN, const double2* __restrict__ post, double* __restrict__ part,
+             unsigned int* __restrict__ counter, double* __restrict__ out_max, unsigned int* __restrict__ err) {
+    constexpr int B = XD<N>::B, P = XD<N>::P, PITCH = XD<N>::PITCH, M1 = N + 1, Q = XD_Q;
+    static_assert(P % 32 == 0, "the consumer group is whole warps");
+    constexpr unsigned SB = XD<N>::STAGE;
+    constexpr ff::Sched SC = ff::make_sched(N);
+    extern __shared__ __align__(128) unsigned char smraw[];
+    double2* stage[2] = {reinterpret_cast<double2*>(smraw), reinterpret_cast<double2*>(smraw) + SB};
+    __shared__ unsigned long long full[2], empty[2];
+    __shared__ int bad_c, bad_p;
+    const int tid = threadIdx.x;
+    const int nrows = c.ny * c.nz;
+    const int nb = (nrows + B - 1) / B;
+    if (tid == 0) {
+        tma::mbar_init(&full[0], Q);
+        tma::mbar_init(&full[1], Q);
+        tma::mbar_init(&empty[0], 1);
+        tma::mbar_init(&empty[1], 1);
+        tma::fence_mbar_init();
+        bad_c = bad_p = 0;
+    }
+    __syncthreads();
+    pdl_wait();  // u* is written by the kernel before this one
+    pdl_trigger();
+    double dm = 0.0;
+    if (tid >= P) {
+        // producers
+        const int tp = tid - P;
+        const double sudtal = (mode == 0) ? 1.0 / coef->pmAlpha : 1.0;
+        int it = 0;
+        for (int bt = blockIdx.x; bt < nb; bt += gridDim.x, it++) {
+            const int s = it & 1;
+            const bool ok = it < 2 || tma::mbar_wait(&empty[s], (unsigned)(((it >> 1) + 1) & 1));
+            if (ff::group_any<2, Q>(!ok)) {
+                bad_p = 1;
+                break;
+            }
+            double2* buf = stage[s];
+            div_batch<N, B, Q, XD_DIV_U>(c, m, ux, uy, uz, bt * B, nrows, sudtal, tp, dm,
+                                         [&](int b, int e, double2 v) { buf[b * PITCH + e] = v; });
+            tma::mbar_arrive(&full[s]);
+        }
+    } else {
+        // consumers
+        int it = 0;
+        for (int bt = blockIdx.x; bt < nb; bt += gridDim.x, it++) {
+            const int s = it & 1;
+            double2* buf = stage[s];
+            if (ff::group_any<1, P>(!tma::mbar_wait(&full[s], (unsigned)((it >> 1) & 1)))) {
+                bad_c = 1;
+                break;
+            }
+            ff::smem_passes<N, B, PITCH, P, -1, 0, SC.np, 4, true, 1>(buf, twN, tid);
+            for (int f = tid; f < B * (N / 2 + 1); f += P) {
+                const int a = f / B, b = f - a * B;
+                const int bn = N - a;
+                double2* rb = buf + b * PITCH;
+                const double2 za = rb[a], zb = rb[a == 0 ? 0 : bn];
+                const double2 E = make_double2(0.5 * (za.x + zb.x), 0.5 * (za.y - zb.y));
+                const double2 O = make_double2(0.5 * (za.y + zb.y), -0.5 * (za.x - zb.x));
+                const double2 xa = cadd(E, cmul(__ldg(&post[a]), O));
+                if (a == 0) {
+                    rb[0] = xa;
+                    rb[N] = cadd(E, cmul(__ldg(&post[N]), O));
+                } else if (bn != a) {
+                    const double2 E2 = make_double2(0.5 * (zb.x + za.x), 0.5 * (zb.y - za.y));
+                    const double2 O2 = make_double2(0.5 * (zb.y + za.y), -0.5 * (zb.x - za.x));
+                    rb[a] = xa;
+                    rb[bn] = cadd(E2, cmul(__ldg(&post[bn]), O2));
+                } else {
+                    rb[a] = xa;
+                }
+            }
+            tma::fence_async_smem();
+            ff::group_sync<1, P>();
+            if (tid == 0) {
+                const int g0 = bt * B, nv = min(B, nrows - g0);
+                for (int b = 0; b < nv; b++)
+                    tma::bulk_store(spec + (size_t)(g0 + b) * M1, buf + b * PITCH, M1 * (unsigned)sizeof(double2));
+                tma::bulk_commit();
+                tma::bulk_wait_read0();  // the stores have read the stage
+                tma::mbar_arrive(&empty[s]);
+            }
+        }
+        if (tid == 0) tma::bulk_wait0();
+    }
+    __syncthreads();
+    if (tid == 0 && (bad_c | bad_p)) atomicOr(err, 4u);
+    double v[1] = {dm};
+    block_max_store<1>(v, part + blockIdx.x);
+    if (!last_block_arrive(counter, gridDim.x)) return;
+    double tot[1];
+    reduce_records<1, true>(part, (int)gridDim.x, tot);
+    if (tid == 0) *out_max = tot[0];
+}
+
 #define XT_SIZES(X) X(8) X(12) X(16) X(24) X(32) X(40) X(48) X(64) X(96) X(128) X(192) X(256) X(384) X(512) \
     X(768) X(1024) X(1152) X(1536)
 
@@ -266,7 +418,8 @@ bool xt_tma_supported(int n) {
 void xt_tma_init() {
 #define X_CASE(n)                                                                                              \
     cudaFuncSetAttribute(k_xb_tma<n>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)XT<n>::smem);          \
-    cudaFuncSetAttribute(k_xf_tma<n>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)XT<n>::smem);
+    cudaFuncSetAttribute(k_xf_tma<n>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)XT<n>::smem);       \
+    cudaFuncSetAttribute(k_xf_div<n>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)XD<n>::smem);
     XT_SIZES(X_CASE)
 #undef X_CASE
 }
@@ -294,6 +447,37 @@ void launch_xf_tma(cudaStream_t st, int nx, int ny, int nz, const double* src, d
     case n:                                                                                                    \
         launch_pdl(k_xf_tma<n>, dim3(xt_grid<n>(nrows, nsm)), dim3(XT<n>::P), XT<n>::smem, st, nrows, src, spec, \
                    twx, post, err);                                                                            \
+        break;
+        XT_SIZES(X_CASE)
+#undef X_CASE
+        default: break;
+    }
+}
+
+// one CTA per SM (the producers' loads and the consumers' transforms share
+// it), at most one batch per CTA
+int xf_div_grid(int n, int nrows, int nsm) {
+    int b = 1;
+    switch (n) {
+#define X_CASE(n) case n: b = XD<n>::B; break;
+        XT_SIZES(X_CASE)
+#undef X_CASE
+        default: break;
+    }
+    const int nb = (nrows + b - 1) / b;
+    return nb < nsm ? nb : nsm;
+}
+
+void launch_xf_div(cudaStream_t st, int mode, const DConst& c, const DMetric& m, const DCoef* coef, const Fields& f,
+                   double2* spec, const double2* twx, const double2* post, double* part, unsigned int* counter,
+                   double* out_max, unsigned int* err) {
+    const int nrows = c.ny * c.nz;
+    const int grid = xf_div_grid(c.nx / 2, nrows, c.nsm > 0 ? c.nsm : 148);
+    switch (c.nx / 2) {
+#define X_CASE(n)                                                                                              \
+    case n:                                                                                                    \
+        launch_pdl(k_xf_div<n>, dim3(grid), dim3(XD<n>::NT), XD<n>::smem, st, mode, c, m, coef, f.ux, f.uy, f.uz, \
+                   spec, twx, post, part, counter, out_max, err);                                              \
         break;
         XT_SIZES(X_CASE)
 #undef X_CASE

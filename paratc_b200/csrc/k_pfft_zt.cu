@@ -74,9 +74,13 @@ __global__ void __launch_bounds__(ZT<N>::P) k_zt_tma(const __grid_constant__ CUt
     for (int b = blockIdx.x; b < nb; b += gridDim.x, it++) {
         const int s = it & 1;
         double2* buf = stage[s];
-        if (!tma::mbar_wait(&mbar[s], (unsigned)((it >> 1) & 1))) s_bad = 1;
-        __syncthreads();
-        if (s_bad) break;
+        // one decision for the whole CTA: a flag read after a plain barrier
+        // could be set by a faster thread's next wait before a slower one
+        // reads it, and the two would then part at the next barrier
+        if (__syncthreads_or(tma::mbar_wait(&mbar[s], (unsigned)((it >> 1) & 1)) ? 0 : 1)) {
+            s_bad = 1;
+            break;
+        }
         ff::smem_passes<N, B, B, P, DIR, 0, SC.np>(buf, tws, tid);
         tma::fence_async_smem();
         __syncthreads();

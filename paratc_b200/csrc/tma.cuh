@@ -21,6 +21,11 @@ __device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier
 __device__ __forceinline__ void mbar_expect_tx(unsigned long long* m, unsigned bytes) {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_addr(m)), "r"(bytes) : "memory");
 }
+// one arrival (release at CTA scope: the arriving thread's shared-memory
+// writes are visible to a thread whose wait sees the phase complete)
+__device__ __forceinline__ void mbar_arrive(unsigned long long* m) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_addr(m)) : "memory");
+}
 // true once phase `parity` of the barrier has completed; false after the spin limit
 __device__ __forceinline__ bool mbar_wait(unsigned long long* m, unsigned parity) {
     const unsigned a = smem_addr(m);

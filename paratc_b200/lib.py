@@ -12,7 +12,7 @@ import os
 
 import numpy as np
 
-from .abi import (LAYOUT_INTERIOR, VISU, VISU_NAMES, ParatcIoOptions, PARATC_ERR_DIV_LIMIT, PARATC_ERR_VEL_LIMIT, PARATC_OK, ParatcDiag,
+from .abi import (LAYOUT_INTERIOR, SCHED_NCHOICES, VISU, VISU_NAMES, ParatcIoOptions, PARATC_ERR_DIV_LIMIT, PARATC_ERR_VEL_LIMIT, PARATC_OK, ParatcDiag,
                   ParatcParams)
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
@@ -455,7 +455,7 @@ class ChannelSystem:
         """Times every supported schedule and keeps the fastest: (choice, ms
         for nrep solves per choice, -1 where unsupported)."""
         ch = ctypes.c_int()
-        t = np.zeros(8)
+        t = np.zeros(SCHED_NCHOICES)
         self._check(self._L.paratc_autotune(self._h, int(nrep), ctypes.byref(ch), _ptr(t)), "paratc_autotune")
         return ch.value, t
 

@@ -32,6 +32,15 @@ def test_library_exports_every_declared_symbol():
     assert set(lib.EXPORTED) <= set(names)
 
 
+def test_header_constants_match_python():
+    # the #define PARATC_* integers that the Python side mirrors
+    hdr = open(os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include", "paratc.h")).read()
+    defs = dict(re.findall(r"#define\s+(PARATC_\w+)\s+(-?\d+)", hdr))
+    assert int(defs["PARATC_SCHED_NCHOICES"]) == abi.SCHED_NCHOICES
+    for n in ("PARATC_OK", "PARATC_ERR_BAD_ARG", "PARATC_ERR_TIMEOUT", "PARATC_ERR_NUMERIC"):
+        assert int(defs[n]) == getattr(abi, n), n
+
+
 def test_header_structs_match_ctypes():
     # offsets that a C compiler gives the structs, checked with a tiny probe
     assert ctypes.sizeof(abi.ParatcParams) % 8 == 0

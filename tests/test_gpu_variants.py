@@ -12,6 +12,7 @@ import pytest
 
 from oracle import oracle_lib as ol
 from paratc_b200 import cases
+from paratc_b200.abi import SCHED_NCHOICES
 from paratc_b200.lib import ChannelSystem
 
 from .helpers import fields_of, rel_err, variant, yp_of
@@ -102,7 +103,8 @@ def test_plane_and_split_transforms(monkeypatch, plane, dims):
 def test_schedules_and_autotune(dims):
     """Every Poisson schedule this grid supports (fused plane transforms,
     separate fixed-length transforms, generic transforms, separate transforms
-    with TMA-fed z passes; staged or streaming y-solve) gives the oracle's
+    with TMA-fed z passes, the same with the warp-specialised divergence
+    source of the x transform; staged or streaming y-solve) gives the oracle's
     fields after two steps; the auto-tuner times all of them and keeps the
     fastest."""
     case = cases.small_channel(*dims)
@@ -117,10 +119,12 @@ def test_schedules_and_autotune(dims):
     choice, times = g.autotune(nrep=3)
     assert times[choice] > 0 and times[choice] == min(t for t in times if t > 0)
     assert g.schedule == choice
-    supported = [c for c in range(8) if times[c] > 0]
+    assert len(times) == SCHED_NCHOICES
+    supported = [c for c in range(SCHED_NCHOICES) if times[c] > 0]
     assert 4 in supported and 5 in supported  # the generic transforms take any 2^a 3^b 5^c size
-    assert (6 in supported) == (dims[2] in (128, 256, 512, 768, 1024))
-    for c in range(8):
+    tma_z = dims[2] in (128, 256, 512, 768, 1024)
+    assert (6 in supported) == tma_z and (8 in supported) == tma_z and (9 in supported) == tma_z
+    for c in range(SCHED_NCHOICES):
         if c not in supported:
             with pytest.raises(Exception):
                 g.schedule = c
