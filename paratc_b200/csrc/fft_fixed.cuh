@@ -237,36 +237,46 @@ struct SmemSt {
 };
 
 // shared-memory accessors with the sequence index major: element e of
-// sequence b at buf[b*PITCH + e]
-template <int PITCH>
+// sequence b at buf[b*PITCH + e], or at buf[b*PITCH + swz8(e)] with SWZ:
+// swz8(e) = e ^ ((e >> 3) & 7) permutes each aligned group of eight 16-byte
+// words, so that the stores of a first Stockham pass (element j*R + r for
+// the lanes' consecutive j, all in one bank group when R is 8 or 16) and the
+// loads of the next one both spread over the eight bank groups
+__device__ __forceinline__ int swz8(int e) { return e ^ ((e >> 3) & 7); }
+template <int PITCH, bool SWZ = false>
 struct SmemLdT {
     const double2* buf;
-    __device__ __forceinline__ double2 operator()(int e, int b) const { return buf[b * PITCH + e]; }
+    __device__ __forceinline__ double2 operator()(int e, int b) const { return buf[b * PITCH + (SWZ ? swz8(e) : e)]; }
 };
-template <int PITCH>
+template <int PITCH, bool SWZ = false>
 struct SmemStT {
     double2* buf;
-    __device__ __forceinline__ void operator()(int e, int b, double2 v) const { buf[b * PITCH + e] = v; }
+    __device__ __forceinline__ void operator()(int e, int b, double2 v) const { buf[b * PITCH + (SWZ ? swz8(e) : e)] = v; }
 };
 
 // passes S..END-1 in place on shared memory, each followed by a barrier;
 // TRANSPOSED selects the layout buf[b*PITCH + e] instead of buf[e*PITCH + b];
-// BAR != 0 synchronises only the P transforming threads (named barrier BAR)
+// BAR != 0 synchronises only the P transforming threads (named barrier BAR);
+// SWZ (TRANSPOSED, N a multiple of 8) keeps the values between passes in the
+// swizzled order: pass 0 reads plain and writes swizzled, the last pass
+// reads swizzled and writes plain
 template <int N, int B, int PITCH, int P, int DIR, int S, int END, int MAXBITS = 4, bool TRANSPOSED = false,
-          int BAR = 0>
+          int BAR = 0, bool SWZ = false>
 __device__ __forceinline__ void smem_passes(double2* buf, const double2* tw, int tid) {
     constexpr Sched SC = make_sched(N, MAXBITS);
+    static_assert(!SWZ || (TRANSPOSED && N % 8 == 0), "the swizzle permutes whole groups of eight");
     if constexpr (S < END) {
         constexpr int R = SC.r[S];
         constexpr int NS = sched_ns(N, S, MAXBITS);
+        constexpr bool SIN = SWZ && S > 0, SOUT = SWZ && S + 1 < END;
         if constexpr (TRANSPOSED)
-            pass<N, B, P, R, NS, DIR, true, SmemLdT<PITCH>, SmemStT<PITCH>, BAR>(SmemLdT<PITCH>{buf},
-                                                                               SmemStT<PITCH>{buf}, tw, tid);
+            pass<N, B, P, R, NS, DIR, true, SmemLdT<PITCH, SIN>, SmemStT<PITCH, SOUT>, BAR>(
+                SmemLdT<PITCH, SIN>{buf}, SmemStT<PITCH, SOUT>{buf}, tw, tid);
         else
             pass<N, B, P, R, NS, DIR, true, SmemLd<PITCH>, SmemSt<PITCH>, BAR>(SmemLd<PITCH>{buf},
                                                                              SmemSt<PITCH>{buf}, tw, tid);
         group_sync<BAR, P>();
-        smem_passes<N, B, PITCH, P, DIR, S + 1, END, MAXBITS, TRANSPOSED, BAR>(buf, tw, tid);
+        smem_passes<N, B, PITCH, P, DIR, S + 1, END, MAXBITS, TRANSPOSED, BAR, SWZ>(buf, tw, tid);
     }
 }
 

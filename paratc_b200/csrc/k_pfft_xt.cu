@@ -45,6 +45,18 @@ struct XT {
     static constexpr int PITCH = pitch();
     static constexpr unsigned STAGE = (unsigned)B * PITCH;  // complex values per stage
     static constexpr size_t smem = 2 * (size_t)STAGE * sizeof(double2);
+    // resident CTAs that the shared memory allows: the register target of
+    // the launch bounds (without it k_xb_tma<1152> takes 236 registers and
+    // runs one CTA per SM: 0.28 of peak against 0.39)
+    static constexpr int mcalc() {
+        const int m = (int)((220 * 1024) / (smem + 1024));
+        return m < 1 ? 1 : (m > 8 ? 8 : m);
+    }
+    static constexpr int MINB = mcalc();
+    // between passes the rows are kept in the swizzled order (fft_fixed.cuh):
+    // with 1 or 2 rows per batch, a first pass's stores otherwise fall in one
+    // bank group
+    static constexpr bool SWZ = N % 8 == 0;
 };
 
 // whether the CTA's iteration i has a batch (and so a load was issued for it)
@@ -63,7 +75,7 @@ __device__ __forceinline__ void xt_fail(unsigned long long* mbar, int it, int nb
 }
 
 template <int N>
-__global__ void __launch_bounds__(XT<N>::P)
+__global__ void __launch_bounds__(XT<N>::P, XT<N>::MINB)
     k_xb_tma(int nrows, int ny, const double2* __restrict__ spec, double* __restrict__ phi,
              const double2* __restrict__ twN, const double2* __restrict__ post, double scale, int padded,
              unsigned int* __restrict__ err) {
@@ -130,7 +142,7 @@ __global__ void __launch_bounds__(XT<N>::P)
             }
         }
         __syncthreads();
-        ff::smem_passes<N, B, PITCH, P, 1, 0, SC.np, 4, true>(buf, twN, tid);
+        ff::smem_passes<N, B, PITCH, P, 1, 0, SC.np, 4, true, 0, XT<N>::SWZ>(buf, twN, tid);
         tma::fence_async_smem();
         __syncthreads();
         if (tid == 0) {
@@ -164,7 +176,7 @@ __global__ void __launch_bounds__(XT<N>::P)
 }
 
 template <int N>
-__global__ void __launch_bounds__(XT<N>::P)
+__global__ void __launch_bounds__(XT<N>::P, XT<N>::MINB)
     k_xf_tma(int nrows, const double* __restrict__ src, double2* __restrict__ spec, const double2* __restrict__ twN,
              const double2* __restrict__ post, unsigned int* __restrict__ err) {
     constexpr int B = XT<N>::B, P = XT<N>::P, PITCH = XT<N>::PITCH, M1 = N + 1;
@@ -207,7 +219,7 @@ __global__ void __launch_bounds__(XT<N>::P)
             s_bad = 1;
             break;
         }
-        ff::smem_passes<N, B, PITCH, P, -1, 0, SC.np, 4, true>(buf, twN, tid);
+        ff::smem_passes<N, B, PITCH, P, -1, 0, SC.np, 4, true, 0, XT<N>::SWZ>(buf, twN, tid);
         // split the packed transform into the nx/2+1 modes, in place: one
         // thread takes the pair (a, N-a) (and a = 0 also writes mode N)
         for (int f = tid; f < B * (N / 2 + 1); f += P) {
