@@ -320,9 +320,10 @@ int paratc_get_precision(paratc_ctx* ctx, int* prec);
  * one CTA), 1 separate compile-time-length x and z transforms, 2 generic
  * mixed-radix transforms (any 2^a 3^b 5^c size), 3 as 1 with the z
  * transforms fed by TMA (persistent CTAs, two shared-memory stages; nz in
- * 128, 256, 512, 768, 1024), 4 as 3 with the divergence source computed by
+ * 128, 256, 512, 768, 1024), 4 as 1 with the divergence source computed by
  * producer warps into the stages of the forward x transform
- * (warp-specialised, one CTA per SM); y = 0 staged (one-warp CTAs, cp.async
+ * (warp-specialised, one CTA per SM), 5 as 4 with the z transforms of 3;
+ * y = 0 staged (one-warp CTAs, cp.async
  * row staging), 1 streaming (a thread per column) spectral y-solve.  The x
  * transforms of the separate-transform schedules are fed by bulk copies
  * where the rows are 16-byte aligned.
@@ -334,7 +335,7 @@ int paratc_get_precision(paratc_ctx* ctx, int* prec);
  * for nrep solves, -1 where unsupported) to
  * times_ms[PARATC_SCHED_NCHOICES] (may be NULL) and keeps the fastest.  All
  * choices solve the same system; results differ by rounding only. */
-#define PARATC_SCHED_NCHOICES 10
+#define PARATC_SCHED_NCHOICES 12
 int paratc_autotune(paratc_ctx* ctx, int nrep, int* choice, double* times_ms);
 int paratc_get_schedule(paratc_ctx* ctx, int* choice);
 /* pin a choice (PARATC_ERR_BAD_ARG when this grid has no such kernels) */

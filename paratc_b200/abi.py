@@ -23,7 +23,7 @@ LAYOUT_INTERIOR = 0
 LAYOUT_HALO = 1
 
 # Poisson schedule choices (PARATC_SCHED_NCHOICES of include/paratc.h)
-SCHED_NCHOICES = 10
+SCHED_NCHOICES = 12
 
 # dump_visu quantities (PARATC_VISU_*)
 VISU_NAMES = ("ux", "uy", "uz", "pr", "wx", "wy", "wz", "wMag", "Q", "lamda2", "scalar")

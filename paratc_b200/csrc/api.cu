@@ -870,23 +870,24 @@ static bool sched_supported(const paratc_ctx* ctx, int choice) {
     if (sc == 0) return pfft_ok && plane_supported(ctx->nx, ctx->nz);
     if (sc == 1) return pfft_ok;
     if (sc == 3) return pfft_ok && ctx->ztma_ok;
-    if (sc == 4) return pfft_ok && ctx->ztma_ok && ctx->xtma;
+    if (sc == 4) return pfft_ok && ctx->xtma;
+    if (sc == 5) return pfft_ok && ctx->ztma_ok && ctx->xtma;
     return true;
 }
 
 static void sched_apply(paratc_ctx* ctx, int choice) {
     const int sc = choice / 2;
     ctx->plane = sc == 0;
-    ctx->pfft = sc == 0 || sc == 1 || sc == 3 || sc == 4;
-    ctx->ztma = sc == 3 || sc == 4;
-    ctx->xdiv = sc == 4;
+    ctx->pfft = sc == 0 || sc == 1 || sc >= 3;
+    ctx->ztma = sc == 3 || sc == 5;
+    ctx->xdiv = sc == 4 || sc == 5;
     ctx->kc.solver_sel = choice % 2 + 1;
     ctx->sched_gen++;
 }
 
 int paratc_get_schedule(paratc_ctx* ctx, int* choice) {
     if (!ctx || !choice) return PARATC_ERR_BAD_ARG;
-    const int sc = ctx->plane ? 0 : (ctx->xdiv ? 4 : (ctx->ztma ? 3 : (ctx->pfft ? 1 : 2)));
+    const int sc = ctx->plane ? 0 : (ctx->xdiv ? (ctx->ztma ? 5 : 4) : (ctx->ztma ? 3 : (ctx->pfft ? 1 : 2)));
     *choice = 2 * sc + (ctx->kc.solver_sel == 2 ? 1 : 0);
     return PARATC_OK;
 }

@@ -360,7 +360,7 @@ __global__ void __launch_bounds__(XD<N>::NT, 1)
                 bad_c = 1;
                 break;
             }
-            ff::smem_passes<N, B, PITCH, P, -1, 0, SC.np, 4, true, 1>(buf, twN, tid);
+            ff::smem_passes<N, B, PITCH, P, -1, 0, SC.np, 4, true, 1, N % 8 == 0>(buf, twN, tid);
             for (int f = tid; f < B * (N / 2 + 1); f += P) {
                 const int a = f / B, b = f - a * B;
                 const int bn = N - a;
