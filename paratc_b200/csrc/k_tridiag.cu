@@ -168,7 +168,7 @@ __host__ __device__ inline int helm_stride(int ny) { return 3 * (ny + 2); }
 // memory; rows are addressed by pointer steps; the wall rows need no case of
 // their own in the sweeps (a(1) = 0, arr(ny+1) = 0, and clcU2Hat's row-1
 // value is substituted before the sweep and its result after it).
-__global__ void __launch_bounds__(128) k_helm(DConst cst, const DCoef* __restrict__ coef, int comp0, Fields fl,
+__global__ void __launch_bounds__(128, 4) k_helm(DConst cst, const DCoef* __restrict__ coef, int comp0, Fields fl,
                                               const double* __restrict__ duy_ym, const double* __restrict__ uy_ym,
                                               const double* __restrict__ facs) {
     extern __shared__ double shf[];
