@@ -21,9 +21,15 @@
 namespace ptc {
 namespace {
 
-template <int N>
+// W = 1: the wide batch (8 columns) for nz = 512 and 768 on large spectra.
+// A batch reads one run of 2B doubles from every one of the nz rows; when
+// those rows span more than 1 GB, runs of 64 B per row leave the copies bound
+// by address translation (nz = 768: 0.36 of peak at 2304 x 192 x 768, 2.7 GB;
+// 0.79 at 512 x 96 x 768), and 128 B per row restores them (0.71) at one CTA
+// per SM.
+template <int N, int W = 0>
 struct ZT {
-    static constexpr int B = ff::Shape<N>::B < 4 ? 4 : ff::Shape<N>::B;
+    static constexpr int B = (W && (N == 512 || N == 768)) ? 8 : (ff::Shape<N>::B < 4 ? 4 : ff::Shape<N>::B);
     static constexpr int P = B * N / ff::Shape<N>::RMAX;
     static constexpr int ROWS = N < 256 ? N : 256;  // TMA box rows (at most 256)
     static constexpr int NBOX = N / ROWS;
@@ -36,11 +42,11 @@ __device__ __forceinline__ bool b_first_unused(int i, int nb) {
     return (long long)blockIdx.x + (long long)i * gridDim.x < nb;
 }
 
-template <int N, int DIR>
-__global__ void __launch_bounds__(ZT<N>::P) k_zt_tma(const __grid_constant__ CUtensorMap tm, int nb,
-                                                       const double2* __restrict__ twN, unsigned int* __restrict__ err) {
-    constexpr int B = ZT<N>::B, P = ZT<N>::P, ROWS = ZT<N>::ROWS, NBOX = ZT<N>::NBOX;
-    constexpr unsigned SB = ZT<N>::STAGE_BYTES;
+template <int N, int DIR, int W>
+__global__ void __launch_bounds__(ZT<N, W>::P) k_zt_tma(const __grid_constant__ CUtensorMap tm, int nb,
+                                                          const double2* __restrict__ twN, unsigned int* __restrict__ err) {
+    constexpr int B = ZT<N, W>::B, P = ZT<N, W>::P, ROWS = ZT<N, W>::ROWS, NBOX = ZT<N, W>::NBOX;
+    constexpr unsigned SB = ZT<N, W>::STAGE_BYTES;
     constexpr ff::Sched SC = ff::make_sched(N);
     extern __shared__ unsigned char smraw[];
     // 1 KB-aligned stages (TMA destinations), then the twiddles, then the barriers
@@ -110,8 +116,13 @@ __global__ void __launch_bounds__(ZT<N>::P) k_zt_tma(const __grid_constant__ CUt
 
 #define ZT_SIZES(X) X(128) X(256) X(512) X(768) X(1024)
 
-template <int N>
-int zt_batch() { return ZT<N>::B; }
+template <int N, int W>
+int zt_batch() { return ZT<N, W>::B; }
+
+// the wide batch where it exists and a batch's rows span more than 1 GB
+bool zt_wide(int ncol, int nz) {
+    return (nz == 512 || nz == 768) && (size_t)ncol * 16 * (size_t)nz > ((size_t)1 << 30);
+}
 
 }  // namespace
 
@@ -139,10 +150,14 @@ bool zt_tma_supported(int nz) {
 
 void zt_tma_init() {
 #define X_CASE(n)                                                                                              \
-    cudaFuncSetAttribute(k_zt_tma<n, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ZT<n>::smem);     \
-    cudaFuncSetAttribute(k_zt_tma<n, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ZT<n>::smem);
+    cudaFuncSetAttribute(k_zt_tma<n, -1, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ZT<n>::smem);  \
+    cudaFuncSetAttribute(k_zt_tma<n, 1, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ZT<n>::smem);
     ZT_SIZES(X_CASE)
 #undef X_CASE
+    cudaFuncSetAttribute(k_zt_tma<512, -1, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ZT<512, 1>::smem);
+    cudaFuncSetAttribute(k_zt_tma<512, 1, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ZT<512, 1>::smem);
+    cudaFuncSetAttribute(k_zt_tma<768, -1, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ZT<768, 1>::smem);
+    cudaFuncSetAttribute(k_zt_tma<768, 1, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ZT<768, 1>::smem);
 }
 
 // the tensor map of the spectrum viewed as [nz][2*ncol] doubles with the
@@ -151,8 +166,9 @@ bool zt_tma_prepare(double2* spec, int ncol, int nz, void* tmap_out) {
     PFN_cuTensorMapEncodeTiled_v12000 enc = tma_encode_fn();
     if (!enc || !zt_tma_supported(nz)) return false;
     int B = 0;
-    switch (nz) {
-#define X_CASE(n) case n: B = zt_batch<n>(); break;
+    if (zt_wide(ncol, nz)) B = nz == 512 ? zt_batch<512, 1>() : zt_batch<768, 1>();
+    else switch (nz) {
+#define X_CASE(n) case n: B = zt_batch<n, 0>(); break;
         ZT_SIZES(X_CASE)
 #undef X_CASE
         default: return false;
@@ -170,21 +186,30 @@ bool zt_tma_prepare(double2* spec, int ncol, int nz, void* tmap_out) {
 void launch_zt_tma(cudaStream_t st, int dir, int ncol, int nz, const void* tmap, const double2* twz, int nsm,
                    unsigned int* err) {
     const CUtensorMap& tm = *reinterpret_cast<const CUtensorMap*>(tmap);
-    switch (nz) {
-#define X_CASE(n)                                                                                              \
-    case n: {                                                                                                  \
-        const int nb = (ncol + ZT<n>::B - 1) / ZT<n>::B;                                                       \
-        const int per_sm = (int)((220 * 1024) / ZT<n>::smem);                                                  \
+#define ZT_LAUNCH(n, w)                                                                                        \
+    {                                                                                                          \
+        const int nb = (ncol + ZT<n, w>::B - 1) / ZT<n, w>::B;                                                 \
+        const int per_sm = (int)((220 * 1024) / ZT<n, w>::smem);                                               \
         int grid = (per_sm > 0 ? per_sm : 1) * nsm;                                                            \
         if (grid > nb) grid = nb;                                                                              \
-        if (dir < 0) launch_pdl(k_zt_tma<n, -1>, dim3(grid), dim3(ZT<n>::P), ZT<n>::smem, st, tm, nb, twz, err); \
-        else launch_pdl(k_zt_tma<n, 1>, dim3(grid), dim3(ZT<n>::P), ZT<n>::smem, st, tm, nb, twz, err);         \
-        break;                                                                                                 \
+        if (dir < 0)                                                                                           \
+            launch_pdl(k_zt_tma<n, -1, w>, dim3(grid), dim3(ZT<n, w>::P), ZT<n, w>::smem, st, tm, nb, twz, err); \
+        else                                                                                                   \
+            launch_pdl(k_zt_tma<n, 1, w>, dim3(grid), dim3(ZT<n, w>::P), ZT<n, w>::smem, st, tm, nb, twz, err);  \
     }
+    if (zt_wide(ncol, nz)) {
+        if (nz == 512) ZT_LAUNCH(512, 1)
+        else ZT_LAUNCH(768, 1)
+        return;
+    }
+    switch (nz) {
+#define X_CASE(n)                                                                                              \
+    case n: ZT_LAUNCH(n, 0) break;
         ZT_SIZES(X_CASE)
 #undef X_CASE
         default: break;
     }
+#undef ZT_LAUNCH
 }
 
 }  // namespace ptc
