@@ -30,8 +30,11 @@ namespace {
 
 template <int N>
 struct XT {
-    static constexpr int B = ff::Shape<N>::B;
-    static constexpr int P = ff::Shape<N>::P;
+    // at least two rows per batch: single-row batches of nx = 3072 ran at 0.40
+    // of peak, two-row ones at 0.47 (one CTA per SM)
+    static constexpr int BM = ff::Shape<N>::B < 2 ? 2 : 1;
+    static constexpr int B = ff::Shape<N>::B * BM;
+    static constexpr int P = ff::Shape<N>::P * BM;
     static constexpr int M1 = N + 1;
     // row pitch in complex values: at least N+1, with B*PITCH residues that
     // spread a quarter warp's (row, element) pairs over the eight 16-byte

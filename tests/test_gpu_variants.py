@@ -71,9 +71,11 @@ def test_generic_fft_path(monkeypatch, dims):
     assert rel_err(phi_g, phi_o) <= TOL_POISSON
 
 
-@pytest.mark.parametrize("dims", [(48, 16, 24), (96, 12, 40), (80, 10, 64)])
+@pytest.mark.parametrize("dims", [(48, 16, 24), (96, 12, 40), (80, 10, 64), (2048, 10, 16), (2304, 10, 16),
+                                  (3072, 10, 16)])
 def test_fixed_length_sizes(dims):
-    """Other compile-time lengths (nx/2 = 24, 48, 40; nz = 24, 40, 64)."""
+    """Other compile-time lengths (nx/2 = 24, 48, 40 and the long rows 1024,
+    1152, 1536 of the bulk-copy x transforms; nz = 24, 40, 64, 16)."""
     case = cases.small_channel(*dims)
     yp = yp_of(case)
     src = cases.gaussian_source(cases.Case("src", case.params, case.mesh, "gauss_src", 7, 1.0))
