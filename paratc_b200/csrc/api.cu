@@ -120,7 +120,9 @@ struct ProfScope {
         if (q >= 0) cudaEventRecord(ctx->ev[2 * q + 1], ctx->st);
     }
 };
-#define PROF(cls) ProfScope prof_scope_##__LINE__(ctx, cls)
+#define PT_CAT2(a, b) a##b
+#define PT_CAT(a, b) PT_CAT2(a, b)
+#define PROF(cls) ProfScope PT_CAT(prof_scope_, __LINE__)(ctx, cls)
 
 void prof_flush(paratc_ctx* ctx) {
     if (ctx->ev_used == 0) return;
