@@ -13,11 +13,13 @@
 // the Neumann ghost copies phi(0) = phi(1), phi(nyp) = phi(nyc) of the
 // padded layout (SetBC_and_UpdateHalo_pr, src/m_BC_and_Halo.f90:115-120).
 // Forward (k_xf_tma): rows of a given source in, FFT, split in place into
-// the nx/2+1 modes of the real transform, spectrum rows out.
+// the nx/2+1 modes of the real transform, spectrum rows out.  Forward of the
+// divergence source (k_xf_div, Poisson schedules 8-11): the same consumer
+// side, with producer warps computing the source rows into the stages.
 //
 // Every wait is bounded: after kSpinLimit polls the CTA records an error
-// (*err |= 2), waits (bounded) for its own copies in flight and stops.  No
-// multicast; only this GPU's memory.
+// (*err |= 2, or 4 for k_xf_div), waits (bounded) for its own copies in
+// flight and stops.  No multicast; only this GPU's memory.
 #include "common.cuh"
 #include "fft_fixed.cuh"
 #include "kernels.cuh"
