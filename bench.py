@@ -109,6 +109,17 @@ def algorithmic_bytes(params):
     }
 
 
+def kernel_fractions(prof, alg, peak):
+    """Fraction of the HBM peak that every kernel class reaches: its
+    compulsory bytes per launch (algorithmic_bytes) over its mean event time,
+    divided by the measured peak (GB/s).  prof: {class: (total ms, launches)}."""
+    out = {}
+    for k, (ms_tot, n) in sorted(prof.items(), key=lambda kv: -kv[1][0]):
+        if k in alg and n > 0 and ms_tot > 0:
+            out[k] = round(alg[k] / (ms_tot / n / 1e3) / 1e9 / peak, 3)
+    return out
+
+
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons every 200 ms during the timed region."""
 
@@ -355,7 +366,7 @@ def run_ours(args):
     roof = {"bound": "hbm", "kernel": kname, "achieved": round(ach, 1), "peak": peak, "unit": "GB/s",
             "frac": round(ach / peak, 4), "traffic": traffic, "peak_kind": peak_kind,
             "algorithmic_bytes_per_launch": alg[kname], "avg_launch_us": round(avg_s * 1e6, 2),
-            "kernel_share": share}
+            "kernel_share": share, "kernel_frac": kernel_fractions(prof, alg, peak)}
     # whole-substep algorithmic bandwidth (every kernel's compulsory bytes / step time)
     step_bytes = sum(alg[k] * v[1] for k, v in prof.items() if k in alg) / args.steps
     roof["step_algorithmic_GBps"] = round(step_bytes / (statistics.mean(ms) / 1e3) / 1e9, 1)
@@ -562,7 +573,7 @@ def run_poisson(args):
                 "roofline": {"bound": "hbm", "kernel": "poisson solve (5 kernels)", "achieved": round(ach, 1),
                              "peak": peak, "unit": "GB/s", "frac": round(ach / peak, 4), "traffic": None,
                              "peak_kind": peak_kind, "algorithmic_bytes_per_launch": alg,
-                             "kernel_us": kern},
+                             "kernel_us": kern, "kernel_frac": kernel_fractions(prof, algorithmic_bytes(p), peak)},
                 "cpu_baseline": base,
                 "e2e": {"value": cells * args.steps / t_e2e, "unit": "grid-point Poisson solves/s",
                         "h2d_bytes_per_step": src.nbytes, "d2h_bytes_per_step": src.nbytes,
