@@ -45,7 +45,8 @@ extern "C" {
 #define PARATC_ERR_NONFINITE  -4  /* NaN/Inf found in a field                    */
 #define PARATC_ERR_DIV_LIMIT  -5  /* max|div u| > div_limit (ChannelIterate:143) */
 #define PARATC_ERR_VEL_LIMIT  -6  /* min(max|u_i|) > vel_limit (ChannelIterate:145) */
-#define PARATC_ERR_TIMEOUT    -7  /* a bounded device wait gave up               */
+#define PARATC_ERR_TIMEOUT    -7  /* a bounded device wait gave up; the context
+                                     keeps reporting it: destroy and recreate it */
 #define PARATC_ERR_IO         -8  /* restart file missing, short or wrong size   */
 #define PARATC_ERR_NO_DEVICE  -9  /* no CUDA device / library built without one  */
 #define PARATC_ERR_NUMERIC   -10  /* lambda2 met complex roots (Clc_lamda2 stops) */
