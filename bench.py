@@ -43,6 +43,8 @@ def _args():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", default="channel_c1")
+    ap.add_argument("--grid", type=int, nargs=3, default=None, metavar=("NX", "NY", "NZ"),
+                    help="poisson_c2 only: solve on this grid instead of 512 x 256 x 512 (profiling other lengths)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
@@ -509,7 +511,7 @@ def run_poisson(args):
     torch.cuda.set_device(local)
     from paratc_b200 import cases
     from paratc_b200.lib import ChannelSystem, mesh_ycoord
-    case = cases.poisson_c2()
+    case = cases.poisson_c2(*args.grid) if args.grid else cases.poisson_c2()
     p = case.params
     yp = mesh_ycoord(case.mesh, p.yly)
     src = cases.gaussian_source(cases.Case("src", p, case.mesh, "gauss_src", 42 + rank, 1.0))
@@ -558,7 +560,8 @@ def run_poisson(args):
         o.close()
         err = float(np.abs(phi_g - phi_o).max() / np.abs(phi_o).max())
         base = {"value": cells / t_o, "unit": "grid-point Poisson solves/s", "cores": threads, "kind": "port",
-                "sample": "one 512x256x512 solve on the C oracle (OpenMP, %d threads), %.1f s" % (threads, t_o)}
+                "sample": "one %dx%dx%d solve on the C oracle (OpenMP, %d threads), %.1f s"
+                          % (p.nxc, p.nyc, p.nzc, threads, t_o)}
     peak, peak_kind = _peaks()
     alg = 6 * 8 * cells
     ach = alg / (ms / args.steps / 1e3) / 1e9
@@ -568,7 +571,7 @@ def run_poisson(args):
                 "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": "f64", "data": "synthetic",
                 "config": {"workload": case.name, "grid": [p.nxc, p.nyc, p.nzc], "precision": "fp64",
-                           "l2": "src and phi 537 MB each > L2, no flush",
+                           "l2": "src and phi %d MB each%s, no flush" % (src.nbytes // 10**6, " > L2" if src.nbytes > L2_BYTES else ""),
                            "max_rel_err_vs_oracle": err, "poisson_schedule": schedule, "autotune_ms": tune_ms, "mean_phi_e2e_equal": bool(np.array_equal(phi_h, phi_g))},
                 "roofline": {"bound": "hbm", "kernel": "poisson solve (5 kernels)", "achieved": round(ach, 1),
                              "peak": peak, "unit": "GB/s", "frac": round(ach / peak, 4), "traffic": None,
