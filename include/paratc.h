@@ -259,8 +259,12 @@ int paratc_poisson_device_async(paratc_ctx* ctx, const double* d_src, double* d_
  * loads the library until exit): grids needing more than
  * 2*(nxc/2+1)*nyc*nzc + O(nxc+nyc+nzc) doubles, or nxc/nzc > 1024, nyc > 256,
  * are rejected with PARATC_ERR_BAD_ARG.  The first call on a device looks up
- * the array's device address (make it before any stream capture).  All calls
- * share the array: calls that overlap on the GPU race. */
+ * the array's device address (once per device, safe from several host
+ * threads; cudaDeviceReset after it is not supported).  The call must not be
+ * made while `stream` is being captured into a CUDA graph: it copies tables
+ * from its stack frame (about 68 KB at the largest sizes) and waits for the
+ * stream, and returns PARATC_ERR_BAD_ARG during capture.  All calls share the
+ * array: calls that overlap on the GPU race. */
 #define PARATC_NOALLOC_SCRATCH_DOUBLES (2 * 1024 * 1024)
 int paratc_poisson_noalloc(const paratc_params* prm, const double* yp,
                            const double* d_src, double* d_phi, void* stream);
@@ -272,6 +276,19 @@ int paratc_project(paratc_ctx* ctx, double* divmax_out);
 
 /* Reductions of src/m_Tools.f90 on the current fields. */
 int paratc_diagnostics(paratc_ctx* ctx, paratc_diag* diag);
+
+/* x profile of a field averaged over the depth and the span,
+ * out[i] = sum_kc sum_jc q(ic, jc, kc) dyp(jc) / (nzc yly), ic = i+1, for
+ * field 0 ux, 1 uy, 2 uz, 3 p, 4 scalar (out: nxc doubles).  No counterpart
+ * in the reference; it is the depth-averaged concentration from which a
+ * gravity current's front is read. */
+int paratc_xprofile(paratc_ctx* ctx, int field, double* out);
+/* Front of a gravity current: the x to the right of x_from (the lock) where
+ * the depth-averaged scalar first falls below `level` (0.5 for a lock
+ * release), interpolated linearly between the cell centres (ic-0.5)*dx;
+ * -1 when it nowhere does.  Not in the reference (a builder-defined
+ * diagnostic of the lock-exchange case). */
+int paratc_front_position(paratc_ctx* ctx, double x_from, double level, double* x_front);
 
 /* ---- restart files (src/m_IOAndVisu.f90:408-512) ----------------------- */
 /* Raw FP64, headerless, Fortran order: ux+uCRF, uy, uz, p, [c],
@@ -297,6 +314,17 @@ int paratc_profile_enable(paratc_ctx* ctx, int on);
 int paratc_profile_get(paratc_ctx* ctx, int k, double* total_ms, int64_t* launches);
 /* Name of kernel class k ("rhs", "helmholtz", "fft_x_fwd", ...). */
 const char* paratc_profile_name(int k);
+
+/* ---- bounded device waits.  No counterpart in the reference (its MPI calls
+ * block).  Every pipeline wait of the TMA-fed kernels (z transforms, x
+ * transforms, divergence-fed x transform, right-hand side) polls its
+ * mbarrier at most 2^22 times; a CTA whose wait runs out records the failure,
+ * waits (with the full limit) for its own copies still in flight and returns,
+ * and the next synchronising call reports PARATC_ERR_TIMEOUT.  This sets the
+ * poll limit of those pipeline waits on this context: polls >= 0 allows that
+ * many polls (0: give up at the first wait), polls < 0 restores the default.
+ * It exists so that tests can drive the timeout path without stalling a GPU. */
+int paratc_set_wait_limit(paratc_ctx* ctx, long long polls);
 
 /* ---- precision of the step.  PARATC_PREC_FP64 (the default) is the
  * reference's arithmetic.  PARATC_PREC_MIXED computes the explicit

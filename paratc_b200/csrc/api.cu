@@ -14,6 +14,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -505,18 +506,24 @@ int paratc_create(const paratc_params* prm, const double* yp, int device, paratc
     ctx->plane = ctx->pfft && plane_supported(ctx->nx, ctx->nz) && std::getenv("PARATC_NO_PLANE") == nullptr;
     cudaError_t ce = cudaStreamCreateWithFlags(&ctx->st, cudaStreamNonBlocking);
     if (ce != cudaSuccess) { delete ctx; return PARATC_ERR_CUDA; }
-    static bool inited = false;
-    if (!inited) {
-        fft_init();
-        tridiag_init();
-        rhs_init();
-        pfft_x_init();
-        pfft_z_init();
-        plane_init();
-        zt_tma_init();
-        xt_tma_init();
-        spectra_init();
-        inited = true;
+    // the kernels' shared-memory limits are attributes of each device: set
+    // them once per device, with that device current
+    {
+        static std::mutex mu;
+        static std::vector<int> done;
+        std::lock_guard<std::mutex> lock(mu);
+        if (std::find(done.begin(), done.end(), ctx->dev) == done.end()) {
+            fft_init();
+            tridiag_init();
+            rhs_init();
+            pfft_x_init();
+            pfft_z_init();
+            plane_init();
+            zt_tma_init();
+            xt_tma_init();
+            spectra_init();
+            done.push_back(ctx->dev);
+        }
     }
     const HostMetrics& h = ctx->hm;
     // ---- constants
@@ -900,6 +907,16 @@ int paratc_set_schedule(paratc_ctx* ctx, int choice) {
     return PARATC_OK;
 }
 
+int paratc_set_wait_limit(paratc_ctx* ctx, long long polls) {
+    if (!ctx) return PARATC_ERR_BAD_ARG;
+    CK(cudaSetDevice(ctx->dev));
+    // word 1 after the error word, read by every TMA-fed kernel at its start
+    const unsigned int v = polls < 0 ? 0u : (unsigned int)std::min<long long>(polls + 1, 0xffffffffLL);
+    CK(cudaMemcpyAsync(ctx->d_zt_err + 1, &v, sizeof(v), cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));  // v lives on this stack frame
+    return PARATC_OK;
+}
+
 int paratc_set_precision(paratc_ctx* ctx, int prec) {
     if (!ctx || (prec != PARATC_PREC_FP64 && prec != PARATC_PREC_MIXED)) return PARATC_ERR_BAD_ARG;
     ctx->kc.fp32_rhs = prec == PARATC_PREC_MIXED ? 1 : 0;
@@ -986,6 +1003,43 @@ int paratc_diagnostics(paratc_ctx* ctx, paratc_diag* diag) {
     int rc = sync(ctx);
     if (rc) return rc;
     diag_out(*ctx->h_diag, diag);
+    return PARATC_OK;
+}
+
+int paratc_xprofile(paratc_ctx* ctx, int field, double* out) {
+    if (!ctx || !out || field < 0 || field > 4) return PARATC_ERR_BAD_ARG;
+    const double* q[5] = {ctx->f.ux, ctx->f.uy, ctx->f.uz, ctx->f.pr, ctx->f.sc};
+    if (!q[field]) return set_err(ctx, PARATC_ERR_BAD_ARG, "xprofile: no scalar in this context");
+    CK(cudaSetDevice(ctx->dev));
+    // d_src (nx*ny*nz doubles, ny >= 3) is free between substeps: the nx*nz
+    // column sums, then the profile
+    double* part = ctx->d_src;
+    double* prof = ctx->d_src + (size_t)ctx->nx * ctx->nz;
+    launch_xprofile(ctx->st, ctx->kc, ctx->dm, q[field], part, prof);
+    ctx->launches += 2;
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(out, prof, (size_t)ctx->nx * sizeof(double), cudaMemcpyDefault, ctx->st));
+    return sync(ctx);
+}
+
+int paratc_front_position(paratc_ctx* ctx, double x_from, double level, double* x_front) {
+    if (!ctx || !x_front) return PARATC_ERR_BAD_ARG;
+    if (!ctx->prm.scalar_on) return set_err(ctx, PARATC_ERR_BAD_ARG, "front position: no scalar in this context");
+    std::vector<double> prof(ctx->nx);
+    int rc = paratc_xprofile(ctx, 4, prof.data());
+    if (rc) return rc;
+    const double dx = ctx->prm.xlx / ctx->nx;
+    *x_front = -1.0;
+    for (int i = 0; i < ctx->nx; i++) {
+        const double x = (i + 0.5) * dx;  // the scalar's cell centres
+        if (x <= x_from || !(prof[i] < level)) continue;
+        const double xm = x - dx;
+        if (i > 0 && xm > x_from && prof[i - 1] >= level)
+            *x_front = xm + (prof[i - 1] - level) / (prof[i - 1] - prof[i]) * dx;
+        else
+            *x_front = x;
+        break;
+    }
     return PARATC_OK;
 }
 

@@ -88,6 +88,11 @@ __device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.lau
 
 __device__ __forceinline__ int wrapi(int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); }
 
+// maximum that keeps a NaN: fmax(x, NaN) returns x, so a field that is NaN
+// everywhere would report a maximum of 0 and pass every guard; with nmax a
+// NaN anywhere reaches the grid-wide result (the non-finite guard's input)
+__device__ __forceinline__ double nmax(double a, double b) { return (a > b || a != a) ? a : b; }
+
 __device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
 __device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {

@@ -71,7 +71,7 @@ __device__ __forceinline__ void div_batch(const DConst& c, const DMetric& m, con
             double2 val = make_double2(0.0, 0.0);
             if (ok[u]) {
                 const double2 d = div_eval(tp[u], c);
-                dm = fmax(dm, fmax(fabs(d.x), fabs(d.y)));
+                dm = nmax(dm, nmax(fabs(d.x), fabs(d.y)));
                 val = make_double2(sudtal * d.x, sudtal * d.y);
             }
             st(b, e, val);

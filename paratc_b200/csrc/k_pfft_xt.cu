@@ -92,6 +92,7 @@ __global__ void __launch_bounds__(XT<N>::P, XT<N>::MINB)
     __shared__ unsigned long long mbar[2];
     __shared__ int s_bad;
     const int tid = threadIdx.x;
+    const long long lim = tma::wait_limit(err);
     const int nb = (nrows + B - 1) / B;
     const int nx = 2 * N, nyt = ny + 2;
     if (tid == 0) {
@@ -120,7 +121,7 @@ __global__ void __launch_bounds__(XT<N>::P, XT<N>::MINB)
         // one decision for the whole CTA: a flag read after a plain barrier
         // could be set by a faster thread's next wait before a slower one
         // reads it, and the two would then part at the next barrier
-        if (__syncthreads_or(tma::mbar_wait(&mbar[s], (unsigned)((it >> 1) & 1)) ? 0 : 1)) {
+        if (__syncthreads_or(tma::mbar_wait(&mbar[s], (unsigned)((it >> 1) & 1), lim) ? 0 : 1)) {
             s_bad = 1;
             break;
         }
@@ -192,6 +193,7 @@ __global__ void __launch_bounds__(XT<N>::P, XT<N>::MINB)
     __shared__ unsigned long long mbar[2];
     __shared__ int s_bad;
     const int tid = threadIdx.x;
+    const long long lim = tma::wait_limit(err);
     const int nb = (nrows + B - 1) / B;
     const int nx = 2 * N;
     if (tid == 0) {
@@ -220,7 +222,7 @@ __global__ void __launch_bounds__(XT<N>::P, XT<N>::MINB)
         // one decision for the whole CTA: a flag read after a plain barrier
         // could be set by a faster thread's next wait before a slower one
         // reads it, and the two would then part at the next barrier
-        if (__syncthreads_or(tma::mbar_wait(&mbar[s], (unsigned)((it >> 1) & 1)) ? 0 : 1)) {
+        if (__syncthreads_or(tma::mbar_wait(&mbar[s], (unsigned)((it >> 1) & 1), lim) ? 0 : 1)) {
             s_bad = 1;
             break;
         }
@@ -326,6 +328,7 @@ __global__ void __launch_bounds__(XD<N>::NT, 1)
     const int tid = threadIdx.x;
     const int nrows = c.ny * c.nz;
     const int nb = (nrows + B - 1) / B;
+    const long long lim = tma::wait_limit(err);
     if (tid == 0) {
         tma::mbar_init(&full[0], Q);
         tma::mbar_init(&full[1], Q);
@@ -345,7 +348,7 @@ __global__ void __launch_bounds__(XD<N>::NT, 1)
         int it = 0;
         for (int bt = blockIdx.x; bt < nb; bt += gridDim.x, it++) {
             const int s = it & 1;
-            const bool ok = it < 2 || tma::mbar_wait(&empty[s], (unsigned)(((it >> 1) + 1) & 1));
+            const bool ok = it < 2 || tma::mbar_wait(&empty[s], (unsigned)(((it >> 1) + 1) & 1), lim);
             if (ff::group_any<2, Q>(!ok)) {
                 bad_p = 1;
                 break;
@@ -361,7 +364,7 @@ __global__ void __launch_bounds__(XD<N>::NT, 1)
         for (int bt = blockIdx.x; bt < nb; bt += gridDim.x, it++) {
             const int s = it & 1;
             double2* buf = stage[s];
-            if (ff::group_any<1, P>(!tma::mbar_wait(&full[s], (unsigned)((it >> 1) & 1)))) {
+            if (ff::group_any<1, P>(!tma::mbar_wait(&full[s], (unsigned)((it >> 1) & 1), lim))) {
                 bad_c = 1;
                 break;
             }

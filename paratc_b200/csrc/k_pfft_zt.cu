@@ -56,6 +56,7 @@ __global__ void __launch_bounds__(ZT<N, W>::P) k_zt_tma(const __grid_constant__ 
     __shared__ unsigned long long mbar[2];
     __shared__ int s_bad;
     const int tid = threadIdx.x;
+    const long long lim = tma::wait_limit(err);
     for (int t = tid; t < N; t += P) tws[t] = twN[t];
     if (tid == 0) {
         tma::mbar_init(&mbar[0], 1);
@@ -83,7 +84,7 @@ __global__ void __launch_bounds__(ZT<N, W>::P) k_zt_tma(const __grid_constant__ 
         // one decision for the whole CTA: a flag read after a plain barrier
         // could be set by a faster thread's next wait before a slower one
         // reads it, and the two would then part at the next barrier
-        if (__syncthreads_or(tma::mbar_wait(&mbar[s], (unsigned)((it >> 1) & 1)) ? 0 : 1)) {
+        if (__syncthreads_or(tma::mbar_wait(&mbar[s], (unsigned)((it >> 1) & 1), lim) ? 0 : 1)) {
             s_bad = 1;
             break;
         }

@@ -114,7 +114,7 @@ __global__ void __launch_bounds__(PL_P, 1)
             const double dwdz0 = c.dzC[0] * w0.x + c.dzC[1] * w1.x + c.dzC[2] * w2.x + c.dzC[3] * w3.x;
             const double dwdz1 = c.dzC[0] * w0.y + c.dzC[1] * w1.y + c.dzC[2] * w2.y + c.dzC[3] * w3.y;
             const double d0 = dudx0 + dvdy0 + dwdz0, d1 = dudx1 + dvdy1 + dwdz1;
-            dm = fmax(dm, fmax(fabs(d0), fabs(d1)));
+            dm = nmax(dm, nmax(fabs(d0), fabs(d1)));
             buf[e * PITCH + k] = make_double2(sudtal * d0, sudtal * d1);
         }
     }

@@ -241,12 +241,12 @@ __global__ void __launch_bounds__(ENDSTEP_THREADS, 2)
                 const double dudx = c.dxC[0] * a[u][0] + c.dxC[1] * u0 + c.dxC[2] * up + c.dxC[3] * a[u][3];
                 const double dvdy = (vp - v0) * rdyp;
                 const double dwdz = c.dzC[0] * a[u][6] + c.dzC[1] * z1 + c.dzC[2] * z2 + c.dzC[3] * a[u][9];
-                mx[0] = fmax(mx[0], fabs(dudx + dvdy + dwdz));
-                mx[1] = fmax(mx[1], fabs(u0));
-                mx[2] = fmax(mx[2], fabs(v0));
-                mx[3] = fmax(mx[3], fabs(z1));
+                mx[0] = nmax(mx[0], fabs(dudx + dvdy + dwdz));
+                mx[1] = nmax(mx[1], fabs(u0));
+                mx[2] = nmax(mx[2], fabs(v0));
+                mx[3] = nmax(mx[3], fabs(z1));
                 if (next)
-                    mx[4] = fmax(mx[4], fabs(u0 + up) * c.rdx + fabs(v0 + vp) * rdyp + fabs(z1 + z2) * c.rdz);
+                    mx[4] = nmax(mx[4], fabs(u0 + up) * c.rdx + fabs(v0 + vp) * rdyp + fabs(z1 + z2) * c.rdz);
                 sm[0] += u0 * dy;
                 if (c.scalar_on) {
                     const double s = a[u][10];
@@ -266,7 +266,7 @@ __global__ void __launch_bounds__(ENDSTEP_THREADS, 2)
     for (int b = threadIdx.x; b < (int)gridDim.x; b += ENDSTEP_THREADS) {
         const double* p = part + (size_t)b * 8;
 #pragma unroll
-        for (int q = 0; q < 5; q++) v[q] = fmax(v[q], __ldcg(&p[q]));
+        for (int q = 0; q < 5; q++) v[q] = nmax(v[q], __ldcg(&p[q]));
 #pragma unroll
         for (int q = 5; q < 8; q++) v[q] += __ldcg(&p[q]);
     }
@@ -274,7 +274,7 @@ __global__ void __launch_bounds__(ENDSTEP_THREADS, 2)
     for (int q = 0; q < 8; q++)
         for (int o = 16; o > 0; o >>= 1) {
             const double y = __shfl_down_sync(0xffffffffu, v[q], o);
-            v[q] = q < 5 ? fmax(v[q], y) : v[q] + y;
+            v[q] = q < 5 ? nmax(v[q], y) : v[q] + y;
         }
     if (lane == 0)
 #pragma unroll
@@ -283,7 +283,7 @@ __global__ void __launch_bounds__(ENDSTEP_THREADS, 2)
     if (threadIdx.x != 0) return;
     double r[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     for (int w = 0; w < ENDSTEP_THREADS / 32; w++)
-        for (int q = 0; q < 8; q++) r[q] = q < 5 ? fmax(r[q], sh[w][q]) : r[q] + sh[w][q];
+        for (int q = 0; q < 8; q++) r[q] = q < 5 ? nmax(r[q], sh[w][q]) : r[q] + sh[w][q];
     DDiag d = *diag;
     DCoef f = *coef;
     d.step_counter += 1;
@@ -299,8 +299,15 @@ __global__ void __launch_bounds__(ENDSTEP_THREADS, 2)
     d.sc_mean = r[6] / nxz / c.yly;
     d.sc2_mean = r[7] / nxz / c.yly;
     if (d.status == 0) {
-        double vmin = fmin(fmin(r[1], r[2]), r[3]);
-        if (!(r[0] == r[0]) || !(vmin == vmin)) { d.status = -4; d.failed_step = d.step_counter; }
+        // the maxima keep a NaN (nmax) and |Inf| stays Inf, so one non-finite
+        // value of u, v, w or div u anywhere makes one of these non-finite;
+        // the sums catch a non-finite scalar.  ChannelIterate's own tests
+        // (src/m_ChannelSystem.f90:143,145) follow: div_limit, then the
+        // smallest of the three velocity maxima against vel_limit.
+        bool finite = true;
+        for (int q = 0; q < 8; q++) finite = finite && isfinite(r[q]);
+        const double vmin = fmin(fmin(r[1], r[2]), r[3]);
+        if (!finite) { d.status = -4; d.failed_step = d.step_counter; }
         else if (r[0] > c.div_limit) { d.status = -5; d.failed_step = d.step_counter; }
         else if (vmin > c.vel_limit) { d.status = -6; d.failed_step = d.step_counter; }
     }
@@ -312,6 +319,31 @@ __global__ void __launch_bounds__(ENDSTEP_THREADS, 2)
         f.dt = (c.icfl == 1) ? fmin(c.cflc / uddxmax, c.dt_max) : c.dt_max;
         *coef = f;
     }
+}
+
+// ---------------------------------------------------------------------------
+// x profile of a field averaged over the depth and the span:
+// prof(i) = sum_k sum_j q(i, j, k) dyp(j) / (nz * yly), the depth-averaged
+// concentration whose 0.5 crossing is the front of a gravity current.  One
+// thread per (i, k) sums its column over j in order; the second kernel adds
+// the nz columns of an i in order, so the result is deterministic.
+// ---------------------------------------------------------------------------
+__global__ void k_xprof_part(DConst c, DMetric m, const double* __restrict__ q, double* __restrict__ part) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int k = blockIdx.y;
+    if (i >= c.nx) return;
+    const double* col = q + (size_t)k * c.nyt * c.nx + i;
+    double s = 0.0;
+    for (int j = 1; j <= c.ny; j++) s += __ldg(&col[(size_t)j * c.nx]) * __ldg(&m.dyp[j]);
+    part[(size_t)k * c.nx + i] = s;
+}
+
+__global__ void k_xprof_final(DConst c, const double* __restrict__ part, double* __restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= c.nx) return;
+    double s = 0.0;
+    for (int k = 0; k < c.nz; k++) s += part[(size_t)k * c.nx + i];
+    out[i] = s / (double)c.nz / c.yly;
 }
 
 __global__ void k_store_divsrc(DCoef* coef, const double* __restrict__ v) {
@@ -353,6 +385,11 @@ void launch_update_uy_ym(cudaStream_t st, int n, double* uy_ym, double* duy_ym) 
 void launch_cfl(cudaStream_t st, const DConst& c, const DMetric& m, const Fields& f, DCoef* coef, double* part) {
     k_cfl<<<cell_grid(c), cell_block(), 0, st>>>(c, m, f.ux, f.uy, f.uz, part);
     k_cfl_final<<<1, 1024, 0, st>>>(c, coef, part, (int)cell_grid_blocks(c));
+}
+
+void launch_xprofile(cudaStream_t st, const DConst& c, const DMetric& m, const double* q, double* part, double* out) {
+    k_xprof_part<<<dim3((c.nx + 127) / 128, c.nz), 128, 0, st>>>(c, m, q, part);
+    k_xprof_final<<<(c.nx + 127) / 128, 128, 0, st>>>(c, part, out);
 }
 
 size_t endstep_blocks(const DConst& c) { return (size_t)2 * (c.nsm > 0 ? c.nsm : 148); }

@@ -45,6 +45,8 @@ void launch_bc_all(cudaStream_t st, const DConst& c, const Fields& f, const doub
 void launch_update_uy_ym(cudaStream_t st, int n, double* uy_ym, double* duy_ym);
 void launch_cfl(cudaStream_t st, const DConst& c, const DMetric& m, const Fields& f, DCoef* coef, double* part);
 size_t endstep_blocks(const DConst& c);
+// x profile of a padded field averaged over y (dyp weights) and z; part holds nx*nz doubles
+void launch_xprofile(cudaStream_t st, const DConst& c, const DMetric& m, const double* q, double* part, double* out);
 void launch_endstep(cudaStream_t st, const DConst& c, const DMetric& m, const Fields& f, DCoef* coef, DDiag* diag,
                     double* part, unsigned int* counter, int next);
 

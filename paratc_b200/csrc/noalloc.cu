@@ -23,17 +23,25 @@
 // device address is obtained once per device, with that device current, by
 // cudaGetSymbolAddress() in noalloc_setup(); the first call of the entry point
 // on a device performs that set-up (and sets the shared-memory limits of the
-// FFT kernels), so that first call should be made before any stream capture.
+// FFT kernels) under a per-device std::call_once, so first calls from several
+// host threads are safe.  The address is kept for the life of the process:
+// cudaDeviceReset() after the first call is not supported.
+//
+// The entry point must not be called while its stream is being captured into
+// a CUDA graph (it returns PARATC_ERR_BAD_ARG then): it copies tables from
+// its stack frame to the device and waits for the stream.
 //
 // All calls share the one array: two calls whose work overlaps on the GPU
 // (different streams, or different host threads) race and corrupt each other.
 // The entry point calls no cudaMalloc, cudaFree or other allocating routine;
-// host-side tables live on the stack.
+// host-side tables live on the stack (about 68 KB at the largest sizes).
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 
 #include "../../include/paratc.h"
 #include "common.cuh"
@@ -48,20 +56,24 @@ static __device__ __align__(256) double g_noalloc_scratch[PARATC_NOALLOC_SCRATCH
 constexpr int kMaxDevices = 64;
 constexpr int kMaxNxz = 1024;    // largest nxc / nzc accepted (host stack tables)
 constexpr int kMaxNy = 256;      // largest nyc accepted (the tridiagonal kernels)
-double* g_scratch_dev[kMaxDevices] = {nullptr};
+std::once_flag g_setup_once[kMaxDevices];
+std::atomic<double*> g_scratch_dev[kMaxDevices];
 
+// once per device, with that device current: the device address of the
+// array and the kernels' shared-memory limits
 int noalloc_setup(int dev) {
-    if (g_scratch_dev[dev]) return PARATC_OK;
-    void* p = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess || p == nullptr) {
-        std::fprintf(stderr, "paratc_poisson_noalloc: cudaGetSymbolAddress failed: %s\n", cudaGetErrorString(e));
-        return PARATC_ERR_CUDA;
-    }
-    fft_init();
-    tridiag_init();
-    g_scratch_dev[dev] = static_cast<double*>(p);
-    return PARATC_OK;
+    std::call_once(g_setup_once[dev], [dev] {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || p == nullptr) {
+            std::fprintf(stderr, "paratc_poisson_noalloc: cudaGetSymbolAddress failed: %s\n", cudaGetErrorString(e));
+            return;
+        }
+        fft_init();
+        tridiag_init();
+        g_scratch_dev[dev].store(static_cast<double*>(p), std::memory_order_release);
+    });
+    return g_scratch_dev[dev].load(std::memory_order_acquire) ? PARATC_OK : PARATC_ERR_CUDA;
 }
 
 bool plan_of(int n, FftPlan& pl) {
@@ -117,10 +129,18 @@ extern "C" int paratc_poisson_noalloc(const paratc_params* prm, const double* yp
     }
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return PARATC_ERR_NO_DEVICE;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    // an error left by an earlier, unrelated call would otherwise be reported
+    // as this call's own by the launch check at the end
+    (void)cudaGetLastError();
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(st, &cap) != cudaSuccess || cap != cudaStreamCaptureStatusNone) {
+        std::fprintf(stderr, "paratc_poisson_noalloc: the stream is being captured; call it outside stream capture\n");
+        return PARATC_ERR_BAD_ARG;
+    }
     int rc = noalloc_setup(dev);
     if (rc != PARATC_OK) return rc;
-    double* scr = g_scratch_dev[dev];
-    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    double* scr = g_scratch_dev[dev].load(std::memory_order_acquire);
 
     // pressure y operator (InitMeshAndMetries, src/m_MeshAndMetries.f90:194-247)
     // and the modified wavenumbers (src/m_Poisson.f90:40-48), on the stack

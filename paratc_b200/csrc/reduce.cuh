@@ -40,7 +40,7 @@ __device__ __forceinline__ void block_max_store(double (&v)[NV], double* __restr
     const int lane = tid & 31, wid = tid >> 5, nw = (nthr + 31) >> 5;
 #pragma unroll
     for (int q = 0; q < NV; q++)
-        for (int o = 16; o > 0; o >>= 1) v[q] = fmax(v[q], __shfl_down_sync(0xffffffffu, v[q], o));
+        for (int o = 16; o > 0; o >>= 1) v[q] = nmax(v[q], __shfl_down_sync(0xffffffffu, v[q], o));
     if (lane == 0)
 #pragma unroll
         for (int q = 0; q < NV; q++) sh[wid][q] = v[q];
@@ -49,7 +49,7 @@ __device__ __forceinline__ void block_max_store(double (&v)[NV], double* __restr
 #pragma unroll
         for (int q = 0; q < NV; q++) {
             double x = lane < nw ? sh[lane][q] : 0.0;
-            for (int o = 16; o > 0; o >>= 1) x = fmax(x, __shfl_down_sync(0xffffffffu, x, o));
+            for (int o = 16; o > 0; o >>= 1) x = nmax(x, __shfl_down_sync(0xffffffffu, x, o));
             if (lane == 0) out_block[q] = x;
         }
     }
@@ -65,12 +65,12 @@ __device__ void reduce_parts(const double* __restrict__ parts, int nparts, doubl
     for (int q = 0; q < NV; q++) v[q] = 0.0;
     for (int b = tid; b < nparts; b += blockDim.x)
 #pragma unroll
-        for (int q = 0; q < NV; q++) v[q] = MAX ? fmax(v[q], parts[(size_t)b * NV + q]) : v[q] + parts[(size_t)b * NV + q];
+        for (int q = 0; q < NV; q++) v[q] = MAX ? nmax(v[q], parts[(size_t)b * NV + q]) : v[q] + parts[(size_t)b * NV + q];
 #pragma unroll
     for (int q = 0; q < NV; q++)
         for (int o = 16; o > 0; o >>= 1) {
             double y = __shfl_down_sync(0xffffffffu, v[q], o);
-            v[q] = MAX ? fmax(v[q], y) : v[q] + y;
+            v[q] = MAX ? nmax(v[q], y) : v[q] + y;
         }
     if (lane == 0)
 #pragma unroll
@@ -83,7 +83,7 @@ __device__ void reduce_parts(const double* __restrict__ parts, int nparts, doubl
             x = lane < nw ? sh[lane][q] : 0.0;
             for (int o = 16; o > 0; o >>= 1) {
                 double y = __shfl_down_sync(0xffffffffu, x, o);
-                x = MAX ? fmax(x, y) : x + y;
+                x = MAX ? nmax(x, y) : x + y;
             }
         }
         out[q] = x;  // valid in thread 0
@@ -124,13 +124,13 @@ __device__ void reduce_records(const double* parts, int nparts, double (&out)[NV
 #pragma unroll
         for (int q = 0; q < NV; q++) {
             const double x = __ldcg(&parts[(size_t)b * NV + q]);
-            v[q] = MAX ? fmax(v[q], x) : v[q] + x;
+            v[q] = MAX ? nmax(v[q], x) : v[q] + x;
         }
 #pragma unroll
     for (int q = 0; q < NV; q++)
         for (int o = 16; o > 0; o >>= 1) {
             const double y = __shfl_down_sync(0xffffffffu, v[q], o);
-            v[q] = MAX ? fmax(v[q], y) : v[q] + y;
+            v[q] = MAX ? nmax(v[q], y) : v[q] + y;
         }
     __syncthreads();
     if (lane == 0)
@@ -140,7 +140,7 @@ __device__ void reduce_records(const double* parts, int nparts, double (&out)[NV
 #pragma unroll
     for (int q = 0; q < NV; q++) {
         double x = 0.0;
-        for (int ww = 0; ww < nw; ww++) x = MAX ? fmax(x, sh[ww][q]) : x + sh[ww][q];
+        for (int ww = 0; ww < nw; ww++) x = MAX ? nmax(x, sh[ww][q]) : x + sh[ww][q];
         out[q] = x;
     }
     __syncthreads();

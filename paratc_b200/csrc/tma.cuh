@@ -26,10 +26,20 @@ __device__ __forceinline__ void mbar_expect_tx(unsigned long long* m, unsigned b
 __device__ __forceinline__ void mbar_arrive(unsigned long long* m) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_addr(m)) : "memory");
 }
-// true once phase `parity` of the barrier has completed; false after the spin limit
-__device__ __forceinline__ bool mbar_wait(unsigned long long* m, unsigned parity) {
+// polls the pipeline waits of a TMA-fed kernel make before they give up.
+// err points at the context's error word; err[1] holds a test setting
+// (paratc_set_wait_limit): 0 keeps kSpinLimit, v > 0 allows v - 1 polls, so
+// that a test can make a wait run out.  The waits that drain a CTA's own
+// copies in flight after a failure always keep kSpinLimit.
+__device__ __forceinline__ long long wait_limit(const unsigned int* err) {
+    const unsigned v = *(volatile const unsigned int*)(err + 1);
+    return v == 0u ? kSpinLimit : (long long)(v - 1u);
+}
+
+// true once phase `parity` of the barrier has completed; false after `limit` polls
+__device__ __forceinline__ bool mbar_wait(unsigned long long* m, unsigned parity, long long limit = kSpinLimit) {
     const unsigned a = smem_addr(m);
-    for (long long it = 0; it < kSpinLimit; it++) {
+    for (long long it = 0; it < limit; it++) {
         unsigned done;
         asm volatile(
             "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"

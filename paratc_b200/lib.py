@@ -35,7 +35,8 @@ EXPORTED = [
     "paratc_spectra2d_setup", "paratc_spectra2d_reset", "paratc_spectra2d_accumulate", "paratc_spectra2d_get",
     "paratc_visu_name", "paratc_visu_quantity", "paratc_dump_visu", "paratc_write_xdmf",
     "paratc_io_options_from_namelist", "paratc_visu_quantity_device", "paratc_autotune", "paratc_get_schedule",
-    "paratc_set_schedule", "paratc_set_precision", "paratc_get_precision",
+    "paratc_set_schedule", "paratc_set_precision", "paratc_get_precision", "paratc_set_wait_limit",
+    "paratc_xprofile", "paratc_front_position",
 ]
 PROF_NKERNELS = 16
 
@@ -80,6 +81,9 @@ def load(path=None):
     L.paratc_set_schedule.argtypes = [ctypes.c_void_p, ctypes.c_int]
     L.paratc_set_precision.argtypes = [ctypes.c_void_p, ctypes.c_int]
     L.paratc_get_precision.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]
+    L.paratc_set_wait_limit.argtypes = [ctypes.c_void_p, ctypes.c_longlong]
+    L.paratc_xprofile.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp]
+    L.paratc_front_position.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double, _dp]
     L.paratc_dump_visu.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_char_p] + [ctypes.c_int] * 7
     L.paratc_write_xdmf.argtypes = [ctypes.POINTER(ParatcParams), _dp, ctypes.c_char_p, ctypes.c_char_p] + \
         [ctypes.c_int] * 6
@@ -450,6 +454,13 @@ class ChannelSystem:
     def precision(self, name):
         self._check(self._L.paratc_set_precision(self._h, {"fp64": 0, "mixed": 1}[name]), "paratc_set_precision")
 
+    def set_wait_limit(self, polls):
+        """Poll limit of the TMA-fed kernels' pipeline waits (None or < 0:
+        the default); a wait that runs out makes the next synchronising call
+        raise PARATC_ERR_TIMEOUT."""
+        self._check(self._L.paratc_set_wait_limit(self._h, -1 if polls is None else int(polls)),
+                    "paratc_set_wait_limit")
+
     # -- Poisson schedule (InitPoissonSolver's auto-tuning)
     def autotune(self, nrep=15):
         """Times every supported schedule and keeps the fastest: (choice, ms
@@ -481,6 +492,22 @@ class ChannelSystem:
         self._check(self._L.paratc_dump_visu(self._h, res_dir.encode(), run_name.encode(), int(ntime), int(save_mask),
                                              skip[0], skip[1], skip[2], int(bool(node)), int(bool(single))),
                     "paratc_dump_visu")
+
+    def xprofile(self, name="c"):
+        """The field averaged over the depth (dyp weights) and the span, one
+        value per x cell."""
+        out = np.zeros(self.params.nxc)
+        q = {"ux": 0, "uy": 1, "uz": 2, "p": 3, "c": 4}[name]
+        self._check(self._L.paratc_xprofile(self._h, q, _ptr(out)), "paratc_xprofile")
+        return out
+
+    def front_position(self, x_from=1.0, level=0.5):
+        """x where the depth-averaged scalar first drops below `level` to the
+        right of x_from (-1 if nowhere)."""
+        x = ctypes.c_double()
+        self._check(self._L.paratc_front_position(self._h, float(x_from), float(level), ctypes.byref(x)),
+                    "paratc_front_position")
+        return x.value
 
     def project(self):
         dm = ctypes.c_double()

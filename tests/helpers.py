@@ -80,3 +80,30 @@ def discrete_poiseuille(o, params):
     dyp = o.metric("dyp")[1:ny + 1]
     u *= params.ubulk / (np.sum(u * dyp) / params.yly)
     return u
+
+
+def rel_l2(a, b):
+    """||a - b||_2 / ||b||_2, the relative L2 error of a field."""
+    a = np.asarray(a)
+    b = np.asarray(b)
+    return float(np.linalg.norm((a - b).ravel()) / max(np.linalg.norm(b.ravel()), 1e-300))
+
+
+def xprofile(q, dyp, yly):
+    """Depth- and span-averaged x profile of an interior field [nz, ny, nx]:
+    sum over y with the dyp weights, mean over z, divided by yly (the
+    definition paratc_xprofile evaluates on the device)."""
+    return np.einsum("kji,j->i", q, dyp) / q.shape[0] / yly
+
+
+def front_position(prof, dx, x_from=1.0, level=0.5):
+    """First x right of x_from where the profile drops below `level`,
+    interpolated between cell centres (i + 0.5) dx; -1 if nowhere."""
+    for i, v in enumerate(prof):
+        x = (i + 0.5) * dx
+        if x <= x_from or not v < level:
+            continue
+        if i > 0 and x - dx > x_from and prof[i - 1] >= level:
+            return x - dx + (prof[i - 1] - level) / (prof[i - 1] - v) * dx
+        return x
+    return -1.0

@@ -80,6 +80,98 @@ def test_namelist_reader():
     assert ro.backup_freq == 5 and ro.cmd_lfile_freq == 2
 
 
+# The reference's own input decks (copied verbatim by
+# tests/golden/make_reference_inputs.py): every value below is the one
+# written in the file, passed through ReadAndInitParameters'
+# derivations (src/m_Parameters.f90:143-187: nxc = nxp - 1, uxBcValue -= uCRF
+# under IsUseCRF else uCRF = 0, GravityDir normalised, SDiffCoe = xnu/Sc,
+# GravityEffVec = GravityDir*GravityEff, FallingVelVec = GravityDir*FallingVel
+# + (uCRF, 0, 0)).
+REF_INPUTS = {
+    "TurbCha0180_4th.standard": dict(
+        scalar=False, grid=(384, 192, 256), flow_type=1, ischeme=3, icfl=2, is_ux_const=1, xnu=2.3310e-4,
+        dt_max=0.02, cflc=1.5, ubulk=0.666666666666666666666666666667, ucrf=0.0, dom=(12.56637061, 2.0, 6.283185307),
+        limits=(2.0, 0.2), gravity=(0.0, 0.0, 0.0), mesh=([1.0, 1.0], [1.0, 1.0], [96, 96], [2, 2], [0, 1]),
+        run=(1, 27000, 0, 9000, 5, b"Cha180_4th", b"./CFD/Results/", b"./CFD/Restart/"),
+        io=(20, 3000, 3000, 1, ("ux", "uy", "uz"), (1, 20, 20), (1, [10, 20, 30, 40, 50, 60, 70, 80, 90]))),
+    "GravityFlow.prm": dict(
+        scalar=True, grid=(192, 96, 128), flow_type=2, ischeme=3, icfl=1, is_ux_const=0, xnu=4.66591665597541e-04,
+        dt_max=0.015, cflc=1.5, ubulk=1.4352, ucrf=0.0, dom=(12.56637061, 1.0, 4.188790205), limits=(4.0, 0.2),
+        gravity=(0.0, 0.0, 0.0), mesh=([1.0, 1.0], [1.0, 1.0], [48, 48], [2, 2], [0, 1]),
+        sc=dict(schmidt=1.0, geff=16.1865, gdir=(8.71557427476582e-02, -9.961946980917460e-01, 0.0),
+                ws=1.679729996151150e-03, bc=(-3, -3), vals=(3.58630091313028, 3.58630091313028, 0.0, 0.0),
+                init=5.0e-3),
+        run=(1, 40000, 1, 10000, 5, b"TurbidityCurrent", b"./CFD/Results/", b"./CFD/Restart/"),
+        io=(20, 5000, 5000, 1, ("ux", "uy", "uz", "scalar"), (1, 20, 10), (0, [5, 10, 15, 20, 25, 30, 35, 40, 45]))),
+    "GravityFlow.small": dict(
+        scalar=True, grid=(96, 96, 96), flow_type=2, ischeme=3, icfl=1, is_ux_const=0, xnu=4.66591665597541e-04,
+        dt_max=0.03, cflc=1.5, ubulk=1.4352, ucrf=0.0, dom=(12.56637061, 1.0, 4.188790205), limits=(4.0, 0.2),
+        gravity=(0.0, 0.0, 0.0), mesh=([1.0, 1.0], [1.0, 1.0], [48, 48], [2, 2], [0, 1]),
+        sc=dict(schmidt=1.0, geff=16.1865, gdir=(8.71557427476582e-02, -9.961946980917460e-01, 0.0),
+                ws=1.679729996151150e-03, bc=(-3, -3), vals=(3.58630091313028, 3.58630091313028, 0.0, 0.0),
+                init=5.0e-3),
+        run=(1, 200, 0, 10000, 5, b"TurbidityCurrent", b"./CFD/Results/", b"./CFD/Restart/"),
+        io=(10, 50, 5000, 1, (), (1, 10, 10), (0, [5, 10, 15, 20, 25, 30, 35, 40, 45]))),
+    "SF_Ri000.prm": dict(
+        scalar=True, grid=(512, 128, 512), flow_type=1, ischeme=3, icfl=1, is_ux_const=0, xnu=2.3310e-4,
+        dt_max=0.03, cflc=1.7, ubulk=0.65, ucrf=0.6, dom=(25.13274123, 2.0, 12.56637061), limits=None,
+        gravity=(1.760473764e-3, 0.0, 0.0), mesh=([1.0, 1.0], [1.0, 1.0], [64, 64], [2, 2], [0, 1]),
+        sc=dict(schmidt=0.7, geff=0.0, gdir=(0.0, 1.0, 0.0), ws=0.0, bc=(-1, -1), vals=(0.0, 1.0, 0.0, 0.0),
+                init=0.5),
+        run=(1, 60000, 0, 12000, 5, b"Ri000_", b"./CFD/Results1/", b"./CFD/Restart1/"), io=None),
+}
+
+
+@pytest.mark.parametrize("fname", sorted(REF_INPUTS))
+def test_namelist_reader_on_reference_inputs(fname):
+    """paratc_params_from_namelist, paratc_run_options_from_namelist and
+    paratc_io_options_from_namelist read the reference's own input files
+    unchanged and give the values written in them."""
+    ex = REF_INPUTS[fname]
+    path = os.path.join(GOLD, fname)
+    p, yp = lib.params_from_namelist(path, scalar_on=ex["scalar"])
+    assert (p.nxc, p.nyc, p.nzc) == ex["grid"]
+    assert (p.flow_type, p.ischeme, p.icfl, p.is_ux_const) == (ex["flow_type"], ex["ischeme"], ex["icfl"],
+                                                               ex["is_ux_const"])
+    assert p.xnu == ex["xnu"] and p.dt_max == ex["dt_max"] and p.cflc == ex["cflc"] and p.ubulk == ex["ubulk"]
+    assert (p.xlx, p.yly, p.zlz) == ex["dom"] and tuple(p.gravity) == ex["gravity"]
+    assert p.ucrf == ex["ucrf"]
+    assert list(p.ux_bc) == [0.0 - ex["ucrf"]] * 6
+    if ex["limits"]:
+        assert (p.vel_limit, p.div_limit) == ex["limits"]
+    sl, cs, nys, st, so = ex["mesh"]
+    ref = cases.Mesh(sl, cs, nys, st, so)
+    assert np.array_equal(yp, lib.mesh_ycoord(ref, p.yly))
+    assert np.array_equal(yp, ol.ycoord(sl, cs, nys, st, so, p.yly))
+    if ex["scalar"]:
+        s = ex["sc"]
+        g = np.array(s["gdir"])
+        g = g / np.sqrt(g[0] * g[0] + g[1] * g[1] + g[2] * g[2])
+        assert p.sdiff == pytest.approx(ex["xnu"] / s["schmidt"], rel=1e-15)
+        assert np.allclose(list(p.gravity_eff_vec), g * s["geff"], rtol=1e-15, atol=0)
+        fv = g * s["ws"]
+        fv[0] += ex["ucrf"]
+        assert np.allclose(list(p.falling_vel_vec), fv, rtol=1e-15, atol=0)
+        assert tuple(p.scalar_bc_option) == s["bc"] and tuple(p.scalar_bc_values) == s["vals"]
+        assert p.scalar_init_value == s["init"]
+    L = lib.load()
+    ro = abi_run_options()
+    assert L.paratc_run_options_from_namelist(path.encode(), ctypes.byref(ro)) == 0
+    assert (ro.ifirst, ro.ilast, ro.restart_flag, ro.backup_freq, ro.cmd_lfile_freq, ro.run_name, ro.res_dir,
+            ro.restart_dir) == ex["run"]
+    if ex["io"]:
+        ivs, sstat, svisu, skip, saved, sp1, sp2 = ex["io"]
+        o = lib.io_options_from_namelist(path, scalar_on=ex["scalar"])
+        assert (o.ivstats, o.save_stat, o.save_visu) == (ivs, sstat, svisu)
+        assert (o.iskip, o.jskip, o.kskip, o.xdmf_set_type) == (skip, skip, skip, 1)
+        assert o.save_mask == lib.visu_mask(*saved)
+        assert (o.clc_spectra1d, o.iv_spec, o.j_for_lcs) == sp1
+        assert o.clc_spectra2d == sp2[0] and o.ny_spec2d == len(sp2[1])
+        # &Spectra2DOpt is read only when clcSpectra2D is set (src/m_FlowCase.f90:209-214)
+        if sp2[0]:
+            assert list(o.iy_spec2d[:len(sp2[1])]) == sp2[1]
+
+
 class abi_run_options(ctypes.Structure):
     _fields_ = [("ifirst", ctypes.c_int32), ("ilast", ctypes.c_int32), ("restart_flag", ctypes.c_int32),
                 ("backup_freq", ctypes.c_int32), ("cmd_lfile_freq", ctypes.c_int32),
