@@ -291,7 +291,7 @@ void enqueue_substep(paratc_ctx* ctx, int ns, int stop = 5) {
     {
         PROF(PK_RHS);
         launch_rhs_tile(st, ctx->kc, ctx->dm, ctx->d_coef, ctx->f, ctx->d_uy_ym, ctx->d_duy_ym, ns, h.gam[ns - 1],
-                        h.the[ns - 1], h.alp[ns - 1], ctx->d_part, ctx->d_counter);
+                        h.the[ns - 1], h.alp[ns - 1], ctx->d_part, ctx->d_counter, ctx->d_zt_err);
     }
     ctx->launches += 1;
     if (stop == 1) return;
@@ -340,20 +340,21 @@ void diag_out(const DDiag& d, paratc_diag* o) {
 }
 
 int sync(paratc_ctx* ctx) {
-    cudaError_t e = cudaStreamSynchronize(ctx->st);
+    // the error word of the TMA-fed kernels comes back with the same wait:
+    // bit 1 z transform, 2 x transform, 4 divergence-fed transform, 8 the
+    // right-hand side's row pipeline (a bounded wait that ran out)
+    unsigned int* hb = reinterpret_cast<unsigned int*>(ctx->h_scal + 15);
+    *hb = 0u;
+    cudaError_t e = cudaMemcpyAsync(hb, ctx->d_zt_err, sizeof(unsigned int), cudaMemcpyDeviceToHost, ctx->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->st);
     if (e != cudaSuccess) return set_err(ctx, PARATC_ERR_CUDA, std::string("kernel execution: ") + cudaGetErrorString(e));
     e = cudaGetLastError();
     if (e != cudaSuccess) return set_err(ctx, PARATC_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(e));
-    if (ctx->ztma || ctx->xtma) {
-        // a TMA-fed transform whose bounded wait ran out left its flag
-        unsigned int* hb = reinterpret_cast<unsigned int*>(ctx->h_scal);
-        e = cudaMemcpyAsync(hb, ctx->d_zt_err, sizeof(unsigned int), cudaMemcpyDeviceToHost, ctx->st);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->st);
-        if (e != cudaSuccess) return set_err(ctx, PARATC_ERR_CUDA, std::string("error flag: ") + cudaGetErrorString(e));
-        if (*hb) return set_err(ctx, PARATC_ERR_TIMEOUT, (*hb & 1u)   ? "z transform: a TMA wait gave up"
-                                                         : (*hb & 2u) ? "x transform: a TMA wait gave up"
-                                                                      : "divergence transform: a stage wait gave up");
-    }
+    if (*hb)
+        return set_err(ctx, PARATC_ERR_TIMEOUT, (*hb & 1u)   ? "z transform: a TMA wait gave up"
+                                                : (*hb & 2u) ? "x transform: a TMA wait gave up"
+                                                : (*hb & 4u) ? "divergence transform: a stage wait gave up"
+                                                             : "right-hand side: a row copy wait gave up");
     return PARATC_OK;
 }
 
@@ -595,6 +596,16 @@ int paratc_create(const paratc_params* prm, const double* yp, int device, paratc
         for (auto* v : ys) buf.insert(buf.end(), v->begin(), v->end());
         buf.insert(buf.end(), hm.wnx.begin(), hm.wnx.end());
         buf.insert(buf.end(), hm.wnz.begin(), hm.wnz.end());
+        // per-row coefficient records of the right-hand side (DMetric::rowmet),
+        // 16-double aligned in the buffer
+        while (buf.size() % ROWMET) buf.push_back(0.0);
+        const size_t o_rowmet = buf.size();
+        for (size_t j = 0; j < ny1; j++) {
+            const double rec[ROWMET] = {hm.yinterp[j], j + 1 < ny1 ? hm.yinterp[j + 1] : 0.0, hm.rdyp[j], hm.rdyc[j],
+                                        hm.dyp[j], hm.ap2c[j], hm.ac2c[j], hm.am2c[j], hm.ap2p[j], hm.ac2p[j],
+                                        hm.am2p[j], hm.ap2cSc[j], hm.ac2cSc[j], hm.am2cSc[j], 0.0, 0.0};
+            buf.insert(buf.end(), rec, rec + ROWMET);
+        }
         if ((rc = dalloc(ctx, &ctx->d_metric, buf.size()))) { paratc_destroy(ctx); return rc; }
         CK(cudaMemcpyAsync(ctx->d_metric, buf.data(), buf.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->st));
         const double* b = ctx->d_metric;
@@ -605,6 +616,7 @@ int paratc_create(const paratc_params* prm, const double* yp, int device, paratc
         for (size_t a = 0; a < sizeof(dst) / sizeof(dst[0]); a++) *dst[a] = b + a * ny1;
         ctx->dm.wnx = b + ys.size() * ny1;
         ctx->dm.wnz = ctx->dm.wnx + ctx->nx;
+        ctx->dm.rowmet = b + o_rowmet;
         // pivots of the spectral y systems (constant for the life of the context)
         launch_pois_factors(ctx->st, kc, ctx->dm, ctx->d_pfac);
         CK(cudaGetLastError());

@@ -28,7 +28,12 @@ struct DMetric {
     const double *ap2cSc, *ac2cSc, *am2cSc;
     const double *ap2cScCN, *ac2cScCN, *am2cScCN;
     const double *wnx, *wnz;
+    // the coefficients one row j of the right-hand side reads, 16 doubles per
+    // row j = 0..nyp (one 128-byte bulk copy): yinterp(j), yinterp(j+1), rdyp,
+    // rdyc, dyp, ap2c, ac2c, am2c, ap2p, ac2p, am2p, ap2cSc, ac2cSc, am2cSc, 0, 0
+    const double* rowmet;
 };
+constexpr int ROWMET = 16;
 
 // grid sizes and the scalar constants every stencil needs
 struct DConst {

@@ -4,12 +4,19 @@
 // A CTA owns a 32 (x) by 8 (z) column tile and marches up a chunk of y rows.
 // For every row j it needs rows j-1, j, j+1 of ux, uy, uz, p (and the
 // scalar) over the tile plus the x/z halo of 3 cells that the interpolated
-// face velocities and the 4th-order stencils read (38 x 14 values per field
-// and row).  Those row-slabs sit in a ring of 3 + PF slots in shared memory;
-// the slabs of rows j+2 .. j+1+PF are copied in with cp.async while row j is
-// computed, so the HBM loads overlap the arithmetic.  The row's metric
-// coefficients (interpolation weights, 1/dy, the d2/dy2 stencils) travel in
-// the same ring, so no global load sits on a row's dependent path.  Each thread computes
+// face velocities and the 4th-order stencils read.  Those row-slabs
+// (40 x 14 values per field and row: the x range starts 4 cells left of the
+// tile so that every copy starts on a 16-byte boundary) sit in a ring of
+// 3 + PF slots in shared memory.  In FP64 the slabs of rows j+2 .. j+1+PF are
+// brought in by the tensor memory accelerator while row j is computed: one
+// warp issues, per field and z-plane, a bulk copy (cp.async.bulk) of the
+// row's 40-value x range -- split in two where the periodic x range wraps --
+// onto the slot's mbarrier, and every thread waits on that barrier (bounded:
+// a wait that runs out records PARATC_ERR_TIMEOUT's bit 8 in the error word,
+// the CTA drains its copies in flight and stops computing).  The row's metric
+// coefficients (interpolation weights, 1/dy, the d2/dy2 stencils) come as one
+// 128-byte record (DMetric::rowmet) in the same copy group, so no global
+// load sits on a row's dependent path.  Each thread computes
 // two z-adjacent cells per row (FP64; one in the FP32 form): RhsX/RhsY/RhsZ
 // (and RhsC) and the new explicit histories, reading every neighbour from
 // shared memory; the six interpolated fields of the reference and their halo
@@ -33,15 +40,16 @@
 #include "common.cuh"
 #include "kernels.cuh"
 #include "reduce.cuh"
+#include "tma.cuh"
 
 namespace ptc {
 namespace {
 
-constexpr int TX = 32, TZ = 8, HX = 3, HZ = 3;
-constexpr int SX = TX + 2 * HX;  // 38
+constexpr int TX = 32, TZ = 8, HX = 4, HZ = 3;
+constexpr int SX = TX + 2 * HX;  // 40: x offsets -4 .. 35 of the tile (the stencils read -3 .. 34)
 constexpr int SZ = TZ + 2 * HZ;  // 14
-constexpr int SLAB = SX * SZ;    // 532 doubles per field and row
-constexpr int PF = 1;            // FP64: rows loaded ahead beyond row j+1 (cp.async groups in flight)
+constexpr int SLAB = SX * SZ;    // 560 doubles per field and row
+constexpr int PF = 1;            // FP64: rows loaded ahead beyond row j+1 (copy groups in flight)
 // per precision: z-adjacent cells per thread (FP64: 2, whose shared stencil
 // taps then load once; FP32: 1) and threads per CTA
 template <class T>
@@ -57,36 +65,9 @@ constexpr size_t rhs_smem_bytes() {
     return (size_t)RhsCfg<T>::NB * (SCALAR ? 5 : 4) * SLAB * sizeof(T);
 }
 
-__device__ __forceinline__ void cp_async8(double* sdst, const double* gsrc) {
-    const unsigned s = (unsigned)__cvta_generic_to_shared(sdst);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gsrc) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
-
-// the per-row metric coefficients a row of the RHS reads, staged in shared
-// memory with the row slabs so that no global load sits on a row's path:
-// 0 yinterp(j), 1 yinterp(j+1), 2 rdyp, 3 rdyc, 4 dyp, 5-7 ap2c/ac2c/am2c,
-// 8-10 ap2p/ac2p/am2p, 11-13 ap2cSc/ac2cSc/am2cSc (row j)
-constexpr int MSTRIDE = 16;
-__device__ __forceinline__ const double* met_base(const DMetric& m, int q) {
-    switch (q) {
-        case 0: return m.yinterp;
-        case 1: return m.yinterp + 1;
-        case 2: return m.rdyp;
-        case 3: return m.rdyc;
-        case 4: return m.dyp;
-        case 5: return m.ap2c;
-        case 6: return m.ac2c;
-        case 7: return m.am2c;
-        case 8: return m.ap2p;
-        case 9: return m.ac2p;
-        case 10: return m.am2p;
-        case 11: return m.ap2cSc;
-        case 12: return m.ac2cSc;
-        default: return m.am2cSc;
-    }
+// the field a copy reads (f = 0 ux, 1 uy, 2 uz, 3 p, 4 scalar)
+__device__ __forceinline__ const double* field_of(const Fields& fl, int f) {
+    return f == 0 ? fl.ux : f == 1 ? fl.uy : f == 2 ? fl.uz : f == 3 ? fl.pr : fl.sc;
 }
 
 __device__ __forceinline__ int modp(int i, int n) {
@@ -99,20 +80,18 @@ __device__ __forceinline__ int modp(int i, int n) {
 template <bool SCALAR, class T>
 __global__ void __launch_bounds__(RhsCfg<T>::NTHR, RhsCfg<T>::MINB)
     k_rhs_tile(DConst c, DMetric m, DCoef* __restrict__ coef, Fields fl, double* __restrict__ uy_ym,
-               double* __restrict__ duy_ym, int ns, double gam, double the, double alp, int ychunk,
-               double* __restrict__ part, unsigned int* __restrict__ counter) {
+               double* __restrict__ duy_ym, int ns, double gam, double the, double alp, double* __restrict__ part,
+               unsigned int* __restrict__ counter, unsigned int* __restrict__ err) {
     constexpr int NF = SCALAR ? 5 : 4;
     constexpr bool F64 = sizeof(T) == 8;
     constexpr int ZC = RhsCfg<T>::ZC, NTHR = RhsCfg<T>::NTHR, NSLOT = RhsCfg<T>::NSLOT, NB = RhsCfg<T>::NB;
-    // FP64 with the scalar runs at the register limit already; there the
-    // coefficients stay plain loads (staging them spills)
-    constexpr bool MSTAGE = !(SCALAR && F64);
-    constexpr int NMET = MSTAGE ? 11 : 0;
-    extern __shared__ __align__(16) unsigned char sm_raw[];
+    // bytes one FP64 row brings into its slot: NF fields x SZ planes x SX values, and the metric record
+    constexpr unsigned ROW_BYTES = (unsigned)(NF * SZ * SX) * 8u + ROWMET * 8u;
+    extern __shared__ __align__(128) unsigned char sm_raw[];
     T* sm = reinterpret_cast<T*>(sm_raw);  // [NB][NF][SLAB]
-    __shared__ __align__(16) double smet[NB][MSTRIDE];
+    __shared__ __align__(128) double smet[NB][ROWMET];
+    __shared__ unsigned long long bar[NB];
     const int lane = threadIdx.x, wq = threadIdx.y, tid = wq * 32 + lane;
-    const double* mbase = tid < NMET ? met_base(m, tid) : nullptr;
     const int nx = c.nx, nz = c.nz, ny = c.ny;
     const size_t pl = (size_t)c.nyt * nx;
     // work = the (tile, row) pairs in tile-major order; block b takes the
@@ -121,7 +100,13 @@ __global__ void __launch_bounds__(RhsCfg<T>::NTHR, RhsCfg<T>::MINB)
     const int ntx = (nx + TX - 1) / TX, ntz = (nz + TZ - 1) / TZ;
     const long long W = (long long)ntx * ntz * ny;
     const long long gbeg = W * blockIdx.x / gridDim.x, gend = W * (blockIdx.x + 1) / gridDim.x;
-    (void)ychunk;
+    const long long lim = F64 ? tma::wait_limit(err) : 0;
+    if (F64 && tid == 0) {
+#pragma unroll
+        for (int q = 0; q < NB; q++) tma::mbar_init(&bar[q], 1);
+        tma::fence_mbar_init();
+    }
+    __syncthreads();
     pdl_wait();
     pdl_trigger();
 
@@ -143,57 +128,89 @@ __global__ void __launch_bounds__(RhsCfg<T>::NTHR, RhsCfg<T>::MINB)
     const T ucrf = F64 ? (T)c.ucrf : (T)c.fucrf, xnu = F64 ? (T)c.xnu : (T)c.fxnu;
     const T tpG = (T)pmGamma, tpT = (T)pmTheta, tpA = (T)pmAlpha, ttb = (T)tb, ttbs = (T)tbs;
     const T tsdiff = F64 ? (T)c.sdiff : (T)c.fsdiff;
-    const double* fsrc[5] = {fl.ux, fl.uy, fl.uz, fl.pr, fl.sc};
     double s3 = 0.0;
+    // FP64 copy pipeline: phase parity per slot and the slots with a copy
+    // group in flight (the same in every thread: issue and wait decisions are
+    // uniform over the CTA)
+    unsigned phase = 0u, pend = 0u;
+    bool failed = false;
 
-    for (long long g = gbeg; g < gend;) {
+    for (long long g = gbeg; g < gend && !failed;) {
         const int tile = (int)(g / ny);
         const int j0 = (int)(g - (long long)tile * ny) + 1;
         const int j1 = (int)min((long long)ny, (long long)j0 + (gend - g) - 1);
         g += j1 - j0 + 1;
         const int i0 = (tile % ntx) * TX, k0 = (tile / ntx) * TZ;
-        size_t goff[NSLOT];
-        int soff[NSLOT];
-        bool sval[NSLOT];
+        // FP32 form: per-thread slab elements, loaded and converted
+        size_t goff[F64 ? 1 : NSLOT];
+        int soff[F64 ? 1 : NSLOT];
+        bool sval[F64 ? 1 : NSLOT];
+        if constexpr (!F64) {
 #pragma unroll
-        for (int s = 0; s < NSLOT; s++) {
-            const int e = tid + s * NTHR;
-            sval[s] = e < SLAB;
-            const int zz = e / SX, xx = e - zz * SX;
-            goff[s] = (size_t)modp(k0 - HZ + zz, nz) * pl + (size_t)modp(i0 - HX + xx, nx);
-            soff[s] = e;
+            for (int s = 0; s < NSLOT; s++) {
+                const int e = tid + s * NTHR;
+                sval[s] = e < SLAB;
+                const int zz = e / SX, xx = e - zz * SX;
+                goff[s] = (size_t)modp(k0 - HZ + zz, nz) * pl + (size_t)modp(i0 - HX + xx, nx);
+                soff[s] = e;
+            }
         }
-        // FP64: cp.async straight into the ring; FP32: load, convert, store
-#define LOAD_ROW(jrow)                                                                   \
+        // FP64: warp 0 issues the row's bulk copies onto the slot's barrier.
+        // Each (field, z-plane) copies the periodic x range [i0-4, i0+36):
+        // nx is even and i0 a multiple of 32, so every piece starts on an
+        // even index (16-byte aligned) and spans an even count of values.
+        const int x0 = modp(i0 - HX, nx);
+        auto issue_row = [&](int jrow) {
+            const int sl = jrow % NB;
+            pend |= 1u << sl;
+            if (wq != 0) return;
+            if (lane == 0) tma::mbar_expect_tx(&bar[sl], ROW_BYTES);
+            __syncwarp();
+            double* dst = reinterpret_cast<double*>(sm) + (size_t)sl * NF * SLAB;
+            for (int q = lane; q < NF * SZ; q += 32) {
+                const int f = q / SZ, zz = q - f * SZ;
+                const double* src = field_of(fl, f) + (size_t)modp(k0 - HZ + zz, nz) * pl + (size_t)jrow * nx;
+                double* d = dst + f * SLAB + zz * SX;
+                int x = x0, col = 0;
+                while (col < SX) {
+                    const int len = min(SX - col, nx - x);
+                    tma::bulk_load(d + col, src + x, (unsigned)len * 8u, &bar[sl]);
+                    col += len;
+                    x = 0;
+                }
+            }
+            if (lane == 0) tma::bulk_load(smet[sl], m.rowmet + (size_t)jrow * ROWMET, ROWMET * 8u, &bar[sl]);
+        };
+        // every thread waits for the row's copies; the CTA stops as one when
+        // any thread's wait ran out
+        auto wait_row = [&](int jrow) -> bool {
+            const int sl = jrow % NB;
+            const bool ok = tma::mbar_wait(&bar[sl], (phase >> sl) & 1u, lim);
+            if (__syncthreads_or(ok ? 0 : 1)) return false;
+            phase ^= 1u << sl;
+            pend &= ~(1u << sl);
+            return true;
+        };
+        // FP32: load, convert, store
+#define LOAD_ROW32(jrow)                                                                 \
     do {                                                                                 \
         T* dst_ = sm + (size_t)((jrow) % NB) * NF * SLAB;                                \
         const size_t ro_ = (size_t)(jrow) * nx;                                          \
         _Pragma("unroll") for (int f_ = 0; f_ < NF; f_++)                                \
-            _Pragma("unroll") for (int s_ = 0; s_ < NSLOT; s_++) if (sval[s_]) {         \
-                if constexpr (F64)                                                       \
-                    cp_async8(reinterpret_cast<double*>(dst_) + f_ * SLAB + soff[s_],    \
-                              fsrc[f_] + goff[s_] + ro_);                                \
-                else                                                                     \
-                    dst_[f_ * SLAB + soff[s_]] = (T)__ldg(fsrc[f_] + goff[s_] + ro_);    \
-            }                                                                            \
-        if (tid < NMET && (jrow) >= 1 && (jrow) <= ny) {                                 \
-            if constexpr (F64) cp_async8(&smet[(jrow) % NB][tid], mbase + (jrow));       \
-            else smet[(jrow) % NB][tid] = __ldg(mbase + (jrow));                         \
-        }                                                                                \
+            _Pragma("unroll") for (int s_ = 0; s_ < NSLOT; s_++) if (sval[s_])           \
+                dst_[f_ * SLAB + soff[s_]] = (T)__ldg(field_of(fl, f_) + goff[s_] + ro_); \
+        if (tid < ROWMET) smet[(jrow) % NB][tid] = __ldg(m.rowmet + (size_t)(jrow) * ROWMET + tid); \
     } while (0)
 
-        LOAD_ROW(j0 - 1);
-        LOAD_ROW(j0);
-        LOAD_ROW(j0 + 1);
         if constexpr (F64) {
-            cp_async_commit();
-            // rows j0+2 .. j0+PF, one commit group each
-#pragma unroll
-            for (int d = 2; d <= PF; d++) {
-                if (j0 + d <= j1 + 1) LOAD_ROW(j0 + d);
-                cp_async_commit();
-            }
+            // rows j0-1 .. j0+1+PF (those that exist), then rows j0-1 and j0 in place
+            for (int d = -1; d <= 1 + PF; d++)
+                if (j0 + d <= j1 + 1) issue_row(j0 + d);
+            if (!wait_row(j0 - 1) || !wait_row(j0)) { failed = true; break; }
         } else {
+            LOAD_ROW32(j0 - 1);
+            LOAD_ROW32(j0);
+            LOAD_ROW32(j0 + 1);
             __syncthreads();
         }
 
@@ -230,19 +247,21 @@ __global__ void __launch_bounds__(RhsCfg<T>::NTHR, RhsCfg<T>::MINB)
         for (int j = j0; j <= j1; j++) {
             // FP32 form: row j+2 in registers now, converted and stored after
             // the arithmetic of row j
-            double pre[NF][NSLOT];
+            double pre[F64 ? 1 : NF][F64 ? 1 : NSLOT];
             double mpre = 0.0;
             const bool more = j + 2 <= j1 + 1;
             if constexpr (F64) {
-                if (j + 1 + PF <= j1 + 1) LOAD_ROW(j + 1 + PF);
-                cp_async_commit();
+                // the slot of row j+1+PF was last read by row j-1's arithmetic,
+                // which every thread finished at the barrier closing it
+                if (j > j0 && j + 1 + PF <= j1 + 1) issue_row(j + 1 + PF);
             } else if (more) {
                 const size_t ro = (size_t)(j + 2) * nx;
 #pragma unroll
                 for (int f = 0; f < NF; f++)
 #pragma unroll
-                    for (int sl = 0; sl < NSLOT; sl++) pre[f][sl] = sval[sl] ? __ldg(fsrc[f] + goff[sl] + ro) : 0.0;
-                if (tid < NMET && j + 2 <= ny) mpre = __ldg(mbase + j + 2);
+                    for (int sl = 0; sl < NSLOT; sl++)
+                        pre[f][sl] = sval[sl] ? __ldg(field_of(fl, f) + goff[sl] + ro) : 0.0;
+                if (tid < ROWMET) mpre = __ldg(m.rowmet + (size_t)(j + 2) * ROWMET + tid);
             }
             double hx0a[ZC], hy0a[ZC], hz0a[ZC], hc0a[ZC];
             size_t q0a[ZC];
@@ -261,8 +280,7 @@ __global__ void __launch_bounds__(RhsCfg<T>::NTHR, RhsCfg<T>::MINB)
             for (int cz = 0; cz < ZC; cz++)
                 u64n[cz] = (!F64 && act[cz] && j + 2 <= ny + 1) ? __ldg(&fl.ux[q0a[cz] + 2 * nx]) : 0.0;
             if constexpr (F64) {
-                cp_async_wait<PF>();  // the group holding row j+1 is complete
-                __syncthreads();
+                if (!wait_row(j + 1)) { failed = true; break; }
             }
             // both cells are computed before any global store, so that the
             // compiler may load a tap the two cells share once
@@ -274,12 +292,12 @@ __global__ void __launch_bounds__(RhsCfg<T>::NTHR, RhsCfg<T>::MINB)
 #define V(S, f, dx, dz) (S)[(f) * SLAB + (w + HZ + (dz)) * SX + (lane + HX + (dx))]
             const bool top = (j == ny);
             const double* M = smet[j % NB];
-#define MET(q, arr) (MSTAGE ? M[q] : __ldg(&m.arr[j]))
-            const double IY1d = MET(0, yinterp), IY3d = MSTAGE ? M[1] : __ldg(&m.yinterp[j + 1]);
+#define MET(q) M[q]
+            const double IY1d = MET(0), IY3d = MET(1);
             const T IY1 = (T)IY1d, IY2 = (T)(1.0 - IY1d), IY3 = (T)IY3d, IY4 = (T)(1.0 - IY3d);
-            const T rdyp = (T)MET(2, rdyp), rdyc = (T)MET(3, rdyc);
-            const double dyp = MET(4, dyp);
-            const T ap2c = (T)MET(5, ap2c), ac2c = (T)MET(6, ac2c), am2c = (T)MET(7, am2c);
+            const T rdyp = (T)MET(2), rdyc = (T)MET(3);
+            const double dyp = MET(4);
+            const T ap2c = (T)MET(5), ac2c = (T)MET(6), am2c = (T)MET(7);
 #pragma unroll
             for (int cz = 0; cz < ZC; cz++) {
             const int w = wq * ZC + cz;
@@ -318,7 +336,7 @@ __global__ void __launch_bounds__(RhsCfg<T>::NTHR, RhsCfg<T>::MINB)
                     if (act[cz]) s3 += SCALAR ? uxc * dyp : (dcq13 + d22) * dyp;
                 } else if (act[cz]) {
                     s3 += SCALAR ? u64c[cz] * dyp
-                                 : (MET(5, ap2c) * u64p[cz] + MET(6, ac2c) * u64c[cz] + MET(7, am2c) * u64m[cz]) * dyp;
+                                 : (MET(5) * u64p[cz] + MET(6) * u64c[cz] + MET(7) * u64m[cz]) * dyp;
                 }
                 conv_x = -h11 - h12 - h13 + xnu * dcq13 + grav(0);
                 const T gradp = dxC(0) * V(Sc, 3, -2, 0) + dxC(1) * V(Sc, 3, -1, 0) + dxC(2) * V(Sc, 3, 0, 0) + dxC(3) * V(Sc, 3, 1, 0);
@@ -342,7 +360,7 @@ __global__ void __launch_bounds__(RhsCfg<T>::NTHR, RhsCfg<T>::MINB)
                 const T vp = V(Sp, 1, 0, 0), vc = V(Sc, 1, 0, 0), vm = V(Sm, 1, 0, 0);
                 const T h22 = ((vp + vc) * (vp + vc) - (vc + vm) * (vc + vm)) * qsucac;
                 const T d11 = dxxC(0) * V(Sc, 1, -2, 0) + dxxC(1) * V(Sc, 1, -1, 0) + dxxC(2) * vc + dxxC(3) * V(Sc, 1, 1, 0) + dxxC(4) * V(Sc, 1, 2, 0);
-                const T d22 = (T)MET(8, ap2p) * vp + (T)MET(9, ac2p) * vc + (T)MET(10, am2p) * vm;
+                const T d22 = (T)MET(8) * vp + (T)MET(9) * vc + (T)MET(10) * vm;
                 const T d33 = dzzC(0) * V(Sc, 1, 0, -2) + dzzC(1) * V(Sc, 1, 0, -1) + dzzC(2) * vc + dzzC(3) * V(Sc, 1, 0, 1) + dzzC(4) * V(Sc, 1, 0, 2);
                 conv_y = -h21 - h22 - h23 + xnu * (d11 + d33) + grav(1);
                 const T gradp = (V(Sc, 3, 0, 0) - V(Sm, 3, 0, 0)) * rdyc;
@@ -401,7 +419,7 @@ __global__ void __launch_bounds__(RhsCfg<T>::NTHR, RhsCfg<T>::MINB)
                 conv_z = conv_z + c3;
                 const T hc2 = ((V(Sp, 1, 0, 0) + fvv(1)) * shyp - (V(Sc, 1, 0, 0) + fvv(1)) * shyc) * rdyp;
                 const T d11 = dxxC(0) * V(Sc, 4, -2, 0) + dxxC(1) * V(Sc, 4, -1, 0) + dxxC(2) * scc + dxxC(3) * V(Sc, 4, 1, 0) + dxxC(4) * V(Sc, 4, 2, 0);
-                const T d22 = (T)__ldg(&m.ap2cSc[j]) * scjp + (T)__ldg(&m.ac2cSc[j]) * scc + (T)__ldg(&m.am2cSc[j]) * scjm;
+                const T d22 = (T)MET(11) * scjp + (T)MET(12) * scc + (T)MET(13) * scjm;
                 const T d33 = dzzC(0) * V(Sc, 4, 0, -2) + dzzC(1) * V(Sc, 4, 0, -1) + dzzC(2) * scc + dzzC(3) * V(Sc, 4, 0, 1) + dzzC(4) * V(Sc, 4, 0, 2);
                 const T convc = -hc1 - hc2 - hc3 + tsdiff * (d11 + d33);
                 o_rc[cz] = tpG * convc + tpT * hc0 + ttbs * d22;
@@ -436,16 +454,24 @@ __global__ void __launch_bounds__(RhsCfg<T>::NTHR, RhsCfg<T>::MINB)
 #pragma unroll
                         for (int sl = 0; sl < NSLOT; sl++)
                             if (sval[sl]) dst[f * SLAB + soff[sl]] = (T)pre[f][sl];
-                    if (tid < NMET && j + 2 <= ny) smet[(j + 2) % NB][tid] = mpre;
+                    if (tid < ROWMET) smet[(j + 2) % NB][tid] = mpre;
                 }
 #pragma unroll
                 for (int cz = 0; cz < ZC; cz++) { u64m[cz] = u64c[cz]; u64c[cz] = u64p[cz]; u64p[cz] = u64n[cz]; }
             }
         __syncthreads();
         }
-#undef LOAD_ROW
+#undef LOAD_ROW32
     }
-    if constexpr (F64) cp_async_wait<0>();
+    if constexpr (F64) {
+        if (failed && tid == 0) {
+            atomicOr(err, 8u);
+            // copies still in flight land in this CTA's slots: wait for them
+            // (full limit) before the CTA can end
+            for (int q = 0; q < NB; q++)
+                if (pend & (1u << q)) tma::mbar_wait(&bar[q], (phase >> q) & 1u);
+        }
+    }
 #undef KC
 #undef dxC
 #undef dzC
@@ -493,14 +519,6 @@ __global__ void __launch_bounds__(RhsCfg<T>::NTHR, RhsCfg<T>::MINB)
 }
 
 // ---------------------------------------------------------------------------
-static int rhs_ychunk(const DConst& c) {
-    const int nxz = ((c.nx + TX - 1) / TX) * ((c.nz + TZ - 1) / TZ);
-    int nch = (4 * 148 + nxz - 1) / nxz;
-    if (nch > c.ny / 4) nch = c.ny / 4;
-    if (nch < 1) nch = 1;
-    return (c.ny + nch - 1) / nch;
-}
-
 // one wave of resident CTAs (MINB per SM for the precision; the record
 // count is sized for the larger)
 static size_t rhs_blocks(const DConst& c, int minb) {
@@ -522,21 +540,23 @@ void rhs_init() {
 
 template <bool SCALAR, class T>
 static void launch_rhs_t(cudaStream_t st, const DConst& c, const DMetric& m, DCoef* coef, const Fields& f, double* uy_ym,
-                         double* duy_ym, int ns, double gam, double the, double alp, double* part, unsigned int* counter) {
+                         double* duy_ym, int ns, double gam, double the, double alp, double* part, unsigned int* counter,
+                         unsigned int* err) {
     const dim3 grd((unsigned)rhs_blocks(c, RhsCfg<T>::MINB));
     const dim3 blk(32, TZ / RhsCfg<T>::ZC);
     launch_pdl(k_rhs_tile<SCALAR, T>, grd, blk, rhs_smem_bytes<SCALAR, T>(), st, c, m, coef, f, uy_ym, duy_ym, ns, gam,
-               the, alp, rhs_ychunk(c), part, counter);
+               the, alp, part, counter, err);
 }
 
 void launch_rhs_tile(cudaStream_t st, const DConst& c, const DMetric& m, DCoef* coef, const Fields& f, double* uy_ym,
-                     double* duy_ym, int ns, double gam, double the, double alp, double* part, unsigned int* counter) {
+                     double* duy_ym, int ns, double gam, double the, double alp, double* part, unsigned int* counter,
+                     unsigned int* err) {
     if (c.fp32_rhs) {
-        if (c.scalar_on) launch_rhs_t<true, float>(st, c, m, coef, f, uy_ym, duy_ym, ns, gam, the, alp, part, counter);
-        else launch_rhs_t<false, float>(st, c, m, coef, f, uy_ym, duy_ym, ns, gam, the, alp, part, counter);
+        if (c.scalar_on) launch_rhs_t<true, float>(st, c, m, coef, f, uy_ym, duy_ym, ns, gam, the, alp, part, counter, err);
+        else launch_rhs_t<false, float>(st, c, m, coef, f, uy_ym, duy_ym, ns, gam, the, alp, part, counter, err);
     } else {
-        if (c.scalar_on) launch_rhs_t<true, double>(st, c, m, coef, f, uy_ym, duy_ym, ns, gam, the, alp, part, counter);
-        else launch_rhs_t<false, double>(st, c, m, coef, f, uy_ym, duy_ym, ns, gam, the, alp, part, counter);
+        if (c.scalar_on) launch_rhs_t<true, double>(st, c, m, coef, f, uy_ym, duy_ym, ns, gam, the, alp, part, counter, err);
+        else launch_rhs_t<false, double>(st, c, m, coef, f, uy_ym, duy_ym, ns, gam, the, alp, part, counter, err);
     }
 }
 

@@ -53,8 +53,10 @@ void launch_endstep(cudaStream_t st, const DConst& c, const DMetric& m, const Fi
 // k_rhs.cu
 size_t rhs_grid_blocks(const DConst& c);
 void rhs_init();
+// err: the context's error word (bit 8: a row wait of the FP64 copy pipeline gave up; err[1]: the test poll limit)
 void launch_rhs_tile(cudaStream_t st, const DConst& c, const DMetric& m, DCoef* coef, const Fields& f, double* uy_ym,
-                     double* duy_ym, int ns, double gam, double the, double alp, double* part, unsigned int* counter);
+                     double* duy_ym, int ns, double gam, double the, double alp, double* part, unsigned int* counter,
+                     unsigned int* err);
 
 // k_tridiag.cu
 int tridiag_partitions(int ny);
