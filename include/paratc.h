@@ -283,11 +283,12 @@ int paratc_diagnostics(paratc_ctx* ctx, paratc_diag* diag);
  * in the reference; it is the depth-averaged concentration from which a
  * gravity current's front is read. */
 int paratc_xprofile(paratc_ctx* ctx, int field, double* out);
-/* Front of a gravity current: the x to the right of x_from (the lock) where
- * the depth-averaged scalar first falls below `level` (0.5 for a lock
- * release), interpolated linearly between the cell centres (ic-0.5)*dx;
- * -1 when it nowhere does.  Not in the reference (a builder-defined
- * diagnostic of the lock-exchange case). */
+/* Front (nose) of a gravity current released from a lock ending at x_from:
+ * the furthest cell centre (ic-0.5)*dx to the right of x_from, within half
+ * the periodic domain, where the depth-averaged scalar is at least `level`,
+ * moved to the level's linear crossing between that cell and the next;
+ * -1 when no cell there reaches `level`.  Not in the reference (a
+ * builder-defined diagnostic of the lock-exchange case). */
 int paratc_front_position(paratc_ctx* ctx, double x_from, double level, double* x_front);
 
 /* ---- restart files (src/m_IOAndVisu.f90:408-512) ----------------------- */

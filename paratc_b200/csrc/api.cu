@@ -1040,18 +1040,21 @@ int paratc_front_position(paratc_ctx* ctx, double x_from, double level, double* 
     std::vector<double> prof(ctx->nx);
     int rc = paratc_xprofile(ctx, 4, prof.data());
     if (rc) return rc;
-    const double dx = ctx->prm.xlx / ctx->nx;
+    // the nose: the furthest cell centre right of x_from, within half the
+    // periodic domain, whose depth average is at least `level`, and the
+    // linear crossing of the level between it and the next cell
+    const int nx = ctx->nx;
+    const double dx = ctx->prm.xlx / nx;
     *x_front = -1.0;
-    for (int i = 0; i < ctx->nx; i++) {
-        const double x = (i + 0.5) * dx;  // the scalar's cell centres
-        if (x <= x_from || !(prof[i] < level)) continue;
-        const double xm = x - dx;
-        if (i > 0 && xm > x_from && prof[i - 1] >= level)
-            *x_front = xm + (prof[i - 1] - level) / (prof[i - 1] - prof[i]) * dx;
-        else
-            *x_front = x;
-        break;
+    int last = -1;
+    for (int i = 0; i < nx; i++) {
+        const double x = (i + 0.5) * dx;
+        if (x > x_from && x < x_from + 0.5 * ctx->prm.xlx && prof[i] >= level) last = i;
     }
+    if (last < 0) return PARATC_OK;
+    const double xl = (last + 0.5) * dx;
+    const double pn = prof[(last + 1) % nx];
+    *x_front = pn < level ? xl + (prof[last] - level) / (prof[last] - pn) * dx : xl;
     return PARATC_OK;
 }
 

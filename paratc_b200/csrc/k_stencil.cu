@@ -19,9 +19,10 @@ namespace ptc {
 // clcPrSrc (src/m_TScheme.f90:48-77) / CheckDivergence (src/m_Tools.f90:54-81)
 // src is the compact interior array (k, j-1, i); scale = 1/pmAlpha, or 1
 // ---------------------------------------------------------------------------
+template <class V>
 __global__ void __launch_bounds__(256) k_prsrc(DConst c, DMetric m, const DCoef* __restrict__ coef, int unit_scale,
-                                               const double* __restrict__ ux, const double* __restrict__ uy,
-                                               const double* __restrict__ uz, double* __restrict__ src,
+                                               const V* __restrict__ ux, const V* __restrict__ uy,
+                                               const V* __restrict__ uz, double* __restrict__ src,
                                                double* __restrict__ part) {
     const int nx = c.nx;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -59,9 +60,10 @@ __global__ void k_reduce_max(const double* __restrict__ part, int nparts, double
 // (src/m_TScheme.f90:82-107,512-532; src/m_BC_and_Halo.f90:23-64,108-122)
 // mode 0: substep; mode 1: pressure-free projection (alpha = 1, p untouched)
 // ---------------------------------------------------------------------------
+template <class V>
 __global__ void __launch_bounds__(256) k_project(DConst c, DMetric m, const DCoef* __restrict__ coef, int mode,
-                                                 const double* __restrict__ phi, double* __restrict__ ux,
-                                                 double* __restrict__ uy, double* __restrict__ uz,
+                                                 const V* __restrict__ phi, V* __restrict__ ux,
+                                                 V* __restrict__ uy, V* __restrict__ uz,
                                                  double* __restrict__ pr, const double* __restrict__ uy_ym) {
     const int nx = c.nx;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -75,7 +77,7 @@ __global__ void __launch_bounds__(256) k_project(DConst c, DMetric m, const DCoe
     const int is = wrapi(i - 2, nx), im = wrapi(i - 1, nx), ip = wrapi(i + 1, nx);
     const size_t zs = (size_t)wrapi(k - 2, c.nz) * pl, zm = (size_t)wrapi(k - 1, c.nz) * pl, zp = (size_t)wrapi(k + 1, c.nz) * pl;
     const size_t q = zc + r0 + i;
-    const double pc = LD(phi, q), pjm = LD(phi, q - nx), pjp = LD(phi, q + nx);
+    const double pc = LD(phi, q), pjm = LD(phi, q - nx), pjp = LD(phi, q + nx);  // in FP64 from either storage
     const double dpdx = c.dxC[0] * LD(phi, zc + r0 + is) + c.dxC[1] * LD(phi, zc + r0 + im) + c.dxC[2] * pc + c.dxC[3] * LD(phi, zc + r0 + ip);
     const double dpdy = (pc - pjm) * __ldg(&m.rdyc[jc]);
     const double dpdz = c.dzC[0] * LD(phi, zs + r0 + i) + c.dzC[1] * LD(phi, zm + r0 + i) + c.dzC[2] * pc + c.dzC[3] * LD(phi, zp + r0 + i);
@@ -112,8 +114,9 @@ __global__ void __launch_bounds__(256) k_project(DConst c, DMetric m, const DCoe
 // ghost rows from the interior: SetBC_and_UpdateHalo, _pr and _scalar
 // (src/m_BC_and_Halo.f90:23-178); one thread per (i, k)
 // ---------------------------------------------------------------------------
-__global__ void k_bc_all(DConst c, double* __restrict__ ux, double* __restrict__ uy, double* __restrict__ uz,
-                         double* __restrict__ pr, double* __restrict__ sc, const double* __restrict__ uy_ym) {
+template <class V>
+__global__ void k_bc_all(DConst c, V* __restrict__ ux, V* __restrict__ uy, V* __restrict__ uz,
+                         double* __restrict__ pr, V* __restrict__ sc, const double* __restrict__ uy_ym) {
     const int nx = c.nx;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int k = blockIdx.y;
@@ -121,17 +124,17 @@ __global__ void k_bc_all(DConst c, double* __restrict__ ux, double* __restrict__
     const size_t pl = (size_t)c.nyt * nx, zc = (size_t)k * pl;
     const size_t g0 = zc + i, r1 = zc + nx + i, rn = zc + (size_t)c.ny * nx + i, gt = zc + (size_t)c.nyp * nx + i;
     const bool ft_ch = (c.flow_type == 1);
-    ux[gt] = ft_ch ? c.uxbc_yp * 2.0 - ux[rn] : ux[rn];
-    uy[gt] = ft_ch ? c.uybc_yp : 0.0;
-    uz[gt] = ft_ch ? c.uzbc_yp * 2.0 - uz[rn] : uz[rn];
-    ux[g0] = c.uxbc_ym * 2.0 - ux[r1];
-    uy[r1] = uy_ym[(size_t)k * nx + i];
-    uz[g0] = c.uzbc_ym * 2.0 - uz[r1];
+    ux[gt] = (V)(ft_ch ? c.uxbc_yp * 2.0 - (double)ux[rn] : (double)ux[rn]);
+    uy[gt] = (V)(ft_ch ? c.uybc_yp : 0.0);
+    uz[gt] = (V)(ft_ch ? c.uzbc_yp * 2.0 - (double)uz[rn] : (double)uz[rn]);
+    ux[g0] = (V)(c.uxbc_ym * 2.0 - (double)ux[r1]);
+    uy[r1] = (V)uy_ym[(size_t)k * nx + i];
+    uz[g0] = (V)(c.uzbc_ym * 2.0 - (double)uz[r1]);
     pr[g0] = pr[r1];
     pr[gt] = pr[rn];
     if (c.scalar_on && sc) {
-        sc[g0] = c.sc_r1b * sc[r1] + c.sc_r2b;
-        sc[gt] = c.sc_r1t * sc[rn] + c.sc_r2t;
+        sc[g0] = (V)(c.sc_r1b * (double)sc[r1] + c.sc_r2b);
+        sc[gt] = (V)(c.sc_r1t * (double)sc[rn] + c.sc_r2t);
     }
 }
 
@@ -148,8 +151,9 @@ __global__ void k_update_uy_ym(int n, double* __restrict__ uy_ym, double* __rest
 // CalcMaxCFL (src/m_Tools.f90:24-49) and the dt choice of ChannelIterate
 // (src/m_ChannelSystem.f90:93-100)
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_cfl(DConst c, DMetric m, const double* __restrict__ ux,
-                                             const double* __restrict__ uy, const double* __restrict__ uz,
+template <class V>
+__global__ void __launch_bounds__(256) k_cfl(DConst c, DMetric m, const V* __restrict__ ux,
+                                             const V* __restrict__ uy, const V* __restrict__ uz,
                                              double* __restrict__ part) {
     const int nx = c.nx;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -199,9 +203,10 @@ __global__ void k_cfl_final(DConst c, DCoef* coef, const double* __restrict__ pa
 constexpr int ENDSTEP_THREADS = 256;
 constexpr int ENDSTEP_U = 4;
 
+template <class V>
 __global__ void __launch_bounds__(ENDSTEP_THREADS, 2)
-    k_endstep(DConst c, DMetric m, const double* __restrict__ ux, const double* __restrict__ uy,
-              const double* __restrict__ uz, const double* __restrict__ sc, DCoef* __restrict__ coef,
+    k_endstep(DConst c, DMetric m, const V* __restrict__ ux, const V* __restrict__ uy,
+              const V* __restrict__ uz, const V* __restrict__ sc, DCoef* __restrict__ coef,
               DDiag* __restrict__ diag, double* __restrict__ part, unsigned int* __restrict__ counter, int next) {
     const int nx = c.nx, ny = c.ny, nz = c.nz;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -215,12 +220,12 @@ __global__ void __launch_bounds__(ENDSTEP_THREADS, 2)
         const int k = r / ny, jc = r - k * ny + 1;
         const int km = k == 0 ? nz - 1 : k - 1, kp = k == nz - 1 ? 0 : k + 1, ku = kp == nz - 1 ? 0 : kp + 1;
         const size_t r0 = (size_t)jc * nx;
-        const double* ur = ux + (size_t)k * pl + r0;
-        const double* vr = uy + (size_t)k * pl + r0;
-        const double* w1 = uz + (size_t)k * pl + r0;
-        const double* w0 = uz + (size_t)km * pl + r0;
-        const double* w2 = uz + (size_t)kp * pl + r0;
-        const double* w3 = uz + (size_t)ku * pl + r0;
+        const V* ur = ux + (size_t)k * pl + r0;
+        const V* vr = uy + (size_t)k * pl + r0;
+        const V* w1 = uz + (size_t)k * pl + r0;
+        const V* w0 = uz + (size_t)km * pl + r0;
+        const V* w2 = uz + (size_t)kp * pl + r0;
+        const V* w3 = uz + (size_t)ku * pl + r0;
         const double rdyp = __ldg(&m.rdyp[jc]), dy = __ldg(&m.dyp[jc]);
         // ENDSTEP_U cells per lane with every load issued before the arithmetic
         for (int i0 = 0; i0 < nx; i0 += 32 * ENDSTEP_U) {
@@ -328,11 +333,12 @@ __global__ void __launch_bounds__(ENDSTEP_THREADS, 2)
 // thread per (i, k) sums its column over j in order; the second kernel adds
 // the nz columns of an i in order, so the result is deterministic.
 // ---------------------------------------------------------------------------
-__global__ void k_xprof_part(DConst c, DMetric m, const double* __restrict__ q, double* __restrict__ part) {
+template <class V>
+__global__ void k_xprof_part(DConst c, DMetric m, const V* __restrict__ q, double* __restrict__ part) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int k = blockIdx.y;
     if (i >= c.nx) return;
-    const double* col = q + (size_t)k * c.nyt * c.nx + i;
+    const V* col = q + (size_t)k * c.nyt * c.nx + i;
     double s = 0.0;
     for (int j = 1; j <= c.ny; j++) s += __ldg(&col[(size_t)j * c.nx]) * __ldg(&m.dyp[j]);
     part[(size_t)k * c.nx + i] = s;
@@ -361,43 +367,78 @@ size_t cell_grid_blocks(const DConst& c) {
     return (size_t)g.x * g.y * g.z;
 }
 
+template <class V>
+static void prsrc_t(cudaStream_t st, const DConst& c, const DMetric& m, const DCoef* coef, int unit_scale,
+                    const FieldSet<V>& f, double* src, double* part, double* out_max) {
+    k_prsrc<V><<<cell_grid(c), cell_block(), 0, st>>>(c, m, coef, unit_scale, f.ux, f.uy, f.uz, src, part);
+    k_reduce_max<<<1, 1024, 0, st>>>(part, (int)cell_grid_blocks(c), out_max);
+}
 void launch_prsrc(cudaStream_t st, const DConst& c, const DMetric& m, const DCoef* coef, int unit_scale,
                   const Fields& f, double* src, double* part, double* out_max) {
-    k_prsrc<<<cell_grid(c), cell_block(), 0, st>>>(c, m, coef, unit_scale, f.ux, f.uy, f.uz, src, part);
-    k_reduce_max<<<1, 1024, 0, st>>>(part, (int)cell_grid_blocks(c), out_max);
+    prsrc_t(st, c, m, coef, unit_scale, f, src, part, out_max);
+}
+void launch_prsrc(cudaStream_t st, const DConst& c, const DMetric& m, const DCoef* coef, int unit_scale,
+                  const Fields32& f, double* src, double* part, double* out_max) {
+    prsrc_t(st, c, m, coef, unit_scale, f, src, part, out_max);
 }
 
 void launch_store_divsrc(cudaStream_t st, DCoef* coef, const double* v) { k_store_divsrc<<<1, 32, 0, st>>>(coef, v); }
 
 void launch_project(cudaStream_t st, const DConst& c, const DMetric& m, const DCoef* coef, int mode, const double* phi,
                     const Fields& f, const double* uy_ym) {
-    launch_pdl(k_project, cell_grid(c), cell_block(), 0, st, c, m, coef, mode, phi, f.ux, f.uy, f.uz, f.pr, uy_ym);
+    launch_pdl(k_project<double>, cell_grid(c), cell_block(), 0, st, c, m, coef, mode, phi, f.ux, f.uy, f.uz, f.pr, uy_ym);
+}
+void launch_project(cudaStream_t st, const DConst& c, const DMetric& m, const DCoef* coef, int mode, const float* phi,
+                    const Fields32& f, const double* uy_ym) {
+    launch_pdl(k_project<float>, cell_grid(c), cell_block(), 0, st, c, m, coef, mode, phi, f.ux, f.uy, f.uz, f.pr, uy_ym);
 }
 
 void launch_bc_all(cudaStream_t st, const DConst& c, const Fields& f, const double* uy_ym) {
-    k_bc_all<<<dim3((c.nx + 127) / 128, c.nz), 128, 0, st>>>(c, f.ux, f.uy, f.uz, f.pr, f.sc, uy_ym);
+    k_bc_all<double><<<dim3((c.nx + 127) / 128, c.nz), 128, 0, st>>>(c, f.ux, f.uy, f.uz, f.pr, f.sc, uy_ym);
+}
+void launch_bc_all(cudaStream_t st, const DConst& c, const Fields32& f, const double* uy_ym) {
+    k_bc_all<float><<<dim3((c.nx + 127) / 128, c.nz), 128, 0, st>>>(c, f.ux, f.uy, f.uz, f.pr, f.sc, uy_ym);
 }
 
 void launch_update_uy_ym(cudaStream_t st, int n, double* uy_ym, double* duy_ym) {
     k_update_uy_ym<<<(n + 255) / 256, 256, 0, st>>>(n, uy_ym, duy_ym);
 }
 
-void launch_cfl(cudaStream_t st, const DConst& c, const DMetric& m, const Fields& f, DCoef* coef, double* part) {
-    k_cfl<<<cell_grid(c), cell_block(), 0, st>>>(c, m, f.ux, f.uy, f.uz, part);
+template <class V>
+static void cfl_t(cudaStream_t st, const DConst& c, const DMetric& m, const FieldSet<V>& f, DCoef* coef, double* part) {
+    k_cfl<V><<<cell_grid(c), cell_block(), 0, st>>>(c, m, f.ux, f.uy, f.uz, part);
     k_cfl_final<<<1, 1024, 0, st>>>(c, coef, part, (int)cell_grid_blocks(c));
 }
+void launch_cfl(cudaStream_t st, const DConst& c, const DMetric& m, const Fields& f, DCoef* coef, double* part) {
+    cfl_t(st, c, m, f, coef, part);
+}
+void launch_cfl(cudaStream_t st, const DConst& c, const DMetric& m, const Fields32& f, DCoef* coef, double* part) {
+    cfl_t(st, c, m, f, coef, part);
+}
 
-void launch_xprofile(cudaStream_t st, const DConst& c, const DMetric& m, const double* q, double* part, double* out) {
-    k_xprof_part<<<dim3((c.nx + 127) / 128, c.nz), 128, 0, st>>>(c, m, q, part);
+template <class V>
+static void xprofile_t(cudaStream_t st, const DConst& c, const DMetric& m, const V* q, double* part, double* out) {
+    k_xprof_part<V><<<dim3((c.nx + 127) / 128, c.nz), 128, 0, st>>>(c, m, q, part);
     k_xprof_final<<<(c.nx + 127) / 128, 128, 0, st>>>(c, part, out);
+}
+void launch_xprofile(cudaStream_t st, const DConst& c, const DMetric& m, const double* q, double* part, double* out) {
+    xprofile_t(st, c, m, q, part, out);
+}
+void launch_xprofile(cudaStream_t st, const DConst& c, const DMetric& m, const float* q, double* part, double* out) {
+    xprofile_t(st, c, m, q, part, out);
 }
 
 size_t endstep_blocks(const DConst& c) { return (size_t)2 * (c.nsm > 0 ? c.nsm : 148); }
 
 void launch_endstep(cudaStream_t st, const DConst& c, const DMetric& m, const Fields& f, DCoef* coef, DDiag* diag,
                     double* part, unsigned int* counter, int next) {
-    launch_pdl(k_endstep, dim3((unsigned)endstep_blocks(c)), dim3(ENDSTEP_THREADS), 0, st, c, m, f.ux, f.uy, f.uz,
-               f.sc, coef, diag, part, counter, next);
+    launch_pdl(k_endstep<double>, dim3((unsigned)endstep_blocks(c)), dim3(ENDSTEP_THREADS), 0, st, c, m, f.ux, f.uy,
+               f.uz, f.sc, coef, diag, part, counter, next);
+}
+void launch_endstep(cudaStream_t st, const DConst& c, const DMetric& m, const Fields32& f, DCoef* coef, DDiag* diag,
+                    double* part, unsigned int* counter, int next) {
+    launch_pdl(k_endstep<float>, dim3((unsigned)endstep_blocks(c)), dim3(ENDSTEP_THREADS), 0, st, c, m, f.ux, f.uy,
+               f.uz, f.sc, coef, diag, part, counter, next);
 }
 
 }  // namespace ptc

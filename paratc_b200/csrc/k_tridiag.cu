@@ -168,7 +168,8 @@ __host__ __device__ inline int helm_stride(int ny) { return 3 * (ny + 2); }
 // memory; rows are addressed by pointer steps; the wall rows need no case of
 // their own in the sweeps (a(1) = 0, arr(ny+1) = 0, and clcU2Hat's row-1
 // value is substituted before the sweep and its result after it).
-__global__ void __launch_bounds__(128, 4) k_helm(DConst cst, const DCoef* __restrict__ coef, int comp0, Fields fl,
+template <class V>
+__global__ void __launch_bounds__(128, 4) k_helm(DConst cst, const DCoef* __restrict__ coef, int comp0, FieldSet<V> fl,
                                               const double* __restrict__ duy_ym, const double* __restrict__ uy_ym,
                                               const double* __restrict__ facs) {
     extern __shared__ double shf[];
@@ -189,23 +190,24 @@ __global__ void __launch_bounds__(128, 4) k_helm(DConst cst, const DCoef* __rest
     const int i = (blockIdx.x * 4 + threadIdx.y) * 32 + threadIdx.x;
     const int k = blockIdx.y;
     if (i >= nx) return;
-    double* u;
-    double* rhs;
+    V* u;
+    V* rhs;
     double add = 0.0;
     if (comp == 0)      { u = fl.ux; rhs = fl.rx; add = coef->rhsx_add; }
     else if (comp == 1) { u = fl.uy; rhs = fl.ry; }
     else if (comp == 2) { u = fl.uz; rhs = fl.rz; }
     else                { u = fl.sc; rhs = fl.rc; }
     const size_t col = (size_t)k * cst.nyt * nx + i;
-    double* rc = rhs + col;
-    double* uc = u + col;
+    // the sweeps run in FP64 whatever the storage: loads convert, stores round
+    V* rc = rhs + col;
+    V* uc = u + col;
     const int nch = (ny + HY_U - 1) / HY_U;
 
     // forward sweep, rows 1..ny: f = ((r + add) - a f_prev) / vecm, written over Rhs
     double A[HY_U], B[HY_U], C[HY_U];
     auto ldr = [&](double (&X)[HY_U], int cc) {
         if (cc >= nch) return;
-        const double* b = rc + (size_t)(cc * HY_U + 1) * nx;
+        const V* b = rc + (size_t)(cc * HY_U + 1) * nx;
         const int nr = ny - cc * HY_U;
 #pragma unroll
         for (int q = 0; q < HY_U; q++) {
@@ -214,7 +216,7 @@ __global__ void __launch_bounds__(128, 4) k_helm(DConst cst, const DCoef* __rest
         }
     };
     double fp = 0.0;
-    double* wp = rc + nx;
+    V* wp = rc + nx;
     auto fwd = [&](const double (&X)[HY_U], int cc) {
         if (cc >= nch) return;
         const int nr = ny - cc * HY_U;
@@ -224,8 +226,8 @@ __global__ void __launch_bounds__(128, 4) k_helm(DConst cst, const DCoef* __rest
         for (int q = 0; q < HY_U; q++) {
             if (q < nr) {
                 const double f = ((X[q] + add) - sa[q] * fp) * sr[q];
-                *wp = f;
-                fp = f;
+                *wp = (V)f;
+                fp = (double)(V)f;  // the value the backward sweep will read
             }
             wp += nx;
         }
@@ -247,8 +249,8 @@ __global__ void __launch_bounds__(128, 4) k_helm(DConst cst, const DCoef* __rest
     auto ldb = [&](double (&D)[HY_U], double (&U)[HY_U], int cc) {
         if (cc >= nch) return;
         const size_t off = (size_t)(ny - cc * HY_U) * nx;
-        const double* bd = rc + off;
-        const double* bu = uc + off;
+        const V* bd = rc + off;
+        const V* bu = uc + off;
         const int nr = ny - cc * HY_U;
 #pragma unroll
         for (int q = 0; q < HY_U; q++) {
@@ -258,7 +260,7 @@ __global__ void __launch_bounds__(128, 4) k_helm(DConst cst, const DCoef* __rest
         }
     };
     double xn = 0.0, unew = 0.0, utop = 0.0;
-    double* up = uc + (size_t)ny * nx;
+    V* up = uc + (size_t)ny * nx;
     auto bwd = [&](const double (&D)[HY_U], const double (&U)[HY_U], int cc) {
         if (cc >= nch) return;
         const int nr = ny - cc * HY_U;
@@ -269,7 +271,7 @@ __global__ void __launch_bounds__(128, 4) k_helm(DConst cst, const DCoef* __rest
                 const double x = D[q] - sw[-q] * xn;
                 xn = x;
                 unew = U[q] + x;
-                *up = unew;
+                *up = (V)unew;
             }
             up -= nx;
         }
@@ -288,11 +290,11 @@ __global__ void __launch_bounds__(128, 4) k_helm(DConst cst, const DCoef* __rest
     }
     // wall rows: unew now holds u(1)
     if (comp == 1) {
-        uc[nx] = uy_ym[(size_t)k * nx + i];
-        uc[(size_t)(ny + 1) * nx] = (cst.flow_type == 1) ? cst.uybc_yp : 0.0;
+        uc[nx] = (V)uy_ym[(size_t)k * nx + i];
+        uc[(size_t)(ny + 1) * nx] = (V)((cst.flow_type == 1) ? cst.uybc_yp : 0.0);
     } else if (comp == 3) {
-        uc[0] = cst.sc_r1b * unew + cst.sc_r2b;
-        uc[(size_t)(ny + 1) * nx] = cst.sc_r1t * utop + cst.sc_r2t;
+        uc[0] = (V)(cst.sc_r1b * unew + cst.sc_r2b);
+        uc[(size_t)(ny + 1) * nx] = (V)(cst.sc_r1t * utop + cst.sc_r2t);
     }
 }
 
@@ -655,19 +657,27 @@ void launch_helm_factors(cudaStream_t st, const DConst& c, const DMetric& m, con
                alp[0], alp[1], alp[2], fac);
 }
 
-static void helm_dispatch(cudaStream_t st, const DConst& c, const DCoef* coef, int comp0, int ncomp, const Fields& f,
-                          const double* duy_ym, const double* uy_ym, const double* fac) {
+template <class V>
+static void helm_dispatch(cudaStream_t st, const DConst& c, const DCoef* coef, int comp0, int ncomp,
+                          const FieldSet<V>& f, const double* duy_ym, const double* uy_ym, const double* fac) {
     dim3 blk(32, 4);
     dim3 grd((c.nx + 127) / 128, c.nz, ncomp);
-    launch_pdl(k_helm, grd, blk, helm_stride(c.ny) * sizeof(double), st, c, coef, comp0, f, duy_ym, uy_ym, fac);
+    launch_pdl(k_helm<V>, grd, blk, helm_stride(c.ny) * sizeof(double), st, c, coef, comp0, f, duy_ym, uy_ym, fac);
 }
 
 void launch_helm(cudaStream_t st, const DConst& c, const DCoef* coef, const Fields& f, const double* duy_ym,
                  const double* uy_ym, const double* fac) {
     helm_dispatch(st, c, coef, 0, 3, f, duy_ym, uy_ym, fac);
 }
+void launch_helm(cudaStream_t st, const DConst& c, const DCoef* coef, const Fields32& f, const double* duy_ym,
+                 const double* uy_ym, const double* fac) {
+    helm_dispatch(st, c, coef, 0, 3, f, duy_ym, uy_ym, fac);
+}
 
 void launch_helm_scalar(cudaStream_t st, const DConst& c, const DCoef* coef, const Fields& f, const double* fac) {
+    helm_dispatch(st, c, coef, 3, 1, f, nullptr, nullptr, fac);
+}
+void launch_helm_scalar(cudaStream_t st, const DConst& c, const DCoef* coef, const Fields32& f, const double* fac) {
     helm_dispatch(st, c, coef, 3, 1, f, nullptr, nullptr, fac);
 }
 

@@ -28,27 +28,44 @@ inline void launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t s
     cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
 }
 
-// device pointers of the fields of one context (padded layout, see common.cuh)
-struct Fields {
-    double *ux, *uy, *uz, *pr, *sc;   // state (sc may be null)
-    double *hx, *hy, *hz, *hc;        // explicit history HistX/Y/Z/C
-    double *rx, *ry, *rz, *rc;        // right-hand sides of the Helmholtz solves
+// device pointers of the fields of one context (padded layout, see
+// common.cuh), in storage type V: double for the FP64 forms, float for the
+// FP32 storage form.  The pressure, which accumulates the potential of every
+// substep, is FP64 in every form.
+template <class V>
+struct FieldSet {
+    V *ux, *uy, *uz;          // velocity state
+    double* pr;               // pressure
+    V* sc;                    // scalar (may be null)
+    V *hx, *hy, *hz, *hc;     // explicit history HistX/Y/Z/C
+    V *rx, *ry, *rz, *rc;     // right-hand sides of the Helmholtz solves
 };
+using Fields = FieldSet<double>;
+using Fields32 = FieldSet<float>;
 
-// k_stencil.cu
+// k_stencil.cu (each for the FP64 fields and for the FP32 storage form)
 size_t cell_grid_blocks(const DConst& c);
 void launch_prsrc(cudaStream_t st, const DConst& c, const DMetric& m, const DCoef* coef, int unit_scale,
                   const Fields& f, double* src, double* part, double* out_max);
+void launch_prsrc(cudaStream_t st, const DConst& c, const DMetric& m, const DCoef* coef, int unit_scale,
+                  const Fields32& f, double* src, double* part, double* out_max);
 void launch_project(cudaStream_t st, const DConst& c, const DMetric& m, const DCoef* coef, int mode, const double* phi,
                     const Fields& f, const double* uy_ym);
+void launch_project(cudaStream_t st, const DConst& c, const DMetric& m, const DCoef* coef, int mode, const float* phi,
+                    const Fields32& f, const double* uy_ym);
 void launch_bc_all(cudaStream_t st, const DConst& c, const Fields& f, const double* uy_ym);
+void launch_bc_all(cudaStream_t st, const DConst& c, const Fields32& f, const double* uy_ym);
 void launch_update_uy_ym(cudaStream_t st, int n, double* uy_ym, double* duy_ym);
 void launch_cfl(cudaStream_t st, const DConst& c, const DMetric& m, const Fields& f, DCoef* coef, double* part);
+void launch_cfl(cudaStream_t st, const DConst& c, const DMetric& m, const Fields32& f, DCoef* coef, double* part);
 size_t endstep_blocks(const DConst& c);
-// x profile of a padded field averaged over y (dyp weights) and z; part holds nx*nz doubles
-void launch_xprofile(cudaStream_t st, const DConst& c, const DMetric& m, const double* q, double* part, double* out);
 void launch_endstep(cudaStream_t st, const DConst& c, const DMetric& m, const Fields& f, DCoef* coef, DDiag* diag,
                     double* part, unsigned int* counter, int next);
+void launch_endstep(cudaStream_t st, const DConst& c, const DMetric& m, const Fields32& f, DCoef* coef, DDiag* diag,
+                    double* part, unsigned int* counter, int next);
+// x profile of a padded field averaged over y (dyp weights) and z; part holds nx*nz doubles
+void launch_xprofile(cudaStream_t st, const DConst& c, const DMetric& m, const double* q, double* part, double* out);
+void launch_xprofile(cudaStream_t st, const DConst& c, const DMetric& m, const float* q, double* part, double* out);
 
 // k_rhs.cu
 size_t rhs_grid_blocks(const DConst& c);
@@ -68,7 +85,10 @@ void launch_helm_factors(cudaStream_t st, const DConst& c, const DMetric& m, con
                          const double* alp, double* fac);
 void launch_helm(cudaStream_t st, const DConst& c, const DCoef* coef, const Fields& f, const double* duy_ym,
                  const double* uy_ym, const double* fac);
+void launch_helm(cudaStream_t st, const DConst& c, const DCoef* coef, const Fields32& f, const double* duy_ym,
+                 const double* uy_ym, const double* fac);
 void launch_helm_scalar(cudaStream_t st, const DConst& c, const DCoef* coef, const Fields& f, const double* fac);
+void launch_helm_scalar(cudaStream_t st, const DConst& c, const DCoef* coef, const Fields32& f, const double* fac);
 void launch_ysolve(cudaStream_t st, const DConst& c, const DMetric& m, double2* spec);
 
 // k_tridiag.cu: spectral y-solve with the pivots computed once per context

@@ -97,13 +97,19 @@ def xprofile(q, dyp, yly):
 
 
 def front_position(prof, dx, x_from=1.0, level=0.5):
-    """First x right of x_from where the profile drops below `level`,
-    interpolated between cell centres (i + 0.5) dx; -1 if nowhere."""
+    """Nose of the current: the furthest cell centre (i + 0.5) dx right of
+    x_from, within half the periodic domain, whose value is at least
+    `level`, moved to the level's linear crossing with the next cell; -1 if
+    no cell there reaches it (the definition paratc_front_position uses)."""
+    n = len(prof)
+    xlx = n * dx
+    last = -1
     for i, v in enumerate(prof):
         x = (i + 0.5) * dx
-        if x <= x_from or not v < level:
-            continue
-        if i > 0 and x - dx > x_from and prof[i - 1] >= level:
-            return x - dx + (prof[i - 1] - level) / (prof[i - 1] - v) * dx
-        return x
-    return -1.0
+        if x_from < x < x_from + 0.5 * xlx and v >= level:
+            last = i
+    if last < 0:
+        return -1.0
+    xl = (last + 0.5) * dx
+    pn = prof[(last + 1) % n]
+    return xl + (prof[last] - level) / (prof[last] - pn) * dx if pn < level else xl

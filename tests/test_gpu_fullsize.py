@@ -117,15 +117,17 @@ def test_lock_exchange_c3_front():
     bottom, CFL-controlled dt) at full size.  20 steps from the lock initial
     state against the oracle: fields relative to their largest magnitude
     within 1e-10 after one step, 1e-8 after two and 1e-6 after 20, and the
-    front position (the x right of the lock at x = 1 where the depth-averaged
-    concentration first drops below FRONT_LEVEL = 0.05) from the device
-    profile equal to the one of the oracle's fields to 1e-9 of a cell.  Then
-    the GPU path alone to step 2000: the front moves downstream (never back by
-    more than a tenth of a cell between samples 100 steps apart), the
-    divergence stays <= 1e-10 and the fields finite.  (A level of 0.5 does not
-    track this current: a full-depth lock collapses to about half the depth,
-    so the depth average right of the gate stays below 0.5 and its 0.5
-    crossing sits at the gate, x = 1.0156, for all 2000 steps.)"""
+    front position (the nose: the furthest x right of the lock at x = 1 where
+    the depth-averaged concentration is at least FRONT_LEVEL = 0.05) from the
+    device profile equal to the one of the oracle's fields to 1e-9 of a cell.
+    Then the GPU path alone to step 2000: the nose moves downstream (never
+    back by more than a tenth of a cell between samples 100 steps apart), the
+    divergence stays <= 1e-10 and the fields finite.  (The first crossing of
+    0.5 does not track this current: the full-depth lock collapses to about
+    half the depth, so the depth average right of the gate stays below 0.5
+    and that crossing sits at the gate, x = 1.0156, for all 2000 steps; the
+    first crossing of 0.05 moves with the nose until the lock has drained
+    near step 900 and then falls back to the gate.)"""
     case = cases.lock_exchange_c3()
     p = case.params
     yp = yp_of(case)
@@ -154,14 +156,15 @@ def test_lock_exchange_c3_front():
             assert rel_err(prof_g, prof_o) <= 1e-8
             xf_o = front_position(prof_o, dx, 1.0, FRONT_LEVEL)
             xf_g = g.front_position(1.0, FRONT_LEVEL)
-            assert xf_o > 1.0 and abs(xf_g - xf_o) <= 1e-9 * dx, (s, xf_g, xf_o)
-            fronts.append((s, xf_g))
+            # -1 while no cell right of the gate reaches the level yet
+            assert abs(xf_g - xf_o) <= 1e-9 * dx, (s, xf_g, xf_o)
+            fronts.append((s, max(xf_g, 1.0)))
     o.close()
     for s in range(21, 2001):
         d = g.iterate(1)
         assert d.divmax <= 1e-10 and np.isfinite(d.dt)
         if s % 100 == 0:
-            fronts.append((s, g.front_position(1.0, FRONT_LEVEL)))
+            fronts.append((s, max(g.front_position(1.0, FRONT_LEVEL), 1.0)))
     print("C3 front position (step, x):", ["%d:%.4f" % sf for sf in fronts])
     xs = [x for _, x in fronts]
     assert all(b >= a - 0.1 * dx for a, b in zip(xs, xs[1:]))
