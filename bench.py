@@ -50,8 +50,9 @@ def _args():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--schedule", type=int, default=-1,
                     help="pin a Poisson schedule (0-11, paratc_set_schedule) instead of auto-tuning it")
-    ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64",
-                    help="mixed: the explicit right-hand side in FP32 arithmetic, all else FP64")
+    ap.add_argument("--precision", choices=["fp64", "mixed", "fp32"], default="fp64",
+                    help="mixed: the explicit right-hand side in FP32 arithmetic, all else FP64; "
+                         "fp32: FP32 storage of everything but the pressure")
     return ap.parse_args()
 
 

@@ -247,6 +247,23 @@ int paratc_poisson_device(paratc_ctx* ctx, const double* d_src, double* d_phi);
  * context's stream (paratc_stream), without waiting for it. */
 int paratc_poisson_device_async(paratc_ctx* ctx, const double* d_src, double* d_phi);
 
+/* clcPPE by FP32 solves with FP64 iterative refinement.  No counterpart in
+ * the reference (its solve is FP64).  The first solve takes the FP64 source
+ * d_src through a spectrum stored in FP32 (the transform and Thomas passes
+ * compute in FP64) into d_phi; each correction computes the FP64 residual
+ * r = src - L phi of the discrete operator the spectral solve inverts
+ * (4th-order D4 D4 in x and z, the Neumann y operator), solves L d = r the
+ * same way and adds d to phi.  Stops when max|r| <= rtol * max|src| or after
+ * max_corr corrections; ncorr and relres (may be NULL) receive the count and
+ * the final max|r| / max|src|.  The source must have zero mean (the gauge
+ * phi_hat(0,0,1) = 0 of the FP64 solve is kept).  Device pointers, compact
+ * interior layout, d_src != d_phi; needs compile-time-length transforms. */
+int paratc_poisson_refined(paratc_ctx* ctx, const double* d_src, double* d_phi, double rtol, int max_corr,
+                           int* ncorr, double* relres);
+/* The same with exactly ncorr corrections, queued on the context's stream
+ * without reading the residual back (for timing). */
+int paratc_poisson_refined_async(paratc_ctx* ctx, const double* d_src, double* d_phi, int ncorr);
+
 /* Poisson solve that allocates no memory.  No counterpart in the reference:
  * it exists for callers that cannot call cudaMalloc (a loop with a fixed
  * memory budget, a host code whose allocator owns all device memory, a
@@ -334,12 +351,24 @@ int paratc_set_wait_limit(paratc_ctx* ctx, long long polls);
  * explicit histories, the Helmholtz and Poisson solves, the projection, the
  * flow-rate constraint sum (s3tot) and every reduction stay FP64, so the
  * divergence after a step is at the FP64 level while the fields differ from
- * the FP64 path by the FP32 rounding of one explicit term per substep.  (An
- * FP32 solve with FP64 iterative refinement is not offered: on this direct
- * FFT-Thomas solver each refinement sweep moves more bytes than the single
- * FP64 solve it replaces.) */
+ * the FP64 path by the FP32 rounding of one explicit term per substep.
+ * PARATC_PREC_FP32 is the FP32 storage form: u, v, w, the scalar, the
+ * explicit histories, the right-hand sides, the spectrum of the Poisson
+ * solve and the potential are stored in FP32 (half the bytes of every pass
+ * over them); the pressure stays FP64.  The right-hand side is computed in
+ * FP32 arithmetic; the Helmholtz sweeps, the transforms, the spectral y-solve
+ * (with its kx = kz = 0 mean mode) and the projection in FP64 arithmetic on
+ * values loaded from FP32; the flow-rate constraint, the guards and the
+ * statistics in FP64.  The divergence of the FP32-stored velocity is limited
+ * by its rounding (about 1e-7 of |u|/dx), not by the solves.  Switching to or
+ * from FP32 converts the state; statistics, spectra, visualisation, restart
+ * and get_fields read an FP64 copy refreshed from it.  The FP32 form needs
+ * compile-time-length transforms for nxc/2 and nzc (else PARATC_ERR_BAD_ARG)
+ * and runs the plane or separate x/z transform kernels of the context's
+ * schedule (the TMA-fed variants stay FP64). */
 #define PARATC_PREC_FP64  0
 #define PARATC_PREC_MIXED 1
+#define PARATC_PREC_FP32  2
 int paratc_set_precision(paratc_ctx* ctx, int prec);
 int paratc_get_precision(paratc_ctx* ctx, int* prec);
 

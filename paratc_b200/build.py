@@ -9,6 +9,7 @@ is newer than its object.
 import concurrent.futures as cf
 import glob
 import os
+import re
 import shutil
 import subprocess
 import sys
@@ -37,11 +38,22 @@ def _headers():
         [os.path.join(ROOT, "include", "paratc.h")]
 
 
+def _included_sources(src):
+    """The .cu files a translation unit includes (the FP32 storage
+    instantiations include the FP64 kernel sources with a switch set)."""
+    out = []
+    for line in open(src):
+        m = re.match(r'\s*#include\s+"([^"]+\.cu)"', line)
+        if m:
+            out.append(os.path.join(os.path.dirname(src), m.group(1)))
+    return out
+
+
 def _stale(obj, src, hdrs):
     if not os.path.exists(obj):
         return True
     t = os.path.getmtime(obj)
-    return any(os.path.getmtime(p) > t for p in [src] + hdrs)
+    return any(os.path.getmtime(p) > t for p in [src] + hdrs + _included_sources(src))
 
 
 def _compile(nvcc, src, obj, verbose_ptxas):

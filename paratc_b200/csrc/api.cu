@@ -50,6 +50,9 @@ struct paratc_ctx {
     DMetric dm;
     FftPlan plx, plz;
     Fields f;
+    int prec = PARATC_PREC_FP64;  // PARATC_PREC_FP64 / _MIXED / _FP32
+    Fields32 f32{};               // float fields of the FP32 storage form (pr = f.pr), allocated on first use
+    float* d_phi32 = nullptr;     // its potential (padded)
     std::vector<void*> allocs;
     double *d_src = nullptr, *d_phi = nullptr, *d_part = nullptr, *d_uy_ym = nullptr, *d_duy_ym = nullptr;
     double *d_metric = nullptr, *d_scal = nullptr;
@@ -283,9 +286,101 @@ void enqueue_poisson(paratc_ctx* ctx, const double* src, double* out, int padded
     enqueue_poisson_tail(ctx, out, padded);
 }
 
+// ---- the FP32 storage form: the same solve on a float2 spectrum (the
+// passes compute in double) with the compile-time-length transforms, one CTA
+// per plane where the plane fits, else the separate x and z kernels
+float2* spec32(paratc_ctx* ctx) { return reinterpret_cast<float2*>(ctx->d_spec); }
+
+// forward transform of the divergence of the float velocity (mode 0:
+// clcPrSrc's source / pmAlpha, max|div| to out_max; 1: unscaled)
+void enqueue_poisson_head32(paratc_ctx* ctx, int mode, double* out_max) {
+    cudaStream_t st = ctx->st;
+    PROF(PK_PRSRC);
+    if (ctx->plane)
+        launch_plane_f(st, mode, ctx->kc, ctx->dm, ctx->d_coef, ctx->f32, nullptr, spec32(ctx), ctx->d_twx,
+                       ctx->d_postx, ctx->d_twz, ctx->d_part, ctx->d_counter + 1, out_max);
+    else
+        launch_pfft_xf(st, mode, ctx->kc, ctx->dm, ctx->d_coef, ctx->f32, nullptr, spec32(ctx), ctx->d_twx,
+                       ctx->d_postx, ctx->d_part, ctx->d_counter + 1, out_max);
+    ctx->launches += 1;
+}
+
+void enqueue_poisson_tail32(paratc_ctx* ctx, float* out, int padded) {
+    cudaStream_t st = ctx->st;
+    if (ctx->plane) {
+        { PROF(PK_YSOLVE); launch_ysolve_fac(st, ctx->kc, ctx->dm, spec32(ctx), ctx->d_pfac); }
+        { PROF(PK_FFTX_B); launch_plane_b(st, ctx->nx, ctx->ny, ctx->nz, spec32(ctx), out, ctx->d_twx, ctx->d_postx,
+                                          ctx->d_twz, ctx->hm.normfft, padded); }
+        ctx->launches += 2;
+        return;
+    }
+    { PROF(PK_FFTZ_F); launch_pfft_z(st, -1, ctx->nx, ctx->ny, ctx->nz, spec32(ctx), ctx->d_twz); }
+    { PROF(PK_YSOLVE); launch_ysolve_fac(st, ctx->kc, ctx->dm, spec32(ctx), ctx->d_pfac); }
+    { PROF(PK_FFTZ_B); launch_pfft_z(st, +1, ctx->nx, ctx->ny, ctx->nz, spec32(ctx), ctx->d_twz); }
+    { PROF(PK_FFTX_B); launch_pfft_xb(st, ctx->nx, ctx->ny, ctx->nz, spec32(ctx), out, ctx->d_twx, ctx->d_postx,
+                                      ctx->hm.normfft, padded); }
+    ctx->launches += 4;
+}
+
+// one solve of the refined standalone Poisson equation: the FP64 array src
+// (compact) through a float2 spectrum into the FP64 potential phi (compact),
+// written (accumulate = 0) or added to it (the corrections)
+void enqueue_solve32(paratc_ctx* ctx, const double* src, double* phi, int accumulate) {
+    cudaStream_t st = ctx->st;
+    if (ctx->plane) {
+        { PROF(PK_FFTX_F); launch_plane_f(st, ctx->kc, src, spec32(ctx), ctx->d_twx, ctx->d_postx, ctx->d_twz); }
+        { PROF(PK_YSOLVE); launch_ysolve_fac(st, ctx->kc, ctx->dm, spec32(ctx), ctx->d_pfac); }
+        { PROF(PK_FFTX_B); launch_plane_b(st, ctx->nx, ctx->ny, ctx->nz, spec32(ctx), phi, ctx->d_twx, ctx->d_postx,
+                                          ctx->d_twz, ctx->hm.normfft, accumulate); }
+        ctx->launches += 3;
+        return;
+    }
+    { PROF(PK_FFTX_F); launch_pfft_xf(st, ctx->kc, src, spec32(ctx), ctx->d_twx, ctx->d_postx); }
+    { PROF(PK_FFTZ_F); launch_pfft_z(st, -1, ctx->nx, ctx->ny, ctx->nz, spec32(ctx), ctx->d_twz); }
+    { PROF(PK_YSOLVE); launch_ysolve_fac(st, ctx->kc, ctx->dm, spec32(ctx), ctx->d_pfac); }
+    { PROF(PK_FFTZ_B); launch_pfft_z(st, +1, ctx->nx, ctx->ny, ctx->nz, spec32(ctx), ctx->d_twz); }
+    { PROF(PK_FFTX_B); launch_pfft_xb(st, ctx->nx, ctx->ny, ctx->nz, spec32(ctx), phi, ctx->d_twx, ctx->d_postx,
+                                      ctx->hm.normfft, accumulate); }
+    ctx->launches += 5;
+}
+
+// the substep of the FP32 storage form: float u, v, w, c, histories,
+// right-hand sides, spectrum and potential, FP64 pressure; the right-hand
+// side in FP32 arithmetic, the Helmholtz sweeps and the transforms in FP64
+// arithmetic, the flow-rate sum and every reduction in FP64
+void enqueue_substep32(paratc_ctx* ctx, int ns, int stop) {
+    cudaStream_t st = ctx->st;
+    const HostMetrics& h = ctx->hm;
+    {
+        PROF(PK_RHS);
+        launch_rhs_tile(st, ctx->kc, ctx->dm, ctx->d_coef, ctx->f32, ctx->d_uy_ym, ctx->d_duy_ym, ns, h.gam[ns - 1],
+                        h.the[ns - 1], h.alp[ns - 1], ctx->d_part, ctx->d_counter, ctx->d_zt_err);
+    }
+    ctx->launches += 1;
+    if (stop == 1) return;
+    if (ctx->prm.scalar_on) { PROF(PK_HELM_SC); launch_helm_scalar(st, ctx->kc, ctx->d_coef, ctx->f32, ctx->d_hfac); ctx->launches++; }
+    { PROF(PK_HELM); launch_helm(st, ctx->kc, ctx->d_coef, ctx->f32, ctx->d_duy_ym, ctx->d_uy_ym, ctx->d_hfac); }
+    ctx->launches += 1;
+    if (stop == 2) return;
+    if (stop == 3) {
+        { PROF(PK_PRSRC); launch_prsrc(st, ctx->kc, ctx->dm, ctx->d_coef, 0, ctx->f32, ctx->d_src, ctx->d_part, &ctx->d_coef->divmax_src); }
+        ctx->launches += 2;
+        return;
+    }
+    enqueue_poisson_head32(ctx, 0, &ctx->d_coef->divmax_src);
+    enqueue_poisson_tail32(ctx, ctx->d_phi32, 1);
+    if (stop == 4) return;
+    { PROF(PK_PROJECT); launch_project(st, ctx->kc, ctx->dm, ctx->d_coef, 0, ctx->d_phi32, ctx->f32, ctx->d_uy_ym); }
+    ctx->launches += 1;
+}
+
 // body of the ns loop of ChannelIterate (src/m_ChannelSystem.f90:102-140),
 // optionally stopped after stage `stop` (1 rhs, 2 helmholtz, 3 prsrc, 4 ppe)
 void enqueue_substep(paratc_ctx* ctx, int ns, int stop = 5) {
+    if (ctx->prec == PARATC_PREC_FP32) {
+        enqueue_substep32(ctx, ns, stop);
+        return;
+    }
     cudaStream_t st = ctx->st;
     const HostMetrics& h = ctx->hm;
     {
@@ -315,8 +410,11 @@ void enqueue_substep(paratc_ctx* ctx, int ns, int stop = 5) {
 
 void enqueue_step(paratc_ctx* ctx) {
     // clcCFL: done by the previous step's end kernel unless the state changed since
+    const bool fp32 = ctx->prec == PARATC_PREC_FP32;
     if (!ctx->next_ready) {
-        { PROF(PK_CFL); launch_cfl(ctx->st, ctx->kc, ctx->dm, ctx->f, ctx->d_coef, ctx->d_part); }
+        PROF(PK_CFL);
+        if (fp32) launch_cfl(ctx->st, ctx->kc, ctx->dm, ctx->f32, ctx->d_coef, ctx->d_part);
+        else launch_cfl(ctx->st, ctx->kc, ctx->dm, ctx->f, ctx->d_coef, ctx->d_part);
         ctx->launches += 2;
     }
     // with a fixed time step (iCFL != 1) the Helmholtz matrices never change:
@@ -327,7 +425,11 @@ void enqueue_step(paratc_ctx* ctx) {
         ctx->hfac_dt = (ctx->prm.icfl == 1) ? -1.0 : ctx->prm.dt_max;
     }
     for (int ns = 1; ns <= ctx->hm.iadvance; ns++) enqueue_substep(ctx, ns);
-    { PROF(PK_CHECK); launch_endstep(ctx->st, ctx->kc, ctx->dm, ctx->f, ctx->d_coef, ctx->d_diag, ctx->d_part, ctx->d_counter + 3, 1); }
+    {
+        PROF(PK_CHECK);
+        if (fp32) launch_endstep(ctx->st, ctx->kc, ctx->dm, ctx->f32, ctx->d_coef, ctx->d_diag, ctx->d_part, ctx->d_counter + 3, 1);
+        else launch_endstep(ctx->st, ctx->kc, ctx->dm, ctx->f, ctx->d_coef, ctx->d_diag, ctx->d_part, ctx->d_counter + 3, 1);
+    }
     ctx->next_ready = true;
     ctx->launches += 1;
 }
@@ -350,11 +452,13 @@ int sync(paratc_ctx* ctx) {
     if (e != cudaSuccess) return set_err(ctx, PARATC_ERR_CUDA, std::string("kernel execution: ") + cudaGetErrorString(e));
     e = cudaGetLastError();
     if (e != cudaSuccess) return set_err(ctx, PARATC_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(e));
-    if (*hb)
-        return set_err(ctx, PARATC_ERR_TIMEOUT, (*hb & 1u)   ? "z transform: a TMA wait gave up"
-                                                : (*hb & 2u) ? "x transform: a TMA wait gave up"
-                                                : (*hb & 4u) ? "divergence transform: a stage wait gave up"
-                                                             : "right-hand side: a row copy wait gave up");
+    if (*hb) {
+        std::string m;
+        const char* names[4] = {"z transform", "x transform", "divergence-fed x transform", "right-hand side"};
+        for (int b = 0; b < 4; b++)
+            if (*hb & (1u << b)) m += (m.empty() ? "" : ", ") + std::string(names[b]);
+        return set_err(ctx, PARATC_ERR_TIMEOUT, m + ": a bounded wait on a copy pipeline gave up");
+    }
     return PARATC_OK;
 }
 
@@ -388,12 +492,54 @@ int copy_field(paratc_ctx* ctx, double* dev, const double* host_src, double* hos
     return PARATC_OK;
 }
 
+// the float arrays of the FP32 storage form, created on first use
+int alloc_fp32(paratc_ctx* ctx) {
+    if (ctx->f32.ux) return PARATC_OK;
+    Fields32& g = ctx->f32;
+    float** a[] = {&g.ux, &g.uy, &g.uz, &g.hx, &g.hy, &g.hz, &g.rx, &g.ry, &g.rz, &ctx->d_phi32};
+    int rc;
+    for (float** q : a)
+        if ((rc = dalloc(ctx, q, ctx->nf))) return rc;
+    if (ctx->prm.scalar_on) {
+        float** b[] = {&g.sc, &g.hc, &g.rc};
+        for (float** q : b)
+            if ((rc = dalloc(ctx, q, ctx->nf))) return rc;
+    }
+    g.pr = ctx->f.pr;  // the pressure stays FP64
+    return PARATC_OK;
+}
+
+// the state (u, v, w, c, ghost rows included) and the explicit histories
+// between the FP64 arrays and the float arrays of the FP32 storage form
+void state_to32(paratc_ctx* ctx) {
+    const Fields& a = ctx->f;
+    const Fields32& b = ctx->f32;
+    const double* src[] = {a.ux, a.uy, a.uz, a.hx, a.hy, a.hz, a.sc, a.hc};
+    float* dst[] = {b.ux, b.uy, b.uz, b.hx, b.hy, b.hz, b.sc, b.hc};
+    for (int q = 0; q < 8; q++)
+        if (src[q] && dst[q]) { launch_cast(ctx->st, ctx->nf, src[q], dst[q]); ctx->launches++; }
+}
+void state_to64(paratc_ctx* ctx) {
+    const Fields& a = ctx->f;
+    const Fields32& b = ctx->f32;
+    const float* src[] = {b.ux, b.uy, b.uz, b.hx, b.hy, b.hz, b.sc, b.hc};
+    double* dst[] = {a.ux, a.uy, a.uz, a.hx, a.hy, a.hz, a.sc, a.hc};
+    for (int q = 0; q < 8; q++)
+        if (src[q] && dst[q]) { launch_cast(ctx->st, ctx->nf, src[q], dst[q]); ctx->launches++; }
+}
+// before a reader of the FP64 arrays (statistics, spectra, visualisation,
+// restart, get_fields) in the FP32 storage form
+void refresh64(paratc_ctx* ctx) {
+    if (ctx->prec == PARATC_PREC_FP32) state_to64(ctx);
+}
+
 int load_state_common(paratc_ctx* ctx, bool wait) {
     // ChannelInitialize after read_restart (src/m_ChannelSystem.f90:63-68)
     launch_update_uy_ym(ctx->st, ctx->nx * ctx->nz, ctx->d_uy_ym, ctx->d_duy_ym);
     CK(cudaMemcpyAsync(ctx->d_coef, ctx->h_coef0, sizeof(DCoef), cudaMemcpyHostToDevice, ctx->st));
     launch_bc_all(ctx->st, ctx->kc, ctx->f, ctx->d_uy_ym);
     ctx->launches += 2;
+    if (ctx->prec == PARATC_PREC_FP32) state_to32(ctx);
     return wait ? sync(ctx) : PARATC_OK;
 }
 
@@ -569,7 +715,7 @@ int paratc_create(const paratc_params* prm, const double* yp, int device, paratc
     // partial-result records of the grid reductions: one per block of k_prsrc /
     // k_cfl, one per block of the RHS and forward-x kernels, 8 per block of the
     // end-of-step kernel
-    ctx->npart = std::max(std::max(cell_grid_blocks(kc), rhs_grid_blocks(kc)),
+    ctx->npart = std::max(std::max(2 * cell_grid_blocks(kc), rhs_grid_blocks(kc)),
                           std::max((size_t)pfft_x_blocks(ctx->nx, ctx->ny, ctx->nz), endstep_blocks(kc) * 8)) + 64;
     if ((rc = dalloc(ctx, &ctx->d_src, ctx->ni)) || (rc = dalloc(ctx, &ctx->d_spec, (size_t)ctx->M1 * ctx->ny * ctx->nz)) ||
         (rc = dalloc(ctx, &ctx->d_part, ctx->npart)) || (rc = dalloc(ctx, &ctx->d_uy_ym, (size_t)ctx->nx * ctx->nz)) ||
@@ -701,6 +847,7 @@ static int get_fields_impl(paratc_ctx* ctx, double* ux, double* uy, double* uz, 
                            double* hy, double* hz, double* hc, int layout, bool wait) {
     if (!ctx || (layout != PARATC_LAYOUT_INTERIOR && layout != PARATC_LAYOUT_HALO)) return PARATC_ERR_BAD_ARG;
     CK(cudaSetDevice(ctx->dev));
+    refresh64(ctx);
     struct { double* d; double* h; } tab[] = {{ctx->f.ux, ux}, {ctx->f.uy, uy}, {ctx->f.uz, uz}, {ctx->f.pr, p},
                                              {ctx->f.sc, c}, {ctx->f.hx, hx}, {ctx->f.hy, hy}, {ctx->f.hz, hz}, {ctx->f.hc, hc}};
     for (auto& t : tab) {
@@ -838,6 +985,12 @@ int paratc_get_work(paratc_ctx* ctx, int which, double* out) {
     CK(cudaSetDevice(ctx->dev));
     double* src[] = {ctx->f.rx, ctx->f.ry, ctx->f.rz, ctx->f.rc, ctx->d_src, ctx->d_phi};
     if (!src[which]) return PARATC_ERR_BAD_ARG;
+    if (ctx->prec == PARATC_PREC_FP32 && which != 4) {
+        // the FP32 storage form's work arrays, widened into the FP64 ones
+        const float* w32[] = {ctx->f32.rx, ctx->f32.ry, ctx->f32.rz, ctx->f32.rc, nullptr, ctx->d_phi32};
+        launch_cast(ctx->st, ctx->nf, w32[which], src[which]);
+        ctx->launches += 1;
+    }
     int rc;
     if (which == 4) {
         CK(cudaMemcpyAsync(out, ctx->d_src, ctx->ni * sizeof(double), cudaMemcpyDefault, ctx->st));
@@ -869,6 +1022,48 @@ int paratc_poisson_device_async(paratc_ctx* ctx, const double* d_src, double* d_
     CK(cudaSetDevice(ctx->dev));
     enqueue_poisson(ctx, d_src, d_phi, 0);
     CK(cudaGetLastError());
+    return PARATC_OK;
+}
+
+int paratc_poisson_refined_async(paratc_ctx* ctx, const double* d_src, double* d_phi, int ncorr) {
+    if (!ctx || !d_src || !d_phi || ncorr < 0 || d_src == d_phi) return PARATC_ERR_BAD_ARG;
+    CK(cudaSetDevice(ctx->dev));
+    if (!ctx->pfft) return set_err(ctx, PARATC_ERR_BAD_ARG, "the refined solve needs compile-time-length transforms");
+    enqueue_solve32(ctx, d_src, d_phi, 0);
+    for (int q = 0; q < ncorr; q++) {
+        // r = src - L phi in FP64 (into the context's compact work array), then
+        // its FP32-spectrum solve added to phi
+        launch_residual(ctx->st, ctx->kc, ctx->dm, d_src, d_phi, ctx->d_src, ctx->d_part, ctx->d_counter + 5,
+                        ctx->d_scal + 2);
+        ctx->launches += 1;
+        enqueue_solve32(ctx, ctx->d_src, d_phi, 1);
+    }
+    CK(cudaGetLastError());
+    return PARATC_OK;
+}
+
+int paratc_poisson_refined(paratc_ctx* ctx, const double* d_src, double* d_phi, double rtol, int max_corr,
+                           int* ncorr, double* relres) {
+    if (!ctx || !d_src || !d_phi || max_corr < 0 || d_src == d_phi) return PARATC_ERR_BAD_ARG;
+    CK(cudaSetDevice(ctx->dev));
+    if (!ctx->pfft) return set_err(ctx, PARATC_ERR_BAD_ARG, "the refined solve needs compile-time-length transforms");
+    enqueue_solve32(ctx, d_src, d_phi, 0);
+    int q = 0;
+    double rel = 0.0;
+    for (;;) {
+        launch_residual(ctx->st, ctx->kc, ctx->dm, d_src, d_phi, ctx->d_src, ctx->d_part, ctx->d_counter + 5,
+                        ctx->d_scal + 2);
+        ctx->launches += 1;
+        CK(cudaMemcpyAsync(ctx->h_scal + 2, ctx->d_scal + 2, 2 * sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
+        const int rc = sync(ctx);
+        if (rc) return rc;
+        rel = ctx->h_scal[2] / std::max(ctx->h_scal[3], 1e-300);
+        if (!(rel > rtol) || q >= max_corr) break;
+        enqueue_solve32(ctx, ctx->d_src, d_phi, 1);
+        q++;
+    }
+    if (ncorr) *ncorr = q;
+    if (relres) *relres = rel;
     return PARATC_OK;
 }
 
@@ -930,15 +1125,31 @@ int paratc_set_wait_limit(paratc_ctx* ctx, long long polls) {
 }
 
 int paratc_set_precision(paratc_ctx* ctx, int prec) {
-    if (!ctx || (prec != PARATC_PREC_FP64 && prec != PARATC_PREC_MIXED)) return PARATC_ERR_BAD_ARG;
+    if (!ctx || (prec != PARATC_PREC_FP64 && prec != PARATC_PREC_MIXED && prec != PARATC_PREC_FP32))
+        return PARATC_ERR_BAD_ARG;
+    CK(cudaSetDevice(ctx->dev));
+    if (prec == PARATC_PREC_FP32 && !(pfft_x_supported(ctx->nx / 2) && pfft_z_supported(ctx->nz)))
+        return set_err(ctx, PARATC_ERR_BAD_ARG,
+                       "the FP32 storage form needs compile-time-length transforms for nxc/2 and nzc");
+    if (prec == PARATC_PREC_FP32 && ctx->prec != PARATC_PREC_FP32) {
+        int rc = alloc_fp32(ctx);
+        if (rc) return rc;
+        state_to32(ctx);
+        // the generic-length transforms have no float2 form
+        if (!ctx->pfft) sched_apply(ctx, plane_supported(ctx->nx, ctx->nz) ? 0 : 2);
+    } else if (prec != PARATC_PREC_FP32 && ctx->prec == PARATC_PREC_FP32) {
+        state_to64(ctx);
+    }
+    ctx->prec = prec;
     ctx->kc.fp32_rhs = prec == PARATC_PREC_MIXED ? 1 : 0;
-    ctx->sched_gen++;  // captured graphs hold the other kernels
-    return PARATC_OK;
+    ctx->next_ready = false;  // the next step takes its CFL from the converted state
+    ctx->sched_gen++;         // captured graphs hold the other kernels
+    return sync(ctx);
 }
 
 int paratc_get_precision(paratc_ctx* ctx, int* prec) {
     if (!ctx || !prec) return PARATC_ERR_BAD_ARG;
-    *prec = ctx->kc.fp32_rhs ? PARATC_PREC_MIXED : PARATC_PREC_FP64;
+    *prec = ctx->prec;
     return PARATC_OK;
 }
 
@@ -992,11 +1203,19 @@ int paratc_project(paratc_ctx* ctx, double* divmax_out) {
     if (!ctx) return PARATC_ERR_BAD_ARG;
     CK(cudaSetDevice(ctx->dev));
     ctx->next_ready = false;
-    launch_bc_all(ctx->st, ctx->kc, ctx->f, ctx->d_uy_ym);
-    enqueue_poisson_head(ctx, 1, nullptr, ctx->d_scal);
-    enqueue_poisson_tail(ctx, ctx->d_phi, 1);
-    launch_project(ctx->st, ctx->kc, ctx->dm, ctx->d_coef, 1, ctx->d_phi, ctx->f, ctx->d_uy_ym);
-    launch_prsrc(ctx->st, ctx->kc, ctx->dm, ctx->d_coef, 1, ctx->f, nullptr, ctx->d_part, ctx->d_scal + 1);
+    if (ctx->prec == PARATC_PREC_FP32) {
+        launch_bc_all(ctx->st, ctx->kc, ctx->f32, ctx->d_uy_ym);
+        enqueue_poisson_head32(ctx, 1, ctx->d_scal);
+        enqueue_poisson_tail32(ctx, ctx->d_phi32, 1);
+        launch_project(ctx->st, ctx->kc, ctx->dm, ctx->d_coef, 1, ctx->d_phi32, ctx->f32, ctx->d_uy_ym);
+        launch_prsrc(ctx->st, ctx->kc, ctx->dm, ctx->d_coef, 1, ctx->f32, nullptr, ctx->d_part, ctx->d_scal + 1);
+    } else {
+        launch_bc_all(ctx->st, ctx->kc, ctx->f, ctx->d_uy_ym);
+        enqueue_poisson_head(ctx, 1, nullptr, ctx->d_scal);
+        enqueue_poisson_tail(ctx, ctx->d_phi, 1);
+        launch_project(ctx->st, ctx->kc, ctx->dm, ctx->d_coef, 1, ctx->d_phi, ctx->f, ctx->d_uy_ym);
+        launch_prsrc(ctx->st, ctx->kc, ctx->dm, ctx->d_coef, 1, ctx->f, nullptr, ctx->d_part, ctx->d_scal + 1);
+    }
     ctx->launches += 4;
     CK(cudaMemcpyAsync(ctx->h_scal, ctx->d_scal, 2 * sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
     int rc = sync(ctx);
@@ -1009,7 +1228,10 @@ int paratc_diagnostics(paratc_ctx* ctx, paratc_diag* diag) {
     if (!ctx || !diag) return PARATC_ERR_BAD_ARG;
     CK(cudaSetDevice(ctx->dev));
     CK(cudaMemsetAsync(ctx->d_diag2, 0, sizeof(DDiag), ctx->st));
-    launch_endstep(ctx->st, ctx->kc, ctx->dm, ctx->f, ctx->d_coef, ctx->d_diag2, ctx->d_part, ctx->d_counter + 3, 0);
+    if (ctx->prec == PARATC_PREC_FP32)
+        launch_endstep(ctx->st, ctx->kc, ctx->dm, ctx->f32, ctx->d_coef, ctx->d_diag2, ctx->d_part, ctx->d_counter + 3, 0);
+    else
+        launch_endstep(ctx->st, ctx->kc, ctx->dm, ctx->f, ctx->d_coef, ctx->d_diag2, ctx->d_part, ctx->d_counter + 3, 0);
     ctx->launches += 1;
     CK(cudaMemcpyAsync(ctx->h_diag, ctx->d_diag2, sizeof(DDiag), cudaMemcpyDeviceToHost, ctx->st));
     int rc = sync(ctx);
@@ -1027,7 +1249,9 @@ int paratc_xprofile(paratc_ctx* ctx, int field, double* out) {
     // column sums, then the profile
     double* part = ctx->d_src;
     double* prof = ctx->d_src + (size_t)ctx->nx * ctx->nz;
-    launch_xprofile(ctx->st, ctx->kc, ctx->dm, q[field], part, prof);
+    const float* q32[5] = {ctx->f32.ux, ctx->f32.uy, ctx->f32.uz, nullptr, ctx->f32.sc};
+    if (ctx->prec == PARATC_PREC_FP32 && field != 3) launch_xprofile(ctx->st, ctx->kc, ctx->dm, q32[field], part, prof);
+    else launch_xprofile(ctx->st, ctx->kc, ctx->dm, q[field], part, prof);
     ctx->launches += 2;
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(out, prof, (size_t)ctx->nx * sizeof(double), cudaMemcpyDefault, ctx->st));
@@ -1065,6 +1289,7 @@ int paratc_write_restart(paratc_ctx* ctx, const char* path, int with_hist) {
     std::vector<double> buf(n);
     FILE* fp = std::fopen(path, "wb");
     if (!fp) return set_err(ctx, PARATC_ERR_IO, std::string("cannot open ") + path);
+    refresh64(ctx);
     std::vector<double*> order = {ctx->f.ux, ctx->f.uy, ctx->f.uz, ctx->f.pr};
     if (ctx->prm.scalar_on) order.push_back(ctx->f.sc);
     if (with_hist) {
@@ -1134,6 +1359,7 @@ int paratc_stats_reset(paratc_ctx* ctx) {
 int paratc_stats_accumulate(paratc_ctx* ctx) {
     if (!ctx) return PARATC_ERR_BAD_ARG;
     CK(cudaSetDevice(ctx->dev));
+    refresh64(ctx);
     const int ns = stats_count(ctx->kc);
     launch_stats(ctx->st, ctx->kc, ctx->dm, ctx->f, ctx->d_coef, ctx->d_stats_part, ctx->d_stats,
                  ctx->d_stats + (size_t)ctx->nyp * ns);
@@ -1188,6 +1414,7 @@ int paratc_spectra_accumulate(paratc_ctx* ctx, int jlcs) {
     CK(cudaSetDevice(ctx->dev));
     int rc = spectra_alloc(ctx);
     if (rc != PARATC_OK) return rc;
+    refresh64(ctx);
     launch_spectra(ctx->st, 0, ctx->kc, ctx->f, jlcs, ctx->d_twxf, ctx->d_spec_part, ctx->d_specx);
     launch_spectra(ctx->st, 1, ctx->kc, ctx->f, jlcs, ctx->d_twz, ctx->d_spec_part, ctx->d_specz);
     ctx->launches += 4;
@@ -1283,6 +1510,7 @@ int paratc_spectra2d_accumulate(paratc_ctx* ctx) {
     if (!ctx) return PARATC_ERR_BAD_ARG;
     if (ctx->nsel2 == 0) return set_err(ctx, PARATC_ERR_BAD_ARG, "spectra2d: not set up");
     CK(cudaSetDevice(ctx->dev));
+    refresh64(ctx);
     launch_spectra2d(ctx->st, ctx->kc, ctx->f, ctx->d_fj, ctx->nfj2, ctx->nsel2, ctx->nmir2, ctx->nfld2, ctx->d_twxf,
                      ctx->d_twz, ctx->d_s2, ctx->d_spec2d);
     ctx->launches += 3;
@@ -1322,6 +1550,7 @@ int paratc_visu_quantity(paratc_ctx* ctx, int q, int iskip, int jskip, int kskip
         if ((rc = dalloc(ctx, &ctx->d_visu, ctx->ni)) || (rc = dalloc(ctx, &ctx->d_visu_bad, 1))) return rc;
     }
     CK(cudaMemsetAsync(ctx->d_visu_bad, 0, sizeof(unsigned int), ctx->st));
+    refresh64(ctx);
     launch_visu(ctx->st, q, iskip, jskip, kskip, node, ctx->kc, ctx->dm, ctx->f, ctx->d_visu, ctx->d_visu_bad);
     ctx->launches += 1;
     CK(cudaGetLastError());
@@ -1349,6 +1578,7 @@ int paratc_visu_quantity_device(paratc_ctx* ctx, int q, int iskip, int jskip, in
         }
         d_nbad = ctx->d_visu_bad;
     }
+    refresh64(ctx);
     launch_visu(ctx->st, q, iskip, jskip, kskip, node, ctx->kc, ctx->dm, ctx->f, d_out, d_nbad);
     ctx->launches += 1;
     CK(cudaGetLastError());

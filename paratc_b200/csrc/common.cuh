@@ -98,6 +98,27 @@ __device__ __forceinline__ int wrapi(int i, int n) { return i < 0 ? i + n : (i >
 // NaN anywhere reaches the grid-wide result (the non-finite guard's input)
 __device__ __forceinline__ double nmax(double a, double b) { return (a > b || a != a) ? a : b; }
 
+// Loads and stores between either storage precision and FP64 registers: the
+// FP32 storage form keeps fields and spectra in float / float2 while every
+// kernel computes in double (loads widen exactly, stores round to nearest).
+// ld_pair / st_pair move the two values at an even index p[0], p[1].
+__device__ __forceinline__ double2 ld_pair(const double* p) { return __ldg(reinterpret_cast<const double2*>(p)); }
+__device__ __forceinline__ double2 ld_pair(const float* p) {
+    const float2 v = __ldg(reinterpret_cast<const float2*>(p));
+    return make_double2(v.x, v.y);
+}
+__device__ __forceinline__ void st_pair(double* p, double2 v) { *reinterpret_cast<double2*>(p) = v; }
+__device__ __forceinline__ void st_pair(float* p, double2 v) {
+    *reinterpret_cast<float2*>(p) = make_float2((float)v.x, (float)v.y);
+}
+__device__ __forceinline__ double2 ld_c(const double2* p) { return *p; }
+__device__ __forceinline__ double2 ld_c(const float2* p) {
+    const float2 v = *p;
+    return make_double2(v.x, v.y);
+}
+__device__ __forceinline__ void st_c(double2* p, double2 v) { *p = v; }
+__device__ __forceinline__ void st_c(float2* p, double2 v) { *p = make_float2((float)v.x, (float)v.y); }
+
 __device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
 __device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {

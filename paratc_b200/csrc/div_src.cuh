@@ -14,25 +14,26 @@ struct DivTaps {
     double um, rdyp;
 };
 
-__device__ __forceinline__ void div_load(DivTaps& t, const DConst& c, const DMetric& m, const double* __restrict__ ux,
-                                         const double* __restrict__ uy, const double* __restrict__ uz, int g, int e) {
+template <class V>
+__device__ __forceinline__ void div_load(DivTaps& t, const DConst& c, const DMetric& m, const V* __restrict__ ux,
+                                         const V* __restrict__ uy, const V* __restrict__ uz, int g, int e) {
     const int nx = c.nx, ny = c.ny, nz = c.nz;
     const size_t pl = (size_t)c.nyt * nx;
     const int k = g / ny, jc = g - k * ny + 1;
     const int km = k == 0 ? nz - 1 : k - 1, kp = k == nz - 1 ? 0 : k + 1, ku = kp == nz - 1 ? 0 : kp + 1;
     const int i0 = 2 * e, im = i0 == 0 ? nx - 1 : i0 - 1, i2 = i0 + 2 == nx ? 0 : i0 + 2;
     const size_t r0 = (size_t)jc * nx;
-    const double* ur = ux + (size_t)k * pl + r0;
-    const double* vr = uy + (size_t)k * pl + r0;
-    t.u01 = __ldg(reinterpret_cast<const double2*>(ur + i0));
-    t.u23 = __ldg(reinterpret_cast<const double2*>(ur + i2));
-    t.um = __ldg(ur + im);
-    t.v0 = __ldg(reinterpret_cast<const double2*>(vr + i0));
-    t.v1 = __ldg(reinterpret_cast<const double2*>(vr + nx + i0));
-    t.w0 = __ldg(reinterpret_cast<const double2*>(uz + (size_t)km * pl + r0 + i0));
-    t.w1 = __ldg(reinterpret_cast<const double2*>(uz + (size_t)k * pl + r0 + i0));
-    t.w2 = __ldg(reinterpret_cast<const double2*>(uz + (size_t)kp * pl + r0 + i0));
-    t.w3 = __ldg(reinterpret_cast<const double2*>(uz + (size_t)ku * pl + r0 + i0));
+    const V* ur = ux + (size_t)k * pl + r0;
+    const V* vr = uy + (size_t)k * pl + r0;
+    t.u01 = ld_pair(ur + i0);
+    t.u23 = ld_pair(ur + i2);
+    t.um = (double)__ldg(ur + im);
+    t.v0 = ld_pair(vr + i0);
+    t.v1 = ld_pair(vr + nx + i0);
+    t.w0 = ld_pair(uz + (size_t)km * pl + r0 + i0);
+    t.w1 = ld_pair(uz + (size_t)k * pl + r0 + i0);
+    t.w2 = ld_pair(uz + (size_t)kp * pl + r0 + i0);
+    t.w3 = ld_pair(uz + (size_t)ku * pl + r0 + i0);
     t.rdyp = __ldg(&m.rdyp[jc]);
 }
 
@@ -49,9 +50,9 @@ __device__ __forceinline__ double2 div_eval(const DivTaps& t, const DConst& c) {
 // the source of every point pair f = start, start + STRIDE, ... < B*N of a
 // batch of B rows from g0 (pair e of row b = f / N), U pairs in flight per
 // thread: st(b, e, value) stores it, the running max|div| goes to dm
-template <int N, int B, int STRIDE, int U, class ST>
-__device__ __forceinline__ void div_batch(const DConst& c, const DMetric& m, const double* __restrict__ ux,
-                                          const double* __restrict__ uy, const double* __restrict__ uz, int g0,
+template <int N, int B, int STRIDE, int U, class V, class ST>
+__device__ __forceinline__ void div_batch(const DConst& c, const DMetric& m, const V* __restrict__ ux,
+                                          const V* __restrict__ uy, const V* __restrict__ uz, int g0,
                                           int nrows, double sudtal, int start, double& dm, const ST& st) {
     for (int f0 = start; f0 < B * N; f0 += U * STRIDE) {
         DivTaps tp[U];

@@ -45,11 +45,13 @@ struct XK {
     static constexpr size_t smem = ((size_t)(N + 1) * PITCH + N) * sizeof(double2);
 };
 
-template <int N>
+// V: storage of the velocity (mode 0/1), S: storage of the spectrum; the
+// given source of mode 2 is FP64
+template <int N, class V, class S>
 __global__ void __launch_bounds__(XK<N>::P)
-    k_xf(int mode, DConst c, DMetric m, const DCoef* __restrict__ coef, const double* __restrict__ ux,
-         const double* __restrict__ uy, const double* __restrict__ uz, const double* __restrict__ src,
-         double2* __restrict__ spec, const double2* __restrict__ twN, const double2* __restrict__ post,
+    k_xf(int mode, DConst c, DMetric m, const DCoef* __restrict__ coef, const V* __restrict__ ux,
+         const V* __restrict__ uy, const V* __restrict__ uz, const double* __restrict__ src,
+         S* __restrict__ spec, const double2* __restrict__ twN, const double2* __restrict__ post,
          double* __restrict__ part, unsigned int* __restrict__ counter, double* __restrict__ out_max) {
     constexpr int B = XK<N>::B, P = XK<N>::P, PITCH = XK<N>::PITCH, M1 = N + 1;
     constexpr ff::Sched SC = ff::make_sched(N);
@@ -86,7 +88,7 @@ __global__ void __launch_bounds__(XK<N>::P)
         const double2 zb = buf[(a == 0 ? 0 : N - a) * PITCH + b];
         const double2 E = make_double2(0.5 * (za.x + zb.x), 0.5 * (za.y - zb.y));
         const double2 O = make_double2(0.5 * (za.y + zb.y), -0.5 * (za.x - zb.x));
-        spec[(size_t)g0 * M1 + f] = cadd(E, cmul(__ldg(&post[a]), O));
+        st_c(spec + (size_t)g0 * M1 + f, cadd(E, cmul(__ldg(&post[a]), O)));
     }
     if (mode == 2) return;
     double v[1] = {dm};
@@ -98,10 +100,12 @@ __global__ void __launch_bounds__(XK<N>::P)
     if (tid == 0) *out_max = tot[0];
 }
 
-template <int N>
+// S: storage of the spectrum, P: of the potential; accumulate != 0 adds the
+// result to phi (unpadded rows: the corrections of the refined solve)
+template <int N, class S, class PH>
 __global__ void __launch_bounds__(XK<N>::P)
-    k_xb(int ny, int nz, const double2* __restrict__ spec, double* __restrict__ phi, const double2* __restrict__ twN,
-         const double2* __restrict__ post, double scale, int padded) {
+    k_xb(int ny, int nz, const S* __restrict__ spec, PH* __restrict__ phi, const double2* __restrict__ twN,
+         const double2* __restrict__ post, double scale, int padded, int accumulate) {
     constexpr int B = XK<N>::B, P = XK<N>::P, PITCH = XK<N>::PITCH, M1 = N + 1;
     constexpr ff::Sched SC = ff::make_sched(N);
     extern __shared__ double2 smx[];
@@ -115,8 +119,9 @@ __global__ void __launch_bounds__(XK<N>::P)
     pdl_trigger();
     for (int f = tid; f < B * M1; f += P) {
         const int b = f / M1, a = f - b * M1;
-        if (g0 + b < nrows) cpa16(&buf[a * PITCH + b], spec + (size_t)g0 * M1 + f);
-        else buf[a * PITCH + b] = make_double2(0.0, 0.0);
+        if (g0 + b >= nrows) buf[a * PITCH + b] = make_double2(0.0, 0.0);
+        else if constexpr (sizeof(S) == sizeof(double2)) cpa16(&buf[a * PITCH + b], spec + (size_t)g0 * M1 + f);
+        else buf[a * PITCH + b] = ld_c(spec + (size_t)g0 * M1 + f);
     }
     cpa_wait_all();
     __syncthreads();
@@ -150,16 +155,21 @@ __global__ void __launch_bounds__(XK<N>::P)
         const int g = g0 + b;
         if (g >= nrows) continue;
         const double2 z = buf[e * PITCH + b];
-        const double2 v = make_double2(z.x * scale, z.y * scale);
+        double2 v = make_double2(z.x * scale, z.y * scale);
         if (!padded) {
-            reinterpret_cast<double2*>(phi + (size_t)g * nx)[e] = v;
+            PH* dst = phi + (size_t)g * nx + 2 * e;
+            if (accumulate) {
+                const double2 o = ld_pair(dst);
+                v = make_double2(o.x + v.x, o.y + v.y);
+            }
+            st_pair(dst, v);
             continue;
         }
         const int k = g / ny, jc = g - k * ny + 1;
-        double* rowp = phi + ((size_t)k * nyt + jc) * nx;
-        reinterpret_cast<double2*>(rowp)[e] = v;
-        if (jc == 1) reinterpret_cast<double2*>(rowp - nx)[e] = v;
-        if (jc == ny) reinterpret_cast<double2*>(rowp + nx)[e] = v;
+        PH* rowp = phi + ((size_t)k * nyt + jc) * nx + 2 * e;
+        st_pair(rowp, v);
+        if (jc == 1) st_pair(rowp - nx, v);
+        if (jc == ny) st_pair(rowp + nx, v);
     }
 }
 
@@ -168,6 +178,9 @@ __global__ void __launch_bounds__(XK<N>::P)
 
 }  // namespace
 
+#ifndef PTC_STORE32
+// FP64 instantiations; the FP32 storage forms (float2 spectra) are compiled
+// in k_pfft_x32.cu from these same kernels
 bool pfft_x_supported(int n) {
     switch (n) {
 #define X_CASE(n) case n:
@@ -188,24 +201,40 @@ int pfft_x_blocks(int nx, int ny, int nz) {
     }
     return (ny * nz + b - 1) / b;
 }
+#define XF_TYPES(X, n) X(n, double, double2)
+#define XB_TYPES(X, n) X(n, double2, double)
+#else
+#define XF_TYPES(X, n) X(n, float, float2) X(n, double, float2)
+#define XB_TYPES(X, n) X(n, float2, float) X(n, float2, double)
+#endif
 
+#ifndef PTC_STORE32
 void pfft_x_init() {
-#define X_CASE(n)                                                                                              \
-    cudaFuncSetAttribute(k_xf<n>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)XK<n>::smem);              \
-    cudaFuncSetAttribute(k_xb<n>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)XK<n>::smem);
+    pfft_x_init32();
+#else
+void pfft_x_init32() {
+#endif
+#define XF_ATTR(n, V, S)                                                                                        \
+    cudaFuncSetAttribute(k_xf<n, V, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)XK<n>::smem);
+#define XB_ATTR(n, S, PH)                                                                                        \
+    cudaFuncSetAttribute(k_xb<n, S, PH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)XK<n>::smem);
+#define X_CASE(n) XF_TYPES(XF_ATTR, n) XB_TYPES(XB_ATTR, n)
     PFFT_X_SIZES(X_CASE)
 #undef X_CASE
+#undef XF_ATTR
+#undef XB_ATTR
 }
 
-void launch_pfft_xf(cudaStream_t st, int mode, const DConst& c, const DMetric& m, const DCoef* coef, const Fields& f,
-                    const double* src, double2* spec, const double2* twx, const double2* post, double* part,
-                    unsigned int* counter, double* out_max) {
+template <class V, class S>
+static void pfft_xf_t(cudaStream_t st, int mode, const DConst& c, const DMetric& m, const DCoef* coef,
+                      const FieldSet<V>& f, const double* src, S* spec, const double2* twx, const double2* post,
+                      double* part, unsigned int* counter, double* out_max) {
     const int nrows = c.ny * c.nz;
     switch (c.nx / 2) {
 #define X_CASE(n)                                                                                              \
     case n:                                                                                                    \
-        launch_pdl(k_xf<n>, dim3((nrows + XK<n>::B - 1) / XK<n>::B), dim3(XK<n>::P), XK<n>::smem, st, mode, c, m, \
-                   coef, f.ux, f.uy, f.uz, src, spec, twx, post, part, counter, out_max);                      \
+        launch_pdl(k_xf<n, V, S>, dim3((nrows + XK<n>::B - 1) / XK<n>::B), dim3(XK<n>::P), XK<n>::smem, st, mode, \
+                   c, m, coef, f.ux, f.uy, f.uz, src, spec, twx, post, part, counter, out_max);               \
         break;
         PFFT_X_SIZES(X_CASE)
 #undef X_CASE
@@ -213,19 +242,51 @@ void launch_pfft_xf(cudaStream_t st, int mode, const DConst& c, const DMetric& m
     }
 }
 
-void launch_pfft_xb(cudaStream_t st, int nx, int ny, int nz, const double2* spec, double* phi, const double2* twx,
-                    const double2* post, double scale, int padded) {
+template <class S, class PH>
+static void pfft_xb_t(cudaStream_t st, int nx, int ny, int nz, const S* spec, PH* phi, const double2* twx,
+                      const double2* post, double scale, int padded, int accumulate) {
     const int nrows = ny * nz;
     switch (nx / 2) {
 #define X_CASE(n)                                                                                              \
     case n:                                                                                                    \
-        launch_pdl(k_xb<n>, dim3((nrows + XK<n>::B - 1) / XK<n>::B), dim3(XK<n>::P), XK<n>::smem, st, ny, nz,    \
-                   spec, phi, twx, post, scale, padded);                                                       \
+        launch_pdl(k_xb<n, S, PH>, dim3((nrows + XK<n>::B - 1) / XK<n>::B), dim3(XK<n>::P), XK<n>::smem, st, ny, \
+                   nz, spec, phi, twx, post, scale, padded, accumulate);                                       \
         break;
         PFFT_X_SIZES(X_CASE)
 #undef X_CASE
         default: break;
     }
 }
+
+#ifndef PTC_STORE32
+void launch_pfft_xf(cudaStream_t st, int mode, const DConst& c, const DMetric& m, const DCoef* coef, const Fields& f,
+                    const double* src, double2* spec, const double2* twx, const double2* post, double* part,
+                    unsigned int* counter, double* out_max) {
+    pfft_xf_t(st, mode, c, m, coef, f, src, spec, twx, post, part, counter, out_max);
+}
+void launch_pfft_xb(cudaStream_t st, int nx, int ny, int nz, const double2* spec, double* phi, const double2* twx,
+                    const double2* post, double scale, int padded) {
+    pfft_xb_t(st, nx, ny, nz, spec, phi, twx, post, scale, padded, 0);
+}
+#else
+void launch_pfft_xf(cudaStream_t st, int mode, const DConst& c, const DMetric& m, const DCoef* coef,
+                    const Fields32& f, const double* src, float2* spec, const double2* twx, const double2* post,
+                    double* part, unsigned int* counter, double* out_max) {
+    pfft_xf_t(st, mode, c, m, coef, f, src, spec, twx, post, part, counter, out_max);
+}
+void launch_pfft_xf(cudaStream_t st, const DConst& c, const double* src, float2* spec, const double2* twx,
+                    const double2* post) {
+    const Fields none = {};
+    pfft_xf_t(st, 2, c, DMetric{}, nullptr, none, src, spec, twx, post, nullptr, nullptr, nullptr);
+}
+void launch_pfft_xb(cudaStream_t st, int nx, int ny, int nz, const float2* spec, float* phi, const double2* twx,
+                    const double2* post, double scale, int padded) {
+    pfft_xb_t(st, nx, ny, nz, spec, phi, twx, post, scale, padded, 0);
+}
+void launch_pfft_xb(cudaStream_t st, int nx, int ny, int nz, const float2* spec, double* phi, const double2* twx,
+                    const double2* post, double scale, int accumulate) {
+    pfft_xb_t(st, nx, ny, nz, spec, phi, twx, post, scale, 0, accumulate);
+}
+#endif
 
 }  // namespace ptc

@@ -25,23 +25,27 @@ struct ZK {
     static constexpr size_t smem = ((size_t)N * B + N) * sizeof(double2);
 };
 
+// global element e of column b, in the spectrum's storage type S (double2,
+// or float2 in the FP32 storage form; the passes compute in double either way)
+template <class S>
 struct GLd {
-    const double2* base;
+    const S* base;
     int ncol, nvalid;
     __device__ __forceinline__ double2 operator()(int e, int b) const {
-        return b < nvalid ? base[(size_t)e * ncol + b] : make_double2(0.0, 0.0);
+        return b < nvalid ? ld_c(base + (size_t)e * ncol + b) : make_double2(0.0, 0.0);
     }
 };
+template <class S>
 struct GSt {
-    double2* base;
+    S* base;
     int ncol, nvalid;
     __device__ __forceinline__ void operator()(int e, int b, double2 v) const {
-        if (b < nvalid) base[(size_t)e * ncol + b] = v;
+        if (b < nvalid) st_c(base + (size_t)e * ncol + b, v);
     }
 };
 
-template <int N, int DIR>
-__global__ void __launch_bounds__(ZK<N>::P) k_zt(int ncol, double2* __restrict__ spec, const double2* __restrict__ twN) {
+template <int N, int DIR, class S>
+__global__ void __launch_bounds__(ZK<N>::P) k_zt(int ncol, S* __restrict__ spec, const double2* __restrict__ twN) {
     constexpr int B = ZK<N>::B, P = ZK<N>::P;
     constexpr ff::Sched SC = ff::make_sched(N);
     extern __shared__ double2 smz[];
@@ -50,8 +54,8 @@ __global__ void __launch_bounds__(ZK<N>::P) k_zt(int ncol, double2* __restrict__
     const int tid = threadIdx.x;
     const int q0 = blockIdx.x * B;
     const int nvalid = min(B, ncol - q0);
-    const GLd gl{spec + q0, ncol, nvalid};
-    const GSt gs{spec + q0, ncol, nvalid};
+    const GLd<S> gl{spec + q0, ncol, nvalid};
+    const GSt<S> gs{spec + q0, ncol, nvalid};
     if constexpr (SC.np == 1) {
         pdl_wait();
         pdl_trigger();
@@ -85,26 +89,35 @@ bool pfft_z_supported(int n) {
 
 void pfft_z_init() {
 #define Z_CASE(n)                                                                                              \
-    cudaFuncSetAttribute(k_zt<n, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ZK<n>::smem);         \
-    cudaFuncSetAttribute(k_zt<n, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ZK<n>::smem);
+    cudaFuncSetAttribute(k_zt<n, -1, double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ZK<n>::smem); \
+    cudaFuncSetAttribute(k_zt<n, 1, double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ZK<n>::smem);  \
+    cudaFuncSetAttribute(k_zt<n, -1, float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ZK<n>::smem);  \
+    cudaFuncSetAttribute(k_zt<n, 1, float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ZK<n>::smem);
     PFFT_Z_SIZES(Z_CASE)
 #undef Z_CASE
 }
 
-void launch_pfft_z(cudaStream_t st, int dir, int nx, int ny, int nz, double2* spec, const double2* twz) {
+template <class S>
+static void pfft_z_t(cudaStream_t st, int dir, int nx, int ny, int nz, S* spec, const double2* twz) {
     const int ncol = ny * (nx / 2 + 1);
     switch (nz) {
-#define Z_CASE(n)                                                                                              \
-    case n: {                                                                                                  \
-        const int grid = (ncol + ZK<n>::B - 1) / ZK<n>::B;                                                     \
-        if (dir < 0) launch_pdl(k_zt<n, -1>, dim3(grid), dim3(ZK<n>::P), ZK<n>::smem, st, ncol, spec, twz);     \
-        else launch_pdl(k_zt<n, 1>, dim3(grid), dim3(ZK<n>::P), ZK<n>::smem, st, ncol, spec, twz);              \
-        break;                                                                                                 \
+#define Z_CASE(n)                                                                                                 \
+    case n: {                                                                                                     \
+        const int grid = (ncol + ZK<n>::B - 1) / ZK<n>::B;                                                        \
+        if (dir < 0) launch_pdl(k_zt<n, -1, S>, dim3(grid), dim3(ZK<n>::P), ZK<n>::smem, st, ncol, spec, twz);     \
+        else launch_pdl(k_zt<n, 1, S>, dim3(grid), dim3(ZK<n>::P), ZK<n>::smem, st, ncol, spec, twz);              \
+        break;                                                                                                    \
     }
         PFFT_Z_SIZES(Z_CASE)
 #undef Z_CASE
         default: break;
     }
+}
+void launch_pfft_z(cudaStream_t st, int dir, int nx, int ny, int nz, double2* spec, const double2* twz) {
+    pfft_z_t(st, dir, nx, ny, nz, spec, twz);
+}
+void launch_pfft_z(cudaStream_t st, int dir, int nx, int ny, int nz, float2* spec, const double2* twz) {
+    pfft_z_t(st, dir, nx, ny, nz, spec, twz);
 }
 
 }  // namespace ptc

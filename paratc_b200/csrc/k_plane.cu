@@ -60,11 +60,13 @@ __device__ __forceinline__ void load_tw(double2* tx, double2* tp, double2* tz, c
 
 // MODE 0: source = divergence of u* / pmAlpha (clcPrSrc) with max|div| to
 // out_max; 1: the divergence unscaled; 2: the compact source array src
-template <int M, int NZ>
+// V: storage of the velocity, S: of the spectrum (the given source of mode 2
+// is FP64); the transforms compute in double either way
+template <int M, int NZ, class V, class S>
 __global__ void __launch_bounds__(PL_P, 1)
-    k_plane_f(int mode, DConst c, DMetric m, const DCoef* __restrict__ coef, const double* __restrict__ ux,
-              const double* __restrict__ uy, const double* __restrict__ uz, const double* __restrict__ src,
-              double2* __restrict__ spec, const double2* __restrict__ twx, const double2* __restrict__ post,
+    k_plane_f(int mode, DConst c, DMetric m, const DCoef* __restrict__ coef, const V* __restrict__ ux,
+              const V* __restrict__ uy, const V* __restrict__ uz, const double* __restrict__ src,
+              S* __restrict__ spec, const double2* __restrict__ twx, const double2* __restrict__ post,
               const double2* __restrict__ twz, double* __restrict__ part, unsigned int* __restrict__ counter,
               double* __restrict__ out_max) {
     constexpr int M1 = PK<M, NZ>::M1, PITCH = PK<M, NZ>::PITCH;
@@ -97,17 +99,17 @@ __global__ void __launch_bounds__(PL_P, 1)
             const int k = f / M, e = f - k * M;
             const int km = k == 0 ? NZ - 1 : k - 1, kp = k == NZ - 1 ? 0 : k + 1, ku = kp == NZ - 1 ? 0 : kp + 1;
             const int i0 = 2 * e, im = i0 == 0 ? nx - 1 : i0 - 1, i2 = i0 + 2 == nx ? 0 : i0 + 2;
-            const double* ur = ux + (size_t)k * pl + r0;
-            const double* vr = uy + (size_t)k * pl + r0;
-            const double2 u01 = __ldg(reinterpret_cast<const double2*>(ur + i0));
-            const double2 u23 = __ldg(reinterpret_cast<const double2*>(ur + i2));
-            const double um = __ldg(ur + im);
-            const double2 v0 = __ldg(reinterpret_cast<const double2*>(vr + i0));
-            const double2 v1 = __ldg(reinterpret_cast<const double2*>(vr + nx + i0));
-            const double2 w0 = __ldg(reinterpret_cast<const double2*>(uz + (size_t)km * pl + r0 + i0));
-            const double2 w1 = __ldg(reinterpret_cast<const double2*>(uz + (size_t)k * pl + r0 + i0));
-            const double2 w2 = __ldg(reinterpret_cast<const double2*>(uz + (size_t)kp * pl + r0 + i0));
-            const double2 w3 = __ldg(reinterpret_cast<const double2*>(uz + (size_t)ku * pl + r0 + i0));
+            const V* ur = ux + (size_t)k * pl + r0;
+            const V* vr = uy + (size_t)k * pl + r0;
+            const double2 u01 = ld_pair(ur + i0);
+            const double2 u23 = ld_pair(ur + i2);
+            const double um = (double)__ldg(ur + im);
+            const double2 v0 = ld_pair(vr + i0);
+            const double2 v1 = ld_pair(vr + nx + i0);
+            const double2 w0 = ld_pair(uz + (size_t)km * pl + r0 + i0);
+            const double2 w1 = ld_pair(uz + (size_t)k * pl + r0 + i0);
+            const double2 w2 = ld_pair(uz + (size_t)kp * pl + r0 + i0);
+            const double2 w3 = ld_pair(uz + (size_t)ku * pl + r0 + i0);
             const double dudx0 = c.dxC[0] * um + c.dxC[1] * u01.x + c.dxC[2] * u01.y + c.dxC[3] * u23.x;
             const double dudx1 = c.dxC[0] * u01.x + c.dxC[1] * u01.y + c.dxC[2] * u23.x + c.dxC[3] * u23.y;
             const double dvdy0 = (v1.x - v0.x) * rdyp, dvdy1 = (v1.y - v0.y) * rdyp;
@@ -141,7 +143,7 @@ __global__ void __launch_bounds__(PL_P, 1)
     ff::smem_passes<NZ, M1, PITCH, PL_P, -1, 0, SZ.np, PL_BITS, true>(buf, tz, tid);
     for (int f = tid; f < M1 * NZ; f += PL_P) {
         const int k = f / M1, kx = f - k * M1;
-        spec[((size_t)k * ny + j) * M1 + kx] = buf[kx * PITCH + k];
+        st_c(spec + ((size_t)k * ny + j) * M1 + kx, buf[kx * PITCH + k]);
     }
     if (mode == 2) return;
     double v[1] = {dm};
@@ -153,10 +155,13 @@ __global__ void __launch_bounds__(PL_P, 1)
     if (tid == 0) *out_max = tot[0];
 }
 
-template <int M, int NZ>
+// S: storage of the spectrum, PH: of the potential; accumulate != 0 adds the
+// result to phi (unpadded rows: the corrections of the refined solve)
+template <int M, int NZ, class S, class PH>
 __global__ void __launch_bounds__(PL_P, 1)
-    k_plane_b(int ny, const double2* __restrict__ spec, double* __restrict__ phi, const double2* __restrict__ twx,
-              const double2* __restrict__ post, const double2* __restrict__ twz, double scale, int padded) {
+    k_plane_b(int ny, const S* __restrict__ spec, PH* __restrict__ phi, const double2* __restrict__ twx,
+              const double2* __restrict__ post, const double2* __restrict__ twz, double scale, int padded,
+              int accumulate) {
     constexpr int M1 = PK<M, NZ>::M1, PITCH = PK<M, NZ>::PITCH;
     constexpr ff::Sched SX = ff::make_sched(M, PL_BITS), SZ = ff::make_sched(NZ, PL_BITS);
     extern __shared__ double2 smp[];
@@ -172,7 +177,8 @@ __global__ void __launch_bounds__(PL_P, 1)
     pdl_trigger();
     for (int f = tid; f < M1 * NZ; f += PL_P) {
         const int k = f / M1, kx = f - k * M1;
-        cpa16p(&buf[kx * PITCH + k], spec + ((size_t)k * ny + j) * M1 + kx);
+        if constexpr (sizeof(S) == sizeof(double2)) cpa16p(&buf[kx * PITCH + k], spec + ((size_t)k * ny + j) * M1 + kx);
+        else buf[kx * PITCH + k] = ld_c(spec + ((size_t)k * ny + j) * M1 + kx);
     }
     asm volatile("cp.async.commit_group;\n" ::: "memory");
     asm volatile("cp.async.wait_group 0;\n" ::: "memory");
@@ -205,15 +211,20 @@ __global__ void __launch_bounds__(PL_P, 1)
     for (int f = tid; f < NZ * M; f += PL_P) {
         const int k = f / M, e = f - k * M;
         const double2 z = buf[e * PITCH + k];
-        const double2 v = make_double2(z.x * scale, z.y * scale);
+        double2 v = make_double2(z.x * scale, z.y * scale);
         if (!padded) {
-            reinterpret_cast<double2*>(phi + ((size_t)k * ny + j) * nx)[e] = v;
+            PH* dst = phi + ((size_t)k * ny + j) * nx + 2 * e;
+            if (accumulate) {
+                const double2 o = ld_pair(dst);
+                v = make_double2(o.x + v.x, o.y + v.y);
+            }
+            st_pair(dst, v);
             continue;
         }
-        double* rowp = phi + ((size_t)k * nyt + (j + 1)) * nx;
-        reinterpret_cast<double2*>(rowp)[e] = v;
-        if (j == 0) reinterpret_cast<double2*>(rowp - nx)[e] = v;
-        if (j == ny - 1) reinterpret_cast<double2*>(rowp + nx)[e] = v;
+        PH* rowp = phi + ((size_t)k * nyt + (j + 1)) * nx + 2 * e;
+        st_pair(rowp, v);
+        if (j == 0) st_pair(rowp - nx, v);
+        if (j == ny - 1) st_pair(rowp + nx, v);
     }
 }
 
@@ -223,6 +234,8 @@ __global__ void __launch_bounds__(PL_P, 1)
 
 }  // namespace
 
+#ifndef PTC_STORE32
+// FP64 instantiations; the FP32 storage forms are compiled in k_plane32.cu
 bool plane_supported(int nx, int nz) {
 #define P_CASE(a, b) \
     if (nx / 2 == a && nz == b) return PK<a, b>::fits;
@@ -230,25 +243,39 @@ bool plane_supported(int nx, int nz) {
 #undef P_CASE
     return false;
 }
-
+#define PF_TYPES(X, a, b) X(a, b, double, double2)
+#define PB_TYPES(X, a, b) X(a, b, double2, double)
 void plane_init() {
-#define P_CASE(a, b)                                                                                           \
-    if constexpr (PK<a, b>::fits) {                                                                            \
-        cudaFuncSetAttribute(k_plane_f<a, b>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PK<a, b>::smem); \
-        cudaFuncSetAttribute(k_plane_b<a, b>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PK<a, b>::smem); \
+    plane_init32();
+#else
+#define PF_TYPES(X, a, b) X(a, b, float, float2) X(a, b, double, float2)
+#define PB_TYPES(X, a, b) X(a, b, float2, float) X(a, b, float2, double)
+void plane_init32() {
+#endif
+#define PF_ATTR(a, b, V, S) \
+    cudaFuncSetAttribute(k_plane_f<a, b, V, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PK<a, b>::smem);
+#define PB_ATTR(a, b, S, PH) \
+    cudaFuncSetAttribute(k_plane_b<a, b, S, PH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PK<a, b>::smem);
+#define P_CASE(a, b)                       \
+    if constexpr (PK<a, b>::fits) {        \
+        PF_TYPES(PF_ATTR, a, b)            \
+        PB_TYPES(PB_ATTR, a, b)            \
     }
     PLANE_PAIRS(P_CASE)
 #undef P_CASE
+#undef PF_ATTR
+#undef PB_ATTR
 }
 
-void launch_plane_f(cudaStream_t st, int mode, const DConst& c, const DMetric& m, const DCoef* coef, const Fields& f,
-                    const double* src, double2* spec, const double2* twx, const double2* post, const double2* twz,
-                    double* part, unsigned int* counter, double* out_max) {
+template <class V, class S>
+static void plane_f_t(cudaStream_t st, int mode, const DConst& c, const DMetric& m, const DCoef* coef,
+                      const FieldSet<V>& f, const double* src, S* spec, const double2* twx, const double2* post,
+                      const double2* twz, double* part, unsigned int* counter, double* out_max) {
 #define P_CASE(a, b)                                                                                           \
     if constexpr (PK<a, b>::fits) {                                                                            \
         if (c.nx / 2 == a && c.nz == b) {                                                                      \
-            launch_pdl(k_plane_f<a, b>, dim3(c.ny), dim3(PL_P), PK<a, b>::smem, st, mode, c, m, coef, f.ux, f.uy, \
-                       f.uz, src, spec, twx, post, twz, part, counter, out_max);                               \
+            launch_pdl(k_plane_f<a, b, V, S>, dim3(c.ny), dim3(PL_P), PK<a, b>::smem, st, mode, c, m, coef, f.ux, \
+                       f.uy, f.uz, src, spec, twx, post, twz, part, counter, out_max);                         \
             return;                                                                                            \
         }                                                                                                      \
     }
@@ -256,18 +283,50 @@ void launch_plane_f(cudaStream_t st, int mode, const DConst& c, const DMetric& m
 #undef P_CASE
 }
 
-void launch_plane_b(cudaStream_t st, int nx, int ny, int nz, const double2* spec, double* phi, const double2* twx,
-                    const double2* post, const double2* twz, double scale, int padded) {
+template <class S, class PH>
+static void plane_b_t(cudaStream_t st, int nx, int ny, int nz, const S* spec, PH* phi, const double2* twx,
+                      const double2* post, const double2* twz, double scale, int padded, int accumulate) {
 #define P_CASE(a, b)                                                                                           \
     if constexpr (PK<a, b>::fits) {                                                                            \
         if (nx / 2 == a && nz == b) {                                                                          \
-            launch_pdl(k_plane_b<a, b>, dim3(ny), dim3(PL_P), PK<a, b>::smem, st, ny, spec, phi, twx, post, twz, \
-                       scale, padded);                                                                         \
+            launch_pdl(k_plane_b<a, b, S, PH>, dim3(ny), dim3(PL_P), PK<a, b>::smem, st, ny, spec, phi, twx, post, \
+                       twz, scale, padded, accumulate);                                                        \
             return;                                                                                            \
         }                                                                                                      \
     }
     PLANE_PAIRS(P_CASE)
 #undef P_CASE
 }
+
+#ifndef PTC_STORE32
+void launch_plane_f(cudaStream_t st, int mode, const DConst& c, const DMetric& m, const DCoef* coef, const Fields& f,
+                    const double* src, double2* spec, const double2* twx, const double2* post, const double2* twz,
+                    double* part, unsigned int* counter, double* out_max) {
+    plane_f_t(st, mode, c, m, coef, f, src, spec, twx, post, twz, part, counter, out_max);
+}
+void launch_plane_b(cudaStream_t st, int nx, int ny, int nz, const double2* spec, double* phi, const double2* twx,
+                    const double2* post, const double2* twz, double scale, int padded) {
+    plane_b_t(st, nx, ny, nz, spec, phi, twx, post, twz, scale, padded, 0);
+}
+#else
+void launch_plane_f(cudaStream_t st, int mode, const DConst& c, const DMetric& m, const DCoef* coef,
+                    const Fields32& f, const double* src, float2* spec, const double2* twx, const double2* post,
+                    const double2* twz, double* part, unsigned int* counter, double* out_max) {
+    plane_f_t(st, mode, c, m, coef, f, src, spec, twx, post, twz, part, counter, out_max);
+}
+void launch_plane_f(cudaStream_t st, const DConst& c, const double* src, float2* spec, const double2* twx,
+                    const double2* post, const double2* twz) {
+    const Fields none = {};
+    plane_f_t(st, 2, c, DMetric{}, nullptr, none, src, spec, twx, post, twz, nullptr, nullptr, nullptr);
+}
+void launch_plane_b(cudaStream_t st, int nx, int ny, int nz, const float2* spec, float* phi, const double2* twx,
+                    const double2* post, const double2* twz, double scale, int padded) {
+    plane_b_t(st, nx, ny, nz, spec, phi, twx, post, twz, scale, padded, 0);
+}
+void launch_plane_b(cudaStream_t st, int nx, int ny, int nz, const float2* spec, double* phi, const double2* twx,
+                    const double2* post, const double2* twz, double scale, int accumulate) {
+    plane_b_t(st, nx, ny, nz, spec, phi, twx, post, twz, scale, 0, accumulate);
+}
+#endif
 
 }  // namespace ptc

@@ -69,6 +69,14 @@ constexpr size_t rhs_smem_bytes() {
 __device__ __forceinline__ const double* field_of(const Fields& fl, int f) {
     return f == 0 ? fl.ux : f == 1 ? fl.uy : f == 2 ? fl.uz : f == 3 ? fl.pr : fl.sc;
 }
+// one value of field f at offset off, widened to double (the pressure is
+// FP64 in every storage form)
+template <class V>
+__device__ __forceinline__ double ld_field(const FieldSet<V>& fl, int f, size_t off) {
+    if (f == 3) return __ldg(fl.pr + off);
+    const V* q = f == 0 ? fl.ux : f == 1 ? fl.uy : f == 2 ? fl.uz : fl.sc;
+    return (double)__ldg(q + off);
+}
 
 __device__ __forceinline__ int modp(int i, int n) {
     int r = i % n;
@@ -77,13 +85,17 @@ __device__ __forceinline__ int modp(int i, int n) {
 
 }  // namespace
 
-template <bool SCALAR, class T>
+// SCALAR: with the scalar transport; T: arithmetic (double, or float for the
+// mixed and FP32 storage forms); V: storage of u, v, w, c, Hist and Rhs
+// (float only in the FP32 storage form, whose arithmetic is float)
+template <bool SCALAR, class T, class V>
 __global__ void __launch_bounds__(RhsCfg<T>::NTHR, RhsCfg<T>::MINB)
-    k_rhs_tile(DConst c, DMetric m, DCoef* __restrict__ coef, Fields fl, double* __restrict__ uy_ym,
+    k_rhs_tile(DConst c, DMetric m, DCoef* __restrict__ coef, FieldSet<V> fl, double* __restrict__ uy_ym,
                double* __restrict__ duy_ym, int ns, double gam, double the, double alp, double* __restrict__ part,
                unsigned int* __restrict__ counter, unsigned int* __restrict__ err) {
     constexpr int NF = SCALAR ? 5 : 4;
     constexpr bool F64 = sizeof(T) == 8;
+    static_assert(!F64 || sizeof(V) == 8, "the FP64 arithmetic form keeps FP64 fields");
     constexpr int ZC = RhsCfg<T>::ZC, NTHR = RhsCfg<T>::NTHR, NSLOT = RhsCfg<T>::NSLOT, NB = RhsCfg<T>::NB;
     // bytes one FP64 row brings into its slot: NF fields x SZ planes x SX values, and the metric record
     constexpr unsigned ROW_BYTES = (unsigned)(NF * SZ * SX) * 8u + ROWMET * 8u;
@@ -163,6 +175,8 @@ __global__ void __launch_bounds__(RhsCfg<T>::NTHR, RhsCfg<T>::MINB)
         auto issue_row = [&](int jrow) {
             const int sl = jrow % NB;
             pend |= 1u << sl;
+            if constexpr (!F64) return;
+            else {
             if (wq != 0) return;
             if (lane == 0) tma::mbar_expect_tx(&bar[sl], ROW_BYTES);
             __syncwarp();
@@ -180,6 +194,7 @@ __global__ void __launch_bounds__(RhsCfg<T>::NTHR, RhsCfg<T>::MINB)
                 }
             }
             if (lane == 0) tma::bulk_load(smet[sl], m.rowmet + (size_t)jrow * ROWMET, ROWMET * 8u, &bar[sl]);
+            }
         };
         // every thread waits for the row's copies; the CTA stops as one when
         // any thread's wait ran out
@@ -198,7 +213,7 @@ __global__ void __launch_bounds__(RhsCfg<T>::NTHR, RhsCfg<T>::MINB)
         const size_t ro_ = (size_t)(jrow) * nx;                                          \
         _Pragma("unroll") for (int f_ = 0; f_ < NF; f_++)                                \
             _Pragma("unroll") for (int s_ = 0; s_ < NSLOT; s_++) if (sval[s_])           \
-                dst_[f_ * SLAB + soff[s_]] = (T)__ldg(field_of(fl, f_) + goff[s_] + ro_); \
+                dst_[f_ * SLAB + soff[s_]] = (T)ld_field(fl, f_, goff[s_] + ro_);           \
         if (tid < ROWMET) smet[(jrow) % NB][tid] = __ldg(m.rowmet + (size_t)(jrow) * ROWMET + tid); \
     } while (0)
 
@@ -260,7 +275,7 @@ __global__ void __launch_bounds__(RhsCfg<T>::NTHR, RhsCfg<T>::MINB)
                 for (int f = 0; f < NF; f++)
 #pragma unroll
                     for (int sl = 0; sl < NSLOT; sl++)
-                        pre[f][sl] = sval[sl] ? __ldg(field_of(fl, f) + goff[sl] + ro) : 0.0;
+                        pre[f][sl] = sval[sl] ? ld_field(fl, f, goff[sl] + ro) : 0.0;
                 if (tid < ROWMET) mpre = __ldg(m.rowmet + (size_t)(j + 2) * ROWMET + tid);
             }
             double hx0a[ZC], hy0a[ZC], hz0a[ZC], hc0a[ZC];
@@ -435,15 +450,15 @@ __global__ void __launch_bounds__(RhsCfg<T>::NTHR, RhsCfg<T>::MINB)
             for (int cz = 0; cz < ZC; cz++) {
                 if (!act[cz]) continue;
                 const size_t q0 = q0a[cz];
-                fl.rx[q0] = (double)o_rx[cz];
-                fl.ry[q0] = (double)o_ry[cz];
-                fl.rz[q0] = (double)o_rz[cz];
-                fl.hx[q0] = (double)o_hx[cz];
-                fl.hy[q0] = (double)o_hy[cz];
-                fl.hz[q0] = (double)o_hz[cz];
+                fl.rx[q0] = (V)o_rx[cz];
+                fl.ry[q0] = (V)o_ry[cz];
+                fl.rz[q0] = (V)o_rz[cz];
+                fl.hx[q0] = (V)o_hx[cz];
+                fl.hy[q0] = (V)o_hy[cz];
+                fl.hz[q0] = (V)o_hz[cz];
                 if (SCALAR) {
-                    fl.rc[q0] = (double)o_rc[cz];
-                    fl.hc[q0] = (double)o_hc[cz];
+                    fl.rc[q0] = (V)o_rc[cz];
+                    fl.hc[q0] = (V)o_hc[cz];
                 }
             }
             if constexpr (!F64) {
@@ -532,20 +547,23 @@ size_t rhs_grid_blocks(const DConst& c) {
 }
 
 void rhs_init() {
-    cudaFuncSetAttribute(k_rhs_tile<false, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rhs_smem_bytes<false, double>());
-    cudaFuncSetAttribute(k_rhs_tile<true, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rhs_smem_bytes<true, double>());
-    cudaFuncSetAttribute(k_rhs_tile<false, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rhs_smem_bytes<false, float>());
-    cudaFuncSetAttribute(k_rhs_tile<true, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rhs_smem_bytes<true, float>());
+#define RHS_ATTR(S, T, V)                                                                                 \
+    cudaFuncSetAttribute(k_rhs_tile<S, T, V>, cudaFuncAttributeMaxDynamicSharedMemorySize,             \
+                         (int)rhs_smem_bytes<S, T>());
+    RHS_ATTR(false, double, double) RHS_ATTR(true, double, double)
+    RHS_ATTR(false, float, double) RHS_ATTR(true, float, double)
+    RHS_ATTR(false, float, float) RHS_ATTR(true, float, float)
+#undef RHS_ATTR
 }
 
-template <bool SCALAR, class T>
-static void launch_rhs_t(cudaStream_t st, const DConst& c, const DMetric& m, DCoef* coef, const Fields& f, double* uy_ym,
-                         double* duy_ym, int ns, double gam, double the, double alp, double* part, unsigned int* counter,
-                         unsigned int* err) {
+template <bool SCALAR, class T, class V>
+static void launch_rhs_t(cudaStream_t st, const DConst& c, const DMetric& m, DCoef* coef, const FieldSet<V>& f,
+                         double* uy_ym, double* duy_ym, int ns, double gam, double the, double alp, double* part,
+                         unsigned int* counter, unsigned int* err) {
     const dim3 grd((unsigned)rhs_blocks(c, RhsCfg<T>::MINB));
     const dim3 blk(32, TZ / RhsCfg<T>::ZC);
-    launch_pdl(k_rhs_tile<SCALAR, T>, grd, blk, rhs_smem_bytes<SCALAR, T>(), st, c, m, coef, f, uy_ym, duy_ym, ns, gam,
-               the, alp, part, counter, err);
+    launch_pdl(k_rhs_tile<SCALAR, T, V>, grd, blk, rhs_smem_bytes<SCALAR, T>(), st, c, m, coef, f, uy_ym, duy_ym, ns,
+               gam, the, alp, part, counter, err);
 }
 
 void launch_rhs_tile(cudaStream_t st, const DConst& c, const DMetric& m, DCoef* coef, const Fields& f, double* uy_ym,
@@ -558,6 +576,13 @@ void launch_rhs_tile(cudaStream_t st, const DConst& c, const DMetric& m, DCoef* 
         if (c.scalar_on) launch_rhs_t<true, double>(st, c, m, coef, f, uy_ym, duy_ym, ns, gam, the, alp, part, counter, err);
         else launch_rhs_t<false, double>(st, c, m, coef, f, uy_ym, duy_ym, ns, gam, the, alp, part, counter, err);
     }
+}
+
+void launch_rhs_tile(cudaStream_t st, const DConst& c, const DMetric& m, DCoef* coef, const Fields32& f, double* uy_ym,
+                     double* duy_ym, int ns, double gam, double the, double alp, double* part, unsigned int* counter,
+                     unsigned int* err) {
+    if (c.scalar_on) launch_rhs_t<true, float>(st, c, m, coef, f, uy_ym, duy_ym, ns, gam, the, alp, part, counter, err);
+    else launch_rhs_t<false, float>(st, c, m, coef, f, uy_ym, duy_ym, ns, gam, the, alp, part, counter, err);
 }
 
 }  // namespace ptc

@@ -7,6 +7,8 @@
 // are index wrap (see common.cuh).  Reductions are per-block tree reductions
 // followed by one single-block pass in a fixed order, so every result is
 // bitwise reproducible run to run.
+#include <algorithm>
+
 #include "common.cuh"
 #include "kernels.cuh"
 #include "reduce.cuh"
@@ -352,6 +354,71 @@ __global__ void k_xprof_final(DConst c, const double* __restrict__ part, double*
     out[i] = s / (double)c.nz / c.yly;
 }
 
+// elementwise conversion between the storage precisions (round to nearest
+// one way, exact the other), for loading and reading the FP32 storage form
+template <class A, class B>
+__global__ void k_cast(size_t n, const A* __restrict__ a, B* __restrict__ b) {
+    for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (size_t)gridDim.x * blockDim.x)
+        b[t] = (B)a[t];
+}
+
+// the residual of the discrete pressure Poisson equation r = src - L phi on
+// compact arrays (k*ny + jc-1)*nx + i: L = D4x D4x + D4z D4z + Lyy, the
+// operator whose eigenvalues the spectral solve inverts (D4 the 4th-order
+// staggered first difference of clcPrSrc / FluidVelUpdate, so D4 D4 has the
+// modified wavenumber of src/m_Poisson.f90:40-48 as its symbol; Lyy the
+// Neumann wall-normal operator am2ph/ac2ph/ap2ph).  max|r| and max|src| go
+// to out[0], out[1] through the last CTA.
+__global__ void __launch_bounds__(256) k_residual(DConst c, DMetric m, const double* __restrict__ src,
+                                                  const double* __restrict__ phi, double* __restrict__ r,
+                                                  double* __restrict__ part, unsigned int* __restrict__ counter,
+                                                  double* __restrict__ out) {
+    const int nx = c.nx, ny = c.ny, nz = c.nz;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int jc = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    const int k = blockIdx.z;
+    // the 7-point D4 D4 weights of offsets -3..3 (a face derivative of cell
+    // values, then the cell derivative of face values)
+    double wx[7], wz[7];
+#pragma unroll
+    for (int q = 0; q < 7; q++) { wx[q] = 0.0; wz[q] = 0.0; }
+#pragma unroll
+    for (int a = 0; a < 4; a++)
+#pragma unroll
+        for (int b = 0; b < 4; b++) {
+            wx[a + b] += c.dxC[a] * c.dxC[b];
+            wz[a + b] += c.dzC[a] * c.dzC[b];
+        }
+    double v[2] = {0.0, 0.0};
+    if (i < nx && jc <= ny) {
+        const size_t row = (size_t)ny * nx;
+        const double* pk = phi + (size_t)k * row + (size_t)(jc - 1) * nx;
+        double lx = 0.0, lz = 0.0;
+#pragma unroll
+        for (int q = 0; q < 7; q++) {
+            lx += wx[q] * __ldg(&pk[wrapi(i - 3 + q, nx)]);
+            const int kq = ((k - 3 + q) % nz + nz) % nz;
+            lz += wz[q] * __ldg(&phi[(size_t)kq * row + (size_t)(jc - 1) * nx + i]);
+        }
+        const double pc = __ldg(&pk[i]);
+        double ly = __ldg(&m.ac2ph[jc]) * pc;
+        if (jc > 1) ly += __ldg(&m.am2ph[jc]) * __ldg(&pk[i - nx]);
+        if (jc < ny) ly += __ldg(&m.ap2ph[jc]) * __ldg(&pk[i + nx]);
+        const size_t q0 = (size_t)k * row + (size_t)(jc - 1) * nx + i;
+        const double s = __ldg(&src[q0]);
+        const double res = s - (lx + lz + ly);
+        r[q0] = res;
+        v[0] = fabs(res);
+        v[1] = fabs(s);
+    }
+    const int bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+    block_max_store<2>(v, part + (size_t)bid * 2);
+    if (!last_block_arrive(counter, gridDim.x * gridDim.y * gridDim.z)) return;
+    double tot[2];
+    reduce_records<2, true>(part, (int)(gridDim.x * gridDim.y * gridDim.z), tot);
+    if (threadIdx.x == 0 && threadIdx.y == 0) { out[0] = tot[0]; out[1] = tot[1]; }
+}
+
 __global__ void k_store_divsrc(DCoef* coef, const double* __restrict__ v) {
     if (threadIdx.x == 0) coef->divmax_src = *v;
 }
@@ -426,6 +493,18 @@ void launch_xprofile(cudaStream_t st, const DConst& c, const DMetric& m, const d
 }
 void launch_xprofile(cudaStream_t st, const DConst& c, const DMetric& m, const float* q, double* part, double* out) {
     xprofile_t(st, c, m, q, part, out);
+}
+
+void launch_cast(cudaStream_t st, size_t n, const double* a, float* b) {
+    k_cast<double, float><<<(unsigned)std::min<size_t>((n + 255) / 256, 4096), 256, 0, st>>>(n, a, b);
+}
+void launch_cast(cudaStream_t st, size_t n, const float* a, double* b) {
+    k_cast<float, double><<<(unsigned)std::min<size_t>((n + 255) / 256, 4096), 256, 0, st>>>(n, a, b);
+}
+
+void launch_residual(cudaStream_t st, const DConst& c, const DMetric& m, const double* src, const double* phi,
+                     double* r, double* part, unsigned int* counter, double* out) {
+    k_residual<<<cell_grid(c), cell_block(), 0, st>>>(c, m, src, phi, r, part, counter, out);
 }
 
 size_t endstep_blocks(const DConst& c) { return (size_t)2 * (c.nsm > 0 ? c.nsm : 148); }

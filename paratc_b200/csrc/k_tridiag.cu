@@ -494,15 +494,18 @@ __global__ void __launch_bounds__(32) k_ys_staged(int ny, int M1, int nz, const 
 
 // Large grids: one thread per real column straight from global memory, the
 // rows of a chunk loaded ahead of its chain, latency hidden by occupancy.
+// R: storage of the spectrum's real parts (double, or float in the FP32
+// storage form); the sweeps run in double either way
+template <class R>
 __global__ void __launch_bounds__(128) k_ys_global(int ny, int M1, int nz, const double* __restrict__ am2ph,
-                                                   double* __restrict__ specd, const double* __restrict__ fac) {
+                                                   R* __restrict__ specd, const double* __restrict__ fac) {
     const int W = 2 * M1, NQ = M1 * nz;
     const int g = blockIdx.x * blockDim.x + threadIdx.x;
     pdl_wait();
     pdl_trigger();
     if (g >= W * nz) return;
     const int kz = g / W, cr = g - kz * W, q = g >> 1;
-    double* col = specd + (size_t)kz * ny * W + cr;
+    R* col = specd + (size_t)kz * ny * W + cr;
     const double* frv = fac + q;
     const double* far = fac + (size_t)NQ * ny + q;
     const bool dc = (q == 0);
@@ -523,8 +526,8 @@ __global__ void __launch_bounds__(128) k_ys_global(int ny, int M1, int nz, const
             const int j = j0 + u;
             if (j < ny) {
                 const double f = (j == 0) ? (dc ? 0.0 : d[u]) * rv[u] : (d[u] - a[u] * fp) * rv[u];
-                col[(size_t)j * W] = f;
-                fp = f;
+                col[(size_t)j * W] = (R)f;
+                fp = (double)(R)f;  // the value the backward sweep reads
             }
         }
     }
@@ -544,7 +547,7 @@ __global__ void __launch_bounds__(128) k_ys_global(int ny, int M1, int nz, const
             const int j = j0 - u;
             if (j >= 0) {
                 const double x = d[u] - ar[u] * xn;
-                col[(size_t)j * W] = x;
+                col[(size_t)j * W] = (R)x;
                 xn = x;
             }
         }
@@ -567,9 +570,15 @@ void launch_ysolve_fac(cudaStream_t st, const DConst& c, const DMetric& m, doubl
         launch_pdl(k_ys_staged, dim3(ctas), dim3(32), sm, st, c.ny, M1, c.nz, m.am2ph, spec, fac);
     } else {
         const int n = 2 * M1 * c.nz;
-        launch_pdl(k_ys_global, dim3((n + 127) / 128), dim3(128), 0, st, c.ny, M1, c.nz, m.am2ph,
+        launch_pdl(k_ys_global<double>, dim3((n + 127) / 128), dim3(128), 0, st, c.ny, M1, c.nz, m.am2ph,
                    reinterpret_cast<double*>(spec), fac);
     }
+}
+
+void launch_ysolve_fac(cudaStream_t st, const DConst& c, const DMetric& m, float2* spec, const double* fac) {
+    const int M1 = c.nx / 2 + 1, n = 2 * M1 * c.nz;
+    launch_pdl(k_ys_global<float>, dim3((n + 127) / 128), dim3(128), 0, st, c.ny, M1, c.nz, m.am2ph,
+               reinterpret_cast<float*>(spec), fac);
 }
 
 // ---------------------------------------------------------------------------

@@ -63,6 +63,12 @@ void launch_endstep(cudaStream_t st, const DConst& c, const DMetric& m, const Fi
                     double* part, unsigned int* counter, int next);
 void launch_endstep(cudaStream_t st, const DConst& c, const DMetric& m, const Fields32& f, DCoef* coef, DDiag* diag,
                     double* part, unsigned int* counter, int next);
+// storage conversions (FP32 storage form)
+void launch_cast(cudaStream_t st, size_t n, const double* a, float* b);
+void launch_cast(cudaStream_t st, size_t n, const float* a, double* b);
+// r = src - L phi (compact arrays) with max|r|, max|src| to out[0..1]; part holds 2 doubles per cell block
+void launch_residual(cudaStream_t st, const DConst& c, const DMetric& m, const double* src, const double* phi,
+                     double* r, double* part, unsigned int* counter, double* out);
 // x profile of a padded field averaged over y (dyp weights) and z; part holds nx*nz doubles
 void launch_xprofile(cudaStream_t st, const DConst& c, const DMetric& m, const double* q, double* part, double* out);
 void launch_xprofile(cudaStream_t st, const DConst& c, const DMetric& m, const float* q, double* part, double* out);
@@ -72,6 +78,10 @@ size_t rhs_grid_blocks(const DConst& c);
 void rhs_init();
 // err: the context's error word (bit 8: a row wait of the FP64 copy pipeline gave up; err[1]: the test poll limit)
 void launch_rhs_tile(cudaStream_t st, const DConst& c, const DMetric& m, DCoef* coef, const Fields& f, double* uy_ym,
+                     double* duy_ym, int ns, double gam, double the, double alp, double* part, unsigned int* counter,
+                     unsigned int* err);
+// FP32 storage form: float fields, FP64 pressure, FP32 arithmetic
+void launch_rhs_tile(cudaStream_t st, const DConst& c, const DMetric& m, DCoef* coef, const Fields32& f, double* uy_ym,
                      double* duy_ym, int ns, double gam, double the, double alp, double* part, unsigned int* counter,
                      unsigned int* err);
 
@@ -94,6 +104,8 @@ void launch_ysolve(cudaStream_t st, const DConst& c, const DMetric& m, double2* 
 // k_tridiag.cu: spectral y-solve with the pivots computed once per context
 void launch_pois_factors(cudaStream_t st, const DConst& c, const DMetric& m, double* fac);
 void launch_ysolve_fac(cudaStream_t st, const DConst& c, const DMetric& m, double2* spec, const double* fac);
+// FP32 storage form: the streaming solve on a float2 spectrum, FP64 sweeps and pivots
+void launch_ysolve_fac(cudaStream_t st, const DConst& c, const DMetric& m, float2* spec, const double* fac);
 
 // k_stats.cu: clcStat accumulation
 int stats_count(const DConst& c);
@@ -148,12 +160,24 @@ void launch_plane_f(cudaStream_t st, int mode, const DConst& c, const DMetric& m
                     double* part, unsigned int* counter, double* out_max);
 void launch_plane_b(cudaStream_t st, int nx, int ny, int nz, const double2* spec, double* phi, const double2* twx,
                     const double2* post, const double2* twz, double scale, int padded);
+void plane_init32();  // the FP32 storage instantiations (k_plane32.cu)
+// FP32 storage form: the step's solve and the refined solve (as launch_pfft_xf / _xb)
+void launch_plane_f(cudaStream_t st, int mode, const DConst& c, const DMetric& m, const DCoef* coef,
+                    const Fields32& f, const double* src, float2* spec, const double2* twx, const double2* post,
+                    const double2* twz, double* part, unsigned int* counter, double* out_max);
+void launch_plane_f(cudaStream_t st, const DConst& c, const double* src, float2* spec, const double2* twx,
+                    const double2* post, const double2* twz);
+void launch_plane_b(cudaStream_t st, int nx, int ny, int nz, const float2* spec, float* phi, const double2* twx,
+                    const double2* post, const double2* twz, double scale, int padded);
+void launch_plane_b(cudaStream_t st, int nx, int ny, int nz, const float2* spec, double* phi, const double2* twx,
+                    const double2* post, const double2* twz, double scale, int accumulate);
 
 // k_pfft_x.cu / k_pfft_z.cu: compile-time-length transforms of the Poisson solve
 bool pfft_x_supported(int n);
 bool pfft_z_supported(int n);
 int pfft_x_blocks(int nx, int ny, int nz);
 void pfft_x_init();
+void pfft_x_init32();  // the FP32 storage instantiations (k_pfft_x32.cu)
 void pfft_z_init();
 void launch_pfft_xf(cudaStream_t st, int mode, const DConst& c, const DMetric& m, const DCoef* coef, const Fields& f,
                     const double* src, double2* spec, const double2* twx, const double2* post, double* part,
@@ -161,6 +185,19 @@ void launch_pfft_xf(cudaStream_t st, int mode, const DConst& c, const DMetric& m
 void launch_pfft_xb(cudaStream_t st, int nx, int ny, int nz, const double2* spec, double* phi, const double2* twx,
                     const double2* post, double scale, int padded);
 void launch_pfft_z(cudaStream_t st, int dir, int nx, int ny, int nz, double2* spec, const double2* twz);
+// FP32 storage form: the step's solve (float velocity, float2 spectrum, float potential)
+void launch_pfft_xf(cudaStream_t st, int mode, const DConst& c, const DMetric& m, const DCoef* coef,
+                    const Fields32& f, const double* src, float2* spec, const double2* twx, const double2* post,
+                    double* part, unsigned int* counter, double* out_max);
+void launch_pfft_xb(cudaStream_t st, int nx, int ny, int nz, const float2* spec, float* phi, const double2* twx,
+                    const double2* post, double scale, int padded);
+void launch_pfft_z(cudaStream_t st, int dir, int nx, int ny, int nz, float2* spec, const double2* twz);
+// the refined solve: an FP64 source array into a float2 spectrum, and the
+// inverse into an FP64 potential (compact rows), added to it when accumulate != 0
+void launch_pfft_xf(cudaStream_t st, const DConst& c, const double* src, float2* spec, const double2* twx,
+                    const double2* post);
+void launch_pfft_xb(cudaStream_t st, int nx, int ny, int nz, const float2* spec, double* phi, const double2* twx,
+                    const double2* post, double scale, int accumulate);
 
 // k_fft.cu
 void fft_init();

@@ -36,7 +36,7 @@ EXPORTED = [
     "paratc_visu_name", "paratc_visu_quantity", "paratc_dump_visu", "paratc_write_xdmf",
     "paratc_io_options_from_namelist", "paratc_visu_quantity_device", "paratc_autotune", "paratc_get_schedule",
     "paratc_set_schedule", "paratc_set_precision", "paratc_get_precision", "paratc_set_wait_limit",
-    "paratc_xprofile", "paratc_front_position",
+    "paratc_xprofile", "paratc_front_position", "paratc_poisson_refined", "paratc_poisson_refined_async",
 ]
 PROF_NKERNELS = 16
 
@@ -83,6 +83,9 @@ def load(path=None):
     L.paratc_get_precision.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]
     L.paratc_set_wait_limit.argtypes = [ctypes.c_void_p, ctypes.c_longlong]
     L.paratc_xprofile.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp]
+    L.paratc_poisson_refined.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double,
+                                         ctypes.c_int, ctypes.POINTER(ctypes.c_int), _dp]
+    L.paratc_poisson_refined_async.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
     L.paratc_front_position.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double, _dp]
     L.paratc_dump_visu.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_char_p] + [ctypes.c_int] * 7
     L.paratc_write_xdmf.argtypes = [ctypes.POINTER(ParatcParams), _dp, ctypes.c_char_p, ctypes.c_char_p] + \
@@ -371,6 +374,20 @@ class ChannelSystem:
         self._check(self._L.paratc_poisson_device_async(self._h, ctypes.c_void_p(d_src_ptr), ctypes.c_void_p(d_phi_ptr)),
                     "paratc_poisson_device_async")
 
+    def poisson_refined(self, d_src_ptr, d_phi_ptr, rtol=1e-12, max_corr=4):
+        """FP32 solves with FP64 iterative refinement (device pointers);
+        returns (corrections, final max|r| / max|src|)."""
+        n, r = ctypes.c_int(), ctypes.c_double()
+        self._check(self._L.paratc_poisson_refined(self._h, ctypes.c_void_p(d_src_ptr), ctypes.c_void_p(d_phi_ptr),
+                                                   float(rtol), int(max_corr), ctypes.byref(n), ctypes.byref(r)),
+                    "paratc_poisson_refined")
+        return n.value, r.value
+
+    def poisson_refined_async(self, d_src_ptr, d_phi_ptr, ncorr):
+        self._check(self._L.paratc_poisson_refined_async(self._h, ctypes.c_void_p(d_src_ptr),
+                                                         ctypes.c_void_p(d_phi_ptr), int(ncorr)),
+                    "paratc_poisson_refined_async")
+
     # -- statistics (clcStat)
     def stats_reset(self):
         self._check(self._L.paratc_stats_reset(self._h), "paratc_stats_reset")
@@ -443,16 +460,18 @@ class ChannelSystem:
                                                  None), "paratc_visu_quantity")
         return out
 
-    # -- precision: "fp64" (default) or "mixed" (FP32 right-hand side)
+    # -- precision: "fp64" (default), "mixed" (FP32 right-hand side) or
+    #    "fp32" (FP32 storage of everything but the pressure)
     @property
     def precision(self):
         v = ctypes.c_int()
         self._check(self._L.paratc_get_precision(self._h, ctypes.byref(v)), "paratc_get_precision")
-        return ("fp64", "mixed")[v.value]
+        return ("fp64", "mixed", "fp32")[v.value]
 
     @precision.setter
     def precision(self, name):
-        self._check(self._L.paratc_set_precision(self._h, {"fp64": 0, "mixed": 1}[name]), "paratc_set_precision")
+        self._check(self._L.paratc_set_precision(self._h, {"fp64": 0, "mixed": 1, "fp32": 2}[name]),
+                    "paratc_set_precision")
 
     def set_wait_limit(self, polls):
         """Poll limit of the TMA-fed kernels' pipeline waits (None or < 0:
