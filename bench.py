@@ -47,6 +47,8 @@ def _args():
                     help="poisson_c2 only: solve on this grid instead of 512 x 256 x 512 (profiling other lengths)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-forms", action="store_true",
+                    help="skip the FP32 / mixed / batched forms that follow the FP64 headline")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--schedule", type=int, default=-1,
                     help="pin a Poisson schedule (0-11, paratc_set_schedule) instead of auto-tuning it")
@@ -344,7 +346,7 @@ def run_ours(args):
     # the mixed form against the FP64 path: the same initial fields advanced by
     # the same number of steps (warm-up, timed, profiled, end to end)
     mixed_err = None
-    if args.precision == "mixed":
+    if args.precision in ("mixed", "fp32"):
         nsteps = args.warmup + 2 * args.steps + (0 if args.no_e2e else args.steps)
         ref = ChannelSystem(p, yp, device=local)
         ref.set_fields(fields["ux"], fields["uy"], fields["uz"], fields["p"], fields["c"])
@@ -356,6 +358,56 @@ def run_ours(args):
             if fr.get(n) is not None:
                 mixed_err[n] = float(np.abs(fm[n] - fr[n]).max() / np.abs(fr[n]).max())
         ref.close()
+
+    # the north star's forms on the same workload and box: the FP32 storage
+    # form and the mixed form against the FP64 path (device time of K steps
+    # after W warm-up steps, L2 flushed between steps, max over ranks; field
+    # error against an FP64 context advanced the same W + K steps from the
+    # same projected state), and the batched C4 ensemble
+    forms = None
+    if not args.no_forms and args.precision == "fp64":
+        forms = {"fp64": {"value": value, "ms_per_step": total_ms / args.steps}}
+        ref = ChannelSystem(p, yp, device=local)
+        ref.set_fields(fields["ux"], fields["uy"], fields["uz"], fields["p"], fields["c"])
+        ref.project()
+        ref.iterate(args.warmup + args.steps)
+        fr = ref.get_fields()
+        ref.close()
+        for form in ("fp32", "mixed"):
+            c2 = ChannelSystem(p, yp, device=local)
+            c2.schedule = schedule
+            c2.set_fields(fields["ux"], fields["uy"], fields["uz"], fields["p"], fields["c"])
+            c2.project()
+            c2.precision = form
+            st2 = torch.cuda.ExternalStream(c2.stream, device=local)
+            for _ in range(args.warmup):
+                c2.iterate_async(1)
+            c2.last_diag()
+            barrier()
+            evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+            for a, b in evs:
+                with torch.cuda.stream(st2):
+                    flush.add_(1.0)
+                a.record(st2)
+                c2.iterate_async(1)
+                b.record(st2)
+            d2 = c2.last_diag()
+            torch.cuda.synchronize()
+            ms2 = replicas.max_over_ranks(sum(a.elapsed_time(b) for a, b in evs), dist, device=local)
+            fm = c2.get_fields()
+            err = {"steps": args.warmup + args.steps}
+            for n in ("ux", "uy", "uz", "p", "c"):
+                if fr.get(n) is not None:
+                    err[n] = float(np.abs(fm[n] - fr[n]).max() / np.abs(fr[n]).max())
+            v2 = ws * p.nxc * p.nyc * p.nzc * iad * args.steps / (ms2 / 1e3)
+            forms[form] = {"value": v2, "ms_per_step": ms2 / args.steps, "speedup_vs_fp64": v2 / value,
+                           "divmax_last_step": d2.divmax, "field_rel_err_vs_fp64_path": err}
+            c2.close()
+        ens = ensemble_measure(args, local, dist, "fp64", steps=max(3, args.steps // 2))
+        ens.pop("_batch").close()
+        ens.pop("_cases")
+        ens["speedup_vs_fp64_single"] = ens["value"] / value
+        forms["batched_c4"] = ens
 
     # roofline of the dominant kernel
     peak, peak_kind = _peaks()
@@ -378,13 +430,15 @@ def run_ours(args):
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None,
-                "dtype": "f64" if args.precision == "fp64" else "f32 rhs + f64", "data": "synthetic",
+                "dtype": {"fp64": "f64", "mixed": "f32 rhs + f64", "fp32": "f32 storage + f64 pressure"}[args.precision],
+                "data": "synthetic",
                 "config": {"workload": case.name, "grid": [p.nxc, p.nyc, p.nzc], "scheme": "RK3",
                            "precision": args.precision, "parallelism": "replicas x%d" % ws,
                            "l2": "flushed between timed steps (256 MB write outside the events)",
                            "divmax_last_step": diag.divmax, "poisson_schedule": schedule, "autotune_ms": tune_ms,
                            "field_rel_err_vs_fp64_path": mixed_err},
-                "roofline": roof, "cpu_baseline": base, "e2e": e2e, "gpu_launches": launches, "clocks": clocks}
+                "roofline": roof, "cpu_baseline": base, "e2e": e2e, "gpu_launches": launches, "clocks": clocks,
+                "forms": forms}
         print(json.dumps(line), flush=True)
     ctx.close()
     if dist is not None:
@@ -392,63 +446,79 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
-def run_ensemble(args):
+def ensemble_measure(args, local, dist, precision, steps=None):
     """The C4 ensemble: 32 channel instances of uneven grids and Re_tau
     advanced together by the batch API, every step-round one CUDA graph
-    launch; reported against the same instances stepped one after another
-    (each alone on the GPU).  The ensemble's working set (several GB) exceeds
-    the L2, so no flush is needed between timed steps."""
+    launch (device time of `steps` steps, max over ranks); and the same
+    instances stepped one after another, each alone on the GPU.  The
+    ensemble's working set (several GB) exceeds the L2, so no flush is needed
+    between timed steps.  Returns the measurement as a dict (with the batch
+    and its cases under "_batch" and "_cases" for the caller to close)."""
     import torch
-    ws, rank, local = _dist()
-    torch.cuda.set_device(local)
-    from paratc_b200 import replicas
-    dist = replicas.init("nccl")
-    from paratc_b200 import cases
+    from paratc_b200 import cases, replicas
     from paratc_b200.lib import BatchSystem, mesh_ycoord
+    ws, rank, _ = _dist()
+    steps = steps or args.steps
     cs = cases.ensemble_c4(seed=replicas.replica_seed(2024, rank))
     yps = [mesh_ycoord(c.mesh, c.params.yly) for c in cs]
     b = BatchSystem([c.params for c in cs], yps, device=local)
     cells = 0
     for c, y, m in zip(cs, yps, b.members):
         f = cases.initial_fields(c, y)
-        m.precision = args.precision
         m.set_fields(f["ux"], f["uy"], f["uz"], f["p"], f["c"])
         m.project()
+        m.precision = precision
         cells += c.params.nxc * c.params.nyc * c.params.nzc
     stream = torch.cuda.ExternalStream(b.stream, device=local)
     b.iterate(args.warmup)
     torch.cuda.synchronize()
-
-    def barrier():
-        if dist is not None:
-            dist.barrier()
-        torch.cuda.synchronize()
-
-    barrier()
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
     sampler = ClockSampler(local)
     sampler.start()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    diags = b.iterate(args.steps)
+    diags = b.iterate(steps)
     e1.record(stream)
     torch.cuda.synchronize()
     clocks = sampler.stop()
     ms = replicas.max_over_ranks(e0.elapsed_time(e1), dist, device=local)
-    value = ws * cells * 3 * args.steps / (ms / 1e3)
+    value = ws * cells * 3 * steps / (ms / 1e3)
     # the same members one at a time, each alone on the GPU
     seq_ms = 0.0
     for m in b.members:
         st = torch.cuda.ExternalStream(m.stream, device=local)
         a, z = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record(st)
-        m.iterate_async(args.steps)
+        m.iterate_async(steps)
         z.record(st)
         m.last_diag()
         torch.cuda.synchronize()
         seq_ms += a.elapsed_time(z)
-    seq_value = cells * 3 * args.steps / (seq_ms / 1e3)
-    # end to end: every member's state in from pinned host memory, one batch
-    # step, every member's state back
+    seq_ms = replicas.max_over_ranks(seq_ms, dist, device=local)
+    seq_value = ws * cells * 3 * steps / (seq_ms / 1e3)
+    return {"value": value, "unit": UNIT, "ms_per_step": ms / steps, "steps": steps, "cells": cells,
+            "precision": precision, "graph_kernels_per_step": b.graph_kernels,
+            "divmax_last_step_max": max(d.divmax for d in diags),
+            "sequential": {"value": seq_value, "ms_per_step": seq_ms / steps,
+                           "note": "the same 32 instances stepped one after another, each alone on the GPU"},
+            "speedup_vs_sequential": value / seq_value, "clocks": clocks, "_batch": b, "_cases": cs}
+
+
+def run_ensemble(args):
+    """The C4 ensemble line (ensemble_measure), with the end-to-end figure:
+    every member's state in from pinned host memory, one batch step, every
+    member's state back."""
+    import torch
+    ws, rank, local = _dist()
+    torch.cuda.set_device(local)
+    from paratc_b200 import replicas
+    dist = replicas.init("nccl")
+    r = ensemble_measure(args, local, dist, args.precision)
+    b = r.pop("_batch")
+    cs = r.pop("_cases")
+    cells = r["cells"]
     names = ["ux", "uy", "uz", "p"]
     host = []
     nbytes = 0
@@ -459,7 +529,9 @@ def run_ensemble(args):
             h[n][...] = cur[n]
             nbytes += h[n].nbytes
         host.append(h)
-    barrier()
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
     # every member on its own stream: its state in, one step, its state out;
     # the members' transfers and steps overlap one another
     t_e2e = 0.0
@@ -474,26 +546,26 @@ def run_ensemble(args):
         t_e2e += time.perf_counter() - t0
     for m in b.members:
         m.last_diag()
+    t_e2e = replicas.max_over_ranks(t_e2e, dist, device=local)
     if rank == 0:
-        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
-                "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+        line = {"metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": ws, "steps": r["steps"],
+                "warmup": args.warmup, "ms_per_step": r["ms_per_step"], "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None,
-                "dtype": "f64" if args.precision == "fp64" else "f32 rhs + f64", "data": "synthetic",
+                "dtype": {"fp64": "f64", "mixed": "f32 rhs + f64", "fp32": "f32 storage + f64 pressure"}[args.precision],
+                "data": "synthetic",
                 "config": {"workload": "ensemble_c4: 32 channels, (nx,nz) in {64,96,128,192}, ny in {48,64,96,128}, "
                                        "Re_tau U[120,395], seed 2024",
                            "cells": cells, "precision": args.precision, "parallelism": "ensemble in one CUDA graph x%d" % ws,
                            "l2": "working set %.1f GB > L2, no flush" % (cells * 17 * 8 / 1e9),
-                           "graph_kernels_per_step": b.graph_kernels,
-                           "divmax_last_step_max": max(d.divmax for d in diags)},
-                "sequential": {"value": seq_value, "unit": UNIT, "ms_per_step": seq_ms / args.steps,
-                               "note": "the same 32 instances stepped one after another, each alone on the GPU"},
-                "speedup_vs_sequential": value / seq_value,
+                           "graph_kernels_per_step": r["graph_kernels_per_step"],
+                           "divmax_last_step_max": r["divmax_last_step_max"]},
+                "sequential": r["sequential"], "speedup_vs_sequential": r["speedup_vs_sequential"],
                 "roofline": None, "cpu_baseline": None,
                 "e2e": {"value": ws * cells * 3 * args.steps / t_e2e, "unit": UNIT, "h2d_bytes_per_step": nbytes,
                         "d2h_bytes_per_step": nbytes,
                         "note": "per step: every member's u,v,w,p from pinned host, one step, back; members pipelined "
                                 "on their own streams (paratc_set_fields_async / steps_async / get_fields_async)"},
-                "gpu_launches": b.graph_kernels * args.steps, "clocks": clocks}
+                "gpu_launches": r["graph_kernels_per_step"] * r["steps"], "clocks": r["clocks"]}
         print(json.dumps(line), flush=True)
     b.close()
     if dist is not None:
@@ -560,9 +632,41 @@ def run_poisson(args):
         t_o = time.perf_counter() - t0
         o.close()
         err = float(np.abs(phi_g - phi_o).max() / np.abs(phi_o).max())
+        if refined is not None:
+            refined["rel_err_vs_oracle"] = float(np.abs(phr - phi_o).max() / np.abs(phi_o).max())
+            refined["rel_err_vs_fp64_path"] = float(np.abs(phr - phi_g).max() / np.abs(phi_g).max())
         base = {"value": cells / t_o, "unit": "grid-point Poisson solves/s", "cores": threads, "kind": "port",
                 "sample": "one %dx%dx%d solve on the C oracle (OpenMP, %d threads), %.1f s"
                           % (p.nxc, p.nyc, p.nzc, threads, t_o)}
+    # the second form of this configuration: FP32 solves (spectrum stored in
+    # FP32, FP64 arithmetic in the passes) with FP64-residual iterative
+    # refinement to max|r| <= 1e-12 max|src|; the corrections needed are
+    # counted once, then that many are timed per solve
+    refined = None
+    if not args.no_forms:
+        d_phr = torch.empty_like(d_src)
+        ncorr, relres = ctx.poisson_refined(d_src.data_ptr(), d_phr.data_ptr(), 1e-12, 4)
+        evr = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+        for _ in range(args.warmup):
+            ctx.poisson_refined_async(d_src.data_ptr(), d_phr.data_ptr(), ncorr)
+        torch.cuda.synchronize()
+        for a, b in evr:
+            a.record(stream)
+            ctx.poisson_refined_async(d_src.data_ptr(), d_phr.data_ptr(), ncorr)
+            b.record(stream)
+        torch.cuda.synchronize()
+        msr = sum(a.elapsed_time(b) for a, b in evr)
+        phr = d_phr.cpu().numpy()
+        # bytes one refined solve moves (8-byte words per cell, spectrum S ~ N
+        # doubles stored as floats): first solve 7 (FP64 source in, FP32
+        # spectrum through x, z, y with FP64 pivots, z, x, FP64 potential
+        # out), each correction 3 (residual: source, potential, r) + 8
+        # (the same solve, potential read and written)
+        words = 7 + 11 * ncorr
+        refined = {"value": cells * args.steps / (msr / 1e3), "unit": "grid-point Poisson solves/s",
+                   "ms_per_solve": msr / args.steps, "corrections": ncorr, "relres": relres,
+                   "speedup_vs_fp64": ms / msr, "bytes_per_cell": 8 * words,
+                   "GBps": 8 * words * cells / (msr / args.steps / 1e3) / 1e9}
     peak, peak_kind = _peaks()
     alg = 6 * 8 * cells
     ach = alg / (ms / args.steps / 1e3) / 1e9
@@ -578,7 +682,7 @@ def run_poisson(args):
                              "peak": peak, "unit": "GB/s", "frac": round(ach / peak, 4), "traffic": None,
                              "peak_kind": peak_kind, "algorithmic_bytes_per_launch": alg,
                              "kernel_us": kern, "kernel_frac": kernel_fractions(prof, algorithmic_bytes(p), peak)},
-                "cpu_baseline": base,
+                "cpu_baseline": base, "fp32_refined": refined,
                 "e2e": {"value": cells * args.steps / t_e2e, "unit": "grid-point Poisson solves/s",
                         "h2d_bytes_per_step": src.nbytes, "d2h_bytes_per_step": src.nbytes,
                         "note": "paratc_poisson with host arrays: source in, potential out"},

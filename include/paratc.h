@@ -335,7 +335,7 @@ const char* paratc_profile_name(int k);
 
 /* ---- bounded device waits.  No counterpart in the reference (its MPI calls
  * block).  Every pipeline wait of the TMA-fed kernels (z transforms, x
- * transforms, divergence-fed x transform, right-hand side) polls its
+ * transforms, divergence-fed x transform) polls its
  * mbarrier at most 2^22 times; a CTA whose wait runs out records the failure,
  * waits (with the full limit) for its own copies still in flight and returns,
  * and the next synchronising call reports PARATC_ERR_TIMEOUT.  This sets the
@@ -399,6 +399,31 @@ int paratc_autotune(paratc_ctx* ctx, int nrep, int* choice, double* times_ms);
 int paratc_get_schedule(paratc_ctx* ctx, int* choice);
 /* pin a choice (PARATC_ERR_BAD_ARG when this grid has no such kernels) */
 int paratc_set_schedule(paratc_ctx* ctx, int choice);
+
+/* ---- Tuning of the launch shapes, with a cache.  The reference tunes only
+ * its Poisson variant (InitPoissonSolver, src/m_Poisson.f90:50-175, four
+ * choices timed at every start).  paratc_autotune_all first runs
+ * paratc_autotune (the Poisson schedule), then times whole steps from the
+ * current state for every compiled launch shape of the right-hand side
+ * (FP64: rows prefetched 1 or 2 ahead, 2 or 1 cells per thread) and of the
+ * Helmholtz sweeps (8 or 4 rows per register chunk), puts the state back
+ * and keeps the fastest.  With cache_path != NULL the picks are written to
+ * that JSON file under a key naming the GPU, the grid, the scalar, the
+ * precision and the flow type, and a later call (or paratc_create, when the
+ * environment variable PARATC_TUNE_CACHE names the file) that finds its key
+ * there applies the picks without searching (from_cache = 1).  All choices
+ * compute the same step; results differ by rounding only. */
+typedef struct paratc_tuning {
+    int32_t schedule;    /* Poisson schedule, as paratc_autotune               */
+    int32_t rhs_var;     /* right-hand-side launch shape                        */
+    int32_t helm_var;    /* Helmholtz launch shape                              */
+    int32_t from_cache;  /* 1 when the picks were read from the cache           */
+    double  step_ms;     /* ms per step of the picks when they were timed       */
+} paratc_tuning;
+int paratc_autotune_all(paratc_ctx* ctx, int nrep, const char* cache_path, paratc_tuning* out);
+int paratc_get_tuning(paratc_ctx* ctx, paratc_tuning* out);
+/* pin a combination (PARATC_ERR_BAD_ARG when one of its parts does not exist here) */
+int paratc_set_tuning(paratc_ctx* ctx, const paratc_tuning* t);
 
 /* ---- Statistics (clcStat, src/m_FlowCase.f90:257-428).  FP64 accumulators
  * on the device: SumStat(k, jc) += <q_k>_xz for the 35 moments of clcStat (40

@@ -95,3 +95,9 @@ class ParatcIoOptions(ctypes.Structure):
         ("clc_spectra2d", ctypes.c_int32), ("ny_spec2d", ctypes.c_int32),
         ("iy_spec2d", ctypes.c_int32 * MAX_SPEC2D),
     ]
+
+
+class ParatcTuning(ctypes.Structure):
+    """paratc_tuning of include/paratc.h."""
+    _fields_ = [("schedule", ctypes.c_int32), ("rhs_var", ctypes.c_int32), ("helm_var", ctypes.c_int32),
+                ("from_cache", ctypes.c_int32), ("step_ms", ctypes.c_double)]

@@ -51,6 +51,8 @@ struct paratc_ctx {
     FftPlan plx, plz;
     Fields f;
     int prec = PARATC_PREC_FP64;  // PARATC_PREC_FP64 / _MIXED / _FP32
+    int tune_from_cache = 0;      // the launch shapes and schedule came from the tuning cache
+    double tune_step_ms = 0.0;    // ms per step of the tuned combination (0: not timed here)
     Fields32 f32{};               // float fields of the FP32 storage form (pr = f.pr), allocated on first use
     float* d_phi32 = nullptr;     // its potential (padded)
     std::vector<void*> allocs;
@@ -104,6 +106,12 @@ struct paratc_ctx {
     double prof_ms[PARATC_PROF_NKERNELS] = {0};
     int64_t prof_n[PARATC_PROF_NKERNELS] = {0};
 };
+
+// tuning cache (defined with paratc_autotune_all)
+static std::string tune_key(const paratc_ctx* ctx);
+static bool tune_cache_read(const char* path, const std::string& key, paratc_tuning* t);
+static bool tuning_valid(const paratc_ctx* ctx, const paratc_tuning& t);
+static void tuning_apply(paratc_ctx* ctx, const paratc_tuning& t);
 
 namespace {
 
@@ -354,7 +362,7 @@ void enqueue_substep32(paratc_ctx* ctx, int ns, int stop) {
     {
         PROF(PK_RHS);
         launch_rhs_tile(st, ctx->kc, ctx->dm, ctx->d_coef, ctx->f32, ctx->d_uy_ym, ctx->d_duy_ym, ns, h.gam[ns - 1],
-                        h.the[ns - 1], h.alp[ns - 1], ctx->d_part, ctx->d_counter, ctx->d_zt_err);
+                        h.the[ns - 1], h.alp[ns - 1], ctx->d_part, ctx->d_counter);
     }
     ctx->launches += 1;
     if (stop == 1) return;
@@ -386,7 +394,7 @@ void enqueue_substep(paratc_ctx* ctx, int ns, int stop = 5) {
     {
         PROF(PK_RHS);
         launch_rhs_tile(st, ctx->kc, ctx->dm, ctx->d_coef, ctx->f, ctx->d_uy_ym, ctx->d_duy_ym, ns, h.gam[ns - 1],
-                        h.the[ns - 1], h.alp[ns - 1], ctx->d_part, ctx->d_counter, ctx->d_zt_err);
+                        h.the[ns - 1], h.alp[ns - 1], ctx->d_part, ctx->d_counter);
     }
     ctx->launches += 1;
     if (stop == 1) return;
@@ -443,8 +451,8 @@ void diag_out(const DDiag& d, paratc_diag* o) {
 
 int sync(paratc_ctx* ctx) {
     // the error word of the TMA-fed kernels comes back with the same wait:
-    // bit 1 z transform, 2 x transform, 4 divergence-fed transform, 8 the
-    // right-hand side's row pipeline (a bounded wait that ran out)
+    // bit 1 z transform, 2 x transform, 4 divergence-fed transform (a bounded
+    // wait that ran out)
     unsigned int* hb = reinterpret_cast<unsigned int*>(ctx->h_scal + 15);
     *hb = 0u;
     cudaError_t e = cudaMemcpyAsync(hb, ctx->d_zt_err, sizeof(unsigned int), cudaMemcpyDeviceToHost, ctx->st);
@@ -454,8 +462,8 @@ int sync(paratc_ctx* ctx) {
     if (e != cudaSuccess) return set_err(ctx, PARATC_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(e));
     if (*hb) {
         std::string m;
-        const char* names[4] = {"z transform", "x transform", "divergence-fed x transform", "right-hand side"};
-        for (int b = 0; b < 4; b++)
+        const char* names[3] = {"z transform", "x transform", "divergence-fed x transform"};
+        for (int b = 0; b < 3; b++)
             if (*hb & (1u << b)) m += (m.empty() ? "" : ", ") + std::string(names[b]);
         return set_err(ctx, PARATC_ERR_TIMEOUT, m + ": a bounded wait on a copy pipeline gave up");
     }
@@ -715,7 +723,7 @@ int paratc_create(const paratc_params* prm, const double* yp, int device, paratc
     // partial-result records of the grid reductions: one per block of k_prsrc /
     // k_cfl, one per block of the RHS and forward-x kernels, 8 per block of the
     // end-of-step kernel
-    ctx->npart = std::max(std::max(2 * cell_grid_blocks(kc), rhs_grid_blocks(kc)),
+    ctx->npart = std::max(std::max(3 * cell_grid_blocks(kc), rhs_grid_blocks(kc)),
                           std::max((size_t)pfft_x_blocks(ctx->nx, ctx->ny, ctx->nz), endstep_blocks(kc) * 8)) + 64;
     if ((rc = dalloc(ctx, &ctx->d_src, ctx->ni)) || (rc = dalloc(ctx, &ctx->d_spec, (size_t)ctx->M1 * ctx->ny * ctx->nz)) ||
         (rc = dalloc(ctx, &ctx->d_part, ctx->npart)) || (rc = dalloc(ctx, &ctx->d_uy_ym, (size_t)ctx->nx * ctx->nz)) ||
@@ -807,6 +815,16 @@ int paratc_create(const paratc_params* prm, const double* yp, int device, paratc
     }
     rc = load_state_common(ctx, true);
     if (rc != PARATC_OK) { paratc_destroy(ctx); return rc; }
+    // picks of an earlier tuning run on this GPU and grid (paratc_autotune_all)
+    if (const char* cache = std::getenv("PARATC_TUNE_CACHE")) {
+        paratc_tuning t;
+        std::memset(&t, 0, sizeof(t));
+        if (tune_cache_read(cache, tune_key(ctx), &t) && tuning_valid(ctx, t)) {
+            tuning_apply(ctx, t);
+            ctx->tune_from_cache = 1;
+            ctx->tune_step_ms = t.step_ms;
+        }
+    }
     *out = ctx;
     return PARATC_OK;
 }
@@ -1034,7 +1052,7 @@ int paratc_poisson_refined_async(paratc_ctx* ctx, const double* d_src, double* d
         // r = src - L phi in FP64 (into the context's compact work array), then
         // its FP32-spectrum solve added to phi
         launch_residual(ctx->st, ctx->kc, ctx->dm, d_src, d_phi, ctx->d_src, ctx->d_part, ctx->d_counter + 5,
-                        ctx->d_scal + 2);
+                        ctx->d_scal + 4);
         ctx->launches += 1;
         enqueue_solve32(ctx, ctx->d_src, d_phi, 1);
     }
@@ -1052,12 +1070,12 @@ int paratc_poisson_refined(paratc_ctx* ctx, const double* d_src, double* d_phi, 
     double rel = 0.0;
     for (;;) {
         launch_residual(ctx->st, ctx->kc, ctx->dm, d_src, d_phi, ctx->d_src, ctx->d_part, ctx->d_counter + 5,
-                        ctx->d_scal + 2);
+                        ctx->d_scal + 4);
         ctx->launches += 1;
-        CK(cudaMemcpyAsync(ctx->h_scal + 2, ctx->d_scal + 2, 2 * sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
+        CK(cudaMemcpyAsync(ctx->h_scal + 4, ctx->d_scal + 4, 2 * sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
         const int rc = sync(ctx);
         if (rc) return rc;
-        rel = ctx->h_scal[2] / std::max(ctx->h_scal[3], 1e-300);
+        rel = ctx->h_scal[4] / std::max(ctx->h_scal[5], 1e-300);
         if (!(rel > rtol) || q >= max_corr) break;
         enqueue_solve32(ctx, ctx->d_src, d_phi, 1);
         q++;
@@ -1197,6 +1215,206 @@ int paratc_autotune(paratc_ctx* ctx, int nrep, int* choice, double* times_ms) {
     sched_apply(ctx, best);
     if (choice) *choice = best;
     return PARATC_OK;
+}
+
+extern "C++" {
+// ---- tuning of the launch shapes and the Poisson schedule, with a cache
+// file.  The key names the GPU, the grid, the scalar, the precision and the
+// flow type; one entry per line,
+//   "NVIDIA B200|128x96x128|s0|p0|f1": {"schedule": 6, "rhs_var": 0, "helm_var": 1, "step_ms": 0.5},
+// so the file is JSON and a line-by-line reader finds an entry.
+static std::string tune_key(const paratc_ctx* ctx) {
+    cudaDeviceProp pr;
+    std::memset(&pr, 0, sizeof(pr));
+    cudaGetDeviceProperties(&pr, ctx->dev);
+    char b[384];
+    std::snprintf(b, sizeof(b), "%s|%dx%dx%d|s%d|p%d|f%d", pr.name, ctx->nx, ctx->ny, ctx->nz, ctx->prm.scalar_on ? 1 : 0,
+                  ctx->prec, ctx->prm.flow_type);
+    return b;
+}
+
+static bool tune_field(const std::string& line, const char* name, double* v) {
+    const std::string pat = std::string("\"") + name + "\":";
+    const size_t p = line.find(pat);
+    if (p == std::string::npos) return false;
+    return std::sscanf(line.c_str() + p + pat.size(), "%lf", v) == 1;
+}
+
+// the cached entry of `key` in `path` (false when the file or the entry is missing)
+static bool tune_cache_read(const char* path, const std::string& key, paratc_tuning* t) {
+    FILE* fp = path ? std::fopen(path, "r") : nullptr;
+    if (!fp) return false;
+    char buf[1024];
+    bool found = false;
+    const std::string k = "\"" + key + "\":";
+    while (!found && std::fgets(buf, sizeof(buf), fp)) {
+        const std::string line(buf);
+        if (line.find(k) == std::string::npos) continue;
+        double sc, rv, hv, ms = 0.0;
+        if (tune_field(line, "schedule", &sc) && tune_field(line, "rhs_var", &rv) && tune_field(line, "helm_var", &hv)) {
+            tune_field(line, "step_ms", &ms);
+            t->schedule = (int32_t)sc;
+            t->rhs_var = (int32_t)rv;
+            t->helm_var = (int32_t)hv;
+            t->step_ms = ms;
+            found = true;
+        }
+    }
+    std::fclose(fp);
+    return found;
+}
+
+// adds or replaces the entry of `key`, keeping the others
+static int tune_cache_write(const char* path, const std::string& key, const paratc_tuning& t) {
+    std::vector<std::string> keep;
+    const std::string k = "\"" + key + "\":";
+    if (FILE* fp = std::fopen(path, "r")) {
+        char buf[1024];
+        while (std::fgets(buf, sizeof(buf), fp)) {
+            std::string line(buf);
+            while (!line.empty() && (line.back() == '\n' || line.back() == ',' || line.back() == ' ')) line.pop_back();
+            if (line.find("\": {") == std::string::npos || line.find(k) != std::string::npos) continue;
+            keep.push_back(line);
+        }
+        std::fclose(fp);
+    }
+    char b[640];
+    std::snprintf(b, sizeof(b), "  \"%s\": {\"schedule\": %d, \"rhs_var\": %d, \"helm_var\": %d, \"step_ms\": %.6f}",
+                  key.c_str(), t.schedule, t.rhs_var, t.helm_var, t.step_ms);
+    keep.push_back(b);
+    FILE* fp = std::fopen(path, "w");
+    if (!fp) return PARATC_ERR_IO;
+    std::fprintf(fp, "{\n");
+    for (size_t q = 0; q < keep.size(); q++) std::fprintf(fp, "%s%s\n", keep[q].c_str(), q + 1 < keep.size() ? "," : "");
+    std::fprintf(fp, "}\n");
+    std::fclose(fp);
+    return PARATC_OK;
+}
+
+static bool tuning_valid(const paratc_ctx* ctx, const paratc_tuning& t) {
+    return sched_supported(ctx, t.schedule) && t.rhs_var >= 0 && t.rhs_var < rhs_variants() && t.helm_var >= 0 &&
+           t.helm_var < helm_variants() && !(ctx->prec == PARATC_PREC_FP32 && t.schedule / 2 == 2);
+}
+
+static void tuning_apply(paratc_ctx* ctx, const paratc_tuning& t) {
+    sched_apply(ctx, t.schedule);
+    ctx->kc.rhs_var = t.rhs_var;
+    ctx->kc.helm_var = t.helm_var;
+}
+
+}  // extern "C++"
+
+int paratc_get_tuning(paratc_ctx* ctx, paratc_tuning* t) {
+    if (!ctx || !t) return PARATC_ERR_BAD_ARG;
+    int sc = 0;
+    paratc_get_schedule(ctx, &sc);
+    t->schedule = sc;
+    t->rhs_var = ctx->kc.rhs_var;
+    t->helm_var = ctx->kc.helm_var;
+    t->from_cache = ctx->tune_from_cache;
+    t->step_ms = ctx->tune_step_ms;
+    return PARATC_OK;
+}
+
+int paratc_set_tuning(paratc_ctx* ctx, const paratc_tuning* t) {
+    if (!ctx || !t || !tuning_valid(ctx, *t)) return PARATC_ERR_BAD_ARG;
+    tuning_apply(ctx, *t);
+    ctx->tune_from_cache = 0;
+    return PARATC_OK;
+}
+
+int paratc_autotune_all(paratc_ctx* ctx, int nrep, const char* cache_path, paratc_tuning* out) {
+    if (!ctx || nrep < 1) return PARATC_ERR_BAD_ARG;
+    CK(cudaSetDevice(ctx->dev));
+    const std::string key = tune_key(ctx);
+    paratc_tuning t;
+    std::memset(&t, 0, sizeof(t));
+    if (tune_cache_read(cache_path, key, &t) && tuning_valid(ctx, t)) {
+        tuning_apply(ctx, t);
+        ctx->tune_from_cache = 1;
+        ctx->tune_step_ms = t.step_ms;
+        return paratc_get_tuning(ctx, out ? out : &t);
+    }
+    // 1. the Poisson schedule (InitPoissonSolver's search, src/m_Poisson.f90:50-175)
+    int sched = 0;
+    int rc = paratc_autotune(ctx, nrep, &sched, nullptr);
+    if (rc) return rc;
+    // 2. the launch shapes, timed by whole steps from a saved state that is
+    // put back afterwards (u, v, w, p, c, histories, uy_ym, the coefficients)
+    rc = sync(ctx);
+    if (rc) return rc;
+    const bool fp32 = ctx->prec == PARATC_PREC_FP32;
+    std::vector<std::pair<void*, size_t>> st;
+    const size_t nb64 = ctx->nf * sizeof(double), nb32 = ctx->nf * sizeof(float);
+    if (fp32) {
+        for (float* q : {ctx->f32.ux, ctx->f32.uy, ctx->f32.uz, ctx->f32.hx, ctx->f32.hy, ctx->f32.hz, ctx->f32.sc, ctx->f32.hc})
+            if (q) st.push_back({q, nb32});
+    } else {
+        for (double* q : {ctx->f.ux, ctx->f.uy, ctx->f.uz, ctx->f.hx, ctx->f.hy, ctx->f.hz, ctx->f.sc, ctx->f.hc})
+            if (q) st.push_back({q, nb64});
+    }
+    st.push_back({ctx->f.pr, nb64});
+    st.push_back({ctx->d_uy_ym, (size_t)ctx->nx * ctx->nz * sizeof(double)});
+    st.push_back({ctx->d_duy_ym, (size_t)ctx->nx * ctx->nz * sizeof(double)});
+    st.push_back({ctx->d_coef, sizeof(DCoef)});
+    size_t total = 0;
+    for (auto& e : st) total += (e.second + 255) & ~(size_t)255;
+    char* save = nullptr;
+    CK(cudaMalloc(&save, total));
+    auto copy_all = [&](bool to_save) {
+        size_t o = 0;
+        for (auto& e : st) {
+            cudaMemcpyAsync(to_save ? save + o : e.first, to_save ? e.first : save + o, e.second,
+                            cudaMemcpyDeviceToDevice, ctx->st);
+            o += (e.second + 255) & ~(size_t)255;
+        }
+    };
+    copy_all(true);
+    const bool ready0 = ctx->next_ready;
+    const double hdt0 = ctx->hfac_dt;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    const int nr = (ctx->prec == PARATC_PREC_FP64) ? rhs_variants() : 1;  // FP32 arithmetic forms have one shape
+    float best = -1.f;
+    paratc_tuning bt = {sched, 0, 0, 0, 0.0};
+    for (int rv = 0; rv < nr; rv++)
+        for (int hv = 0; hv < helm_variants(); hv++) {
+            ctx->kc.rhs_var = rv;
+            ctx->kc.helm_var = hv;
+            copy_all(false);
+            ctx->next_ready = false;
+            ctx->hfac_dt = -1.0;
+            enqueue_step(ctx);  // warm-up
+            cudaEventRecord(e0, ctx->st);
+            for (int q = 0; q < nrep; q++) enqueue_step(ctx);
+            cudaEventRecord(e1, ctx->st);
+            if ((rc = sync(ctx))) break;
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            ms /= (float)nrep;
+            if (best < 0.f || ms < best) { best = ms; bt.rhs_var = rv; bt.helm_var = hv; }
+        }
+    copy_all(false);
+    CK(cudaMemsetAsync(ctx->d_diag, 0, sizeof(DDiag), ctx->st));
+    const int rc2 = sync(ctx);
+    cudaFree(save);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    ctx->next_ready = false;
+    ctx->hfac_dt = -1.0;
+    (void)ready0;
+    (void)hdt0;
+    if (rc) return rc;
+    if (rc2) return rc2;
+    bt.step_ms = best;
+    tuning_apply(ctx, bt);
+    ctx->sched_gen++;
+    ctx->tune_from_cache = 0;
+    ctx->tune_step_ms = best;
+    if (cache_path && (rc = tune_cache_write(cache_path, key, bt)))
+        return set_err(ctx, rc, std::string("cannot write the tuning cache ") + cache_path);
+    return paratc_get_tuning(ctx, out ? out : &bt);
 }
 
 int paratc_project(paratc_ctx* ctx, double* divmax_out) {

@@ -6,16 +6,13 @@
 // scalar) over the tile plus the x/z halo of 3 cells that the interpolated
 // face velocities and the 4th-order stencils read.  Those row-slabs
 // (40 x 14 values per field and row: the x range starts 4 cells left of the
-// tile so that every copy starts on a 16-byte boundary) sit in a ring of
-// 3 + PF slots in shared memory.  In FP64 the slabs of rows j+2 .. j+1+PF are
-// brought in by the tensor memory accelerator while row j is computed: one
-// warp issues, per field and z-plane, a bulk copy (cp.async.bulk) of the
-// row's 40-value x range -- split in two where the periodic x range wraps --
-// onto the slot's mbarrier, and every thread waits on that barrier (bounded:
-// a wait that runs out records PARATC_ERR_TIMEOUT's bit 8 in the error word,
-// the CTA drains its copies in flight and stops computing).  The row's metric
-// coefficients (interpolation weights, 1/dy, the d2/dy2 stencils) come as one
-// 128-byte record (DMetric::rowmet) in the same copy group, so no global
+// tile so that every 16-byte pair of values is aligned and never straddles
+// the periodic wrap) sit in a ring of 3 + PF slots in shared memory.  In FP64
+// the slabs of rows j+2 .. j+1+PF are copied in with 16-byte cp.async while
+// row j is computed, one commit group per row, so the HBM loads overlap the
+// arithmetic.  The row's metric coefficients (interpolation weights, 1/dy,
+// the d2/dy2 stencils) come as one 128-byte record (DMetric::rowmet) in the
+// same group, so no global
 // load sits on a row's dependent path.  Each thread computes
 // two z-adjacent cells per row (FP64; one in the FP32 form): RhsX/RhsY/RhsZ
 // (and RhsC) and the new explicit histories, reading every neighbour from
@@ -40,7 +37,6 @@
 #include "common.cuh"
 #include "kernels.cuh"
 #include "reduce.cuh"
-#include "tma.cuh"
 
 namespace ptc {
 namespace {
@@ -49,21 +45,35 @@ constexpr int TX = 32, TZ = 8, HX = 4, HZ = 3;
 constexpr int SX = TX + 2 * HX;  // 40: x offsets -4 .. 35 of the tile (the stencils read -3 .. 34)
 constexpr int SZ = TZ + 2 * HZ;  // 14
 constexpr int SLAB = SX * SZ;    // 560 doubles per field and row
-constexpr int PF = 1;            // FP64: rows loaded ahead beyond row j+1 (copy groups in flight)
-// per precision: z-adjacent cells per thread (FP64: 2, whose shared stencil
-// taps then load once; FP32: 1) and threads per CTA
-template <class T>
+// The launch shape, per precision and compiled variant VAR (the tuner's
+// choice, paratc_autotune_all): PF rows loaded ahead beyond row j+1 (copy
+// groups in flight; FP64), ZC z-adjacent cells per thread (2 lets the shared
+// stencil taps of the two cells load once; FP32: 1) and the threads per CTA.
+// FP64 variants: 0 PF 1, ZC 2 (128 threads); 1 PF 2, ZC 2; 2 PF 1, ZC 1
+// (256 threads).  The FP32 forms have one variant.
+constexpr int RHS_NVAR = 3;
+template <class T, int VAR = 0>
 struct RhsCfg {
-    static constexpr int NB = sizeof(T) == 8 ? 3 + PF : 4;  // ring slots: rows j-1..j+1 and the rows in flight
-    static constexpr int MINB = 2;                            // resident CTAs per SM (FP64: 3 spills and is slower)
-    static constexpr int ZC = sizeof(T) == 8 ? 2 : 1;
+    static constexpr bool F64 = sizeof(T) == 8;
+    static constexpr int PF = (F64 && VAR == 1) ? 2 : 1;
+    static constexpr int NB = F64 ? 3 + PF : 4;  // ring slots: rows j-1..j+1 and the rows in flight
+    static constexpr int MINB = 2;               // resident CTAs per SM (FP64, 2 cells: 3 spills and is slower)
+    static constexpr int ZC = (F64 && VAR != 2) ? 2 : 1;
     static constexpr int NTHR = TX * TZ / ZC;  // 128 or 256
     static constexpr int NSLOT = (SLAB + NTHR - 1) / NTHR;
 };
-template <bool SCALAR, class T>
+template <bool SCALAR, class T, int VAR = 0>
 constexpr size_t rhs_smem_bytes() {
-    return (size_t)RhsCfg<T>::NB * (SCALAR ? 5 : 4) * SLAB * sizeof(T);
+    return (size_t)RhsCfg<T, VAR>::NB * (SCALAR ? 5 : 4) * SLAB * sizeof(T);
 }
+
+__device__ __forceinline__ void cp_async16(void* sdst, const void* gsrc) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(sdst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
 // the field a copy reads (f = 0 ux, 1 uy, 2 uz, 3 p, 4 scalar)
 __device__ __forceinline__ const double* field_of(const Fields& fl, int f) {
@@ -88,21 +98,21 @@ __device__ __forceinline__ int modp(int i, int n) {
 // SCALAR: with the scalar transport; T: arithmetic (double, or float for the
 // mixed and FP32 storage forms); V: storage of u, v, w, c, Hist and Rhs
 // (float only in the FP32 storage form, whose arithmetic is float)
-template <bool SCALAR, class T, class V>
-__global__ void __launch_bounds__(RhsCfg<T>::NTHR, RhsCfg<T>::MINB)
+template <bool SCALAR, class T, class V, int VAR>
+__global__ void __launch_bounds__(RhsCfg<T, VAR>::NTHR, RhsCfg<T, VAR>::MINB)
     k_rhs_tile(DConst c, DMetric m, DCoef* __restrict__ coef, FieldSet<V> fl, double* __restrict__ uy_ym,
                double* __restrict__ duy_ym, int ns, double gam, double the, double alp, double* __restrict__ part,
-               unsigned int* __restrict__ counter, unsigned int* __restrict__ err) {
+               unsigned int* __restrict__ counter) {
     constexpr int NF = SCALAR ? 5 : 4;
     constexpr bool F64 = sizeof(T) == 8;
     static_assert(!F64 || sizeof(V) == 8, "the FP64 arithmetic form keeps FP64 fields");
-    constexpr int ZC = RhsCfg<T>::ZC, NTHR = RhsCfg<T>::NTHR, NSLOT = RhsCfg<T>::NSLOT, NB = RhsCfg<T>::NB;
-    // bytes one FP64 row brings into its slot: NF fields x SZ planes x SX values, and the metric record
-    constexpr unsigned ROW_BYTES = (unsigned)(NF * SZ * SX) * 8u + ROWMET * 8u;
+    using CFG = RhsCfg<T, VAR>;
+    constexpr int ZC = CFG::ZC, NTHR = CFG::NTHR, NSLOT = CFG::NSLOT, NB = CFG::NB, PF = CFG::PF;
+    // FP64 copies: 16-byte pairs, NPAIR per (field, z-plane) row, NP2 per thread and field
+    constexpr int NPAIR = SX / 2, NPR = SZ * NPAIR, NP2 = (NPR + NTHR - 1) / NTHR;
     extern __shared__ __align__(128) unsigned char sm_raw[];
     T* sm = reinterpret_cast<T*>(sm_raw);  // [NB][NF][SLAB]
     __shared__ __align__(128) double smet[NB][ROWMET];
-    __shared__ unsigned long long bar[NB];
     const int lane = threadIdx.x, wq = threadIdx.y, tid = wq * 32 + lane;
     const int nx = c.nx, nz = c.nz, ny = c.ny;
     const size_t pl = (size_t)c.nyt * nx;
@@ -112,13 +122,6 @@ __global__ void __launch_bounds__(RhsCfg<T>::NTHR, RhsCfg<T>::MINB)
     const int ntx = (nx + TX - 1) / TX, ntz = (nz + TZ - 1) / TZ;
     const long long W = (long long)ntx * ntz * ny;
     const long long gbeg = W * blockIdx.x / gridDim.x, gend = W * (blockIdx.x + 1) / gridDim.x;
-    const long long lim = F64 ? tma::wait_limit(err) : 0;
-    if (F64 && tid == 0) {
-#pragma unroll
-        for (int q = 0; q < NB; q++) tma::mbar_init(&bar[q], 1);
-        tma::fence_mbar_init();
-    }
-    __syncthreads();
     pdl_wait();
     pdl_trigger();
 
@@ -141,13 +144,8 @@ __global__ void __launch_bounds__(RhsCfg<T>::NTHR, RhsCfg<T>::MINB)
     const T tpG = (T)pmGamma, tpT = (T)pmTheta, tpA = (T)pmAlpha, ttb = (T)tb, ttbs = (T)tbs;
     const T tsdiff = F64 ? (T)c.sdiff : (T)c.fsdiff;
     double s3 = 0.0;
-    // FP64 copy pipeline: phase parity per slot and the slots with a copy
-    // group in flight (the same in every thread: issue and wait decisions are
-    // uniform over the CTA)
-    unsigned phase = 0u, pend = 0u;
-    bool failed = false;
 
-    for (long long g = gbeg; g < gend && !failed;) {
+    for (long long g = gbeg; g < gend;) {
         const int tile = (int)(g / ny);
         const int j0 = (int)(g - (long long)tile * ny) + 1;
         const int j1 = (int)min((long long)ny, (long long)j0 + (gend - g) - 1);
@@ -167,45 +165,29 @@ __global__ void __launch_bounds__(RhsCfg<T>::NTHR, RhsCfg<T>::MINB)
                 soff[s] = e;
             }
         }
-        // FP64: warp 0 issues the row's bulk copies onto the slot's barrier.
-        // Each (field, z-plane) copies the periodic x range [i0-4, i0+36):
-        // nx is even and i0 a multiple of 32, so every piece starts on an
-        // even index (16-byte aligned) and spans an even count of values.
-        const int x0 = modp(i0 - HX, nx);
-        auto issue_row = [&](int jrow) {
-            const int sl = jrow % NB;
-            pend |= 1u << sl;
-            if constexpr (!F64) return;
-            else {
-            if (wq != 0) return;
-            if (lane == 0) tma::mbar_expect_tx(&bar[sl], ROW_BYTES);
-            __syncwarp();
-            double* dst = reinterpret_cast<double*>(sm) + (size_t)sl * NF * SLAB;
-            for (int q = lane; q < NF * SZ; q += 32) {
-                const int f = q / SZ, zz = q - f * SZ;
-                const double* src = field_of(fl, f) + (size_t)modp(k0 - HZ + zz, nz) * pl + (size_t)jrow * nx;
-                double* d = dst + f * SLAB + zz * SX;
-                int x = x0, col = 0;
-                while (col < SX) {
-                    const int len = min(SX - col, nx - x);
-                    tma::bulk_load(d + col, src + x, (unsigned)len * 8u, &bar[sl]);
-                    col += len;
-                    x = 0;
-                }
+        // FP64: the 16-byte pairs this thread copies (the same for every field)
+        size_t gp[F64 ? NP2 : 1];
+        int sp[F64 ? NP2 : 1];
+        bool vp[F64 ? NP2 : 1];
+        if constexpr (F64) {
+#pragma unroll
+            for (int q = 0; q < NP2; q++) {
+                const int e = tid + q * NTHR;
+                vp[q] = e < NPR;
+                const int zz = e / NPAIR, pp = e - zz * NPAIR;
+                gp[q] = (size_t)modp(k0 - HZ + zz, nz) * pl + (size_t)modp(i0 - HX + 2 * pp, nx);
+                sp[q] = zz * SX + 2 * pp;
             }
-            if (lane == 0) tma::bulk_load(smet[sl], m.rowmet + (size_t)jrow * ROWMET, ROWMET * 8u, &bar[sl]);
-            }
-        };
-        // every thread waits for the row's copies; the CTA stops as one when
-        // any thread's wait ran out
-        auto wait_row = [&](int jrow) -> bool {
-            const int sl = jrow % NB;
-            const bool ok = tma::mbar_wait(&bar[sl], (phase >> sl) & 1u, lim);
-            if (__syncthreads_or(ok ? 0 : 1)) return false;
-            phase ^= 1u << sl;
-            pend &= ~(1u << sl);
-            return true;
-        };
+        }
+#define LOAD_ROW64(jrow)                                                                             \
+    do {                                                                                             \
+        double* dst_ = reinterpret_cast<double*>(sm) + (size_t)((jrow) % NB) * NF * SLAB;           \
+        const size_t ro_ = (size_t)(jrow) * nx;                                                      \
+        _Pragma("unroll") for (int f_ = 0; f_ < NF; f_++)                                            \
+            _Pragma("unroll") for (int q_ = 0; q_ < NP2; q_++) if (vp[q_])                           \
+                cp_async16(dst_ + f_ * SLAB + sp[q_], field_of(fl, f_) + gp[q_] + ro_);              \
+        if (tid < ROWMET / 2) cp_async16(&smet[(jrow) % NB][2 * tid], m.rowmet + (size_t)(jrow) * ROWMET + 2 * tid); \
+    } while (0)
         // FP32: load, convert, store
 #define LOAD_ROW32(jrow)                                                                 \
     do {                                                                                 \
@@ -218,10 +200,16 @@ __global__ void __launch_bounds__(RhsCfg<T>::NTHR, RhsCfg<T>::MINB)
     } while (0)
 
         if constexpr (F64) {
-            // rows j0-1 .. j0+1+PF (those that exist), then rows j0-1 and j0 in place
-            for (int d = -1; d <= 1 + PF; d++)
-                if (j0 + d <= j1 + 1) issue_row(j0 + d);
-            if (!wait_row(j0 - 1) || !wait_row(j0)) { failed = true; break; }
+            // rows j0-1 .. j0+1 in one commit group, rows j0+2 .. j0+PF one group each
+            LOAD_ROW64(j0 - 1);
+            LOAD_ROW64(j0);
+            LOAD_ROW64(j0 + 1);
+            cp_async_commit();
+#pragma unroll
+            for (int d = 2; d <= PF; d++) {
+                if (j0 + d <= j1 + 1) LOAD_ROW64(j0 + d);
+                cp_async_commit();
+            }
         } else {
             LOAD_ROW32(j0 - 1);
             LOAD_ROW32(j0);
@@ -268,7 +256,8 @@ __global__ void __launch_bounds__(RhsCfg<T>::NTHR, RhsCfg<T>::MINB)
             if constexpr (F64) {
                 // the slot of row j+1+PF was last read by row j-1's arithmetic,
                 // which every thread finished at the barrier closing it
-                if (j > j0 && j + 1 + PF <= j1 + 1) issue_row(j + 1 + PF);
+                if (j + 1 + PF <= j1 + 1) LOAD_ROW64(j + 1 + PF);
+                cp_async_commit();
             } else if (more) {
                 const size_t ro = (size_t)(j + 2) * nx;
 #pragma unroll
@@ -295,7 +284,8 @@ __global__ void __launch_bounds__(RhsCfg<T>::NTHR, RhsCfg<T>::MINB)
             for (int cz = 0; cz < ZC; cz++)
                 u64n[cz] = (!F64 && act[cz] && j + 2 <= ny + 1) ? __ldg(&fl.ux[q0a[cz] + 2 * nx]) : 0.0;
             if constexpr (F64) {
-                if (!wait_row(j + 1)) { failed = true; break; }
+                cp_async_wait<PF>();  // the group holding row j+1 is complete
+                __syncthreads();
             }
             // both cells are computed before any global store, so that the
             // compiler may load a tap the two cells share once
@@ -477,16 +467,9 @@ __global__ void __launch_bounds__(RhsCfg<T>::NTHR, RhsCfg<T>::MINB)
         __syncthreads();
         }
 #undef LOAD_ROW32
+#undef LOAD_ROW64
     }
-    if constexpr (F64) {
-        if (failed && tid == 0) {
-            atomicOr(err, 8u);
-            // copies still in flight land in this CTA's slots: wait for them
-            // (full limit) before the CTA can end
-            for (int q = 0; q < NB; q++)
-                if (pend & (1u << q)) tma::mbar_wait(&bar[q], (phase >> q) & 1u);
-        }
-    }
+    if constexpr (F64) cp_async_wait<0>();
 #undef KC
 #undef dxC
 #undef dzC
@@ -543,46 +526,61 @@ static size_t rhs_blocks(const DConst& c, int minb) {
 }
 
 size_t rhs_grid_blocks(const DConst& c) {
-    return rhs_blocks(c, RhsCfg<double>::MINB > RhsCfg<float>::MINB ? RhsCfg<double>::MINB : RhsCfg<float>::MINB);
+    return rhs_blocks(c, 2);  // MINB of every variant
 }
 
+int rhs_variants() { return RHS_NVAR; }
+
 void rhs_init() {
-#define RHS_ATTR(S, T, V)                                                                                 \
-    cudaFuncSetAttribute(k_rhs_tile<S, T, V>, cudaFuncAttributeMaxDynamicSharedMemorySize,             \
-                         (int)rhs_smem_bytes<S, T>());
-    RHS_ATTR(false, double, double) RHS_ATTR(true, double, double)
-    RHS_ATTR(false, float, double) RHS_ATTR(true, float, double)
-    RHS_ATTR(false, float, float) RHS_ATTR(true, float, float)
+#define RHS_ATTR(S, T, V, VAR)                                                                            \
+    cudaFuncSetAttribute(k_rhs_tile<S, T, V, VAR>, cudaFuncAttributeMaxDynamicSharedMemorySize,        \
+                         (int)rhs_smem_bytes<S, T, VAR>());
+    RHS_ATTR(false, double, double, 0) RHS_ATTR(true, double, double, 0)
+    RHS_ATTR(false, double, double, 1) RHS_ATTR(true, double, double, 1)
+    RHS_ATTR(false, double, double, 2) RHS_ATTR(true, double, double, 2)
+    RHS_ATTR(false, float, double, 0) RHS_ATTR(true, float, double, 0)
+    RHS_ATTR(false, float, float, 0) RHS_ATTR(true, float, float, 0)
 #undef RHS_ATTR
 }
 
-template <bool SCALAR, class T, class V>
+template <bool SCALAR, class T, int VAR, class V>
 static void launch_rhs_t(cudaStream_t st, const DConst& c, const DMetric& m, DCoef* coef, const FieldSet<V>& f,
                          double* uy_ym, double* duy_ym, int ns, double gam, double the, double alp, double* part,
-                         unsigned int* counter, unsigned int* err) {
-    const dim3 grd((unsigned)rhs_blocks(c, RhsCfg<T>::MINB));
-    const dim3 blk(32, TZ / RhsCfg<T>::ZC);
-    launch_pdl(k_rhs_tile<SCALAR, T, V>, grd, blk, rhs_smem_bytes<SCALAR, T>(), st, c, m, coef, f, uy_ym, duy_ym, ns,
-               gam, the, alp, part, counter, err);
+                         unsigned int* counter) {
+    using CFG = RhsCfg<T, VAR>;
+    const dim3 grd((unsigned)rhs_blocks(c, CFG::MINB));
+    const dim3 blk(32, TZ / CFG::ZC);
+    launch_pdl(k_rhs_tile<SCALAR, T, V, VAR>, grd, blk, rhs_smem_bytes<SCALAR, T, VAR>(), st, c, m, coef, f, uy_ym,
+               duy_ym, ns, gam, the, alp, part, counter);
+}
+
+template <bool SCALAR>
+static void launch_rhs64(cudaStream_t st, const DConst& c, const DMetric& m, DCoef* coef, const Fields& f,
+                         double* uy_ym, double* duy_ym, int ns, double gam, double the, double alp, double* part,
+                         unsigned int* counter) {
+    if (c.rhs_var == 1)
+        launch_rhs_t<SCALAR, double, 1>(st, c, m, coef, f, uy_ym, duy_ym, ns, gam, the, alp, part, counter);
+    else if (c.rhs_var == 2)
+        launch_rhs_t<SCALAR, double, 2>(st, c, m, coef, f, uy_ym, duy_ym, ns, gam, the, alp, part, counter);
+    else
+        launch_rhs_t<SCALAR, double, 0>(st, c, m, coef, f, uy_ym, duy_ym, ns, gam, the, alp, part, counter);
 }
 
 void launch_rhs_tile(cudaStream_t st, const DConst& c, const DMetric& m, DCoef* coef, const Fields& f, double* uy_ym,
-                     double* duy_ym, int ns, double gam, double the, double alp, double* part, unsigned int* counter,
-                     unsigned int* err) {
+                     double* duy_ym, int ns, double gam, double the, double alp, double* part, unsigned int* counter) {
     if (c.fp32_rhs) {
-        if (c.scalar_on) launch_rhs_t<true, float>(st, c, m, coef, f, uy_ym, duy_ym, ns, gam, the, alp, part, counter, err);
-        else launch_rhs_t<false, float>(st, c, m, coef, f, uy_ym, duy_ym, ns, gam, the, alp, part, counter, err);
+        if (c.scalar_on) launch_rhs_t<true, float, 0>(st, c, m, coef, f, uy_ym, duy_ym, ns, gam, the, alp, part, counter);
+        else launch_rhs_t<false, float, 0>(st, c, m, coef, f, uy_ym, duy_ym, ns, gam, the, alp, part, counter);
     } else {
-        if (c.scalar_on) launch_rhs_t<true, double>(st, c, m, coef, f, uy_ym, duy_ym, ns, gam, the, alp, part, counter, err);
-        else launch_rhs_t<false, double>(st, c, m, coef, f, uy_ym, duy_ym, ns, gam, the, alp, part, counter, err);
+        if (c.scalar_on) launch_rhs64<true>(st, c, m, coef, f, uy_ym, duy_ym, ns, gam, the, alp, part, counter);
+        else launch_rhs64<false>(st, c, m, coef, f, uy_ym, duy_ym, ns, gam, the, alp, part, counter);
     }
 }
 
 void launch_rhs_tile(cudaStream_t st, const DConst& c, const DMetric& m, DCoef* coef, const Fields32& f, double* uy_ym,
-                     double* duy_ym, int ns, double gam, double the, double alp, double* part, unsigned int* counter,
-                     unsigned int* err) {
-    if (c.scalar_on) launch_rhs_t<true, float>(st, c, m, coef, f, uy_ym, duy_ym, ns, gam, the, alp, part, counter, err);
-    else launch_rhs_t<false, float>(st, c, m, coef, f, uy_ym, duy_ym, ns, gam, the, alp, part, counter, err);
+                     double* duy_ym, int ns, double gam, double the, double alp, double* part, unsigned int* counter) {
+    if (c.scalar_on) launch_rhs_t<true, float, 0>(st, c, m, coef, f, uy_ym, duy_ym, ns, gam, the, alp, part, counter);
+    else launch_rhs_t<false, float, 0>(st, c, m, coef, f, uy_ym, duy_ym, ns, gam, the, alp, part, counter);
 }
 
 }  // namespace ptc

@@ -367,8 +367,14 @@ __global__ void k_cast(size_t n, const A* __restrict__ a, B* __restrict__ b) {
 // operator whose eigenvalues the spectral solve inverts (D4 the 4th-order
 // staggered first difference of clcPrSrc / FluidVelUpdate, so D4 D4 has the
 // modified wavenumber of src/m_Poisson.f90:40-48 as its symbol; Lyy the
-// Neumann wall-normal operator am2ph/ac2ph/ap2ph).  max|r| and max|src| go
-// to out[0], out[1] through the last CTA.
+// Neumann wall-normal operator am2ph/ac2ph/ap2ph).  The spectral solve
+// replaces the kx = kz = 0 equation of row 1 by phi_hat = 0
+// (src/m_Poisson.f90:399-404); that equation's residual is the plane mean of
+// r at row 1, nonzero whenever the source's dy-weighted mean is, and it is
+// removed (k_resid_row1) so that the corrections see only the equations the
+// solve keeps.  Record per CTA: max|r| over rows 2..ny, max|src|, and the sum
+// of r over its row-1 cells; the last CTA writes out[0] = max|r| (rows
+// 2..ny), out[1] = max|src|, out[2] = the row-1 plane mean.
 __global__ void __launch_bounds__(256) k_residual(DConst c, DMetric m, const double* __restrict__ src,
                                                   const double* __restrict__ phi, double* __restrict__ r,
                                                   double* __restrict__ part, unsigned int* __restrict__ counter,
@@ -389,7 +395,7 @@ __global__ void __launch_bounds__(256) k_residual(DConst c, DMetric m, const dou
             wx[a + b] += c.dxC[a] * c.dxC[b];
             wz[a + b] += c.dzC[a] * c.dzC[b];
         }
-    double v[2] = {0.0, 0.0};
+    double v[2] = {0.0, 0.0}, s1[1] = {0.0};
     if (i < nx && jc <= ny) {
         const size_t row = (size_t)ny * nx;
         const double* pk = phi + (size_t)k * row + (size_t)(jc - 1) * nx;
@@ -408,15 +414,45 @@ __global__ void __launch_bounds__(256) k_residual(DConst c, DMetric m, const dou
         const double s = __ldg(&src[q0]);
         const double res = s - (lx + lz + ly);
         r[q0] = res;
-        v[0] = fabs(res);
+        if (jc == 1) s1[0] = res;
+        else v[0] = fabs(res);
         v[1] = fabs(s);
     }
+    const unsigned nb = gridDim.x * gridDim.y * gridDim.z;
     const int bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
     block_max_store<2>(v, part + (size_t)bid * 2);
-    if (!last_block_arrive(counter, gridDim.x * gridDim.y * gridDim.z)) return;
-    double tot[2];
-    reduce_records<2, true>(part, (int)(gridDim.x * gridDim.y * gridDim.z), tot);
-    if (threadIdx.x == 0 && threadIdx.y == 0) { out[0] = tot[0]; out[1] = tot[1]; }
+    __syncthreads();
+    block_sum_store<1>(s1, part + (size_t)nb * 2 + bid);
+    if (!last_block_arrive(counter, nb)) return;
+    double tot[2], sum[1];
+    reduce_records<2, true>(part, (int)nb, tot);
+    reduce_records<1, false>(part + (size_t)nb * 2, (int)nb, sum);
+    if (threadIdx.x == 0 && threadIdx.y == 0) {
+        out[0] = tot[0];
+        out[1] = tot[1];
+        out[2] = sum[0] / ((double)nx * (double)nz);
+    }
+}
+
+// row 1 of the residual minus its plane mean (the dropped kx = kz = 0
+// equation), and out[0] = max(out[0], max|r| of the corrected row 1)
+__global__ void __launch_bounds__(256) k_resid_row1(DConst c, double* __restrict__ r, double* __restrict__ part,
+                                                    unsigned int* __restrict__ counter, double* __restrict__ out) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int nx = c.nx;
+    double v[1] = {0.0};
+    if (t < nx * c.nz) {
+        const int k = t / nx, i = t - k * nx;
+        double* q = r + (size_t)k * c.ny * nx + i;
+        const double x = *q - out[2];
+        *q = x;
+        v[0] = fabs(x);
+    }
+    block_max_store<1>(v, part + blockIdx.x);
+    if (!last_block_arrive(counter, gridDim.x)) return;
+    double tot[1];
+    reduce_records<1, true>(part, (int)gridDim.x, tot);
+    if (threadIdx.x == 0) out[0] = nmax(out[0], tot[0]);
 }
 
 __global__ void k_store_divsrc(DCoef* coef, const double* __restrict__ v) {
@@ -505,6 +541,7 @@ void launch_cast(cudaStream_t st, size_t n, const float* a, double* b) {
 void launch_residual(cudaStream_t st, const DConst& c, const DMetric& m, const double* src, const double* phi,
                      double* r, double* part, unsigned int* counter, double* out) {
     k_residual<<<cell_grid(c), cell_block(), 0, st>>>(c, m, src, phi, r, part, counter, out);
+    k_resid_row1<<<(c.nx * c.nz + 255) / 256, 256, 0, st>>>(c, r, part, counter, out);
 }
 
 size_t endstep_blocks(const DConst& c) { return (size_t)2 * (c.nsm > 0 ? c.nsm : 148); }

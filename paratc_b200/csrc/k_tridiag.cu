@@ -158,7 +158,10 @@ struct PoisDiag {
 // SetBC_and_UpdateHaloForPrSrc / _scalar give them.
 // ---------------------------------------------------------------------------
 namespace {
-constexpr int HY_U = 8;  // rows per chunk; three chunks in registers, two in flight
+// rows per chunk (three chunks in registers, two in flight): 8, or 4 in the
+// tuner's second variant (DConst::helm_var = 1)
+constexpr int HY_U = 8;
+constexpr int HELM_NVAR = 2;
 __host__ __device__ inline int helm_stride(int ny) { return 3 * (ny + 2); }
 }  // namespace
 
@@ -168,7 +171,7 @@ __host__ __device__ inline int helm_stride(int ny) { return 3 * (ny + 2); }
 // memory; rows are addressed by pointer steps; the wall rows need no case of
 // their own in the sweeps (a(1) = 0, arr(ny+1) = 0, and clcU2Hat's row-1
 // value is substituted before the sweep and its result after it).
-template <class V>
+template <class V, int HU>
 __global__ void __launch_bounds__(128, 4) k_helm(DConst cst, const DCoef* __restrict__ coef, int comp0, FieldSet<V> fl,
                                               const double* __restrict__ duy_ym, const double* __restrict__ uy_ym,
                                               const double* __restrict__ facs) {
@@ -201,29 +204,29 @@ __global__ void __launch_bounds__(128, 4) k_helm(DConst cst, const DCoef* __rest
     // the sweeps run in FP64 whatever the storage: loads convert, stores round
     V* rc = rhs + col;
     V* uc = u + col;
-    const int nch = (ny + HY_U - 1) / HY_U;
+    const int nch = (ny + HU - 1) / HU;
 
     // forward sweep, rows 1..ny: f = ((r + add) - a f_prev) / vecm, written over Rhs
-    double A[HY_U], B[HY_U], C[HY_U];
-    auto ldr = [&](double (&X)[HY_U], int cc) {
+    double A[HU], B[HU], C[HU];
+    auto ldr = [&](double (&X)[HU], int cc) {
         if (cc >= nch) return;
-        const V* b = rc + (size_t)(cc * HY_U + 1) * nx;
-        const int nr = ny - cc * HY_U;
+        const V* b = rc + (size_t)(cc * HU + 1) * nx;
+        const int nr = ny - cc * HU;
 #pragma unroll
-        for (int q = 0; q < HY_U; q++) {
+        for (int q = 0; q < HU; q++) {
             if (q < nr) X[q] = *b;
             b += nx;
         }
     };
     double fp = 0.0;
     V* wp = rc + nx;
-    auto fwd = [&](const double (&X)[HY_U], int cc) {
+    auto fwd = [&](const double (&X)[HU], int cc) {
         if (cc >= nch) return;
-        const int nr = ny - cc * HY_U;
-        const double* sa = SA + cc * HY_U + 1;
-        const double* sr = SR + cc * HY_U + 1;
+        const int nr = ny - cc * HU;
+        const double* sa = SA + cc * HU + 1;
+        const double* sr = SR + cc * HU + 1;
 #pragma unroll
-        for (int q = 0; q < HY_U; q++) {
+        for (int q = 0; q < HU; q++) {
             if (q < nr) {
                 const double f = ((X[q] + add) - sa[q] * fp) * sr[q];
                 *wp = (V)f;
@@ -245,15 +248,15 @@ __global__ void __launch_bounds__(128, 4) k_helm(DConst cst, const DCoef* __rest
         ldr(C, c + 5);
     }
     // backward sweep, rows ny..1: x = f - arr(j+1) x(j+1), u += x
-    double DA[HY_U], DB[HY_U], DC[HY_U], UA[HY_U], UB[HY_U], UC[HY_U];
-    auto ldb = [&](double (&D)[HY_U], double (&U)[HY_U], int cc) {
+    double DA[HU], DB[HU], DC[HU], UA[HU], UB[HU], UC[HU];
+    auto ldb = [&](double (&D)[HU], double (&U)[HU], int cc) {
         if (cc >= nch) return;
-        const size_t off = (size_t)(ny - cc * HY_U) * nx;
+        const size_t off = (size_t)(ny - cc * HU) * nx;
         const V* bd = rc + off;
         const V* bu = uc + off;
-        const int nr = ny - cc * HY_U;
+        const int nr = ny - cc * HU;
 #pragma unroll
-        for (int q = 0; q < HY_U; q++) {
+        for (int q = 0; q < HU; q++) {
             if (q < nr) { D[q] = *bd; U[q] = *bu; }
             bd -= nx;
             bu -= nx;
@@ -261,12 +264,12 @@ __global__ void __launch_bounds__(128, 4) k_helm(DConst cst, const DCoef* __rest
     };
     double xn = 0.0, unew = 0.0, utop = 0.0;
     V* up = uc + (size_t)ny * nx;
-    auto bwd = [&](const double (&D)[HY_U], const double (&U)[HY_U], int cc) {
+    auto bwd = [&](const double (&D)[HU], const double (&U)[HU], int cc) {
         if (cc >= nch) return;
-        const int nr = ny - cc * HY_U;
-        const double* sw = SW + ny + 1 - cc * HY_U;
+        const int nr = ny - cc * HU;
+        const double* sw = SW + ny + 1 - cc * HU;
 #pragma unroll
-        for (int q = 0; q < HY_U; q++) {
+        for (int q = 0; q < HU; q++) {
             if (q < nr) {
                 const double x = D[q] - sw[-q] * xn;
                 xn = x;
@@ -611,6 +614,7 @@ void tridiag_init() {
 int tridiag_part_len(int ny) { return part_len(ny); }
 
 size_t helm_fac_doubles(int ny) { return (size_t)9 * helm_stride(ny); }
+int helm_variants() { return HELM_NVAR; }
 
 // pivots of the Helmholtz matrices of substeps ns0..ns0+nsub-1 for the
 // current dt (coef->dt): one thread per (substep, type) runs the forward
@@ -671,7 +675,12 @@ static void helm_dispatch(cudaStream_t st, const DConst& c, const DCoef* coef, i
                           const FieldSet<V>& f, const double* duy_ym, const double* uy_ym, const double* fac) {
     dim3 blk(32, 4);
     dim3 grd((c.nx + 127) / 128, c.nz, ncomp);
-    launch_pdl(k_helm<V>, grd, blk, helm_stride(c.ny) * sizeof(double), st, c, coef, comp0, f, duy_ym, uy_ym, fac);
+    if (c.helm_var == 1)
+        launch_pdl(k_helm<V, 4>, grd, blk, helm_stride(c.ny) * sizeof(double), st, c, coef, comp0, f, duy_ym, uy_ym,
+                   fac);
+    else
+        launch_pdl(k_helm<V, HY_U>, grd, blk, helm_stride(c.ny) * sizeof(double), st, c, coef, comp0, f, duy_ym,
+                   uy_ym, fac);
 }
 
 void launch_helm(cudaStream_t st, const DConst& c, const DCoef* coef, const Fields& f, const double* duy_ym,

@@ -66,7 +66,9 @@ void launch_endstep(cudaStream_t st, const DConst& c, const DMetric& m, const Fi
 // storage conversions (FP32 storage form)
 void launch_cast(cudaStream_t st, size_t n, const double* a, float* b);
 void launch_cast(cudaStream_t st, size_t n, const float* a, double* b);
-// r = src - L phi (compact arrays) with max|r|, max|src| to out[0..1]; part holds 2 doubles per cell block
+// r = src - L phi (compact arrays) without the pinned kx = kz = 0 equation of
+// row 1, max|r| and max|src| to out[0..1] (out[2] scratch); part holds 3
+// doubles per cell block
 void launch_residual(cudaStream_t st, const DConst& c, const DMetric& m, const double* src, const double* phi,
                      double* r, double* part, unsigned int* counter, double* out);
 // x profile of a padded field averaged over y (dyp weights) and z; part holds nx*nz doubles
@@ -76,14 +78,11 @@ void launch_xprofile(cudaStream_t st, const DConst& c, const DMetric& m, const f
 // k_rhs.cu
 size_t rhs_grid_blocks(const DConst& c);
 void rhs_init();
-// err: the context's error word (bit 8: a row wait of the FP64 copy pipeline gave up; err[1]: the test poll limit)
 void launch_rhs_tile(cudaStream_t st, const DConst& c, const DMetric& m, DCoef* coef, const Fields& f, double* uy_ym,
-                     double* duy_ym, int ns, double gam, double the, double alp, double* part, unsigned int* counter,
-                     unsigned int* err);
+                     double* duy_ym, int ns, double gam, double the, double alp, double* part, unsigned int* counter);
 // FP32 storage form: float fields, FP64 pressure, FP32 arithmetic
 void launch_rhs_tile(cudaStream_t st, const DConst& c, const DMetric& m, DCoef* coef, const Fields32& f, double* uy_ym,
-                     double* duy_ym, int ns, double gam, double the, double alp, double* part, unsigned int* counter,
-                     unsigned int* err);
+                     double* duy_ym, int ns, double gam, double the, double alp, double* part, unsigned int* counter);
 
 // k_tridiag.cu
 int tridiag_partitions(int ny);
@@ -91,6 +90,8 @@ bool tridiag_supported(int ny);
 void tridiag_init();
 int tridiag_part_len(int ny);
 size_t helm_fac_doubles(int ny);
+int helm_variants();  // compiled Helmholtz launch shapes (DConst::helm_var < helm_variants())
+int rhs_variants();   // compiled FP64 right-hand-side launch shapes (DConst::rhs_var < rhs_variants())
 void launch_helm_factors(cudaStream_t st, const DConst& c, const DMetric& m, const DCoef* coef, int ns0, int nsub,
                          const double* alp, double* fac);
 void launch_helm(cudaStream_t st, const DConst& c, const DCoef* coef, const Fields& f, const double* duy_ym,

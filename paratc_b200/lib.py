@@ -12,7 +12,7 @@ import os
 
 import numpy as np
 
-from .abi import (LAYOUT_INTERIOR, SCHED_NCHOICES, VISU, VISU_NAMES, ParatcIoOptions, PARATC_ERR_DIV_LIMIT, PARATC_ERR_VEL_LIMIT, PARATC_OK, ParatcDiag,
+from .abi import (ParatcTuning, LAYOUT_INTERIOR, SCHED_NCHOICES, VISU, VISU_NAMES, ParatcIoOptions, PARATC_ERR_DIV_LIMIT, PARATC_ERR_VEL_LIMIT, PARATC_OK, ParatcDiag,
                   ParatcParams)
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
@@ -37,6 +37,7 @@ EXPORTED = [
     "paratc_io_options_from_namelist", "paratc_visu_quantity_device", "paratc_autotune", "paratc_get_schedule",
     "paratc_set_schedule", "paratc_set_precision", "paratc_get_precision", "paratc_set_wait_limit",
     "paratc_xprofile", "paratc_front_position", "paratc_poisson_refined", "paratc_poisson_refined_async",
+    "paratc_autotune_all", "paratc_get_tuning", "paratc_set_tuning",
 ]
 PROF_NKERNELS = 16
 
@@ -83,6 +84,9 @@ def load(path=None):
     L.paratc_get_precision.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]
     L.paratc_set_wait_limit.argtypes = [ctypes.c_void_p, ctypes.c_longlong]
     L.paratc_xprofile.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp]
+    L.paratc_autotune_all.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_char_p, ctypes.POINTER(ParatcTuning)]
+    L.paratc_get_tuning.argtypes = [ctypes.c_void_p, ctypes.POINTER(ParatcTuning)]
+    L.paratc_set_tuning.argtypes = [ctypes.c_void_p, ctypes.POINTER(ParatcTuning)]
     L.paratc_poisson_refined.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double,
                                          ctypes.c_int, ctypes.POINTER(ctypes.c_int), _dp]
     L.paratc_poisson_refined_async.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
@@ -488,6 +492,25 @@ class ChannelSystem:
         t = np.zeros(SCHED_NCHOICES)
         self._check(self._L.paratc_autotune(self._h, int(nrep), ctypes.byref(ch), _ptr(t)), "paratc_autotune")
         return ch.value, t
+
+    def autotune_all(self, nrep=5, cache_path=None):
+        """Poisson schedule, then the right-hand-side and Helmholtz launch
+        shapes by whole steps; picks cached in cache_path (JSON) when given.
+        Returns the ParatcTuning applied."""
+        t = ParatcTuning()
+        self._check(self._L.paratc_autotune_all(self._h, int(nrep), None if cache_path is None else cache_path.encode(),
+                                                ctypes.byref(t)), "paratc_autotune_all")
+        return t
+
+    @property
+    def tuning(self):
+        t = ParatcTuning()
+        self._check(self._L.paratc_get_tuning(self._h, ctypes.byref(t)), "paratc_get_tuning")
+        return t
+
+    @tuning.setter
+    def tuning(self, t):
+        self._check(self._L.paratc_set_tuning(self._h, ctypes.byref(t)), "paratc_set_tuning")
 
     @property
     def schedule(self):

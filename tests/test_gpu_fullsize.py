@@ -40,6 +40,17 @@ def test_poisson_c2_full_size():
     # linearity: solve(2 src) = 2 solve(src) exactly up to rounding
     phi_2 = g.poisson(2.0 * src)
     assert rel_err(phi_2, 2.0 * phi_g) <= 1e-14
+    # the FP32 solve with FP64 iterative refinement (the configuration's
+    # second form): relative residual <= 1e-12 and the oracle's potential to
+    # 1e-12, like the FP64 solve
+    import torch
+    d_src = torch.from_numpy(src).cuda()
+    d_phi = torch.empty_like(d_src)
+    n, r = g.poisson_refined(d_src.data_ptr(), d_phi.data_ptr(), 1e-12, 4)
+    e = rel_err(d_phi.cpu().numpy(), phi_o)
+    print("C2 refined: %d corrections, relres %.2e, rel err vs oracle %.2e" % (n, r, e))
+    assert r <= 1e-12 and n <= 3
+    assert e <= 1e-12
     g.close()
 
 

@@ -141,33 +141,3 @@ def test_bounded_wait_timeout(schedule):
     h.close()
     o.close()
 
-
-def test_rhs_row_wait_timeout():
-    """The FP64 right-hand side brings its row slabs in by bulk copies onto
-    mbarriers; with the poll limit at zero its first row wait gives up, every
-    CTA drains its copies and stops, and the step returns
-    PARATC_ERR_TIMEOUT.  A fresh context then steps like the oracle."""
-    case = variant("channel")
-    g, f = _ctx(case)
-    g.set_fields(f["ux"], f["uy"], f["uz"], f["p"])
-    g.project()
-    g.set_wait_limit(0)
-    with pytest.raises(ParatcError) as e:
-        g.iterate(1)
-    assert e.value.code == abi.PARATC_ERR_TIMEOUT
-    assert "right-hand side" in str(e.value)
-    g.close()
-    yp = yp_of(case)
-    h = ChannelSystem(case.params, yp)
-    o = ol.Oracle(case.params, yp)
-    for x in (h, o):
-        x.set_fields(f["ux"], f["uy"], f["uz"], f["p"])
-        x.project()
-    h.iterate(1)
-    rc, _ = o.step()
-    assert rc == 0
-    fh, fo = h.get_fields(), o.get_fields()
-    for n in ("ux", "uy", "uz", "p"):
-        assert rel_err(fh[n], fo[n]) <= 1e-10, n
-    h.close()
-    o.close()
