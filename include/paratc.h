@@ -363,8 +363,8 @@ int paratc_set_wait_limit(paratc_ctx* ctx, long long polls);
  * by its rounding (about 1e-7 of |u|/dx), not by the solves.  Switching to or
  * from FP32 converts the state; statistics, spectra, visualisation, restart
  * and get_fields read an FP64 copy refreshed from it.  The FP32 form needs
- * compile-time-length transforms for nxc/2 and nzc (else PARATC_ERR_BAD_ARG)
- * and runs the plane or separate x/z transform kernels of the context's
+ * nxc % 4 == 0 and compile-time-length transforms for nxc/2 and nzc (else
+ * PARATC_ERR_BAD_ARG) and runs the plane or separate x/z transform kernels of the context's
  * schedule (the TMA-fed variants stay FP64). */
 #define PARATC_PREC_FP64  0
 #define PARATC_PREC_MIXED 1

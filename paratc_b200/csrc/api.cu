@@ -333,13 +333,14 @@ void enqueue_poisson_tail32(paratc_ctx* ctx, float* out, int padded) {
 // one solve of the refined standalone Poisson equation: the FP64 array src
 // (compact) through a float2 spectrum into the FP64 potential phi (compact),
 // written (accumulate = 0) or added to it (the corrections)
-void enqueue_solve32(paratc_ctx* ctx, const double* src, double* phi, int accumulate) {
+// (the correction also subtracts *shift, the row-1 plane mean of phi, from phi)
+void enqueue_solve32(paratc_ctx* ctx, const double* src, double* phi, int accumulate, const double* shift) {
     cudaStream_t st = ctx->st;
     if (ctx->plane) {
         { PROF(PK_FFTX_F); launch_plane_f(st, ctx->kc, src, spec32(ctx), ctx->d_twx, ctx->d_postx, ctx->d_twz); }
         { PROF(PK_YSOLVE); launch_ysolve_fac(st, ctx->kc, ctx->dm, spec32(ctx), ctx->d_pfac); }
         { PROF(PK_FFTX_B); launch_plane_b(st, ctx->nx, ctx->ny, ctx->nz, spec32(ctx), phi, ctx->d_twx, ctx->d_postx,
-                                          ctx->d_twz, ctx->hm.normfft, accumulate); }
+                                          ctx->d_twz, ctx->hm.normfft, accumulate, shift); }
         ctx->launches += 3;
         return;
     }
@@ -348,7 +349,7 @@ void enqueue_solve32(paratc_ctx* ctx, const double* src, double* phi, int accumu
     { PROF(PK_YSOLVE); launch_ysolve_fac(st, ctx->kc, ctx->dm, spec32(ctx), ctx->d_pfac); }
     { PROF(PK_FFTZ_B); launch_pfft_z(st, +1, ctx->nx, ctx->ny, ctx->nz, spec32(ctx), ctx->d_twz); }
     { PROF(PK_FFTX_B); launch_pfft_xb(st, ctx->nx, ctx->ny, ctx->nz, spec32(ctx), phi, ctx->d_twx, ctx->d_postx,
-                                      ctx->hm.normfft, accumulate); }
+                                      ctx->hm.normfft, accumulate, shift); }
     ctx->launches += 5;
 }
 
@@ -723,7 +724,7 @@ int paratc_create(const paratc_params* prm, const double* yp, int device, paratc
     // partial-result records of the grid reductions: one per block of k_prsrc /
     // k_cfl, one per block of the RHS and forward-x kernels, 8 per block of the
     // end-of-step kernel
-    ctx->npart = std::max(std::max(3 * cell_grid_blocks(kc), rhs_grid_blocks(kc)),
+    ctx->npart = std::max(std::max(4 * cell_grid_blocks(kc), rhs_grid_blocks(kc)),
                           std::max((size_t)pfft_x_blocks(ctx->nx, ctx->ny, ctx->nz), endstep_blocks(kc) * 8)) + 64;
     if ((rc = dalloc(ctx, &ctx->d_src, ctx->ni)) || (rc = dalloc(ctx, &ctx->d_spec, (size_t)ctx->M1 * ctx->ny * ctx->nz)) ||
         (rc = dalloc(ctx, &ctx->d_part, ctx->npart)) || (rc = dalloc(ctx, &ctx->d_uy_ym, (size_t)ctx->nx * ctx->nz)) ||
@@ -1047,14 +1048,14 @@ int paratc_poisson_refined_async(paratc_ctx* ctx, const double* d_src, double* d
     if (!ctx || !d_src || !d_phi || ncorr < 0 || d_src == d_phi) return PARATC_ERR_BAD_ARG;
     CK(cudaSetDevice(ctx->dev));
     if (!ctx->pfft) return set_err(ctx, PARATC_ERR_BAD_ARG, "the refined solve needs compile-time-length transforms");
-    enqueue_solve32(ctx, d_src, d_phi, 0);
+    enqueue_solve32(ctx, d_src, d_phi, 0, nullptr);
     for (int q = 0; q < ncorr; q++) {
         // r = src - L phi in FP64 (into the context's compact work array), then
         // its FP32-spectrum solve added to phi
         launch_residual(ctx->st, ctx->kc, ctx->dm, d_src, d_phi, ctx->d_src, ctx->d_part, ctx->d_counter + 5,
                         ctx->d_scal + 4);
         ctx->launches += 1;
-        enqueue_solve32(ctx, ctx->d_src, d_phi, 1);
+        enqueue_solve32(ctx, ctx->d_src, d_phi, 1, ctx->d_scal + 7);
     }
     CK(cudaGetLastError());
     return PARATC_OK;
@@ -1065,7 +1066,7 @@ int paratc_poisson_refined(paratc_ctx* ctx, const double* d_src, double* d_phi, 
     if (!ctx || !d_src || !d_phi || max_corr < 0 || d_src == d_phi) return PARATC_ERR_BAD_ARG;
     CK(cudaSetDevice(ctx->dev));
     if (!ctx->pfft) return set_err(ctx, PARATC_ERR_BAD_ARG, "the refined solve needs compile-time-length transforms");
-    enqueue_solve32(ctx, d_src, d_phi, 0);
+    enqueue_solve32(ctx, d_src, d_phi, 0, nullptr);
     int q = 0;
     double rel = 0.0;
     for (;;) {
@@ -1077,7 +1078,7 @@ int paratc_poisson_refined(paratc_ctx* ctx, const double* d_src, double* d_phi, 
         if (rc) return rc;
         rel = ctx->h_scal[4] / std::max(ctx->h_scal[5], 1e-300);
         if (!(rel > rtol) || q >= max_corr) break;
-        enqueue_solve32(ctx, ctx->d_src, d_phi, 1);
+        enqueue_solve32(ctx, ctx->d_src, d_phi, 1, ctx->d_scal + 7);
         q++;
     }
     if (ncorr) *ncorr = q;
@@ -1146,9 +1147,9 @@ int paratc_set_precision(paratc_ctx* ctx, int prec) {
     if (!ctx || (prec != PARATC_PREC_FP64 && prec != PARATC_PREC_MIXED && prec != PARATC_PREC_FP32))
         return PARATC_ERR_BAD_ARG;
     CK(cudaSetDevice(ctx->dev));
-    if (prec == PARATC_PREC_FP32 && !(pfft_x_supported(ctx->nx / 2) && pfft_z_supported(ctx->nz)))
+    if (prec == PARATC_PREC_FP32 && !(pfft_x_supported(ctx->nx / 2) && pfft_z_supported(ctx->nz) && ctx->nx % 4 == 0))
         return set_err(ctx, PARATC_ERR_BAD_ARG,
-                       "the FP32 storage form needs compile-time-length transforms for nxc/2 and nzc");
+                       "the FP32 storage form needs nxc % 4 == 0 and compile-time-length transforms for nxc/2 and nzc");
     if (prec == PARATC_PREC_FP32 && ctx->prec != PARATC_PREC_FP32) {
         int rc = alloc_fp32(ctx);
         if (rc) return rc;

@@ -105,7 +105,8 @@ __global__ void __launch_bounds__(XK<N>::P)
 template <int N, class S, class PH>
 __global__ void __launch_bounds__(XK<N>::P)
     k_xb(int ny, int nz, const S* __restrict__ spec, PH* __restrict__ phi, const double2* __restrict__ twN,
-         const double2* __restrict__ post, double scale, int padded, int accumulate) {
+         const double2* __restrict__ post, double scale, int padded, int accumulate,
+         const double* __restrict__ shift) {
     constexpr int B = XK<N>::B, P = XK<N>::P, PITCH = XK<N>::PITCH, M1 = N + 1;
     constexpr ff::Sched SC = ff::make_sched(N);
     extern __shared__ double2 smx[];
@@ -159,8 +160,10 @@ __global__ void __launch_bounds__(XK<N>::P)
         if (!padded) {
             PH* dst = phi + (size_t)g * nx + 2 * e;
             if (accumulate) {
+                // phi += correction - the row-1 plane mean of phi (the gauge)
                 const double2 o = ld_pair(dst);
-                v = make_double2(o.x + v.x, o.y + v.y);
+                const double sh = shift ? *shift : 0.0;
+                v = make_double2(o.x + v.x - sh, o.y + v.y - sh);
             }
             st_pair(dst, v);
             continue;
@@ -244,13 +247,13 @@ static void pfft_xf_t(cudaStream_t st, int mode, const DConst& c, const DMetric&
 
 template <class S, class PH>
 static void pfft_xb_t(cudaStream_t st, int nx, int ny, int nz, const S* spec, PH* phi, const double2* twx,
-                      const double2* post, double scale, int padded, int accumulate) {
+                      const double2* post, double scale, int padded, int accumulate, const double* shift) {
     const int nrows = ny * nz;
     switch (nx / 2) {
 #define X_CASE(n)                                                                                              \
     case n:                                                                                                    \
         launch_pdl(k_xb<n, S, PH>, dim3((nrows + XK<n>::B - 1) / XK<n>::B), dim3(XK<n>::P), XK<n>::smem, st, ny, \
-                   nz, spec, phi, twx, post, scale, padded, accumulate);                                       \
+                   nz, spec, phi, twx, post, scale, padded, accumulate, shift);                                \
         break;
         PFFT_X_SIZES(X_CASE)
 #undef X_CASE
@@ -266,7 +269,7 @@ void launch_pfft_xf(cudaStream_t st, int mode, const DConst& c, const DMetric& m
 }
 void launch_pfft_xb(cudaStream_t st, int nx, int ny, int nz, const double2* spec, double* phi, const double2* twx,
                     const double2* post, double scale, int padded) {
-    pfft_xb_t(st, nx, ny, nz, spec, phi, twx, post, scale, padded, 0);
+    pfft_xb_t(st, nx, ny, nz, spec, phi, twx, post, scale, padded, 0, nullptr);
 }
 #else
 void launch_pfft_xf(cudaStream_t st, int mode, const DConst& c, const DMetric& m, const DCoef* coef,
@@ -281,11 +284,11 @@ void launch_pfft_xf(cudaStream_t st, const DConst& c, const double* src, float2*
 }
 void launch_pfft_xb(cudaStream_t st, int nx, int ny, int nz, const float2* spec, float* phi, const double2* twx,
                     const double2* post, double scale, int padded) {
-    pfft_xb_t(st, nx, ny, nz, spec, phi, twx, post, scale, padded, 0);
+    pfft_xb_t(st, nx, ny, nz, spec, phi, twx, post, scale, padded, 0, nullptr);
 }
 void launch_pfft_xb(cudaStream_t st, int nx, int ny, int nz, const float2* spec, double* phi, const double2* twx,
-                    const double2* post, double scale, int accumulate) {
-    pfft_xb_t(st, nx, ny, nz, spec, phi, twx, post, scale, 0, accumulate);
+                    const double2* post, double scale, int accumulate, const double* shift) {
+    pfft_xb_t(st, nx, ny, nz, spec, phi, twx, post, scale, 0, accumulate, shift);
 }
 #endif
 

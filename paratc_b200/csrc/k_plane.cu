@@ -161,7 +161,7 @@ template <int M, int NZ, class S, class PH>
 __global__ void __launch_bounds__(PL_P, 1)
     k_plane_b(int ny, const S* __restrict__ spec, PH* __restrict__ phi, const double2* __restrict__ twx,
               const double2* __restrict__ post, const double2* __restrict__ twz, double scale, int padded,
-              int accumulate) {
+              int accumulate, const double* __restrict__ shift) {
     constexpr int M1 = PK<M, NZ>::M1, PITCH = PK<M, NZ>::PITCH;
     constexpr ff::Sched SX = ff::make_sched(M, PL_BITS), SZ = ff::make_sched(NZ, PL_BITS);
     extern __shared__ double2 smp[];
@@ -215,8 +215,10 @@ __global__ void __launch_bounds__(PL_P, 1)
         if (!padded) {
             PH* dst = phi + ((size_t)k * ny + j) * nx + 2 * e;
             if (accumulate) {
+                // phi += correction - the row-1 plane mean of phi (the gauge)
                 const double2 o = ld_pair(dst);
-                v = make_double2(o.x + v.x, o.y + v.y);
+                const double sh = shift ? *shift : 0.0;
+                v = make_double2(o.x + v.x - sh, o.y + v.y - sh);
             }
             st_pair(dst, v);
             continue;
@@ -285,12 +287,13 @@ static void plane_f_t(cudaStream_t st, int mode, const DConst& c, const DMetric&
 
 template <class S, class PH>
 static void plane_b_t(cudaStream_t st, int nx, int ny, int nz, const S* spec, PH* phi, const double2* twx,
-                      const double2* post, const double2* twz, double scale, int padded, int accumulate) {
+                      const double2* post, const double2* twz, double scale, int padded, int accumulate,
+                      const double* shift) {
 #define P_CASE(a, b)                                                                                           \
     if constexpr (PK<a, b>::fits) {                                                                            \
         if (nx / 2 == a && nz == b) {                                                                          \
             launch_pdl(k_plane_b<a, b, S, PH>, dim3(ny), dim3(PL_P), PK<a, b>::smem, st, ny, spec, phi, twx, post, \
-                       twz, scale, padded, accumulate);                                                        \
+                       twz, scale, padded, accumulate, shift);                                                 \
             return;                                                                                            \
         }                                                                                                      \
     }
@@ -306,7 +309,7 @@ void launch_plane_f(cudaStream_t st, int mode, const DConst& c, const DMetric& m
 }
 void launch_plane_b(cudaStream_t st, int nx, int ny, int nz, const double2* spec, double* phi, const double2* twx,
                     const double2* post, const double2* twz, double scale, int padded) {
-    plane_b_t(st, nx, ny, nz, spec, phi, twx, post, twz, scale, padded, 0);
+    plane_b_t(st, nx, ny, nz, spec, phi, twx, post, twz, scale, padded, 0, nullptr);
 }
 #else
 void launch_plane_f(cudaStream_t st, int mode, const DConst& c, const DMetric& m, const DCoef* coef,
@@ -321,11 +324,11 @@ void launch_plane_f(cudaStream_t st, const DConst& c, const double* src, float2*
 }
 void launch_plane_b(cudaStream_t st, int nx, int ny, int nz, const float2* spec, float* phi, const double2* twx,
                     const double2* post, const double2* twz, double scale, int padded) {
-    plane_b_t(st, nx, ny, nz, spec, phi, twx, post, twz, scale, padded, 0);
+    plane_b_t(st, nx, ny, nz, spec, phi, twx, post, twz, scale, padded, 0, nullptr);
 }
 void launch_plane_b(cudaStream_t st, int nx, int ny, int nz, const float2* spec, double* phi, const double2* twx,
-                    const double2* post, const double2* twz, double scale, int accumulate) {
-    plane_b_t(st, nx, ny, nz, spec, phi, twx, post, twz, scale, 0, accumulate);
+                    const double2* post, const double2* twz, double scale, int accumulate, const double* shift) {
+    plane_b_t(st, nx, ny, nz, spec, phi, twx, post, twz, scale, 0, accumulate, shift);
 }
 #endif
 

@@ -79,6 +79,11 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 __device__ __forceinline__ const double* field_of(const Fields& fl, int f) {
     return f == 0 ? fl.ux : f == 1 ? fl.uy : f == 2 ? fl.uz : f == 3 ? fl.pr : fl.sc;
 }
+// the float field f (0 ux, 1 uy, 2 uz, 4 scalar) of the FP32 storage form
+template <class V>
+__device__ __forceinline__ const V* fieldv(const FieldSet<V>& fl, int f) {
+    return f == 0 ? fl.ux : f == 1 ? fl.uy : f == 2 ? fl.uz : fl.sc;
+}
 // one value of field f at offset off, widened to double (the pressure is
 // FP64 in every storage form)
 template <class V>
@@ -110,6 +115,12 @@ __global__ void __launch_bounds__(RhsCfg<T, VAR>::NTHR, RhsCfg<T, VAR>::MINB)
     constexpr int ZC = CFG::ZC, NTHR = CFG::NTHR, NSLOT = CFG::NSLOT, NB = CFG::NB, PF = CFG::PF;
     // FP64 copies: 16-byte pairs, NPAIR per (field, z-plane) row, NP2 per thread and field
     constexpr int NPAIR = SX / 2, NPR = SZ * NPAIR, NP2 = (NPR + NTHR - 1) / NTHR;
+    // FP32 storage: u, v, w (and c) come as 16-byte quads by cp.async (one per
+    // thread and field: SZ * SX / 4 = 140 <= NTHR), the FP64 pressure through
+    // registers, converted; needs nx % 4 == 0 (paratc_set_precision checks)
+    constexpr bool F32S = !F64 && sizeof(V) == 4;
+    constexpr int NQUAD = SZ * (SX / 4);
+    static_assert(!F32S || NQUAD <= NTHR, "one quad per thread and field");
     extern __shared__ __align__(128) unsigned char sm_raw[];
     T* sm = reinterpret_cast<T*>(sm_raw);  // [NB][NF][SLAB]
     __shared__ __align__(128) double smet[NB][ROWMET];
@@ -151,6 +162,16 @@ __global__ void __launch_bounds__(RhsCfg<T, VAR>::NTHR, RhsCfg<T, VAR>::MINB)
         const int j1 = (int)min((long long)ny, (long long)j0 + (gend - g) - 1);
         g += j1 - j0 + 1;
         const int i0 = (tile % ntx) * TX, k0 = (tile / ntx) * TZ;
+        // FP32 storage: the quad this thread copies for every float field
+        size_t gq = 0;
+        int sq = 0;
+        bool vq = false;
+        if constexpr (F32S) {
+            vq = tid < NQUAD;
+            const int zz = tid / (SX / 4), qq = tid - zz * (SX / 4);
+            gq = (size_t)modp(k0 - HZ + zz, nz) * pl + (size_t)modp(i0 - HX + 4 * qq, nx);
+            sq = zz * SX + 4 * qq;
+        }
         // FP32 form: per-thread slab elements, loaded and converted
         size_t goff[F64 ? 1 : NSLOT];
         int soff[F64 ? 1 : NSLOT];
@@ -188,14 +209,20 @@ __global__ void __launch_bounds__(RhsCfg<T, VAR>::NTHR, RhsCfg<T, VAR>::MINB)
                 cp_async16(dst_ + f_ * SLAB + sp[q_], field_of(fl, f_) + gp[q_] + ro_);              \
         if (tid < ROWMET / 2) cp_async16(&smet[(jrow) % NB][2 * tid], m.rowmet + (size_t)(jrow) * ROWMET + 2 * tid); \
     } while (0)
-        // FP32: load, convert, store
+        // FP32: load, convert, store (FP32 storage: the float fields by
+        // cp.async quads, the pressure converted)
 #define LOAD_ROW32(jrow)                                                                 \
     do {                                                                                 \
         T* dst_ = sm + (size_t)((jrow) % NB) * NF * SLAB;                                \
         const size_t ro_ = (size_t)(jrow) * nx;                                          \
-        _Pragma("unroll") for (int f_ = 0; f_ < NF; f_++)                                \
+        _Pragma("unroll") for (int f_ = 0; f_ < NF; f_++) {                              \
+            if (F32S && f_ != 3) {                                                       \
+                if (vq) cp_async16(dst_ + f_ * SLAB + sq, fieldv(fl, f_) + gq + ro_);    \
+                continue;                                                                \
+            }                                                                            \
             _Pragma("unroll") for (int s_ = 0; s_ < NSLOT; s_++) if (sval[s_])           \
                 dst_[f_ * SLAB + soff[s_]] = (T)ld_field(fl, f_, goff[s_] + ro_);           \
+        }                                                                                \
         if (tid < ROWMET) smet[(jrow) % NB][tid] = __ldg(m.rowmet + (size_t)(jrow) * ROWMET + tid); \
     } while (0)
 
@@ -214,6 +241,10 @@ __global__ void __launch_bounds__(RhsCfg<T, VAR>::NTHR, RhsCfg<T, VAR>::MINB)
             LOAD_ROW32(j0 - 1);
             LOAD_ROW32(j0);
             LOAD_ROW32(j0 + 1);
+            if constexpr (F32S) {
+                cp_async_commit();
+                cp_async_wait<0>();
+            }
             __syncthreads();
         }
 
@@ -258,14 +289,24 @@ __global__ void __launch_bounds__(RhsCfg<T, VAR>::NTHR, RhsCfg<T, VAR>::MINB)
                 // which every thread finished at the barrier closing it
                 if (j + 1 + PF <= j1 + 1) LOAD_ROW64(j + 1 + PF);
                 cp_async_commit();
-            } else if (more) {
-                const size_t ro = (size_t)(j + 2) * nx;
+            } else {
+                if (more) {
+                    const size_t ro = (size_t)(j + 2) * nx;
+                    T* dst = sm + (size_t)((j + 2) % NB) * NF * SLAB;
 #pragma unroll
-                for (int f = 0; f < NF; f++)
+                    for (int f = 0; f < NF; f++) {
+                        if (F32S && f != 3) {
+                            // the slot of row j+2 was last read by row j-2's arithmetic
+                            if (vq) cp_async16(dst + f * SLAB + sq, fieldv(fl, f) + gq + ro);
+                            continue;
+                        }
 #pragma unroll
-                    for (int sl = 0; sl < NSLOT; sl++)
-                        pre[f][sl] = sval[sl] ? ld_field(fl, f, goff[sl] + ro) : 0.0;
-                if (tid < ROWMET) mpre = __ldg(m.rowmet + (size_t)(j + 2) * ROWMET + tid);
+                        for (int sl = 0; sl < NSLOT; sl++)
+                            pre[f][sl] = sval[sl] ? ld_field(fl, f, goff[sl] + ro) : 0.0;
+                    }
+                    if (tid < ROWMET) mpre = __ldg(m.rowmet + (size_t)(j + 2) * ROWMET + tid);
+                }
+                if constexpr (F32S) cp_async_commit();  // one group per row, empty or not
             }
             double hx0a[ZC], hy0a[ZC], hz0a[ZC], hc0a[ZC];
             size_t q0a[ZC];
@@ -285,6 +326,9 @@ __global__ void __launch_bounds__(RhsCfg<T, VAR>::NTHR, RhsCfg<T, VAR>::MINB)
                 u64n[cz] = (!F64 && act[cz] && j + 2 <= ny + 1) ? __ldg(&fl.ux[q0a[cz] + 2 * nx]) : 0.0;
             if constexpr (F64) {
                 cp_async_wait<PF>();  // the group holding row j+1 is complete
+                __syncthreads();
+            } else if constexpr (F32S) {
+                cp_async_wait<1>();  // row j+1's quads (the newest group is row j+2's)
                 __syncthreads();
             }
             // both cells are computed before any global store, so that the
@@ -455,10 +499,12 @@ __global__ void __launch_bounds__(RhsCfg<T, VAR>::NTHR, RhsCfg<T, VAR>::MINB)
                 if (more) {
                     T* dst = sm + (size_t)((j + 2) % NB) * NF * SLAB;
 #pragma unroll
-                    for (int f = 0; f < NF; f++)
+                    for (int f = 0; f < NF; f++) {
+                        if (F32S && f != 3) continue;  // copied by cp.async
 #pragma unroll
                         for (int sl = 0; sl < NSLOT; sl++)
                             if (sval[sl]) dst[f * SLAB + soff[sl]] = (T)pre[f][sl];
+                    }
                     if (tid < ROWMET) smet[(j + 2) % NB][tid] = mpre;
                 }
 #pragma unroll

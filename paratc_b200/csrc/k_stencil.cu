@@ -372,9 +372,13 @@ __global__ void k_cast(size_t n, const A* __restrict__ a, B* __restrict__ b) {
 // (src/m_Poisson.f90:399-404); that equation's residual is the plane mean of
 // r at row 1, nonzero whenever the source's dy-weighted mean is, and it is
 // removed (k_resid_row1) so that the corrections see only the equations the
-// solve keeps.  Record per CTA: max|r| over rows 2..ny, max|src|, and the sum
-// of r over its row-1 cells; the last CTA writes out[0] = max|r| (rows
-// 2..ny), out[1] = max|src|, out[2] = the row-1 plane mean.
+// solve keeps.  The same pinned equation fixes the additive constant of phi
+// (the plane mean of phi at row 1 is zero); out[3] receives that mean of the
+// current phi, which the next correction subtracts (a constant is invisible
+// to the residual, and FP32 rounding in the inverse transforms shifts it).
+// Record per CTA: max|r| over rows 2..ny, max|src|, and the sums of r and
+// phi over its row-1 cells; the last CTA writes out[0] = max|r| (rows
+// 2..ny), out[1] = max|src|, out[2], out[3] = the row-1 plane means of r, phi.
 __global__ void __launch_bounds__(256) k_residual(DConst c, DMetric m, const double* __restrict__ src,
                                                   const double* __restrict__ phi, double* __restrict__ r,
                                                   double* __restrict__ part, unsigned int* __restrict__ counter,
@@ -395,7 +399,7 @@ __global__ void __launch_bounds__(256) k_residual(DConst c, DMetric m, const dou
             wx[a + b] += c.dxC[a] * c.dxC[b];
             wz[a + b] += c.dzC[a] * c.dzC[b];
         }
-    double v[2] = {0.0, 0.0}, s1[1] = {0.0};
+    double v[2] = {0.0, 0.0}, s1[2] = {0.0, 0.0};
     if (i < nx && jc <= ny) {
         const size_t row = (size_t)ny * nx;
         const double* pk = phi + (size_t)k * row + (size_t)(jc - 1) * nx;
@@ -414,7 +418,7 @@ __global__ void __launch_bounds__(256) k_residual(DConst c, DMetric m, const dou
         const double s = __ldg(&src[q0]);
         const double res = s - (lx + lz + ly);
         r[q0] = res;
-        if (jc == 1) s1[0] = res;
+        if (jc == 1) { s1[0] = res; s1[1] = pc; }
         else v[0] = fabs(res);
         v[1] = fabs(s);
     }
@@ -422,15 +426,16 @@ __global__ void __launch_bounds__(256) k_residual(DConst c, DMetric m, const dou
     const int bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
     block_max_store<2>(v, part + (size_t)bid * 2);
     __syncthreads();
-    block_sum_store<1>(s1, part + (size_t)nb * 2 + bid);
+    block_sum_store<2>(s1, part + (size_t)nb * 2 + (size_t)bid * 2);
     if (!last_block_arrive(counter, nb)) return;
-    double tot[2], sum[1];
+    double tot[2], sum[2];
     reduce_records<2, true>(part, (int)nb, tot);
-    reduce_records<1, false>(part + (size_t)nb * 2, (int)nb, sum);
+    reduce_records<2, false>(part + (size_t)nb * 2, (int)nb, sum);
     if (threadIdx.x == 0 && threadIdx.y == 0) {
         out[0] = tot[0];
         out[1] = tot[1];
         out[2] = sum[0] / ((double)nx * (double)nz);
+        out[3] = sum[1] / ((double)nx * (double)nz);
     }
 }
 

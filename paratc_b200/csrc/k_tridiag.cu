@@ -230,7 +230,7 @@ __global__ void __launch_bounds__(128, 4) k_helm(DConst cst, const DCoef* __rest
             if (q < nr) {
                 const double f = ((X[q] + add) - sa[q] * fp) * sr[q];
                 *wp = (V)f;
-                fp = (double)(V)f;  // the value the backward sweep will read
+                fp = f;  // the chain stays FP64 (no conversion on the dependent path)
             }
             wp += nx;
         }
@@ -391,20 +391,28 @@ __device__ __forceinline__ void cpa16t(void* sdst, const void* gsrc) {
     const unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gsrc) : "memory");
 }
+__device__ __forceinline__ void cpa8t(void* sdst, const void* gsrc) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gsrc) : "memory");
+}
 constexpr int YS_U = 8;  // rows loaded ahead of the dependent chain
 }  // namespace
 
 // Small grids (one wave): a one-warp CTA stages 16 complex columns of the
 // spectrum and their factors in shared memory with cp.async, then lane l
-// sweeps the real (l even) or imaginary (l odd) part of column l/2.
+// sweeps the real (l even) or imaginary (l odd) part of column l/2.  S: the
+// spectrum's storage (double2, or float2 in the FP32 storage form; the
+// sweeps run in double either way).
+template <class S>
 __global__ void __launch_bounds__(32) k_ys_staged(int ny, int M1, int nz, const double* __restrict__ am2ph,
-                                                  double2* __restrict__ spec, const double* __restrict__ fac) {
+                                                  S* __restrict__ spec, const double* __restrict__ fac) {
+    using R = decltype(S::x);
     extern __shared__ double2 sy[];
     const int lane = threadIdx.x;
     const int NQ = M1 * nz;
     const int q0 = blockIdx.x * 16;
     const int nv = min(16, NQ - q0);
-    double2* sd = sy;                                          // [ny][16] spectrum
+    S* sd = reinterpret_cast<S*>(sy);                          // [ny][16] spectrum
     double* srv = reinterpret_cast<double*>(sy + ny * 16);     // [ny][16] 1/vecm
     double* sar = srv + ny * 16;                               // [ny][16] arr
     double* sa = sar + ny * 16;                                // am2ph[0..ny]
@@ -417,7 +425,7 @@ __global__ void __launch_bounds__(32) k_ys_staged(int ny, int M1, int nz, const 
     const bool cval = cq < nv;
     const int qq = q0 + (cval ? cq : 0);
     const int kz = qq / M1, kx = qq - kz * M1;
-    double2* scol = spec + (size_t)kz * ny * M1 + kx;
+    S* scol = spec + (size_t)kz * ny * M1 + kx;
     const char* gsrc;
     char* sdst;
     size_t gstride;
@@ -425,9 +433,9 @@ __global__ void __launch_bounds__(32) k_ys_staged(int ny, int M1, int nz, const 
     bool cvalid;
     if (lane < 16) {
         gsrc = reinterpret_cast<const char*>(scol);
-        gstride = (size_t)M1 * sizeof(double2);
+        gstride = (size_t)M1 * sizeof(S);
         sdst = reinterpret_cast<char*>(sd + lane);
-        sstride = 16 * sizeof(double2);
+        sstride = 16 * sizeof(S);
         cvalid = cval;
     } else {
         const int pr = (lane & 7) * 2;
@@ -438,13 +446,17 @@ __global__ void __launch_bounds__(32) k_ys_staged(int ny, int M1, int nz, const 
         sstride = 16 * sizeof(double);
         cvalid = pr < nv;
     }
-    if (cvalid)
-        for (int j = 0; j < ny; j++) cpa16t(sdst + (size_t)j * sstride, gsrc + (size_t)j * gstride);
+    if (cvalid) {
+        if (lane < 16 && sizeof(S) == 8)
+            for (int j = 0; j < ny; j++) cpa8t(sdst + (size_t)j * sstride, gsrc + (size_t)j * gstride);
+        else
+            for (int j = 0; j < ny; j++) cpa16t(sdst + (size_t)j * sstride, gsrc + (size_t)j * gstride);
+    }
     for (int j = lane; j <= ny; j += 32) sa[j] = __ldg(&am2ph[j]);
     asm volatile("cp.async.commit_group;\n" ::: "memory");
     asm volatile("cp.async.wait_group 0;\n" ::: "memory");
     __syncthreads();
-    double* sdd = reinterpret_cast<double*>(sd);
+    R* sdd = reinterpret_cast<R*>(sd);
     const int cp = lane >> 1;  // complex column of this lane's real or imaginary part
     const bool dc = (q0 + cp) == 0;
     double fp = 0.0;
@@ -454,7 +466,7 @@ __global__ void __launch_bounds__(32) k_ys_staged(int ny, int M1, int nz, const 
         for (int u = 0; u < YS_U; u++) {
             const int j = j0 + u;
             if (j < ny) {
-                d[u] = sdd[j * 32 + lane];
+                d[u] = (double)sdd[j * 32 + lane];
                 rv[u] = srv[j * 16 + cp];
                 a[u] = sa[j + 1];
             }
@@ -464,7 +476,7 @@ __global__ void __launch_bounds__(32) k_ys_staged(int ny, int M1, int nz, const 
             const int j = j0 + u;
             if (j < ny) {
                 const double f = (j == 0) ? (dc ? 0.0 : d[u]) * rv[u] : (d[u] - a[u] * fp) * rv[u];
-                sdd[j * 32 + lane] = f;
+                sdd[j * 32 + lane] = (R)f;
                 fp = f;
             }
         }
@@ -476,7 +488,7 @@ __global__ void __launch_bounds__(32) k_ys_staged(int ny, int M1, int nz, const 
         for (int u = 0; u < YS_U; u++) {
             const int j = j0 - u;
             if (j >= 0) {
-                d[u] = sdd[j * 32 + lane];
+                d[u] = (double)sdd[j * 32 + lane];
                 ar[u] = sar[(j + 1) * 16 + cp];
             }
         }
@@ -485,7 +497,7 @@ __global__ void __launch_bounds__(32) k_ys_staged(int ny, int M1, int nz, const 
             const int j = j0 - u;
             if (j >= 0) {
                 const double x = d[u] - ar[u] * xn;
-                sdd[j * 32 + lane] = x;
+                sdd[j * 32 + lane] = (R)x;
                 xn = x;
             }
         }
@@ -530,7 +542,7 @@ __global__ void __launch_bounds__(128) k_ys_global(int ny, int M1, int nz, const
             if (j < ny) {
                 const double f = (j == 0) ? (dc ? 0.0 : d[u]) * rv[u] : (d[u] - a[u] * fp) * rv[u];
                 col[(size_t)j * W] = (R)f;
-                fp = (double)(R)f;  // the value the backward sweep reads
+                fp = f;  // the chain stays FP64 (no conversion on the dependent path)
             }
         }
     }
@@ -562,26 +574,31 @@ void launch_pois_factors(cudaStream_t st, const DConst& c, const DMetric& m, dou
     k_pois_factors<<<(NQ + 127) / 128, 128, 0, st>>>(c.ny, M1, c.nz, m, fac, fac + (size_t)NQ * c.ny);
 }
 
+// the staged kernel's shared memory: the spectrum block (16 B per complex
+// value, whatever the storage, so that the factor arrays stay 16-byte
+// aligned), the two factor blocks and am2ph
 static size_t ys_staged_smem(int ny) { return (size_t)ny * 16 * 2 * sizeof(double2) + (size_t)(ny + 1) * sizeof(double); }
 
-void launch_ysolve_fac(cudaStream_t st, const DConst& c, const DMetric& m, double2* spec, const double* fac) {
+template <class S>
+static void ysolve_fac_t(cudaStream_t st, const DConst& c, const DMetric& m, S* spec, const double* fac) {
+    using R = decltype(S::x);
     const int M1 = c.nx / 2 + 1, NQ = M1 * c.nz;
     const size_t sm = ys_staged_smem(c.ny);
     const int per_sm = sm > 0 ? (int)((220 * 1024) / sm) : 0;
     const int ctas = (NQ + 15) / 16;
     if (per_sm >= 1 && (c.solver_sel == 1 || (c.solver_sel == 0 && ctas <= per_sm * c.nsm))) {
-        launch_pdl(k_ys_staged, dim3(ctas), dim3(32), sm, st, c.ny, M1, c.nz, m.am2ph, spec, fac);
+        launch_pdl(k_ys_staged<S>, dim3(ctas), dim3(32), sm, st, c.ny, M1, c.nz, m.am2ph, spec, fac);
     } else {
         const int n = 2 * M1 * c.nz;
-        launch_pdl(k_ys_global<double>, dim3((n + 127) / 128), dim3(128), 0, st, c.ny, M1, c.nz, m.am2ph,
-                   reinterpret_cast<double*>(spec), fac);
+        launch_pdl(k_ys_global<R>, dim3((n + 127) / 128), dim3(128), 0, st, c.ny, M1, c.nz, m.am2ph,
+                   reinterpret_cast<R*>(spec), fac);
     }
 }
-
+void launch_ysolve_fac(cudaStream_t st, const DConst& c, const DMetric& m, double2* spec, const double* fac) {
+    ysolve_fac_t(st, c, m, spec, fac);
+}
 void launch_ysolve_fac(cudaStream_t st, const DConst& c, const DMetric& m, float2* spec, const double* fac) {
-    const int M1 = c.nx / 2 + 1, n = 2 * M1 * c.nz;
-    launch_pdl(k_ys_global<float>, dim3((n + 127) / 128), dim3(128), 0, st, c.ny, M1, c.nz, m.am2ph,
-               reinterpret_cast<float*>(spec), fac);
+    ysolve_fac_t(st, c, m, spec, fac);
 }
 
 // ---------------------------------------------------------------------------
@@ -607,7 +624,8 @@ void tridiag_init() {
     cudaFuncSetAttribute(k_ysolve<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
     cudaFuncSetAttribute(k_ysolve<12>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
     cudaFuncSetAttribute(k_ysolve<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
-    cudaFuncSetAttribute(k_ys_staged, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
+    cudaFuncSetAttribute(k_ys_staged<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
+    cudaFuncSetAttribute(k_ys_staged<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
     cudaFuncSetAttribute(k_helm_factors, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
 }
 

@@ -67,8 +67,8 @@ void launch_endstep(cudaStream_t st, const DConst& c, const DMetric& m, const Fi
 void launch_cast(cudaStream_t st, size_t n, const double* a, float* b);
 void launch_cast(cudaStream_t st, size_t n, const float* a, double* b);
 // r = src - L phi (compact arrays) without the pinned kx = kz = 0 equation of
-// row 1, max|r| and max|src| to out[0..1] (out[2] scratch); part holds 3
-// doubles per cell block
+// row 1, max|r| and max|src| to out[0..1], the row-1 plane means of r and phi
+// to out[2..3]; part holds 4 doubles per cell block
 void launch_residual(cudaStream_t st, const DConst& c, const DMetric& m, const double* src, const double* phi,
                      double* r, double* part, unsigned int* counter, double* out);
 // x profile of a padded field averaged over y (dyp weights) and z; part holds nx*nz doubles
@@ -171,7 +171,7 @@ void launch_plane_f(cudaStream_t st, const DConst& c, const double* src, float2*
 void launch_plane_b(cudaStream_t st, int nx, int ny, int nz, const float2* spec, float* phi, const double2* twx,
                     const double2* post, const double2* twz, double scale, int padded);
 void launch_plane_b(cudaStream_t st, int nx, int ny, int nz, const float2* spec, double* phi, const double2* twx,
-                    const double2* post, const double2* twz, double scale, int accumulate);
+                    const double2* post, const double2* twz, double scale, int accumulate, const double* shift);
 
 // k_pfft_x.cu / k_pfft_z.cu: compile-time-length transforms of the Poisson solve
 bool pfft_x_supported(int n);
@@ -198,7 +198,7 @@ void launch_pfft_z(cudaStream_t st, int dir, int nx, int ny, int nz, float2* spe
 void launch_pfft_xf(cudaStream_t st, const DConst& c, const double* src, float2* spec, const double2* twx,
                     const double2* post);
 void launch_pfft_xb(cudaStream_t st, int nx, int ny, int nz, const float2* spec, double* phi, const double2* twx,
-                    const double2* post, double scale, int accumulate);
+                    const double2* post, double scale, int accumulate, const double* shift);
 
 // k_fft.cu
 void fft_init();
