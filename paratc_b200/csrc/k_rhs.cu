@@ -251,9 +251,10 @@ __global__ void __launch_bounds__(RhsCfg<T, VAR>::NTHR, RhsCfg<T, VAR>::MINB)
         const int i = i0 + lane;
         int kk[ZC];
         bool act[ZC];
-        // explicit histories of the next row are loaded one row ahead
-        double hxn[ZC], hyn[ZC], hzn[ZC], hcn[ZC];
-        double u64m[ZC], u64c[ZC], u64p[ZC];  // FP32 form: FP64 ux of the own column, rows j-1, j, j+1
+        // explicit histories of the next row are loaded one row ahead, held
+        // in their storage type (widened where used, so the loads stay in flight)
+        V hxn[ZC], hyn[ZC], hzn[ZC], hcn[ZC];
+        V u64m[ZC], u64c[ZC], u64p[ZC];  // FP32 forms: ux of the own column, rows j-1, j, j+1
 #pragma unroll
         for (int cz = 0; cz < ZC; cz++) {
             kk[cz] = k0 + wq * ZC + cz;
@@ -308,7 +309,7 @@ __global__ void __launch_bounds__(RhsCfg<T, VAR>::NTHR, RhsCfg<T, VAR>::MINB)
                 }
                 if constexpr (F32S) cp_async_commit();  // one group per row, empty or not
             }
-            double hx0a[ZC], hy0a[ZC], hz0a[ZC], hc0a[ZC];
+            V hx0a[ZC], hy0a[ZC], hz0a[ZC], hc0a[ZC];
             size_t q0a[ZC];
 #pragma unroll
             for (int cz = 0; cz < ZC; cz++) {
@@ -320,10 +321,10 @@ __global__ void __launch_bounds__(RhsCfg<T, VAR>::NTHR, RhsCfg<T, VAR>::MINB)
                 }
             }
             // FP32 form: ux of row j+2 for the next row's s3tot term, one row ahead
-            double u64n[ZC];
+            V u64n[ZC];
 #pragma unroll
             for (int cz = 0; cz < ZC; cz++)
-                u64n[cz] = (!F64 && act[cz] && j + 2 <= ny + 1) ? __ldg(&fl.ux[q0a[cz] + 2 * nx]) : 0.0;
+                u64n[cz] = (!F64 && act[cz] && j + 2 <= ny + 1) ? __ldg(&fl.ux[q0a[cz] + 2 * nx]) : (V)0;
             if constexpr (F64) {
                 cp_async_wait<PF>();  // the group holding row j+1 is complete
                 __syncthreads();

@@ -159,7 +159,7 @@ struct PoisDiag {
 // ---------------------------------------------------------------------------
 namespace {
 // rows per chunk (three chunks in registers, two in flight): 8, or 4 in the
-// tuner's second variant (DConst::helm_var = 1)
+// tuner's second variant (DConst::helm_var = 1); twice that for float storage
 constexpr int HY_U = 8;
 constexpr int HELM_NVAR = 2;
 __host__ __device__ inline int helm_stride(int ny) { return 3 * (ny + 2); }
@@ -207,8 +207,11 @@ __global__ void __launch_bounds__(128, 4) k_helm(DConst cst, const DCoef* __rest
     const int nch = (ny + HU - 1) / HU;
 
     // forward sweep, rows 1..ny: f = ((r + add) - a f_prev) / vecm, written over Rhs
-    double A[HU], B[HU], C[HU];
-    auto ldr = [&](double (&X)[HU], int cc) {
+    const double a0 = (comp == 1) ? duy_ym[(size_t)k * nx + i] : 0.0;
+    // the register ring holds rows in their storage type and widens them
+    // where they are used, so that the loads of later chunks stay in flight
+    V A[HU], B[HU], C[HU];
+    auto ldr = [&](V (&X)[HU], int cc) {
         if (cc >= nch) return;
         const V* b = rc + (size_t)(cc * HU + 1) * nx;
         const int nr = ny - cc * HU;
@@ -220,7 +223,7 @@ __global__ void __launch_bounds__(128, 4) k_helm(DConst cst, const DCoef* __rest
     };
     double fp = 0.0;
     V* wp = rc + nx;
-    auto fwd = [&](const double (&X)[HU], int cc) {
+    auto fwd = [&](const V (&X)[HU], int cc) {
         if (cc >= nch) return;
         const int nr = ny - cc * HU;
         const double* sa = SA + cc * HU + 1;
@@ -228,7 +231,9 @@ __global__ void __launch_bounds__(128, 4) k_helm(DConst cst, const DCoef* __rest
 #pragma unroll
         for (int q = 0; q < HU; q++) {
             if (q < nr) {
-                const double f = ((X[q] + add) - sa[q] * fp) * sr[q];
+                // clcU2Hat: the row-1 value is the wall increment (kept in FP64)
+                const double xq = (comp == 1 && cc == 0 && q == 0) ? a0 : (double)X[q];
+                const double f = ((xq + add) - sa[q] * fp) * sr[q];
                 *wp = (V)f;
                 fp = f;  // the chain stays FP64 (no conversion on the dependent path)
             }
@@ -236,7 +241,6 @@ __global__ void __launch_bounds__(128, 4) k_helm(DConst cst, const DCoef* __rest
         }
     };
     ldr(A, 0);
-    if (comp == 1) A[0] = duy_ym[(size_t)k * nx + i];  // clcU2Hat: the row-1 value is the wall increment
     ldr(B, 1);
     ldr(C, 2);
     for (int c = 0; c < nch; c += 3) {
@@ -248,8 +252,8 @@ __global__ void __launch_bounds__(128, 4) k_helm(DConst cst, const DCoef* __rest
         ldr(C, c + 5);
     }
     // backward sweep, rows ny..1: x = f - arr(j+1) x(j+1), u += x
-    double DA[HU], DB[HU], DC[HU], UA[HU], UB[HU], UC[HU];
-    auto ldb = [&](double (&D)[HU], double (&U)[HU], int cc) {
+    V DA[HU], DB[HU], DC[HU], UA[HU], UB[HU], UC[HU];
+    auto ldb = [&](V (&D)[HU], V (&U)[HU], int cc) {
         if (cc >= nch) return;
         const size_t off = (size_t)(ny - cc * HU) * nx;
         const V* bd = rc + off;
@@ -264,16 +268,16 @@ __global__ void __launch_bounds__(128, 4) k_helm(DConst cst, const DCoef* __rest
     };
     double xn = 0.0, unew = 0.0, utop = 0.0;
     V* up = uc + (size_t)ny * nx;
-    auto bwd = [&](const double (&D)[HU], const double (&U)[HU], int cc) {
+    auto bwd = [&](const V (&D)[HU], const V (&U)[HU], int cc) {
         if (cc >= nch) return;
         const int nr = ny - cc * HU;
         const double* sw = SW + ny + 1 - cc * HU;
 #pragma unroll
         for (int q = 0; q < HU; q++) {
             if (q < nr) {
-                const double x = D[q] - sw[-q] * xn;
+                const double x = (double)D[q] - sw[-q] * xn;
                 xn = x;
-                unew = U[q] + x;
+                unew = (double)U[q] + x;
                 *up = (V)unew;
             }
             up -= nx;
@@ -284,7 +288,7 @@ __global__ void __launch_bounds__(128, 4) k_helm(DConst cst, const DCoef* __rest
     ldb(DC, UC, 2);
     for (int c = 0; c < nch; c += 3) {
         bwd(DA, UA, c);
-        if (c == 0) utop = DA[0] + UA[0];  // u(ny): x(ny) = f(ny)
+        if (c == 0) utop = (double)DA[0] + (double)UA[0];  // u(ny): x(ny) = f(ny)
         ldb(DA, UA, c + 3);
         bwd(DB, UB, c + 1);
         ldb(DB, UB, c + 4);
@@ -526,7 +530,8 @@ __global__ void __launch_bounds__(128) k_ys_global(int ny, int M1, int nz, const
     const bool dc = (q == 0);
     double fp = 0.0;
     for (int j0 = 0; j0 < ny; j0 += YS_U) {
-        double d[YS_U], rv[YS_U], a[YS_U];
+        R d[YS_U];  // in the storage type: widened at use, so the loads stay in flight
+        double rv[YS_U], a[YS_U];
 #pragma unroll
         for (int u = 0; u < YS_U; u++) {
             const int j = j0 + u;
@@ -540,7 +545,8 @@ __global__ void __launch_bounds__(128) k_ys_global(int ny, int M1, int nz, const
         for (int u = 0; u < YS_U; u++) {
             const int j = j0 + u;
             if (j < ny) {
-                const double f = (j == 0) ? (dc ? 0.0 : d[u]) * rv[u] : (d[u] - a[u] * fp) * rv[u];
+                const double du = (double)d[u];
+                const double f = (j == 0) ? (dc ? 0.0 : du) * rv[u] : (du - a[u] * fp) * rv[u];
                 col[(size_t)j * W] = (R)f;
                 fp = f;  // the chain stays FP64 (no conversion on the dependent path)
             }
@@ -548,7 +554,8 @@ __global__ void __launch_bounds__(128) k_ys_global(int ny, int M1, int nz, const
     }
     double xn = fp;
     for (int j0 = ny - 2; j0 >= 0; j0 -= YS_U) {
-        double d[YS_U], ar[YS_U];
+        R d[YS_U];
+        double ar[YS_U];
 #pragma unroll
         for (int u = 0; u < YS_U; u++) {
             const int j = j0 - u;
@@ -561,7 +568,7 @@ __global__ void __launch_bounds__(128) k_ys_global(int ny, int M1, int nz, const
         for (int u = 0; u < YS_U; u++) {
             const int j = j0 - u;
             if (j >= 0) {
-                const double x = d[u] - ar[u] * xn;
+                const double x = (double)d[u] - ar[u] * xn;
                 col[(size_t)j * W] = (R)x;
                 xn = x;
             }
@@ -693,11 +700,14 @@ static void helm_dispatch(cudaStream_t st, const DConst& c, const DCoef* coef, i
                           const FieldSet<V>& f, const double* duy_ym, const double* uy_ym, const double* fac) {
     dim3 blk(32, 4);
     dim3 grd((c.nx + 127) / 128, c.nz, ncomp);
+    // rows per chunk: FP64 8 (variant 1: 4); float storage, whose ring takes
+    // half the registers, 16 (variant 1: 8)
+    constexpr int H0 = sizeof(V) == 4 ? 2 * HY_U : HY_U;
     if (c.helm_var == 1)
-        launch_pdl(k_helm<V, 4>, grd, blk, helm_stride(c.ny) * sizeof(double), st, c, coef, comp0, f, duy_ym, uy_ym,
-                   fac);
+        launch_pdl(k_helm<V, H0 / 2>, grd, blk, helm_stride(c.ny) * sizeof(double), st, c, coef, comp0, f, duy_ym,
+                   uy_ym, fac);
     else
-        launch_pdl(k_helm<V, HY_U>, grd, blk, helm_stride(c.ny) * sizeof(double), st, c, coef, comp0, f, duy_ym,
+        launch_pdl(k_helm<V, H0>, grd, blk, helm_stride(c.ny) * sizeof(double), st, c, coef, comp0, f, duy_ym,
                    uy_ym, fac);
 }
 
