@@ -91,15 +91,19 @@ def _traffic_table():
     return out
 
 
-def algorithmic_bytes(params):
-    """Compulsory HBM bytes per launch of each kernel class (FP64 words of 8 B,
-    N cells; spectral arrays hold (nx/2+1)*ny*nz complex values)."""
+def algorithmic_bytes(params, precision="fp64"):
+    """Compulsory HBM bytes per launch of each kernel class (N cells; spectral
+    arrays hold (nx/2+1)*ny*nz complex values, S doubles).  FP64 and mixed
+    forms: 8-byte words.  FP32 storage form: 4-byte velocity, scalar,
+    histories, right-hand sides, potential and spectrum; the pressure stays
+    8 bytes."""
     N = params.nxc * params.nyc * params.nzc
     S = 2 * (params.nxc // 2 + 1) * params.nyc * params.nzc  # doubles in the spectral array
     sc = 1 if params.scalar_on else 0
-    w = 8
+    w = 4 if precision == "fp32" else 8
+    wp = 8  # the pressure
     return {
-        "rhs": (7 + 6 + 4 * sc) * w * N,          # u,v,w,p,H* in; Rhs*,H* out
+        "rhs": (12 + 4 * sc) * w * N + wp * N,    # u,v,w,p,H* in; Rhs*,H* out
         "helmholtz": 9 * w * N,                   # Rhs*, u* in; u* out
         "helmholtz_scalar": 3 * w * N,
         "prsrc": w * (3 * N + S),                 # u,v,w in; x spectrum out (source fused into the x transform)
@@ -108,7 +112,7 @@ def algorithmic_bytes(params):
         "ysolve": 2 * w * S,
         "fft_z_bwd": 2 * w * S,
         "fft_x_bwd": w * (S + N),
-        "project": 9 * w * N,                     # phi,u,v,w,p in; u,v,w,p out
+        "project": 7 * w * N + 2 * wp * N,        # phi,u,v,w,p in; u,v,w,p out
         "cfl": 3 * w * N,
         "check": (3 + sc) * w * N,
     }
@@ -411,12 +415,13 @@ def run_ours(args):
 
     # roofline of the dominant kernel
     peak, peak_kind = _peaks()
-    alg = algorithmic_bytes(p)
+    alg = algorithmic_bytes(p, args.precision)
     dom = max(prof.items(), key=lambda kv: kv[1][0])
     kname, (kms, kn) = dom
     avg_s = kms / kn / 1e3
     ach = alg[kname] / avg_s / 1e9
-    traffic = _traffic_table().get((args.workload, kname))
+    tkey = ("fp32_" + kname) if args.precision == "fp32" else kname
+    traffic = _traffic_table().get((args.workload, tkey))
     share = {k: round(v[0] / sum(x[0] for x in prof.values()), 4) for k, v in sorted(prof.items(), key=lambda kv: -kv[1][0])}
     roof = {"bound": "hbm", "kernel": kname, "achieved": round(ach, 1), "peak": peak, "unit": "GB/s",
             "frac": round(ach / peak, 4), "traffic": traffic, "peak_kind": peak_kind,
