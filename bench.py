@@ -52,6 +52,9 @@ def _args():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--schedule", type=int, default=-1,
                     help="pin a Poisson schedule (0-11, paratc_set_schedule) instead of auto-tuning it")
+    ap.add_argument("--batch-mode", choices=["grouped", "streams"], default="grouped",
+                    help="ensemble_c4: one launch per kernel instantiation over the members (grouped) or "
+                         "every member's own launches on its own stream")
     ap.add_argument("--precision", choices=["fp64", "mixed", "fp32"], default="fp64",
                     help="mixed: the explicit right-hand side in FP32 arithmetic, all else FP64; "
                          "fp32: FP32 storage of everything but the pressure")
@@ -407,11 +410,17 @@ def run_ours(args):
             forms[form] = {"value": v2, "ms_per_step": ms2 / args.steps, "speedup_vs_fp64": v2 / value,
                            "divmax_last_step": d2.divmax, "field_rel_err_vs_fp64_path": err}
             c2.close()
-        ens = ensemble_measure(args, local, dist, "fp64", steps=max(3, args.steps // 2))
-        ens.pop("_batch").close()
-        ens.pop("_cases")
-        ens["speedup_vs_fp64_single"] = ens["value"] / value
-        forms["batched_c4"] = ens
+        # the C4 ensemble: member launches on member streams, and grouped
+        # launches in FP64 and in the FP32 storage form
+        for key, prec, mode in (("batched_c4_streams", "fp64", "streams"), ("batched_c4", "fp64", "grouped"),
+                                ("batched_c4_fp32", "fp32", "grouped")):
+            ens = ensemble_measure(args, local, dist, prec, steps=max(3, args.steps // 2), mode=mode)
+            ens.pop("_batch").close()
+            ens.pop("_cases")
+            ens.pop("clocks", None)
+            ens["speedup_vs_fp64_single"] = ens["value"] / value
+            forms[key] = ens
+        forms["batched_c4"]["speedup_vs_streams"] = forms["batched_c4"]["value"] / forms["batched_c4_streams"]["value"]
 
     # roofline of the dominant kernel
     peak, peak_kind = _peaks()
@@ -451,14 +460,17 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
-def ensemble_measure(args, local, dist, precision, steps=None):
+def ensemble_measure(args, local, dist, precision, steps=None, mode="grouped"):
     """The C4 ensemble: 32 channel instances of uneven grids and Re_tau
     advanced together by the batch API, every step-round one CUDA graph
     launch (device time of `steps` steps, max over ranks); and the same
-    instances stepped one after another, each alone on the GPU.  The
-    ensemble's working set (several GB) exceeds the L2, so no flush is needed
-    between timed steps.  Returns the measurement as a dict (with the batch
-    and its cases under "_batch" and "_cases" for the caller to close)."""
+    instances stepped one after another, each alone on the GPU.  mode
+    "grouped": one launch per kernel instantiation and stage over all members
+    (paratc_batch_set_mode); "streams": every member's own launches on its
+    own stream.  The ensemble's working set (several GB) exceeds the L2, so
+    no flush is needed between timed steps.  Returns the measurement as a
+    dict (with the batch and its cases under "_batch" and "_cases" for the
+    caller to close)."""
     import torch
     from paratc_b200 import cases, replicas
     from paratc_b200.lib import BatchSystem, mesh_ycoord
@@ -474,6 +486,7 @@ def ensemble_measure(args, local, dist, precision, steps=None):
         m.project()
         m.precision = precision
         cells += c.params.nxc * c.params.nyc * c.params.nzc
+    b.mode = mode
     stream = torch.cuda.ExternalStream(b.stream, device=local)
     b.iterate(args.warmup)
     torch.cuda.synchronize()
@@ -504,7 +517,7 @@ def ensemble_measure(args, local, dist, precision, steps=None):
     seq_ms = replicas.max_over_ranks(seq_ms, dist, device=local)
     seq_value = ws * cells * 3 * steps / (seq_ms / 1e3)
     return {"value": value, "unit": UNIT, "ms_per_step": ms / steps, "steps": steps, "cells": cells,
-            "precision": precision, "graph_kernels_per_step": b.graph_kernels,
+            "precision": precision, "mode": mode, "graph_kernels_per_step": b.graph_kernels,
             "divmax_last_step_max": max(d.divmax for d in diags),
             "sequential": {"value": seq_value, "ms_per_step": seq_ms / steps,
                            "note": "the same 32 instances stepped one after another, each alone on the GPU"},
@@ -520,7 +533,7 @@ def run_ensemble(args):
     torch.cuda.set_device(local)
     from paratc_b200 import replicas
     dist = replicas.init("nccl")
-    r = ensemble_measure(args, local, dist, args.precision)
+    r = ensemble_measure(args, local, dist, args.precision, mode=args.batch_mode)
     b = r.pop("_batch")
     cs = r.pop("_cases")
     cells = r["cells"]
@@ -560,7 +573,8 @@ def run_ensemble(args):
                 "data": "synthetic",
                 "config": {"workload": "ensemble_c4: 32 channels, (nx,nz) in {64,96,128,192}, ny in {48,64,96,128}, "
                                        "Re_tau U[120,395], seed 2024",
-                           "cells": cells, "precision": args.precision, "parallelism": "ensemble in one CUDA graph x%d" % ws,
+                           "cells": cells, "precision": args.precision, "batch_mode": args.batch_mode,
+                           "parallelism": "ensemble in one CUDA graph x%d" % ws,
                            "l2": "working set %.1f GB > L2, no flush" % (cells * 17 * 8 / 1e9),
                            "graph_kernels_per_step": r["graph_kernels_per_step"],
                            "divmax_last_step_max": r["divmax_last_step_max"]},

@@ -569,6 +569,31 @@ int paratc_batch_member(paratc_batch* b, int i, paratc_ctx** ctx);
 int paratc_batch_steps(paratc_batch* b, int nsteps, int use_graph, paratc_diag* diag);
 /* Kernels one graph launch of the batch runs (0 before the first capture). */
 int64_t paratc_batch_graph_kernels(paratc_batch* b);
+/* How a batch step launches its kernels.
+ * PARATC_BATCH_STREAMS (the default): every member enqueues its own step on
+ * its own stream, one kernel per stage and member (the members' kernels run
+ * concurrently).
+ * PARATC_BATCH_GROUPED: every stage of the step is ONE launch per kernel
+ * instantiation over all members that share it, on the batch's stream: each
+ * member's CTAs run that member's launch shape on its own fields, reading
+ * its arguments from a device table (so a member computes exactly what its
+ * own launches compute).  Members sharing precision, scalar flag and launch
+ * shapes share the right-hand side, Helmholtz, y-solve, projection and
+ * end-of-step launches; the x transforms are grouped by nxc, the z
+ * transforms by nzc.  The batch sets every member's Poisson schedule to the
+ * separate compile-time-length transforms (paratc_set_schedule choice 2 or
+ * 3, keeping the y-solve kind); a member without them (nxc/2 or nzc not a
+ * compiled length) makes the call fail with PARATC_ERR_BAD_ARG.  The tables
+ * are rebuilt when a member's schedule, precision or launch shapes change.
+ * Both modes take the ordinary step first where a member is not steady
+ * (see above), and capture the rest in one graph with use_graph != 0. */
+#define PARATC_BATCH_STREAMS 0
+#define PARATC_BATCH_GROUPED 1
+int paratc_batch_set_mode(paratc_batch* b, int mode);
+int paratc_batch_get_mode(paratc_batch* b, int* mode);
+/* Kernel launches of one steady step of the batch in its mode (grouped: the
+ * plan's launches; streams: the last captured graph's kernels, 0 before). */
+int64_t paratc_batch_step_launches(paratc_batch* b);
 /* The stream the batch's graph is launched on (cudaStream_t); work queued on
  * it before paratc_batch_steps precedes the steps, work queued after them
  * follows them. */

@@ -25,6 +25,10 @@ LAYOUT_HALO = 1
 # Poisson schedule choices (PARATC_SCHED_NCHOICES of include/paratc.h)
 SCHED_NCHOICES = 12
 
+# launch modes of an ensemble (PARATC_BATCH_*)
+BATCH_STREAMS = 0
+BATCH_GROUPED = 1
+
 # dump_visu quantities (PARATC_VISU_*)
 VISU_NAMES = ("ux", "uy", "uz", "pr", "wx", "wy", "wz", "wMag", "Q", "lamda2", "scalar")
 VISU = {n: q for q, n in enumerate(VISU_NAMES)}

@@ -14,8 +14,12 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <functional>
+#include <map>
+#include <memory>
 #include <mutex>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "../../include/paratc.h"
@@ -1844,6 +1848,32 @@ int paratc_dump_visu(paratc_ctx* ctx, const char* res_dir, const char* run_name,
 // ---------------------------------------------------------------------------
 // ensembles
 // ---------------------------------------------------------------------------
+namespace {
+
+// one launch of a grouped step
+struct GrpLaunch {
+    std::function<void(cudaStream_t)> run;
+};
+
+// the grouped form of a step: every stage is one launch per kernel
+// instantiation over the members that share it (GrpTab, kernels.cuh)
+struct GrpPlan {
+    std::vector<void*> dev;                   // device tables
+    std::vector<paratc_ctx*> fac;             // members whose Helmholtz pivots change every step (iCFL = 1)
+    std::vector<std::vector<GrpLaunch>> sub;  // the launches of substep ns at index ns - 1
+    std::vector<GrpLaunch> end;               // end of step
+    std::vector<int> gens;                    // the members' sched_gen the tables were built from
+    int64_t kernels = 0;                      // launches per step
+    bool built = false;
+};
+
+void grp_free(GrpPlan& P) {
+    for (void* d : P.dev) cudaFree(d);
+    P = GrpPlan();
+}
+
+}  // namespace
+
 struct paratc_batch {
     int n = 0, dev = 0;
     std::vector<paratc_ctx*> m;
@@ -1854,6 +1884,8 @@ struct paratc_batch {
     std::vector<int> gens;              // the members' sched_gen when the graph was captured
     bool graph_failed = false;
     int64_t graph_kernels = 0;
+    int mode = PARATC_BATCH_STREAMS;    // PARATC_BATCH_STREAMS or PARATC_BATCH_GROUPED
+    GrpPlan plan;                       // the grouped launches (PARATC_BATCH_GROUPED)
     std::string err;
 };
 
@@ -1890,19 +1922,269 @@ cudaError_t batch_fork_members(paratc_batch* b) {
     return cudaSuccess;
 }
 
+// ---- grouped launches -------------------------------------------------------
+
+// the members gathered for one kernel instantiation
+template <class E>
+struct GrpAcc {
+    DConst key{};  // a member's constants: the launcher picks the instantiation from them
+    std::vector<E> e;
+    std::vector<dim3> g;
+    size_t smem = 0;  // the largest member's dynamic shared memory
+    void add(const DConst& k, const E& x, dim3 grid, size_t sm = 0) {
+        if ((size_t)grid.x * grid.y * grid.z == 0) return;  // nothing to do for this member
+        if (e.empty()) key = k;
+        e.push_back(x);
+        g.push_back(grid);
+        smem = std::max(smem, sm);
+    }
+};
+
+// the tables of one instantiation on the device, PT_MAXMEM members each,
+// with the CTA count of each
+template <class E>
+bool grp_upload(GrpPlan& P, const GrpAcc<E>& a, std::vector<std::pair<const GrpTab<E>*, int>>& out) {
+    for (size_t s0 = 0; s0 < a.e.size(); s0 += PT_MAXMEM) {
+        const int n = (int)std::min<size_t>(PT_MAXMEM, a.e.size() - s0);
+        std::unique_ptr<GrpTab<E>> h(new GrpTab<E>());
+        h->nmem = n;
+        long long blk = 0;
+        for (int i = 0; i < n; i++) {
+            const dim3 g = a.g[s0 + i];
+            h->b0[i] = (int)blk;
+            h->g[i][0] = g.x;
+            h->g[i][1] = g.y;
+            h->g[i][2] = g.z;
+            h->e[i] = a.e[s0 + i];
+            blk += (long long)g.x * g.y * g.z;
+        }
+        if (blk > 0x7fffffffLL) return false;
+        h->b0[n] = (int)blk;
+        void* d = nullptr;
+        if (cudaMalloc(&d, sizeof(GrpTab<E>)) != cudaSuccess) return false;
+        P.dev.push_back(d);
+        if (cudaMemcpy(d, h.get(), sizeof(GrpTab<E>), cudaMemcpyHostToDevice) != cudaSuccess) return false;
+        out.push_back({static_cast<const GrpTab<E>*>(d), (int)blk});
+    }
+    return true;
+}
+
+// one launch per table of every instantiation in m, in key order
+template <class K, class E, class F>
+bool grp_emit(GrpPlan& P, std::map<K, GrpAcc<E>>& m, std::vector<GrpLaunch>& out, F launch) {
+    for (auto& kv : m) {
+        std::vector<std::pair<const GrpTab<E>*, int>> tabs;
+        if (!grp_upload(P, kv.second, tabs)) return false;
+        const K key = kv.first;
+        const DConst kc = kv.second.key;
+        const size_t smem = kv.second.smem;
+        for (auto& t : tabs) {
+            const GrpTab<E>* tab = t.first;
+            const int nblk = t.second;
+            out.push_back({[=](cudaStream_t st) { launch(st, key, kc, tab, nblk, smem); }});
+        }
+    }
+    return true;
+}
+
+// the Poisson schedule of the grouped step: the separate compile-time-length
+// x and z transforms with register-fed z passes (choice 2 or 3, the y-solve
+// kind kept), the form every member of a table shares
+bool grp_schedule(paratc_ctx* c) {
+    const int y = c->kc.solver_sel == 2 ? 1 : 0;
+    const bool ok = c->pfft && !c->plane && !c->ztma && !c->xdiv;
+    if (ok) return true;
+    if (!sched_supported(c, 2 + y)) return false;
+    sched_apply(c, 2 + y);
+    return true;
+}
+
+// the grouped form of the k_xb launch: the plain kernel (no bulk copies)
+int grp_build(paratc_batch* b) {
+    grp_free(b->plan);
+    GrpPlan& P = b->plan;
+    for (auto* c : b->m)
+        if (!grp_schedule(c)) {
+            b->err = "grouped batch: a member has no compile-time-length transforms for nxc/2 and nzc";
+            return PARATC_ERR_BAD_ARG;
+        }
+    int maxiad = 0;
+    for (auto* c : b->m) maxiad = std::max(maxiad, c->hm.iadvance);
+    P.sub.assign(maxiad, {});
+    using K4 = std::tuple<int, int, int, int>;
+    bool ok = true;
+    for (int ns = 1; ns <= maxiad && ok; ns++) {
+        std::map<K4, GrpAcc<RhsArgs<double>>> rhs64;
+        std::map<int, GrpAcc<RhsArgs<float>>> rhs32;
+        std::map<int, GrpAcc<HelmArgs<double>>> hs64, h64;
+        std::map<int, GrpAcc<HelmArgs<float>>> hs32, h32;
+        std::map<int, GrpAcc<XfArgs<double, double2>>> xf64;
+        std::map<int, GrpAcc<XfArgs<float, float2>>> xf32;
+        std::map<int, GrpAcc<ZtArgs<double2>>> zt64;
+        std::map<int, GrpAcc<ZtArgs<float2>>> zt32;
+        std::map<int, GrpAcc<YsArgs<double2>>> ys64;
+        std::map<int, GrpAcc<YsArgs<float2>>> ys32;
+        std::map<int, GrpAcc<XbArgs<double2, double>>> xb64;
+        std::map<int, GrpAcc<XbArgs<float2, float>>> xb32;
+        std::map<int, GrpAcc<ProjArgs<double>>> pj64;
+        std::map<int, GrpAcc<ProjArgs<float>>> pj32;
+        for (auto* c : b->m) {
+            if (c->hm.iadvance < ns) continue;
+            const DConst& k = c->kc;
+            const HostMetrics& h = c->hm;
+            const int M1 = c->nx / 2 + 1, kind = ys_kind(k);
+            const double gam = h.gam[ns - 1], the = h.the[ns - 1], alp = h.alp[ns - 1];
+            if (c->prec == PARATC_PREC_FP32) {
+                float2* sp = spec32(c);
+                rhs32[k.scalar_on].add(k, RhsArgs<float>{k, c->dm, c->d_coef, c->f32, c->d_uy_ym, c->d_duy_ym, gam,
+                                                          the, alp, c->d_part, c->d_counter},
+                                       rhs_member_grid(k, 1));
+                if (c->prm.scalar_on)
+                    hs32[k.helm_var].add(k, HelmArgs<float>{k, c->d_coef, c->f32, nullptr, nullptr, c->d_hfac, 3},
+                                         helm_member_grid(k, 1), helm_smem(k));
+                h32[k.helm_var].add(k, HelmArgs<float>{k, c->d_coef, c->f32, c->d_duy_ym, c->d_uy_ym, c->d_hfac, 0},
+                                    helm_member_grid(k, 3), helm_smem(k));
+                xf32[c->nx].add(k, XfArgs<float, float2>{k, c->dm, c->d_coef, c->f32.ux, c->f32.uy, c->f32.uz, sp,
+                                                         c->d_twx, c->d_postx, c->d_part, c->d_counter + 1,
+                                                         &c->d_coef->divmax_src},
+                                pfft_x_member_grid(k));
+                zt32[c->nz].add(k, ZtArgs<float2>{c->ny * M1, sp, c->d_twz}, pfft_z_member_grid(k));
+                ys32[kind].add(k, YsArgs<float2>{c->ny, M1, c->nz, c->dm.am2ph, sp, c->d_pfac},
+                               ys_member_grid(k, kind), ys_smem(k, kind));
+                xb32[c->nx].add(k, XbArgs<float2, float>{c->ny, c->nz, sp, c->d_phi32, c->d_twx, c->d_postx,
+                                                         h.normfft},
+                                pfft_x_member_grid(k));
+                pj32[0].add(k, ProjArgs<float>{k, c->dm, c->d_coef, c->d_phi32, c->f32.ux, c->f32.uy, c->f32.uz,
+                                               c->f32.pr, c->d_uy_ym},
+                            cell_member_grid(k));
+            } else {
+                double2* sp = c->d_spec;
+                rhs64[K4(k.scalar_on, k.fp32_rhs, k.fp32_rhs ? 0 : k.rhs_var, 0)].add(
+                    k, RhsArgs<double>{k, c->dm, c->d_coef, c->f, c->d_uy_ym, c->d_duy_ym, gam, the, alp, c->d_part,
+                                       c->d_counter},
+                    rhs_member_grid(k, k.fp32_rhs));
+                if (c->prm.scalar_on)
+                    hs64[k.helm_var].add(k, HelmArgs<double>{k, c->d_coef, c->f, nullptr, nullptr, c->d_hfac, 3},
+                                         helm_member_grid(k, 1), helm_smem(k));
+                h64[k.helm_var].add(k, HelmArgs<double>{k, c->d_coef, c->f, c->d_duy_ym, c->d_uy_ym, c->d_hfac, 0},
+                                    helm_member_grid(k, 3), helm_smem(k));
+                xf64[c->nx].add(k, XfArgs<double, double2>{k, c->dm, c->d_coef, c->f.ux, c->f.uy, c->f.uz, sp,
+                                                           c->d_twx, c->d_postx, c->d_part, c->d_counter + 1,
+                                                           &c->d_coef->divmax_src},
+                                pfft_x_member_grid(k));
+                zt64[c->nz].add(k, ZtArgs<double2>{c->ny * M1, sp, c->d_twz}, pfft_z_member_grid(k));
+                ys64[kind].add(k, YsArgs<double2>{c->ny, M1, c->nz, c->dm.am2ph, sp, c->d_pfac},
+                               ys_member_grid(k, kind), ys_smem(k, kind));
+                xb64[c->nx].add(k, XbArgs<double2, double>{c->ny, c->nz, sp, c->d_phi, c->d_twx, c->d_postx,
+                                                           h.normfft},
+                                pfft_x_member_grid(k));
+                pj64[0].add(k, ProjArgs<double>{k, c->dm, c->d_coef, c->d_phi, c->f.ux, c->f.uy, c->f.uz, c->f.pr,
+                                                c->d_uy_ym},
+                            cell_member_grid(k));
+            }
+        }
+        std::vector<GrpLaunch>& L = P.sub[ns - 1];
+        const int nsv = ns;
+        auto rhs = [nsv](cudaStream_t st, auto, const DConst& kc, auto tab, int nblk, size_t) {
+            launch_rhs_grp(st, kc, tab, nblk, nsv);
+        };
+        auto helm = [](cudaStream_t st, int, const DConst& kc, auto tab, int nblk, size_t sm) {
+            launch_helm_grp(st, kc, tab, nblk, sm);
+        };
+        auto xf = [](cudaStream_t st, int nx, const DConst&, auto tab, int nblk, size_t) { launch_xf_grp(st, nx, tab, nblk); };
+        auto ztf = [](cudaStream_t st, int nz, const DConst&, auto tab, int nblk, size_t) {
+            launch_zt_grp(st, -1, nz, tab, nblk);
+        };
+        auto ztb = [](cudaStream_t st, int nz, const DConst&, auto tab, int nblk, size_t) {
+            launch_zt_grp(st, 1, nz, tab, nblk);
+        };
+        auto ys = [](cudaStream_t st, int kind, const DConst&, auto tab, int nblk, size_t sm) {
+            launch_ys_grp(st, kind, tab, nblk, sm);
+        };
+        auto xb = [](cudaStream_t st, int nx, const DConst&, auto tab, int nblk, size_t) { launch_xb_grp(st, nx, tab, nblk); };
+        auto pj = [](cudaStream_t st, int, const DConst&, auto tab, int nblk, size_t) { launch_project_grp(st, tab, nblk); };
+        // the substep's stages in the order of enqueue_substep, each stage's
+        // instantiations one after another
+        ok = ok && grp_emit(P, rhs64, L, rhs) && grp_emit(P, rhs32, L, rhs);
+        ok = ok && grp_emit(P, hs64, L, helm) && grp_emit(P, hs32, L, helm);
+        ok = ok && grp_emit(P, h64, L, helm) && grp_emit(P, h32, L, helm);
+        ok = ok && grp_emit(P, xf64, L, xf) && grp_emit(P, xf32, L, xf);
+        ok = ok && grp_emit(P, zt64, L, ztf) && grp_emit(P, zt32, L, ztf);
+        ok = ok && grp_emit(P, ys64, L, ys) && grp_emit(P, ys32, L, ys);
+        ok = ok && grp_emit(P, zt64, L, ztb) && grp_emit(P, zt32, L, ztb);
+        ok = ok && grp_emit(P, xb64, L, xb) && grp_emit(P, xb32, L, xb);
+        ok = ok && grp_emit(P, pj64, L, pj) && grp_emit(P, pj32, L, pj);
+        P.kernels += (int64_t)L.size();
+    }
+    if (ok) {
+        std::map<int, GrpAcc<EndArgs<double>>> e64;
+        std::map<int, GrpAcc<EndArgs<float>>> e32;
+        for (auto* c : b->m) {
+            const DConst& k = c->kc;
+            if (c->prec == PARATC_PREC_FP32)
+                e32[0].add(k, EndArgs<float>{k, c->dm, c->f32.ux, c->f32.uy, c->f32.uz, c->f32.sc, c->d_coef,
+                                             c->d_diag, c->d_part, c->d_counter + 3},
+                           endstep_member_grid(k));
+            else
+                e64[0].add(k, EndArgs<double>{k, c->dm, c->f.ux, c->f.uy, c->f.uz, c->f.sc, c->d_coef, c->d_diag,
+                                              c->d_part, c->d_counter + 3},
+                           endstep_member_grid(k));
+            if (c->prm.icfl == 1) P.fac.push_back(c);
+        }
+        auto es = [](cudaStream_t st, int, const DConst&, auto tab, int nblk, size_t) { launch_endstep_grp(st, tab, nblk); };
+        ok = grp_emit(P, e64, P.end, es) && grp_emit(P, e32, P.end, es);
+        P.kernels += (int64_t)P.end.size() + (int64_t)P.fac.size();
+    }
+    if (!ok) {
+        grp_free(b->plan);
+        b->err = "grouped batch: could not build the launch tables";
+        return PARATC_ERR_CUDA;
+    }
+    for (auto* c : b->m) P.gens.push_back(c->sched_gen);
+    P.built = true;
+    return PARATC_OK;
+}
+
+// the plan is current: built from the members' present schedules and forms
+bool grp_current(const paratc_batch* b) {
+    if (!b->plan.built) return false;
+    for (int i = 0; i < b->n; i++)
+        if (b->m[i]->sched_gen != b->plan.gens[i]) return false;
+    return true;
+}
+
+// one grouped step of every member on b->st (every member steady)
+void grp_enqueue_step(paratc_batch* b) {
+    cudaStream_t st = b->st;
+    for (auto* c : b->plan.fac)
+        launch_helm_factors(st, c->kc, c->dm, c->d_coef, 1, c->hm.iadvance, c->hm.alp, c->d_hfac);
+    for (auto& v : b->plan.sub)
+        for (auto& l : v) l.run(st);
+    for (auto& l : b->plan.end) l.run(st);
+    for (auto* c : b->m) {
+        c->next_ready = true;
+        c->launches += b->plan.kernels / b->n;
+    }
+}
+
 int batch_capture(paratc_batch* b) {
     cudaGraph_t g = nullptr;
     int64_t l0 = 0;
     for (auto* c : b->m) l0 += c->launches;
     cudaError_t e = cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess) return (int)e;
-    bool ok = cudaEventRecord(b->fork, b->st) == cudaSuccess;
-    for (int i = 0; ok && i < b->n; i++) {
-        paratc_ctx* c = b->m[i];
-        ok = cudaStreamWaitEvent(c->st, b->fork, 0) == cudaSuccess;
-        if (ok) enqueue_step(c);
-        ok = ok && cudaEventRecord(b->join[i], c->st) == cudaSuccess;
-        ok = ok && cudaStreamWaitEvent(b->st, b->join[i], 0) == cudaSuccess;
+    bool ok = true;
+    if (b->mode == PARATC_BATCH_GROUPED) {
+        grp_enqueue_step(b);  // every launch on b->st
+    } else {
+        ok = cudaEventRecord(b->fork, b->st) == cudaSuccess;
+        for (int i = 0; ok && i < b->n; i++) {
+            paratc_ctx* c = b->m[i];
+            ok = cudaStreamWaitEvent(c->st, b->fork, 0) == cudaSuccess;
+            if (ok) enqueue_step(c);
+            ok = ok && cudaEventRecord(b->join[i], c->st) == cudaSuccess;
+            ok = ok && cudaStreamWaitEvent(b->st, b->join[i], 0) == cudaSuccess;
+        }
     }
     e = cudaStreamEndCapture(b->st, &g);
     if (!ok || e != cudaSuccess || !g) {
@@ -1919,7 +2201,7 @@ int batch_capture(paratc_batch* b) {
     }
     int64_t l1 = 0;
     for (auto* c : b->m) l1 += c->launches;
-    b->graph_kernels = l1 - l0;
+    b->graph_kernels = b->mode == PARATC_BATCH_GROUPED ? b->plan.kernels : l1 - l0;
     b->gens.clear();
     for (auto* c : b->m) b->gens.push_back(c->sched_gen);
     return 0;
@@ -1963,6 +2245,7 @@ int paratc_batch_destroy(paratc_batch* b) {
     if (!b) return PARATC_OK;
     if (b->st) cudaStreamSynchronize(b->st);
     batch_free_graph(b);
+    grp_free(b->plan);
     for (cudaEvent_t e : b->join)
         if (e) cudaEventDestroy(e);
     if (b->fork) cudaEventDestroy(b->fork);
@@ -1981,6 +2264,37 @@ int paratc_batch_member(paratc_batch* b, int i, paratc_ctx** ctx) {
 
 int64_t paratc_batch_graph_kernels(paratc_batch* b) { return b ? b->graph_kernels : 0; }
 
+int paratc_batch_set_mode(paratc_batch* b, int mode) {
+    if (!b || (mode != PARATC_BATCH_STREAMS && mode != PARATC_BATCH_GROUPED)) return PARATC_ERR_BAD_ARG;
+    if (cudaSetDevice(b->dev) != cudaSuccess) return PARATC_ERR_CUDA;
+    if (cudaStreamSynchronize(b->st) != cudaSuccess) return PARATC_ERR_CUDA;  // no graph of the old mode in flight
+    batch_free_graph(b);
+    b->graph_failed = false;
+    b->graph_kernels = 0;
+    grp_free(b->plan);
+    b->mode = mode;
+    if (mode == PARATC_BATCH_GROUPED) {
+        const int rc = grp_build(b);
+        if (rc != PARATC_OK) {
+            b->mode = PARATC_BATCH_STREAMS;
+            return rc;
+        }
+    }
+    return PARATC_OK;
+}
+
+int paratc_batch_get_mode(paratc_batch* b, int* mode) {
+    if (!b || !mode) return PARATC_ERR_BAD_ARG;
+    *mode = b->mode;
+    return PARATC_OK;
+}
+
+int64_t paratc_batch_step_launches(paratc_batch* b) {
+    if (!b) return 0;
+    if (b->mode == PARATC_BATCH_GROUPED) return b->plan.built ? b->plan.kernels : 0;
+    return b->graph_kernels;
+}
+
 void* paratc_batch_stream(paratc_batch* b) { return b ? (void*)b->st : nullptr; }
 
 int paratc_batch_steps(paratc_batch* b, int nsteps, int use_graph, paratc_diag* diag) {
@@ -1993,12 +2307,43 @@ int paratc_batch_steps(paratc_batch* b, int nsteps, int use_graph, paratc_diag* 
     }
     int s = 0;
     const bool graph = use_graph && !b->graph_failed;
+    if (b->mode == PARATC_BATCH_GROUPED && !grp_current(b)) {
+        // a member changed its schedule, form or launch shapes: new tables
+        batch_free_graph(b);
+        const int rc = grp_build(b);
+        if (rc != PARATC_OK) return rc;
+    }
     if (graph && b->exec) {
         // a member re-tuned since the capture: the graph holds its old kernels
         for (int i = 0; i < b->n; i++)
             if (b->m[i]->sched_gen != b->gens[i]) { batch_free_graph(b); break; }
     }
-    if (graph) {
+    if (b->mode == PARATC_BATCH_GROUPED) {
+        // the grouped launches need every member in the steady state: a member
+        // that is not takes one ordinary step first (all of them, in step)
+        bool steady = true;
+        for (auto* c : b->m) steady = steady && member_steady(c);
+        if (!steady) {
+            for (auto* c : b->m) enqueue_step(c);
+            s++;
+        }
+        if (s < nsteps) {
+            if (batch_join_members(b) != cudaSuccess) return PARATC_ERR_CUDA;
+            if (graph && !b->exec && batch_capture(b) != 0) {
+                b->graph_failed = true;
+                batch_free_graph(b);
+            }
+            for (; s < nsteps; s++) {
+                if (b->exec) {
+                    if (cudaGraphLaunch(b->exec, b->st) != cudaSuccess) return PARATC_ERR_CUDA;
+                    for (auto* c : b->m) c->launches += b->graph_kernels / b->n;
+                } else {
+                    grp_enqueue_step(b);
+                }
+            }
+            if (batch_fork_members(b) != cudaSuccess) return PARATC_ERR_CUDA;
+        }
+    } else if (graph) {
         bool steady = true;
         for (auto* c : b->m) steady = steady && member_steady(c);
         if (!steady) {

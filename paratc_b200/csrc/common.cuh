@@ -95,6 +95,58 @@ __device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.lau
 
 __device__ __forceinline__ int wrapi(int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); }
 
+// The block a CTA works as.  OwnGrid: its own launch (blockIdx, gridDim).
+// SubGrid: its block within one member's launch shape inside a grouped
+// launch over the members of an ensemble (every member keeps the block
+// counts of its own launch, so its reductions see the same partial records).
+struct OwnGrid {
+    __device__ __forceinline__ unsigned x() const { return blockIdx.x; }
+    __device__ __forceinline__ unsigned y() const { return blockIdx.y; }
+    __device__ __forceinline__ unsigned z() const { return blockIdx.z; }
+    __device__ __forceinline__ unsigned gx() const { return gridDim.x; }
+    __device__ __forceinline__ unsigned gy() const { return gridDim.y; }
+    __device__ __forceinline__ unsigned gz() const { return gridDim.z; }
+};
+struct SubGrid {
+    unsigned bx, by, bz, nx, ny, nz;
+    __device__ __forceinline__ unsigned x() const { return bx; }
+    __device__ __forceinline__ unsigned y() const { return by; }
+    __device__ __forceinline__ unsigned z() const { return bz; }
+    __device__ __forceinline__ unsigned gx() const { return nx; }
+    __device__ __forceinline__ unsigned gy() const { return ny; }
+    __device__ __forceinline__ unsigned gz() const { return nz; }
+};
+
+// a grouped launch's table: member i owns blocks [b0[i], b0[i+1]) of a
+// one-dimensional grid and launches with shape (gx, gy, gz) of its own
+constexpr int PT_MAXMEM = 64;
+template <class E>
+struct GrpTab {
+    int nmem;
+    int b0[PT_MAXMEM + 1];
+    unsigned g[PT_MAXMEM][3];
+    E e[PT_MAXMEM];
+};
+// the member of this CTA, and its block in the member's launch shape
+template <class E>
+__device__ __forceinline__ int grp_member(const GrpTab<E>* __restrict__ t, SubGrid& sg) {
+    int lo = 0, hi = t->nmem - 1;
+    const int b = (int)blockIdx.x;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (t->b0[mid] <= b) lo = mid;
+        else hi = mid - 1;
+    }
+    const unsigned l = (unsigned)(b - t->b0[lo]);
+    sg.nx = t->g[lo][0];
+    sg.ny = t->g[lo][1];
+    sg.nz = t->g[lo][2];
+    sg.bx = l % sg.nx;
+    sg.by = (l / sg.nx) % sg.ny;
+    sg.bz = l / (sg.nx * sg.ny);
+    return lo;
+}
+
 // maximum that keeps a NaN: fmax(x, NaN) returns x, so a field that is NaN
 // everywhere would report a maximum of 0 and pass every guard; with nmax a
 // NaN anywhere reaches the grid-wide result (the non-finite guard's input)

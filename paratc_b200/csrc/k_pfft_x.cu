@@ -47,12 +47,15 @@ struct XK {
 
 // V: storage of the velocity (mode 0/1), S: storage of the spectrum; the
 // given source of mode 2 is FP64
-template <int N, class V, class S>
-__global__ void __launch_bounds__(XK<N>::P)
-    k_xf(int mode, DConst c, DMetric m, const DCoef* __restrict__ coef, const V* __restrict__ ux,
-         const V* __restrict__ uy, const V* __restrict__ uz, const double* __restrict__ src,
-         S* __restrict__ spec, const double2* __restrict__ twN, const double2* __restrict__ post,
-         double* __restrict__ part, unsigned int* __restrict__ counter, double* __restrict__ out_max) {
+// G: the block this CTA works as (OwnGrid, or SubGrid in a grouped launch)
+template <int N, class V, class S, class G>
+__device__ __forceinline__ void xf_body(const G& grid, int mode, const DConst& c, const DMetric& m,
+                                        const DCoef* __restrict__ coef, const V* __restrict__ ux,
+                                        const V* __restrict__ uy, const V* __restrict__ uz,
+                                        const double* __restrict__ src, S* __restrict__ spec,
+                                        const double2* __restrict__ twN, const double2* __restrict__ post,
+                                        double* __restrict__ part, unsigned int* __restrict__ counter,
+                                        double* __restrict__ out_max) {
     constexpr int B = XK<N>::B, P = XK<N>::P, PITCH = XK<N>::PITCH, M1 = N + 1;
     constexpr ff::Sched SC = ff::make_sched(N);
     extern __shared__ double2 smx[];
@@ -60,7 +63,7 @@ __global__ void __launch_bounds__(XK<N>::P)
     double2* tws = smx + (N + 1) * PITCH;
     const int tid = threadIdx.x;
     const int nx = 2 * N, nrows = c.ny * c.nz;
-    const int g0 = blockIdx.x * B;
+    const int g0 = grid.x() * B;
     for (int t = tid; t < N; t += P) tws[t] = twN[t];
     pdl_wait();
     pdl_trigger();
@@ -92,21 +95,38 @@ __global__ void __launch_bounds__(XK<N>::P)
     }
     if (mode == 2) return;
     double v[1] = {dm};
-    const unsigned int nblocks = gridDim.x;
-    block_max_store<1>(v, part + blockIdx.x);
+    const unsigned int nblocks = grid.gx();
+    block_max_store<1>(v, part + grid.x());
     if (!last_block_arrive(counter, nblocks)) return;
     double tot[1];
     reduce_records<1, true>(part, (int)nblocks, tot);
     if (tid == 0) *out_max = tot[0];
 }
 
+template <int N, class V, class S>
+__global__ void __launch_bounds__(XK<N>::P)
+    k_xf(int mode, DConst c, DMetric m, const DCoef* __restrict__ coef, const V* __restrict__ ux,
+         const V* __restrict__ uy, const V* __restrict__ uz, const double* __restrict__ src,
+         S* __restrict__ spec, const double2* __restrict__ twN, const double2* __restrict__ post,
+         double* __restrict__ part, unsigned int* __restrict__ counter, double* __restrict__ out_max) {
+    xf_body<N>(OwnGrid{}, mode, c, m, coef, ux, uy, uz, src, spec, twN, post, part, counter, out_max);
+}
+
+template <int N, class V, class S>
+__global__ void __launch_bounds__(XK<N>::P) k_xf_grp(const GrpTab<XfArgs<V, S>>* __restrict__ t) {
+    SubGrid g;
+    const XfArgs<V, S>& a = t->e[grp_member(t, g)];
+    xf_body<N>(g, 0, a.c, a.m, a.coef, a.ux, a.uy, a.uz, (const double*)nullptr, a.spec, a.tw, a.post, a.part,
+               a.counter, a.out_max);
+}
+
 // S: storage of the spectrum, P: of the potential; accumulate != 0 adds the
 // result to phi (unpadded rows: the corrections of the refined solve)
-template <int N, class S, class PH>
-__global__ void __launch_bounds__(XK<N>::P)
-    k_xb(int ny, int nz, const S* __restrict__ spec, PH* __restrict__ phi, const double2* __restrict__ twN,
-         const double2* __restrict__ post, double scale, int padded, int accumulate,
-         const double* __restrict__ shift) {
+template <int N, class S, class PH, class G>
+__device__ __forceinline__ void xb_body(const G& grid, int ny, int nz, const S* __restrict__ spec,
+                                        PH* __restrict__ phi, const double2* __restrict__ twN,
+                                        const double2* __restrict__ post, double scale, int padded, int accumulate,
+                                        const double* __restrict__ shift) {
     constexpr int B = XK<N>::B, P = XK<N>::P, PITCH = XK<N>::PITCH, M1 = N + 1;
     constexpr ff::Sched SC = ff::make_sched(N);
     extern __shared__ double2 smx[];
@@ -114,7 +134,7 @@ __global__ void __launch_bounds__(XK<N>::P)
     double2* tws = smx + (N + 1) * PITCH;
     const int tid = threadIdx.x;
     const int nx = 2 * N, nrows = ny * nz;
-    const int g0 = blockIdx.x * B;
+    const int g0 = grid.x() * B;
     for (int t = tid; t < N; t += P) tws[t] = twN[t];
     pdl_wait();
     pdl_trigger();
@@ -176,6 +196,21 @@ __global__ void __launch_bounds__(XK<N>::P)
     }
 }
 
+template <int N, class S, class PH>
+__global__ void __launch_bounds__(XK<N>::P)
+    k_xb(int ny, int nz, const S* __restrict__ spec, PH* __restrict__ phi, const double2* __restrict__ twN,
+         const double2* __restrict__ post, double scale, int padded, int accumulate,
+         const double* __restrict__ shift) {
+    xb_body<N>(OwnGrid{}, ny, nz, spec, phi, twN, post, scale, padded, accumulate, shift);
+}
+
+template <int N, class S, class PH>
+__global__ void __launch_bounds__(XK<N>::P) k_xb_grp(const GrpTab<XbArgs<S, PH>>* __restrict__ t) {
+    SubGrid g;
+    const XbArgs<S, PH>& a = t->e[grp_member(t, g)];
+    xb_body<N>(g, a.ny, a.nz, a.spec, a.phi, a.tw, a.post, a.scale, 1, 0, (const double*)nullptr);
+}
+
 #define PFFT_X_SIZES(X) X(8) X(12) X(16) X(24) X(32) X(40) X(48) X(64) X(96) X(128) X(192) X(256) X(384) X(512) \
     X(768) X(1024) X(1152) X(1536)
 
@@ -206,9 +241,13 @@ int pfft_x_blocks(int nx, int ny, int nz) {
 }
 #define XF_TYPES(X, n) X(n, double, double2)
 #define XB_TYPES(X, n) X(n, double2, double)
+#define XG_V double
+#define XG_S double2
 #else
 #define XF_TYPES(X, n) X(n, float, float2) X(n, double, float2)
 #define XB_TYPES(X, n) X(n, float2, float) X(n, float2, double)
+#define XG_V float
+#define XG_S float2
 #endif
 
 #ifndef PTC_STORE32
@@ -221,9 +260,13 @@ void pfft_x_init32() {
     cudaFuncSetAttribute(k_xf<n, V, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)XK<n>::smem);
 #define XB_ATTR(n, S, PH)                                                                                        \
     cudaFuncSetAttribute(k_xb<n, S, PH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)XK<n>::smem);
-#define X_CASE(n) XF_TYPES(XF_ATTR, n) XB_TYPES(XB_ATTR, n)
+#define XG_ATTR(n)                                                                                              \
+    cudaFuncSetAttribute(k_xf_grp<n, XG_V, XG_S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)XK<n>::smem); \
+    cudaFuncSetAttribute(k_xb_grp<n, XG_S, XG_V>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)XK<n>::smem);
+#define X_CASE(n) XF_TYPES(XF_ATTR, n) XB_TYPES(XB_ATTR, n) XG_ATTR(n)
     PFFT_X_SIZES(X_CASE)
 #undef X_CASE
+#undef XG_ATTR
 #undef XF_ATTR
 #undef XB_ATTR
 }
@@ -261,7 +304,30 @@ static void pfft_xb_t(cudaStream_t st, int nx, int ny, int nz, const S* spec, PH
     }
 }
 
+// grouped launches of the step's forward (divergence source) and inverse
+// (padded potential) transforms: one member's shape is its row blocks
+void launch_xf_grp(cudaStream_t st, int nx, const GrpTab<XfArgs<XG_V, XG_S>>* t, int nblk) {
+    switch (nx / 2) {
+#define X_CASE(n)                                                                                              \
+    case n: launch_pdl(k_xf_grp<n, XG_V, XG_S>, dim3((unsigned)nblk), dim3(XK<n>::P), XK<n>::smem, st, t); break;
+        PFFT_X_SIZES(X_CASE)
+#undef X_CASE
+        default: break;
+    }
+}
+void launch_xb_grp(cudaStream_t st, int nx, const GrpTab<XbArgs<XG_S, XG_V>>* t, int nblk) {
+    switch (nx / 2) {
+#define X_CASE(n)                                                                                              \
+    case n: launch_pdl(k_xb_grp<n, XG_S, XG_V>, dim3((unsigned)nblk), dim3(XK<n>::P), XK<n>::smem, st, t); break;
+        PFFT_X_SIZES(X_CASE)
+#undef X_CASE
+        default: break;
+    }
+}
+
 #ifndef PTC_STORE32
+dim3 pfft_x_member_grid(const DConst& c) { return dim3((unsigned)pfft_x_blocks(c.nx, c.ny, c.nz)); }
+
 void launch_pfft_xf(cudaStream_t st, int mode, const DConst& c, const DMetric& m, const DCoef* coef, const Fields& f,
                     const double* src, double2* spec, const double2* twx, const double2* post, double* part,
                     unsigned int* counter, double* out_max) {

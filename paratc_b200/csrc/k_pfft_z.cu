@@ -44,15 +44,17 @@ struct GSt {
     }
 };
 
-template <int N, int DIR, class S>
-__global__ void __launch_bounds__(ZK<N>::P) k_zt(int ncol, S* __restrict__ spec, const double2* __restrict__ twN) {
+// G: the block this CTA works as (OwnGrid, or SubGrid in a grouped launch)
+template <int N, int DIR, class S, class G>
+__device__ __forceinline__ void zt_body(const G& grid, int ncol, S* __restrict__ spec,
+                                        const double2* __restrict__ twN) {
     constexpr int B = ZK<N>::B, P = ZK<N>::P;
     constexpr ff::Sched SC = ff::make_sched(N);
     extern __shared__ double2 smz[];
     double2* buf = smz;
     double2* tws = smz + N * B;
     const int tid = threadIdx.x;
-    const int q0 = blockIdx.x * B;
+    const int q0 = grid.x() * B;
     const int nvalid = min(B, ncol - q0);
     const GLd<S> gl{spec + q0, ncol, nvalid};
     const GSt<S> gs{spec + q0, ncol, nvalid};
@@ -70,6 +72,18 @@ __global__ void __launch_bounds__(ZK<N>::P) k_zt(int ncol, S* __restrict__ spec,
         constexpr int L = SC.np - 1;
         ff::pass<N, B, P, SC.r[L], ff::sched_ns(N, L), DIR, false>(ff::SmemLd<B>{buf}, gs, tws, tid);
     }
+}
+
+template <int N, int DIR, class S>
+__global__ void __launch_bounds__(ZK<N>::P) k_zt(int ncol, S* __restrict__ spec, const double2* __restrict__ twN) {
+    zt_body<N, DIR>(OwnGrid{}, ncol, spec, twN);
+}
+
+template <int N, int DIR, class S>
+__global__ void __launch_bounds__(ZK<N>::P) k_zt_grp(const GrpTab<ZtArgs<S>>* __restrict__ t) {
+    SubGrid g;
+    const ZtArgs<S>& a = t->e[grp_member(t, g)];
+    zt_body<N, DIR>(g, a.ncol, a.spec, a.tw);
 }
 
 #define PFFT_Z_SIZES(X) X(8) X(12) X(16) X(24) X(30) X(32) X(40) X(48) X(64) X(96) X(128) X(192) X(256) X(384) \
@@ -92,9 +106,43 @@ void pfft_z_init() {
     cudaFuncSetAttribute(k_zt<n, -1, double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ZK<n>::smem); \
     cudaFuncSetAttribute(k_zt<n, 1, double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ZK<n>::smem);  \
     cudaFuncSetAttribute(k_zt<n, -1, float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ZK<n>::smem);  \
-    cudaFuncSetAttribute(k_zt<n, 1, float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ZK<n>::smem);
+    cudaFuncSetAttribute(k_zt<n, 1, float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ZK<n>::smem);      \
+    cudaFuncSetAttribute(k_zt_grp<n, -1, double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ZK<n>::smem); \
+    cudaFuncSetAttribute(k_zt_grp<n, 1, double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ZK<n>::smem);  \
+    cudaFuncSetAttribute(k_zt_grp<n, -1, float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ZK<n>::smem);  \
+    cudaFuncSetAttribute(k_zt_grp<n, 1, float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ZK<n>::smem);
     PFFT_Z_SIZES(Z_CASE)
 #undef Z_CASE
+}
+
+dim3 pfft_z_member_grid(const DConst& c) {
+    const int ncol = c.ny * (c.nx / 2 + 1);
+    switch (c.nz) {
+#define Z_CASE(n) case n: return dim3((ncol + ZK<n>::B - 1) / ZK<n>::B);
+        PFFT_Z_SIZES(Z_CASE)
+#undef Z_CASE
+        default: return dim3(0);
+    }
+}
+
+template <class S>
+static void zt_grp_t(cudaStream_t st, int dir, int nz, const GrpTab<ZtArgs<S>>* t, int nblk) {
+    switch (nz) {
+#define Z_CASE(n)                                                                                               \
+    case n:                                                                                                     \
+        if (dir < 0) launch_pdl(k_zt_grp<n, -1, S>, dim3((unsigned)nblk), dim3(ZK<n>::P), ZK<n>::smem, st, t);  \
+        else launch_pdl(k_zt_grp<n, 1, S>, dim3((unsigned)nblk), dim3(ZK<n>::P), ZK<n>::smem, st, t);           \
+        break;
+        PFFT_Z_SIZES(Z_CASE)
+#undef Z_CASE
+        default: break;
+    }
+}
+void launch_zt_grp(cudaStream_t st, int dir, int nz, const GrpTab<ZtArgs<double2>>* t, int nblk) {
+    zt_grp_t(st, dir, nz, t, nblk);
+}
+void launch_zt_grp(cudaStream_t st, int dir, int nz, const GrpTab<ZtArgs<float2>>* t, int nblk) {
+    zt_grp_t(st, dir, nz, t, nblk);
 }
 
 template <class S>

@@ -103,11 +103,12 @@ __device__ __forceinline__ int modp(int i, int n) {
 // SCALAR: with the scalar transport; T: arithmetic (double, or float for the
 // mixed and FP32 storage forms); V: storage of u, v, w, c, Hist and Rhs
 // (float only in the FP32 storage form, whose arithmetic is float)
-template <bool SCALAR, class T, class V, int VAR>
-__global__ void __launch_bounds__(RhsCfg<T, VAR>::NTHR, RhsCfg<T, VAR>::MINB)
-    k_rhs_tile(DConst c, DMetric m, DCoef* __restrict__ coef, FieldSet<V> fl, double* __restrict__ uy_ym,
-               double* __restrict__ duy_ym, int ns, double gam, double the, double alp, double* __restrict__ part,
-               unsigned int* __restrict__ counter) {
+// G: the block this CTA works as (OwnGrid, or SubGrid in a grouped launch)
+template <bool SCALAR, class T, class V, int VAR, class G>
+__device__ __forceinline__ void rhs_body(const G& grid, const DConst& c, const DMetric& m, DCoef* __restrict__ coef,
+                                         const FieldSet<V>& fl, double* __restrict__ uy_ym,
+                                         double* __restrict__ duy_ym, int ns, double gam, double the, double alp,
+                                         double* __restrict__ part, unsigned int* __restrict__ counter) {
     constexpr int NF = SCALAR ? 5 : 4;
     constexpr bool F64 = sizeof(T) == 8;
     static_assert(!F64 || sizeof(V) == 8, "the FP64 arithmetic form keeps FP64 fields");
@@ -132,7 +133,7 @@ __global__ void __launch_bounds__(RhsCfg<T, VAR>::NTHR, RhsCfg<T, VAR>::MINB)
     // covers the grid with at most one row of imbalance
     const int ntx = (nx + TX - 1) / TX, ntz = (nz + TZ - 1) / TZ;
     const long long W = (long long)ntx * ntz * ny;
-    const long long gbeg = W * blockIdx.x / gridDim.x, gend = W * (blockIdx.x + 1) / gridDim.x;
+    const long long gbeg = W * grid.x() / grid.gx(), gend = W * (grid.x() + 1) / grid.gx();
     pdl_wait();
     pdl_trigger();
 
@@ -528,8 +529,8 @@ __global__ void __launch_bounds__(RhsCfg<T, VAR>::NTHR, RhsCfg<T, VAR>::MINB)
 
     // flow-rate constraint and the substep coefficients (last CTA)
     double s3v[1] = {s3};
-    const unsigned int nblocks = gridDim.x * gridDim.y * gridDim.z;
-    const int bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+    const unsigned int nblocks = grid.gx() * grid.gy() * grid.gz();
+    const int bid = grid.x() + grid.gx() * (grid.y() + grid.gy() * grid.z());
     block_sum_store<1>(s3v, part + bid);
     if (!last_block_arrive(counter, nblocks)) return;
     double tot[1];
@@ -563,6 +564,73 @@ __global__ void __launch_bounds__(RhsCfg<T, VAR>::NTHR, RhsCfg<T, VAR>::MINB)
     *coef = f;
 }
 
+// the arguments of one launch, read from shared memory by the FP32-arithmetic
+// forms (the grouped launch reads its member's record from there too, so a
+// member of a grouped ensemble rounds exactly as its own launch); fill(a)
+// writes the record
+template <bool SCALAR, class T, class V, int VAR, class Fill>
+__device__ __forceinline__ void rhs_from_shared(const SubGrid& g, Fill fill, int ns) {
+    __shared__ RhsArgs<V> a;
+    fill(a);
+    __syncthreads();
+    rhs_body<SCALAR, T, V, VAR>(g, a.c, a.m, a.coef, a.fl, a.uy_ym, a.duy_ym, ns, a.gam, a.the, a.alp, a.part,
+                                a.counter);
+}
+
+template <bool SCALAR, class T, class V, int VAR>
+__global__ void __launch_bounds__(RhsCfg<T, VAR>::NTHR, RhsCfg<T, VAR>::MINB)
+    k_rhs_tile(DConst c, DMetric m, DCoef* __restrict__ coef, FieldSet<V> fl, double* __restrict__ uy_ym,
+               double* __restrict__ duy_ym, int ns, double gam, double the, double alp, double* __restrict__ part,
+               unsigned int* __restrict__ counter) {
+    if constexpr (sizeof(T) == 8) {
+        rhs_body<SCALAR, T, V, VAR>(OwnGrid{}, c, m, coef, fl, uy_ym, duy_ym, ns, gam, the, alp, part, counter);
+    } else {
+        const SubGrid g{blockIdx.x, blockIdx.y, blockIdx.z, gridDim.x, gridDim.y, gridDim.z};
+        rhs_from_shared<SCALAR, T, V, VAR>(
+            g,
+            [&](RhsArgs<V>& a) {
+                if (threadIdx.x == 0 && threadIdx.y == 0) {
+                    a.c = c;
+                    a.m = m;
+                    a.coef = coef;
+                    a.fl = fl;
+                    a.uy_ym = uy_ym;
+                    a.duy_ym = duy_ym;
+                    a.gam = gam;
+                    a.the = the;
+                    a.alp = alp;
+                    a.part = part;
+                    a.counter = counter;
+                }
+            },
+            ns);
+    }
+}
+
+// the members of an ensemble in one launch: member i's blocks run its own
+// launch shape on its own fields
+// (the member's record is copied to shared memory first: read from there,
+// its constants are reloaded after the barriers of the row loop rather than
+// held in registers, which the one-context FP64 kernel takes straight from
+// its parameter bank)
+template <bool SCALAR, class T, class V, int VAR>
+__global__ void __launch_bounds__(RhsCfg<T, VAR>::NTHR, RhsCfg<T, VAR>::MINB)
+    k_rhs_grp(const GrpTab<RhsArgs<V>>* __restrict__ t, int ns) {
+    static_assert(sizeof(RhsArgs<V>) % 8 == 0, "copied in 8-byte words");
+    SubGrid g;
+    const int mi = grp_member(t, g);
+    rhs_from_shared<SCALAR, T, V, VAR>(
+        g,
+        [&](RhsArgs<V>& a) {
+            const unsigned long long* src = reinterpret_cast<const unsigned long long*>(&t->e[mi]);
+            unsigned long long* dst = reinterpret_cast<unsigned long long*>(&a);
+            for (int w = threadIdx.y * 32 + threadIdx.x; w < (int)(sizeof(RhsArgs<V>) / 8);
+                 w += RhsCfg<T, VAR>::NTHR)
+                dst[w] = __ldg(&src[w]);
+        },
+        ns);
+}
+
 // ---------------------------------------------------------------------------
 // one wave of resident CTAs (MINB per SM for the precision; the record
 // count is sized for the larger)
@@ -581,6 +649,8 @@ int rhs_variants() { return RHS_NVAR; }
 void rhs_init() {
 #define RHS_ATTR(S, T, V, VAR)                                                                            \
     cudaFuncSetAttribute(k_rhs_tile<S, T, V, VAR>, cudaFuncAttributeMaxDynamicSharedMemorySize,        \
+                         (int)rhs_smem_bytes<S, T, VAR>());                                            \
+    cudaFuncSetAttribute(k_rhs_grp<S, T, V, VAR>, cudaFuncAttributeMaxDynamicSharedMemorySize,         \
                          (int)rhs_smem_bytes<S, T, VAR>());
     RHS_ATTR(false, double, double, 0) RHS_ATTR(true, double, double, 0)
     RHS_ATTR(false, double, double, 1) RHS_ATTR(true, double, double, 1)
@@ -622,6 +692,42 @@ void launch_rhs_tile(cudaStream_t st, const DConst& c, const DMetric& m, DCoef* 
         if (c.scalar_on) launch_rhs64<true>(st, c, m, coef, f, uy_ym, duy_ym, ns, gam, the, alp, part, counter);
         else launch_rhs64<false>(st, c, m, coef, f, uy_ym, duy_ym, ns, gam, the, alp, part, counter);
     }
+}
+
+// ---- grouped launches: the shape of one member's launch, and one launch
+// over a table of members that share the instantiation (scalar, arithmetic,
+// storage, launch shape)
+dim3 rhs_member_grid(const DConst& c, int f32arith) {
+    return dim3((unsigned)rhs_blocks(c, f32arith ? RhsCfg<float, 0>::MINB : RhsCfg<double, 0>::MINB));
+}
+
+template <bool SCALAR, class T, int VAR, class V>
+static void rhs_grp_t(cudaStream_t st, const GrpTab<RhsArgs<V>>* t, int nblk, int ns) {
+    using CFG = RhsCfg<T, VAR>;
+    launch_pdl(k_rhs_grp<SCALAR, T, V, VAR>, dim3((unsigned)nblk), dim3(32, TZ / CFG::ZC),
+               rhs_smem_bytes<SCALAR, T, VAR>(), st, t, ns);
+}
+
+void launch_rhs_grp(cudaStream_t st, const DConst& key, const GrpTab<RhsArgs<double>>* t, int nblk, int ns) {
+    const bool s = key.scalar_on != 0;
+    if (key.fp32_rhs) {
+        if (s) rhs_grp_t<true, float, 0>(st, t, nblk, ns);
+        else rhs_grp_t<false, float, 0>(st, t, nblk, ns);
+    } else if (key.rhs_var == 1) {
+        if (s) rhs_grp_t<true, double, 1>(st, t, nblk, ns);
+        else rhs_grp_t<false, double, 1>(st, t, nblk, ns);
+    } else if (key.rhs_var == 2) {
+        if (s) rhs_grp_t<true, double, 2>(st, t, nblk, ns);
+        else rhs_grp_t<false, double, 2>(st, t, nblk, ns);
+    } else {
+        if (s) rhs_grp_t<true, double, 0>(st, t, nblk, ns);
+        else rhs_grp_t<false, double, 0>(st, t, nblk, ns);
+    }
+}
+
+void launch_rhs_grp(cudaStream_t st, const DConst& key, const GrpTab<RhsArgs<float>>* t, int nblk, int ns) {
+    if (key.scalar_on) rhs_grp_t<true, float, 0>(st, t, nblk, ns);
+    else rhs_grp_t<false, float, 0>(st, t, nblk, ns);
 }
 
 void launch_rhs_tile(cudaStream_t st, const DConst& c, const DMetric& m, DCoef* coef, const Fields32& f, double* uy_ym,

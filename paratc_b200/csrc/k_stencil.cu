@@ -62,15 +62,16 @@ __global__ void k_reduce_max(const double* __restrict__ part, int nparts, double
 // (src/m_TScheme.f90:82-107,512-532; src/m_BC_and_Halo.f90:23-64,108-122)
 // mode 0: substep; mode 1: pressure-free projection (alpha = 1, p untouched)
 // ---------------------------------------------------------------------------
-template <class V>
-__global__ void __launch_bounds__(256) k_project(DConst c, DMetric m, const DCoef* __restrict__ coef, int mode,
-                                                 const V* __restrict__ phi, V* __restrict__ ux,
-                                                 V* __restrict__ uy, V* __restrict__ uz,
-                                                 double* __restrict__ pr, const double* __restrict__ uy_ym) {
+// G: the block this CTA works as (OwnGrid, or SubGrid in a grouped launch)
+template <class V, class G>
+__device__ __forceinline__ void project_body(const G& grid, const DConst& c, const DMetric& m,
+                                             const DCoef* __restrict__ coef, int mode, const V* __restrict__ phi,
+                                             V* __restrict__ ux, V* __restrict__ uy, V* __restrict__ uz,
+                                             double* __restrict__ pr, const double* __restrict__ uy_ym) {
     const int nx = c.nx;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int jc = blockIdx.y * blockDim.y + threadIdx.y + 1;
-    const int k = blockIdx.z;
+    const int i = grid.x() * blockDim.x + threadIdx.x;
+    const int jc = grid.y() * blockDim.y + threadIdx.y + 1;
+    const int k = grid.z();
     pdl_wait();
     if (i >= nx || jc > c.ny) return;
     const double alpha = mode == 0 ? coef->pmAlpha : 1.0;
@@ -110,6 +111,21 @@ __global__ void __launch_bounds__(256) k_project(DConst c, DMetric m, const DCoe
         if (jc == 1) pr[q - nx] = pn;
         if (jc == c.ny) pr[q + nx] = pn;
     }
+}
+
+template <class V>
+__global__ void __launch_bounds__(256) k_project(DConst c, DMetric m, const DCoef* __restrict__ coef, int mode,
+                                                 const V* __restrict__ phi, V* __restrict__ ux,
+                                                 V* __restrict__ uy, V* __restrict__ uz,
+                                                 double* __restrict__ pr, const double* __restrict__ uy_ym) {
+    project_body(OwnGrid{}, c, m, coef, mode, phi, ux, uy, uz, pr, uy_ym);
+}
+
+template <class V>
+__global__ void __launch_bounds__(256) k_project_grp(const GrpTab<ProjArgs<V>>* __restrict__ t) {
+    SubGrid g;
+    const ProjArgs<V>& a = t->e[grp_member(t, g)];
+    project_body(g, a.c, a.m, a.coef, 0, a.phi, a.ux, a.uy, a.uz, a.pr, a.uy_ym);
 }
 
 // ---------------------------------------------------------------------------
@@ -205,20 +221,21 @@ __global__ void k_cfl_final(DConst c, DCoef* coef, const double* __restrict__ pa
 constexpr int ENDSTEP_THREADS = 256;
 constexpr int ENDSTEP_U = 4;
 
-template <class V>
-__global__ void __launch_bounds__(ENDSTEP_THREADS, 2)
-    k_endstep(DConst c, DMetric m, const V* __restrict__ ux, const V* __restrict__ uy,
-              const V* __restrict__ uz, const V* __restrict__ sc, DCoef* __restrict__ coef,
-              DDiag* __restrict__ diag, double* __restrict__ part, unsigned int* __restrict__ counter, int next) {
+template <class V, class G>
+__device__ __forceinline__ void endstep_body(const G& grid, const DConst& c, const DMetric& m, const V* __restrict__ ux,
+                                             const V* __restrict__ uy, const V* __restrict__ uz,
+                                             const V* __restrict__ sc, DCoef* __restrict__ coef,
+                                             DDiag* __restrict__ diag, double* __restrict__ part,
+                                             unsigned int* __restrict__ counter, int next) {
     const int nx = c.nx, ny = c.ny, nz = c.nz;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int nwarps = gridDim.x * (ENDSTEP_THREADS / 32);
+    const int nwarps = grid.gx() * (ENDSTEP_THREADS / 32);
     const size_t pl = (size_t)c.nyt * nx;
     double mx[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
     double sm[3] = {0.0, 0.0, 0.0};
     pdl_wait();
     pdl_trigger();
-    for (int r = blockIdx.x * (ENDSTEP_THREADS / 32) + warp; r < ny * nz; r += nwarps) {
+    for (int r = grid.x() * (ENDSTEP_THREADS / 32) + warp; r < ny * nz; r += nwarps) {
         const int k = r / ny, jc = r - k * ny + 1;
         const int km = k == 0 ? nz - 1 : k - 1, kp = k == nz - 1 ? 0 : k + 1, ku = kp == nz - 1 ? 0 : kp + 1;
         const size_t r0 = (size_t)jc * nx;
@@ -263,14 +280,14 @@ __global__ void __launch_bounds__(ENDSTEP_THREADS, 2)
             }
         }
     }
-    block_max_store<5>(mx, part + (size_t)blockIdx.x * 8);
+    block_max_store<5>(mx, part + (size_t)grid.x() * 8);
     __syncthreads();
-    block_sum_store<3>(sm, part + (size_t)blockIdx.x * 8 + 5);
-    if (!last_block_arrive(counter, gridDim.x)) return;
+    block_sum_store<3>(sm, part + (size_t)grid.x() * 8 + 5);
+    if (!last_block_arrive(counter, grid.gx())) return;
     // the last CTA: records in index order, thread t takes records t, t+256, ...
     __shared__ double sh[ENDSTEP_THREADS / 32][8];
     double v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    for (int b = threadIdx.x; b < (int)gridDim.x; b += ENDSTEP_THREADS) {
+    for (int b = threadIdx.x; b < (int)grid.gx(); b += ENDSTEP_THREADS) {
         const double* p = part + (size_t)b * 8;
 #pragma unroll
         for (int q = 0; q < 5; q++) v[q] = nmax(v[q], __ldcg(&p[q]));
@@ -326,6 +343,21 @@ __global__ void __launch_bounds__(ENDSTEP_THREADS, 2)
         f.dt = (c.icfl == 1) ? fmin(c.cflc / uddxmax, c.dt_max) : c.dt_max;
         *coef = f;
     }
+}
+
+template <class V>
+__global__ void __launch_bounds__(ENDSTEP_THREADS, 2)
+    k_endstep(DConst c, DMetric m, const V* __restrict__ ux, const V* __restrict__ uy,
+              const V* __restrict__ uz, const V* __restrict__ sc, DCoef* __restrict__ coef,
+              DDiag* __restrict__ diag, double* __restrict__ part, unsigned int* __restrict__ counter, int next) {
+    endstep_body(OwnGrid{}, c, m, ux, uy, uz, sc, coef, diag, part, counter, next);
+}
+
+template <class V>
+__global__ void __launch_bounds__(ENDSTEP_THREADS, 2) k_endstep_grp(const GrpTab<EndArgs<V>>* __restrict__ t) {
+    SubGrid g;
+    const EndArgs<V>& a = t->e[grp_member(t, g)];
+    endstep_body(g, a.c, a.m, a.ux, a.uy, a.uz, a.sc, a.coef, a.diag, a.part, a.counter, 1);
 }
 
 // ---------------------------------------------------------------------------
@@ -550,6 +582,22 @@ void launch_residual(cudaStream_t st, const DConst& c, const DMetric& m, const d
 }
 
 size_t endstep_blocks(const DConst& c) { return (size_t)2 * (c.nsm > 0 ? c.nsm : 148); }
+
+// grouped launches (one member's shape: its own launch's)
+dim3 cell_member_grid(const DConst& c) { return cell_grid(c); }
+dim3 endstep_member_grid(const DConst& c) { return dim3((unsigned)endstep_blocks(c)); }
+void launch_project_grp(cudaStream_t st, const GrpTab<ProjArgs<double>>* t, int nblk) {
+    launch_pdl(k_project_grp<double>, dim3((unsigned)nblk), cell_block(), 0, st, t);
+}
+void launch_project_grp(cudaStream_t st, const GrpTab<ProjArgs<float>>* t, int nblk) {
+    launch_pdl(k_project_grp<float>, dim3((unsigned)nblk), cell_block(), 0, st, t);
+}
+void launch_endstep_grp(cudaStream_t st, const GrpTab<EndArgs<double>>* t, int nblk) {
+    launch_pdl(k_endstep_grp<double>, dim3((unsigned)nblk), dim3(ENDSTEP_THREADS), 0, st, t);
+}
+void launch_endstep_grp(cudaStream_t st, const GrpTab<EndArgs<float>>* t, int nblk) {
+    launch_pdl(k_endstep_grp<float>, dim3((unsigned)nblk), dim3(ENDSTEP_THREADS), 0, st, t);
+}
 
 void launch_endstep(cudaStream_t st, const DConst& c, const DMetric& m, const Fields& f, DCoef* coef, DDiag* diag,
                     double* part, unsigned int* counter, int next) {

@@ -171,13 +171,14 @@ __host__ __device__ inline int helm_stride(int ny) { return 3 * (ny + 2); }
 // memory; rows are addressed by pointer steps; the wall rows need no case of
 // their own in the sweeps (a(1) = 0, arr(ny+1) = 0, and clcU2Hat's row-1
 // value is substituted before the sweep and its result after it).
-template <class V, int HU>
-__global__ void __launch_bounds__(128, 4) k_helm(DConst cst, const DCoef* __restrict__ coef, int comp0, FieldSet<V> fl,
-                                              const double* __restrict__ duy_ym, const double* __restrict__ uy_ym,
-                                              const double* __restrict__ facs) {
+// G: the block this CTA works as (OwnGrid, or SubGrid in a grouped launch)
+template <class V, int HU, class G>
+__device__ __forceinline__ void helm_body(const G& grid, const DConst& cst, const DCoef* __restrict__ coef, int comp0,
+                                          const FieldSet<V>& fl, const double* __restrict__ duy_ym,
+                                          const double* __restrict__ uy_ym, const double* __restrict__ facs) {
     extern __shared__ double shf[];
     const int nx = cst.nx, ny = cst.ny;
-    const int comp = comp0 + blockIdx.z;
+    const int comp = comp0 + (int)grid.z();
     const int t = comp == 1 ? 1 : (comp == 3 ? 2 : 0);
     pdl_wait();
     pdl_trigger();
@@ -190,8 +191,8 @@ __global__ void __launch_bounds__(128, 4) k_helm(DConst cst, const DCoef* __rest
     const double* SA = shf;
     const double* SR = shf + (ny + 2);
     const double* SW = shf + 2 * (ny + 2);
-    const int i = (blockIdx.x * 4 + threadIdx.y) * 32 + threadIdx.x;
-    const int k = blockIdx.y;
+    const int i = (grid.x() * 4 + threadIdx.y) * 32 + threadIdx.x;
+    const int k = grid.y();
     if (i >= nx) return;
     V* u;
     V* rhs;
@@ -305,6 +306,20 @@ __global__ void __launch_bounds__(128, 4) k_helm(DConst cst, const DCoef* __rest
     }
 }
 
+template <class V, int HU>
+__global__ void __launch_bounds__(128, 4) k_helm(DConst cst, const DCoef* __restrict__ coef, int comp0, FieldSet<V> fl,
+                                              const double* __restrict__ duy_ym, const double* __restrict__ uy_ym,
+                                              const double* __restrict__ facs) {
+    helm_body<V, HU>(OwnGrid{}, cst, coef, comp0, fl, duy_ym, uy_ym, facs);
+}
+
+template <class V, int HU>
+__global__ void __launch_bounds__(128, 4) k_helm_grp(const GrpTab<HelmArgs<V>>* __restrict__ t) {
+    SubGrid g;
+    const HelmArgs<V>& a = t->e[grp_member(t, g)];
+    helm_body<V, HU>(g, a.c, a.coef, a.comp0, a.fl, a.duy_ym, a.uy_ym, a.fac);
+}
+
 // ---------------------------------------------------------------------------
 // spectral y-solve of clcPPE_x1 (src/m_Poisson.f90:383-430) on the complex
 // coefficients spec[(k*ny + j)*(nx/2+1) + kx].  The real and imaginary parts
@@ -407,14 +422,14 @@ constexpr int YS_U = 8;  // rows loaded ahead of the dependent chain
 // sweeps the real (l even) or imaginary (l odd) part of column l/2.  S: the
 // spectrum's storage (double2, or float2 in the FP32 storage form; the
 // sweeps run in double either way).
-template <class S>
-__global__ void __launch_bounds__(32) k_ys_staged(int ny, int M1, int nz, const double* __restrict__ am2ph,
-                                                  S* __restrict__ spec, const double* __restrict__ fac) {
+template <class S, class G>
+__device__ __forceinline__ void ys_staged_body(const G& grid, int ny, int M1, int nz, const double* __restrict__ am2ph,
+                                               S* __restrict__ spec, const double* __restrict__ fac) {
     using R = decltype(S::x);
     extern __shared__ double2 sy[];
     const int lane = threadIdx.x;
     const int NQ = M1 * nz;
-    const int q0 = blockIdx.x * 16;
+    const int q0 = grid.x() * 16;
     const int nv = min(16, NQ - q0);
     S* sd = reinterpret_cast<S*>(sy);                          // [ny][16] spectrum
     double* srv = reinterpret_cast<double*>(sy + ny * 16);     // [ny][16] 1/vecm
@@ -511,15 +526,21 @@ __global__ void __launch_bounds__(32) k_ys_staged(int ny, int M1, int nz, const 
         for (int j = half; j < ny; j += 2) scol[(size_t)j * M1] = sd[j * 16 + cq];
 }
 
+template <class S>
+__global__ void __launch_bounds__(32) k_ys_staged(int ny, int M1, int nz, const double* __restrict__ am2ph,
+                                                  S* __restrict__ spec, const double* __restrict__ fac) {
+    ys_staged_body(OwnGrid{}, ny, M1, nz, am2ph, spec, fac);
+}
+
 // Large grids: one thread per real column straight from global memory, the
 // rows of a chunk loaded ahead of its chain, latency hidden by occupancy.
 // R: storage of the spectrum's real parts (double, or float in the FP32
 // storage form); the sweeps run in double either way
-template <class R>
-__global__ void __launch_bounds__(128) k_ys_global(int ny, int M1, int nz, const double* __restrict__ am2ph,
-                                                   R* __restrict__ specd, const double* __restrict__ fac) {
+template <class R, class G>
+__device__ __forceinline__ void ys_global_body(const G& grid, int ny, int M1, int nz, const double* __restrict__ am2ph,
+                                               R* __restrict__ specd, const double* __restrict__ fac) {
     const int W = 2 * M1, NQ = M1 * nz;
-    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    const int g = grid.x() * blockDim.x + threadIdx.x;
     pdl_wait();
     pdl_trigger();
     if (g >= W * nz) return;
@@ -576,6 +597,27 @@ __global__ void __launch_bounds__(128) k_ys_global(int ny, int M1, int nz, const
     }
 }
 
+template <class R>
+__global__ void __launch_bounds__(128) k_ys_global(int ny, int M1, int nz, const double* __restrict__ am2ph,
+                                                   R* __restrict__ specd, const double* __restrict__ fac) {
+    ys_global_body(OwnGrid{}, ny, M1, nz, am2ph, specd, fac);
+}
+
+// grouped: kind 0 staged (S the spectrum), 1 streaming (its real parts)
+template <class S>
+__global__ void __launch_bounds__(32) k_ys_staged_grp(const GrpTab<YsArgs<S>>* __restrict__ t) {
+    SubGrid g;
+    const YsArgs<S>& a = t->e[grp_member(t, g)];
+    ys_staged_body(g, a.ny, a.M1, a.nz, a.am2ph, a.spec, a.fac);
+}
+template <class S>
+__global__ void __launch_bounds__(128) k_ys_global_grp(const GrpTab<YsArgs<S>>* __restrict__ t) {
+    using R = decltype(S::x);
+    SubGrid g;
+    const YsArgs<S>& a = t->e[grp_member(t, g)];
+    ys_global_body(g, a.ny, a.M1, a.nz, a.am2ph, reinterpret_cast<R*>(a.spec), a.fac);
+}
+
 void launch_pois_factors(cudaStream_t st, const DConst& c, const DMetric& m, double* fac) {
     const int M1 = c.nx / 2 + 1, NQ = M1 * c.nz;
     k_pois_factors<<<(NQ + 127) / 128, 128, 0, st>>>(c.ny, M1, c.nz, m, fac, fac + (size_t)NQ * c.ny);
@@ -586,20 +628,45 @@ void launch_pois_factors(cudaStream_t st, const DConst& c, const DMetric& m, dou
 // aligned), the two factor blocks and am2ph
 static size_t ys_staged_smem(int ny) { return (size_t)ny * 16 * 2 * sizeof(double2) + (size_t)(ny + 1) * sizeof(double); }
 
-template <class S>
-static void ysolve_fac_t(cudaStream_t st, const DConst& c, const DMetric& m, S* spec, const double* fac) {
-    using R = decltype(S::x);
+// 0: the staged kernel (the grid fits one wave of it, or solver_sel = 1),
+// 1: the streaming one
+int ys_kind(const DConst& c) {
     const int M1 = c.nx / 2 + 1, NQ = M1 * c.nz;
     const size_t sm = ys_staged_smem(c.ny);
     const int per_sm = sm > 0 ? (int)((220 * 1024) / sm) : 0;
     const int ctas = (NQ + 15) / 16;
-    if (per_sm >= 1 && (c.solver_sel == 1 || (c.solver_sel == 0 && ctas <= per_sm * c.nsm))) {
-        launch_pdl(k_ys_staged<S>, dim3(ctas), dim3(32), sm, st, c.ny, M1, c.nz, m.am2ph, spec, fac);
+    return (per_sm >= 1 && (c.solver_sel == 1 || (c.solver_sel == 0 && ctas <= per_sm * c.nsm))) ? 0 : 1;
+}
+dim3 ys_member_grid(const DConst& c, int kind) {
+    const int M1 = c.nx / 2 + 1, NQ = M1 * c.nz;
+    return kind == 0 ? dim3((NQ + 15) / 16) : dim3((2 * M1 * c.nz + 127) / 128);
+}
+size_t ys_smem(const DConst& c, int kind) { return kind == 0 ? ys_staged_smem(c.ny) : 0; }
+
+template <class S>
+static void ysolve_fac_t(cudaStream_t st, const DConst& c, const DMetric& m, S* spec, const double* fac) {
+    using R = decltype(S::x);
+    const int M1 = c.nx / 2 + 1;
+    const int kind = ys_kind(c);
+    if (kind == 0) {
+        launch_pdl(k_ys_staged<S>, ys_member_grid(c, 0), dim3(32), ys_smem(c, 0), st, c.ny, M1, c.nz, m.am2ph, spec,
+                   fac);
     } else {
-        const int n = 2 * M1 * c.nz;
-        launch_pdl(k_ys_global<R>, dim3((n + 127) / 128), dim3(128), 0, st, c.ny, M1, c.nz, m.am2ph,
+        launch_pdl(k_ys_global<R>, ys_member_grid(c, 1), dim3(128), 0, st, c.ny, M1, c.nz, m.am2ph,
                    reinterpret_cast<R*>(spec), fac);
     }
+}
+
+template <class S>
+static void ys_grp_t(cudaStream_t st, int kind, const GrpTab<YsArgs<S>>* t, int nblk, size_t smem) {
+    if (kind == 0) launch_pdl(k_ys_staged_grp<S>, dim3((unsigned)nblk), dim3(32), smem, st, t);
+    else launch_pdl(k_ys_global_grp<S>, dim3((unsigned)nblk), dim3(128), 0, st, t);
+}
+void launch_ys_grp(cudaStream_t st, int kind, const GrpTab<YsArgs<double2>>* t, int nblk, size_t smem) {
+    ys_grp_t(st, kind, t, nblk, smem);
+}
+void launch_ys_grp(cudaStream_t st, int kind, const GrpTab<YsArgs<float2>>* t, int nblk, size_t smem) {
+    ys_grp_t(st, kind, t, nblk, smem);
 }
 void launch_ysolve_fac(cudaStream_t st, const DConst& c, const DMetric& m, double2* spec, const double* fac) {
     ysolve_fac_t(st, c, m, spec, fac);
@@ -633,6 +700,8 @@ void tridiag_init() {
     cudaFuncSetAttribute(k_ysolve<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
     cudaFuncSetAttribute(k_ys_staged<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
     cudaFuncSetAttribute(k_ys_staged<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
+    cudaFuncSetAttribute(k_ys_staged_grp<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
+    cudaFuncSetAttribute(k_ys_staged_grp<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
     cudaFuncSetAttribute(k_helm_factors, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
 }
 
@@ -695,11 +764,27 @@ void launch_helm_factors(cudaStream_t st, const DConst& c, const DMetric& m, con
                alp[0], alp[1], alp[2], fac);
 }
 
+dim3 helm_member_grid(const DConst& c, int ncomp) { return dim3((c.nx + 127) / 128, c.nz, ncomp); }
+size_t helm_smem(const DConst& c) { return helm_stride(c.ny) * sizeof(double); }
+
+template <class V>
+static void helm_grp_t(cudaStream_t st, const DConst& key, const GrpTab<HelmArgs<V>>* t, int nblk, size_t smem) {
+    constexpr int H0 = sizeof(V) == 4 ? 2 * HY_U : HY_U;
+    if (key.helm_var == 1) launch_pdl(k_helm_grp<V, H0 / 2>, dim3((unsigned)nblk), dim3(32, 4), smem, st, t);
+    else launch_pdl(k_helm_grp<V, H0>, dim3((unsigned)nblk), dim3(32, 4), smem, st, t);
+}
+void launch_helm_grp(cudaStream_t st, const DConst& key, const GrpTab<HelmArgs<double>>* t, int nblk, size_t smem) {
+    helm_grp_t(st, key, t, nblk, smem);
+}
+void launch_helm_grp(cudaStream_t st, const DConst& key, const GrpTab<HelmArgs<float>>* t, int nblk, size_t smem) {
+    helm_grp_t(st, key, t, nblk, smem);
+}
+
 template <class V>
 static void helm_dispatch(cudaStream_t st, const DConst& c, const DCoef* coef, int comp0, int ncomp,
                           const FieldSet<V>& f, const double* duy_ym, const double* uy_ym, const double* fac) {
     dim3 blk(32, 4);
-    dim3 grd((c.nx + 127) / 128, c.nz, ncomp);
+    dim3 grd = helm_member_grid(c, ncomp);
     // rows per chunk: FP64 8 (variant 1: 4); float storage, whose ring takes
     // half the registers, 16 (variant 1: 8)
     constexpr int H0 = sizeof(V) == 4 ? 2 * HY_U : HY_U;

@@ -200,6 +200,114 @@ void launch_pfft_xf(cudaStream_t st, const DConst& c, const double* src, float2*
 void launch_pfft_xb(cudaStream_t st, int nx, int ny, int nz, const float2* spec, double* phi, const double2* twx,
                     const double2* post, double scale, int accumulate, const double* shift);
 
+// ---- grouped launches over the members of an ensemble.  One launch runs
+// one kernel instantiation for every member of a table (GrpTab in
+// common.cuh): member i's CTAs take its own launch shape (the *_member_grid
+// functions, the same shape its own launch has) on its own fields, so each
+// member computes exactly what its own launches compute.  Argument records:
+template <class V>
+struct RhsArgs {  // k_rhs_tile
+    DConst c;
+    DMetric m;
+    DCoef* coef;
+    FieldSet<V> fl;
+    double *uy_ym, *duy_ym;
+    double gam, the, alp;  // the substep's RK3 coefficients
+    double* part;
+    unsigned int* counter;
+};
+template <class V>
+struct HelmArgs {  // k_helm, components comp0 .. comp0 + grid z - 1
+    DConst c;
+    const DCoef* coef;
+    FieldSet<V> fl;
+    const double *duy_ym, *uy_ym, *fac;
+    int comp0;
+};
+template <class V, class S>
+struct XfArgs {  // k_xf, divergence source of the substep (mode 0)
+    DConst c;
+    DMetric m;
+    const DCoef* coef;
+    const V *ux, *uy, *uz;
+    S* spec;
+    const double2 *tw, *post;
+    double* part;
+    unsigned int* counter;
+    double* out_max;
+};
+template <class S>
+struct ZtArgs {  // k_zt
+    int ncol;
+    S* spec;
+    const double2* tw;
+};
+template <class S>
+struct YsArgs {  // k_ys_staged / k_ys_global
+    int ny, M1, nz;
+    const double* am2ph;
+    S* spec;
+    const double* fac;
+};
+template <class S, class PH>
+struct XbArgs {  // k_xb into the padded potential
+    int ny, nz;
+    const S* spec;
+    PH* phi;
+    const double2 *tw, *post;
+    double scale;
+};
+template <class V>
+struct ProjArgs {  // k_project, substep mode
+    DConst c;
+    DMetric m;
+    const DCoef* coef;
+    const V* phi;
+    V *ux, *uy, *uz;
+    double* pr;
+    const double* uy_ym;
+};
+template <class V>
+struct EndArgs {  // k_endstep with the next step's clcCFL
+    DConst c;
+    DMetric m;
+    const V *ux, *uy, *uz, *sc;
+    DCoef* coef;
+    DDiag* diag;
+    double* part;
+    unsigned int* counter;
+};
+
+// key: the member whose DConst selects the instantiation (scalar_on,
+// fp32_rhs, rhs_var, helm_var, nx, nz, ...); nblk: the table's total CTAs
+dim3 rhs_member_grid(const DConst& c, int f32arith);
+void launch_rhs_grp(cudaStream_t st, const DConst& key, const GrpTab<RhsArgs<double>>* t, int nblk, int ns);
+void launch_rhs_grp(cudaStream_t st, const DConst& key, const GrpTab<RhsArgs<float>>* t, int nblk, int ns);
+dim3 helm_member_grid(const DConst& c, int ncomp);
+size_t helm_smem(const DConst& c);
+void launch_helm_grp(cudaStream_t st, const DConst& key, const GrpTab<HelmArgs<double>>* t, int nblk, size_t smem);
+void launch_helm_grp(cudaStream_t st, const DConst& key, const GrpTab<HelmArgs<float>>* t, int nblk, size_t smem);
+// the y-solve: kind 0 staged, 1 streaming (ys_kind), per member
+int ys_kind(const DConst& c);
+dim3 ys_member_grid(const DConst& c, int kind);
+size_t ys_smem(const DConst& c, int kind);
+void launch_ys_grp(cudaStream_t st, int kind, const GrpTab<YsArgs<double2>>* t, int nblk, size_t smem);
+void launch_ys_grp(cudaStream_t st, int kind, const GrpTab<YsArgs<float2>>* t, int nblk, size_t smem);
+dim3 pfft_x_member_grid(const DConst& c);
+void launch_xf_grp(cudaStream_t st, int nx, const GrpTab<XfArgs<double, double2>>* t, int nblk);
+void launch_xf_grp(cudaStream_t st, int nx, const GrpTab<XfArgs<float, float2>>* t, int nblk);
+void launch_xb_grp(cudaStream_t st, int nx, const GrpTab<XbArgs<double2, double>>* t, int nblk);
+void launch_xb_grp(cudaStream_t st, int nx, const GrpTab<XbArgs<float2, float>>* t, int nblk);
+dim3 pfft_z_member_grid(const DConst& c);
+void launch_zt_grp(cudaStream_t st, int dir, int nz, const GrpTab<ZtArgs<double2>>* t, int nblk);
+void launch_zt_grp(cudaStream_t st, int dir, int nz, const GrpTab<ZtArgs<float2>>* t, int nblk);
+dim3 cell_member_grid(const DConst& c);
+void launch_project_grp(cudaStream_t st, const GrpTab<ProjArgs<double>>* t, int nblk);
+void launch_project_grp(cudaStream_t st, const GrpTab<ProjArgs<float>>* t, int nblk);
+dim3 endstep_member_grid(const DConst& c);
+void launch_endstep_grp(cudaStream_t st, const GrpTab<EndArgs<double>>* t, int nblk);
+void launch_endstep_grp(cudaStream_t st, const GrpTab<EndArgs<float>>* t, int nblk);
+
 // k_fft.cu
 void fft_init();
 size_t fft_smem_need(int nx, int nz);

@@ -12,7 +12,7 @@ import os
 
 import numpy as np
 
-from .abi import (ParatcTuning, LAYOUT_INTERIOR, SCHED_NCHOICES, VISU, VISU_NAMES, ParatcIoOptions, PARATC_ERR_DIV_LIMIT, PARATC_ERR_VEL_LIMIT, PARATC_OK, ParatcDiag,
+from .abi import (BATCH_GROUPED, BATCH_STREAMS, ParatcTuning, LAYOUT_INTERIOR, SCHED_NCHOICES, VISU, VISU_NAMES, ParatcIoOptions, PARATC_ERR_DIV_LIMIT, PARATC_ERR_VEL_LIMIT, PARATC_OK, ParatcDiag,
                   ParatcParams)
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
@@ -37,7 +37,8 @@ EXPORTED = [
     "paratc_io_options_from_namelist", "paratc_visu_quantity_device", "paratc_autotune", "paratc_get_schedule",
     "paratc_set_schedule", "paratc_set_precision", "paratc_get_precision", "paratc_set_wait_limit",
     "paratc_xprofile", "paratc_front_position", "paratc_poisson_refined", "paratc_poisson_refined_async",
-    "paratc_autotune_all", "paratc_get_tuning", "paratc_set_tuning",
+    "paratc_autotune_all", "paratc_get_tuning", "paratc_set_tuning", "paratc_batch_set_mode",
+    "paratc_batch_get_mode", "paratc_batch_step_launches",
 ]
 PROF_NKERNELS = 16
 
@@ -135,6 +136,10 @@ def load(path=None):
                                    _dp]
     L.paratc_batch_stream.argtypes = [ctypes.c_void_p]
     L.paratc_batch_stream.restype = ctypes.c_void_p
+    L.paratc_batch_set_mode.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    L.paratc_batch_get_mode.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]
+    L.paratc_batch_step_launches.argtypes = [ctypes.c_void_p]
+    L.paratc_batch_step_launches.restype = ctypes.c_int64
     L.paratc_spectra_reset.argtypes = [ctypes.c_void_p]
     L.paratc_spectra_accumulate.argtypes = [ctypes.c_void_p, ctypes.c_int]
     L.paratc_spectra_get.argtypes = [ctypes.c_void_p, _dp, _dp, ctypes.POINTER(ctypes.c_int),
@@ -635,6 +640,29 @@ class BatchSystem:
     @property
     def graph_kernels(self):
         return int(self._L.paratc_batch_graph_kernels(self._h))
+
+    @property
+    def mode(self):
+        """'streams' (every member launches its own kernels on its own
+        stream) or 'grouped' (one launch per kernel instantiation over the
+        members, paratc_batch_set_mode)."""
+        v = ctypes.c_int()
+        rc = self._L.paratc_batch_get_mode(self._h, ctypes.byref(v))
+        if rc != PARATC_OK:
+            raise ParatcError(rc, "paratc_batch_get_mode")
+        return {BATCH_STREAMS: "streams", BATCH_GROUPED: "grouped"}[v.value]
+
+    @mode.setter
+    def mode(self, name):
+        v = {"streams": BATCH_STREAMS, "grouped": BATCH_GROUPED}[name]
+        rc = self._L.paratc_batch_set_mode(self._h, v)
+        if rc != PARATC_OK:
+            raise ParatcError(rc, "paratc_batch_set_mode")
+
+    @property
+    def step_launches(self):
+        """Kernel launches of one steady step in the batch's mode."""
+        return int(self._L.paratc_batch_step_launches(self._h))
 
     @property
     def stream(self):
