@@ -1969,6 +1969,27 @@ bool grp_upload(GrpPlan& P, const GrpAcc<E>& a, std::vector<std::pair<const GrpT
     return true;
 }
 
+// the right-hand-side CTAs of a group: one wave of the device shared by the
+// members in proportion to their rows, at least one each and at most the
+// member's own block count (each CTA runs consecutive logical blocks of its
+// member, see rhs_body)
+template <class K, class V>
+void grp_balance_rhs(std::map<K, GrpAcc<RhsArgs<V>>>& m) {
+    for (auto& kv : m) {
+        GrpAcc<RhsArgs<V>>& a = kv.second;
+        long long tot = 0;
+        for (auto& e : a.e) tot += rhs_work_rows(e.c);
+        if (tot <= 0 || a.e.empty()) continue;
+        const long long wave = rhs_wave(a.e[0].c);
+        for (size_t i = 0; i < a.e.size(); i++) {
+            const long long w = rhs_work_rows(a.e[i].c);
+            long long b = (wave * w + tot / 2) / tot;
+            b = std::max(1LL, std::min(b, (long long)a.e[i].nlog));
+            a.g[i] = dim3((unsigned)b);
+        }
+    }
+}
+
 // one launch per table of every instantiation in m, in key order
 template <class K, class E, class F>
 bool grp_emit(GrpPlan& P, std::map<K, GrpAcc<E>>& m, std::vector<GrpLaunch>& out, F launch) {
@@ -2037,7 +2058,8 @@ int grp_build(paratc_batch* b) {
             if (c->prec == PARATC_PREC_FP32) {
                 float2* sp = spec32(c);
                 rhs32[k.scalar_on].add(k, RhsArgs<float>{k, c->dm, c->d_coef, c->f32, c->d_uy_ym, c->d_duy_ym, gam,
-                                                          the, alp, c->d_part, c->d_counter},
+                                                          the, alp, c->d_part, c->d_counter,
+                                                          (int)rhs_member_grid(k, 1).x, 0},
                                        rhs_member_grid(k, 1));
                 if (c->prm.scalar_on)
                     hs32[k.helm_var].add(k, HelmArgs<float>{k, c->d_coef, c->f32, nullptr, nullptr, c->d_hfac, 3},
@@ -2061,7 +2083,7 @@ int grp_build(paratc_batch* b) {
                 double2* sp = c->d_spec;
                 rhs64[K4(k.scalar_on, k.fp32_rhs, k.fp32_rhs ? 0 : k.rhs_var, 0)].add(
                     k, RhsArgs<double>{k, c->dm, c->d_coef, c->f, c->d_uy_ym, c->d_duy_ym, gam, the, alp, c->d_part,
-                                       c->d_counter},
+                                       c->d_counter, (int)rhs_member_grid(k, k.fp32_rhs).x, 0},
                     rhs_member_grid(k, k.fp32_rhs));
                 if (c->prm.scalar_on)
                     hs64[k.helm_var].add(k, HelmArgs<double>{k, c->d_coef, c->f, nullptr, nullptr, c->d_hfac, 3},
@@ -2105,6 +2127,8 @@ int grp_build(paratc_batch* b) {
         auto pj = [](cudaStream_t st, int, const DConst&, auto tab, int nblk, size_t) { launch_project_grp(st, tab, nblk); };
         // the substep's stages in the order of enqueue_substep, each stage's
         // instantiations one after another
+        grp_balance_rhs(rhs64);
+        grp_balance_rhs(rhs32);
         ok = ok && grp_emit(P, rhs64, L, rhs) && grp_emit(P, rhs32, L, rhs);
         ok = ok && grp_emit(P, hs64, L, helm) && grp_emit(P, hs32, L, helm);
         ok = ok && grp_emit(P, h64, L, helm) && grp_emit(P, h32, L, helm);

@@ -127,9 +127,10 @@ struct GrpTab {
     unsigned g[PT_MAXMEM][3];
     E e[PT_MAXMEM];
 };
-// the member of this CTA, and its block in the member's launch shape
-template <class E>
-__device__ __forceinline__ int grp_member(const GrpTab<E>* __restrict__ t, SubGrid& sg) {
+// the member of this CTA, and its block in the member's launch shape (Tab:
+// a GrpTab, or any table with the same nmem / b0 / g members)
+template <class Tab>
+__device__ __forceinline__ int grp_member(const Tab* __restrict__ t, SubGrid& sg) {
     int lo = 0, hi = t->nmem - 1;
     const int b = (int)blockIdx.x;
     while (lo < hi) {

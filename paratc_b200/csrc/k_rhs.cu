@@ -103,12 +103,19 @@ __device__ __forceinline__ int modp(int i, int n) {
 // SCALAR: with the scalar transport; T: arithmetic (double, or float for the
 // mixed and FP32 storage forms); V: storage of u, v, w, c, Hist and Rhs
 // (float only in the FP32 storage form, whose arithmetic is float)
-// G: the block this CTA works as (OwnGrid, or SubGrid in a grouped launch)
-template <bool SCALAR, class T, class V, int VAR, class G>
+// G: the block this CTA works as (OwnGrid, or SubGrid in a grouped launch).
+// MULTI (grouped launches): the member's own launch shape has nlog blocks
+// ("logical blocks"), and this CTA runs the consecutive logical blocks
+// [nlog*b/B, nlog*(b+1)/B) of the B CTAs the member has here, one after
+// another without restarting its row pipeline; it stores the flow-rate
+// partial of each logical block as that block's own CTA would, so the
+// member's records, and its result, are those of its own launch.
+template <bool SCALAR, class T, class V, int VAR, bool MULTI = false, class G>
 __device__ __forceinline__ void rhs_body(const G& grid, const DConst& c, const DMetric& m, DCoef* __restrict__ coef,
                                          const FieldSet<V>& fl, double* __restrict__ uy_ym,
                                          double* __restrict__ duy_ym, int ns, double gam, double the, double alp,
-                                         double* __restrict__ part, unsigned int* __restrict__ counter) {
+                                         double* __restrict__ part, unsigned int* __restrict__ counter,
+                                         int nlog = 0) {
     constexpr int NF = SCALAR ? 5 : 4;
     constexpr bool F64 = sizeof(T) == 8;
     static_assert(!F64 || sizeof(V) == 8, "the FP64 arithmetic form keeps FP64 fields");
@@ -133,7 +140,16 @@ __device__ __forceinline__ void rhs_body(const G& grid, const DConst& c, const D
     // covers the grid with at most one row of imbalance
     const int ntx = (nx + TX - 1) / TX, ntz = (nz + TZ - 1) / TZ;
     const long long W = (long long)ntx * ntz * ny;
-    const long long gbeg = W * grid.x() / grid.gx(), gend = W * (grid.x() + 1) / grid.gx();
+    long long gbeg = W * grid.x() / grid.gx(), gend = W * (grid.x() + 1) / grid.gx();
+    int lb = 0, lb1 = 0;      // MULTI: the logical block being run, and the end of this CTA's
+    long long lb_end = 0;     // the work index where logical block lb ends
+    if constexpr (MULTI) {
+        lb = (int)((long long)nlog * grid.x() / grid.gx());
+        lb1 = (int)((long long)nlog * (grid.x() + 1) / grid.gx());
+        gbeg = W * lb / nlog;
+        gend = W * lb1 / nlog;
+        lb_end = W * (lb + 1) / nlog;
+    }
     pdl_wait();
     pdl_trigger();
 
@@ -513,6 +529,17 @@ __device__ __forceinline__ void rhs_body(const G& grid, const DConst& c, const D
                 for (int cz = 0; cz < ZC; cz++) { u64m[cz] = u64c[cz]; u64c[cz] = u64p[cz]; u64p[cz] = u64n[cz]; }
             }
         __syncthreads();
+            if constexpr (MULTI) {
+                // row j was work item tile*ny + j - 1: a logical block ends here
+                if ((long long)tile * ny + j == lb_end && lb + 1 < lb1) {
+                    double v[1] = {s3};
+                    block_sum_store<1>(v, part + lb);
+                    __syncthreads();  // its scratch is reused by the next store
+                    s3 = 0.0;
+                    lb++;
+                    lb_end = W * (lb + 1) / nlog;
+                }
+            }
         }
 #undef LOAD_ROW32
 #undef LOAD_ROW64
@@ -531,10 +558,10 @@ __device__ __forceinline__ void rhs_body(const G& grid, const DConst& c, const D
     double s3v[1] = {s3};
     const unsigned int nblocks = grid.gx() * grid.gy() * grid.gz();
     const int bid = grid.x() + grid.gx() * (grid.y() + grid.gy() * grid.z());
-    block_sum_store<1>(s3v, part + bid);
+    block_sum_store<1>(s3v, part + (MULTI ? lb : bid));
     if (!last_block_arrive(counter, nblocks)) return;
     double tot[1];
-    reduce_records<1, false>(part, (int)nblocks, tot);
+    reduce_records<1, false>(part, MULTI ? nlog : (int)nblocks, tot);
     if (tid != 0) return;
     DCoef f = *coef;
     f.pmGamma = pmGamma;
@@ -564,17 +591,15 @@ __device__ __forceinline__ void rhs_body(const G& grid, const DConst& c, const D
     *coef = f;
 }
 
-// the arguments of one launch, read from shared memory by the FP32-arithmetic
-// forms (the grouped launch reads its member's record from there too, so a
-// member of a grouped ensemble rounds exactly as its own launch); fill(a)
+// the arguments of a grouped launch's member, read from shared memory; fill(a)
 // writes the record
-template <bool SCALAR, class T, class V, int VAR, class Fill>
+template <bool SCALAR, class T, class V, int VAR, bool MULTI, class Fill>
 __device__ __forceinline__ void rhs_from_shared(const SubGrid& g, Fill fill, int ns) {
     __shared__ RhsArgs<V> a;
     fill(a);
     __syncthreads();
-    rhs_body<SCALAR, T, V, VAR>(g, a.c, a.m, a.coef, a.fl, a.uy_ym, a.duy_ym, ns, a.gam, a.the, a.alp, a.part,
-                                a.counter);
+    rhs_body<SCALAR, T, V, VAR, MULTI>(g, a.c, a.m, a.coef, a.fl, a.uy_ym, a.duy_ym, ns, a.gam, a.the, a.alp,
+                                       a.part, a.counter, a.nlog);
 }
 
 template <bool SCALAR, class T, class V, int VAR>
@@ -582,29 +607,7 @@ __global__ void __launch_bounds__(RhsCfg<T, VAR>::NTHR, RhsCfg<T, VAR>::MINB)
     k_rhs_tile(DConst c, DMetric m, DCoef* __restrict__ coef, FieldSet<V> fl, double* __restrict__ uy_ym,
                double* __restrict__ duy_ym, int ns, double gam, double the, double alp, double* __restrict__ part,
                unsigned int* __restrict__ counter) {
-    if constexpr (sizeof(T) == 8) {
-        rhs_body<SCALAR, T, V, VAR>(OwnGrid{}, c, m, coef, fl, uy_ym, duy_ym, ns, gam, the, alp, part, counter);
-    } else {
-        const SubGrid g{blockIdx.x, blockIdx.y, blockIdx.z, gridDim.x, gridDim.y, gridDim.z};
-        rhs_from_shared<SCALAR, T, V, VAR>(
-            g,
-            [&](RhsArgs<V>& a) {
-                if (threadIdx.x == 0 && threadIdx.y == 0) {
-                    a.c = c;
-                    a.m = m;
-                    a.coef = coef;
-                    a.fl = fl;
-                    a.uy_ym = uy_ym;
-                    a.duy_ym = duy_ym;
-                    a.gam = gam;
-                    a.the = the;
-                    a.alp = alp;
-                    a.part = part;
-                    a.counter = counter;
-                }
-            },
-            ns);
-    }
+    rhs_body<SCALAR, T, V, VAR>(OwnGrid{}, c, m, coef, fl, uy_ym, duy_ym, ns, gam, the, alp, part, counter);
 }
 
 // the members of an ensemble in one launch: member i's blocks run its own
@@ -619,7 +622,7 @@ __global__ void __launch_bounds__(RhsCfg<T, VAR>::NTHR, RhsCfg<T, VAR>::MINB)
     static_assert(sizeof(RhsArgs<V>) % 8 == 0, "copied in 8-byte words");
     SubGrid g;
     const int mi = grp_member(t, g);
-    rhs_from_shared<SCALAR, T, V, VAR>(
+    rhs_from_shared<SCALAR, T, V, VAR, true>(
         g,
         [&](RhsArgs<V>& a) {
             const unsigned long long* src = reinterpret_cast<const unsigned long long*>(&t->e[mi]);
@@ -700,6 +703,10 @@ void launch_rhs_tile(cudaStream_t st, const DConst& c, const DMetric& m, DCoef* 
 dim3 rhs_member_grid(const DConst& c, int f32arith) {
     return dim3((unsigned)rhs_blocks(c, f32arith ? RhsCfg<float, 0>::MINB : RhsCfg<double, 0>::MINB));
 }
+
+long long rhs_work_rows(const DConst& c) { return (long long)((c.nx + TX - 1) / TX) * ((c.nz + TZ - 1) / TZ) * c.ny; }
+
+int rhs_wave(const DConst& c) { return RhsCfg<double, 0>::MINB * (c.nsm > 0 ? c.nsm : 148); }
 
 template <bool SCALAR, class T, int VAR, class V>
 static void rhs_grp_t(cudaStream_t st, const GrpTab<RhsArgs<V>>* t, int nblk, int ns) {

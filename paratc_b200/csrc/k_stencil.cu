@@ -63,7 +63,9 @@ __global__ void k_reduce_max(const double* __restrict__ part, int nparts, double
 // mode 0: substep; mode 1: pressure-free projection (alpha = 1, p untouched)
 // ---------------------------------------------------------------------------
 // G: the block this CTA works as (OwnGrid, or SubGrid in a grouped launch)
-template <class V, class G>
+// KZ: z planes per thread (1; the grouped launch takes 4, so that a thread
+// reads its member's constants once for four cells)
+template <class V, int KZ = 1, class G>
 __device__ __forceinline__ void project_body(const G& grid, const DConst& c, const DMetric& m,
                                              const DCoef* __restrict__ coef, int mode, const V* __restrict__ phi,
                                              V* __restrict__ ux, V* __restrict__ uy, V* __restrict__ uz,
@@ -71,10 +73,13 @@ __device__ __forceinline__ void project_body(const G& grid, const DConst& c, con
     const int nx = c.nx;
     const int i = grid.x() * blockDim.x + threadIdx.x;
     const int jc = grid.y() * blockDim.y + threadIdx.y + 1;
-    const int k = grid.z();
     pdl_wait();
     if (i >= nx || jc > c.ny) return;
     const double alpha = mode == 0 ? coef->pmAlpha : 1.0;
+#pragma unroll
+    for (int kk = 0; kk < KZ; kk++) {
+    const int k = grid.z() * KZ + kk;
+    if (KZ > 1 && k >= c.nz) break;
     const size_t pl = (size_t)c.nyt * nx;
     const size_t r0 = (size_t)jc * nx, zc = (size_t)k * pl;
     const int is = wrapi(i - 2, nx), im = wrapi(i - 1, nx), ip = wrapi(i + 1, nx);
@@ -111,6 +116,7 @@ __device__ __forceinline__ void project_body(const G& grid, const DConst& c, con
         if (jc == 1) pr[q - nx] = pn;
         if (jc == c.ny) pr[q + nx] = pn;
     }
+    }
 }
 
 template <class V>
@@ -121,11 +127,12 @@ __global__ void __launch_bounds__(256) k_project(DConst c, DMetric m, const DCoe
     project_body(OwnGrid{}, c, m, coef, mode, phi, ux, uy, uz, pr, uy_ym);
 }
 
+constexpr int PROJ_KZ = 4;
 template <class V>
 __global__ void __launch_bounds__(256) k_project_grp(const GrpTab<ProjArgs<V>>* __restrict__ t) {
     SubGrid g;
     const ProjArgs<V>& a = t->e[grp_member(t, g)];
-    project_body(g, a.c, a.m, a.coef, 0, a.phi, a.ux, a.uy, a.uz, a.pr, a.uy_ym);
+    project_body<V, PROJ_KZ>(g, a.c, a.m, a.coef, 0, a.phi, a.ux, a.uy, a.uz, a.pr, a.uy_ym);
 }
 
 // ---------------------------------------------------------------------------
@@ -584,7 +591,10 @@ void launch_residual(cudaStream_t st, const DConst& c, const DMetric& m, const d
 size_t endstep_blocks(const DConst& c) { return (size_t)2 * (c.nsm > 0 ? c.nsm : 148); }
 
 // grouped launches (one member's shape: its own launch's)
-dim3 cell_member_grid(const DConst& c) { return cell_grid(c); }
+dim3 cell_member_grid(const DConst& c) {
+    const dim3 g = cell_grid(c);
+    return dim3(g.x, g.y, (g.z + PROJ_KZ - 1) / PROJ_KZ);  // the grouped projection's shape
+}
 dim3 endstep_member_grid(const DConst& c) { return dim3((unsigned)endstep_blocks(c)); }
 void launch_project_grp(cudaStream_t st, const GrpTab<ProjArgs<double>>* t, int nblk) {
     launch_pdl(k_project_grp<double>, dim3((unsigned)nblk), cell_block(), 0, st, t);

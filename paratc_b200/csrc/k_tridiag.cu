@@ -171,8 +171,10 @@ __host__ __device__ inline int helm_stride(int ny) { return 3 * (ny + 2); }
 // memory; rows are addressed by pointer steps; the wall rows need no case of
 // their own in the sweeps (a(1) = 0, arr(ny+1) = 0, and clcU2Hat's row-1
 // value is substituted before the sweep and its result after it).
-// G: the block this CTA works as (OwnGrid, or SubGrid in a grouped launch)
-template <class V, int HU, class G>
+// G: the block this CTA works as (OwnGrid, or SubGrid in a grouped launch).
+// Z4: the grouped launch's CTA shape, 32 columns of 4 z planes (one per
+// warp), so that a narrow member (nx < 128) leaves no warp idle
+template <class V, int HU, bool Z4 = false, class G>
 __device__ __forceinline__ void helm_body(const G& grid, const DConst& cst, const DCoef* __restrict__ coef, int comp0,
                                           const FieldSet<V>& fl, const double* __restrict__ duy_ym,
                                           const double* __restrict__ uy_ym, const double* __restrict__ facs) {
@@ -191,9 +193,9 @@ __device__ __forceinline__ void helm_body(const G& grid, const DConst& cst, cons
     const double* SA = shf;
     const double* SR = shf + (ny + 2);
     const double* SW = shf + 2 * (ny + 2);
-    const int i = (grid.x() * 4 + threadIdx.y) * 32 + threadIdx.x;
-    const int k = grid.y();
-    if (i >= nx) return;
+    const int i = Z4 ? (int)grid.x() * 32 + (int)threadIdx.x : (int)(grid.x() * 4 + threadIdx.y) * 32 + (int)threadIdx.x;
+    const int k = Z4 ? (int)grid.y() * 4 + (int)threadIdx.y : (int)grid.y();
+    if (i >= nx || (Z4 && k >= cst.nz)) return;
     V* u;
     V* rhs;
     double add = 0.0;
@@ -317,7 +319,7 @@ template <class V, int HU>
 __global__ void __launch_bounds__(128, 4) k_helm_grp(const GrpTab<HelmArgs<V>>* __restrict__ t) {
     SubGrid g;
     const HelmArgs<V>& a = t->e[grp_member(t, g)];
-    helm_body<V, HU>(g, a.c, a.coef, a.comp0, a.fl, a.duy_ym, a.uy_ym, a.fac);
+    helm_body<V, HU, true>(g, a.c, a.coef, a.comp0, a.fl, a.duy_ym, a.uy_ym, a.fac);
 }
 
 // ---------------------------------------------------------------------------
@@ -764,7 +766,9 @@ void launch_helm_factors(cudaStream_t st, const DConst& c, const DMetric& m, con
                alp[0], alp[1], alp[2], fac);
 }
 
-dim3 helm_member_grid(const DConst& c, int ncomp) { return dim3((c.nx + 127) / 128, c.nz, ncomp); }
+static dim3 helm_grid(const DConst& c, int ncomp) { return dim3((c.nx + 127) / 128, c.nz, ncomp); }
+// the grouped launch's shape (32 columns x 4 z planes per CTA)
+dim3 helm_member_grid(const DConst& c, int ncomp) { return dim3((c.nx + 31) / 32, (c.nz + 3) / 4, ncomp); }
 size_t helm_smem(const DConst& c) { return helm_stride(c.ny) * sizeof(double); }
 
 template <class V>
@@ -784,7 +788,7 @@ template <class V>
 static void helm_dispatch(cudaStream_t st, const DConst& c, const DCoef* coef, int comp0, int ncomp,
                           const FieldSet<V>& f, const double* duy_ym, const double* uy_ym, const double* fac) {
     dim3 blk(32, 4);
-    dim3 grd = helm_member_grid(c, ncomp);
+    dim3 grd = helm_grid(c, ncomp);
     // rows per chunk: FP64 8 (variant 1: 4); float storage, whose ring takes
     // half the registers, 16 (variant 1: 8)
     constexpr int H0 = sizeof(V) == 4 ? 2 * HY_U : HY_U;

@@ -215,6 +215,8 @@ struct RhsArgs {  // k_rhs_tile
     double gam, the, alp;  // the substep's RK3 coefficients
     double* part;
     unsigned int* counter;
+    int nlog;  // blocks of the member's own launch (its flow-rate records)
+    int pad;
 };
 template <class V>
 struct HelmArgs {  // k_helm, components comp0 .. comp0 + grid z - 1
@@ -281,6 +283,8 @@ struct EndArgs {  // k_endstep with the next step's clcCFL
 // key: the member whose DConst selects the instantiation (scalar_on,
 // fp32_rhs, rhs_var, helm_var, nx, nz, ...); nblk: the table's total CTAs
 dim3 rhs_member_grid(const DConst& c, int f32arith);
+long long rhs_work_rows(const DConst& c);  // (tile, row) work items of the right-hand side
+int rhs_wave(const DConst& c);             // resident right-hand-side CTAs of the device
 void launch_rhs_grp(cudaStream_t st, const DConst& key, const GrpTab<RhsArgs<double>>* t, int nblk, int ns);
 void launch_rhs_grp(cudaStream_t st, const DConst& key, const GrpTab<RhsArgs<float>>* t, int nblk, int ns);
 dim3 helm_member_grid(const DConst& c, int ncomp);
