@@ -388,7 +388,9 @@ int paratc_get_precision(paratc_ctx* ctx, int* prec);
  * where the rows are 16-byte aligned.
  * paratc_create picks a schedule by rule; paratc_autotune times nrep solves
  * in the step's form (divergence source, transforms, y-solve, inverse with
- * the Neumann ghosts; the state is not touched) for every supported choice,
+ * the Neumann ghosts; the state is not touched; in the context's storage
+ * form, so an FP32-storage context times the float2 solve and skips the
+ * generic transforms) for every supported choice,
  * in three interleaved rounds (each choice keeps its fastest round, so a
  * clock that drifts during the search favours none), writes the times (ms
  * for nrep solves, -1 where unsupported) to

@@ -311,6 +311,9 @@ void enqueue_poisson_head32(paratc_ctx* ctx, int mode, double* out_max) {
     if (ctx->plane)
         launch_plane_f(st, mode, ctx->kc, ctx->dm, ctx->d_coef, ctx->f32, nullptr, spec32(ctx), ctx->d_twx,
                        ctx->d_postx, ctx->d_twz, ctx->d_part, ctx->d_counter + 1, out_max);
+    else if (ctx->xdiv)
+        launch_xf_div(st, mode, ctx->kc, ctx->dm, ctx->d_coef, ctx->f32, spec32(ctx), ctx->d_twx, ctx->d_postx,
+                      ctx->d_part, ctx->d_counter + 1, out_max, ctx->d_zt_err);
     else
         launch_pfft_xf(st, mode, ctx->kc, ctx->dm, ctx->d_coef, ctx->f32, nullptr, spec32(ctx), ctx->d_twx,
                        ctx->d_postx, ctx->d_part, ctx->d_counter + 1, out_max);
@@ -329,8 +332,15 @@ void enqueue_poisson_tail32(paratc_ctx* ctx, float* out, int padded) {
     { PROF(PK_FFTZ_F); launch_pfft_z(st, -1, ctx->nx, ctx->ny, ctx->nz, spec32(ctx), ctx->d_twz); }
     { PROF(PK_YSOLVE); launch_ysolve_fac(st, ctx->kc, ctx->dm, spec32(ctx), ctx->d_pfac); }
     { PROF(PK_FFTZ_B); launch_pfft_z(st, +1, ctx->nx, ctx->ny, ctx->nz, spec32(ctx), ctx->d_twz); }
-    { PROF(PK_FFTX_B); launch_pfft_xb(st, ctx->nx, ctx->ny, ctx->nz, spec32(ctx), out, ctx->d_twx, ctx->d_postx,
-                                      ctx->hm.normfft, padded); }
+    if (ctx->xtma && aligned16(out)) {
+        PROF(PK_FFTX_B);
+        launch_xb_tma(st, ctx->nx, ctx->ny, ctx->nz, spec32(ctx), out, ctx->d_twx, ctx->d_postx, ctx->hm.normfft,
+                      padded, ctx->kc.nsm, ctx->d_zt_err);
+    } else {
+        PROF(PK_FFTX_B);
+        launch_pfft_xb(st, ctx->nx, ctx->ny, ctx->nz, spec32(ctx), out, ctx->d_twx, ctx->d_postx, ctx->hm.normfft,
+                       padded);
+    }
     ctx->launches += 4;
 }
 
@@ -1193,13 +1203,21 @@ int paratc_autotune(paratc_ctx* ctx, int nrep, int* choice, double* times_ms) {
         for (int q = 0; q < PARATC_SCHED_NCHOICES && rc == PARATC_OK; q++) {
             const int c = (q + round * 3) % PARATC_SCHED_NCHOICES;  // another order each round
             if (!sched_supported(ctx, c)) continue;
+            const bool f32 = ctx->prec == PARATC_PREC_FP32;
+            if (f32 && c / 2 == 2) continue;  // the generic transforms have no float2 form
             sched_apply(ctx, c);
             // the step's form of the solve: divergence source, transforms,
-            // y-solve, inverse into phi with its Neumann ghosts (state untouched)
+            // y-solve, inverse into phi with its Neumann ghosts (state
+            // untouched), in the context's storage form
             for (int r = 0; r < nrep + 1; r++) {
                 if (r == 1) cudaEventRecord(e0, ctx->st);
-                enqueue_poisson_head(ctx, 1, nullptr, ctx->d_scal);
-                enqueue_poisson_tail(ctx, ctx->d_phi, 1);
+                if (f32) {
+                    enqueue_poisson_head32(ctx, 1, ctx->d_scal);
+                    enqueue_poisson_tail32(ctx, ctx->d_phi32, 1);
+                } else {
+                    enqueue_poisson_head(ctx, 1, nullptr, ctx->d_scal);
+                    enqueue_poisson_tail(ctx, ctx->d_phi, 1);
+                }
             }
             cudaEventRecord(e1, ctx->st);
             rc = sync(ctx);

@@ -181,6 +181,134 @@ __global__ void __launch_bounds__(XT<N>::P, XT<N>::MINB)
     }
 }
 
+// The inverse of the FP32 storage form: float2 spectrum rows in, float phi
+// rows out, the merge, the passes and the scaling in double as above.  A
+// float2 row has N+1 (odd) values, so a row starts 16-byte aligned only at
+// an even index: rows are loaded two at a time (the batches hold an even
+// number of rows and start at an even row; a batch's odd last row is loaded
+// with the one float2 after it, inside the spectrum's allocation, which
+// holds the FP64 spectrum's bytes).  The float rows land at the start of the
+// stage and are widened by a merge that reads all its inputs before the
+// barrier and writes the double2 rows after it; the phi rows leave through
+// coalesced stores of the threads.
+template <int N>
+__global__ void __launch_bounds__(XT<N>::P, XT<N>::MINB)
+    k_xb_tma32(int nrows, int ny, const float2* __restrict__ spec, float* __restrict__ phi,
+               const double2* __restrict__ twN, const double2* __restrict__ post, double scale, int padded,
+               unsigned int* __restrict__ err) {
+    constexpr int B = XT<N>::B, P = XT<N>::P, PITCH = XT<N>::PITCH, M1 = N + 1;
+    static_assert(B % 2 == 0, "row pairs");
+    constexpr int NPAIR = B * (N / 2 + 1);
+    constexpr int KP = (NPAIR + P - 1) / P;  // merge pairs per thread
+    constexpr unsigned SB = XT<N>::STAGE;
+    constexpr ff::Sched SC = ff::make_sched(N);
+    extern __shared__ __align__(128) unsigned char smraw[];
+    double2* stage[2] = {reinterpret_cast<double2*>(smraw), reinterpret_cast<double2*>(smraw) + SB};
+    __shared__ unsigned long long mbar[2];
+    __shared__ int s_bad;
+    const int tid = threadIdx.x;
+    const long long lim = tma::wait_limit(err);
+    const int nb = (nrows + B - 1) / B;
+    const int nx = 2 * N, nyt = ny + 2;
+    if (tid == 0) {
+        tma::mbar_init(&mbar[0], 1);
+        tma::mbar_init(&mbar[1], 1);
+        tma::fence_mbar_init();
+        s_bad = 0;
+    }
+    __syncthreads();
+    pdl_wait();
+    pdl_trigger();
+    auto issue = [&](int s, int bt) {
+        const int g0 = bt * B, nv = min(B, nrows - g0);
+        float2* fs = reinterpret_cast<float2*>(stage[s]);
+        unsigned bytes = 0;
+        for (int b = 0; b < nv; b += 2) bytes += (unsigned)(b + 1 < nv ? 2 * M1 : M1 + 1) * (unsigned)sizeof(float2);
+        tma::mbar_expect_tx(&mbar[s], bytes);
+        for (int b = 0; b < nv; b += 2) {
+            const unsigned n2 = (unsigned)(b + 1 < nv ? 2 * M1 : M1 + 1) * (unsigned)sizeof(float2);
+            tma::bulk_load(fs + b * M1, spec + (size_t)(g0 + b) * M1, n2, &mbar[s]);
+        }
+    };
+    if (tid == 0) {
+        if ((int)blockIdx.x < nb) issue(0, blockIdx.x);
+        if ((int)(blockIdx.x + gridDim.x) < nb) issue(1, blockIdx.x + gridDim.x);
+    }
+    int it = 0;
+    for (int bt = blockIdx.x; bt < nb; bt += gridDim.x, it++) {
+        const int s = it & 1;
+        double2* buf = stage[s];
+        const float2* fs = reinterpret_cast<const float2*>(buf);
+        if (__syncthreads_or(tma::mbar_wait(&mbar[s], (unsigned)((it >> 1) & 1), lim) ? 0 : 1)) {
+            s_bad = 1;
+            break;
+        }
+        const int g0 = bt * B, nv = min(B, nrows - g0);
+        // merge, reading every float input first (the double2 rows overlay them)
+        float2 xa_[KP], xb_[KP];
+#pragma unroll
+        for (int k = 0; k < KP; k++) {
+            const int f = tid + k * P;
+            if (f < NPAIR) {
+                const int a = f / B, b = f - a * B;
+                xa_[k] = fs[b * M1 + a];
+                xb_[k] = fs[b * M1 + (N - a)];
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < KP; k++) {
+            const int f = tid + k * P;
+            if (f >= NPAIR) continue;
+            const int a = f / B, b = f - a * B;
+            const int bn = N - a;
+            double2* rb = buf + b * PITCH;
+            double2 xa = make_double2(xa_[k].x, xa_[k].y), xb = make_double2(xb_[k].x, xb_[k].y);
+            if (a == 0) { xa.y = 0.0; xb.y = 0.0; }
+            const double2 e2a = make_double2(xa.x + xb.x, xa.y - xb.y);
+            const double2 da = make_double2(xa.x - xb.x, xa.y + xb.y);
+            const double2 o2a = cmulc(da, __ldg(&post[a]));
+            const double2 za = make_double2(scale * (e2a.x - o2a.y), scale * (e2a.y + o2a.x));
+            if (a == 0) {
+                rb[0] = za;
+            } else {
+                const double2 e2b = make_double2(xb.x + xa.x, xb.y - xa.y);
+                const double2 db = make_double2(xb.x - xa.x, xb.y + xa.y);
+                const double2 o2b = cmulc(db, __ldg(&post[bn]));
+                rb[a] = za;
+                if (bn != a) rb[bn] = make_double2(scale * (e2b.x - o2b.y), scale * (e2b.y + o2b.x));
+            }
+        }
+        __syncthreads();
+        ff::smem_passes<N, B, PITCH, P, 1, 0, SC.np, 4, true, 0, XT<N>::SWZ>(buf, twN, tid);
+        __syncthreads();
+        // phi rows (and the Neumann ghost copies) by coalesced float2 stores
+        for (int e = tid; e < nv * N; e += P) {
+            const int b = e / N, i = e - b * N;
+            const double2 z = buf[b * PITCH + i];
+            const float2 v = make_float2((float)z.x, (float)z.y);
+            const int g = g0 + b;
+            if (!padded) {
+                reinterpret_cast<float2*>(phi + (size_t)g * nx)[i] = v;
+                continue;
+            }
+            const int k = g / ny, jc = g - k * ny + 1;
+            float2* rowp = reinterpret_cast<float2*>(phi + ((size_t)k * nyt + jc) * nx);
+            rowp[i] = v;
+            if (jc == 1) rowp[i - N] = v;
+            if (jc == ny) rowp[i + N] = v;
+        }
+        // the stage's generic reads are done before the next bulk load writes it
+        tma::fence_async_smem();
+        __syncthreads();
+        if (tid == 0) {
+            const int bn = bt + 2 * gridDim.x;
+            if (bn < nb) issue(s, bn);
+        }
+    }
+    if (tid == 0 && s_bad) xt_fail(mbar, it, nb, err);
+}
+
 template <int N>
 __global__ void __launch_bounds__(XT<N>::P, XT<N>::MINB)
     k_xf_tma(int nrows, const double* __restrict__ src, double2* __restrict__ spec, const double2* __restrict__ twN,
@@ -311,10 +439,14 @@ struct XD {
     static constexpr size_t smem = 2 * (size_t)STAGE * sizeof(double2);
 };
 
-template <int N>
+// V: storage of the velocity, S: of the spectrum.  The FP32 storage form
+// (float, float2) writes the spectrum rows with the consumers' own coalesced
+// stores: a float2 row of N+1 values starts 16-byte aligned only at even
+// rows, which a bulk store needs.
+template <int N, class V, class S>
 __global__ void __launch_bounds__(XD<N>::NT, 1)
-    k_xf_div(int mode, DConst c, DMetric m, const DCoef* __restrict__ coef, const double* __restrict__ ux,
-             const double* __restrict__ uy, const double* __restrict__ uz, double2* __restrict__ spec,
+    k_xf_div(int mode, DConst c, DMetric m, const DCoef* __restrict__ coef, const V* __restrict__ ux,
+             const V* __restrict__ uy, const V* __restrict__ uz, S* __restrict__ spec,
              const double2* __restrict__ twN, const double2* __restrict__ post, double* __restrict__ part,
              unsigned int* __restrict__ counter, double* __restrict__ out_max, unsigned int* __restrict__ err) {
     constexpr int B = XD<N>::B, P = XD<N>::P, PITCH = XD<N>::PITCH, M1 = N + 1, Q = XD_Q;
@@ -369,6 +501,30 @@ __global__ void __launch_bounds__(XD<N>::NT, 1)
                 break;
             }
             ff::smem_passes<N, B, PITCH, P, -1, 0, SC.np, 4, true, 1, N % 8 == 0>(buf, twN, tid);
+            if constexpr (sizeof(S) != sizeof(double2)) {
+                // the split straight to the float2 spectrum rows (consecutive
+                // threads take consecutive modes of one row: coalesced stores)
+                const int g0 = bt * B, nv = min(B, nrows - g0);
+                for (int f = tid; f < nv * (N / 2 + 1); f += P) {
+                    const int b = f / (N / 2 + 1), a = f - b * (N / 2 + 1);
+                    const int bn = N - a;
+                    const double2* rb = buf + b * PITCH;
+                    S* out = spec + (size_t)(g0 + b) * M1;
+                    const double2 za = rb[a], zb = rb[a == 0 ? 0 : bn];
+                    const double2 E = make_double2(0.5 * (za.x + zb.x), 0.5 * (za.y - zb.y));
+                    const double2 O = make_double2(0.5 * (za.y + zb.y), -0.5 * (za.x - zb.x));
+                    st_c(out + a, cadd(E, cmul(__ldg(&post[a]), O)));
+                    if (a == 0) {
+                        st_c(out + N, cadd(E, cmul(__ldg(&post[N]), O)));
+                    } else if (bn != a) {
+                        const double2 E2 = make_double2(0.5 * (zb.x + za.x), 0.5 * (zb.y - za.y));
+                        const double2 O2 = make_double2(0.5 * (zb.y + za.y), -0.5 * (zb.x - za.x));
+                        st_c(out + bn, cadd(E2, cmul(__ldg(&post[bn]), O2)));
+                    }
+                }
+                ff::group_sync<1, P>();  // every consumer has read the stage
+                if (tid == 0) tma::mbar_arrive(&empty[s]);
+            } else {
             for (int f = tid; f < B * (N / 2 + 1); f += P) {
                 const int a = f / B, b = f - a * B;
                 const int bn = N - a;
@@ -394,10 +550,12 @@ __global__ void __launch_bounds__(XD<N>::NT, 1)
             if (tid == 0) {
                 const int g0 = bt * B, nv = min(B, nrows - g0);
                 for (int b = 0; b < nv; b++)
-                    tma::bulk_store(spec + (size_t)(g0 + b) * M1, buf + b * PITCH, M1 * (unsigned)sizeof(double2));
+                    tma::bulk_store(reinterpret_cast<double2*>(spec) + (size_t)(g0 + b) * M1, buf + b * PITCH,
+                                    M1 * (unsigned)sizeof(double2));
                 tma::bulk_commit();
                 tma::bulk_wait_read0();  // the stores have read the stage
                 tma::mbar_arrive(&empty[s]);
+            }
             }
         }
         if (tid == 0) tma::bulk_wait0();
@@ -438,8 +596,11 @@ bool xt_tma_supported(int n) {
 void xt_tma_init() {
 #define X_CASE(n)                                                                                              \
     cudaFuncSetAttribute(k_xb_tma<n>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)XT<n>::smem);          \
+    cudaFuncSetAttribute(k_xb_tma32<n>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)XT<n>::smem);        \
     cudaFuncSetAttribute(k_xf_tma<n>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)XT<n>::smem);       \
-    cudaFuncSetAttribute(k_xf_div<n>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)XD<n>::smem);
+    cudaFuncSetAttribute(k_xf_div<n, double, double2>, cudaFuncAttributeMaxDynamicSharedMemorySize,          \
+                         (int)XD<n>::smem);                                                                    \
+    cudaFuncSetAttribute(k_xf_div<n, float, float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)XD<n>::smem);
     XT_SIZES(X_CASE)
 #undef X_CASE
 }
@@ -452,6 +613,21 @@ void launch_xb_tma(cudaStream_t st, int nx, int ny, int nz, const double2* spec,
     case n:                                                                                                    \
         launch_pdl(k_xb_tma<n>, dim3(xt_grid<n>(nrows, nsm)), dim3(XT<n>::P), XT<n>::smem, st, nrows, ny, spec, \
                    phi, twx, post, scale, padded, err);                                                        \
+        break;
+        XT_SIZES(X_CASE)
+#undef X_CASE
+        default: break;
+    }
+}
+
+void launch_xb_tma(cudaStream_t st, int nx, int ny, int nz, const float2* spec, float* phi, const double2* twx,
+                   const double2* post, double scale, int padded, int nsm, unsigned int* err) {
+    const int nrows = ny * nz;
+    switch (nx / 2) {
+#define X_CASE(n)                                                                                              \
+    case n:                                                                                                    \
+        launch_pdl(k_xb_tma32<n>, dim3(xt_grid<n>(nrows, nsm)), dim3(XT<n>::P), XT<n>::smem, st, nrows, ny,   \
+                   spec, phi, twx, post, scale, padded, err);                                                  \
         break;
         XT_SIZES(X_CASE)
 #undef X_CASE
@@ -488,21 +664,32 @@ int xf_div_grid(int n, int nrows, int nsm) {
     return nb < nsm ? nb : nsm;
 }
 
-void launch_xf_div(cudaStream_t st, int mode, const DConst& c, const DMetric& m, const DCoef* coef, const Fields& f,
-                   double2* spec, const double2* twx, const double2* post, double* part, unsigned int* counter,
-                   double* out_max, unsigned int* err) {
+template <class V, class S>
+static void xf_div_t(cudaStream_t st, int mode, const DConst& c, const DMetric& m, const DCoef* coef,
+                     const FieldSet<V>& f, S* spec, const double2* twx, const double2* post, double* part,
+                     unsigned int* counter, double* out_max, unsigned int* err) {
     const int nrows = c.ny * c.nz;
     const int grid = xf_div_grid(c.nx / 2, nrows, c.nsm > 0 ? c.nsm : 148);
     switch (c.nx / 2) {
 #define X_CASE(n)                                                                                              \
     case n:                                                                                                    \
-        launch_pdl(k_xf_div<n>, dim3(grid), dim3(XD<n>::NT), XD<n>::smem, st, mode, c, m, coef, f.ux, f.uy, f.uz, \
-                   spec, twx, post, part, counter, out_max, err);                                              \
+        launch_pdl(k_xf_div<n, V, S>, dim3(grid), dim3(XD<n>::NT), XD<n>::smem, st, mode, c, m, coef, f.ux, f.uy, \
+                   f.uz, spec, twx, post, part, counter, out_max, err);                                        \
         break;
         XT_SIZES(X_CASE)
 #undef X_CASE
         default: break;
     }
+}
+void launch_xf_div(cudaStream_t st, int mode, const DConst& c, const DMetric& m, const DCoef* coef, const Fields& f,
+                   double2* spec, const double2* twx, const double2* post, double* part, unsigned int* counter,
+                   double* out_max, unsigned int* err) {
+    xf_div_t(st, mode, c, m, coef, f, spec, twx, post, part, counter, out_max, err);
+}
+void launch_xf_div(cudaStream_t st, int mode, const DConst& c, const DMetric& m, const DCoef* coef,
+                   const Fields32& f, float2* spec, const double2* twx, const double2* post, double* part,
+                   unsigned int* counter, double* out_max, unsigned int* err) {
+    xf_div_t(st, mode, c, m, coef, f, spec, twx, post, part, counter, out_max, err);
 }
 
 }  // namespace ptc

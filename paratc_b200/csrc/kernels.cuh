@@ -146,12 +146,19 @@ void launch_xb_tma(cudaStream_t st, int nx, int ny, int nz, const double2* spec,
                    const double2* post, double scale, int padded, int nsm, unsigned int* err);
 void launch_xf_tma(cudaStream_t st, int nx, int ny, int nz, const double* src, double2* spec, const double2* twx,
                    const double2* post, int nsm, unsigned int* err);
+// FP32 storage form: float2 spectrum rows in (two per bulk copy), float phi out
+void launch_xb_tma(cudaStream_t st, int nx, int ny, int nz, const float2* spec, float* phi, const double2* twx,
+                   const double2* post, double scale, int padded, int nsm, unsigned int* err);
 // the divergence source of clcPrSrc (mode 0: / pmAlpha, 1: unscaled) and its
 // forward x transform, warp-specialised (one CTA per SM; grid records to part)
 int xf_div_grid(int n, int nrows, int nsm);
 void launch_xf_div(cudaStream_t st, int mode, const DConst& c, const DMetric& m, const DCoef* coef, const Fields& f,
                    double2* spec, const double2* twx, const double2* post, double* part, unsigned int* counter,
                    double* out_max, unsigned int* err);
+// FP32 storage form: float velocity in, float2 spectrum rows out
+void launch_xf_div(cudaStream_t st, int mode, const DConst& c, const DMetric& m, const DCoef* coef,
+                   const Fields32& f, float2* spec, const double2* twx, const double2* post, double* part,
+                   unsigned int* counter, double* out_max, unsigned int* err);
 
 // k_plane.cu: both transforms of a y-plane in one CTA (planes that fit shared memory)
 bool plane_supported(int nx, int nz);

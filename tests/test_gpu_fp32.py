@@ -81,9 +81,10 @@ def _case(name):
     return cases.small_channel(64, 48, 64) if name == "channel_64" else variant(name)
 
 
-# the plane transforms (schedule 0), the separate x / z transforms (3), and
-# the default schedule of smaller variants (scalar, CFL-controlled dt, AB2)
-@pytest.mark.parametrize("name,schedule", [("channel_64", 0), ("channel_64", 3), ("channel", -1),
+# the plane transforms (schedule 0), the separate x / z transforms (3), the
+# divergence-fed x transform (8), and the default schedule of smaller
+# variants (scalar, CFL-controlled dt, AB2)
+@pytest.mark.parametrize("name,schedule", [("channel_64", 0), ("channel_64", 3), ("channel_64", 8), ("channel", -1),
                                            ("halfchannel_scalar", -1), ("channel_cfl", -1), ("channel_ab2", -1)])
 def test_fp32_storage_steps_track_fp64(name, schedule):
     case = _case(name)
