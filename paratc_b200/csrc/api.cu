@@ -329,10 +329,12 @@ void enqueue_poisson_tail32(paratc_ctx* ctx, float* out, int padded) {
         ctx->launches += 2;
         return;
     }
-    { PROF(PK_FFTZ_F); launch_pfft_z(st, -1, ctx->nx, ctx->ny, ctx->nz, spec32(ctx), ctx->d_twz); }
+    { PROF(PK_FFTZ_F); launch_pfft_z(st, -1, ctx->nx, ctx->ny, ctx->nz, spec32(ctx), ctx->d_twz, 1); }
     { PROF(PK_YSOLVE); launch_ysolve_fac(st, ctx->kc, ctx->dm, spec32(ctx), ctx->d_pfac); }
-    { PROF(PK_FFTZ_B); launch_pfft_z(st, +1, ctx->nx, ctx->ny, ctx->nz, spec32(ctx), ctx->d_twz); }
-    if (ctx->xtma && aligned16(out)) {
+    { PROF(PK_FFTZ_B); launch_pfft_z(st, +1, ctx->nx, ctx->ny, ctx->nz, spec32(ctx), ctx->d_twz, 1); }
+    // (the bulk-copy-fed kernel loads the odd-length float2 rows in pairs: an
+    // even row count, which every compiled nz gives)
+    if (ctx->xtma && aligned16(out) && (ctx->ny * ctx->nz) % 2 == 0) {
         PROF(PK_FFTX_B);
         launch_xb_tma(st, ctx->nx, ctx->ny, ctx->nz, spec32(ctx), out, ctx->d_twx, ctx->d_postx, ctx->hm.normfft,
                       padded, ctx->kc.nsm, ctx->d_zt_err);
@@ -359,9 +361,9 @@ void enqueue_solve32(paratc_ctx* ctx, const double* src, double* phi, int accumu
         return;
     }
     { PROF(PK_FFTX_F); launch_pfft_xf(st, ctx->kc, src, spec32(ctx), ctx->d_twx, ctx->d_postx); }
-    { PROF(PK_FFTZ_F); launch_pfft_z(st, -1, ctx->nx, ctx->ny, ctx->nz, spec32(ctx), ctx->d_twz); }
+    { PROF(PK_FFTZ_F); launch_pfft_z(st, -1, ctx->nx, ctx->ny, ctx->nz, spec32(ctx), ctx->d_twz, 0); }
     { PROF(PK_YSOLVE); launch_ysolve_fac(st, ctx->kc, ctx->dm, spec32(ctx), ctx->d_pfac); }
-    { PROF(PK_FFTZ_B); launch_pfft_z(st, +1, ctx->nx, ctx->ny, ctx->nz, spec32(ctx), ctx->d_twz); }
+    { PROF(PK_FFTZ_B); launch_pfft_z(st, +1, ctx->nx, ctx->ny, ctx->nz, spec32(ctx), ctx->d_twz, 0); }
     { PROF(PK_FFTX_B); launch_pfft_xb(st, ctx->nx, ctx->ny, ctx->nz, spec32(ctx), phi, ctx->d_twx, ctx->d_postx,
                                       ctx->hm.normfft, accumulate, shift); }
     ctx->launches += 5;

@@ -185,4 +185,33 @@ __device__ __forceinline__ double2 cmulc(double2 a, double2 b) {  // a * conj(b)
 __device__ __forceinline__ double2 cconj(double2 a) { return make_double2(a.x, -a.y); }
 __device__ __forceinline__ double2 cscale(double2 a, double s) { return make_double2(a.x * s, a.y * s); }
 
+// the same for float2 (the FP32 arithmetic of the transforms)
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ float2 cmulc(float2 a, float2 b) {
+    return make_float2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
+}
+
+// a complex type's real type and constructor, and conversions between the
+// two complex types
+template <class C>
+struct Cx;
+template <>
+struct Cx<double2> {
+    using R = double;
+    static __device__ __forceinline__ double2 make(double x, double y) { return make_double2(x, y); }
+};
+template <>
+struct Cx<float2> {
+    using R = float;
+    static __device__ __forceinline__ float2 make(float x, float y) { return make_float2(x, y); }
+};
+template <class C, class D>
+__device__ __forceinline__ C cto(D v) {
+    return Cx<C>::make((typename Cx<C>::R)v.x, (typename Cx<C>::R)v.y);
+}
+
 }  // namespace ptc

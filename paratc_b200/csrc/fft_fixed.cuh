@@ -79,49 +79,54 @@ __host__ __device__ constexpr double s16(int k) { return c16(k - 4); }
 
 // v * exp(DIR 2 pi i k / M) for M in {2, 4, 8, 16}, with the trivial angles
 // done exactly
-template <int M, int K, int DIR>
-__device__ __forceinline__ double2 rot(double2 v) {
+// (C: double2, or float2 for the FP32 arithmetic of the FP32 storage form;
+// the constants are rounded to C's real type)
+template <int M, int K, int DIR, class C>
+__device__ __forceinline__ C rot(C v) {
+    using R = typename Cx<C>::R;
     constexpr int k16 = (K * (16 / M)) & 15;
     if constexpr (k16 == 0) return v;
-    else if constexpr (k16 == 8) return make_double2(-v.x, -v.y);
-    else if constexpr (k16 == 4) return DIR < 0 ? make_double2(v.y, -v.x) : make_double2(-v.y, v.x);
-    else if constexpr (k16 == 12) return DIR < 0 ? make_double2(-v.y, v.x) : make_double2(v.y, -v.x);
+    else if constexpr (k16 == 8) return Cx<C>::make(-v.x, -v.y);
+    else if constexpr (k16 == 4) return DIR < 0 ? Cx<C>::make(v.y, -v.x) : Cx<C>::make(-v.y, v.x);
+    else if constexpr (k16 == 12) return DIR < 0 ? Cx<C>::make(-v.y, v.x) : Cx<C>::make(v.y, -v.x);
     else {
-        constexpr double c = c16(k16), s = DIR * s16(k16);
-        return make_double2(v.x * c - v.y * s, v.x * s + v.y * c);
+        constexpr R c = (R)c16(k16), s = (R)(DIR * s16(k16));
+        return Cx<C>::make(v.x * c - v.y * s, v.x * s + v.y * c);
     }
 }
 
-template <int DIR>
-__device__ __forceinline__ void dft2(double2* v) {
-    const double2 t = v[0];
+template <int DIR, class C>
+__device__ __forceinline__ void dft2(C* v) {
+    const C t = v[0];
     v[0] = cadd(t, v[1]);
     v[1] = csub(t, v[1]);
 }
 
-template <int DIR>
-__device__ __forceinline__ void dft3(double2* v) {
-    const double c = -0.5, s = DIR * 0.86602540378443864676;  // cos, sin of 2 pi / 3
-    const double2 t1 = cadd(v[1], v[2]), t2 = csub(v[1], v[2]);
-    const double2 mm = make_double2(v[0].x + c * t1.x, v[0].y + c * t1.y);
-    const double2 it = make_double2(-s * t2.y, s * t2.x);
+template <int DIR, class C>
+__device__ __forceinline__ void dft3(C* v) {
+    using R = typename Cx<C>::R;
+    const R c = (R)-0.5, s = (R)(DIR * 0.86602540378443864676);  // cos, sin of 2 pi / 3
+    const C t1 = cadd(v[1], v[2]), t2 = csub(v[1], v[2]);
+    const C mm = Cx<C>::make(v[0].x + c * t1.x, v[0].y + c * t1.y);
+    const C it = Cx<C>::make(-s * t2.y, s * t2.x);
     v[0] = cadd(v[0], t1);
     v[1] = cadd(mm, it);
     v[2] = csub(mm, it);
 }
 
-template <int DIR>
-__device__ __forceinline__ void dft5(double2* v) {
-    const double c1 = 0.30901699437494742410, c2 = -0.80901699437494742410;  // cos 2pi/5, cos 4pi/5
-    const double s1 = DIR * 0.95105651629515357212, s2 = DIR * 0.58778525229247312917;
-    const double2 a1 = cadd(v[1], v[4]), b1 = csub(v[1], v[4]);
-    const double2 a2 = cadd(v[2], v[3]), b2 = csub(v[2], v[3]);
-    const double2 m1 = make_double2(v[0].x + c1 * a1.x + c2 * a2.x, v[0].y + c1 * a1.y + c2 * a2.y);
-    const double2 m2 = make_double2(v[0].x + c2 * a1.x + c1 * a2.x, v[0].y + c2 * a1.y + c1 * a2.y);
-    const double2 n1 = make_double2(s1 * b1.x + s2 * b2.x, s1 * b1.y + s2 * b2.y);
-    const double2 n2 = make_double2(s2 * b1.x - s1 * b2.x, s2 * b1.y - s1 * b2.y);
-    const double2 in1 = make_double2(-n1.y, n1.x), in2 = make_double2(-n2.y, n2.x);
-    v[0] = make_double2(v[0].x + a1.x + a2.x, v[0].y + a1.y + a2.y);
+template <int DIR, class C>
+__device__ __forceinline__ void dft5(C* v) {
+    using R = typename Cx<C>::R;
+    const R c1 = (R)0.30901699437494742410, c2 = (R)-0.80901699437494742410;  // cos 2pi/5, cos 4pi/5
+    const R s1 = (R)(DIR * 0.95105651629515357212), s2 = (R)(DIR * 0.58778525229247312917);
+    const C a1 = cadd(v[1], v[4]), b1 = csub(v[1], v[4]);
+    const C a2 = cadd(v[2], v[3]), b2 = csub(v[2], v[3]);
+    const C m1 = Cx<C>::make(v[0].x + c1 * a1.x + c2 * a2.x, v[0].y + c1 * a1.y + c2 * a2.y);
+    const C m2 = Cx<C>::make(v[0].x + c2 * a1.x + c1 * a2.x, v[0].y + c2 * a1.y + c1 * a2.y);
+    const C n1 = Cx<C>::make(s1 * b1.x + s2 * b2.x, s1 * b1.y + s2 * b2.y);
+    const C n2 = Cx<C>::make(s2 * b1.x - s1 * b2.x, s2 * b1.y - s1 * b2.y);
+    const C in1 = Cx<C>::make(-n1.y, n1.x), in2 = Cx<C>::make(-n2.y, n2.x);
+    v[0] = Cx<C>::make(v[0].x + a1.x + a2.x, v[0].y + a1.y + a2.y);
     v[1] = cadd(m1, in1);
     v[4] = csub(m1, in1);
     v[2] = cadd(m2, in2);
@@ -130,24 +135,24 @@ __device__ __forceinline__ void dft5(double2* v) {
 
 // radix-2 combination of the half-length DFTs of the even (E) and odd (O)
 // samples: X[k] = E[k] + W^k O[k], X[k + H] = E[k] - W^k O[k], W = exp(DIR 2 pi i / 2H)
-template <int H, int DIR, int K = 0>
-__device__ __forceinline__ void combine(const double2* E, const double2* O, double2* X) {
+template <int H, int DIR, int K = 0, class C>
+__device__ __forceinline__ void combine(const C* E, const C* O, C* X) {
     if constexpr (K < H) {
-        const double2 t = rot<2 * H, K, DIR>(O[K]);
+        const C t = rot<2 * H, K, DIR>(O[K]);
         X[K] = cadd(E[K], t);
         X[K + H] = csub(E[K], t);
         combine<H, DIR, K + 1>(E, O, X);
     }
 }
 
-template <int R, int DIR>
-__device__ __forceinline__ void dft(double2* v) {
+template <int R, int DIR, class C>
+__device__ __forceinline__ void dft(C* v) {
     if constexpr (R == 2) dft2<DIR>(v);
     else if constexpr (R == 3) dft3<DIR>(v);
     else if constexpr (R == 5) dft5<DIR>(v);
     else {
         constexpr int H = R / 2;
-        double2 e[H], o[H];
+        C e[H], o[H];
 #pragma unroll
         for (int q = 0; q < H; q++) { e[q] = v[2 * q]; o[q] = v[2 * q + 1]; }
         dft<H, DIR>(e);
@@ -185,13 +190,14 @@ __device__ __forceinline__ bool group_any(bool pred) {
 // sequences of length N, P threads.  LD(e, b) loads element e of sequence b,
 // ST(e, b, v) stores it; SYNC_MID puts a block barrier between all loads and
 // all stores (an in-place pass on shared memory).  tw: exp(-2 pi i m / N).
-template <int N, int B, int P, int R, int NS, int DIR, bool SYNC_MID, class LD, class ST, int BAR = 0>
-__device__ __forceinline__ void pass(const LD& ld, const ST& st, const double2* tw, int tid) {
+template <int N, int B, int P, int R, int NS, int DIR, bool SYNC_MID, class LD, class ST, int BAR = 0,
+          class C = double2>
+__device__ __forceinline__ void pass(const LD& ld, const ST& st, const C* tw, int tid) {
     constexpr int NB = N / R;
     constexpr int TOT = B * NB;
     constexpr int PER = (TOT + P - 1) / P;
     constexpr int TS = N / (NS * R);
-    double2 v[PER][R];
+    C v[PER][R];
     int jb[PER];
 #pragma unroll
     for (int u = 0; u < PER; u++) {
@@ -205,7 +211,7 @@ __device__ __forceinline__ void pass(const LD& ld, const ST& st, const double2* 
             if constexpr (NS > 1) {
 #pragma unroll
                 for (int r = 1; r < R; r++) {
-                    const double2 w = tw[kk * r * TS];
+                    const C w = tw[kk * r * TS];
                     v[u][r] = (DIR < 0) ? cmul(v[u][r], w) : cmulc(v[u][r], w);
                 }
             }
@@ -225,15 +231,15 @@ __device__ __forceinline__ void pass(const LD& ld, const ST& st, const double2* 
 }
 
 // shared-memory accessors of the layout buf[e*PITCH + b]
-template <int PITCH>
+template <int PITCH, class C = double2>
 struct SmemLd {
-    const double2* buf;
-    __device__ __forceinline__ double2 operator()(int e, int b) const { return buf[e * PITCH + b]; }
+    const C* buf;
+    __device__ __forceinline__ C operator()(int e, int b) const { return buf[e * PITCH + b]; }
 };
-template <int PITCH>
+template <int PITCH, class C = double2>
 struct SmemSt {
-    double2* buf;
-    __device__ __forceinline__ void operator()(int e, int b, double2 v) const { buf[e * PITCH + b] = v; }
+    C* buf;
+    __device__ __forceinline__ void operator()(int e, int b, C v) const { buf[e * PITCH + b] = v; }
 };
 
 // shared-memory accessors with the sequence index major: element e of
@@ -243,15 +249,15 @@ struct SmemSt {
 // the lanes' consecutive j, all in one bank group when R is 8 or 16) and the
 // loads of the next one both spread over the eight bank groups
 __device__ __forceinline__ int swz8(int e) { return e ^ ((e >> 3) & 7); }
-template <int PITCH, bool SWZ = false>
+template <int PITCH, bool SWZ = false, class C = double2>
 struct SmemLdT {
-    const double2* buf;
-    __device__ __forceinline__ double2 operator()(int e, int b) const { return buf[b * PITCH + (SWZ ? swz8(e) : e)]; }
+    const C* buf;
+    __device__ __forceinline__ C operator()(int e, int b) const { return buf[b * PITCH + (SWZ ? swz8(e) : e)]; }
 };
-template <int PITCH, bool SWZ = false>
+template <int PITCH, bool SWZ = false, class C = double2>
 struct SmemStT {
-    double2* buf;
-    __device__ __forceinline__ void operator()(int e, int b, double2 v) const { buf[b * PITCH + (SWZ ? swz8(e) : e)] = v; }
+    C* buf;
+    __device__ __forceinline__ void operator()(int e, int b, C v) const { buf[b * PITCH + (SWZ ? swz8(e) : e)] = v; }
 };
 
 // passes S..END-1 in place on shared memory, each followed by a barrier;
@@ -261,8 +267,8 @@ struct SmemStT {
 // swizzled order: pass 0 reads plain and writes swizzled, the last pass
 // reads swizzled and writes plain
 template <int N, int B, int PITCH, int P, int DIR, int S, int END, int MAXBITS = 4, bool TRANSPOSED = false,
-          int BAR = 0, bool SWZ = false>
-__device__ __forceinline__ void smem_passes(double2* buf, const double2* tw, int tid) {
+          int BAR = 0, bool SWZ = false, class C = double2>
+__device__ __forceinline__ void smem_passes(C* buf, const C* tw, int tid) {
     constexpr Sched SC = make_sched(N, MAXBITS);
     static_assert(!SWZ || (TRANSPOSED && N % 8 == 0), "the swizzle permutes whole groups of eight");
     if constexpr (S < END) {
@@ -270,13 +276,13 @@ __device__ __forceinline__ void smem_passes(double2* buf, const double2* tw, int
         constexpr int NS = sched_ns(N, S, MAXBITS);
         constexpr bool SIN = SWZ && S > 0, SOUT = SWZ && S + 1 < END;
         if constexpr (TRANSPOSED)
-            pass<N, B, P, R, NS, DIR, true, SmemLdT<PITCH, SIN>, SmemStT<PITCH, SOUT>, BAR>(
-                SmemLdT<PITCH, SIN>{buf}, SmemStT<PITCH, SOUT>{buf}, tw, tid);
+            pass<N, B, P, R, NS, DIR, true, SmemLdT<PITCH, SIN, C>, SmemStT<PITCH, SOUT, C>, BAR>(
+                SmemLdT<PITCH, SIN, C>{buf}, SmemStT<PITCH, SOUT, C>{buf}, tw, tid);
         else
-            pass<N, B, P, R, NS, DIR, true, SmemLd<PITCH>, SmemSt<PITCH>, BAR>(SmemLd<PITCH>{buf},
-                                                                             SmemSt<PITCH>{buf}, tw, tid);
+            pass<N, B, P, R, NS, DIR, true, SmemLd<PITCH, C>, SmemSt<PITCH, C>, BAR>(SmemLd<PITCH, C>{buf},
+                                                                                   SmemSt<PITCH, C>{buf}, tw, tid);
         group_sync<BAR, P>();
-        smem_passes<N, B, PITCH, P, DIR, S + 1, END, MAXBITS, TRANSPOSED, BAR, SWZ>(buf, tw, tid);
+        smem_passes<N, B, PITCH, P, DIR, S + 1, END, MAXBITS, TRANSPOSED, BAR, SWZ, C>(buf, tw, tid);
     }
 }
 

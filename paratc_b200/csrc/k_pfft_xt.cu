@@ -20,6 +20,8 @@
 // Every wait is bounded: after kSpinLimit polls the CTA records an error
 // (*err |= 2, or 4 for k_xf_div), waits (bounded) for its own copies in
 // flight and stops.  No multicast; only this GPU's memory.
+#include <type_traits>
+
 #include "common.cuh"
 #include "fft_fixed.cuh"
 #include "kernels.cuh"
@@ -182,14 +184,16 @@ __global__ void __launch_bounds__(XT<N>::P, XT<N>::MINB)
 }
 
 // The inverse of the FP32 storage form: float2 spectrum rows in, float phi
-// rows out, the merge, the passes and the scaling in double as above.  A
-// float2 row has N+1 (odd) values, so a row starts 16-byte aligned only at
-// an even index: rows are loaded two at a time (the batches hold an even
-// number of rows and start at an even row; a batch's odd last row is loaded
-// with the one float2 after it, inside the spectrum's allocation, which
-// holds the FP64 spectrum's bytes).  The float rows land at the start of the
-// stage and are widened by a merge that reads all its inputs before the
-// barrier and writes the double2 rows after it; the phi rows leave through
+// rows out, the merge and the passes in float (the stages hold float2, half
+// the FP64 stage, and the float2 twiddles sit after them).  A float2 row has
+// N+1 (odd) values, so a row starts 16-byte aligned only at an even index:
+// rows are loaded two at a time (the batches hold an even number of rows and
+// start at an even row, and the host launches the kernel for an even row
+// count only; an odd last row would be loaded with the one float2 after it,
+// inside the spectrum's allocation, which holds the FP64 spectrum's bytes).
+// The rows land contiguously at the start of the stage
+// and are moved to the pitched layout by the merge, which reads all its
+// inputs before a barrier and writes after it; the phi rows leave through
 // coalesced stores of the threads.
 template <int N>
 __global__ void __launch_bounds__(XT<N>::P, XT<N>::MINB)
@@ -201,15 +205,18 @@ __global__ void __launch_bounds__(XT<N>::P, XT<N>::MINB)
     constexpr int NPAIR = B * (N / 2 + 1);
     constexpr int KP = (NPAIR + P - 1) / P;  // merge pairs per thread
     constexpr unsigned SB = XT<N>::STAGE;
+    static_assert(2 * SB >= (unsigned)N, "the twiddles fit after the float2 stages");
     constexpr ff::Sched SC = ff::make_sched(N);
     extern __shared__ __align__(128) unsigned char smraw[];
-    double2* stage[2] = {reinterpret_cast<double2*>(smraw), reinterpret_cast<double2*>(smraw) + SB};
+    float2* stage[2] = {reinterpret_cast<float2*>(smraw), reinterpret_cast<float2*>(smraw) + SB};
+    float2* tws = reinterpret_cast<float2*>(smraw) + 2 * SB;
     __shared__ unsigned long long mbar[2];
     __shared__ int s_bad;
     const int tid = threadIdx.x;
     const long long lim = tma::wait_limit(err);
     const int nb = (nrows + B - 1) / B;
     const int nx = 2 * N, nyt = ny + 2;
+    for (int t = tid; t < N; t += P) tws[t] = cto<float2>(twN[t]);
     if (tid == 0) {
         tma::mbar_init(&mbar[0], 1);
         tma::mbar_init(&mbar[1], 1);
@@ -221,38 +228,37 @@ __global__ void __launch_bounds__(XT<N>::P, XT<N>::MINB)
     pdl_trigger();
     auto issue = [&](int s, int bt) {
         const int g0 = bt * B, nv = min(B, nrows - g0);
-        float2* fs = reinterpret_cast<float2*>(stage[s]);
         unsigned bytes = 0;
         for (int b = 0; b < nv; b += 2) bytes += (unsigned)(b + 1 < nv ? 2 * M1 : M1 + 1) * (unsigned)sizeof(float2);
         tma::mbar_expect_tx(&mbar[s], bytes);
         for (int b = 0; b < nv; b += 2) {
             const unsigned n2 = (unsigned)(b + 1 < nv ? 2 * M1 : M1 + 1) * (unsigned)sizeof(float2);
-            tma::bulk_load(fs + b * M1, spec + (size_t)(g0 + b) * M1, n2, &mbar[s]);
+            tma::bulk_load(stage[s] + b * M1, spec + (size_t)(g0 + b) * M1, n2, &mbar[s]);
         }
     };
     if (tid == 0) {
         if ((int)blockIdx.x < nb) issue(0, blockIdx.x);
         if ((int)(blockIdx.x + gridDim.x) < nb) issue(1, blockIdx.x + gridDim.x);
     }
+    const float fsc = (float)scale;
     int it = 0;
     for (int bt = blockIdx.x; bt < nb; bt += gridDim.x, it++) {
         const int s = it & 1;
-        double2* buf = stage[s];
-        const float2* fs = reinterpret_cast<const float2*>(buf);
+        float2* buf = stage[s];
         if (__syncthreads_or(tma::mbar_wait(&mbar[s], (unsigned)((it >> 1) & 1), lim) ? 0 : 1)) {
             s_bad = 1;
             break;
         }
         const int g0 = bt * B, nv = min(B, nrows - g0);
-        // merge, reading every float input first (the double2 rows overlay them)
+        // merge, reading every input first (the pitched rows overlay them)
         float2 xa_[KP], xb_[KP];
 #pragma unroll
         for (int k = 0; k < KP; k++) {
             const int f = tid + k * P;
             if (f < NPAIR) {
                 const int a = f / B, b = f - a * B;
-                xa_[k] = fs[b * M1 + a];
-                xb_[k] = fs[b * M1 + (N - a)];
+                xa_[k] = buf[b * M1 + a];
+                xb_[k] = buf[b * M1 + (N - a)];
             }
         }
         __syncthreads();
@@ -262,31 +268,31 @@ __global__ void __launch_bounds__(XT<N>::P, XT<N>::MINB)
             if (f >= NPAIR) continue;
             const int a = f / B, b = f - a * B;
             const int bn = N - a;
-            double2* rb = buf + b * PITCH;
-            double2 xa = make_double2(xa_[k].x, xa_[k].y), xb = make_double2(xb_[k].x, xb_[k].y);
-            if (a == 0) { xa.y = 0.0; xb.y = 0.0; }
-            const double2 e2a = make_double2(xa.x + xb.x, xa.y - xb.y);
-            const double2 da = make_double2(xa.x - xb.x, xa.y + xb.y);
-            const double2 o2a = cmulc(da, __ldg(&post[a]));
-            const double2 za = make_double2(scale * (e2a.x - o2a.y), scale * (e2a.y + o2a.x));
+            float2* rb = buf + b * PITCH;
+            float2 xa = xa_[k], xb = xb_[k];
+            if (a == 0) { xa.y = 0.f; xb.y = 0.f; }
+            const float2 e2a = make_float2(xa.x + xb.x, xa.y - xb.y);
+            const float2 da = make_float2(xa.x - xb.x, xa.y + xb.y);
+            const float2 o2a = cmulc(da, cto<float2>(__ldg(&post[a])));
+            const float2 za = make_float2(fsc * (e2a.x - o2a.y), fsc * (e2a.y + o2a.x));
             if (a == 0) {
                 rb[0] = za;
             } else {
-                const double2 e2b = make_double2(xb.x + xa.x, xb.y - xa.y);
-                const double2 db = make_double2(xb.x - xa.x, xb.y + xa.y);
-                const double2 o2b = cmulc(db, __ldg(&post[bn]));
+                const float2 e2b = make_float2(xb.x + xa.x, xb.y - xa.y);
+                const float2 db = make_float2(xb.x - xa.x, xb.y + xa.y);
+                const float2 o2b = cmulc(db, cto<float2>(__ldg(&post[bn])));
                 rb[a] = za;
-                if (bn != a) rb[bn] = make_double2(scale * (e2b.x - o2b.y), scale * (e2b.y + o2b.x));
+                if (bn != a) rb[bn] = make_float2(fsc * (e2b.x - o2b.y), fsc * (e2b.y + o2b.x));
             }
         }
         __syncthreads();
-        ff::smem_passes<N, B, PITCH, P, 1, 0, SC.np, 4, true, 0, XT<N>::SWZ>(buf, twN, tid);
+        ff::smem_passes<N, B, PITCH, P, 1, 0, SC.np, 4, true, 0, XT<N>::SWZ>(buf, static_cast<const float2*>(tws),
+                                                                             tid);
         __syncthreads();
         // phi rows (and the Neumann ghost copies) by coalesced float2 stores
         for (int e = tid; e < nv * N; e += P) {
             const int b = e / N, i = e - b * N;
-            const double2 z = buf[b * PITCH + i];
-            const float2 v = make_float2((float)z.x, (float)z.y);
+            const float2 v = buf[b * PITCH + i];
             const int g = g0 + b;
             if (!padded) {
                 reinterpret_cast<float2*>(phi + (size_t)g * nx)[i] = v;
@@ -451,16 +457,28 @@ __global__ void __launch_bounds__(XD<N>::NT, 1)
              unsigned int* __restrict__ counter, double* __restrict__ out_max, unsigned int* __restrict__ err) {
     constexpr int B = XD<N>::B, P = XD<N>::P, PITCH = XD<N>::PITCH, M1 = N + 1, Q = XD_Q;
     static_assert(P % 32 == 0, "the consumer group is whole warps");
+    // the passes' complex type: float2 for the FP32 storage form (the stages
+    // hold float2, half the FP64 stage, and the float2 twiddles sit after
+    // them), double2 otherwise (the twiddles read from the global table)
+    using A = std::conditional_t<sizeof(S) == sizeof(float2), float2, double2>;
+    constexpr bool F32 = sizeof(A) == sizeof(float2);
     constexpr unsigned SB = XD<N>::STAGE;
+    static_assert(!F32 || 2 * SB >= (unsigned)N, "the twiddles fit after the float2 stages");
     constexpr ff::Sched SC = ff::make_sched(N);
     extern __shared__ __align__(128) unsigned char smraw[];
-    double2* stage[2] = {reinterpret_cast<double2*>(smraw), reinterpret_cast<double2*>(smraw) + SB};
+    A* stage[2] = {reinterpret_cast<A*>(smraw), reinterpret_cast<A*>(smraw) + SB};
+    float2* tws32 = reinterpret_cast<float2*>(smraw) + 2 * SB;
     __shared__ unsigned long long full[2], empty[2];
     __shared__ int bad_c, bad_p;
     const int tid = threadIdx.x;
     const int nrows = c.ny * c.nz;
     const int nb = (nrows + B - 1) / B;
     const long long lim = tma::wait_limit(err);
+    if constexpr (F32)
+        for (int t = tid; t < N; t += XD<N>::NT) tws32[t] = cto<float2>(twN[t]);
+    const A* tw;
+    if constexpr (F32) tw = reinterpret_cast<const A*>(tws32);
+    else tw = reinterpret_cast<const A*>(twN);
     if (tid == 0) {
         tma::mbar_init(&full[0], Q);
         tma::mbar_init(&full[1], Q);
@@ -485,9 +503,9 @@ __global__ void __launch_bounds__(XD<N>::NT, 1)
                 bad_p = 1;
                 break;
             }
-            double2* buf = stage[s];
+            A* buf = stage[s];
             div_batch<N, B, Q, XD_DIV_U>(c, m, ux, uy, uz, bt * B, nrows, sudtal, tp, dm,
-                                         [&](int b, int e, double2 v) { buf[b * PITCH + e] = v; });
+                                         [&](int b, int e, double2 v) { buf[b * PITCH + e] = cto<A>(v); });
             tma::mbar_arrive(&full[s]);
         }
     } else {
@@ -495,12 +513,12 @@ __global__ void __launch_bounds__(XD<N>::NT, 1)
         int it = 0;
         for (int bt = blockIdx.x; bt < nb; bt += gridDim.x, it++) {
             const int s = it & 1;
-            double2* buf = stage[s];
+            A* buf = stage[s];
             if (ff::group_any<1, P>(!tma::mbar_wait(&full[s], (unsigned)((it >> 1) & 1), lim))) {
                 bad_c = 1;
                 break;
             }
-            ff::smem_passes<N, B, PITCH, P, -1, 0, SC.np, 4, true, 1, N % 8 == 0>(buf, twN, tid);
+            ff::smem_passes<N, B, PITCH, P, -1, 0, SC.np, 4, true, 1, N % 8 == 0>(buf, tw, tid);
             if constexpr (sizeof(S) != sizeof(double2)) {
                 // the split straight to the float2 spectrum rows (consecutive
                 // threads take consecutive modes of one row: coalesced stores)
@@ -508,18 +526,19 @@ __global__ void __launch_bounds__(XD<N>::NT, 1)
                 for (int f = tid; f < nv * (N / 2 + 1); f += P) {
                     const int b = f / (N / 2 + 1), a = f - b * (N / 2 + 1);
                     const int bn = N - a;
-                    const double2* rb = buf + b * PITCH;
+                    const A* rb = buf + b * PITCH;
                     S* out = spec + (size_t)(g0 + b) * M1;
-                    const double2 za = rb[a], zb = rb[a == 0 ? 0 : bn];
-                    const double2 E = make_double2(0.5 * (za.x + zb.x), 0.5 * (za.y - zb.y));
-                    const double2 O = make_double2(0.5 * (za.y + zb.y), -0.5 * (za.x - zb.x));
-                    st_c(out + a, cadd(E, cmul(__ldg(&post[a]), O)));
+                    const A za = rb[a], zb = rb[a == 0 ? 0 : bn];
+                    const float h = 0.5f;
+                    const A E = Cx<A>::make(h * (za.x + zb.x), h * (za.y - zb.y));
+                    const A O = Cx<A>::make(h * (za.y + zb.y), -h * (za.x - zb.x));
+                    out[a] = cto<S>(cadd(E, cmul(cto<A>(__ldg(&post[a])), O)));
                     if (a == 0) {
-                        st_c(out + N, cadd(E, cmul(__ldg(&post[N]), O)));
+                        out[N] = cto<S>(cadd(E, cmul(cto<A>(__ldg(&post[N])), O)));
                     } else if (bn != a) {
-                        const double2 E2 = make_double2(0.5 * (zb.x + za.x), 0.5 * (zb.y - za.y));
-                        const double2 O2 = make_double2(0.5 * (zb.y + za.y), -0.5 * (zb.x - za.x));
-                        st_c(out + bn, cadd(E2, cmul(__ldg(&post[bn]), O2)));
+                        const A E2 = Cx<A>::make(h * (zb.x + za.x), h * (zb.y - za.y));
+                        const A O2 = Cx<A>::make(h * (zb.y + za.y), -h * (zb.x - za.x));
+                        out[bn] = cto<S>(cadd(E2, cmul(cto<A>(__ldg(&post[bn])), O2)));
                     }
                 }
                 ff::group_sync<1, P>();  // every consumer has read the stage
@@ -528,7 +547,7 @@ __global__ void __launch_bounds__(XD<N>::NT, 1)
             for (int f = tid; f < B * (N / 2 + 1); f += P) {
                 const int a = f / B, b = f - a * B;
                 const int bn = N - a;
-                double2* rb = buf + b * PITCH;
+                A* rb = buf + b * PITCH;
                 const double2 za = rb[a], zb = rb[a == 0 ? 0 : bn];
                 const double2 E = make_double2(0.5 * (za.x + zb.x), 0.5 * (za.y - zb.y));
                 const double2 O = make_double2(0.5 * (za.y + zb.y), -0.5 * (za.x - zb.x));

@@ -199,7 +199,9 @@ void launch_pfft_xf(cudaStream_t st, int mode, const DConst& c, const DMetric& m
                     double* part, unsigned int* counter, double* out_max);
 void launch_pfft_xb(cudaStream_t st, int nx, int ny, int nz, const float2* spec, float* phi, const double2* twx,
                     const double2* post, double scale, int padded);
-void launch_pfft_z(cudaStream_t st, int dir, int nx, int ny, int nz, float2* spec, const double2* twz);
+// f32arith: the passes in float (the FP32 storage form's step), else in
+// double (the refined solve)
+void launch_pfft_z(cudaStream_t st, int dir, int nx, int ny, int nz, float2* spec, const double2* twz, int f32arith);
 // the refined solve: an FP64 source array into a float2 spectrum, and the
 // inverse into an FP64 potential (compact rows), added to it when accumulate != 0
 void launch_pfft_xf(cudaStream_t st, const DConst& c, const double* src, float2* spec, const double2* twx,
