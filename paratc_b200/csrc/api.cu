@@ -70,6 +70,8 @@ struct paratc_ctx {
     bool xtma = false;     // x transforms through the bulk-copy-fed persistent kernels (split path)
     bool xdiv = false;     // the divergence source by producer warps of the forward x transform
     alignas(64) unsigned char zt_tmap[128];  // its tensor map (a CUtensorMap)
+    alignas(64) unsigned char zt_tmap32[128];  // the same over the float2 spectrum of the FP32 storage form
+    bool ztma32_ok = false;                    // that map is encoded (ncol even, nz supported)
     unsigned int* d_zt_err = nullptr;        // set by a TMA-fed kernel whose bounded wait ran out
     int sched_gen = 0;   // bumped whenever the Poisson schedule changes (captured graphs hold the old one)
     double* d_pfac = nullptr;   // pivots of the spectral y systems (1/vecm, then arr), computed once
@@ -329,9 +331,13 @@ void enqueue_poisson_tail32(paratc_ctx* ctx, float* out, int padded) {
         ctx->launches += 2;
         return;
     }
-    { PROF(PK_FFTZ_F); launch_pfft_z(st, -1, ctx->nx, ctx->ny, ctx->nz, spec32(ctx), ctx->d_twz, 1); }
+    const int ncol = ctx->ny * (ctx->nx / 2 + 1);
+    const bool zt = ctx->ztma && ctx->ztma32_ok;
+    if (zt) { PROF(PK_FFTZ_F); launch_zt_tma32(st, -1, ncol, ctx->nz, ctx->zt_tmap32, ctx->d_twz, ctx->kc.nsm, ctx->d_zt_err); }
+    else { PROF(PK_FFTZ_F); launch_pfft_z(st, -1, ctx->nx, ctx->ny, ctx->nz, spec32(ctx), ctx->d_twz, 1); }
     { PROF(PK_YSOLVE); launch_ysolve_fac(st, ctx->kc, ctx->dm, spec32(ctx), ctx->d_pfac); }
-    { PROF(PK_FFTZ_B); launch_pfft_z(st, +1, ctx->nx, ctx->ny, ctx->nz, spec32(ctx), ctx->d_twz, 1); }
+    if (zt) { PROF(PK_FFTZ_B); launch_zt_tma32(st, +1, ncol, ctx->nz, ctx->zt_tmap32, ctx->d_twz, ctx->kc.nsm, ctx->d_zt_err); }
+    else { PROF(PK_FFTZ_B); launch_pfft_z(st, +1, ctx->nx, ctx->ny, ctx->nz, spec32(ctx), ctx->d_twz, 1); }
     // (the bulk-copy-fed kernel loads the odd-length float2 rows in pairs: an
     // even row count, which every compiled nz gives)
     if (ctx->xtma && aligned16(out) && (ctx->ny * ctx->nz) % 2 == 0) {
@@ -531,6 +537,8 @@ int alloc_fp32(paratc_ctx* ctx) {
             if ((rc = dalloc(ctx, q, ctx->nf))) return rc;
     }
     g.pr = ctx->f.pr;  // the pressure stays FP64
+    if (ctx->pfft && zt_tma_supported(ctx->nz))
+        ctx->ztma32_ok = zt_tma_prepare(spec32(ctx), ctx->ny * (ctx->nx / 2 + 1), ctx->nz, ctx->zt_tmap32);
     return PARATC_OK;
 }
 

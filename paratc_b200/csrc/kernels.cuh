@@ -135,6 +135,10 @@ void launch_visu(cudaStream_t st, int q, int iskip, int jskip, int kskip, int no
 bool zt_tma_supported(int nz);
 void zt_tma_init();
 bool zt_tma_prepare(double2* spec, int ncol, int nz, void* tmap_out);
+// the FP32 storage form's float2 spectrum (float passes); needs ncol even
+bool zt_tma_prepare(float2* spec, int ncol, int nz, void* tmap_out);
+void launch_zt_tma32(cudaStream_t st, int dir, int ncol, int nz, const void* tmap, const double2* twz, int nsm,
+                     unsigned int* err);
 void launch_zt_tma(cudaStream_t st, int dir, int ncol, int nz, const void* tmap, const double2* twz, int nsm,
                    unsigned int* err);
 

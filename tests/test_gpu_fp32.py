@@ -19,6 +19,7 @@ import pytest
 
 from oracle import oracle_lib as ol
 from paratc_b200 import cases
+from paratc_b200.abi import FT_HC
 from paratc_b200.lib import ChannelSystem
 
 from .helpers import fields_of, rel_err, variant, yp_of
@@ -78,13 +79,20 @@ def _pair(case):
 
 
 def _case(name):
-    return cases.small_channel(64, 48, 64) if name == "channel_64" else variant(name)
+    if name == "channel_64":
+        return cases.small_channel(64, 48, 64)
+    if name == "channel_z128":  # TMA-fed z transforms (nz >= 128) on the float2 spectrum
+        return cases.small_channel(32, 24, 128)
+    if name == "channel_z128_odd":  # ny * (nx/2+1) odd (a half channel): no float2 map, register-fed z
+        return cases.small_channel(32, 25, 128, flow_type=FT_HC, xnu=1e-3, yly=1.0, is_ux_const=0)
+    return variant(name)
 
 
 # the plane transforms (schedule 0), the separate x / z transforms (3), the
-# divergence-fed x transform (8), and the default schedule of smaller
-# variants (scalar, CFL-controlled dt, AB2)
-@pytest.mark.parametrize("name,schedule", [("channel_64", 0), ("channel_64", 3), ("channel_64", 8), ("channel", -1),
+# divergence-fed x transform (8), the TMA-fed z transforms (6), and the
+# default schedule of smaller variants (scalar, CFL-controlled dt, AB2)
+@pytest.mark.parametrize("name,schedule", [("channel_64", 0), ("channel_64", 3), ("channel_64", 8), ("channel_z128", 6),
+                                           ("channel_z128_odd", 6), ("channel", -1),
                                            ("halfchannel_scalar", -1), ("channel_cfl", -1), ("channel_ab2", -1)])
 def test_fp32_storage_steps_track_fp64(name, schedule):
     case = _case(name)
