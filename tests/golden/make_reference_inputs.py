@@ -4,7 +4,7 @@ fixtures of the namelist reader (paratc_params_from_namelist and friends).
 The reference ships no tests; these input decks are the only files it holds
 whose parse is known: the values a Fortran NAMELIST read gives are the ones
 written in them.  Run from the repository root with the reference checked
-out at REF (default /root/reference); it writes the four files below and
+out at REF (default /root/reference); it writes the files below and
 reference_inputs.sha256 (their SHA-256 digests).  The copies are verbatim.
 """
 import hashlib
@@ -19,6 +19,9 @@ FILES = {
     "Input/GravityFlow/GravityFlow.prm": "GravityFlow.prm",
     "Input/GravityFlow/GravityFlow.small": "GravityFlow.small",
     "Input/StratifiedFlow/SF_Ri000.prm": "SF_Ri000.prm",
+    "Input/StratifiedFlow/SF_Ri018.prm": "SF_Ri018.prm",
+    "Input/StratifiedFlow/SF_Ri120.prm": "SF_Ri120.prm",
+    "Input/StratifiedFlow/SF_Ri480.prm": "SF_Ri480.prm",
 }
 
 

@@ -122,6 +122,23 @@ REF_INPUTS = {
 }
 
 
+def _sf(ubulk, ucrf, dom, grid, geff, ilast, name, k):
+    """A stratified-flow deck: SF_Ri000's values with the ones that deck changes."""
+    d = dict(REF_INPUTS["SF_Ri000.prm"])
+    d.update(ubulk=ubulk, ucrf=ucrf, dom=dom, grid=grid)
+    d["sc"] = dict(d["sc"], geff=geff)
+    d["run"] = (1, ilast, 0, 12000, 5, name, b"./CFD/Results%d/" % k, b"./CFD/Restart%d/" % k)
+    return d
+
+
+REF_INPUTS["SF_Ri018.prm"] = _sf(0.75, 0.6, (25.13274123, 2.0, 12.56637061), (512, 128, 512), 0.03168852775, 60000,
+                                 b"Ri018_", 2)
+REF_INPUTS["SF_Ri120.prm"] = _sf(1.0, 0.6, (25.13274123, 2.0, 12.56637061), (512, 128, 512), 0.2112568517, 60000,
+                                 b"Ri120_", 3)
+REF_INPUTS["SF_Ri480.prm"] = _sf(1.6, 1.0, (56.54866776, 2.0, 25.13274123), (1152, 128, 1024), 0.8450274067, 90000,
+                                 b"Ri480_", 4)
+
+
 @pytest.mark.parametrize("fname", sorted(REF_INPUTS))
 def test_namelist_reader_on_reference_inputs(fname):
     """paratc_params_from_namelist, paratc_run_options_from_namelist and
