@@ -47,6 +47,10 @@ struct XK {
     static constexpr int P = ff::Shape<N>::P;
     static constexpr int PITCH = B + 1;  // odd pitch: row-order accesses hit distinct banks
     static constexpr size_t smem = ((size_t)(N + 1) * PITCH + N) * sizeof(A);
+    // resident CTAs the launch bounds of k_xf ask for: 24 warps per SM (80
+    // registers, a few spills; the FP32 form's k_xf<64> at C1 went from 0.14
+    // to 0.17 of the HBM peak)
+    static constexpr int MINB = 768 / P;
 };
 
 // V: storage of the velocity (mode 0/1), S: storage of the spectrum; the
@@ -114,7 +118,7 @@ __device__ __forceinline__ void xf_body(const G& grid, int mode, const DConst& c
 }
 
 template <int N, class V, class S, class A>
-__global__ void __launch_bounds__(XK<N, A>::P)
+__global__ void __launch_bounds__(XK<N, A>::P, XK<N, A>::MINB)
     k_xf(int mode, DConst c, DMetric m, const DCoef* __restrict__ coef, const V* __restrict__ ux,
          const V* __restrict__ uy, const V* __restrict__ uz, const double* __restrict__ src,
          S* __restrict__ spec, const double2* __restrict__ twN, const double2* __restrict__ post,

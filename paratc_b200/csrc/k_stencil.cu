@@ -119,12 +119,15 @@ __device__ __forceinline__ void project_body(const G& grid, const DConst& c, con
     }
 }
 
+// z planes per thread of the one-context projection (2 measured slower at
+// C1: 0.596 of the HBM peak against 0.648)
+constexpr int PROJ_KZ1 = 1;
 template <class V>
 __global__ void __launch_bounds__(256) k_project(DConst c, DMetric m, const DCoef* __restrict__ coef, int mode,
                                                  const V* __restrict__ phi, V* __restrict__ ux,
                                                  V* __restrict__ uy, V* __restrict__ uz,
                                                  double* __restrict__ pr, const double* __restrict__ uy_ym) {
-    project_body(OwnGrid{}, c, m, coef, mode, phi, ux, uy, uz, pr, uy_ym);
+    project_body<V, PROJ_KZ1>(OwnGrid{}, c, m, coef, mode, phi, ux, uy, uz, pr, uy_ym);
 }
 
 constexpr int PROJ_KZ = 4;
@@ -531,13 +534,19 @@ void launch_prsrc(cudaStream_t st, const DConst& c, const DMetric& m, const DCoe
 
 void launch_store_divsrc(cudaStream_t st, DCoef* coef, const double* v) { k_store_divsrc<<<1, 32, 0, st>>>(coef, v); }
 
+static dim3 project_grid(const DConst& c) {
+    const dim3 g = cell_grid(c);
+    return dim3(g.x, g.y, (g.z + PROJ_KZ1 - 1) / PROJ_KZ1);
+}
 void launch_project(cudaStream_t st, const DConst& c, const DMetric& m, const DCoef* coef, int mode, const double* phi,
                     const Fields& f, const double* uy_ym) {
-    launch_pdl(k_project<double>, cell_grid(c), cell_block(), 0, st, c, m, coef, mode, phi, f.ux, f.uy, f.uz, f.pr, uy_ym);
+    launch_pdl(k_project<double>, project_grid(c), cell_block(), 0, st, c, m, coef, mode, phi, f.ux, f.uy, f.uz, f.pr,
+               uy_ym);
 }
 void launch_project(cudaStream_t st, const DConst& c, const DMetric& m, const DCoef* coef, int mode, const float* phi,
                     const Fields32& f, const double* uy_ym) {
-    launch_pdl(k_project<float>, cell_grid(c), cell_block(), 0, st, c, m, coef, mode, phi, f.ux, f.uy, f.uz, f.pr, uy_ym);
+    launch_pdl(k_project<float>, project_grid(c), cell_block(), 0, st, c, m, coef, mode, phi, f.ux, f.uy, f.uz, f.pr,
+               uy_ym);
 }
 
 void launch_bc_all(cudaStream_t st, const DConst& c, const Fields& f, const double* uy_ym) {
