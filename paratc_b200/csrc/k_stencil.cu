@@ -221,7 +221,7 @@ __global__ void k_cfl_final(DConst c, DCoef* coef, const double* __restrict__ pa
 // CalcUxAver / ClcMeanValue (src/m_Tools.f90:54-110,256-301) for the step's
 // diagnostics and guards, and (next != 0) clcCFL (src/m_TScheme.f90:20-46)
 // of the step that follows, which reads the same velocity.  A warp takes whole
-// x rows (grid-stride over the (k, jc) rows, one wave of CTAs); every CTA
+// x rows (grid-stride over the (jc, k) rows, k fastest, one wave of CTAs); every CTA
 // stores one record of 5 maxima and 3 sums and the last CTA to finish reduces
 // the records in index order.  It first fills the diagnostics from this
 // step's dt and CFL number, then writes the next step's: cflmp = uddxmax*dt
@@ -246,7 +246,9 @@ __device__ __forceinline__ void endstep_body(const G& grid, const DConst& c, con
     pdl_wait();
     pdl_trigger();
     for (int r = grid.x() * (ENDSTEP_THREADS / 32) + warp; r < ny * nz; r += nwarps) {
-        const int k = r / ny, jc = r - k * ny + 1;
+        // k fastest: the warps of a CTA take consecutive z planes of one row
+        // jc, so the four w planes of dw/dz are shared through L1
+        const int jm = r / nz, k = r - jm * nz, jc = jm + 1;
         const int km = k == 0 ? nz - 1 : k - 1, kp = k == nz - 1 ? 0 : k + 1, ku = kp == nz - 1 ? 0 : kp + 1;
         const size_t r0 = (size_t)jc * nx;
         const V* ur = ux + (size_t)k * pl + r0;
