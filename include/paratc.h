@@ -407,8 +407,9 @@ int paratc_set_schedule(paratc_ctx* ctx, int choice);
  * choices timed at every start).  paratc_autotune_all first runs
  * paratc_autotune (the Poisson schedule), then times whole steps from the
  * current state for every compiled launch shape of the right-hand side
- * (FP64: rows prefetched 1 or 2 ahead, 2 or 1 cells per thread) and of the
- * Helmholtz sweeps (8 or 4 rows per register chunk), puts the state back
+ * (FP64: rows prefetched 1 or 2 ahead, 2 or 1 cells per thread; FP32
+ * storage: 1 or 2 cells per thread) and of the Helmholtz sweeps (8 or 4
+ * rows per register chunk), puts the state back
  * and keeps the fastest.  With cache_path != NULL the picks are written to
  * that JSON file under a key naming the GPU, the grid, the scalar, the
  * precision and the flow type, and a later call (or paratc_create, when the

@@ -1325,7 +1325,7 @@ static int tune_cache_write(const char* path, const std::string& key, const para
 }
 
 static bool tuning_valid(const paratc_ctx* ctx, const paratc_tuning& t) {
-    return sched_supported(ctx, t.schedule) && t.rhs_var >= 0 && t.rhs_var < rhs_variants() && t.helm_var >= 0 &&
+    return sched_supported(ctx, t.schedule) && t.rhs_var >= 0 && t.rhs_var < rhs_variants(ctx->prec) && t.helm_var >= 0 &&
            t.helm_var < helm_variants() && !(ctx->prec == PARATC_PREC_FP32 && t.schedule / 2 == 2);
 }
 
@@ -1408,7 +1408,7 @@ int paratc_autotune_all(paratc_ctx* ctx, int nrep, const char* cache_path, parat
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
-    const int nr = (ctx->prec == PARATC_PREC_FP64) ? rhs_variants() : 1;  // FP32 arithmetic forms have one shape
+    const int nr = rhs_variants(ctx->prec);  // FP64 3 launch shapes, FP32 storage 2, mixed 1
     float best = -1.f;
     paratc_tuning bt = {sched, 0, 0, 0, 0.0};
     for (int rv = 0; rv < nr; rv++)

@@ -48,17 +48,20 @@ constexpr int SLAB = SX * SZ;    // 560 doubles per field and row
 // The launch shape, per precision and compiled variant VAR (the tuner's
 // choice, paratc_autotune_all): PF rows loaded ahead beyond row j+1 (copy
 // groups in flight; FP64), ZC z-adjacent cells per thread (2 lets the shared
-// stencil taps of the two cells load once; FP32: 1) and the threads per CTA.
+// stencil taps of the two cells load once) and the threads per CTA.
 // FP64 variants: 0 PF 1, ZC 2 (128 threads); 1 PF 2, ZC 2; 2 PF 1, ZC 1
-// (256 threads).  The FP32 forms have one variant.
+// (256 threads).  FP32 storage: 0 ZC 1 (256 threads), 1 ZC 2 (128 threads).
+// The mixed form (FP32 arithmetic on FP64 fields) has one variant.
 constexpr int RHS_NVAR = 3;
 template <class T, int VAR = 0>
 struct RhsCfg {
     static constexpr bool F64 = sizeof(T) == 8;
     static constexpr int PF = (F64 && VAR == 1) ? 2 : 1;
     static constexpr int NB = F64 ? 3 + PF : 4;  // ring slots: rows j-1..j+1 and the rows in flight
-    static constexpr int MINB = 2;               // resident CTAs per SM (FP64, 2 cells: 3 spills and is slower)
-    static constexpr int ZC = (F64 && VAR != 2) ? 2 : 1;
+    // resident CTAs per SM: 2 (FP64 with 2 cells: 3 spills and is slower);
+    // 3 for the FP32 storage form's two-cell shape (168 registers, no spills)
+    static constexpr int MINB = (!F64 && VAR == 1) ? 3 : 2;
+    static constexpr int ZC = F64 ? (VAR != 2 ? 2 : 1) : (VAR == 1 ? 2 : 1);
     static constexpr int NTHR = TX * TZ / ZC;  // 128 or 256
     static constexpr int NSLOT = (SLAB + NTHR - 1) / NTHR;
 };
@@ -123,12 +126,11 @@ __device__ __forceinline__ void rhs_body(const G& grid, const DConst& c, const D
     constexpr int ZC = CFG::ZC, NTHR = CFG::NTHR, NSLOT = CFG::NSLOT, NB = CFG::NB, PF = CFG::PF;
     // FP64 copies: 16-byte pairs, NPAIR per (field, z-plane) row, NP2 per thread and field
     constexpr int NPAIR = SX / 2, NPR = SZ * NPAIR, NP2 = (NPR + NTHR - 1) / NTHR;
-    // FP32 storage: u, v, w (and c) come as 16-byte quads by cp.async (one per
-    // thread and field: SZ * SX / 4 = 140 <= NTHR), the FP64 pressure through
+    // FP32 storage: u, v, w (and c) come as 16-byte quads by cp.async (SZ *
+    // SX / 4 = 140 per field, NQ2 per thread), the FP64 pressure through
     // registers, converted; needs nx % 4 == 0 (paratc_set_precision checks)
     constexpr bool F32S = !F64 && sizeof(V) == 4;
-    constexpr int NQUAD = SZ * (SX / 4);
-    static_assert(!F32S || NQUAD <= NTHR, "one quad per thread and field");
+    constexpr int NQUAD = SZ * (SX / 4), NQ2 = (NQUAD + NTHR - 1) / NTHR;
     extern __shared__ __align__(128) unsigned char sm_raw[];
     T* sm = reinterpret_cast<T*>(sm_raw);  // [NB][NF][SLAB]
     __shared__ __align__(128) double smet[NB][ROWMET];
@@ -179,15 +181,17 @@ __device__ __forceinline__ void rhs_body(const G& grid, const DConst& c, const D
         const int j1 = (int)min((long long)ny, (long long)j0 + (gend - g) - 1);
         g += j1 - j0 + 1;
         const int i0 = (tile % ntx) * TX, k0 = (tile / ntx) * TZ;
-        // FP32 storage: the quad this thread copies for every float field
-        size_t gq = 0;
-        int sq = 0;
-        bool vq = false;
-        if constexpr (F32S) {
-            vq = tid < NQUAD;
-            const int zz = tid / (SX / 4), qq = tid - zz * (SX / 4);
-            gq = (size_t)modp(k0 - HZ + zz, nz) * pl + (size_t)modp(i0 - HX + 4 * qq, nx);
-            sq = zz * SX + 4 * qq;
+        // FP32 storage: the quads this thread copies for every float field
+        size_t gq[NQ2];
+        int sq[NQ2];
+        bool vq[NQ2];
+#pragma unroll
+        for (int s4 = 0; s4 < NQ2; s4++) {
+            const int e = tid + s4 * NTHR;
+            vq[s4] = F32S && e < NQUAD;
+            const int zz = e / (SX / 4), qq = e - zz * (SX / 4);
+            gq[s4] = vq[s4] ? (size_t)modp(k0 - HZ + zz, nz) * pl + (size_t)modp(i0 - HX + 4 * qq, nx) : 0;
+            sq[s4] = zz * SX + 4 * qq;
         }
         // FP32 form: per-thread slab elements, loaded and converted
         size_t goff[F64 ? 1 : NSLOT];
@@ -234,7 +238,8 @@ __device__ __forceinline__ void rhs_body(const G& grid, const DConst& c, const D
         const size_t ro_ = (size_t)(jrow) * nx;                                          \
         _Pragma("unroll") for (int f_ = 0; f_ < NF; f_++) {                              \
             if (F32S && f_ != 3) {                                                       \
-                if (vq) cp_async16(dst_ + f_ * SLAB + sq, fieldv(fl, f_) + gq + ro_);    \
+                _Pragma("unroll") for (int s4_ = 0; s4_ < NQ2; s4_++) if (vq[s4_])       \
+                    cp_async16(dst_ + f_ * SLAB + sq[s4_], fieldv(fl, f_) + gq[s4_] + ro_); \
                 continue;                                                                \
             }                                                                            \
             _Pragma("unroll") for (int s_ = 0; s_ < NSLOT; s_++) if (sval[s_])           \
@@ -315,7 +320,9 @@ __device__ __forceinline__ void rhs_body(const G& grid, const DConst& c, const D
                     for (int f = 0; f < NF; f++) {
                         if (F32S && f != 3) {
                             // the slot of row j+2 was last read by row j-2's arithmetic
-                            if (vq) cp_async16(dst + f * SLAB + sq, fieldv(fl, f) + gq + ro);
+#pragma unroll
+                            for (int s4 = 0; s4 < NQ2; s4++)
+                                if (vq[s4]) cp_async16(dst + f * SLAB + sq[s4], fieldv(fl, f) + gq[s4] + ro);
                             continue;
                         }
 #pragma unroll
@@ -644,10 +651,13 @@ static size_t rhs_blocks(const DConst& c, int minb) {
 }
 
 size_t rhs_grid_blocks(const DConst& c) {
-    return rhs_blocks(c, 2);  // MINB of every variant
+    return rhs_blocks(c, 3);  // the largest MINB of the variants
 }
 
 int rhs_variants() { return RHS_NVAR; }
+// the launch shapes the tuner tries per precision form: FP64 3, FP32
+// storage 2, mixed 1
+int rhs_variants(int prec) { return prec == 0 ? RHS_NVAR : (prec == 2 ? 2 : 1); }
 
 void rhs_init() {
 #define RHS_ATTR(S, T, V, VAR)                                                                            \
@@ -660,6 +670,7 @@ void rhs_init() {
     RHS_ATTR(false, double, double, 2) RHS_ATTR(true, double, double, 2)
     RHS_ATTR(false, float, double, 0) RHS_ATTR(true, float, double, 0)
     RHS_ATTR(false, float, float, 0) RHS_ATTR(true, float, float, 0)
+    RHS_ATTR(false, float, float, 1) RHS_ATTR(true, float, float, 1)
 #undef RHS_ATTR
 }
 
@@ -739,8 +750,13 @@ void launch_rhs_grp(cudaStream_t st, const DConst& key, const GrpTab<RhsArgs<flo
 
 void launch_rhs_tile(cudaStream_t st, const DConst& c, const DMetric& m, DCoef* coef, const Fields32& f, double* uy_ym,
                      double* duy_ym, int ns, double gam, double the, double alp, double* part, unsigned int* counter) {
-    if (c.scalar_on) launch_rhs_t<true, float, 0>(st, c, m, coef, f, uy_ym, duy_ym, ns, gam, the, alp, part, counter);
-    else launch_rhs_t<false, float, 0>(st, c, m, coef, f, uy_ym, duy_ym, ns, gam, the, alp, part, counter);
+    if (c.rhs_var == 1) {
+        if (c.scalar_on) launch_rhs_t<true, float, 1>(st, c, m, coef, f, uy_ym, duy_ym, ns, gam, the, alp, part, counter);
+        else launch_rhs_t<false, float, 1>(st, c, m, coef, f, uy_ym, duy_ym, ns, gam, the, alp, part, counter);
+    } else {
+        if (c.scalar_on) launch_rhs_t<true, float, 0>(st, c, m, coef, f, uy_ym, duy_ym, ns, gam, the, alp, part, counter);
+        else launch_rhs_t<false, float, 0>(st, c, m, coef, f, uy_ym, duy_ym, ns, gam, the, alp, part, counter);
+    }
 }
 
 }  // namespace ptc

@@ -122,6 +122,41 @@ def test_fp32_storage_steps_track_fp64(name, schedule):
     g32.close()
 
 
+@pytest.mark.parametrize("name", ["channel_64", "halfchannel_scalar", "channel_cfl"])
+def test_fp32_two_cell_rhs_shape(name):
+    """The FP32 storage form's second launch shape of the right-hand side
+    (two z-adjacent cells per thread, 128 threads; the tuner's rhs_var 1)
+    keeps the form's bounds against the FP64 path and agrees with the
+    one-cell shape to within them."""
+    case = _case(name)
+    g64, g32 = _pair(case)
+    gb = ChannelSystem(case.params, yp_of(case))
+    f = fields_of(case, yp_of(case))
+    gb.set_fields(f["ux"], f["uy"], f["uz"], f["p"], f["c"])
+    gb.project()
+    for g in (g32, gb):
+        g.precision = "fp32"
+    t = gb.tuning
+    t.rhs_var = 1
+    gb.tuning = t
+    assert gb.tuning.rhs_var == 1 and g32.tuning.rhs_var == 0
+    worst_div = 0.0
+    for _ in range(NSTEP):
+        g64.iterate(1)
+        g32.iterate(1)
+        worst_div = max(worst_div, gb.iterate(1).divmax)
+    f64, f32, fb = g64.get_fields(), g32.get_fields(), gb.get_fields()
+    for n in ("ux", "uy", "uz", "p", "c"):
+        if f64.get(n) is None:
+            continue
+        tol = FP32_PR if n == "p" else FP32_VEL
+        assert rel_err(fb[n], f64[n]) <= tol, (n, rel_err(fb[n], f64[n]))
+        assert rel_err(fb[n], f32[n]) <= tol, (n, rel_err(fb[n], f32[n]))
+    assert worst_div <= FP32_DIV
+    for g in (g64, g32, gb):
+        g.close()
+
+
 def test_fp32_switch_round_trip():
     case = variant("channel")
     yp = yp_of(case)
