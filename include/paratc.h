@@ -409,7 +409,8 @@ int paratc_set_schedule(paratc_ctx* ctx, int choice);
  * current state for every compiled launch shape of the right-hand side
  * (FP64: rows prefetched 1 or 2 ahead, 2 or 1 cells per thread; FP32
  * storage: 1 or 2 cells per thread) and of the Helmholtz sweeps (8 or 4
- * rows per register chunk), puts the state back
+ * rows per register chunk; FP32 storage also float-arithmetic sweeps), puts
+ * the state back
  * and keeps the fastest.  With cache_path != NULL the picks are written to
  * that JSON file under a key naming the GPU, the grid, the scalar, the
  * precision and the flow type, and a later call (or paratc_create, when the

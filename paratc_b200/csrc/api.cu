@@ -1326,7 +1326,7 @@ static int tune_cache_write(const char* path, const std::string& key, const para
 
 static bool tuning_valid(const paratc_ctx* ctx, const paratc_tuning& t) {
     return sched_supported(ctx, t.schedule) && t.rhs_var >= 0 && t.rhs_var < rhs_variants(ctx->prec) && t.helm_var >= 0 &&
-           t.helm_var < helm_variants() && !(ctx->prec == PARATC_PREC_FP32 && t.schedule / 2 == 2);
+           t.helm_var < helm_variants(ctx->prec) && !(ctx->prec == PARATC_PREC_FP32 && t.schedule / 2 == 2);
 }
 
 static void tuning_apply(paratc_ctx* ctx, const paratc_tuning& t) {
@@ -1412,7 +1412,7 @@ int paratc_autotune_all(paratc_ctx* ctx, int nrep, const char* cache_path, parat
     float best = -1.f;
     paratc_tuning bt = {sched, 0, 0, 0, 0.0};
     for (int rv = 0; rv < nr; rv++)
-        for (int hv = 0; hv < helm_variants(); hv++) {
+        for (int hv = 0; hv < helm_variants(ctx->prec); hv++) {
             ctx->kc.rhs_var = rv;
             ctx->kc.helm_var = hv;
             copy_all(false);

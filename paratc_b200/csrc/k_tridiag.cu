@@ -18,6 +18,8 @@
 // partitioned reduced-system solver (part_eliminate / part_reduced /
 // k_ysolve) computes its pivots in place; the allocation-free Poisson entry
 // point uses it because it has no room to keep pivots between calls.
+#include <type_traits>
+
 #include "common.cuh"
 #include "kernels.cuh"
 
@@ -173,8 +175,12 @@ __host__ __device__ inline int helm_stride(int ny) { return 3 * (ny + 2); }
 // value is substituted before the sweep and its result after it).
 // G: the block this CTA works as (OwnGrid, or SubGrid in a grouped launch).
 // Z4: the grouped launch's CTA shape, 32 columns of 4 z planes (one per
-// warp), so that a narrow member (nx < 128) leaves no warp idle
-template <class V, int HU, bool Z4 = false, class G>
+// warp), so that a narrow member (nx < 128) leaves no warp idle.
+// W: the sweeps' arithmetic, double (FP64 in every form), or float for the
+// FP32 storage form's third launch shape, whose rows are stored in float
+// anyway: widening each value to FP64 and rounding it back put conversions
+// and FP64 latencies on every row of the chain
+template <class V, int HU, bool Z4 = false, class W = double, class G>
 __device__ __forceinline__ void helm_body(const G& grid, const DConst& cst, const DCoef* __restrict__ coef, int comp0,
                                           const FieldSet<V>& fl, const double* __restrict__ duy_ym,
                                           const double* __restrict__ uy_ym, const double* __restrict__ facs) {
@@ -187,12 +193,13 @@ __device__ __forceinline__ void helm_body(const G& grid, const DConst& cst, cons
     {
         const double* F = facs + (size_t)((coef->ns - 1) * 3 + t) * helm_stride(ny);
         const int tid = threadIdx.y * 32 + threadIdx.x;
-        for (int q = tid; q < helm_stride(ny); q += 128) shf[q] = F[q];
+        W* shw = reinterpret_cast<W*>(shf);
+        for (int q = tid; q < helm_stride(ny); q += 128) shw[q] = (W)F[q];
     }
     __syncthreads();
-    const double* SA = shf;
-    const double* SR = shf + (ny + 2);
-    const double* SW = shf + 2 * (ny + 2);
+    const W* SA = reinterpret_cast<const W*>(shf);
+    const W* SR = SA + (ny + 2);
+    const W* SW = SA + 2 * (ny + 2);
     const int i = Z4 ? (int)grid.x() * 32 + (int)threadIdx.x : (int)(grid.x() * 4 + threadIdx.y) * 32 + (int)threadIdx.x;
     const int k = Z4 ? (int)grid.y() * 4 + (int)threadIdx.y : (int)grid.y();
     if (i >= nx || (Z4 && k >= cst.nz)) return;
@@ -204,7 +211,8 @@ __device__ __forceinline__ void helm_body(const G& grid, const DConst& cst, cons
     else if (comp == 2) { u = fl.uz; rhs = fl.rz; }
     else                { u = fl.sc; rhs = fl.rc; }
     const size_t col = (size_t)k * cst.nyt * nx + i;
-    // the sweeps run in FP64 whatever the storage: loads convert, stores round
+    // the sweeps run in W (FP64 unless chosen otherwise): loads convert, stores round
+    const W addw = (W)add;
     V* rc = rhs + col;
     V* uc = u + col;
     const int nch = (ny + HU - 1) / HU;
@@ -224,21 +232,21 @@ __device__ __forceinline__ void helm_body(const G& grid, const DConst& cst, cons
             b += nx;
         }
     };
-    double fp = 0.0;
+    W fp = 0;
     V* wp = rc + nx;
     auto fwd = [&](const V (&X)[HU], int cc) {
         if (cc >= nch) return;
         const int nr = ny - cc * HU;
-        const double* sa = SA + cc * HU + 1;
-        const double* sr = SR + cc * HU + 1;
+        const W* sa = SA + cc * HU + 1;
+        const W* sr = SR + cc * HU + 1;
 #pragma unroll
         for (int q = 0; q < HU; q++) {
             if (q < nr) {
                 // clcU2Hat: the row-1 value is the wall increment (kept in FP64)
-                const double xq = (comp == 1 && cc == 0 && q == 0) ? a0 : (double)X[q];
-                const double f = ((xq + add) - sa[q] * fp) * sr[q];
+                const W xq = (comp == 1 && cc == 0 && q == 0) ? (W)a0 : (W)X[q];
+                const W f = ((xq + addw) - sa[q] * fp) * sr[q];
                 *wp = (V)f;
-                fp = f;  // the chain stays FP64 (no conversion on the dependent path)
+                fp = f;  // the chain stays in W (no conversion on the dependent path)
             }
             wp += nx;
         }
@@ -269,18 +277,18 @@ __device__ __forceinline__ void helm_body(const G& grid, const DConst& cst, cons
             bu -= nx;
         }
     };
-    double xn = 0.0, unew = 0.0, utop = 0.0;
+    W xn = 0, unew = 0, utop = 0;
     V* up = uc + (size_t)ny * nx;
     auto bwd = [&](const V (&D)[HU], const V (&U)[HU], int cc) {
         if (cc >= nch) return;
         const int nr = ny - cc * HU;
-        const double* sw = SW + ny + 1 - cc * HU;
+        const W* sw = SW + ny + 1 - cc * HU;
 #pragma unroll
         for (int q = 0; q < HU; q++) {
             if (q < nr) {
-                const double x = (double)D[q] - sw[-q] * xn;
+                const W x = (W)D[q] - sw[-q] * xn;
                 xn = x;
-                unew = (double)U[q] + x;
+                unew = (W)U[q] + x;
                 *up = (V)unew;
             }
             up -= nx;
@@ -291,7 +299,7 @@ __device__ __forceinline__ void helm_body(const G& grid, const DConst& cst, cons
     ldb(DC, UC, 2);
     for (int c = 0; c < nch; c += 3) {
         bwd(DA, UA, c);
-        if (c == 0) utop = (double)DA[0] + (double)UA[0];  // u(ny): x(ny) = f(ny)
+        if (c == 0) utop = (W)DA[0] + (W)UA[0];  // u(ny): x(ny) = f(ny)
         ldb(DA, UA, c + 3);
         bwd(DB, UB, c + 1);
         ldb(DB, UB, c + 4);
@@ -303,23 +311,23 @@ __device__ __forceinline__ void helm_body(const G& grid, const DConst& cst, cons
         uc[nx] = (V)uy_ym[(size_t)k * nx + i];
         uc[(size_t)(ny + 1) * nx] = (V)((cst.flow_type == 1) ? cst.uybc_yp : 0.0);
     } else if (comp == 3) {
-        uc[0] = (V)(cst.sc_r1b * unew + cst.sc_r2b);
-        uc[(size_t)(ny + 1) * nx] = (V)(cst.sc_r1t * utop + cst.sc_r2t);
+        uc[0] = (V)(cst.sc_r1b * (double)unew + cst.sc_r2b);
+        uc[(size_t)(ny + 1) * nx] = (V)(cst.sc_r1t * (double)utop + cst.sc_r2t);
     }
 }
 
-template <class V, int HU>
+template <class V, int HU, class W = double>
 __global__ void __launch_bounds__(128, 4) k_helm(DConst cst, const DCoef* __restrict__ coef, int comp0, FieldSet<V> fl,
                                               const double* __restrict__ duy_ym, const double* __restrict__ uy_ym,
                                               const double* __restrict__ facs) {
-    helm_body<V, HU>(OwnGrid{}, cst, coef, comp0, fl, duy_ym, uy_ym, facs);
+    helm_body<V, HU, false, W>(OwnGrid{}, cst, coef, comp0, fl, duy_ym, uy_ym, facs);
 }
 
-template <class V, int HU>
+template <class V, int HU, class W = double>
 __global__ void __launch_bounds__(128, 4) k_helm_grp(const GrpTab<HelmArgs<V>>* __restrict__ t) {
     SubGrid g;
     const HelmArgs<V>& a = t->e[grp_member(t, g)];
-    helm_body<V, HU, true>(g, a.c, a.coef, a.comp0, a.fl, a.duy_ym, a.uy_ym, a.fac);
+    helm_body<V, HU, true, W>(g, a.c, a.coef, a.comp0, a.fl, a.duy_ym, a.uy_ym, a.fac);
 }
 
 // ---------------------------------------------------------------------------
@@ -711,6 +719,9 @@ int tridiag_part_len(int ny) { return part_len(ny); }
 
 size_t helm_fac_doubles(int ny) { return (size_t)9 * helm_stride(ny); }
 int helm_variants() { return HELM_NVAR; }
+// the Helmholtz launch shapes of precision form prec: FP32 storage adds
+// float-arithmetic sweeps (helm_var 2)
+int helm_variants(int prec) { return prec == 2 ? HELM_NVAR + 1 : HELM_NVAR; }
 
 // pivots of the Helmholtz matrices of substeps ns0..ns0+nsub-1 for the
 // current dt (coef->dt): one thread per (substep, type) runs the forward
@@ -774,7 +785,9 @@ size_t helm_smem(const DConst& c) { return helm_stride(c.ny) * sizeof(double); }
 template <class V>
 static void helm_grp_t(cudaStream_t st, const DConst& key, const GrpTab<HelmArgs<V>>* t, int nblk, size_t smem) {
     constexpr int H0 = sizeof(V) == 4 ? 2 * HY_U : HY_U;
+    using WF = std::conditional_t<sizeof(V) == 4, float, double>;  // helm_var 2: float sweeps (FP32 storage)
     if (key.helm_var == 1) launch_pdl(k_helm_grp<V, H0 / 2>, dim3((unsigned)nblk), dim3(32, 4), smem, st, t);
+    else if (key.helm_var == 2) launch_pdl(k_helm_grp<V, H0, WF>, dim3((unsigned)nblk), dim3(32, 4), smem, st, t);
     else launch_pdl(k_helm_grp<V, H0>, dim3((unsigned)nblk), dim3(32, 4), smem, st, t);
 }
 void launch_helm_grp(cudaStream_t st, const DConst& key, const GrpTab<HelmArgs<double>>* t, int nblk, size_t smem) {
@@ -792,8 +805,12 @@ static void helm_dispatch(cudaStream_t st, const DConst& c, const DCoef* coef, i
     // rows per chunk: FP64 8 (variant 1: 4); float storage, whose ring takes
     // half the registers, 16 (variant 1: 8)
     constexpr int H0 = sizeof(V) == 4 ? 2 * HY_U : HY_U;
+    using WF = std::conditional_t<sizeof(V) == 4, float, double>;  // helm_var 2: float sweeps (FP32 storage)
     if (c.helm_var == 1)
         launch_pdl(k_helm<V, H0 / 2>, grd, blk, helm_stride(c.ny) * sizeof(double), st, c, coef, comp0, f, duy_ym,
+                   uy_ym, fac);
+    else if (c.helm_var == 2)
+        launch_pdl(k_helm<V, H0, WF>, grd, blk, helm_stride(c.ny) * sizeof(double), st, c, coef, comp0, f, duy_ym,
                    uy_ym, fac);
     else
         launch_pdl(k_helm<V, H0>, grd, blk, helm_stride(c.ny) * sizeof(double), st, c, coef, comp0, f, duy_ym,

@@ -91,6 +91,7 @@ void tridiag_init();
 int tridiag_part_len(int ny);
 size_t helm_fac_doubles(int ny);
 int helm_variants();  // compiled Helmholtz launch shapes (DConst::helm_var < helm_variants())
+int helm_variants(int prec);  // the shapes of precision form prec: FP64 and mixed 2, FP32 storage 3 (float sweeps)
 int rhs_variants();          // compiled FP64 right-hand-side launch shapes (DConst::rhs_var < rhs_variants())
 int rhs_variants(int prec);  // the shapes of precision form prec (PARATC_PREC_*): FP64 3, FP32 storage 2, mixed 1
 void launch_helm_factors(cudaStream_t st, const DConst& c, const DMetric& m, const DCoef* coef, int ns0, int nsub,

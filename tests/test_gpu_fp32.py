@@ -122,12 +122,14 @@ def test_fp32_storage_steps_track_fp64(name, schedule):
     g32.close()
 
 
+@pytest.mark.parametrize("shape", [(1, 0), (0, 2), (1, 2)])
 @pytest.mark.parametrize("name", ["channel_64", "halfchannel_scalar", "channel_cfl"])
-def test_fp32_two_cell_rhs_shape(name):
-    """The FP32 storage form's second launch shape of the right-hand side
-    (two z-adjacent cells per thread, 128 threads; the tuner's rhs_var 1)
-    keeps the form's bounds against the FP64 path and agrees with the
-    one-cell shape to within them."""
+def test_fp32_launch_shapes(name, shape):
+    """The FP32 storage form's other launch shapes, (rhs_var, helm_var):
+    the right-hand side with two z-adjacent cells per thread (rhs_var 1) and
+    the Helmholtz sweeps in float arithmetic (helm_var 2).  Each keeps the
+    form's bounds against the FP64 path and agrees with the default shapes
+    (0, 0) within them."""
     case = _case(name)
     g64, g32 = _pair(case)
     gb = ChannelSystem(case.params, yp_of(case))
@@ -137,9 +139,10 @@ def test_fp32_two_cell_rhs_shape(name):
     for g in (g32, gb):
         g.precision = "fp32"
     t = gb.tuning
-    t.rhs_var = 1
+    t.rhs_var, t.helm_var = shape
     gb.tuning = t
-    assert gb.tuning.rhs_var == 1 and g32.tuning.rhs_var == 0
+    assert (gb.tuning.rhs_var, gb.tuning.helm_var) == shape
+    assert (g32.tuning.rhs_var, g32.tuning.helm_var) == (0, 0)
     worst_div = 0.0
     for _ in range(NSTEP):
         g64.iterate(1)
