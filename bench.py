@@ -50,6 +50,10 @@ def _args():
     ap.add_argument("--no-forms", action="store_true",
                     help="skip the FP32 / mixed / batched forms that follow the FP64 headline")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--rhs-var", type=int, default=-1,
+                    help="with --schedule: pin the right-hand-side launch shape too (paratc_tuning.rhs_var)")
+    ap.add_argument("--helm-var", type=int, default=-1,
+                    help="with --schedule: pin the Helmholtz launch shape too (paratc_tuning.helm_var)")
     ap.add_argument("--schedule", type=int, default=-1,
                     help="pin a Poisson schedule (0-11, paratc_set_schedule) instead of auto-tuning it")
     ap.add_argument("--batch-mode", choices=["grouped", "streams"], default="streams",
@@ -194,6 +198,13 @@ def _tune_step(ctx, args):
     pinned.  Returns the schedule and the picks."""
     if args.schedule >= 0:
         ctx.schedule = args.schedule
+        if args.rhs_var >= 0 or args.helm_var >= 0:
+            t = ctx.tuning
+            if args.rhs_var >= 0:
+                t.rhs_var = args.rhs_var
+            if args.helm_var >= 0:
+                t.helm_var = args.helm_var
+            ctx.tuning = t
         return args.schedule, None
     t = ctx.autotune_all(nrep=3)
     return t.schedule, {"schedule": t.schedule, "rhs_var": t.rhs_var, "helm_var": t.helm_var,
