@@ -130,6 +130,93 @@ __global__ void __launch_bounds__(256) k_project(DConst c, DMetric m, const DCoe
     project_body<V, PROJ_KZ1>(OwnGrid{}, c, m, coef, mode, phi, ux, uy, uz, pr, uy_ym);
 }
 
+// The one-context projection with two x-adjacent cells per thread (nx even):
+// the cells' loads and stores move as pairs at an even index (float2 /
+// double2), so a thread issues 12 loads for two cells instead of 13 per
+// cell, and the x taps of the pair share two of their five values.  Every
+// cell's arithmetic is project_body's, in the same order, so the two kernels
+// give the same bits.
+namespace {
+__device__ __forceinline__ double2 ld_pv(const double* p) { return *reinterpret_cast<const double2*>(p); }
+__device__ __forceinline__ double2 ld_pv(const float* p) {
+    const float2 v = *reinterpret_cast<const float2*>(p);
+    return make_double2(v.x, v.y);
+}
+}  // namespace
+
+template <class V>
+__global__ void __launch_bounds__(256) k_project2(DConst c, DMetric m, const DCoef* __restrict__ coef, int mode,
+                                                  const V* __restrict__ phi, V* __restrict__ ux, V* __restrict__ uy,
+                                                  V* __restrict__ uz, double* __restrict__ pr,
+                                                  const double* __restrict__ uy_ym) {
+    const int nx = c.nx;
+    const int i = 2 * (int)(blockIdx.x * blockDim.x + threadIdx.x);
+    const int jc = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    const int k = blockIdx.z;
+    pdl_wait();
+    if (i >= nx || jc > c.ny) return;
+    const double alpha = mode == 0 ? coef->pmAlpha : 1.0;
+    const size_t pl = (size_t)c.nyt * nx;
+    const size_t r0 = (size_t)jc * nx, zc = (size_t)k * pl;
+    const size_t zs = (size_t)wrapi(k - 2, c.nz) * pl, zm = (size_t)wrapi(k - 1, c.nz) * pl, zp = (size_t)wrapi(k + 1, c.nz) * pl;
+    const size_t q = zc + r0 + i;
+    // phi at i-2 .. i+3 of the row (pairs at even indices, wrapped), and the pair's y and z neighbours
+    const double2 xm = ld_pair(phi + zc + r0 + wrapi(i - 2, nx));
+    const double2 x0 = ld_pair(phi + q);
+    const double2 xp = ld_pair(phi + zc + r0 + wrapi(i + 2, nx));
+    const double2 ym = ld_pair(phi + q - nx), yp = ld_pair(phi + q + nx);
+    const double2 z2 = ld_pair(phi + zs + r0 + i), z1 = ld_pair(phi + zm + r0 + i), z3 = ld_pair(phi + zp + r0 + i);
+    const double2 u0 = ld_pv(ux + q), v0 = ld_pv(uy + q), w0 = ld_pv(uz + q);
+    const double rdyc = __ldg(&m.rdyc[jc]);
+    // cell i: x taps i-2, i-1, i, i+1; cell i+1: i-1, i, i+1, i+2
+    const double pc[2] = {x0.x, x0.y}, pjm[2] = {ym.x, ym.y}, pjp[2] = {yp.x, yp.y};
+    const double ps[2] = {xm.x, xm.y}, pm[2] = {xm.y, x0.x}, pp[2] = {x0.y, xp.x};
+    const double zsv[2] = {z2.x, z2.y}, zmv[2] = {z1.x, z1.y}, zpv[2] = {z3.x, z3.y};
+    const double uv[2] = {u0.x, u0.y}, vv[2] = {v0.x, v0.y}, wv[2] = {w0.x, w0.y};
+    double uxn[2], uyn[2], uzn[2];
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+        const double dpdx = c.dxC[0] * ps[h] + c.dxC[1] * pm[h] + c.dxC[2] * pc[h] + c.dxC[3] * pp[h];
+        const double dpdy = (pc[h] - pjm[h]) * rdyc;
+        const double dpdz = c.dzC[0] * zsv[h] + c.dzC[1] * zmv[h] + c.dzC[2] * pc[h] + c.dzC[3] * zpv[h];
+        uxn[h] = uv[h] - alpha * dpdx;
+        uyn[h] = vv[h] - alpha * dpdy;
+        uzn[h] = wv[h] - alpha * dpdz;
+    }
+    const bool ft_ch = (c.flow_type == 1);
+    if (jc == 1) {
+        const double2 w = *reinterpret_cast<const double2*>(uy_ym + (size_t)k * nx + i);
+        uyn[0] = w.x;
+        uyn[1] = w.y;
+    }
+    st_pair(ux + q, make_double2(uxn[0], uxn[1]));
+    st_pair(uy + q, make_double2(uyn[0], uyn[1]));
+    st_pair(uz + q, make_double2(uzn[0], uzn[1]));
+    if (jc == 1) {
+        st_pair(ux + q - nx, make_double2(c.uxbc_ym * 2.0 - uxn[0], c.uxbc_ym * 2.0 - uxn[1]));
+        st_pair(uz + q - nx, make_double2(c.uzbc_ym * 2.0 - uzn[0], c.uzbc_ym * 2.0 - uzn[1]));
+    }
+    if (jc == c.ny) {
+        st_pair(ux + q + nx, ft_ch ? make_double2(c.uxbc_yp * 2.0 - uxn[0], c.uxbc_yp * 2.0 - uxn[1])
+                                   : make_double2(uxn[0], uxn[1]));
+        st_pair(uy + q + nx, ft_ch ? make_double2(c.uybc_yp, c.uybc_yp) : make_double2(0.0, 0.0));
+        st_pair(uz + q + nx, ft_ch ? make_double2(c.uzbc_yp * 2.0 - uzn[0], c.uzbc_yp * 2.0 - uzn[1])
+                                   : make_double2(uzn[0], uzn[1]));
+    }
+    if (mode == 0) {
+        const double beta = coef->pmBeta;
+        const double bp = -(beta * __ldg(&m.ap2ph[jc]));
+        const double bc = -(beta * __ldg(&m.ac2ph[jc])) + 1.0;
+        const double bm = -(beta * __ldg(&m.am2ph[jc]));
+        const double2 p0 = *reinterpret_cast<const double2*>(pr + q);
+        const double2 pn = make_double2(p0.x + bp * pjp[0] + bc * pc[0] + bm * pjm[0],
+                                        p0.y + bp * pjp[1] + bc * pc[1] + bm * pjm[1]);
+        st_pair(pr + q, pn);
+        if (jc == 1) st_pair(pr + q - nx, pn);
+        if (jc == c.ny) st_pair(pr + q + nx, pn);
+    }
+}
+
 constexpr int PROJ_KZ = 4;
 template <class V>
 __global__ void __launch_bounds__(256) k_project_grp(const GrpTab<ProjArgs<V>>* __restrict__ t) {
@@ -540,15 +627,24 @@ static dim3 project_grid(const DConst& c) {
     const dim3 g = cell_grid(c);
     return dim3(g.x, g.y, (g.z + PROJ_KZ1 - 1) / PROJ_KZ1);
 }
+// two cells per thread where nx is even (k_project2), one otherwise
+template <class V>
+static void project_t(cudaStream_t st, const DConst& c, const DMetric& m, const DCoef* coef, int mode, const V* phi,
+                      const FieldSet<V>& f, const double* uy_ym) {
+    if (c.nx % 2 == 0)
+        launch_pdl(k_project2<V>, dim3((c.nx + 63) / 64, (c.ny + 7) / 8, c.nz), cell_block(), 0, st, c, m, coef, mode,
+                   phi, f.ux, f.uy, f.uz, f.pr, uy_ym);
+    else
+        launch_pdl(k_project<V>, project_grid(c), cell_block(), 0, st, c, m, coef, mode, phi, f.ux, f.uy, f.uz, f.pr,
+                   uy_ym);
+}
 void launch_project(cudaStream_t st, const DConst& c, const DMetric& m, const DCoef* coef, int mode, const double* phi,
                     const Fields& f, const double* uy_ym) {
-    launch_pdl(k_project<double>, project_grid(c), cell_block(), 0, st, c, m, coef, mode, phi, f.ux, f.uy, f.uz, f.pr,
-               uy_ym);
+    project_t(st, c, m, coef, mode, phi, f, uy_ym);
 }
 void launch_project(cudaStream_t st, const DConst& c, const DMetric& m, const DCoef* coef, int mode, const float* phi,
                     const Fields32& f, const double* uy_ym) {
-    launch_pdl(k_project<float>, project_grid(c), cell_block(), 0, st, c, m, coef, mode, phi, f.ux, f.uy, f.uz, f.pr,
-               uy_ym);
+    project_t(st, c, m, coef, mode, phi, f, uy_ym);
 }
 
 void launch_bc_all(cudaStream_t st, const DConst& c, const Fields& f, const double* uy_ym) {
