@@ -345,7 +345,55 @@ __device__ __forceinline__ void endstep_body(const G& grid, const DConst& c, con
         const V* w2 = uz + (size_t)kp * pl + r0;
         const V* w3 = uz + (size_t)ku * pl + r0;
         const double rdyp = __ldg(&m.rdyp[jc]), dy = __ldg(&m.dyp[jc]);
-        // ENDSTEP_U cells per lane with every load issued before the arithmetic
+        // one cell's contribution: a = ux(i-1), ux(i), ux(i+1), ux(i+2), uy(j),
+        // uy(j+1), uz(k-1 .. k+2), scalar
+        auto cell = [&](const double (&a)[11]) {
+            const double u0 = a[1], up = a[2], v0 = a[4], vp = a[5], z1 = a[7], z2 = a[8];
+            const double dudx = c.dxC[0] * a[0] + c.dxC[1] * u0 + c.dxC[2] * up + c.dxC[3] * a[3];
+            const double dvdy = (vp - v0) * rdyp;
+            const double dwdz = c.dzC[0] * a[6] + c.dzC[1] * z1 + c.dzC[2] * z2 + c.dzC[3] * a[9];
+            mx[0] = nmax(mx[0], fabs(dudx + dvdy + dwdz));
+            mx[1] = nmax(mx[1], fabs(u0));
+            mx[2] = nmax(mx[2], fabs(v0));
+            mx[3] = nmax(mx[3], fabs(z1));
+            if (next) mx[4] = nmax(mx[4], fabs(u0 + up) * c.rdx + fabs(v0 + vp) * rdyp + fabs(z1 + z2) * c.rdz);
+            sm[0] += u0 * dy;
+            if (c.scalar_on) {
+                const double s = a[10];
+                sm[1] += dy * s;
+                sm[2] += dy * s * s;
+            }
+        };
+        if (nx % 2 == 0) {
+            // nx even: two adjacent cells per lane and pair, every load a pair at
+            // an even index (ux at i-2 .. i+3 in three pairs), ENDSTEP_U / 2
+            // pairs per lane in flight
+            constexpr int EP = ENDSTEP_U / 2;
+            const V* sr = c.scalar_on ? sc + (size_t)k * pl + r0 : nullptr;
+            for (int i0 = 0; i0 < nx; i0 += 64 * EP) {
+                double2 t[EP][10];
+#pragma unroll
+                for (int u = 0; u < EP; u++) {
+                    const int i = min(i0 + 2 * lane + 64 * u, nx - 2);
+                    t[u][0] = ld_pair(ur + wrapi(i - 2, nx)); t[u][1] = ld_pair(ur + i); t[u][2] = ld_pair(ur + wrapi(i + 2, nx));
+                    t[u][3] = ld_pair(vr + i); t[u][4] = ld_pair(vr + nx + i);
+                    t[u][5] = ld_pair(w0 + i); t[u][6] = ld_pair(w1 + i); t[u][7] = ld_pair(w2 + i); t[u][8] = ld_pair(w3 + i);
+                    t[u][9] = sr ? ld_pair(sr + i) : make_double2(0.0, 0.0);
+                }
+#pragma unroll
+                for (int u = 0; u < EP; u++) {
+                    if (i0 + 2 * lane + 64 * u >= nx) continue;
+                    const double a0[11] = {t[u][0].y, t[u][1].x, t[u][1].y, t[u][2].x, t[u][3].x, t[u][4].x,
+                                           t[u][5].x, t[u][6].x, t[u][7].x, t[u][8].x, t[u][9].x};
+                    const double a1[11] = {t[u][1].x, t[u][1].y, t[u][2].x, t[u][2].y, t[u][3].y, t[u][4].y,
+                                           t[u][5].y, t[u][6].y, t[u][7].y, t[u][8].y, t[u][9].y};
+                    cell(a0);
+                    cell(a1);
+                }
+            }
+            continue;
+        }
+        // nx odd: ENDSTEP_U cells per lane with every load issued before the arithmetic
         for (int i0 = 0; i0 < nx; i0 += 32 * ENDSTEP_U) {
             double a[ENDSTEP_U][11];
 #pragma unroll
@@ -360,22 +408,7 @@ __device__ __forceinline__ void endstep_body(const G& grid, const DConst& c, con
 #pragma unroll
             for (int u = 0; u < ENDSTEP_U; u++) {
                 if (i0 + lane + 32 * u >= nx) continue;
-                const double u0 = a[u][1], up = a[u][2], v0 = a[u][4], vp = a[u][5], z1 = a[u][7], z2 = a[u][8];
-                const double dudx = c.dxC[0] * a[u][0] + c.dxC[1] * u0 + c.dxC[2] * up + c.dxC[3] * a[u][3];
-                const double dvdy = (vp - v0) * rdyp;
-                const double dwdz = c.dzC[0] * a[u][6] + c.dzC[1] * z1 + c.dzC[2] * z2 + c.dzC[3] * a[u][9];
-                mx[0] = nmax(mx[0], fabs(dudx + dvdy + dwdz));
-                mx[1] = nmax(mx[1], fabs(u0));
-                mx[2] = nmax(mx[2], fabs(v0));
-                mx[3] = nmax(mx[3], fabs(z1));
-                if (next)
-                    mx[4] = nmax(mx[4], fabs(u0 + up) * c.rdx + fabs(v0 + vp) * rdyp + fabs(z1 + z2) * c.rdz);
-                sm[0] += u0 * dy;
-                if (c.scalar_on) {
-                    const double s = a[u][10];
-                    sm[1] += dy * s;
-                    sm[2] += dy * s * s;
-                }
+                cell(a[u]);
             }
         }
     }
