@@ -44,7 +44,7 @@ def _args():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", default="channel_c1")
     ap.add_argument("--grid", type=int, nargs=3, default=None, metavar=("NX", "NY", "NZ"),
-                    help="poisson_c2 only: solve on this grid instead of 512 x 256 x 512 (profiling other lengths)")
+                    help="poisson_c2 and poisson_c2_zslabs: solve on this grid instead of 512 x 256 x 512")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-forms", action="store_true",
@@ -737,6 +737,99 @@ def run_poisson(args):
     ctx.close()
 
 
+def run_poisson_slabs(args):
+    """C2's Poisson solve split over the ranks as z slabs (paratc_slab_*):
+    every rank transforms its planes along x, one NCCL all-to-all gives it
+    all planes of its x modes, it solves the z transforms and y-Thomas
+    systems there, a second all-to-all returns the planes, and it transforms
+    them back.  Total work is fixed as N grows (strong scaling); `value` is
+    grid points solved per second of the slowest rank.  With one rank the
+    exchanges are device copies.  Every rank also solves the whole grid on
+    its own GPU (paratc_poisson_device) and reports the largest difference
+    over its planes."""
+    import torch
+    ws, rank, local = _dist()
+    torch.cuda.set_device(local)
+    dev = "cuda:%d" % local
+    from paratc_b200 import cases, replicas, slabs
+    from paratc_b200.lib import ChannelSystem, mesh_ycoord
+    dist = replicas.init("nccl") if ws > 1 else None
+    case = cases.poisson_c2(*args.grid) if args.grid else cases.poisson_c2()
+    p = case.params
+    yp = mesh_ycoord(case.mesh, p.yly)
+    src = cases.gaussian_source(cases.Case("src", p, case.mesh, "gauss_src", 42, 1.0))  # one problem for all ranks
+    cells = p.nxc * p.nyc * p.nzc
+    plan = slabs.SlabPoisson(p, yp, rank, ws, device=local)
+    d_src = torch.from_numpy(np.ascontiguousarray(src[plan.k0:plan.k0 + plan.nzl])).to(dev).reshape(-1)
+    d_phi = torch.empty_like(d_src)
+    buf, xslab = plan.buffers(torch, dev)
+    if dist is not None:
+        exchange = slabs.nccl_exchange()
+    else:
+        def exchange(s, r, sc, rc):
+            slabs.LocalExchange.all_to_all([s], [r], [sc], [rc])
+    st = torch.cuda.current_stream()
+
+    def solve():
+        plan.solve(d_src, d_phi, exchange, buf, xslab, stream=st.cuda_stream)
+
+    for _ in range(args.warmup):
+        solve()
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    sampler = ClockSampler(local)
+    sampler.start()
+    a.record(st)
+    for _ in range(args.steps):
+        solve()
+    b.record(st)
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    plan.sync(st.cuda_stream)
+    ms = replicas.max_over_ranks(a.elapsed_time(b), dist)
+    # stage times of one more solve (events between the stages)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(6)]
+    ev[0].record(st); plan.forward(d_src, buf, st.cuda_stream)
+    ev[1].record(st); exchange(buf, xslab, plan.send_counts, plan.recv_counts)
+    ev[2].record(st); plan.middle(xslab, st.cuda_stream)
+    ev[3].record(st); exchange(xslab, buf, plan.recv_counts, plan.send_counts)
+    ev[4].record(st); plan.backward(buf, d_phi, st.cuda_stream)
+    ev[5].record(st)
+    torch.cuda.synchronize()
+    stages = dict(zip(["forward_x", "exchange_1", "middle_zyz", "exchange_2", "backward_x"],
+                      [round(ev[i].elapsed_time(ev[i + 1]), 3) for i in range(5)]))
+    phi_local = d_phi.cpu().numpy().reshape(plan.nzl, p.nyc, p.nxc)
+    # the one-GPU solve of the whole grid on this rank's GPU
+    ctx = ChannelSystem(p, yp, device=local)
+    g_src = torch.from_numpy(src).to(dev)
+    g_phi = torch.empty_like(g_src)
+    torch.cuda.synchronize()
+    ctx.poisson_device(g_src.data_ptr(), g_phi.data_ptr())
+    ref = g_phi.cpu().numpy()
+    ctx.close()
+    err = float(np.abs(phi_local - ref[plan.k0:plan.k0 + plan.nzl]).max() / np.abs(ref).max())
+    err = replicas.max_over_ranks(err, dist)
+    if rank == 0:
+        line = {"metric": "grid-point Poisson solves/s", "value": cells * args.steps / (ms / 1e3),
+                "unit": "grid-point Poisson solves/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+                "dtype": "f64", "data": "synthetic",
+                "config": {"workload": case.name + "_zslabs", "grid": [p.nxc, p.nyc, p.nzc], "ranks": ws,
+                           "planes_rank0": plan.nzl, "modes_rank0": plan.nxl,
+                           "exchange": "NCCL all_to_all_single" if dist is not None else "device copies (one rank)",
+                           "l2": "src and phi exceed the L2 at one rank, no flush",
+                           "max_rel_err_vs_one_gpu_solve": err},
+                "stages_ms_rank0": stages,
+                "e2e": None, "gpu_launches": 7 * args.steps, "clocks": clocks}
+        print(json.dumps(line), flush=True)
+    plan.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def run_diagnostics(args):
     """The output-side kernels on C1 (128 x 96 x 128, fields after 20 steps):
     one clcStat accumulation, one 1-D spectra sample (x and z), one 2-D
@@ -805,6 +898,8 @@ def main():
         run_ensemble(args)
     elif args.workload == "poisson_c2":
         run_poisson(args)
+    elif args.workload == "poisson_c2_zslabs":
+        run_poisson_slabs(args)
     elif args.workload == "diagnostics_c1":
         run_diagnostics(args)
     else:

@@ -594,6 +594,50 @@ int64_t paratc_batch_graph_kernels(paratc_batch* b);
 #define PARATC_BATCH_STREAMS 0
 #define PARATC_BATCH_GROUPED 1
 int paratc_batch_set_mode(paratc_batch* b, int mode);
+/* ---- z-slab Poisson solve over several GPUs.  Replaces clcPPE_x1
+ * (src/m_Poisson.f90:352-452) with its six pencil transposes
+ * (transpose_y1_to_x1 ... transpose_x1_to_y1, src/m_Decomp2d.f90:585-1000,
+ * MPI_ALLTOALLW) on a 1-D slab decomposition: rank r of G owns the planes
+ * kc in [k0_r, k0_r + nzl_r) in physical space and the modes kx in
+ * [kx0_r, kx0_r + nxl_r) of the x spectrum (0 <= kx <= nxc/2) after the
+ * first exchange.  One solve is
+ *   paratc_slab_forward   x R2HC of the local planes, packed by destination
+ *   caller: all-to-all    send -> xslab (counts from paratc_slab_counts)
+ *   paratc_slab_middle    z transform, y-Thomas, inverse z transform, in place
+ *   caller: all-to-all    xslab -> recv (the counts swapped)
+ *   paratc_slab_backward  unpack, inverse x transform, scaled by 1/(nxc nzc)
+ * The exchanges are the caller's (NCCL all-to-all between GPUs, through
+ * torch.distributed or ncclSend/ncclRecv; MPI_Alltoallv in a host code), so
+ * the library links no communicator.  Buffers are device arrays of doubles
+ * (complex values as (re, im) pairs): d_send and d_recv hold
+ * 2*nzl*nyc*(nxc/2+1), d_xslab 2*nzc*nyc*nxl doubles.  Every call queues its
+ * kernels on `stream` (a cudaStream_t, NULL = default) and returns. */
+typedef struct paratc_slab paratc_slab;
+/* The balanced split of n items over nranks: rank `rank` gets [*start,
+ * *start + *count), the first n % nranks ranks one item more.  Needs no
+ * device. */
+int paratc_slab_partition(int n, int nranks, int rank, int* start, int* count);
+/* A rank's plan on `device`: planes and modes from paratc_slab_partition over
+ * nzc and nxc/2+1 (nranks <= PARATC_SLAB_MAX_RANKS, at most one rank per
+ * plane and per mode); needs nxc/2 and nzc with factors 2, 3 and 5 only and
+ * 3 <= nyc <= 256. */
+#define PARATC_SLAB_MAX_RANKS 64
+int paratc_slab_create(const paratc_params* prm, const double* yp, int device, int rank, int nranks,
+                       paratc_slab** out);
+int paratc_slab_destroy(paratc_slab* s);
+/* Per-peer counts of the forward exchange, in doubles (nranks entries each):
+ * send[q] goes from this rank to rank q, recv[q] comes from rank q.  The
+ * backward exchange sends recv[q] and receives send[q].  Either may be NULL. */
+int paratc_slab_counts(const paratc_slab* s, int64_t* send, int64_t* recv);
+/* d_src: the local planes, nzl*nyc*nxc doubles (interior layout). */
+int paratc_slab_forward(paratc_slab* s, const double* d_src, double* d_send, void* stream);
+int paratc_slab_middle(paratc_slab* s, double* d_xslab, void* stream);
+/* d_phi: the local planes of phi, nzl*nyc*nxc doubles (interior layout). */
+int paratc_slab_backward(paratc_slab* s, const double* d_recv, double* d_phi, void* stream);
+/* Waits for `stream`; PARATC_ERR_TIMEOUT if a bulk-copy-fed transform of
+ * this plan gave up a bounded wait since the plan was created (its results
+ * are then not to be used). */
+int paratc_slab_sync(paratc_slab* s, void* stream);
 int paratc_batch_get_mode(paratc_batch* b, int* mode);
 /* Kernel launches of one steady step of the batch in its mode (grouped: the
  * plan's launches; streams: the last captured graph's kernels, 0 before). */

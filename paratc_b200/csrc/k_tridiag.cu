@@ -349,7 +349,7 @@ __global__ void __launch_bounds__(512) k_ysolve(DConst cst, DMetric m, double* _
     const bool act = cr < ncol;
     const int s = w * MR + 1;
     const double lam = act ? __ldg(&m.wnx[kx]) + __ldg(&m.wnz[k]) : 0.0;
-    const bool dc = (kx == 0 && k == 0);
+    const bool dc = (kx + cst.kx0 == 0 && k == 0);
     double* col = specd + (size_t)k * ny * ncol + (act ? cr : 0);
     double a[MR], c[MR], f[MR][1];
 #pragma unroll

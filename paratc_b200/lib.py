@@ -38,7 +38,9 @@ EXPORTED = [
     "paratc_set_schedule", "paratc_set_precision", "paratc_get_precision", "paratc_set_wait_limit",
     "paratc_xprofile", "paratc_front_position", "paratc_poisson_refined", "paratc_poisson_refined_async",
     "paratc_autotune_all", "paratc_get_tuning", "paratc_set_tuning", "paratc_batch_set_mode",
-    "paratc_batch_get_mode", "paratc_batch_step_launches",
+    "paratc_batch_get_mode", "paratc_batch_step_launches", "paratc_slab_partition", "paratc_slab_create",
+    "paratc_slab_destroy", "paratc_slab_counts", "paratc_slab_forward", "paratc_slab_middle", "paratc_slab_backward",
+    "paratc_slab_sync",
 ]
 PROF_NKERNELS = 16
 
@@ -140,6 +142,15 @@ def load(path=None):
     L.paratc_batch_get_mode.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]
     L.paratc_batch_step_launches.argtypes = [ctypes.c_void_p]
     L.paratc_batch_step_launches.restype = ctypes.c_int64
+    L.paratc_slab_partition.argtypes = [ctypes.c_int] * 3 + [_i32p] * 2
+    L.paratc_slab_create.argtypes = [ctypes.POINTER(ParatcParams), _dp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                     ctypes.POINTER(ctypes.c_void_p)]
+    L.paratc_slab_destroy.argtypes = [ctypes.c_void_p]
+    L.paratc_slab_counts.argtypes = [ctypes.c_void_p] + [ctypes.POINTER(ctypes.c_int64)] * 2
+    L.paratc_slab_forward.argtypes = [ctypes.c_void_p] * 4
+    L.paratc_slab_middle.argtypes = [ctypes.c_void_p] * 3
+    L.paratc_slab_backward.argtypes = [ctypes.c_void_p] * 4
+    L.paratc_slab_sync.argtypes = [ctypes.c_void_p] * 2
     L.paratc_spectra_reset.argtypes = [ctypes.c_void_p]
     L.paratc_spectra_accumulate.argtypes = [ctypes.c_void_p, ctypes.c_int]
     L.paratc_spectra_get.argtypes = [ctypes.c_void_p, _dp, _dp, ctypes.POINTER(ctypes.c_int),
