@@ -178,10 +178,12 @@ extern "C" int paratc_slab_create(const paratc_params* prm, const double* yp, in
     if (device < 0 || device >= ndev || cudaSetDevice(device) != cudaSuccess) { delete s; return PARATC_ERR_BAD_ARG; }
     s->dev = device;
     cudaDeviceGetAttribute(&s->nsm, cudaDevAttrMultiProcessorCount, device);
-    // the generic transforms' and the partitioned y-solve's shared-memory
-    // limits (attributes of the device; setting them again is harmless)
+    // the transforms' and the partitioned y-solve's shared-memory limits
+    // (attributes of the device; setting them again is harmless)
     fft_init();
     tridiag_init();
+    xt_tma_init();
+    zt_tma_init();
 
     const int nyp = ny + 1;
     std::vector<double> tab;

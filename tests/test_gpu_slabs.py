@@ -96,3 +96,43 @@ def test_slab_create_rejects_bad_splits():
         slabs.SlabPoisson(p, yp, 0, 9)   # more ranks than planes (nzc = 8)
     with pytest.raises(lib.ParatcError):
         slabs.SlabPoisson(p, yp, 2, 2)   # rank outside [0, nranks)
+
+
+_FRESH = r"""
+import sys
+sys.path.insert(0, %r)
+import numpy as np, torch
+from oracle import oracle_lib as ol
+from paratc_b200 import cases, lib, slabs
+case = cases.small_channel(128, 32, 128)
+p = case.params
+yp = lib.mesh_ycoord(case.mesh, p.yly)
+plans = [slabs.SlabPoisson(p, yp, r, 2, device=0) for r in range(2)]  # before any context
+rng = np.random.Generator(np.random.PCG64(21))
+src = rng.standard_normal((p.nzc, p.nyc, p.nxc)); src -= src.mean()
+d = torch.from_numpy(src).cuda()
+srcs = [d[pl.k0:pl.k0 + pl.nzl].contiguous().reshape(-1) for pl in plans]
+phis = [torch.empty_like(s) for s in srcs]
+bufs = [pl.buffers(torch, "cuda") for pl in plans]
+slabs.LocalExchange.solve(plans, srcs, phis, [b[0] for b in bufs], [b[1] for b in bufs])
+for pl in plans:
+    pl.sync()
+phi = torch.cat(phis).reshape(p.nzc, p.nyc, p.nxc).cpu().numpy()
+o = ol.Oracle(p, yp)
+ref = o.poisson(src)
+print("ERR", float(np.abs(phi - ref).max() / np.abs(ref).max()))
+"""
+
+
+def test_slab_plan_in_a_fresh_process():
+    """A plan made before any context (the compiled-length x and z
+    transforms, 128 x 32 x 128 over 2 ranks) in a process of its own."""
+    import os
+    import subprocess
+    import sys
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    out = subprocess.run([sys.executable, "-c", _FRESH % root], capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stderr[-2000:]
+    err = float(out.stdout.split("ERR")[-1])
+    assert err <= TOL, err
