@@ -44,7 +44,6 @@ struct DConst {
     int fp32_rhs;    // 1: the explicit right-hand side computed in FP32 arithmetic (FP64 state)
     int rhs_var;     // compiled launch shape of the FP64 right-hand side (the tuner's pick)
     int helm_var;    // compiled launch shape of the Helmholtz sweeps (the tuner's pick)
-    int kx0;         // global mode number of spectral column 0 (a z-slab rank's share of kx; 0 otherwise)
     double dxC[4], dzC[4], dxxC[5], dzzC[5], IC[4];
     double rdx, rdz;
     double ucrf, xnu, grav[3], sdiff, gev[3], fvv[3];

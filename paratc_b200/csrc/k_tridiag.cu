@@ -349,7 +349,7 @@ __global__ void __launch_bounds__(512) k_ysolve(DConst cst, DMetric m, double* _
     const bool act = cr < ncol;
     const int s = w * MR + 1;
     const double lam = act ? __ldg(&m.wnx[kx]) + __ldg(&m.wnz[k]) : 0.0;
-    const bool dc = (kx + cst.kx0 == 0 && k == 0);
+    const bool dc = (kx == 0 && k == 0);
     double* col = specd + (size_t)k * ny * ncol + (act ? cr : 0);
     double a[MR], c[MR], f[MR][1];
 #pragma unroll
@@ -395,13 +395,16 @@ __global__ void __launch_bounds__(512) k_ysolve(DConst cst, DMetric m, double* _
 // The kx = kz = 0 system has row 1 replaced by phi = 0 (b = 1, c = 0,
 // f = 0; src/m_Poisson.f90:399-404).
 // ---------------------------------------------------------------------------
-__global__ void k_pois_factors(int ny, int M1, int nz, DMetric m, double* __restrict__ rv, double* __restrict__ ar) {
+// dc_here: column 0 is the kx = kz = 0 system (false for a z-slab rank
+// whose modes start above kx = 0; m.wnx then starts at its first mode)
+__device__ __forceinline__ void pois_factors_body(int ny, int M1, int nz, const DMetric& m, double* __restrict__ rv,
+                                                  double* __restrict__ ar, bool dc_here) {
     const int NQ = M1 * nz;
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= NQ) return;
     const int kz = q / M1, kx = q - kz * M1;
     const double wx = m.wnx[kx], wz = m.wnz[kz];
-    const bool dc = (q == 0);
+    const bool dc = dc_here && (q == 0);
     double vecm = dc ? 1.0 : __dadd_rn(__dadd_rn(m.ac2ph[1], wx), wz);
     rv[q] = 1.0 / vecm;
     ar[q] = 0.0;
@@ -413,6 +416,13 @@ __global__ void k_pois_factors(int ny, int M1, int nz, DMetric m, double* __rest
         rv[(size_t)(jc - 1) * NQ + q] = 1.0 / vecm;
         ar[(size_t)(jc - 1) * NQ + q] = arr;
     }
+}
+__global__ void k_pois_factors(int ny, int M1, int nz, DMetric m, double* __restrict__ rv, double* __restrict__ ar) {
+    pois_factors_body(ny, M1, nz, m, rv, ar, true);
+}
+__global__ void k_pois_factors_slab(int ny, int M1, int nz, DMetric m, double* __restrict__ rv, double* __restrict__ ar,
+                                    int dc_here) {
+    pois_factors_body(ny, M1, nz, m, rv, ar, dc_here != 0);
 }
 
 namespace {
@@ -434,7 +444,8 @@ constexpr int YS_U = 8;  // rows loaded ahead of the dependent chain
 // sweeps run in double either way).
 template <class S, class G>
 __device__ __forceinline__ void ys_staged_body(const G& grid, int ny, int M1, int nz, const double* __restrict__ am2ph,
-                                               S* __restrict__ spec, const double* __restrict__ fac) {
+                                               S* __restrict__ spec, const double* __restrict__ fac,
+                                               bool dc_here = true) {
     using R = decltype(S::x);
     extern __shared__ double2 sy[];
     const int lane = threadIdx.x;
@@ -487,7 +498,7 @@ __device__ __forceinline__ void ys_staged_body(const G& grid, int ny, int M1, in
     __syncthreads();
     R* sdd = reinterpret_cast<R*>(sd);
     const int cp = lane >> 1;  // complex column of this lane's real or imaginary part
-    const bool dc = (q0 + cp) == 0;
+    const bool dc = dc_here && (q0 + cp) == 0;
     double fp = 0.0;
     for (int j0 = 0; j0 < ny; j0 += YS_U) {
         double d[YS_U], rv[YS_U], a[YS_U];
@@ -548,7 +559,8 @@ __global__ void __launch_bounds__(32) k_ys_staged(int ny, int M1, int nz, const 
 // storage form); the sweeps run in double either way
 template <class R, class G>
 __device__ __forceinline__ void ys_global_body(const G& grid, int ny, int M1, int nz, const double* __restrict__ am2ph,
-                                               R* __restrict__ specd, const double* __restrict__ fac) {
+                                               R* __restrict__ specd, const double* __restrict__ fac,
+                                               bool dc_here = true) {
     const int W = 2 * M1, NQ = M1 * nz;
     const int g = grid.x() * blockDim.x + threadIdx.x;
     pdl_wait();
@@ -558,7 +570,7 @@ __device__ __forceinline__ void ys_global_body(const G& grid, int ny, int M1, in
     R* col = specd + (size_t)kz * ny * W + cr;
     const double* frv = fac + q;
     const double* far = fac + (size_t)NQ * ny + q;
-    const bool dc = (q == 0);
+    const bool dc = dc_here && (q == 0);
     double fp = 0.0;
     for (int j0 = 0; j0 < ny; j0 += YS_U) {
         R d[YS_U];  // in the storage type: widened at use, so the loads stay in flight
@@ -633,6 +645,23 @@ void launch_pois_factors(cudaStream_t st, const DConst& c, const DMetric& m, dou
     k_pois_factors<<<(NQ + 127) / 128, 128, 0, st>>>(c.ny, M1, c.nz, m, fac, fac + (size_t)NQ * c.ny);
 }
 
+// the same kernels for a z-slab rank's x-mode slab, whose column 0 is the
+// kx = kz = 0 system only on the rank holding kx = 0
+__global__ void __launch_bounds__(32) k_ys_staged_slab(int ny, int M1, int nz, const double* __restrict__ am2ph,
+                                                       double2* __restrict__ spec, const double* __restrict__ fac,
+                                                       int dc_here) {
+    ys_staged_body(OwnGrid{}, ny, M1, nz, am2ph, spec, fac, dc_here != 0);
+}
+__global__ void __launch_bounds__(128) k_ys_global_slab(int ny, int M1, int nz, const double* __restrict__ am2ph,
+                                                        double* __restrict__ specd, const double* __restrict__ fac,
+                                                        int dc_here) {
+    ys_global_body(OwnGrid{}, ny, M1, nz, am2ph, specd, fac, dc_here != 0);
+}
+void launch_pois_factors_slab(cudaStream_t st, const DConst& c, const DMetric& m, double* fac, int dc_here) {
+    const int M1 = c.nx / 2 + 1, NQ = M1 * c.nz;
+    k_pois_factors_slab<<<(NQ + 127) / 128, 128, 0, st>>>(c.ny, M1, c.nz, m, fac, fac + (size_t)NQ * c.ny, dc_here);
+}
+
 // the staged kernel's shared memory: the spectrum block (16 B per complex
 // value, whatever the storage, so that the factor arrays stay 16-byte
 // aligned), the two factor blocks and am2ph
@@ -681,6 +710,16 @@ void launch_ys_grp(cudaStream_t st, int kind, const GrpTab<YsArgs<float2>>* t, i
 void launch_ysolve_fac(cudaStream_t st, const DConst& c, const DMetric& m, double2* spec, const double* fac) {
     ysolve_fac_t(st, c, m, spec, fac);
 }
+void launch_ysolve_fac_slab(cudaStream_t st, const DConst& c, const DMetric& m, double2* spec, const double* fac,
+                            int dc_here) {
+    const int M1 = c.nx / 2 + 1;
+    if (ys_kind(c) == 0)
+        launch_pdl(k_ys_staged_slab, ys_member_grid(c, 0), dim3(32), ys_smem(c, 0), st, c.ny, M1, c.nz, m.am2ph, spec,
+                   fac, dc_here);
+    else
+        launch_pdl(k_ys_global_slab, ys_member_grid(c, 1), dim3(128), 0, st, c.ny, M1, c.nz, m.am2ph,
+                   reinterpret_cast<double*>(spec), fac, dc_here);
+}
 void launch_ysolve_fac(cudaStream_t st, const DConst& c, const DMetric& m, float2* spec, const double* fac) {
     ysolve_fac_t(st, c, m, spec, fac);
 }
@@ -712,6 +751,7 @@ void tridiag_init() {
     cudaFuncSetAttribute(k_ys_staged<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
     cudaFuncSetAttribute(k_ys_staged_grp<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
     cudaFuncSetAttribute(k_ys_staged_grp<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
+    cudaFuncSetAttribute(k_ys_staged_slab, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
     cudaFuncSetAttribute(k_helm_factors, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
 }
 

@@ -106,6 +106,10 @@ void launch_ysolve(cudaStream_t st, const DConst& c, const DMetric& m, double2* 
 
 // k_tridiag.cu: spectral y-solve with the pivots computed once per context
 void launch_pois_factors(cudaStream_t st, const DConst& c, const DMetric& m, double* fac);
+// a z-slab rank's x-mode slab (dc_here: its column 0 is kx = kz = 0)
+void launch_pois_factors_slab(cudaStream_t st, const DConst& c, const DMetric& m, double* fac, int dc_here);
+void launch_ysolve_fac_slab(cudaStream_t st, const DConst& c, const DMetric& m, double2* spec, const double* fac,
+                            int dc_here);
 void launch_ysolve_fac(cudaStream_t st, const DConst& c, const DMetric& m, double2* spec, const double* fac);
 // FP32 storage form: the streaming solve on a float2 spectrum, FP64 sweeps and pivots
 void launch_ysolve_fac(cudaStream_t st, const DConst& c, const DMetric& m, float2* spec, const double* fac);

@@ -31,9 +31,11 @@
 // 16-byte aligned, else the generic k_fft_x_r2c / k_fft_x_c2r; the TMA-fed z
 // transform (k_zt_tma, its tensor map encoded over the caller's x-slab)
 // where nzc has a compiled length, else the generic k_fft_z; and the
-// partitioned y-solve (k_ysolve, pivots computed in place, so no per-column
-// pivot table has to follow the modes).  The solve is the same discrete
-// system as paratc_poisson_device().
+// stored-pivot y-Thomas sweeps of the one-GPU solve (k_ys_staged /
+// k_ys_global bodies), their pivots computed once per plan for the rank's
+// modes (m.wnx offset to kx0; only the rank holding kx = 0 has the
+// kx = kz = 0 system with row 1 replaced by phi = 0).  The solve is the
+// same discrete system as paratc_poisson_device().
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -124,6 +126,7 @@ struct paratc_slab {
     bool xt = false, zt = false;    // compiled-length x / z transforms available
     const void* zt_for = nullptr;   // the x-slab the tensor map below was encoded for
     alignas(64) unsigned char zt_map[128];
+    double* d_fac = nullptr;    // pivots of the x-slab's columns: 1/vecm then arr, nyc*nxl*nzc each
     double* d_tab = nullptr;    // am2ph ac2ph ap2ph (nyp+1 each) | wnx (M1) | wnz (nz) | twx postx twz
     DConst kc{};
     DMetric dm{};
@@ -217,7 +220,8 @@ extern "C" int paratc_slab_create(const paratc_params* prm, const double* yp, in
     s->kc.nx = 2 * (s->nxl - 1);
     s->kc.ny = ny; s->kc.nz = nz; s->kc.nyp = nyp; s->kc.nyt = ny + 2;
     s->kc.nsm = s->nsm;
-    s->kc.kx0 = s->kx0;
+    // the staged sweep copies pivot pairs as 16-byte units: an even column count
+    if ((s->nxl * nz) % 2) s->kc.solver_sel = 2;
     std::memset(&s->dm, 0, sizeof(s->dm));
     s->dm.am2ph = s->d_tab;
     s->dm.ac2ph = s->d_tab + (nyp + 1);
@@ -227,6 +231,18 @@ extern "C" int paratc_slab_create(const paratc_params* prm, const double* yp, in
     s->twx = reinterpret_cast<const double2*>(s->d_tab + o_tw);
     s->postx = s->twx + nx / 2;
     s->twz = s->postx + M1;
+    const size_t nq = (size_t)s->nxl * nz;
+    if ((e = cudaMalloc(&s->d_fac, 2 * nq * ny * sizeof(double))) != cudaSuccess) {
+        std::fprintf(stderr, "paratc_slab_create: %s\n", cudaGetErrorString(e));
+        paratc_slab_destroy(s);
+        return e == cudaErrorMemoryAllocation ? PARATC_ERR_OOM : PARATC_ERR_CUDA;
+    }
+    launch_pois_factors_slab(0, s->kc, s->dm, s->d_fac, s->kx0 == 0);
+    if ((e = cudaGetLastError()) != cudaSuccess || (e = cudaDeviceSynchronize()) != cudaSuccess) {
+        std::fprintf(stderr, "paratc_slab_create: %s\n", cudaGetErrorString(e));
+        paratc_slab_destroy(s);
+        return PARATC_ERR_CUDA;
+    }
     s->xt = xt_tma_supported(nx / 2);
     s->zt = zt_tma_supported(nz);
     *out = s;
@@ -239,6 +255,7 @@ extern "C" int paratc_slab_destroy(paratc_slab* s) {
     if (s->d_spec) cudaFree(s->d_spec);
     if (s->d_tab) cudaFree(s->d_tab);
     if (s->d_err) cudaFree(s->d_err);
+    if (s->d_fac) cudaFree(s->d_fac);
     delete s;
     return PARATC_OK;
 }
@@ -283,7 +300,7 @@ extern "C" int paratc_slab_middle(paratc_slab* s, double* d_xslab, void* stream)
     const bool zt = s->zt && s->zt_for == xs;
     if (zt) launch_zt_tma(st, -1, ncol, s->nz, s->zt_map, s->twz, s->nsm, s->d_err);
     else launch_fft_z(st, -1, s->kc.nx, s->ny, s->nz, xs, s->plz, s->twz);
-    launch_ysolve(st, s->kc, s->dm, xs);
+    launch_ysolve_fac_slab(st, s->kc, s->dm, xs, s->d_fac, s->kx0 == 0);
     if (zt) launch_zt_tma(st, +1, ncol, s->nz, s->zt_map, s->twz, s->nsm, s->d_err);
     else launch_fft_z(st, +1, s->kc.nx, s->ny, s->nz, xs, s->plz, s->twz);
     return slab_finish("paratc_slab_middle");
