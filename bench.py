@@ -788,7 +788,7 @@ def run_poisson_slabs(args):
     torch.cuda.synchronize()
     clocks = sampler.stop()
     plan.sync(st.cuda_stream)
-    ms = replicas.max_over_ranks(a.elapsed_time(b), dist)
+    ms = replicas.max_over_ranks(a.elapsed_time(b), dist, device=local)
     # stage times of one more solve (events between the stages)
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(6)]
     ev[0].record(st); plan.forward(d_src, buf, st.cuda_stream)
@@ -810,7 +810,7 @@ def run_poisson_slabs(args):
     ref = g_phi.cpu().numpy()
     ctx.close()
     err = float(np.abs(phi_local - ref[plan.k0:plan.k0 + plan.nzl]).max() / np.abs(ref).max())
-    err = replicas.max_over_ranks(err, dist)
+    err = replicas.max_over_ranks(err, dist, device=local)
     if rank == 0:
         line = {"metric": "grid-point Poisson solves/s", "value": cells * args.steps / (ms / 1e3),
                 "unit": "grid-point Poisson solves/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
