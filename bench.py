@@ -739,14 +739,17 @@ def run_poisson(args):
 
 def run_poisson_slabs(args):
     """C2's Poisson solve split over the ranks as z slabs (paratc_slab_*):
-    every rank transforms its planes along x, one NCCL all-to-all gives it
-    all planes of its x modes, it solves the z transforms and y-Thomas
-    systems there, a second all-to-all returns the planes, and it transforms
-    them back.  Total work is fixed as N grows (strong scaling); `value` is
-    grid points solved per second of the slowest rank.  With one rank the
-    exchanges are device copies.  Every rank also solves the whole grid on
-    its own GPU (paratc_poisson_device) and reports the largest difference
-    over its planes."""
+    every rank transforms its planes along x, an exchange gives it all
+    planes of its x modes, it solves the z transforms and y-Thomas systems
+    there, a second exchange returns the planes, and it transforms them back.
+    Two forms of the exchange are timed: the peer form (the headline: the
+    library's scatter / gather kernels store into and load from every rank's
+    x-slab, mapped by CUDA IPC) and the all-to-all form (NCCL
+    all_to_all_single; device copies with one rank).  Total work is fixed as
+    N grows (strong scaling); `value` is grid points solved per second of
+    the slowest rank.  Every rank also solves the whole grid on its own GPU
+    (paratc_poisson_device) and reports the largest difference over its
+    planes."""
     import torch
     ws, rank, local = _dist()
     torch.cuda.set_device(local)
@@ -811,18 +814,63 @@ def run_poisson_slabs(args):
     ctx.close()
     err = float(np.abs(phi_local - ref[plan.k0:plan.k0 + plan.nzl]).max() / np.abs(ref).max())
     err = replicas.max_over_ranks(err, dist, device=local)
+    # the peer form: the scatter kernel stores every value into its owner's
+    # x-slab (IPC-mapped across processes), the gather kernel loads it back;
+    # no collective library on the data path
+    peer, why = None, None
+    if dist is None:
+        def peer_solve(out):
+            slabs.LocalPeers.solve([plan], [d_src], [out], stream=st.cuda_stream)
+    else:
+        try:
+            peer = slabs.PeerExchange(plan, dist, stream=st.cuda_stream)
+        except Exception as e:  # every rank learns whether all ranks mapped their peers
+            why = "peer mapping failed on rank %d: %s" % (rank, e)
+        ok = replicas.max_over_ranks(0.0 if peer is not None else 1.0, dist, device=local) == 0.0
+
+        def peer_solve(out):
+            peer.solve(d_src, out)
+        if not ok:
+            peer_solve = None
+    peer_line = None
+    if peer_solve is not None:
+        d_phi2 = torch.empty_like(d_src)
+        for _ in range(args.warmup):
+            peer_solve(d_phi2)
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        a.record(st)
+        for _ in range(args.steps):
+            peer_solve(d_phi2)
+        b.record(st)
+        torch.cuda.synchronize()
+        plan.sync(st.cuda_stream)
+        ms_p = replicas.max_over_ranks(a.elapsed_time(b), dist, device=local)
+        same = float(np.array_equal(d_phi2.cpu().numpy().reshape(plan.nzl, p.nyc, p.nxc), phi_local))
+        same = replicas.max_over_ranks(1.0 - same, dist, device=local) == 0.0
+        peer_line = {"value": cells * args.steps / (ms_p / 1e3), "ms_per_step": ms_p / args.steps,
+                     "bitwise_equal_to_all_to_all_form": bool(same),
+                     "exchange": "scatter / gather kernels into IPC-mapped x-slabs" if dist is not None
+                                 else "scatter / gather kernels (one rank)"}
+        if peer is not None:
+            peer.close()
+    nccl_line = {"value": cells * args.steps / (ms / 1e3), "ms_per_step": ms / args.steps,
+                 "exchange": "NCCL all_to_all_single" if dist is not None else "device copies (one rank)",
+                 "stages_ms_rank0": stages}
+    head = peer_line if peer_line is not None else nccl_line
     if rank == 0:
-        line = {"metric": "grid-point Poisson solves/s", "value": cells * args.steps / (ms / 1e3),
+        line = {"metric": "grid-point Poisson solves/s", "value": head["value"],
                 "unit": "grid-point Poisson solves/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
-                "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
-                "dtype": "f64", "data": "synthetic",
+                "ms_per_step": head["ms_per_step"], "higher_is_better": True, "scaling": "strong",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic",
                 "config": {"workload": case.name + "_zslabs", "grid": [p.nxc, p.nyc, p.nzc], "ranks": ws,
-                           "planes_rank0": plan.nzl, "modes_rank0": plan.nxl,
-                           "exchange": "NCCL all_to_all_single" if dist is not None else "device copies (one rank)",
+                           "planes_rank0": plan.nzl, "modes_rank0": plan.nxl, "exchange": head["exchange"],
                            "l2": "src and phi exceed the L2 at one rank, no flush",
                            "max_rel_err_vs_one_gpu_solve": err},
-                "stages_ms_rank0": stages,
-                "e2e": None, "gpu_launches": 7 * args.steps, "clocks": clocks}
+                "peer_form": peer_line if peer_line is not None else {"unavailable": why},
+                "all_to_all_form": nccl_line,
+                "e2e": None, "gpu_launches": (5 if peer_line is not None else 7) * args.steps, "clocks": clocks}
         print(json.dumps(line), flush=True)
     plan.close()
     if dist is not None:

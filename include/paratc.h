@@ -634,6 +634,28 @@ int paratc_slab_forward(paratc_slab* s, const double* d_src, double* d_send, voi
 int paratc_slab_middle(paratc_slab* s, double* d_xslab, void* stream);
 /* d_phi: the local planes of phi, nzl*nyc*nxc doubles (interior layout). */
 int paratc_slab_backward(paratc_slab* s, const double* d_recv, double* d_phi, void* stream);
+/* Peer form: no collective library.  Each plan owns an x-slab
+ * (paratc_slab_xslab, 2*nzc*nyc*nxl doubles); xslabs[q] (nranks device
+ * pointers, host array) is rank q's, this rank's own included, mapped here
+ * with paratc_ipc_open when q is another process.  forward_peers transforms
+ * the local planes and stores every value straight into its owner's x-slab
+ * (plain stores over NVLink); backward_peers loads the rank's planes back
+ * from all x-slabs and transforms them.  The caller orders the ranks: every
+ * rank's forward_peers completes before any rank's paratc_slab_middle (on
+ * its own x-slab), every middle before any backward_peers, every
+ * backward_peers before the next forward_peers (a stream synchronisation
+ * and a barrier of the processes at each point).  Ranks in one process on
+ * one stream need no barrier. */
+double* paratc_slab_xslab(paratc_slab* s);
+int paratc_slab_forward_peers(paratc_slab* s, const double* d_src, const double* const* xslabs, void* stream);
+int paratc_slab_backward_peers(paratc_slab* s, const double* const* xslabs, double* d_phi, void* stream);
+/* CUDA IPC of a device allocation's base address (cudaIpcGetMemHandle /
+ * cudaIpcOpenMemHandle with lazy peer access): the handle is
+ * PARATC_IPC_HANDLE_BYTES opaque bytes to send to the other processes. */
+#define PARATC_IPC_HANDLE_BYTES 64
+int paratc_ipc_get_handle(const void* d_ptr, void* handle);
+int paratc_ipc_open(const void* handle, void** d_ptr);
+int paratc_ipc_close(void* d_ptr);
 /* Waits for `stream`; PARATC_ERR_TIMEOUT if a bulk-copy-fed transform of
  * this plan gave up a bounded wait since the plan was created (its results
  * are then not to be used). */

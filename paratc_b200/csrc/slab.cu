@@ -26,6 +26,17 @@
 // The only reordering is the pack of the forward exchange and the matching
 // unpack of the backward one (k_slab_pack), an HBM-bound copy.
 //
+// Peer form (no collective library): every rank's plan owns its x-slab,
+// whose device address the other ranks map (CUDA IPC, paratc_ipc_*); the
+// forward scatter (k_slab_scatter) stores each value of the local planes'
+// spectrum straight into its owner's x-slab over NVLink, and the backward
+// gather loads them back from there, so pack, exchange and unpack are one
+// kernel each way, with plain loads and stores to peer memory (no TMA, no
+// multicast).  The ordering between ranks is the caller's: all ranks'
+// scatters complete before any rank's middle step, all middle steps before
+// any gather, all gathers before the next scatter (a stream synchronisation
+// and a barrier of the host processes at each of the three points).
+//
 // The kernels are the library's own: the bulk-copy-fed x transforms
 // (k_xf_tma / k_xb_tma) where nxc/2 has a compiled length and the arrays are
 // 16-byte aligned, else the generic k_fft_x_r2c / k_fft_x_c2r; the TMA-fed z
@@ -83,6 +94,27 @@ __global__ void __launch_bounds__(256) k_slab_pack(int dir, int nzl, int ny, int
     }
 }
 
+struct SlabPeers {
+    double2* p[PARATC_SLAB_MAX_RANKS];
+};
+
+// dir 0: scatter the local planes' spectrum into every rank's x-slab;
+// dir 1: gather it back.  Value (kl, jc, kx) of this rank (planes from k0)
+// lives in owner q's x-slab at ((k0 + kl)*ny + jc-1)*nxl_q + kx - kx0_q.
+__global__ void __launch_bounds__(256) k_slab_scatter(int dir, int nzl, int ny, int M1, int G, int k0,
+                                                      double2* __restrict__ spec, SlabPeers peers) {
+    const size_t total = (size_t)nzl * ny * M1;
+    for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
+        const int kx = (int)(e % M1);
+        const size_t row = e / M1;
+        const int q = split_owner(M1, G, kx);
+        const int kx0 = split_start(M1, G, q), nxl = split_count(M1, G, q);
+        double2* x = peers.p[q] + ((size_t)k0 * ny + row) * nxl + (kx - kx0);
+        if (dir == 0) *x = spec[e];
+        else spec[e] = *x;
+    }
+}
+
 bool radix_plan(int n, FftPlan& pl) {
     pl.n = n;
     pl.nr = 0;
@@ -122,6 +154,7 @@ struct paratc_slab {
     double normfft = 0.0;
     FftPlan plx{}, plz{};
     double2* d_spec = nullptr;  // [nzl][ny][M1]
+    double2* d_xslab = nullptr; // [nz][ny][nxl], the plan's own x-slab (peer form)
     unsigned int* d_err = nullptr;  // bounded-wait failure word of the TMA-fed kernels (+ their poll setting)
     bool xt = false, zt = false;    // compiled-length x / z transforms available
     const void* zt_for = nullptr;   // the x-slab the tensor map below was encoded for
@@ -232,7 +265,8 @@ extern "C" int paratc_slab_create(const paratc_params* prm, const double* yp, in
     s->postx = s->twx + nx / 2;
     s->twz = s->postx + M1;
     const size_t nq = (size_t)s->nxl * nz;
-    if ((e = cudaMalloc(&s->d_fac, 2 * nq * ny * sizeof(double))) != cudaSuccess) {
+    if ((e = cudaMalloc(&s->d_fac, 2 * nq * ny * sizeof(double))) != cudaSuccess ||
+        (e = cudaMalloc(&s->d_xslab, nq * ny * sizeof(double2))) != cudaSuccess) {
         std::fprintf(stderr, "paratc_slab_create: %s\n", cudaGetErrorString(e));
         paratc_slab_destroy(s);
         return e == cudaErrorMemoryAllocation ? PARATC_ERR_OOM : PARATC_ERR_CUDA;
@@ -256,6 +290,7 @@ extern "C" int paratc_slab_destroy(paratc_slab* s) {
     if (s->d_tab) cudaFree(s->d_tab);
     if (s->d_err) cudaFree(s->d_err);
     if (s->d_fac) cudaFree(s->d_fac);
+    if (s->d_xslab) cudaFree(s->d_xslab);
     delete s;
     return PARATC_OK;
 }
@@ -318,6 +353,76 @@ extern "C" int paratc_slab_backward(paratc_slab* s, const double* d_recv, double
     else
         launch_fft_x_c2r(st, s->nx, s->ny, s->nzl * s->ny, s->d_spec, d_phi, s->plx, s->twx, s->postx, s->normfft, 0);
     return slab_finish("paratc_slab_backward");
+}
+
+extern "C" double* paratc_slab_xslab(paratc_slab* s) { return s ? reinterpret_cast<double*>(s->d_xslab) : nullptr; }
+
+static int slab_peers(const paratc_slab* s, const double* const* xslabs, SlabPeers& pp) {
+    if (!xslabs) return PARATC_ERR_BAD_ARG;
+    for (int q = 0; q < s->nranks; q++) {
+        if (!xslabs[q] || !aligned16(xslabs[q])) return PARATC_ERR_BAD_ARG;
+        pp.p[q] = const_cast<double2*>(reinterpret_cast<const double2*>(xslabs[q]));
+    }
+    return PARATC_OK;
+}
+
+extern "C" int paratc_slab_forward_peers(paratc_slab* s, const double* d_src, const double* const* xslabs,
+                                         void* stream) {
+    SlabPeers pp{};
+    if (!s || !d_src || slab_peers(s, xslabs, pp) != PARATC_OK) return PARATC_ERR_BAD_ARG;
+    cudaSetDevice(s->dev);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const size_t n = (size_t)s->nzl * s->ny * s->M1;
+    if (s->xt && aligned16(d_src))
+        launch_xf_tma(st, s->nx, s->ny, s->nzl, d_src, s->d_spec, s->twx, s->postx, s->nsm, s->d_err);
+    else
+        launch_fft_x_r2c(st, s->nx, s->nzl * s->ny, d_src, s->d_spec, s->plx, s->twx, s->postx);
+    k_slab_scatter<<<grid_blocks(n, s->nsm), 256, 0, st>>>(0, s->nzl, s->ny, s->M1, s->nranks, s->k0, s->d_spec, pp);
+    return slab_finish("paratc_slab_forward_peers");
+}
+
+extern "C" int paratc_slab_backward_peers(paratc_slab* s, const double* const* xslabs, double* d_phi, void* stream) {
+    SlabPeers pp{};
+    if (!s || !d_phi || slab_peers(s, xslabs, pp) != PARATC_OK) return PARATC_ERR_BAD_ARG;
+    cudaSetDevice(s->dev);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const size_t n = (size_t)s->nzl * s->ny * s->M1;
+    k_slab_scatter<<<grid_blocks(n, s->nsm), 256, 0, st>>>(1, s->nzl, s->ny, s->M1, s->nranks, s->k0, s->d_spec, pp);
+    if (s->xt && aligned16(d_phi))
+        launch_xb_tma(st, s->nx, s->ny, s->nzl, s->d_spec, d_phi, s->twx, s->postx, s->normfft, 0, s->nsm, s->d_err);
+    else
+        launch_fft_x_c2r(st, s->nx, s->ny, s->nzl * s->ny, s->d_spec, d_phi, s->plx, s->twx, s->postx, s->normfft, 0);
+    return slab_finish("paratc_slab_backward_peers");
+}
+
+extern "C" int paratc_ipc_get_handle(const void* d_ptr, void* handle) {
+    if (!d_ptr || !handle) return PARATC_ERR_BAD_ARG;
+    cudaIpcMemHandle_t h;
+    const cudaError_t e = cudaIpcGetMemHandle(&h, const_cast<void*>(d_ptr));
+    if (e != cudaSuccess) {
+        std::fprintf(stderr, "paratc_ipc_get_handle: %s\n", cudaGetErrorString(e));
+        return PARATC_ERR_CUDA;
+    }
+    static_assert(sizeof(h) <= PARATC_IPC_HANDLE_BYTES, "IPC handle size");
+    std::memcpy(handle, &h, sizeof(h));
+    return PARATC_OK;
+}
+
+extern "C" int paratc_ipc_open(const void* handle, void** d_ptr) {
+    if (!handle || !d_ptr) return PARATC_ERR_BAD_ARG;
+    cudaIpcMemHandle_t h;
+    std::memcpy(&h, handle, sizeof(h));
+    const cudaError_t e = cudaIpcOpenMemHandle(d_ptr, h, cudaIpcMemLazyEnablePeerAccess);
+    if (e != cudaSuccess) {
+        std::fprintf(stderr, "paratc_ipc_open: %s\n", cudaGetErrorString(e));
+        return PARATC_ERR_CUDA;
+    }
+    return PARATC_OK;
+}
+
+extern "C" int paratc_ipc_close(void* d_ptr) {
+    if (!d_ptr) return PARATC_ERR_BAD_ARG;
+    return cudaIpcCloseMemHandle(d_ptr) == cudaSuccess ? PARATC_OK : PARATC_ERR_CUDA;
 }
 
 extern "C" int paratc_slab_sync(paratc_slab* s, void* stream) {

@@ -40,7 +40,8 @@ EXPORTED = [
     "paratc_autotune_all", "paratc_get_tuning", "paratc_set_tuning", "paratc_batch_set_mode",
     "paratc_batch_get_mode", "paratc_batch_step_launches", "paratc_slab_partition", "paratc_slab_create",
     "paratc_slab_destroy", "paratc_slab_counts", "paratc_slab_forward", "paratc_slab_middle", "paratc_slab_backward",
-    "paratc_slab_sync",
+    "paratc_slab_sync", "paratc_slab_xslab", "paratc_slab_forward_peers", "paratc_slab_backward_peers",
+    "paratc_ipc_get_handle", "paratc_ipc_open", "paratc_ipc_close",
 ]
 PROF_NKERNELS = 16
 
@@ -151,6 +152,13 @@ def load(path=None):
     L.paratc_slab_middle.argtypes = [ctypes.c_void_p] * 3
     L.paratc_slab_backward.argtypes = [ctypes.c_void_p] * 4
     L.paratc_slab_sync.argtypes = [ctypes.c_void_p] * 2
+    L.paratc_slab_xslab.argtypes = [ctypes.c_void_p]
+    L.paratc_slab_xslab.restype = ctypes.c_void_p
+    L.paratc_slab_forward_peers.argtypes = [ctypes.c_void_p] * 4
+    L.paratc_slab_backward_peers.argtypes = [ctypes.c_void_p] * 4
+    L.paratc_ipc_get_handle.argtypes = [ctypes.c_void_p] * 2
+    L.paratc_ipc_open.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]
+    L.paratc_ipc_close.argtypes = [ctypes.c_void_p]
     L.paratc_spectra_reset.argtypes = [ctypes.c_void_p]
     L.paratc_spectra_accumulate.argtypes = [ctypes.c_void_p, ctypes.c_int]
     L.paratc_spectra_get.argtypes = [ctypes.c_void_p, _dp, _dp, ctypes.POINTER(ctypes.c_int),

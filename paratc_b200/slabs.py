@@ -15,6 +15,15 @@ torch.distributed.all_to_all_single (NCCL between GPUs, gloo on CPU
 tensors); `LocalExchange` runs several ranks' plans in one process on one
 device and moves the blocks with device copies.  Sizes are in doubles
 (complex values as (re, im) pairs).
+
+The peer form needs no collective library: every plan owns its x-slab, the
+other ranks map it (CUDA IPC), and the library's scatter kernel stores each
+value of the local spectrum straight into its owner's x-slab over NVLink
+(the gather loads it back).  `PeerExchange` does the IPC mapping through
+torch.distributed and orders the ranks with a stream synchronisation and a
+barrier at the three points where one rank's kernels read or overwrite
+another's x-slab; `LocalPeers` runs several plans in one process on one
+stream, where stream order is enough.
 """
 import ctypes
 
@@ -126,6 +135,27 @@ class SlabPoisson:
         self._check(self._L.paratc_slab_backward(self._h, self._ptr(recv), self._ptr(phi), self._stream(stream)),
                     "paratc_slab_backward")
 
+    @property
+    def xslab_ptr(self):
+        """Device address of the plan's own x-slab (the peer form)."""
+        return int(self._L.paratc_slab_xslab(self._h))
+
+    @staticmethod
+    def _table(ptrs):
+        return (ctypes.c_void_p * len(ptrs))(*[ctypes.c_void_p(int(p)) for p in ptrs])
+
+    def forward_peers(self, src, xslab_ptrs, stream=None):
+        self._check(self._L.paratc_slab_forward_peers(self._h, self._ptr(src), self._table(xslab_ptrs),
+                                                      self._stream(stream)), "paratc_slab_forward_peers")
+
+    def backward_peers(self, xslab_ptrs, phi, stream=None):
+        self._check(self._L.paratc_slab_backward_peers(self._h, self._table(xslab_ptrs), self._ptr(phi),
+                                                       self._stream(stream)), "paratc_slab_backward_peers")
+
+    def middle_own(self, stream=None):
+        self._check(self._L.paratc_slab_middle(self._h, ctypes.c_void_p(self.xslab_ptr), self._stream(stream)),
+                    "paratc_slab_middle")
+
     def sync(self, stream=None):
         """Waits for the stream; raises if a bounded wait of the plan's
         bulk-copy-fed transforms ran out (PARATC_ERR_TIMEOUT)."""
@@ -185,3 +215,68 @@ class LocalExchange:
         LocalExchange.all_to_all(xslabs, sends, [p.recv_counts for p in plans], [p.send_counts for p in plans])
         for p, b, f in zip(plans, sends, phis):
             p.backward(b, f)
+
+
+class LocalPeers:
+    """The peer form with all ranks' plans in one process on one device:
+    the x-slab table is the plans' own x-slabs, stream order keeps the
+    stages apart."""
+
+    @staticmethod
+    def solve(plans, srcs, phis, stream=None):
+        ptrs = [p.xslab_ptr for p in plans]
+        for p, s in zip(plans, srcs):
+            p.forward_peers(s, ptrs, stream)
+        for p in plans:
+            p.middle_own(stream)
+        for p, f in zip(plans, phis):
+            p.backward_peers(ptrs, f, stream)
+
+
+class PeerExchange:
+    """The peer form across processes (one rank per GPU): maps every other
+    rank's x-slab through CUDA IPC (handles exchanged with
+    torch.distributed.all_gather_object) and runs a solve with a stream
+    synchronisation and a barrier where the ranks must wait for one another."""
+
+    def __init__(self, plan, dist, stream=None):
+        L = load()
+        self.plan, self.dist, self.stream = plan, dist, stream
+        h = (ctypes.c_char * 64)()
+        own = plan.xslab_ptr
+        rc = L.paratc_ipc_get_handle(ctypes.c_void_p(own), h)
+        if rc != PARATC_OK:
+            raise ParatcError(rc, "paratc_ipc_get_handle")
+        handles = [None] * plan.nranks
+        dist.all_gather_object(handles, bytes(h))
+        self.ptrs, self._opened = [], []
+        for q, hq in enumerate(handles):
+            if q == plan.rank:
+                self.ptrs.append(own)
+                continue
+            buf = (ctypes.c_char * 64).from_buffer_copy(hq)
+            p = ctypes.c_void_p()
+            rc = L.paratc_ipc_open(buf, ctypes.byref(p))
+            if rc != PARATC_OK:
+                raise ParatcError(rc, "paratc_ipc_open(rank %d)" % q)
+            self.ptrs.append(int(p.value))
+            self._opened.append(p)
+
+    def _wait_all(self):
+        self.plan.sync(self.stream)
+        self.dist.barrier()
+
+    def solve(self, src, phi):
+        self.plan.forward_peers(src, self.ptrs, self.stream)
+        self._wait_all()       # every rank's values are in every x-slab
+        self.plan.middle_own(self.stream)
+        self._wait_all()       # every x-slab solved
+        self.plan.backward_peers(self.ptrs, phi, self.stream)
+        self._wait_all()       # every rank has read its planes back
+
+    def close(self):
+        L = load()
+        for p in self._opened:
+            L.paratc_ipc_close(p)
+        self._opened = []
+

@@ -136,3 +136,48 @@ def test_slab_plan_in_a_fresh_process():
     assert out.returncode == 0, out.stderr[-2000:]
     err = float(out.stdout.split("ERR")[-1])
     assert err <= TOL, err
+
+
+@pytest.mark.parametrize("dims,g", [((64, 48, 40), 1), ((64, 48, 40), 3), ((128, 96, 128), 4), ((96, 20, 30), 7)])
+def test_slab_peer_form_matches_exchange_form(dims, g):
+    """The peer form (scatter into every rank's x-slab, gather back) gives
+    bitwise the all-to-all form's potential, and the one-GPU solve's to 1e-12."""
+    import torch
+
+    case = cases.small_channel(*dims)
+    p = case.params
+    yp = lib.mesh_ycoord(case.mesh, p.yly)
+    src = torch.from_numpy(_source((p.nzc, p.nyc, p.nxc), 13)).cuda()
+    phi_x = _slab_solve(p, yp, src, g).cpu().numpy()
+    plans = [slabs.SlabPoisson(p, yp, r, g, device=0) for r in range(g)]
+    srcs = [src[pl.k0:pl.k0 + pl.nzl].contiguous().reshape(-1) for pl in plans]
+    for rep in range(2):  # twice: x-slabs and spectra are reused
+        phis = [torch.full_like(s, float("nan")) for s in srcs]
+        slabs.LocalPeers.solve(plans, srcs, phis)
+        torch.cuda.synchronize()
+        for pl in plans:
+            pl.sync()
+        phi = torch.cat(phis).reshape(p.nzc, p.nyc, p.nxc).cpu().numpy()
+        assert np.array_equal(phi, phi_x), (dims, g, rep)
+    ref = lib.ChannelSystem(p, yp)
+    phi_ref = torch.empty_like(src)
+    ref.poisson_device(src.data_ptr(), phi_ref.data_ptr())
+    b = phi_ref.cpu().numpy()
+    assert np.abs(phi_x - b).max() / np.abs(b).max() <= TOL
+    ref.close()
+    for pl in plans:
+        pl.close()
+
+
+def test_ipc_handle_of_a_plan_x_slab():
+    """The handle the peer form sends to other processes is produced for the
+    plan's own allocation (opening it needs another process)."""
+    import ctypes
+
+    case = cases.small_channel(16, 12, 8)
+    p = case.params
+    pl = slabs.SlabPoisson(p, lib.mesh_ycoord(case.mesh, p.yly), 0, 2, device=0)
+    h = (ctypes.c_char * 64)()
+    assert lib.load().paratc_ipc_get_handle(ctypes.c_void_p(pl.xslab_ptr), h) == 0
+    assert any(bytes(h))
+    pl.close()
