@@ -239,28 +239,22 @@ class PeerExchange:
     torch.distributed.all_gather_object) and runs a solve with a stream
     synchronisation and a barrier where the ranks must wait for one another."""
 
-    def __init__(self, plan, dist, stream=None):
-        L = load()
+    def __init__(self, plan, dist, stream=None, ipc=None):
+        """ipc: (get_handle(ptr) -> bytes, open(bytes) -> ptr, close(ptr)),
+        the library's CUDA IPC calls by default."""
         self.plan, self.dist, self.stream = plan, dist, stream
-        h = (ctypes.c_char * 64)()
+        self._ipc = ipc or (ipc_get_handle, ipc_open, ipc_close)
         own = plan.xslab_ptr
-        rc = L.paratc_ipc_get_handle(ctypes.c_void_p(own), h)
-        if rc != PARATC_OK:
-            raise ParatcError(rc, "paratc_ipc_get_handle")
         handles = [None] * plan.nranks
-        dist.all_gather_object(handles, bytes(h))
+        dist.all_gather_object(handles, self._ipc[0](own))
         self.ptrs, self._opened = [], []
         for q, hq in enumerate(handles):
             if q == plan.rank:
                 self.ptrs.append(own)
                 continue
-            buf = (ctypes.c_char * 64).from_buffer_copy(hq)
-            p = ctypes.c_void_p()
-            rc = L.paratc_ipc_open(buf, ctypes.byref(p))
-            if rc != PARATC_OK:
-                raise ParatcError(rc, "paratc_ipc_open(rank %d)" % q)
-            self.ptrs.append(int(p.value))
-            self._opened.append(p)
+            ptr = self._ipc[1](hq)
+            self.ptrs.append(ptr)
+            self._opened.append(ptr)
 
     def _wait_all(self):
         self.plan.sync(self.stream)
@@ -275,8 +269,30 @@ class PeerExchange:
         self._wait_all()       # every rank has read its planes back
 
     def close(self):
-        L = load()
         for p in self._opened:
-            L.paratc_ipc_close(p)
+            self._ipc[2](p)
         self._opened = []
+
+
+def ipc_get_handle(ptr):
+    """The CUDA IPC handle (bytes) of the device allocation at ptr."""
+    h = (ctypes.c_char * 64)()
+    rc = load().paratc_ipc_get_handle(ctypes.c_void_p(int(ptr)), h)
+    if rc != PARATC_OK:
+        raise ParatcError(rc, "paratc_ipc_get_handle")
+    return bytes(h)
+
+
+def ipc_open(handle):
+    """Maps another process's allocation; returns its device address here."""
+    buf = (ctypes.c_char * 64).from_buffer_copy(handle)
+    p = ctypes.c_void_p()
+    rc = load().paratc_ipc_open(buf, ctypes.byref(p))
+    if rc != PARATC_OK:
+        raise ParatcError(rc, "paratc_ipc_open")
+    return int(p.value)
+
+
+def ipc_close(ptr):
+    load().paratc_ipc_close(ctypes.c_void_p(int(ptr)))
 

@@ -3,7 +3,9 @@ split against the library's paratc_slab_partition, the per-peer counts, the
 pack map of the forward exchange, and the two all-to-all exchanges of a
 solve run through the same exchange function the GPUs use (gloo ranks here,
 NCCL on GPUs) on an index-tagged spectrum: after the first exchange every
-rank must hold all planes of its modes, after the second its own planes."""
+rank must hold all planes of its modes, after the second its own planes.
+The peer form's host side (IPC handle exchange, pointer table, the waits
+between its stages) runs on gloo ranks with a fake plan."""
 import json
 import os
 import socket
@@ -108,3 +110,66 @@ def test_exchanges_over_gloo_ranks(tmp_path, ws, dims):
     for r in range(ws):
         res = json.load(open(tmp_path / ("rank%d.json" % r)))
         assert res == {"xslab": True, "planes": True}, (r, res)
+
+
+class _FakePlan:
+    """Records the peer form's calls in order (no device)."""
+
+    def __init__(self, rank, nranks, log):
+        self.rank, self.nranks, self.log = rank, nranks, log
+        self.xslab_ptr = 0x1000 * (rank + 1)
+
+    def forward_peers(self, src, ptrs, stream):
+        self.log.append(("forward", list(ptrs)))
+
+    def middle_own(self, stream):
+        self.log.append(("middle",))
+
+    def backward_peers(self, ptrs, phi, stream):
+        self.log.append(("backward", list(ptrs)))
+
+    def sync(self, stream):
+        self.log.append(("sync",))
+
+
+def _peer_worker(rank, ws, port, out_dir):
+    os.environ.update({"MASTER_ADDR": "127.0.0.1", "MASTER_PORT": str(port), "RANK": str(rank),
+                       "WORLD_SIZE": str(ws), "LOCAL_RANK": str(rank)})
+    sys.path.insert(0, ROOT)
+    from paratc_b200 import replicas, slabs as sl
+    dist = replicas.init("gloo", timeout_s=60)
+    log = []
+    opened, closed = [], []
+    ipc = (lambda ptr: b"H%08x" % ptr,                      # a handle names the owner's address
+           lambda h: (opened.append(h), 0x900000 + int(h[1:], 16))[1],  # mapped at another address here
+           lambda ptr: closed.append(ptr))
+    plan = _FakePlan(rank, ws, log)
+    pe = sl.PeerExchange(plan, dist, ipc=ipc)
+    orig = dist.barrier
+    dist.barrier = lambda *a, **k: (log.append(("barrier",)), orig())[1]
+    pe.solve(None, None)
+    dist.barrier = orig
+    pe.close()
+    dist.barrier()
+    dist.destroy_process_group()
+    with open(os.path.join(out_dir, "peer%d.json" % rank), "w") as f:
+        json.dump({"ptrs": pe.ptrs, "log": log, "opened": [h.decode() for h in opened], "closed": closed}, f)
+
+
+def test_peer_exchange_over_gloo_ranks(tmp_path):
+    """The peer form's host side on 3 gloo ranks with a fake plan and fake
+    IPC: every rank's table holds its own x-slab at its own index and the
+    others' mapped addresses, and each solve is scatter, wait, middle, wait,
+    gather, wait (a stream synchronisation and a barrier at each wait)."""
+    ws = 3
+    mp.start_processes(_peer_worker, args=(ws, _free_port(), str(tmp_path)), nprocs=ws, join=True,
+                       start_method="spawn")
+    for r in range(ws):
+        res = json.load(open(tmp_path / ("peer%d.json" % r)))
+        want = [0x1000 * (q + 1) if q == r else 0x900000 + 0x1000 * (q + 1) for q in range(ws)]
+        assert res["ptrs"] == want
+        assert sorted(res["opened"]) == sorted("H%08x" % (0x1000 * (q + 1)) for q in range(ws) if q != r)
+        assert sorted(res["closed"]) == sorted(p for q, p in enumerate(want) if q != r)
+        kinds = [e[0] for e in res["log"]]
+        assert kinds == ["forward", "sync", "barrier", "middle", "sync", "barrier", "backward", "sync", "barrier"]
+        assert res["log"][0][1] == want and res["log"][6][1] == want
