@@ -81,11 +81,35 @@ __device__ __forceinline__ void xt_fail(unsigned long long* mbar, int it, int nb
     }
 }
 
-template <int N>
-__global__ void __launch_bounds__(XT<N>::P, XT<N>::MINB)
-    k_xb_tma(int nrows, int ny, const double2* __restrict__ spec, double* __restrict__ phi,
-             const double2* __restrict__ twN, const double2* __restrict__ post, double scale, int padded,
-             unsigned int* __restrict__ err) {
+// Where the inverse finds spectrum row g: one contiguous row of the
+// spectrum (RowsContig), or the segments of the row that the ranks of a
+// z-slab decomposition hold in their x-slabs (RowsGathered: modes
+// [kx0_q, kx0_q + nxl_q) of local row g = (kl, jc) in rank q's x-slab at
+// ((k0*ny + g)*nxl_q), one bulk copy per segment; the x-slabs may be other
+// GPUs' memory, mapped here, read by plain (non-multicast) bulk copies).
+struct RowsContig {
+    const double2* spec;
+    __device__ __forceinline__ void load(double2* dst, int g, int M1, unsigned long long* mbar) const {
+        tma::bulk_load(dst, spec + (size_t)g * M1, M1 * (unsigned)sizeof(double2), mbar);
+    }
+};
+struct RowsGathered {
+    const XtGather* t;  // the kernel's __grid_constant__ parameter
+    int ny;
+    __device__ __forceinline__ void load(double2* dst, int g, int M1, unsigned long long* mbar) const {
+        const int G = t->G, base = M1 / G, rem = M1 - base * G;
+        const size_t row = (size_t)t->k0 * ny + g;
+        for (int q = 0; q < G; q++) {
+            const int kx0 = q * base + (q < rem ? q : rem), nxl = base + (q < rem ? 1 : 0);
+            tma::bulk_load(dst + kx0, t->p[q] + row * nxl, nxl * (unsigned)sizeof(double2), mbar);
+        }
+    }
+};
+
+template <int N, class Rows>
+__device__ __forceinline__ void xb_tma_body(int nrows, int ny, const Rows& rows, double* __restrict__ phi,
+                                            const double2* __restrict__ twN, const double2* __restrict__ post,
+                                            double scale, int padded, unsigned int* __restrict__ err) {
     constexpr int B = XT<N>::B, P = XT<N>::P, PITCH = XT<N>::PITCH, M1 = N + 1;
     constexpr unsigned SB = XT<N>::STAGE;
     constexpr ff::Sched SC = ff::make_sched(N);
@@ -109,8 +133,7 @@ __global__ void __launch_bounds__(XT<N>::P, XT<N>::MINB)
     auto issue = [&](int s, int bt) {
         const int g0 = bt * B, nv = min(B, nrows - g0);
         tma::mbar_expect_tx(&mbar[s], (unsigned)nv * M1 * (unsigned)sizeof(double2));
-        for (int b = 0; b < nv; b++)
-            tma::bulk_load(stage[s] + b * PITCH, spec + (size_t)(g0 + b) * M1, M1 * (unsigned)sizeof(double2), &mbar[s]);
+        for (int b = 0; b < nv; b++) rows.load(stage[s] + b * PITCH, g0 + b, M1, &mbar[s]);
     };
     if (tid == 0) {
         if ((int)blockIdx.x < nb) issue(0, blockIdx.x);
@@ -181,6 +204,23 @@ __global__ void __launch_bounds__(XT<N>::P, XT<N>::MINB)
         tma::bulk_wait0();
         if (s_bad) xt_fail(mbar, it, nb, err);
     }
+}
+
+template <int N>
+__global__ void __launch_bounds__(XT<N>::P, XT<N>::MINB)
+    k_xb_tma(int nrows, int ny, const double2* __restrict__ spec, double* __restrict__ phi,
+             const double2* __restrict__ twN, const double2* __restrict__ post, double scale, int padded,
+             unsigned int* __restrict__ err) {
+    xb_tma_body<N>(nrows, ny, RowsContig{spec}, phi, twN, post, scale, padded, err);
+}
+
+// the same inverse with the rows gathered from the ranks' x-slabs
+template <int N>
+__global__ void __launch_bounds__(XT<N>::P, XT<N>::MINB)
+    k_xb_tma_gather(int nrows, int ny, const __grid_constant__ XtGather gt, double* __restrict__ phi,
+                    const double2* __restrict__ twN, const double2* __restrict__ post, double scale,
+                    unsigned int* __restrict__ err) {
+    xb_tma_body<N>(nrows, ny, RowsGathered{&gt, ny}, phi, twN, post, scale, 0, err);
 }
 
 // The inverse of the FP32 storage form: float2 spectrum rows in, float phi
@@ -617,6 +657,7 @@ void xt_tma_init() {
     cudaFuncSetAttribute(k_xb_tma<n>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)XT<n>::smem);          \
     cudaFuncSetAttribute(k_xb_tma32<n>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)XT<n>::smem);        \
     cudaFuncSetAttribute(k_xf_tma<n>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)XT<n>::smem);       \
+    cudaFuncSetAttribute(k_xb_tma_gather<n>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)XT<n>::smem);\
     cudaFuncSetAttribute(k_xf_div<n, double, double2>, cudaFuncAttributeMaxDynamicSharedMemorySize,          \
                          (int)XD<n>::smem);                                                                    \
     cudaFuncSetAttribute(k_xf_div<n, float, float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)XD<n>::smem);
@@ -647,6 +688,21 @@ void launch_xb_tma(cudaStream_t st, int nx, int ny, int nz, const float2* spec, 
     case n:                                                                                                    \
         launch_pdl(k_xb_tma32<n>, dim3(xt_grid<n>(nrows, nsm)), dim3(XT<n>::P), XT<n>::smem, st, nrows, ny,   \
                    spec, phi, twx, post, scale, padded, err);                                                  \
+        break;
+        XT_SIZES(X_CASE)
+#undef X_CASE
+        default: break;
+    }
+}
+
+void launch_xb_tma_gather(cudaStream_t st, int nx, int ny, int nz, const XtGather& gt, double* phi, const double2* twx,
+                          const double2* post, double scale, int nsm, unsigned int* err) {
+    const int nrows = ny * nz;
+    switch (nx / 2) {
+#define X_CASE(n)                                                                                              \
+    case n:                                                                                                    \
+        launch_pdl(k_xb_tma_gather<n>, dim3(xt_grid<n>(nrows, nsm)), dim3(XT<n>::P), XT<n>::smem, st, nrows, ny, \
+                   gt, phi, twx, post, scale, err);                                                            \
         break;
         XT_SIZES(X_CASE)
 #undef X_CASE

@@ -151,6 +151,16 @@ void launch_zt_tma(cudaStream_t st, int dir, int ncol, int nz, const void* tmap,
 // k_pfft_xt.cu: x transforms fed by bulk copies (persistent CTAs, two stages);
 // row pointers must be 16-byte aligned
 bool xt_tma_supported(int n);
+// the x-slabs of the ranks of a z-slab decomposition (device addresses,
+// mapped here where they are other GPUs' memory), this rank's first plane
+struct XtGather {
+    const double2* p[64];
+    int G, k0;
+};
+// the inverse x transform of this rank's planes, its spectrum rows gathered
+// from the x-slabs (compact phi rows)
+void launch_xb_tma_gather(cudaStream_t st, int nx, int ny, int nz, const XtGather& gt, double* phi, const double2* twx,
+                          const double2* post, double scale, int nsm, unsigned int* err);
 void xt_tma_init();
 void launch_xb_tma(cudaStream_t st, int nx, int ny, int nz, const double2* spec, double* phi, const double2* twx,
                    const double2* post, double scale, int padded, int nsm, unsigned int* err);

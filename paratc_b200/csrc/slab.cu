@@ -97,6 +97,7 @@ __global__ void __launch_bounds__(256) k_slab_pack(int dir, int nzl, int ny, int
 struct SlabPeers {
     double2* p[PARATC_SLAB_MAX_RANKS];
 };
+static_assert(PARATC_SLAB_MAX_RANKS <= sizeof(XtGather::p) / sizeof(XtGather::p[0]), "gather table size");
 
 // dir 0: scatter the local planes' spectrum into every rank's x-slab;
 // dir 1: gather it back.  Value (kl, jc, kx) of this rank (planes from k0)
@@ -387,11 +388,20 @@ extern "C" int paratc_slab_backward_peers(paratc_slab* s, const double* const* x
     cudaSetDevice(s->dev);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const size_t n = (size_t)s->nzl * s->ny * s->M1;
-    k_slab_scatter<<<grid_blocks(n, s->nsm), 256, 0, st>>>(1, s->nzl, s->ny, s->M1, s->nranks, s->k0, s->d_spec, pp);
-    if (s->xt && aligned16(d_phi))
-        launch_xb_tma(st, s->nx, s->ny, s->nzl, s->d_spec, d_phi, s->twx, s->postx, s->normfft, 0, s->nsm, s->d_err);
-    else
+    if (s->xt && aligned16(d_phi)) {
+        // the inverse x transform loads its rows' segments straight from the
+        // x-slabs (bulk copies, peer memory included): gather and transform
+        // in one kernel
+        XtGather gt{};
+        for (int q = 0; q < s->nranks; q++) gt.p[q] = pp.p[q];
+        gt.G = s->nranks;
+        gt.k0 = s->k0;
+        launch_xb_tma_gather(st, s->nx, s->ny, s->nzl, gt, d_phi, s->twx, s->postx, s->normfft, s->nsm, s->d_err);
+    } else {
+        k_slab_scatter<<<grid_blocks(n, s->nsm), 256, 0, st>>>(1, s->nzl, s->ny, s->M1, s->nranks, s->k0, s->d_spec,
+                                                               pp);
         launch_fft_x_c2r(st, s->nx, s->ny, s->nzl * s->ny, s->d_spec, d_phi, s->plx, s->twx, s->postx, s->normfft, 0);
+    }
     return slab_finish("paratc_slab_backward_peers");
 }
 
