@@ -355,10 +355,35 @@ __global__ void __launch_bounds__(XT<N>::P, XT<N>::MINB)
     if (tid == 0 && s_bad) xt_fail(mbar, it, nb, err);
 }
 
-template <int N>
-__global__ void __launch_bounds__(XT<N>::P, XT<N>::MINB)
-    k_xf_tma(int nrows, const double* __restrict__ src, double2* __restrict__ spec, const double2* __restrict__ twN,
-             const double2* __restrict__ post, unsigned int* __restrict__ err) {
+// Where the forward sends spectrum row g: one contiguous row of the spectrum
+// by bulk stores from thread 0 (RowsToSpec), or every mode straight into its
+// owner's x-slab of a z-slab decomposition by plain stores of all threads
+// (RowsScattered: mode kx of local row g = (kl, jc) to rank q's x-slab at
+// ((k0*ny + g)*nxl_q + kx - kx0_q); the x-slabs may be other GPUs' memory,
+// written over NVLink).  `bulk` tells the kernel which of the two it is.
+struct RowsToSpec {
+    static constexpr bool bulk = true;
+    double2* spec;
+    __device__ __forceinline__ void store(int g, const double2* row, int M1) const {
+        tma::bulk_store(spec + (size_t)g * M1, row, M1 * (unsigned)sizeof(double2));
+    }
+};
+struct RowsScattered {
+    static constexpr bool bulk = false;
+    const XtGather* t;  // the kernel's __grid_constant__ parameter (pointers written through)
+    int ny;
+    __device__ __forceinline__ void put(int g, int kx, double2 v, int M1) const {
+        const int G = t->G, base = M1 / G, rem = M1 - base * G, cut = rem * (base + 1);
+        const int q = kx < cut ? kx / (base + 1) : rem + (kx - cut) / base;
+        const int kx0 = q * base + (q < rem ? q : rem), nxl = base + (q < rem ? 1 : 0);
+        const_cast<double2*>(t->p[q])[((size_t)t->k0 * ny + g) * nxl + (kx - kx0)] = v;
+    }
+};
+
+template <int N, class Out>
+__device__ __forceinline__ void xf_tma_body(int nrows, const double* __restrict__ src, const Out& out,
+                                            const double2* __restrict__ twN, const double2* __restrict__ post,
+                                            unsigned int* __restrict__ err) {
     constexpr int B = XT<N>::B, P = XT<N>::P, PITCH = XT<N>::PITCH, M1 = N + 1;
     constexpr unsigned SB = XT<N>::STAGE;
     constexpr ff::Sched SC = ff::make_sched(N);
@@ -423,24 +448,52 @@ __global__ void __launch_bounds__(XT<N>::P, XT<N>::MINB)
                 rb[a] = xa;
             }
         }
-        tma::fence_async_smem();
-        __syncthreads();
-        if (tid == 0) {
-            const int g0 = bt * B, nv = min(B, nrows - g0);
-            for (int b = 0; b < nv; b++)
-                tma::bulk_store(spec + (size_t)(g0 + b) * M1, buf + b * PITCH, M1 * (unsigned)sizeof(double2));
-            tma::bulk_commit();
-            const int bn = bt + 2 * gridDim.x;
-            if (bn < nb) {
-                tma::bulk_wait_read0();
-                issue(s, bn);
+        if constexpr (Out::bulk) {
+            tma::fence_async_smem();
+            __syncthreads();
+            if (tid == 0) {
+                const int g0 = bt * B, nv = min(B, nrows - g0);
+                for (int b = 0; b < nv; b++) out.store(g0 + b, buf + b * PITCH, M1);
+                tma::bulk_commit();
+                const int bn = bt + 2 * gridDim.x;
+                if (bn < nb) {
+                    tma::bulk_wait_read0();
+                    issue(s, bn);
+                }
             }
+        } else {
+            __syncthreads();
+            const int g0 = bt * B, nv = min(B, nrows - g0);
+            for (int f = tid; f < nv * M1; f += P) {
+                const int b = f / M1, kx = f - b * M1;
+                out.put(g0 + b, kx, buf[b * PITCH + kx], M1);
+            }
+            tma::fence_async_smem();  // this thread's stage accesses before the refill's async writes
+            __syncthreads();          // every thread has read the stage before it is refilled
+            const int bn = bt + 2 * gridDim.x;
+            if (tid == 0 && bn < nb) issue(s, bn);
         }
     }
     if (tid == 0) {
         tma::bulk_wait0();
         if (s_bad) xt_fail(mbar, it, nb, err);
     }
+}
+
+template <int N>
+__global__ void __launch_bounds__(XT<N>::P, XT<N>::MINB)
+    k_xf_tma(int nrows, const double* __restrict__ src, double2* __restrict__ spec, const double2* __restrict__ twN,
+             const double2* __restrict__ post, unsigned int* __restrict__ err) {
+    xf_tma_body<N>(nrows, src, RowsToSpec{spec}, twN, post, err);
+}
+
+// the same forward transform with every mode stored straight into its
+// owner's x-slab
+template <int N>
+__global__ void __launch_bounds__(XT<N>::P, XT<N>::MINB)
+    k_xf_tma_scatter(int nrows, int ny, const double* __restrict__ src, const __grid_constant__ XtGather gt,
+                     const double2* __restrict__ twN, const double2* __restrict__ post, unsigned int* __restrict__ err) {
+    xf_tma_body<N>(nrows, src, RowsScattered{&gt, ny}, twN, post, err);
 }
 
 // ---------------------------------------------------------------------------
@@ -658,6 +711,7 @@ void xt_tma_init() {
     cudaFuncSetAttribute(k_xb_tma32<n>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)XT<n>::smem);        \
     cudaFuncSetAttribute(k_xf_tma<n>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)XT<n>::smem);       \
     cudaFuncSetAttribute(k_xb_tma_gather<n>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)XT<n>::smem);\
+    cudaFuncSetAttribute(k_xf_tma_scatter<n>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)XT<n>::smem);\
     cudaFuncSetAttribute(k_xf_div<n, double, double2>, cudaFuncAttributeMaxDynamicSharedMemorySize,          \
                          (int)XD<n>::smem);                                                                    \
     cudaFuncSetAttribute(k_xf_div<n, float, float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)XD<n>::smem);
@@ -703,6 +757,21 @@ void launch_xb_tma_gather(cudaStream_t st, int nx, int ny, int nz, const XtGathe
     case n:                                                                                                    \
         launch_pdl(k_xb_tma_gather<n>, dim3(xt_grid<n>(nrows, nsm)), dim3(XT<n>::P), XT<n>::smem, st, nrows, ny, \
                    gt, phi, twx, post, scale, err);                                                            \
+        break;
+        XT_SIZES(X_CASE)
+#undef X_CASE
+        default: break;
+    }
+}
+
+void launch_xf_tma_scatter(cudaStream_t st, int nx, int ny, int nz, const double* src, const XtGather& gt,
+                           const double2* twx, const double2* post, int nsm, unsigned int* err) {
+    const int nrows = ny * nz;
+    switch (nx / 2) {
+#define X_CASE(n)                                                                                              \
+    case n:                                                                                                    \
+        launch_pdl(k_xf_tma_scatter<n>, dim3(xt_grid<n>(nrows, nsm)), dim3(XT<n>::P), XT<n>::smem, st, nrows,   \
+                   ny, src, gt, twx, post, err);                                                               \
         break;
         XT_SIZES(X_CASE)
 #undef X_CASE

@@ -161,6 +161,10 @@ struct XtGather {
 // from the x-slabs (compact phi rows)
 void launch_xb_tma_gather(cudaStream_t st, int nx, int ny, int nz, const XtGather& gt, double* phi, const double2* twx,
                           const double2* post, double scale, int nsm, unsigned int* err);
+// the forward x transform of this rank's planes (compact source rows), every
+// mode stored into its owner's x-slab
+void launch_xf_tma_scatter(cudaStream_t st, int nx, int ny, int nz, const double* src, const XtGather& gt,
+                           const double2* twx, const double2* post, int nsm, unsigned int* err);
 void xt_tma_init();
 void launch_xb_tma(cudaStream_t st, int nx, int ny, int nz, const double2* spec, double* phi, const double2* twx,
                    const double2* post, double scale, int padded, int nsm, unsigned int* err);

@@ -374,11 +374,19 @@ extern "C" int paratc_slab_forward_peers(paratc_slab* s, const double* d_src, co
     cudaSetDevice(s->dev);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const size_t n = (size_t)s->nzl * s->ny * s->M1;
-    if (s->xt && aligned16(d_src))
-        launch_xf_tma(st, s->nx, s->ny, s->nzl, d_src, s->d_spec, s->twx, s->postx, s->nsm, s->d_err);
-    else
+    if (s->xt && aligned16(d_src)) {
+        // transform and scatter in one kernel: the modes leave shared memory
+        // straight for their owners' x-slabs
+        XtGather gt{};
+        for (int q = 0; q < s->nranks; q++) gt.p[q] = pp.p[q];
+        gt.G = s->nranks;
+        gt.k0 = s->k0;
+        launch_xf_tma_scatter(st, s->nx, s->ny, s->nzl, d_src, gt, s->twx, s->postx, s->nsm, s->d_err);
+    } else {
         launch_fft_x_r2c(st, s->nx, s->nzl * s->ny, d_src, s->d_spec, s->plx, s->twx, s->postx);
-    k_slab_scatter<<<grid_blocks(n, s->nsm), 256, 0, st>>>(0, s->nzl, s->ny, s->M1, s->nranks, s->k0, s->d_spec, pp);
+        k_slab_scatter<<<grid_blocks(n, s->nsm), 256, 0, st>>>(0, s->nzl, s->ny, s->M1, s->nranks, s->k0, s->d_spec,
+                                                               pp);
+    }
     return slab_finish("paratc_slab_forward_peers");
 }
 
