@@ -610,8 +610,10 @@ int paratc_batch_set_mode(paratc_batch* b, int mode);
  * torch.distributed or ncclSend/ncclRecv; MPI_Alltoallv in a host code), so
  * the library links no communicator.  Buffers are device arrays of doubles
  * (complex values as (re, im) pairs): d_send and d_recv hold
- * 2*nzl*nyc*(nxc/2+1), d_xslab 2*nzc*nyc*nxl doubles.  Every call queues its
- * kernels on `stream` (a cudaStream_t, NULL = default) and returns. */
+ * 2*nzl*nyc*(nxc/2+1), d_xslab 2*nzc*nyc*nxl doubles.  Every call makes
+ * the plan's device current, queues its kernels on `stream` (a cudaStream_t,
+ * NULL = default) and returns.  Calls on one plan must not run concurrently;
+ * the plan's buffers are reused by every solve. */
 typedef struct paratc_slab paratc_slab;
 /* The balanced split of n items over nranks: rank `rank` gets [*start,
  * *start + *count), the first n % nranks ranks one item more.  Needs no
