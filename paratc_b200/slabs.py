@@ -242,6 +242,9 @@ class PeerExchange:
     def __init__(self, plan, dist, stream=None, ipc=None):
         """ipc: (get_handle(ptr) -> bytes, open(bytes) -> ptr, close(ptr)),
         the library's CUDA IPC calls by default."""
+        if dist.get_world_size() != plan.nranks or dist.get_rank() != plan.rank:
+            raise ValueError("plan of rank %d of %d in a process group of rank %d of %d"
+                             % (plan.rank, plan.nranks, dist.get_rank(), dist.get_world_size()))
         self.plan, self.dist, self.stream = plan, dist, stream
         self._ipc = ipc or (ipc_get_handle, ipc_open, ipc_close)
         own = plan.xslab_ptr
@@ -269,9 +272,12 @@ class PeerExchange:
         self._wait_all()       # every rank has read its planes back
 
     def close(self):
+        """Unmaps the other ranks' x-slabs, then waits for every rank to do
+        the same, so that a plan may free its x-slab once this returns."""
         for p in self._opened:
             self._ipc[2](p)
         self._opened = []
+        self.dist.barrier()
 
 
 def ipc_get_handle(ptr):

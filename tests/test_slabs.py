@@ -150,7 +150,6 @@ def _peer_worker(rank, ws, port, out_dir):
     pe.solve(None, None)
     dist.barrier = orig
     pe.close()
-    dist.barrier()
     dist.destroy_process_group()
     with open(os.path.join(out_dir, "peer%d.json" % rank), "w") as f:
         json.dump({"ptrs": pe.ptrs, "log": log, "opened": [h.decode() for h in opened], "closed": closed}, f)
