@@ -238,9 +238,48 @@ def cpu_baseline(case, yp, fields, seconds, max_steps=200):
             "sample": "%d full RK3 steps of %s on the C oracle (OpenMP, %d threads), %.1f s" % (n, case.name, threads, el)}
 
 
+def run_reference_poisson(args):
+    """The reference arm of the Poisson workloads: the oracle's clcPPE (FFTW-
+    style halfcomplex transforms and the Thomas sweeps, OpenMP over all host
+    threads) on the same grid and source, `steps` solves after `warmup`."""
+    from paratc_b200 import cases
+    from oracle import oracle_lib as ol
+    case = cases.poisson_c2(*args.grid) if args.grid else cases.poisson_c2()
+    p = case.params
+    m = case.mesh
+    yp = ol.ycoord(m.section_length, m.section_cstret, m.nyc_section, m.stret_type, m.stret_option, p.yly)
+    src = cases.gaussian_source(cases.Case("src", p, case.mesh, "gauss_src", 42, 1.0))
+    threads = os.cpu_count() or 1
+    o = ol.Oracle(p, yp, threads=threads)
+    for _ in range(args.warmup):
+        o.poisson(src)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        o.poisson(src)
+    el = time.perf_counter() - t0
+    o.close()
+    cells = p.nxc * p.nyc * p.nzc
+    val = cells * args.steps / el
+    unit = "grid-point Poisson solves/s"
+    line = {"impl": "reference", "metric": unit, "value": val, "unit": unit, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
+            "higher_is_better": True, "scaling": "strong" if args.workload.endswith("zslabs") else "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": case.name + ("_zslabs" if args.workload.endswith("zslabs") else ""),
+                       "grid": [p.nxc, p.nyc, p.nzc], "precision": "fp64", "parallelism": "host threads"},
+            "cpu_baseline": {"value": val, "unit": unit, "cores": threads, "kind": "port",
+                             "sample": "%d Poisson solves of %s on the C oracle (OpenMP, %d threads)"
+                                       % (args.steps, case.name, threads)},
+            "e2e": {"value": val, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
 def run_reference(args):
     ws, rank, _ = _dist()
     if rank != 0:
+        return
+    if args.workload in ("poisson_c2", "poisson_c2_zslabs"):
+        run_reference_poisson(args)
         return
     from paratc_b200 import cases
     from oracle import oracle_lib as ol
