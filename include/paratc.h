@@ -636,7 +636,8 @@ int paratc_slab_forward(paratc_slab* s, const double* d_src, double* d_send, voi
 int paratc_slab_middle(paratc_slab* s, double* d_xslab, void* stream);
 /* d_phi: the local planes of phi, nzl*nyc*nxc doubles (interior layout). */
 int paratc_slab_backward(paratc_slab* s, const double* d_recv, double* d_phi, void* stream);
-/* Peer form: no collective library.  Each plan owns an x-slab
+/* Peer form: no collective library; replaces the same transposes as the
+ * all-to-all form (src/m_Decomp2d.f90:585-1000).  Each plan owns an x-slab
  * (paratc_slab_xslab, 2*nzc*nyc*nxl doubles); xslabs[q] (nranks device
  * pointers, host array) is rank q's, this rank's own included, mapped here
  * with paratc_ipc_open when q is another process.  forward_peers transforms
@@ -653,7 +654,8 @@ int paratc_slab_forward_peers(paratc_slab* s, const double* d_src, const double*
 int paratc_slab_backward_peers(paratc_slab* s, const double* const* xslabs, double* d_phi, void* stream);
 /* CUDA IPC of a device allocation's base address (cudaIpcGetMemHandle /
  * cudaIpcOpenMemHandle with lazy peer access): the handle is
- * PARATC_IPC_HANDLE_BYTES opaque bytes to send to the other processes. */
+ * PARATC_IPC_HANDLE_BYTES opaque bytes to send to the other processes.  No
+ * counterpart in the reference, whose ranks exchange only through MPI. */
 #define PARATC_IPC_HANDLE_BYTES 64
 int paratc_ipc_get_handle(const void* d_ptr, void* handle);
 int paratc_ipc_open(const void* handle, void** d_ptr);
