@@ -172,3 +172,22 @@ def test_peer_exchange_over_gloo_ranks(tmp_path):
         kinds = [e[0] for e in res["log"]]
         assert kinds == ["forward", "sync", "barrier", "middle", "sync", "barrier", "backward", "sync", "barrier"]
         assert res["log"][0][1] == want and res["log"][6][1] == want
+
+
+def test_local_exchange_moves_rank_ordered_blocks():
+    """slabs.LocalExchange.all_to_all (the one-process exchange of the GPU
+    tests) on CPU tensors: block r -> q lands at q's offset for r."""
+    import torch
+    nx, ny, nz, g = 20, 3, 7, 3
+    counts = [slabs.slab_counts(nx, ny, nz, g, r) for r in range(g)]
+    sends = [torch.arange(sum(c[0]), dtype=torch.float64) + 1000.0 * r for r, c in enumerate(counts)]
+    recvs = [torch.full((sum(c[1]),), -1.0, dtype=torch.float64) for c in counts]
+    slabs.LocalExchange.all_to_all(sends, recvs, [c[0] for c in counts], [c[1] for c in counts])
+    for q in range(g):
+        off = 0
+        for r in range(g):
+            n = counts[q][1][r]
+            so = sum(counts[r][0][:q])
+            assert torch.equal(recvs[q][off:off + n], sends[r][so:so + n])
+            off += n
+        assert off == recvs[q].numel()
